@@ -1,0 +1,113 @@
+# SPDX-License-Identifier: Apache-2.0
+"""ctypes binding of liballoy_dfsph.so (include/alloy_dfsph.h). There is no fallback: if the library is missing or
+does not load, ``lib()`` raises."""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "liballoy_dfsph.so"
+
+ADF_OK, ADF_ERR_VALUE, ADF_ERR_CAPACITY, ADF_ERR_CUDA, ADF_ERR_STATE = 0, 1, 2, 3, 4
+
+# every entry point of include/alloy_dfsph.h
+EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_density_ratio", "adf_get_report",
+           "adf_active_mass", "adf_get_warm_starts", "adf_set_warm_starts", "adf_state_arrays", "adf_reset",
+           "adf_add_emitter", "adf_set_emitter_pool", "adf_emitter_state", "adf_set_emitter_enabled", "adf_add_sink",
+           "adf_neighbor_rows", "adf_debug_field", "adf_world_sum", "adf_kernel_launches", "adf_profile_enable",
+           "adf_profile_read", "adf_list_stats")
+PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
+              "apply", "xsph", "finish", "emit")
+
+
+class Params(C.Structure):
+    """adf_params"""
+    _fields_ = [("kind", C.c_int), ("particle_radius", C.c_double), ("h", C.c_double), ("sigma", C.c_double),
+                ("n_full", C.c_double), ("tot_min", C.c_double), ("lattice_grad", C.c_double),
+                ("wall_offset", C.c_double), ("wall_amplitude", C.c_double), ("taper0", C.c_double),
+                ("taper1", C.c_double), ("reach", C.c_double), ("tol_den", C.c_double), ("tol_div", C.c_double),
+                ("max_error_factor", C.c_double), ("min_it", C.c_int), ("max_it", C.c_int), ("omega", C.c_double),
+                ("warm_den", C.c_double), ("warm_div", C.c_double), ("min_nb", C.c_double),
+                ("divergence_solve", C.c_int), ("two_sided", C.c_int), ("xsph_c", C.c_double),
+                ("capacity", C.c_int), ("v_sep", C.c_double), ("relief_speed", C.c_double),
+                ("project_eps", C.c_double), ("has_bounds", C.c_int), ("bounds_lo", C.c_double * 3),
+                ("bounds_hi", C.c_double * 3)]
+
+
+class ModelDesc(C.Structure):
+    """adf_model"""
+    _fields_ = [("n", C.c_int), ("world_count", C.c_int), ("world_start", C.POINTER(C.c_int32)),
+                ("q_host", C.POINTER(C.c_float)), ("mass", C.c_void_p), ("rest_density", C.c_void_p),
+                ("radius", C.c_void_p), ("flags", C.c_void_p), ("phase", C.c_void_p), ("world", C.c_void_p),
+                ("gravity", C.c_void_p)]
+
+
+class Report(C.Structure):
+    """adf_report"""
+    _fields_ = [(name, C.c_void_p) for name in (
+        "density_err", "divergence_err", "iters_density", "iters_divergence", "mass_in", "mass_out", "mass_initial",
+        "escaped", "neighbor_overflow", "max_speed", "density_err_max", "projected", "nonfinite", "emitter_overflow",
+        "density_tol")]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load (once) and declare the library. Raises when it is missing: this package has no CPU fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"liballoy_dfsph.so not found at {LIB_PATH}; build it with `python -m alloy_b200.build`")
+    L = C.CDLL(str(LIB_PATH))
+    P, vp, i = C.c_void_p, C.c_void_p, C.c_int
+    L.adf_last_error.restype = C.c_char_p
+    L.adf_create.argtypes = [C.POINTER(Params), C.POINTER(ModelDesc), i, C.POINTER(P)]
+    L.adf_destroy.argtypes = [P]
+    L.adf_destroy.restype = None
+    L.adf_step.argtypes = [P, vp, vp, vp, vp, vp, C.c_double, vp]
+    L.adf_density_ratio.argtypes = [P, vp, vp, vp, vp, vp]
+    L.adf_get_report.argtypes = [P, C.POINTER(Report), vp]
+    L.adf_active_mass.argtypes = [P, vp, vp]
+    L.adf_get_warm_starts.argtypes = [P, vp, vp, vp]
+    L.adf_set_warm_starts.argtypes = [P, vp, vp, vp]
+    L.adf_state_arrays.argtypes = [P, C.POINTER(vp), C.POINTER(vp)]
+    L.adf_reset.argtypes = [P, vp, vp, vp, vp]
+    L.adf_add_emitter.argtypes = [P, i, vp, vp, i, vp, C.c_float, vp, i]
+    L.adf_set_emitter_pool.argtypes = [P, i, vp, i]
+    L.adf_emitter_state.argtypes = [P, vp, vp]
+    L.adf_set_emitter_enabled.argtypes = [P, i, i]
+    L.adf_add_sink.argtypes = [P, i, vp, vp]
+    L.adf_neighbor_rows.argtypes = [P, vp, vp, vp]
+    L.adf_debug_field.argtypes = [P, C.c_char_p, vp, vp]
+    L.adf_world_sum.argtypes = [P, vp, vp, vp, vp]
+    L.adf_kernel_launches.argtypes = [P]
+    L.adf_kernel_launches.restype = C.c_int64
+    L.adf_profile_enable.argtypes = [P, i]
+    L.adf_profile_read.argtypes = [P, vp, vp]
+    L.adf_list_stats.argtypes = [P, vp, vp, vp]
+    for name in EXPORTS:
+        if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+class CapacityError(RuntimeError):
+    """A fixed capacity was exceeded (alloy.core.errors.CapacityError's role)."""
+
+
+def check(rc: int, what: str = "") -> int:
+    """Map an ADF status code to the reference's exception types."""
+    if rc >= 0 and rc == ADF_OK:
+        return rc
+    code = -rc if rc < 0 else rc
+    msg = lib().adf_last_error().decode(errors="replace")
+    text = f"{what}: {msg}" if what and msg and not msg.startswith(what) else (msg or what)
+    if code == ADF_ERR_VALUE:
+        raise ValueError(text)
+    if code == ADF_ERR_CAPACITY:
+        raise CapacityError(text)
+    raise RuntimeError(f"liballoy_dfsph error {code}: {text}")

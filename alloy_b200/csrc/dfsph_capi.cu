@@ -1,0 +1,909 @@
+// SPDX-License-Identifier: Apache-2.0
+// C ABI of the B200 DFSPH step (include/alloy_dfsph.h): the solver object, its fixed-capacity device memory and the
+// per-step launch sequence (solver.py:218-268 order). Pressure solves run their iterations with a one-ahead host
+// check: iteration k+1 is enqueued before the host reads iteration k's unconverged-world count, so the GPU never
+// idles on the read; an iteration enqueued after every world converged changes nothing (converged worlds skip every
+// kernel, pressure.py:289-290, 326-327).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/alloy_dfsph.h"
+#include "dfsph_kernels.cuh"
+
+using namespace adf;
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(x)                                                                               \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) return fail(ADF_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+inline int blocks(long long n, int b = BLOCK) { return (int)((n + b - 1) / b); }
+
+template <class T> int dalloc(T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(count, 1));
+  if (e != cudaSuccess) return fail(ADF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return ADF_OK;
+}
+}  // namespace
+
+struct adf_solver {
+  adf_params prm;
+  int n = 0, W = 0, K = 64, device = 0;
+  std::vector<int> ws_host;
+  std::vector<WorldGrid> grids;
+  std::vector<int> world_cells_h;
+  int total_cells = 0, n_keys = 0, n_tiles = 0;
+  DevP d{};
+  std::vector<void*> owned;
+  int* world_cells = nullptr;
+  int* tile_sums = nullptr;
+  // per-world statistics outside DevP
+  int *iters_den = nullptr, *iters_div = nullptr, *emit_overflow = nullptr;
+  float *den_err = nullptr, *div_err = nullptr, *den_err_max = nullptr, *den_tol = nullptr;
+  long long *mass_in = nullptr, *mass0 = nullptr, *tmp_mass = nullptr;
+  uint8_t* mask_d = nullptr;
+  // emitters and sinks
+  std::vector<Emit> em_h;
+  std::vector<float> off_local_h;
+  std::vector<int> off_emitter_h, off_rank_h, pool_h;
+  std::vector<int> enabled_h;
+  Emit* em_d = nullptr;
+  float* off_local_d = nullptr;
+  int *off_emitter_d = nullptr, *off_rank_d = nullptr, *pool_d = nullptr, *enabled_d = nullptr;
+  int *cursor_d = nullptr, *emit_now_d = nullptr;
+  float* t_acc_d = nullptr;
+  std::vector<Sink> sinks_h;
+  Sink* sinks_d = nullptr;
+  // host side of the iteration loop
+  int* pinned = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  long long launches = 0;
+  bool built = false;  // a step or density_ratio ran (lists exist)
+  // live kernel timing (adf_profile_enable)
+  bool prof_on = false;
+  std::vector<cudaEvent_t> prof_pool;
+  std::vector<std::pair<int, int>> prof_marks;  // (kind, first event of the pair)
+  size_t prof_used = 0;
+  int prof_open = -1;
+  long long* list_entries = nullptr;
+
+  template <class T> int alloc(T** p, size_t count) {
+    int rc = dalloc(p, count);
+    if (rc == ADF_OK) owned.push_back((void*)*p);
+    return rc;
+  }
+};
+
+namespace {
+
+#define LAUNCH(s, kern, grid, block, stream, ...)          \
+  do {                                                     \
+    kern<<<(grid), (block), 0, (cudaStream_t)(stream)>>>(__VA_ARGS__); \
+    ++(s)->launches;                                       \
+  } while (0)
+
+void prof_begin(adf_solver* s, int kind, cudaStream_t st) {
+  if (!s->prof_on || s->prof_used + 2 > s->prof_pool.size()) return;
+  int e = (int)s->prof_used;
+  s->prof_used += 2;
+  cudaEventRecord(s->prof_pool[e], st);
+  s->prof_marks.push_back({kind, e});
+  s->prof_open = e;
+}
+
+void prof_end(adf_solver* s, cudaStream_t st) {
+  if (s->prof_open < 0) return;
+  cudaEventRecord(s->prof_pool[s->prof_open + 1], st);
+  s->prof_open = -1;
+}
+
+int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ADF_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return ADF_OK;
+}
+
+// Per-world cell grids over each world's start-state bounding box with a margin; cells are 1.001 h wide (every pair
+// closer than h lies in adjacent cells despite float rounding of the cell coordinate) and coarser only where a
+// world's box would need more than 2^25 cells. Particles outside a grid are clamped into its border cells, which
+// keeps every neighbour query exact.
+void size_grids(adf_solver* s, const float* q_host) {
+  const double cw0 = 1.001 * s->prm.h;
+  s->grids.assign(s->W, WorldGrid{});
+  s->world_cells_h.assign(s->W, 0);
+  long long base = 0;
+  for (int w = 0; w < s->W; ++w) {
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool any = false;
+    for (int i = s->ws_host[w]; i < s->ws_host[w + 1] && q_host; ++i) {
+      for (int a = 0; a < 3; ++a) {
+        double x = q_host[3 * i + a];
+        if (!std::isfinite(x)) continue;
+        if (!any) { lo[a] = hi[a] = x; }
+        lo[a] = std::min(lo[a], x);
+        hi[a] = std::max(hi[a], x);
+      }
+      any = true;
+    }
+    double cw = cw0;
+    int dim[3];
+    for (;;) {
+      double cells = 1.0;
+      for (int a = 0; a < 3; ++a) {
+        double margin = 4.0 * cw + 0.1 * (hi[a] - lo[a]);
+        dim[a] = (int)std::ceil((hi[a] - lo[a] + 2.0 * margin) / cw) + 1;
+        cells *= dim[a];
+      }
+      if (cells <= 33554432.0) break;
+      cw *= 1.5;
+    }
+    WorldGrid g;
+    g.inv_cw = (float)(1.0 / cw);
+    double m0 = 4.0 * cw + 0.1 * (hi[0] - lo[0]), m1 = 4.0 * cw + 0.1 * (hi[1] - lo[1]),
+           m2 = 4.0 * cw + 0.1 * (hi[2] - lo[2]);
+    g.ox = (float)(lo[0] - m0);
+    g.oy = (float)(lo[1] - m1);
+    g.oz = (float)(lo[2] - m2);
+    g.nx = dim[0];
+    g.ny = dim[1];
+    g.nz = dim[2];
+    g.base = (int)base;
+    s->grids[w] = g;
+    s->world_cells_h[w] = dim[0] * dim[1] * dim[2];
+    base += s->world_cells_h[w];
+  }
+  s->total_cells = (int)base;
+}
+
+void set_solve_params(adf_solver* s, DevP& P, int mode, double dt) {
+  const adf_params& p = s->prm;
+  P.mode = mode;
+  P.dt = (float)dt;
+  P.warm = (float)(mode == 0 ? p.warm_div : p.warm_den);
+  double tol = mode == 0 ? p.tol_div : p.tol_den;
+  P.tol = (float)tol;
+  P.tol_max = (float)(tol * p.max_error_factor);
+  P.relief = (mode == 1 && p.relief_speed > 0.0) ? (float)(p.relief_speed * dt * p.lattice_grad) : (float)(1.0e30);
+}
+
+int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
+  const int n = s->n;
+  prof_begin(s, 0, st);
+  LAUNCH(s, k_classify, blocks(n), BLOCK, st, P);
+  LAUNCH(s, k_scan_tiles, s->n_tiles, SCAN_THREADS, st, P.counts, s->n_keys, s->tile_sums);
+  LAUNCH(s, k_scan_tile_sums, 1, SCAN_THREADS, st, s->tile_sums, s->n_tiles);
+  LAUNCH(s, k_scan_apply, s->n_tiles, SCAN_THREADS, st, P.counts, s->n_keys, s->tile_sums, P.cell_start);
+  LAUNCH(s, k_post_scan, blocks(std::max(s->W, 1)), BLOCK, st, P, s->world_cells);
+  LAUNCH(s, k_scatter, blocks(n), BLOCK, st, P);
+  prof_end(s, st);
+  prof_begin(s, 1, st);
+  LAUNCH(s, k_lists, blocks(n), BLOCK, st, P);
+  prof_end(s, st);
+  prof_begin(s, 2, st);
+  LAUNCH(s, k_wall_slots, blocks(n), BLOCK, st, P);
+  prof_end(s, st);
+  prof_begin(s, 3, st);
+  LAUNCH(s, k_density_alpha, blocks(n), BLOCK, st, P);
+  prof_end(s, st);
+  s->built = true;
+  return check_launch();
+}
+
+void enqueue_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
+  const int n = s->n;
+  prof_begin(s, 5, st);
+  LAUNCH(s, k_accel, blocks(n), BLOCK, st, P);
+  prof_end(s, st);
+  prof_begin(s, 6, st);
+  LAUNCH(s, k_jacobi, blocks(n), BLOCK, st, P);
+  prof_end(s, st);
+  prof_begin(s, 7, st);
+  if (P.n_chunks > 0)
+    LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, P.err_orig, P.chunk_begin, P.chunk_end, P.part_sum, P.part_max,
+           P.n_unconv);
+  else
+    cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
+  if (s->W > 0) LAUNCH(s, k_world_check, s->W, 256, st, P, 1, (double*)nullptr, (float*)nullptr);
+  prof_end(s, st);
+}
+
+// pressure.py:355-390 + solve_driver.py:121-186 (Jacobi branch) + pressure.py:393-480
+int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st) {
+  set_solve_params(s, P, mode, dt);
+  const int n = s->n, W = s->W;
+  CK(cudaMemsetAsync(P.err_orig, 0, sizeof(float) * n, st));
+  CK(cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st));
+  prof_begin(s, 4, st);
+  LAUNCH(s, k_solve_init, blocks(n), BLOCK, st, P);
+  prof_end(s, st);
+  if (W > 0) LAUNCH(s, k_begin_solve, blocks(W), BLOCK, st, P);
+  int rc = check_launch();
+  if (rc) return rc;
+  const int limit = s->prm.max_it + 2;
+  enqueue_iteration(s, P, st);
+  CK(cudaMemcpyAsync(&s->pinned[0], P.n_unconv, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(s->ev[0], st));
+  for (int it = 1;; ++it) {
+    if (it < limit) {
+      enqueue_iteration(s, P, st);
+      CK(cudaMemcpyAsync(&s->pinned[it & 1], P.n_unconv, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaEventRecord(s->ev[it & 1], st));
+    }
+    CK(cudaEventSynchronize(s->ev[(it - 1) & 1]));
+    if (s->pinned[(it - 1) & 1] == 0 || it >= limit) break;
+  }
+  rc = check_launch();
+  if (rc) return rc;
+  prof_begin(s, 8, st);
+  LAUNCH(s, k_apply, blocks(n), BLOCK, st, P);
+  prof_end(s, st);
+  if (mode == 0) {
+    CK(cudaMemcpyAsync(s->iters_div, P.iters, sizeof(int) * W, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->div_err, P.err_mean, sizeof(float) * W, cudaMemcpyDeviceToDevice, st));
+  } else {
+    CK(cudaMemcpyAsync(s->iters_den, P.iters, sizeof(int) * W, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->den_err, P.err_mean, sizeof(float) * W, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(s->den_err_max, P.emax, sizeof(float) * W, cudaMemcpyDeviceToDevice, st));
+  }
+  return check_launch();
+}
+
+// Re-upload the emitter tables; the layer clocks and cursors of the first n_carry emitters are kept.
+int upload_emitters(adf_solver* s, int n_carry) {
+  int n_old = 0;
+  std::vector<float> t_old;
+  std::vector<int> c_old;
+  if (s->em_d) {
+    n_old = n_carry;
+    t_old.resize(n_old);
+    c_old.resize(n_old);
+    if (n_old > 0) {
+      CK(cudaMemcpy(t_old.data(), s->t_acc_d, sizeof(float) * n_old, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(c_old.data(), s->cursor_d, sizeof(int) * n_old, cudaMemcpyDeviceToHost));
+    }
+    void* olds[] = {s->em_d, s->off_local_d, s->off_emitter_d, s->off_rank_d, s->pool_d, s->enabled_d, s->cursor_d,
+                    s->emit_now_d, s->t_acc_d};
+    for (void* p : olds) cudaFree(p);
+  }
+  int ne = (int)s->em_h.size();
+  int no = (int)s->off_emitter_h.size();
+  int rc = dalloc(&s->em_d, ne) | dalloc(&s->off_local_d, 3 * (size_t)no) | dalloc(&s->off_emitter_d, no) |
+           dalloc(&s->off_rank_d, no) | dalloc(&s->pool_d, s->pool_h.size()) | dalloc(&s->enabled_d, ne) |
+           dalloc(&s->cursor_d, ne) | dalloc(&s->emit_now_d, ne) | dalloc(&s->t_acc_d, ne);
+  if (rc) return fail(ADF_ERR_CUDA, "emitter tables: cudaMalloc failed");
+  std::vector<float> t(ne, 0.0f);
+  std::vector<int> c(ne, 0);
+  for (int e = 0; e < n_old; ++e) { t[e] = t_old[e]; c[e] = c_old[e]; }
+  CK(cudaMemcpy(s->em_d, s->em_h.data(), sizeof(Emit) * ne, cudaMemcpyHostToDevice));
+  if (no) {
+    CK(cudaMemcpy(s->off_local_d, s->off_local_h.data(), sizeof(float) * 3 * no, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->off_emitter_d, s->off_emitter_h.data(), sizeof(int) * no, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->off_rank_d, s->off_rank_h.data(), sizeof(int) * no, cudaMemcpyHostToDevice));
+  }
+  if (!s->pool_h.empty())
+    CK(cudaMemcpy(s->pool_d, s->pool_h.data(), sizeof(int) * s->pool_h.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->enabled_d, s->enabled_h.data(), sizeof(int) * ne, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->cursor_d, c.data(), sizeof(int) * ne, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->t_acc_d, t.data(), sizeof(float) * ne, cudaMemcpyHostToDevice));
+  return ADF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* adf_last_error(void) { return g_err.c_str(); }
+
+int adf_create(const adf_params* params, const adf_model* m, int device, adf_solver** out) {
+  if (!params || !m || !out) return fail(ADF_ERR_VALUE, "adf_create: null argument");
+  *out = nullptr;
+  const adf_params& p = *params;
+  if (m->n < 0 || m->world_count < 0) return fail(ADF_ERR_VALUE, "adf_create: negative sizes");
+  if (p.capacity < 8 || p.capacity > MAXCAP)
+    return fail(ADF_ERR_VALUE, "neighbor_capacity must be in [8, " + std::to_string(MAXCAP) + "], got " +
+                                   std::to_string(p.capacity));
+  if (!(p.h > 0.0) || !(p.particle_radius > 0.0)) return fail(ADF_ERR_VALUE, "particle_radius and h must be > 0");
+  if (p.kind != 0 && p.kind != 1) return fail(ADF_ERR_VALUE, "kernel must be 0 (cubic) or 1 (wendland_c2)");
+  if (!m->world_start) return fail(ADF_ERR_VALUE, "world_start is required");
+  for (int w = 0; w < m->world_count; ++w)
+    if (m->world_start[w + 1] < m->world_start[w])
+      return fail(ADF_ERR_VALUE, "particles must be contiguous per world (Model.particle_world sorted)");
+  if (m->world_count > 0 && (m->world_start[0] < 0 || m->world_start[m->world_count] > m->n))
+    return fail(ADF_ERR_VALUE, "world_start out of range");
+  if (m->n > 0 && (!m->mass || !m->rest_density || !m->radius || !m->flags || !m->phase || !m->world || !m->gravity))
+    return fail(ADF_ERR_VALUE, "adf_create: a model array is null");
+  CK(cudaSetDevice(device));
+  adf_solver* s = new adf_solver();
+  s->prm = p;
+  s->n = m->n;
+  s->W = m->world_count;
+  s->K = p.capacity;
+  s->device = device;
+  s->ws_host.assign(m->world_start, m->world_start + m->world_count + 1);
+  if (s->W == 0) s->ws_host.assign(1, 0);
+  size_grids(s, m->q_host);
+  const int n = std::max(s->n, 1), W = std::max(s->W, 1);
+  s->n_keys = 2 * s->total_cells;
+  s->n_tiles = std::max((s->n_keys + SCAN_TILE - 1) / SCAN_TILE, 1);
+
+  DevP& d = s->d;
+  d.kc = make_kc(p.kind, p.h, p.sigma);
+  d.n = s->n;
+  d.W = s->W;
+  d.K = s->K;
+  d.total_cells = s->total_cells;
+  d.n_full = (float)p.n_full;
+  d.tot_min = (float)p.tot_min;
+  d.wall_offset = (float)p.wall_offset;
+  d.wall_amp = (float)p.wall_amplitude;
+  d.taper0 = (float)p.taper0;
+  d.taper1 = (float)p.taper1;
+  d.reach = (float)p.reach;
+  d.omega = (float)p.omega;
+  d.warm_den = (float)p.warm_den;
+  d.min_nb = (float)p.min_nb;
+  d.xsph_c = (float)p.xsph_c;
+  d.v_sep = (float)p.v_sep;
+  d.eps = (float)p.project_eps;
+  d.two_sided = p.two_sided;
+  d.min_it = p.min_it;
+  d.max_it = p.max_it;
+  d.has_bounds = p.has_bounds;
+  for (int a = 0; a < 3; ++a) {
+    d.blo[a] = (float)p.bounds_lo[a];
+    d.bhi[a] = (float)p.bounds_hi[a];
+  }
+  d.mass = m->mass;
+  d.rho0 = m->rest_density;
+  d.flags = m->flags;
+  d.phase = m->phase;
+  d.world = m->world;
+  d.gravity = m->gravity;
+
+  // chunk table of the per-world reductions (reduce.py:167-182)
+  std::vector<int> cb, ce, cs(1, 0);
+  for (int w = 0; w < s->W; ++w) {
+    for (int b = s->ws_host[w]; b < s->ws_host[w + 1]; b += 256) {
+      cb.push_back(b);
+      ce.push_back(std::min(b + 256, s->ws_host[w + 1]));
+    }
+    cs.push_back((int)cb.size());
+  }
+  d.n_chunks = (int)cb.size();
+
+  int rc = 0;
+  float* wall_vol = nullptr;
+  WorldGrid* grid = nullptr;
+  int *chunk_begin = nullptr, *chunk_end = nullptr, *world_chunk_start = nullptr;
+  rc |= s->alloc(&wall_vol, n);
+  rc |= s->alloc(&grid, W);
+  rc |= s->alloc(&s->world_cells, W);
+  rc |= s->alloc(&d.key_of, n);
+  rc |= s->alloc(&d.counts, s->n_keys);
+  rc |= s->alloc(&d.cell_start, (size_t)s->n_keys + 1);
+  rc |= s->alloc(&s->tile_sums, s->n_tiles);
+  rc |= s->alloc(&d.nfw, 2);
+  rc |= s->alloc(&d.pos, n);
+  rc |= s->alloc(&d.vel, n);
+  rc |= s->alloc(&d.vel2, n);
+  rc |= s->alloc(&d.id_of, n);
+  rc |= s->alloc(&d.world_s, n);
+  rc |= s->alloc(&d.kv_s, n);
+  rc |= s->alloc(&d.kd_s, n);
+  rc |= s->alloc(&d.nbr, (size_t)s->K * n);
+  rc |= s->alloc(&d.cnt, n);
+  rc |= s->alloc(&d.slot_g, n);
+  rc |= s->alloc(&d.slot_vb, n);
+  rc |= s->alloc(&d.slot_n, n);
+  rc |= s->alloc(&d.slot_xb, n);
+  rc |= s->alloc(&d.ratio, n);
+  rc |= s->alloc(&d.alpha, n);
+  rc |= s->alloc(&d.neff, n);
+  rc |= s->alloc(&d.reg, n);
+  rc |= s->alloc(&d.src, n);
+  rc |= s->alloc(&d.kappa, n);
+  rc |= s->alloc(&d.lower, n);
+  rc |= s->alloc(&d.kr, n);
+  rc |= s->alloc(&d.acc, n);
+  rc |= s->alloc(&d.err_orig, n);
+  rc |= s->alloc(&d.kv, n);
+  rc |= s->alloc(&d.kd, n);
+  rc |= s->alloc(&d.converged, W);
+  rc |= s->alloc(&d.iters, W);
+  rc |= s->alloc(&d.err_mean, W);
+  rc |= s->alloc(&d.n_unconv, 1);
+  rc |= s->alloc(&d.n_active, W);
+  rc |= s->alloc(&d.overflow, W);
+  rc |= s->alloc(&d.escaped, W);
+  rc |= s->alloc(&d.projected, W);
+  rc |= s->alloc(&d.nonfinite, W);
+  rc |= s->alloc(&d.wall_overflow, W);
+  rc |= s->alloc(&d.max_speed_bits, W);
+  rc |= s->alloc(&d.mass_out, W);
+  rc |= s->alloc(&chunk_begin, cb.size());
+  rc |= s->alloc(&chunk_end, ce.size());
+  rc |= s->alloc(&world_chunk_start, cs.size());
+  rc |= s->alloc(&d.part_sum, cb.size());
+  rc |= s->alloc(&d.part_max, cb.size());
+  rc |= s->alloc(&d.emax, W);
+  rc |= s->alloc(&s->iters_den, W);
+  rc |= s->alloc(&s->iters_div, W);
+  rc |= s->alloc(&s->emit_overflow, W);
+  rc |= s->alloc(&s->den_err, W);
+  rc |= s->alloc(&s->div_err, W);
+  rc |= s->alloc(&s->den_err_max, W);
+  rc |= s->alloc(&s->den_tol, W);
+  rc |= s->alloc(&s->mass_in, W);
+  rc |= s->alloc(&s->mass0, W);
+  rc |= s->alloc(&s->tmp_mass, W);
+  rc |= s->alloc(&s->mask_d, W);
+  if (rc) {
+    std::string msg = g_err;
+    adf_destroy(s);
+    return fail(ADF_ERR_CUDA, "adf_create: " + msg);
+  }
+  d.wall_vol = wall_vol;
+  d.grid = grid;
+  d.chunk_begin = chunk_begin;
+  d.chunk_end = chunk_end;
+  d.world_chunk_start = world_chunk_start;
+  auto fin = [&](int code) {
+    if (code != ADF_OK) {
+      std::string msg = g_err;
+      adf_destroy(s);
+      return fail(code, msg);
+    }
+    return ADF_OK;
+  };
+#define CKC(x)                                                                                       \
+  do {                                                                                               \
+    cudaError_t e_ = (x);                                                                            \
+    if (e_ != cudaSuccess) return fin(fail(ADF_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_))); \
+  } while (0)
+  CKC(cudaMemcpy(grid, s->grids.data(), sizeof(WorldGrid) * s->W, cudaMemcpyHostToDevice));
+  CKC(cudaMemcpy(s->world_cells, s->world_cells_h.data(), sizeof(int) * s->W, cudaMemcpyHostToDevice));
+  if (!cb.empty()) {
+    CKC(cudaMemcpy(chunk_begin, cb.data(), sizeof(int) * cb.size(), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(chunk_end, ce.data(), sizeof(int) * ce.size(), cudaMemcpyHostToDevice));
+  }
+  CKC(cudaMemcpy(world_chunk_start, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice));
+  CKC(cudaMemset(d.counts, 0, sizeof(int) * std::max(s->n_keys, 1)));
+  CKC(cudaMemset(d.nfw, 0, sizeof(int) * 2));
+  CKC(cudaMemset(d.kv, 0, sizeof(float) * n));
+  CKC(cudaMemset(d.kd, 0, sizeof(float) * n));
+  CKC(cudaMemset(d.err_orig, 0, sizeof(float) * n));
+  void* zero_w[] = {d.overflow, d.escaped, d.projected, d.nonfinite, d.wall_overflow, d.max_speed_bits, d.converged,
+                    d.iters, d.err_mean, s->iters_den, s->iters_div, s->emit_overflow, s->den_err, s->div_err,
+                    s->den_err_max, d.emax};
+  for (void* z : zero_w) CKC(cudaMemset(z, 0, 4 * W));
+  CKC(cudaMemset(d.mass_out, 0, 8 * W));
+  CKC(cudaMemset(s->mass_in, 0, 8 * W));
+  CKC(cudaMemset(d.n_active, 0, 8 * W));
+  std::vector<float> tol(W, (float)p.tol_den);
+  CKC(cudaMemcpy(s->den_tol, tol.data(), sizeof(float) * W, cudaMemcpyHostToDevice));
+  if (s->n > 0) {
+    k_wall_volume<<<blocks(s->n), BLOCK>>>(s->n, m->flags, m->radius, wall_vol);
+    ++s->launches;
+    // initial liquid mass per world (runtime.py:387-389)
+    CKC(cudaMemset(s->mass0, 0, 8 * W));
+    k_active_mass<<<blocks(s->n), BLOCK>>>(d, s->mass0);
+    ++s->launches;
+  } else {
+    CKC(cudaMemset(s->mass0, 0, 8 * W));
+  }
+  CKC(cudaGetLastError());
+  CKC(cudaHostAlloc((void**)&s->pinned, 2 * sizeof(int), cudaHostAllocDefault));
+  CKC(cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming));
+  CKC(cudaDeviceSynchronize());
+#undef CKC
+  *out = s;
+  return ADF_OK;
+}
+
+void adf_destroy(adf_solver* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  cudaDeviceSynchronize();
+  for (void* p : s->owned) cudaFree(p);
+  void* em[] = {s->em_d, s->off_local_d, s->off_emitter_d, s->off_rank_d, s->pool_d, s->enabled_d, s->cursor_d,
+                s->emit_now_d, s->t_acc_d, s->sinks_d};
+  for (void* p : em)
+    if (p) cudaFree(p);
+  if (s->pinned) cudaFreeHost(s->pinned);
+  if (s->list_entries) cudaFree(s->list_entries);
+  for (auto& e : s->prof_pool) cudaEventDestroy(e);
+  for (auto& e : s->ev)
+    if (e) cudaEventDestroy(e);
+  delete s;
+}
+
+int adf_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out, float* qd_out, const float* f_ext,
+             double dt, void* stream) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_step: null solver");
+  if (!(dt > 0.0)) return fail(ADF_ERR_VALUE, "SolverDFSPH.step: dt must be > 0, got " + std::to_string(dt));
+  if (s->n == 0) return ADF_OK;
+  if (!q_in || !qd_in || !q_out || !qd_out) return fail(ADF_ERR_VALUE, "adf_step: null state array");
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaSetDevice(s->device));
+  const size_t bytes = sizeof(float) * 3 * (size_t)s->n;
+  if (q_out != q_in) CK(cudaMemcpyAsync(q_out, q_in, bytes, cudaMemcpyDeviceToDevice, st));
+  if (qd_out != qd_in) CK(cudaMemcpyAsync(qd_out, qd_in, bytes, cudaMemcpyDeviceToDevice, st));
+  DevP P = s->d;
+  P.q = q_out;
+  P.qd = qd_out;
+  P.f_ext = f_ext;
+  P.dt = (float)dt;
+  P.n_sinks = (int)s->sinks_h.size();
+  P.sinks = s->sinks_d;
+  CK(cudaMemsetAsync(P.max_speed_bits, 0, sizeof(int) * std::max(s->W, 1), st));
+  int rc = prepare(s, P, st);
+  if (rc) return rc;
+  if (s->prm.divergence_solve) {
+    rc = solve(s, P, 0, dt, st);
+    if (rc) return rc;
+  }
+  P.dt = (float)dt;
+  prof_begin(s, 9, st);
+  LAUNCH(s, k_xsph, blocks(s->n), BLOCK, st, P);
+  prof_end(s, st);
+  std::swap(P.vel, P.vel2);
+  rc = solve(s, P, 1, dt, st);
+  if (rc) return rc;
+  prof_begin(s, 10, st);
+  LAUNCH(s, k_finish, blocks(s->n), BLOCK, st, P);
+  prof_end(s, st);
+  const int ne = (int)s->em_h.size();
+  if (ne > 0) {
+    prof_begin(s, 11, st);
+    LAUNCH(s, k_emit_clock, blocks(ne), BLOCK, st, s->em_d, ne, (float)dt, s->enabled_d, s->t_acc_d, s->emit_now_d);
+    int no = (int)s->off_emitter_h.size();
+    if (no > 0)
+      LAUNCH(s, k_emit, blocks(no), BLOCK, st, P, s->em_d, no, s->off_emitter_d, s->off_rank_d, s->off_local_d,
+             s->emit_now_d, s->cursor_d, s->pool_d, s->mass_in, s->emit_overflow);
+    LAUNCH(s, k_emit_cursor, blocks(ne), BLOCK, st, s->em_d, ne, s->emit_now_d, s->cursor_d);
+    prof_end(s, st);
+  }
+  return check_launch();
+}
+
+int adf_density_ratio(adf_solver* s, const float* q, const float* qd, float* ratio_out, float* active_out,
+                      void* stream) {
+  if (!s || !q || !qd) return fail(ADF_ERR_VALUE, "adf_density_ratio: null argument");
+  if (s->n == 0) return ADF_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaSetDevice(s->device));
+  DevP P = s->d;
+  P.q = const_cast<float*>(q);
+  P.qd = const_cast<float*>(qd);
+  int rc = prepare(s, P, st);
+  if (rc) return rc;
+  if (ratio_out) {
+    CK(cudaMemsetAsync(ratio_out, 0, sizeof(float) * s->n, st));
+    LAUNCH(s, k_unsort_n, blocks(s->n), BLOCK, st, s->n, P.nfw, P.id_of, P.ratio, 1, 0, ratio_out, 1);
+  }
+  if (active_out) {
+    CK(cudaMemsetAsync(active_out, 0, sizeof(float) * s->n, st));
+    LAUNCH(s, k_fill_ones, blocks(s->n), BLOCK, st, s->n, P.nfw, P.id_of, active_out);
+  }
+  return check_launch();
+}
+
+int adf_get_report(adf_solver* s, adf_report* r, void* stream) {
+  if (!s || !r) return fail(ADF_ERR_VALUE, "adf_get_report: null argument");
+  CK(cudaSetDevice(s->device));
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  const int W = s->W;
+  if (W == 0) return ADF_OK;
+  auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (!dst) return ADF_OK;
+    CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return ADF_OK;
+  };
+  int rc = 0;
+  rc |= cp(r->density_err, s->den_err, 4 * W);
+  rc |= cp(r->divergence_err, s->div_err, 4 * W);
+  rc |= cp(r->iters_density, s->iters_den, 4 * W);
+  rc |= cp(r->iters_divergence, s->iters_div, 4 * W);
+  rc |= cp(r->mass_in, s->mass_in, 8 * W);
+  rc |= cp(r->mass_out, s->d.mass_out, 8 * W);
+  rc |= cp(r->mass_initial, s->mass0, 8 * W);
+  rc |= cp(r->escaped, s->d.escaped, 4 * W);
+  rc |= cp(r->neighbor_overflow, s->d.overflow, 4 * W);
+  rc |= cp(r->max_speed, s->d.max_speed_bits, 4 * W);
+  rc |= cp(r->density_err_max, s->den_err_max, 4 * W);
+  rc |= cp(r->projected, s->d.projected, 4 * W);
+  rc |= cp(r->nonfinite, s->d.nonfinite, 4 * W);
+  rc |= cp(r->emitter_overflow, s->emit_overflow, 4 * W);
+  rc |= cp(r->density_tol, s->den_tol, 4 * W);
+  return rc ? ADF_ERR_CUDA : ADF_OK;
+}
+
+int adf_active_mass(adf_solver* s, int64_t* out_host, void* stream) {
+  if (!s || !out_host) return fail(ADF_ERR_VALUE, "adf_active_mass: null argument");
+  CK(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int W = std::max(s->W, 1);
+  CK(cudaMemsetAsync(s->tmp_mass, 0, 8 * W, st));
+  if (s->n > 0) LAUNCH(s, k_active_mass, blocks(s->n), BLOCK, st, s->d, s->tmp_mass);
+  CK(cudaStreamSynchronize(st));
+  if (s->W) CK(cudaMemcpy(out_host, s->tmp_mass, 8 * s->W, cudaMemcpyDeviceToHost));
+  return check_launch();
+}
+
+int adf_get_warm_starts(adf_solver* s, float* kv, float* kd, void* stream) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_get_warm_starts: null solver");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (kv) CK(cudaMemcpyAsync(kv, s->d.kv, sizeof(float) * s->n, cudaMemcpyDeviceToDevice, st));
+  if (kd) CK(cudaMemcpyAsync(kd, s->d.kd, sizeof(float) * s->n, cudaMemcpyDeviceToDevice, st));
+  return ADF_OK;
+}
+
+int adf_set_warm_starts(adf_solver* s, const float* kv, const float* kd, void* stream) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_warm_starts: null solver");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (kv) CK(cudaMemcpyAsync(s->d.kv, kv, sizeof(float) * s->n, cudaMemcpyDeviceToDevice, st));
+  if (kd) CK(cudaMemcpyAsync(s->d.kd, kd, sizeof(float) * s->n, cudaMemcpyDeviceToDevice, st));
+  return ADF_OK;
+}
+
+int adf_reset(adf_solver* s, const uint8_t* world_mask, const int32_t* flags0, const int8_t* phase0, void* stream) {
+  if (!s || !flags0 || !phase0) return fail(ADF_ERR_VALUE, "adf_reset: null argument");
+  const int W = s->W;
+  std::vector<uint8_t> mask(std::max(W, 1), 1);
+  if (world_mask)
+    for (int w = 0; w < W; ++w) mask[w] = world_mask[w] ? 1 : 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaStreamSynchronize(st));
+  CK(cudaMemcpy(s->mask_d, mask.data(), std::max(W, 1), cudaMemcpyHostToDevice));
+  if (s->n > 0) LAUNCH(s, k_reset, blocks(s->n), BLOCK, st, s->d, s->mask_d, flags0, phase0);
+  CK(cudaStreamSynchronize(st));
+  auto zero_masked = [&](void* dev, size_t elem) -> int {
+    std::vector<unsigned char> h(elem * std::max(W, 1));
+    CK(cudaMemcpy(h.data(), dev, elem * W, cudaMemcpyDeviceToHost));
+    for (int w = 0; w < W; ++w)
+      if (mask[w]) std::memset(h.data() + elem * w, 0, elem);
+    CK(cudaMemcpy(dev, h.data(), elem * W, cudaMemcpyHostToDevice));
+    return ADF_OK;
+  };
+  if (W > 0) {
+    int rc = 0;
+    rc |= zero_masked(s->d.escaped, 4) | zero_masked(s->d.projected, 4) | zero_masked(s->d.overflow, 4);
+    rc |= zero_masked(s->d.nonfinite, 4) | zero_masked(s->emit_overflow, 4) | zero_masked(s->mass_in, 8);
+    rc |= zero_masked(s->d.mass_out, 8);
+    if (rc) return rc;
+  }
+  const int ne = (int)s->em_h.size();
+  if (ne > 0) {  // emitters.rewind: layer clock and cursor of the masked worlds' emitters back to 0
+    std::vector<float> t(ne);
+    std::vector<int> c(ne);
+    CK(cudaMemcpy(t.data(), s->t_acc_d, sizeof(float) * ne, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(c.data(), s->cursor_d, sizeof(int) * ne, cudaMemcpyDeviceToHost));
+    for (int e = 0; e < ne; ++e)
+      if (mask[s->em_h[e].world]) {
+        t[e] = 0.0f;
+        c[e] = 0;
+      }
+    CK(cudaMemcpy(s->t_acc_d, t.data(), sizeof(float) * ne, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->cursor_d, c.data(), sizeof(int) * ne, cudaMemcpyHostToDevice));
+  }
+  return check_launch();
+}
+
+int adf_add_emitter(adf_solver* s, int world, const float* xform, const float* offsets, int n_off,
+                    const float* velocity, float interval, const int32_t* pool, int pool_size) {
+  if (!s || !xform || !velocity || (n_off > 0 && !offsets) || (pool_size > 0 && !pool))
+    return -fail(ADF_ERR_VALUE, "adf_add_emitter: null argument");
+  if (world < 0 || world >= s->W) return -fail(ADF_ERR_VALUE, "add_emitter: world " + std::to_string(world) +
+                                                                 " out of range");
+  if (!(interval > 0.0f)) return -fail(ADF_ERR_VALUE, "add_emitter: interval must be > 0");
+  for (int k = 0; k < pool_size; ++k)
+    if (pool[k] < s->ws_host[world] || pool[k] >= s->ws_host[world + 1])
+      return -fail(ADF_ERR_VALUE, "add_emitter: pool particle outside the emitter's world");
+  Emit e{};
+  e.world = world;
+  e.n_layer = n_off;
+  e.pool_begin = (int)s->pool_h.size();
+  e.pool_size = pool_size;
+  std::memcpy(e.xform, xform, sizeof(float) * 7);
+  std::memcpy(e.vel, velocity, sizeof(float) * 3);
+  e.interval = interval;
+  int idx = (int)s->em_h.size();
+  s->em_h.push_back(e);
+  s->enabled_h.push_back(1);
+  for (int c = 0; c < n_off; ++c) {
+    s->off_emitter_h.push_back(idx);
+    s->off_rank_h.push_back(c);
+    for (int a = 0; a < 3; ++a) s->off_local_h.push_back(offsets[3 * c + a]);
+  }
+  s->pool_h.insert(s->pool_h.end(), pool, pool + pool_size);
+  int rc = upload_emitters(s, idx);
+  if (rc) return -rc;
+  return idx;
+}
+
+int adf_state_arrays(adf_solver* s, float** kv, float** kd) {
+  if (!s || !kv || !kd) return fail(ADF_ERR_VALUE, "adf_state_arrays: null argument");
+  *kv = s->d.kv;
+  *kd = s->d.kd;
+  return ADF_OK;
+}
+
+int adf_set_emitter_pool(adf_solver* s, int e, const int32_t* pool, int pool_size) {
+  if (!s || (pool_size > 0 && !pool)) return fail(ADF_ERR_VALUE, "adf_set_emitter_pool: null argument");
+  int ne = (int)s->em_h.size();
+  if (e < 0 || e >= ne) return fail(ADF_ERR_VALUE, "set_emitter_pool: emitter " + std::to_string(e) + " does not exist");
+  const int w = s->em_h[e].world;
+  for (int k = 0; k < pool_size; ++k)
+    if (pool[k] < s->ws_host[w] || pool[k] >= s->ws_host[w + 1])
+      return fail(ADF_ERR_VALUE, "set_emitter_pool: pool particle outside the emitter's world");
+  // rebuild the concatenated pool table with emitter e's new pool
+  std::vector<int> pools;
+  for (int k = 0; k < ne; ++k) {
+    int b = (int)pools.size();
+    if (k == e) pools.insert(pools.end(), pool, pool + pool_size);
+    else pools.insert(pools.end(), s->pool_h.begin() + s->em_h[k].pool_begin,
+                      s->pool_h.begin() + s->em_h[k].pool_begin + s->em_h[k].pool_size);
+    s->em_h[k].pool_size = (int)pools.size() - b;
+    s->em_h[k].pool_begin = b;
+  }
+  s->pool_h.swap(pools);
+  return upload_emitters(s, ne);
+}
+
+int adf_emitter_state(adf_solver* s, float* t_acc, int32_t* cursor) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_emitter_state: null solver");
+  int ne = (int)s->em_h.size();
+  if (ne == 0) return ADF_OK;
+  CK(cudaDeviceSynchronize());
+  if (t_acc) CK(cudaMemcpy(t_acc, s->t_acc_d, sizeof(float) * ne, cudaMemcpyDeviceToHost));
+  if (cursor) CK(cudaMemcpy(cursor, s->cursor_d, sizeof(int) * ne, cudaMemcpyDeviceToHost));
+  return ADF_OK;
+}
+
+int adf_set_emitter_enabled(adf_solver* s, int e, int enabled) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_emitter_enabled: null solver");
+  int ne = (int)s->em_h.size();
+  if (e < 0 || e >= ne)
+    return fail(ADF_ERR_VALUE, "set_emitter_enabled: emitter " + std::to_string(e) + " does not exist (" +
+                                   std::to_string(ne) + " emitters)");
+  s->enabled_h[e] = enabled ? 1 : 0;
+  int v = s->enabled_h[e];
+  CK(cudaMemcpy(s->enabled_d + e, &v, sizeof(int), cudaMemcpyHostToDevice));
+  return ADF_OK;
+}
+
+int adf_add_sink(adf_solver* s, int world, const float* xform, const float* half) {
+  if (!s || !xform || !half) return -fail(ADF_ERR_VALUE, "adf_add_sink: null argument");
+  if (world < 0 || world >= s->W) return -fail(ADF_ERR_VALUE, "add_sink: world " + std::to_string(world) +
+                                                                 " out of range");
+  Sink k{};
+  k.world = world;
+  std::memcpy(k.xform, xform, sizeof(float) * 7);
+  std::memcpy(k.half, half, sizeof(float) * 3);
+  s->sinks_h.push_back(k);
+  if (s->sinks_d) cudaFree(s->sinks_d);
+  s->sinks_d = nullptr;
+  if (dalloc(&s->sinks_d, s->sinks_h.size())) return -ADF_ERR_CUDA;
+  cudaError_t e = cudaMemcpy(s->sinks_d, s->sinks_h.data(), sizeof(Sink) * s->sinks_h.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return -fail(ADF_ERR_CUDA, cudaGetErrorString(e));
+  return (int)s->sinks_h.size() - 1;
+}
+
+int adf_neighbor_rows(adf_solver* s, int32_t* rows, int32_t* count, void* stream) {
+  if (!s || !rows || !count) return fail(ADF_ERR_VALUE, "adf_neighbor_rows: null argument");
+  if (!s->built) return fail(ADF_ERR_STATE, "adf_neighbor_rows: no lists yet (step or density_ratio first)");
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  const int n = s->n, K = s->K;
+  int nfw[2];
+  CK(cudaMemcpy(nfw, s->d.nfw, sizeof(nfw), cudaMemcpyDeviceToHost));
+  std::vector<int> id(n), cnt(n), nbr((size_t)K * n);
+  CK(cudaMemcpy(id.data(), s->d.id_of, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(cnt.data(), s->d.cnt, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(nbr.data(), s->d.nbr, sizeof(int) * (size_t)K * n, cudaMemcpyDeviceToHost));
+  std::fill(rows, rows + (size_t)n * K, -1);
+  std::fill(count, count + n, 0);
+  for (int p = 0; p < nfw[0]; ++p) {
+    int i = id[p];
+    count[i] = cnt[p];
+    for (int k = 0; k < cnt[p]; ++k) rows[(size_t)i * K + k] = id[nbr[(size_t)k * n + p]];
+  }
+  return ADF_OK;
+}
+
+int adf_debug_field(adf_solver* s, const char* name, float* out, void* stream) {
+  if (!s || !name || !out) return fail(ADF_ERR_VALUE, "adf_debug_field: null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevP& d = s->d;
+  struct F { const char* nm; const float* ptr; int stride, comp, ncomp; };
+  const F fields[] = {
+      {"ratio", d.ratio, 1, 0, 1}, {"alpha", d.alpha, 1, 0, 1}, {"neff", d.neff, 1, 0, 1}, {"reg", d.reg, 1, 0, 1},
+      {"src", d.src, 1, 0, 1}, {"kappa", d.kappa, 1, 0, 1}, {"lower", d.lower, 1, 0, 1},
+      {"slot_psi", (const float*)d.slot_g, 4, 3, 1}, {"slot_phi", (const float*)d.slot_vb, 4, 3, 1},
+      {"acc", (const float*)d.acc, 4, 0, 3}, {"slot_g", (const float*)d.slot_g, 4, 0, 3},
+      {"slot_vb", (const float*)d.slot_vb, 4, 0, 3}, {"slot_n", (const float*)d.slot_n, 4, 0, 3}};
+  for (const F& f : fields) {
+    if (std::strcmp(f.nm, name) != 0) continue;
+    CK(cudaMemsetAsync(out, 0, sizeof(float) * f.ncomp * (size_t)s->n, st));
+    LAUNCH(s, k_unsort_n, blocks(s->n), BLOCK, st, s->n, d.nfw, d.id_of, f.ptr, f.stride, f.comp, out, f.ncomp);
+    return check_launch();
+  }
+  if (std::strcmp(name, "err") == 0) {
+    CK(cudaMemcpyAsync(out, d.err_orig, sizeof(float) * s->n, cudaMemcpyDeviceToDevice, st));
+    return ADF_OK;
+  }
+  return fail(ADF_ERR_VALUE, std::string("adf_debug_field: unknown field ") + name);
+}
+
+int adf_world_sum(adf_solver* s, const float* values, double* out_sum, float* out_max, void* stream) {
+  if (!s || !values || !out_sum || !out_max) return fail(ADF_ERR_VALUE, "adf_world_sum: null argument");
+  if (s->W == 0) return ADF_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevP& P = s->d;
+  if (P.n_chunks > 0)
+    LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, values, P.chunk_begin, P.chunk_end, P.part_sum, P.part_max,
+           (int*)nullptr);
+  LAUNCH(s, k_world_check, s->W, 256, st, P, 0, out_sum, out_max);
+  return check_launch();
+}
+
+int64_t adf_kernel_launches(const adf_solver* s) { return s ? s->launches : 0; }
+
+int adf_profile_enable(adf_solver* s, int enable) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_profile_enable: null solver");
+  if (enable && s->prof_pool.empty()) {
+    s->prof_pool.resize(16384);
+    for (auto& e : s->prof_pool) CK(cudaEventCreate(&e));
+  }
+  s->prof_on = enable != 0;
+  return ADF_OK;
+}
+
+int adf_profile_read(adf_solver* s, double* ms, int64_t* launches) {
+  if (!s || !ms || !launches) return fail(ADF_ERR_VALUE, "adf_profile_read: null argument");
+  for (int k = 0; k < ADF_PROF_KINDS; ++k) {
+    ms[k] = 0.0;
+    launches[k] = 0;
+  }
+  if (!s->prof_marks.empty()) CK(cudaEventSynchronize(s->prof_pool[s->prof_marks.back().second + 1]));
+  for (auto& m : s->prof_marks) {
+    float t = 0.0f;
+    CK(cudaEventElapsedTime(&t, s->prof_pool[m.second], s->prof_pool[m.second + 1]));
+    ms[m.first] += t;
+    launches[m.first] += 1;
+  }
+  s->prof_marks.clear();
+  s->prof_used = 0;
+  return ADF_OK;
+}
+
+int adf_list_stats(adf_solver* s, int32_t* fluid, int64_t* entries, void* stream) {
+  if (!s || !fluid || !entries) return fail(ADF_ERR_VALUE, "adf_list_stats: null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!s->list_entries) CK(cudaMalloc(&s->list_entries, sizeof(long long)));
+  CK(cudaMemsetAsync(s->list_entries, 0, sizeof(long long), st));
+  if (s->n > 0) LAUNCH(s, k_count_entries, blocks(s->n), BLOCK, st, s->n, s->d.nfw, s->d.cnt, s->list_entries);
+  CK(cudaStreamSynchronize(st));
+  int nfw[2];
+  CK(cudaMemcpy(nfw, s->d.nfw, sizeof(nfw), cudaMemcpyDeviceToHost));
+  long long e = 0;
+  CK(cudaMemcpy(&e, s->list_entries, sizeof(e), cudaMemcpyDeviceToHost));
+  *fluid = nfw[0];
+  *entries = e;
+  return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,982 @@
+// SPDX-License-Identifier: Apache-2.0
+// DFSPH step kernels for sm_100a. One thread per particle; particles of every world are sorted by (class, world,
+// cell) at the start of each step so that a warp's neighbour gathers land in a few cells (L1/L2 locality) and every
+// array the neighbour loops stream is structure-of-arrays (float4 position+mass, float4 velocity+rest density).
+//
+// Sorted space: fluid particles occupy [0, nf), boundary (wall) particles [nf, nf + nw); other particles (spares,
+// retired, foreign) stay in the caller's arrays only. Results never depend on where a particle lands inside its
+// cell: neighbour rows are kept in ascending original particle id (the reference's order), wall-colour sums run in
+// ascending wall-particle id, and per-world float64 reductions run over the caller's particle order.
+#pragma once
+
+#include <cstdint>
+
+#include "dfsph_math.cuh"
+
+namespace adf {
+
+constexpr int BLOCK = 256;
+constexpr int MAXCAP = 128;      // largest neighbor_capacity
+constexpr int MAXWALL = 160;     // wall particles within h of one fluid particle (far above any lattice wall)
+constexpr int FLAG_ACTIVE = 1;
+constexpr int FLAG_PROXY = 2;
+constexpr int PROJECT_PASSES = 4;  // integrate.py:50
+
+struct WorldGrid {
+  float ox, oy, oz, inv_cw;  // origin, 1 / cell width
+  int nx, ny, nz, base;      // cells per axis, first cell of the world in the class-0 key space
+};
+
+struct Emit {
+  int world, n_layer, pool_begin, pool_size;
+  float xform[7];
+  float vel[3];
+  float interval;
+};
+
+struct Sink {
+  int world;
+  float xform[7];
+  float half[3];
+};
+
+// Everything a kernel needs, passed by value.
+struct DevP {
+  KC kc;
+  int n;            // particle capacity (caller's n)
+  int W;
+  int K;            // neighbour capacity
+  int total_cells;  // cells of all worlds (one class)
+  float dt, n_full, tot_min, wall_offset, wall_amp, taper0, taper1, reach, omega, warm, warm_den, min_nb;
+  float xsph_c, v_sep, relief, eps;
+  int mode;  // 0 divergence, 1 density
+  int two_sided;
+  float tol, tol_max;
+  int min_it, max_it;
+  int has_bounds;
+  float blo[3], bhi[3];
+  int n_sinks;
+  const Sink* sinks;
+  // caller model (original order)
+  const float* mass;
+  const float* rho0;
+  int32_t* flags;
+  int8_t* phase;
+  const int32_t* world;
+  const float* wall_vol;
+  const float* gravity;
+  const float* f_ext;
+  // state in/out (original order, [n][3])
+  float* q;
+  float* qd;
+  // persistent warm starts (original order)
+  float* kv;
+  float* kd;
+  // sorting
+  const WorldGrid* grid;
+  int* key_of;
+  int* counts;      // [2 total_cells]
+  int* cell_start;  // [2 total_cells + 1]
+  int* nfw;         // [2]: nf, nw
+  // sorted space
+  float4* pos;   // x y z, mass (fluid) or wall volume (walls)
+  float4* vel;   // vx vy vz, rest density
+  float4* vel2;  // XSPH output
+  int* id_of;
+  int* world_s;
+  float* kv_s;
+  float* kd_s;
+  int* nbr;  // [K][n] sorted positions, ascending original id
+  int* cnt;
+  float4* slot_g;   // dPsi/dx (3), psi; psi < 0: no slot
+  float4* slot_vb;  // wall velocity (3), phi
+  float4* slot_n;   // outward normal (3), 0
+  float4* slot_xb;  // surface point (3), 0
+  float* ratio;
+  float* alpha;
+  float* neff;
+  float* reg;
+  float* src;
+  float* kappa;
+  float* lower;
+  float* kr;  // kappa / rho0
+  float4* acc;
+  float* err_orig;  // original order
+  // per world
+  int* converged;
+  int* iters;
+  float* err_mean;
+  int* n_unconv;
+  double* n_active;
+  int* overflow;
+  int* escaped;
+  int* projected;
+  int* nonfinite;
+  int* wall_overflow;
+  int* max_speed_bits;  // float bits of a non-negative max
+  long long* mass_out;
+  // reductions (original order)
+  const int* chunk_begin;
+  const int* chunk_end;
+  const int* world_chunk_start;
+  int n_chunks;
+  double* part_sum;
+  float* part_max;
+  float* emax;
+};
+
+__device__ __forceinline__ bool is_fluid_orig(const DevP& P, int i) {
+  return (P.flags[i] & FLAG_ACTIVE) != 0 && P.phase[i] >= 1;
+}
+
+__device__ __forceinline__ void cell_coords(const WorldGrid& g, float x, float y, float z, int& cx, int& cy, int& cz) {
+  float fx = floorf(__fmul_rn(__fsub_rn(x, g.ox), g.inv_cw));
+  float fy = floorf(__fmul_rn(__fsub_rn(y, g.oy), g.inv_cw));
+  float fz = floorf(__fmul_rn(__fsub_rn(z, g.oz), g.inv_cw));
+  fx = fminf(fmaxf(fx, 0.0f), (float)(g.nx - 1));
+  fy = fminf(fmaxf(fy, 0.0f), (float)(g.ny - 1));
+  fz = fminf(fmaxf(fz, 0.0f), (float)(g.nz - 1));
+  cx = (int)fx;
+  cy = (int)fy;
+  cz = (int)fz;
+}
+
+// ------------------------------------------------------------------------------------------------ sorting
+// Groups (neighbors.py:36-51): fluid = ACTIVE and phase >= 1; wall = a boundary particle (PROXY at creation),
+// ACTIVE, in a world; every other particle stays out of the sorted arrays.
+__global__ void k_classify(DevP P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  int w = P.world[i];
+  int cls = -1;
+  if (w >= 0 && w < P.W) {
+    if (is_fluid_orig(P, i)) cls = 0;
+    else if (P.wall_vol[i] > 0.0f && (P.flags[i] & FLAG_ACTIVE) != 0) cls = 1;
+  }
+  if (cls < 0) {
+    P.key_of[i] = -1;
+    return;
+  }
+  const WorldGrid g = P.grid[w];
+  int cx, cy, cz;
+  cell_coords(g, P.q[3 * i], P.q[3 * i + 1], P.q[3 * i + 2], cx, cy, cz);
+  int key = cls * P.total_cells + g.base + (cz * g.ny + cy) * g.nx + cx;
+  P.key_of[i] = key;
+  atomicAdd(&P.counts[key], 1);
+}
+
+// Exclusive scan of n ints in three passes (per-block sums, a one-block scan of those, per-block scan + offset).
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* smem, int& total) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int s = (lane < (int)(blockDim.x >> 5)) ? smem[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    smem[lane] = s;
+  }
+  __syncthreads();
+  int off = wid > 0 ? smem[wid - 1] : 0;
+  total = smem[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return off + x - v;
+}
+
+__global__ void k_scan_tiles(const int* in, int n, int* tile_sums) {
+  __shared__ int smem[32];
+  int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) s += (base + k < n) ? in[base + k] : 0;
+  int total;
+  block_exclusive_scan(s, smem, total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_tile_sums(int* tile_sums, int n_tiles) {
+  __shared__ int smem[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b = 0; b < n_tiles; b += blockDim.x) {
+    int i = b + threadIdx.x;
+    int v = i < n_tiles ? tile_sums[i] : 0;
+    int total;
+    int ex = block_exclusive_scan(v, smem, total);
+    int c = carry;
+    if (i < n_tiles) tile_sums[i] = c + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry = c + total;
+    __syncthreads();
+  }
+}
+
+__global__ void k_scan_apply(const int* in, int n, const int* tile_off, int* out) {
+  __shared__ int smem[32];
+  int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  int v[SCAN_ITEMS];
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    s += v[k];
+  }
+  int total;
+  int ex = block_exclusive_scan(s, smem, total) + tile_off[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    int idx = base + k;
+    if (idx < n) out[idx] = ex;
+    ex += v[k];
+    if (idx == n - 1) out[n] = ex;
+  }
+}
+
+// Fluid and wall counts, and each world's liquid count (n_active, an exact integer in float64).
+__global__ void k_post_scan(DevP P, const int* world_cells) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w == 0) {
+    int nf = P.cell_start[P.total_cells];
+    P.nfw[0] = nf;
+    P.nfw[1] = P.cell_start[2 * P.total_cells] - nf;
+  }
+  if (w >= P.W) return;
+  int b = P.grid[w].base;
+  P.n_active[w] = (double)(P.cell_start[b + world_cells[w]] - P.cell_start[b]);
+}
+
+// Place each particle in its cell's range and gather its data into the sorted arrays. The counts go back to zero.
+__global__ void k_scatter(DevP P) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  int key = P.key_of[i];
+  if (key < 0) return;
+  int p = P.cell_start[key] + atomicSub(&P.counts[key], 1) - 1;
+  bool fluid = key < P.total_cells;
+  float m = fluid ? P.mass[i] : P.wall_vol[i];
+  P.pos[p] = make_float4(P.q[3 * i], P.q[3 * i + 1], P.q[3 * i + 2], m);
+  P.vel[p] = make_float4(P.qd[3 * i], P.qd[3 * i + 1], P.qd[3 * i + 2], P.rho0[i]);
+  P.id_of[p] = i;
+  P.world_s[p] = P.world[i];
+  if (fluid) {
+    P.kv_s[p] = P.kv[i];
+    P.kd_s[p] = P.kd[i];
+  }
+}
+
+// ----------------------------------------------------------------------------------------- neighbour rows
+// neighbors.py:160-195: fluid neighbours j != i of the same world with |x_j - x_i|^2 < h^2, ascending original id,
+// the lowest K kept; a world's overflow counter counts particles with more than K.
+__global__ void __launch_bounds__(BLOCK) k_lists(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  int w = P.world_s[p];
+  const WorldGrid g = P.grid[w];
+  float4 xi = P.pos[p];
+  int cx, cy, cz;
+  cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
+  unsigned long long buf[MAXCAP];
+  int m = 0, total = 0;
+  const int K = P.K;
+  for (int dz = -1; dz <= 1; ++dz) {
+    int z = cz + dz;
+    if (z < 0 || z >= g.nz) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      int y = cy + dy;
+      if (y < 0 || y >= g.ny) continue;
+      int row = g.base + (z * g.ny + y) * g.nx;
+      int x0 = max(cx - 1, 0), x1 = min(cx + 1, g.nx - 1);
+      int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
+      for (int j = b; j < e; ++j) {
+        if (j == p) continue;
+        float4 xj = P.pos[j];
+        float r2 = dot_plain(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z);
+        if (r2 < P.kc.h2) {
+          ++total;
+          unsigned long long key = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
+          if (m == K && key >= buf[K - 1]) continue;
+          int at = (m < K) ? m : K - 1;
+          while (at > 0 && buf[at - 1] > key) {
+            buf[at] = buf[at - 1];
+            --at;
+          }
+          buf[at] = key;
+          if (m < K) ++m;
+        }
+      }
+    }
+  }
+  for (int k = 0; k < m; ++k) P.nbr[(size_t)k * P.n + p] = (int)(unsigned)(buf[k] & 0xffffffffull);
+  P.cnt[p] = m;
+  if (total > K) atomicAdd(&P.overflow[w], 1);
+}
+
+// --------------------------------------------------------------------------------------- particle-wall slot
+// particle_walls.py:65-119 + boundary.py:241-287: colour c = sum V_j W over the world's wall particles (ascending
+// wall id), its gradient and mean velocity; the distance phi with Psi(phi) = c; the slot filled as a flat wall at phi
+// with the fitted amplitude, offset and C1 taper. One slot per particle (no SDF shapes), so the inclusion-exclusion
+// combine of boundary.py:336-396 is the identity.
+__global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int nf = P.nfw[0];
+  if (p >= nf) return;
+  int nw = P.nfw[1];
+  P.slot_g[p] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+  if (nw == 0) return;
+  int w = P.world_s[p];
+  const WorldGrid g = P.grid[w];
+  float4 xi = P.pos[p];
+  int cx, cy, cz;
+  cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
+  unsigned long long buf[MAXWALL];
+  int m = 0;
+  for (int dz = -1; dz <= 1; ++dz) {
+    int z = cz + dz;
+    if (z < 0 || z >= g.nz) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      int y = cy + dy;
+      if (y < 0 || y >= g.ny) continue;
+      int row = P.total_cells + g.base + (z * g.ny + y) * g.nx;
+      int x0 = max(cx - 1, 0), x1 = min(cx + 1, g.nx - 1);
+      int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
+      for (int j = b; j < e; ++j) {
+        float4 xj = P.pos[j];
+        float dx = xi.x - xj.x, dy2 = xi.y - xj.y, dz2 = xi.z - xj.z;
+        float W, F;
+        wf(P.kc, dot_plain(dx, dy2, dz2, dx, dy2, dz2), W, F);
+        float wj = xj.w * W;
+        if (wj > 0.0f) {
+          if (m >= MAXWALL) {
+            atomicAdd(&P.wall_overflow[w], 1);
+            continue;
+          }
+          unsigned long long key = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
+          int at = m;
+          while (at > 0 && buf[at - 1] > key) {
+            buf[at] = buf[at - 1];
+            --at;
+          }
+          buf[at] = key;
+          ++m;
+        }
+      }
+    }
+  }
+  if (m == 0) return;
+  float c = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+  for (int k = 0; k < m; ++k) {
+    int j = (int)(unsigned)(buf[k] & 0xffffffffull);
+    float4 xj = P.pos[j];
+    float4 vj = P.vel[j];
+    float dx = xi.x - xj.x, dy2 = xi.y - xj.y, dz2 = xi.z - xj.z;
+    float W, F;
+    wf(P.kc, dot_plain(dx, dy2, dz2, dx, dy2, dz2), W, F);
+    float vol = xj.w;
+    float wj = vol * W;
+    c = c + wj;
+    gx = ADF_FMA(vol, dx * F, gx);
+    gy = ADF_FMA(vol, dy2 * F, gy);
+    gz = ADF_FMA(vol, dz2 * F, gz);
+    mx = ADF_FMA(wj, vj.x, mx);
+    my = ADF_FMA(wj, vj.y, my);
+    mz = ADF_FMA(wj, vj.z, mz);
+  }
+  mx = mx / c;
+  my = my / c;
+  mz = mz / c;
+  float lg = __fsqrt_rn(dot_plain(gx, gy, gz, gx, gy, gz));
+  if (c < (float)(1.0e-4) || lg <= 0.0f) return;
+  float phi = colour_distance(P.kc, minr(c, 1.0f));
+  if (!(phi < P.reach && phi + P.wall_offset < P.kc.h)) return;
+  float nx = -gx / lg, ny = -gy / lg, nz = -gz / lg;
+  float psi, dpsi;
+  halfspace(P.kc, phi + P.wall_offset, psi, dpsi);
+  psi = psi * P.wall_amp;
+  dpsi = dpsi * P.wall_amp;
+  if (phi > P.taper0) {
+    float L = P.taper1 - P.taper0;
+    float t = minr((phi - P.taper0) / L, 1.0f);
+    float sm = 1.0f - (t * t) * (3.0f - 2.0f * t);
+    float dsm = ((6.0f * t) * (t - 1.0f)) / L;
+    float p0 = psi;
+    psi = p0 * sm;
+    dpsi = ADF_FMA(p0, dsm, dpsi * sm);
+  }
+  P.slot_g[p] = make_float4(dpsi * nx, dpsi * ny, dpsi * nz, psi);
+  P.slot_vb[p] = make_float4(mx, my, mz, phi);
+  P.slot_n[p] = make_float4(nx, ny, nz, 0.0f);
+  P.slot_xb[p] = make_float4(ADF_FMA(-phi, nx, xi.x), ADF_FMA(-phi, ny, xi.y), ADF_FMA(-phi, nz, xi.z), 0.0f);
+}
+
+// ------------------------------------------------------------------------------------------ density, factor
+// pressure.py:144-193
+__global__ void __launch_bounds__(BLOCK) k_density_alpha(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  float4 xi = P.pos[p];
+  float mi = xi.w;
+  float inv_r0 = 1.0f / P.vel[p].w;
+  float bi = mi * inv_r0;
+  float rho = mi * P.kc.sigma;
+  float Gx = 0.0f, Gy = 0.0f, Gz = 0.0f, sq = 0.0f;
+  int c = P.cnt[p];
+  const int* row = P.nbr + p;
+  for (int k = 0; k < c; ++k) {
+    int j = row[(size_t)k * P.n];
+    float4 xj = P.pos[j];
+    float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+    float r2 = dot_plain(rx, ry, rz, rx, ry, rz);
+    float W, F;
+    wf(P.kc, r2, W, F);
+    float mj = xj.w;
+    rho = ADF_FMA(mj, W, rho);
+    float a = mj * inv_r0;
+    float aF = a * F;
+    Gx = ADF_FMA(aF, rx, Gx);
+    Gy = ADF_FMA(aF, ry, Gy);
+    Gz = ADF_FMA(aF, rz, Gz);
+    sq = ADF_FMA(bi * a, (F * F) * r2, sq);
+  }
+  float psi = 0.0f;
+  float4 sg = P.slot_g[p];
+  if (sg.w >= 0.0f) {
+    psi = sg.w;
+    Gx = Gx + sg.x;
+    Gy = Gy + sg.y;
+    Gz = Gz + sg.z;
+  }
+  float lam = 0.0f;
+  float tot = (dotf(Gx, Gy, Gz, Gx, Gy, Gz) + sq) + lam;
+  lam = lam + maxr(P.tot_min - tot, 0.0f);
+  tot = maxr(tot, P.tot_min);
+  P.reg[p] = lam;
+  P.ratio[p] = ADF_FMA(rho, inv_r0, psi);
+  P.alpha[p] = (tot > (float)(1.0e-12)) ? 1.0f / tot : 0.0f;
+  P.neff[p] = ADF_FMA(psi, P.n_full, (float)c);
+}
+
+// --------------------------------------------------------------------------------------------- solve start
+// pressure.py:196-261
+__global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  float4 xi = P.pos[p];
+  float4 vi = P.vel[p];
+  float inv_r0 = 1.0f / vi.w;
+  float rate = 0.0f;
+  int c = P.cnt[p];
+  const int* row = P.nbr + p;
+  for (int k = 0; k < c; ++k) {
+    int j = row[(size_t)k * P.n];
+    float4 xj = P.pos[j];
+    float4 vj = P.vel[j];
+    float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+    float W, F;
+    wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
+    float aF = (xj.w * inv_r0) * F;
+    rate = ADF_FMA(aF, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, rx, ry, rz), rate);
+  }
+  float4 sg = P.slot_g[p];
+  if (sg.w >= 0.0f) {
+    float4 vb = P.slot_vb[p];
+    rate = rate + dotf(vi.x - vb.x, vi.y - vb.y, vi.z - vb.z, sg.x, sg.y, sg.z);
+  }
+  const float dt = P.dt;
+  float kap, lb, s;
+  if (P.mode == 0) {
+    float kdv = 0.0f;
+    if (P.two_sided) kdv = maxr((P.warm_den * minr(P.kd_s[p], (float)(2.5e-4))) / (dt * dt), 0.0f);
+    lb = -kdv;
+    float r = rate;
+    if (kdv <= 0.0f) {
+      r = maxr(rate, 0.0f);
+      lb = 0.0f;
+    }
+    if (P.neff[p] < P.min_nb) {
+      r = 0.0f;
+      lb = 0.0f;
+    }
+    s = r;
+    kap = maxr((P.warm * minr(P.kv_s[p], 0.5f)) / dt, lb);
+  } else {
+    float ratio = P.ratio[p];
+    float rs = ADF_FMA(dt, rate, ratio);
+    if (ratio - 1.0f > P.relief) rs = ADF_FMA(dt, rate, 1.0f + P.relief);
+    s = rs;
+    lb = 0.0f;
+    kap = (P.warm * minr(P.kd_s[p], (float)(2.5e-4))) / (dt * dt);
+  }
+  P.src[p] = s;
+  P.lower[p] = lb;
+  P.kappa[p] = kap;
+  P.kr[p] = kap / vi.w;
+}
+
+__global__ void k_begin_solve(DevP P) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W) return;
+  P.iters[w] = 0;
+  P.err_mean[w] = 0.0f;
+  if (P.n_active[w] > 0.0) {
+    P.converged[w] = 0;
+    atomicAdd(P.n_unconv, 1);
+  } else {
+    P.converged[w] = 1;
+  }
+}
+
+// ------------------------------------------------------------------------------------------ Jacobi sweep
+// pressure.py:264-291: a_i = -sum_j m_j (k_i/rho0_i + k_j/rho0_j) grad W_ij - k_i sum_b dPsi_b
+__device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, float& ax, float& ay, float& az) {
+  float ki = P.kr[p];
+  ax = ay = az = 0.0f;
+  int c = P.cnt[p];
+  const int* row = P.nbr + p;
+  for (int k = 0; k < c; ++k) {
+    int j = row[(size_t)k * P.n];
+    float4 xj = P.pos[j];
+    float krj = P.kr[j];
+    float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+    float W, F;
+    wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
+    float cF = (xj.w * (ki + krj)) * F;
+    ax = ADF_FMA(-cF, rx, ax);
+    ay = ADF_FMA(-cF, ry, ay);
+    az = ADF_FMA(-cF, rz, az);
+  }
+  float4 sg = P.slot_g[p];
+  if (sg.w >= 0.0f) {
+    float kk = P.kappa[p];
+    ax = ADF_FMA(-kk, sg.x, ax);
+    ay = ADF_FMA(-kk, sg.y, ay);
+    az = ADF_FMA(-kk, sg.z, az);
+  }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  if (P.converged[P.world_s[p]]) return;
+  float ax, ay, az;
+  pressure_accel(P, p, P.pos[p], ax, ay, az);
+  P.acc[p] = make_float4(ax, ay, az, 0.0f);
+}
+
+// pressure.py:294-352
+__global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  if (P.converged[P.world_s[p]]) return;
+  float4 xi = P.pos[p];
+  float4 ai = P.acc[p];
+  float r0 = P.vel[p].w;
+  float inv_r0 = 1.0f / r0;
+  float ar = 0.0f;
+  int c = P.cnt[p];
+  const int* row = P.nbr + p;
+  for (int k = 0; k < c; ++k) {
+    int j = row[(size_t)k * P.n];
+    float4 xj = P.pos[j];
+    float4 aj = P.acc[j];
+    float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+    float W, F;
+    wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
+    float aF = (xj.w * inv_r0) * F;
+    ar = ADF_FMA(aF, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz), ar);
+  }
+  float4 sg = P.slot_g[p];
+  if (sg.w >= 0.0f) ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
+  float kap = P.kappa[p];
+  ar = ADF_FMA(-P.reg[p], kap, ar);
+  const float dt = P.dt;
+  const bool div = P.mode == 0;
+  float dtn = div ? dt : dt * dt;
+  float scale = div ? 1.0f / dt : 1.0f / (dt * dt);
+  ar = ar * dtn;
+  float s = div ? -P.src[p] : 1.0f - P.src[p];
+  float r = s - ar;
+  float lb = P.lower[p];
+  float knew = maxr(kap - ((P.omega * r) * P.alpha[p]) * scale, lb);
+  P.kappa[p] = knew;
+  P.kr[p] = knew / r0;
+  float e = maxr(-r, 0.0f);
+  if (knew > lb) e = fabsf(r);
+  if (div) {
+    if (P.neff[p] < P.min_nb) e = 0.0f;
+    e = e * dt;
+  }
+  P.err_orig[P.id_of[p]] = e;
+}
+
+// ------------------------------------------------------------------------------------- per-world reductions
+// Fixed tree order (the oracle mirrors it): lanes fold in groups of 32 with offsets 16..1, then the 8 group sums
+// with offsets 4, 2, 1. Chunks of 256 particles are aligned to each world's start in the caller's order.
+__device__ __forceinline__ double fold256(double v, double* sm) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    double s[8];
+#pragma unroll
+    for (int g = 0; g < 8; ++g) s[g] = sm[g];
+#pragma unroll
+    for (int o = 4; o >= 1; o >>= 1)
+#pragma unroll
+      for (int l = 0; l < o; ++l) s[l] = s[l] + s[l + o];
+    r = s[0];
+  }
+  __syncthreads();
+  return r;
+}
+
+__device__ __forceinline__ float block_max256(float v, float* sm) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float r = -3.4e38f;
+  if (threadIdx.x == 0)
+    for (int g = 0; g < 8; ++g) r = fmaxf(r, sm[g]);
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_chunk_sum(const float* __restrict__ v, const int* chunk_begin,
+                                                   const int* chunk_end, double* part_sum, float* part_max,
+                                                   int* n_unconv) {
+  __shared__ double smd[8];
+  __shared__ float smf[8];
+  int c = blockIdx.x;
+  int i = chunk_begin[c] + threadIdx.x;
+  bool in = i < chunk_end[c];
+  float x = in ? v[i] : 0.0f;
+  double s = fold256(in ? (double)x : 0.0, smd);
+  float m = block_max256(in ? x : -3.4e38f, smf);
+  if (threadIdx.x == 0) {
+    part_sum[c] = s;
+    part_max[c] = m;
+    if (c == 0 && n_unconv) *n_unconv = 0;
+  }
+}
+
+// One block per world: the chunk partials (lane l takes chunks l, l + 256, ...), then the stop test
+// (pressure.py:370-390) when `check` is set.
+__global__ void __launch_bounds__(256) k_world_check(DevP P, int check, double* out_sum, float* out_max) {
+  __shared__ double smd[8];
+  __shared__ float smf[8];
+  int w = blockIdx.x;
+  int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
+  double a = 0.0;
+  float m = -3.4e38f;
+  for (int c = c0 + threadIdx.x; c < c1; c += 256) {
+    a = a + P.part_sum[c];
+    m = fmaxf(m, P.part_max[c]);
+  }
+  double s = fold256(a, smd);
+  float mx = block_max256(m, smf);
+  if (threadIdx.x != 0) return;
+  mx = maxr(mx, 0.0f);
+  if (!check) {
+    out_sum[w] = s;
+    out_max[w] = mx;
+    return;
+  }
+  P.emax[w] = mx;
+  if (P.converged[w]) return;
+  int it = P.iters[w] + 1;
+  P.iters[w] = it;
+  double na = P.n_active[w];
+  float mean = (float)(s / (na > 1.0 ? na : 1.0));
+  P.err_mean[w] = mean;
+  if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+  else atomicAdd(P.n_unconv, 1);
+}
+
+// ---------------------------------------------------------------------------------------- apply pressure
+// pressure.py:393-414 (lone particles: a push limited like a rigid contact's depenetration) and 461-480
+// (v += dt a, warm start stored dt-free). A lone particle has no neighbours, so no other particle reads its kappa.
+__global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const float dt = P.dt;
+  float4 vi = P.vel[p];
+  float kap = P.kappa[p];
+  float4 sg = P.slot_g[p];
+  if (P.cnt[p] == 0 && kap > 0.0f && sg.w >= 0.0f) {
+    float ps = sg.w;
+    float4 vbs = P.slot_vb[p];
+    float vbx = ps * vbs.x, vby = ps * vbs.y, vbz = ps * vbs.z;
+    float g = __fsqrt_rn(dot_plain(sg.x, sg.y, sg.z, sg.x, sg.y, sg.z));
+    if (g > 0.0f) {
+      if (ps > 0.0f) {
+        vbx = vbx / ps;
+        vby = vby / ps;
+        vbz = vbz / ps;
+      }
+      float nx = -sg.x / g, ny = -sg.y / g, nz = -sg.z / g;
+      float u = dotf(vi.x - vbx, vi.y - vby, vi.z - vbz, nx, ny, nz);
+      kap = minr(kap, maxr(P.v_sep - u, 0.0f) / (dt * g));
+      P.kappa[p] = kap;
+      P.kr[p] = kap / vi.w;
+    }
+  }
+  float ax, ay, az;
+  pressure_accel(P, p, P.pos[p], ax, ay, az);
+  P.acc[p] = make_float4(ax, ay, az, 0.0f);
+  P.vel[p] = make_float4(ADF_FMA(dt, ax, vi.x), ADF_FMA(dt, ay, vi.y), ADF_FMA(dt, az, vi.z), vi.w);
+  if (P.mode == 0) P.kv_s[p] = kap * dt;
+  else P.kd_s[p] = (kap * dt) * dt;
+}
+
+// ----------------------------------------------------------------------------------------- non-pressure
+// integrate.py:150-178: gravity, external force, XSPH with Monaghan's symmetric weight m_j / rho_bar_ij.
+__global__ void __launch_bounds__(BLOCK) k_xsph(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const float dt = P.dt;
+  float4 vi = P.vel[p];
+  int w = P.world_s[p];
+  float gx = P.gravity[3 * w], gy = P.gravity[3 * w + 1], gz = P.gravity[3 * w + 2];
+  float4 xi = P.pos[p];
+  if (P.f_ext) {
+    int i = P.id_of[p];
+    gx = gx + P.f_ext[3 * i] / xi.w;
+    gy = gy + P.f_ext[3 * i + 1] / xi.w;
+    gz = gz + P.f_ext[3 * i + 2] / xi.w;
+  }
+  float vx = ADF_FMA(dt, gx, vi.x), vy = ADF_FMA(dt, gy, vi.y), vz = ADF_FMA(dt, gz, vi.z);
+  const float c = P.xsph_c;
+  if (c > 0.0f) {
+    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    float rho_i = P.ratio[p] * vi.w;
+    int cn = P.cnt[p];
+    const int* row = P.nbr + p;
+    for (int k = 0; k < cn; ++k) {
+      int j = row[(size_t)k * P.n];
+      float4 vj = P.vel[j];
+      float rho_bar = 0.5f * (rho_i + P.ratio[j] * vj.w);
+      if (rho_bar > 0.0f) {
+        float4 xj = P.pos[j];
+        float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+        float W, F;
+        wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
+        float cw = (xj.w / rho_bar) * W;
+        cx = ADF_FMA(cw, vj.x - vi.x, cx);
+        cy = ADF_FMA(cw, vj.y - vi.y, cy);
+        cz = ADF_FMA(cw, vj.z - vi.z, cz);
+      }
+    }
+    vx = ADF_FMA(c, cx, vx);
+    vy = ADF_FMA(c, cy, vy);
+    vz = ADF_FMA(c, cz, vz);
+  }
+  P.vel2[p] = make_float4(vx, vy, vz, vi.w);
+}
+
+// ------------------------------------------------------------------------------------------------ finish
+// integrate.py:181-185 advection, particle_walls.py:131-135 wall advance, integrate.py:212-309 projection out of the
+// particle wall's advected slot plane (no SDF shapes: the sweep finds none), emitters.py:134-164 sinks and escape
+// box, integrate.py:312-326 speed; results written back to the caller's order.
+__device__ __forceinline__ bool in_box(const Sink& s, float x, float y, float z) {
+  float inv[4] = {-s.xform[3], -s.xform[4], -s.xform[5], s.xform[6]};
+  float lx, ly, lz;
+  quat_rotate(inv, x - s.xform[0], y - s.xform[1], z - s.xform[2], lx, ly, lz);
+  return fabsf(lx) <= s.half[0] && fabsf(ly) <= s.half[1] && fabsf(lz) <= s.half[2];
+}
+
+__global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int nf = P.nfw[0];
+  if (p >= nf + P.nfw[1]) return;
+  const float dt = P.dt;
+  int i = P.id_of[p];
+  float4 xi = P.pos[p];
+  float4 vi = P.vel[p];
+  float x = ADF_FMA(dt, vi.x, xi.x), y = ADF_FMA(dt, vi.y, xi.y), z = ADF_FMA(dt, vi.z, xi.z);
+  if (p >= nf) {  // wall particle
+    P.q[3 * i] = x;
+    P.q[3 * i + 1] = y;
+    P.q[3 * i + 2] = z;
+    return;
+  }
+  int w = P.world_s[p];
+  float vx = vi.x, vy = vi.y, vz = vi.z;
+  float4 sg = P.slot_g[p];
+  if (sg.w >= 0.0f) {
+    float4 nn = P.slot_n[p], vb = P.slot_vb[p], xb = P.slot_xb[p];
+    float px = ADF_FMA(dt, vb.x, xb.x), py = ADF_FMA(dt, vb.y, xb.y), pz = ADF_FMA(dt, vb.z, xb.z);
+    int moved = 0;
+    for (int pass = 0; pass < PROJECT_PASSES; ++pass) {
+      float d = dotf(x - px, y - py, z - pz, nn.x, nn.y, nn.z);
+      if (!(d < P.eps)) break;
+      float push = P.eps - d;
+      x = ADF_FMA(push, nn.x, x);
+      y = ADF_FMA(push, nn.y, y);
+      z = ADF_FMA(push, nn.z, z);
+      float vn = dotf(vx - vb.x, vy - vb.y, vz - vb.z, nn.x, nn.y, nn.z);
+      if (vn < 0.0f) {
+        vx = ADF_FMA(-vn, nn.x, vx);
+        vy = ADF_FMA(-vn, nn.y, vy);
+        vz = ADF_FMA(-vn, nn.z, vz);
+      }
+      moved = 1;
+    }
+    if (moved) atomicAdd(&P.projected[w], 1);
+  }
+  int gone = 0;
+  for (int s = 0; s < P.n_sinks; ++s)
+    if (P.sinks[s].world == w && in_box(P.sinks[s], x, y, z)) gone = 1;
+  if (P.has_bounds && gone == 0) {
+    bool out = x < P.blo[0] || y < P.blo[1] || z < P.blo[2] || x > P.bhi[0] || y > P.bhi[1] || z > P.bhi[2];
+    if (out || !isfinite((x + y) + z)) {
+      gone = 2;
+      atomicAdd(&P.escaped[w], 1);
+    }
+  }
+  if (gone) {
+    P.flags[i] = P.flags[i] & ~FLAG_ACTIVE;
+    P.phase[i] = (int8_t)-2;
+    vx = vy = vz = 0.0f;
+    atomicAdd((unsigned long long*)&P.mass_out[w], (unsigned long long)to_fixed(P.mass[i]));
+  } else {
+    float sp = __fsqrt_rn(dotf(vx, vy, vz, vx, vy, vz));
+    if (isfinite(sp) && isfinite((x + y) + z)) atomicMax(&P.max_speed_bits[w], __float_as_int(sp));
+    else {
+      atomicAdd(&P.nonfinite[w], 1);
+      atomicMax(&P.max_speed_bits[w], __float_as_int(1.0e30f));
+    }
+  }
+  P.q[3 * i] = x;
+  P.q[3 * i + 1] = y;
+  P.q[3 * i + 2] = z;
+  P.qd[3 * i] = vx;
+  P.qd[3 * i + 1] = vy;
+  P.qd[3 * i + 2] = vz;
+  P.kv[i] = P.kv_s[p];
+  P.kd[i] = P.kd_s[p];
+}
+
+// ---------------------------------------------------------------------------------------------- emitters
+// emitters.py:67-126: per emitter a layer clock; each due layer places its particles (spares of the emitter's
+// pool, in pool order) at the region's lattice offsets with the emitter's velocity; the cursor then advances.
+__global__ void k_emit_clock(const Emit* em, int n_e, float dt, const int* enabled, float* t_acc, int* emit_now) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_e) return;
+  emit_now[e] = 0;
+  if (enabled[e] == 0) return;
+  float t = t_acc[e] + dt;
+  if (t >= em[e].interval) {
+    t -= em[e].interval;
+    emit_now[e] = 1;
+  }
+  t_acc[e] = t;
+}
+
+__global__ void k_emit(DevP P, const Emit* em, int n_off, const int* off_emitter, const int* off_rank,
+                       const float* off_local, const int* emit_now, const int* cursor, const int* pool_ids,
+                       long long* mass_in, int* emit_overflow) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_off) return;
+  int e = off_emitter[c];
+  if (emit_now[e] == 0) return;
+  const Emit E = em[e];
+  int slot = cursor[e] + off_rank[c];
+  int w = E.world;
+  if (slot >= E.pool_size) {
+    atomicAdd(&emit_overflow[w], 1);
+    return;
+  }
+  int i = pool_ids[E.pool_begin + slot];
+  float rx, ry, rz;
+  quat_rotate(E.xform + 3, off_local[3 * c], off_local[3 * c + 1], off_local[3 * c + 2], rx, ry, rz);
+  float x = rx + E.xform[0], y = ry + E.xform[1], z = rz + E.xform[2];
+  P.q[3 * i] = x;
+  P.q[3 * i + 1] = y;
+  P.q[3 * i + 2] = z;
+  P.qd[3 * i] = E.vel[0];
+  P.qd[3 * i + 1] = E.vel[1];
+  P.qd[3 * i + 2] = E.vel[2];
+  P.flags[i] = P.flags[i] | FLAG_ACTIVE;
+  P.phase[i] = (int8_t)1;
+  atomicAdd((unsigned long long*)&mass_in[w], (unsigned long long)to_fixed(P.mass[i]));
+  float sp = __fsqrt_rn(dotf(E.vel[0], E.vel[1], E.vel[2], E.vel[0], E.vel[1], E.vel[2]));
+  if (isfinite(sp) && isfinite((x + y) + z)) atomicMax(&P.max_speed_bits[w], __float_as_int(sp));
+  else {
+    atomicAdd(&P.nonfinite[w], 1);
+    atomicMax(&P.max_speed_bits[w], __float_as_int(1.0e30f));
+  }
+}
+
+__global__ void k_emit_cursor(const Emit* em, int n_e, const int* emit_now, int* cursor) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_e) return;
+  if (emit_now[e] != 0) cursor[e] = min(cursor[e] + em[e].n_layer, em[e].pool_size);
+}
+
+// ------------------------------------------------------------------------------------------------- misc
+__global__ void k_wall_volume(int n, const int32_t* flags, const float* radius, float* wall_vol) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float r = radius[i];
+  wall_vol[i] = (flags[i] & FLAG_PROXY) ? (float)(8.0 * (double)r * (double)r * (double)r) : 0.0f;
+}
+
+__global__ void k_active_mass(DevP P, long long* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  int w = P.world[i];
+  if (w < 0 || w >= P.W || !is_fluid_orig(P, i)) return;
+  atomicAdd((unsigned long long*)&out[w], (unsigned long long)to_fixed(P.mass[i]));
+}
+
+__global__ void k_unsort_n(int n, const int* nfw, const int* id_of, const float* f, int stride, int comp, float* out,
+                           int ncomp) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || p >= nfw[0]) return;
+  int i = id_of[p];
+  for (int c = 0; c < ncomp; ++c) out[ncomp * i + c] = f[(size_t)stride * p + comp + c];
+}
+
+__global__ void k_fill_ones(int n, const int* nfw, const int* id_of, float* out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || p >= nfw[0]) return;
+  out[id_of[p]] = 1.0f;
+}
+
+__global__ void k_count_entries(int n, const int* nfw, const int* cnt, long long* out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = (p < n && p < nfw[0]) ? cnt[p] : 0;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd((unsigned long long*)out, (unsigned long long)c);
+}
+
+__global__ void k_reset(DevP P, const uint8_t* mask, const int32_t* flags0, const int8_t* phase0) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  int w = P.world[i];
+  if (w >= 0 && w < P.W && mask[w]) {
+    P.kv[i] = 0.0f;
+    P.kd[i] = 0.0f;
+    P.flags[i] = flags0[i];
+    P.phase[i] = phase0[i];
+  }
+}
+
+}  // namespace adf

@@ -1,0 +1,489 @@
+# SPDX-License-Identifier: Apache-2.0
+"""``SolverDFSPH``: the reference's DFSPH liquid solver interface (alloy/solvers/sph/solver.py:57-479) over the
+B200 CUDA library (include/alloy_dfsph.h, liballoy_dfsph.so).
+
+The class keeps the reference's constructor, ``step(state_in, state_out, control, contacts, dt)`` contract (dt > 0,
+early return for an empty model, state_out may alias state_in, nothing allocated per step), its report, ledger,
+reset, emitter and protocol methods and the ``alloy_state_arrays`` keys. Everything the step computes runs in the
+library's sm_100a kernels; this module holds host logic only (validation, constants, emitter tables) and has no CPU
+fallback: without a CUDA device or the library it raises.
+
+Scope of the CUDA path: cubic or Wendland kernel, relaxed Jacobi pressure solves, XSPH, particle walls (boundary
+particles flagged PROXY), emitters, sinks and the escape box. Settings outside it are refused in the constructor
+(``DFSPHConfig.unsupported``); ``pressure_solver="cg"`` and the resting-jitter rule fall back with a warning, as
+the reference itself falls back from CG (solver.py:89-91).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import logging
+from typing import ClassVar
+
+import numpy as np
+import torch
+
+from ... import _lib
+from .config import (PHASE_HELD, PHASE_SPARE, DFSPHConfig, host_constants, snap_down, stable_dt)
+from .model import ParticleFlags
+from .types import SPHReport
+
+log = logging.getLogger("alloy.sph")
+
+FIX_SCALE = float(2**40)
+_ACTIVE = int(ParticleFlags.ACTIVE)
+
+
+class _DevView:
+    """A raw device pointer seen as an array (``__cuda_array_interface__``) so torch can wrap library storage."""
+
+    def __init__(self, ptr: int, shape: tuple, typestr: str):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 2, "strides": None}
+
+
+def _ptr(a, dtype=None, shape0=None, what="array") -> int:
+    """Device pointer of a contiguous CUDA array (torch tensor, or anything with __cuda_array_interface__)."""
+    if a is None:
+        return 0
+    if isinstance(a, torch.Tensor):
+        if not a.is_cuda:
+            raise ValueError(f"SolverDFSPH: {what} must be on a CUDA device")
+        if not a.is_contiguous():
+            raise ValueError(f"SolverDFSPH: {what} must be contiguous")
+        if dtype is not None and a.dtype != dtype:
+            raise ValueError(f"SolverDFSPH: {what} must be {dtype}, got {a.dtype}")
+        if shape0 is not None and a.shape[0] != shape0:
+            raise ValueError(f"SolverDFSPH: {what} has {a.shape[0]} rows, expected {shape0}")
+        return a.data_ptr()
+    cai = getattr(a, "__cuda_array_interface__", None)
+    if cai is None:
+        raise TypeError(f"SolverDFSPH: {what} is not a CUDA array")
+    return int(cai["data"][0])
+
+
+def _host(a) -> np.ndarray:
+    if isinstance(a, torch.Tensor):
+        return a.detach().cpu().numpy()
+    if hasattr(a, "numpy"):
+        return a.numpy()
+    return np.asarray(a)
+
+
+def sph_phase(phase: np.ndarray) -> np.ndarray:
+    """The SPH solver's particles at build: liquid, spares and held (config.py:36-38)."""
+    return (phase >= PHASE_SPARE) | (phase == PHASE_HELD)
+
+
+def layer_offsets(half_extents: np.ndarray, velocity_local: np.ndarray, spacing: float) -> np.ndarray:
+    """Lattice points on the region's mid cross-section perpendicular to the velocity, whole spacings across each
+    side with 1e-6 of a cell's slack (emitters.py:48-64)."""
+    v = np.asarray(velocity_local, dtype=np.float64)
+    axis = int(np.argmax(np.abs(v))) if float(np.linalg.norm(v)) > 0.0 else 2
+    others = [a for a in range(3) if a != axis]
+    grids = []
+    for a in others:
+        n = max(int(np.floor(2.0 * half_extents[a] / spacing + 1.0e-6)), 1)
+        grids.append((np.arange(n) - 0.5 * (n - 1)) * spacing)
+    ga, gb = np.meshgrid(grids[0], grids[1], indexing="ij")
+    pts = np.zeros((ga.size, 3))
+    pts[:, others[0]] = ga.ravel()
+    pts[:, others[1]] = gb.ravel()
+    return pts.astype(np.float32)
+
+
+def quat_rotate_inv(q, v) -> np.ndarray:
+    """v rotated by the inverse of unit quaternion q = (x, y, z, w)."""
+    u = -np.asarray(q[:3], np.float64)
+    w = float(q[3])
+    v = np.asarray(v, np.float64)
+    return v * (2.0 * w * w - 1.0) + 2.0 * w * np.cross(u, v) + 2.0 * u * np.dot(u, v)
+
+
+def _xform7(region) -> np.ndarray:
+    x = np.asarray(tuple(region), np.float32).reshape(-1)
+    if x.size == 3:
+        x = np.concatenate([x, np.array([0.0, 0.0, 0.0, 1.0], np.float32)])
+    if x.size != 7:
+        raise ValueError("region must be a transform (px, py, pz, qx, qy, qz, qw)")
+    return x
+
+
+class SolverDFSPH:
+    """Divergence-free SPH (Bender & Koschier 2017) on B200: sorted-cell neighbour lists, particle walls,
+    per-world float64 convergence (module doc)."""
+
+    plugin_name: ClassVar[str] = "sph"
+    routes: ClassVar[frozenset[str]] = frozenset({"liquid_sph"})
+    alloy_clock_safety: ClassVar[float] = 1.0
+    Config = DFSPHConfig
+
+    def __init__(self, model, config: DFSPHConfig | None = None, *, capacity_per_world: int | None = None,
+                 soft_particles=None, soft_half_thickness: float = 0.0, soft_inertia: bool = True):
+        self.model = model
+        self.config = cfg = config or DFSPHConfig()
+        cfg.validate()
+        if soft_particles is not None:
+            raise ValueError("SolverDFSPH: soft walls (VBD faces) are not part of this build's CUDA path")
+        self._lib = _lib.lib()
+        n = int(model.particle_count)
+        W = int(model.world_count)
+        self.n, self.world_count = n, W
+        ns = getattr(model, "sph", None)
+        if ns is None or getattr(ns, "phase", None) is None or getattr(ns, "rest_density", None) is None:
+            raise ValueError("SolverDFSPH needs the sph:* custom attributes; call SolverDFSPH.register_custom_attributes"
+                             "(builder) before adding particles")
+        phase = _host(ns.phase).astype(np.int8) if n else np.zeros(0, np.int8)
+        world = _host(model.particle_world).astype(np.int32) if n else np.zeros(0, np.int32)
+        sph = sph_phase(phase)
+        if np.any(world[sph] < 0):
+            raise ValueError("SPH particles must belong to a world (particle_world >= 0)")
+        if n and np.any(np.diff(world[world >= 0]) < 0):
+            raise ValueError("particles must be contiguous per world (Model.particle_world sorted)")
+        ws = np.zeros(W + 1, np.int32)
+        if n:
+            ws[:] = _host(model.particle_world_start)[: W + 1]
+        self.world_start = ws
+        flags = _host(model.particle_flags).astype(np.int32) if n else np.zeros(0, np.int32)
+        proxy = (flags & int(ParticleFlags.PROXY)) != 0
+        if np.any(proxy & (world < 0)):
+            raise ValueError(f"SolverDFSPH: {int(np.sum(proxy & (world < 0)))} particle-wall particles are in no "
+                             "world (world -1); a wall needs the world of the liquid it bounds")
+        mu = _host(getattr(ns, "viscosity", None)) if getattr(ns, "viscosity", None) is not None and n else np.zeros(0)
+        mu_max = float(np.max(mu[sph])) if n and np.any(sph) and len(mu) else 0.0
+        missing = cfg.unsupported(mu_max)
+        if missing:
+            raise ValueError("SolverDFSPH (B200 build): not implemented on the CUDA path: " + ", ".join(missing))
+        self.pressure_solver = cfg.pressure_solver
+        if self.pressure_solver == "cg":
+            log.warning("SolverDFSPH: pressure_solver 'cg' is not in this build's CUDA path; using 'jacobi'")
+            self.pressure_solver = "jacobi"
+        if cfg.rest_jitter_speed:
+            log.warning("SolverDFSPH: the resting-jitter tolerance rule is not in this build's CUDA path; the density"
+                        " solve runs at max_density_error")
+        self._check_capacity(capacity_per_world, phase, ws)
+        if n and isinstance(model.particle_mass, torch.Tensor) and not model.particle_mass.is_cuda:
+            raise ValueError("SolverDFSPH: the model must live on a CUDA device (Model.finalize(device='cuda'))")
+        self.device = model.particle_mass.device if isinstance(model.particle_mass, torch.Tensor) else \
+            torch.device("cuda", 0)
+        self.hc = host_constants(cfg)
+        self._params = self._make_params(cfg, self.hc)
+        q_host = np.ascontiguousarray(_host(model.particle_q), np.float32).reshape(-1) if n else np.zeros(0, np.float32)
+        md = _lib.ModelDesc()
+        md.n, md.world_count = n, W
+        md.world_start = ws.ctypes.data_as(C.POINTER(C.c_int32))
+        md.q_host = q_host.ctypes.data_as(C.POINTER(C.c_float))
+        md.mass = _ptr(model.particle_mass, torch.float32, n, "particle_mass")
+        md.rest_density = _ptr(ns.rest_density, torch.float32, n, "sph.rest_density")
+        md.radius = _ptr(model.particle_radius, torch.float32, n, "particle_radius")
+        md.flags = _ptr(model.particle_flags, torch.int32, n, "particle_flags")
+        md.phase = _ptr(ns.phase, torch.int8, n, "sph.phase")
+        md.world = _ptr(model.particle_world, torch.int32, n, "particle_world")
+        md.gravity = _ptr(model.gravity, torch.float32, None, "gravity")
+        handle = C.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.check(self._lib.adf_create(C.byref(self._params), C.byref(md), self.device.index or 0,
+                                            C.byref(handle)), "SolverDFSPH")
+        self._h = handle
+        kv, kd = C.c_void_p(), C.c_void_p()
+        _lib.check(self._lib.adf_state_arrays(self._h, C.byref(kv), C.byref(kd)))
+        self._kv = torch.as_tensor(_DevView(kv.value, (max(n, 1),), "<f4"), device=self.device)[:n]
+        self._kd = torch.as_tensor(_DevView(kd.value, (max(n, 1),), "<f4"), device=self.device)[:n]
+        self._flags0 = model.particle_flags.clone() if n else None
+        self._phase0 = ns.phase.clone() if n else None
+        # emitter host table (runtime.py:452-525)
+        self._em_world: list[int] = []
+        self._em_pool: list[np.ndarray] = []
+        self._em_own: list[bool] = []
+        self._sinks = 0
+        self.bounds = None if cfg.world_bounds is None else cfg.world_bounds
+        log.info("SolverDFSPH (B200): %d particles in %d worlds, r=%g m, h=%g m, kernel=%s", n, W,
+                 cfg.particle_radius, cfg.h, cfg.kernel)
+
+    # ------------------------------------------------------------------------------------------------- setup
+    @staticmethod
+    def _make_params(cfg: DFSPHConfig, hc) -> _lib.Params:
+        p = _lib.Params()
+        p.kind = cfg.kernel_id
+        p.particle_radius = cfg.particle_radius
+        p.h, p.sigma, p.n_full, p.tot_min, p.lattice_grad = hc.h, hc.sigma, hc.n_full, hc.tot_min, hc.lattice_grad
+        p.wall_offset, p.wall_amplitude = hc.wall_offset, hc.wall_amplitude
+        p.taper0, p.taper1, p.reach = hc.taper0, hc.taper1, hc.reach
+        p.tol_den, p.tol_div = cfg.max_density_error, cfg.max_divergence_error
+        p.max_error_factor = cfg.max_error_factor
+        p.min_it, p.max_it = cfg.min_iterations, cfg.max_iterations
+        p.omega, p.warm_den, p.warm_div = cfg.jacobi_omega, cfg.warm_start_density, cfg.warm_start_divergence
+        p.min_nb = cfg.min_neighbors_divergence
+        p.divergence_solve, p.two_sided = int(cfg.divergence_solve), int(cfg.divergence_two_sided)
+        p.xsph_c = cfg.xsph_c if cfg.viscosity in ("xsph", "auto") else 0.0
+        p.capacity = cfg.neighbor_capacity
+        p.v_sep = cfg.contact_separation_speed
+        p.relief_speed = cfg.compression_relief_speed or 0.0
+        p.project_eps = hc.project_eps
+        if cfg.world_bounds is not None:
+            p.has_bounds = 1
+            for a in range(3):
+                p.bounds_lo[a], p.bounds_hi[a] = cfg.world_bounds[0][a], cfg.world_bounds[1][a]
+        return p
+
+    def _check_capacity(self, capacity_per_world, phase, ws) -> None:
+        if capacity_per_world is None:
+            return
+        for w in range(self.world_count):
+            have = int(np.count_nonzero(sph_phase(phase[ws[w]:ws[w + 1]])))
+            if have < capacity_per_world:
+                raise _lib.CapacityError(f"SolverDFSPH: world {w} has {have} SPH particle slots, "
+                                         f"capacity_per_world={capacity_per_world}")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._lib.adf_destroy(h)
+            finally:
+                self._h = None
+
+    def _stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    # ------------------------------------------------------------------------------------------------- step
+    def step(self, state_in, state_out, control, contacts, dt: float, *, observables=None) -> None:
+        del control, contacts, observables
+        if not dt > 0.0:
+            raise ValueError(f"SolverDFSPH.step: dt must be > 0, got {dt}")
+        if self.n == 0:
+            return
+        n = self.n
+        f = getattr(state_in, "particle_f", None)
+        rc = self._lib.adf_step(self._h, _ptr(state_in.particle_q, torch.float32, n, "particle_q"),
+                                _ptr(state_in.particle_qd, torch.float32, n, "particle_qd"),
+                                _ptr(state_out.particle_q, torch.float32, n, "particle_q"),
+                                _ptr(state_out.particle_qd, torch.float32, n, "particle_qd"),
+                                _ptr(f, torch.float32, n, "particle_f") if f is not None else None,
+                                float(dt), self._stream())
+        _lib.check(rc, "SolverDFSPH.step")
+
+    # ------------------------------------------------------------------------------------------------- reports
+    def _world_arrays(self) -> dict[str, np.ndarray]:
+        W = max(self.world_count, 1)
+        arrs = {"density_err": np.zeros(W, np.float32), "divergence_err": np.zeros(W, np.float32),
+                "iters_density": np.zeros(W, np.int32), "iters_divergence": np.zeros(W, np.int32),
+                "mass_in": np.zeros(W, np.int64), "mass_out": np.zeros(W, np.int64),
+                "mass_initial": np.zeros(W, np.int64), "escaped": np.zeros(W, np.int32),
+                "neighbor_overflow": np.zeros(W, np.int32), "max_speed": np.zeros(W, np.float32),
+                "density_err_max": np.zeros(W, np.float32), "projected": np.zeros(W, np.int32),
+                "nonfinite": np.zeros(W, np.int32), "emitter_overflow": np.zeros(W, np.int32),
+                "density_tol": np.zeros(W, np.float32)}
+        r = _lib.Report(**{k: v.ctypes.data for k, v in arrs.items()})
+        _lib.check(self._lib.adf_get_report(self._h, C.byref(r), self._stream()), "report")
+        return {k: v[: self.world_count] for k, v in arrs.items()}
+
+    def _active_mass(self) -> np.ndarray:
+        out = np.zeros(max(self.world_count, 1), np.int64)
+        _lib.check(self._lib.adf_active_mass(self._h, out.ctypes.data, self._stream()), "mass")
+        return out[: self.world_count]
+
+    def report(self) -> SPHReport:
+        a = self._world_arrays()
+        it_den, it_div = a["iters_density"].copy(), a["iters_divergence"].copy()
+        mx = self.config.max_iterations
+        return SPHReport(
+            density_err=a["density_err"].astype(np.float64), divergence_err=a["divergence_err"].astype(np.float64),
+            iters_density=it_den, iters_divergence=it_div,
+            mass_active=self._active_mass().astype(np.float64) / FIX_SCALE,
+            mass_in=a["mass_in"].astype(np.float64) / FIX_SCALE, mass_out=a["mass_out"].astype(np.float64) / FIX_SCALE,
+            escaped=a["escaped"].copy(), neighbor_overflow=a["neighbor_overflow"].copy(),
+            max_speed=a["max_speed"].astype(np.float64), unconverged=(it_den >= mx) | (it_div >= mx),
+            density_tol=a["density_tol"].astype(np.float64))
+
+    def diagnostics(self) -> dict[str, np.ndarray]:
+        """Per-world counters beyond SPHReport (runtime.py:410-418)."""
+        a = self._world_arrays()
+        return {"density_err_max": a["density_err_max"].astype(np.float64), "projected": a["projected"],
+                "nonfinite": a["nonfinite"], "emitter_overflow": a["emitter_overflow"],
+                "swept": np.zeros(self.world_count, np.int32), "cavitating": np.zeros(self.world_count, np.int32)}
+
+    def mass_ledger(self) -> dict[str, np.ndarray]:
+        """Exact int64 fixed-point ledger per world: initial, in, out, active (active + out == initial + in)."""
+        a = self._world_arrays()
+        return {"initial": a["mass_initial"].copy(), "in": a["mass_in"].copy(), "out": a["mass_out"].copy(),
+                "active": self._active_mass(), "scale": np.float64(FIX_SCALE)}
+
+    def density_ratio(self, state) -> tuple[np.ndarray, np.ndarray]:
+        """Density ratio rho/rho0 of every particle of ``state`` and the active-liquid mask (solver.py:386-393)."""
+        if self.n == 0:
+            return np.zeros(0), np.zeros(0, dtype=bool)
+        ratio = torch.zeros(self.n, dtype=torch.float32, device=self.device)
+        active = torch.zeros(self.n, dtype=torch.float32, device=self.device)
+        _lib.check(self._lib.adf_density_ratio(self._h, _ptr(state.particle_q), _ptr(state.particle_qd),
+                                               ratio.data_ptr(), active.data_ptr(), self._stream()), "density_ratio")
+        return ratio.cpu().numpy(), active.cpu().numpy() > 0.0
+
+    def neighbor_rows(self) -> tuple[np.ndarray, np.ndarray]:
+        """The last lists as global particle ids [n, capacity] (-1 past count) and counts (neighbors.py:285-295)."""
+        K = self.config.neighbor_capacity
+        rows = np.zeros((self.n, K), np.int32)
+        cnt = np.zeros(self.n, np.int32)
+        _lib.check(self._lib.adf_neighbor_rows(self._h, rows.ctypes.data, cnt.ctypes.data, self._stream()),
+                   "neighbor_rows")
+        return rows, cnt
+
+    def debug_field(self, name: str) -> np.ndarray:
+        """A per-particle field of the last step in particle order (parity tests)."""
+        three = name in ("acc", "slot_g", "slot_vb", "slot_n")
+        out = torch.zeros((self.n, 3) if three else self.n, dtype=torch.float32, device=self.device)
+        _lib.check(self._lib.adf_debug_field(self._h, name.encode(), out.data_ptr(), self._stream()), "debug_field")
+        return out.cpu().numpy()
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.adf_kernel_launches(self._h))
+
+    def profile(self, enable: bool) -> None:
+        """Time every kernel group with CUDA events on the launch stream (``profile_read``)."""
+        _lib.check(self._lib.adf_profile_enable(self._h, int(bool(enable))), "profile")
+
+    def profile_read(self) -> dict[str, tuple[float, int]]:
+        """{kind: (milliseconds, launches)} since the last read (include/alloy_dfsph.h ADF_PROF_KINDS)."""
+        ms = np.zeros(len(_lib.PROF_KINDS), np.float64)
+        cnt = np.zeros(len(_lib.PROF_KINDS), np.int64)
+        _lib.check(self._lib.adf_profile_read(self._h, ms.ctypes.data, cnt.ctypes.data), "profile_read")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.PROF_KINDS)}
+
+    def list_stats(self) -> tuple[int, int]:
+        """(liquid particles, neighbour-row entries) of the last list build."""
+        nf = np.zeros(1, np.int32)
+        ne = np.zeros(1, np.int64)
+        _lib.check(self._lib.adf_list_stats(self._h, nf.ctypes.data, ne.ctypes.data, self._stream()), "list_stats")
+        return int(nf[0]), int(ne[0])
+
+    # ------------------------------------------------------------------------------------------------- control
+    def reset(self, state=None, world_mask=None, flags: int | None = None) -> None:
+        """Masked worlds (all when None) back to their build-time SPH configuration (solver.py:353-362)."""
+        del state, flags
+        if self.n == 0:
+            return
+        mask = None
+        if world_mask is not None:
+            m = _host(world_mask).astype(np.uint8)[: self.world_count]
+            mask = np.ascontiguousarray(m)
+        _lib.check(self._lib.adf_reset(self._h, mask.ctypes.data if mask is not None else None,
+                                       self._flags0.data_ptr(), self._phase0.data_ptr(), self._stream()), "reset")
+
+    def choose_dt(self, control_dt: float) -> float:
+        """CFL step from the last step's max speed, snapped down to the control grid (solver.py:424-426)."""
+        a = self._world_arrays()
+        v = float(np.max(a["max_speed"])) if self.world_count else 0.0
+        return snap_down(stable_dt(self.config, v), control_dt)
+
+    def alloy_stable_dt(self, state, contacts, out) -> None:
+        """out[w] = clamp(cfl 2r / |v|max, dt_min, dt_max) over the state's liquid (runtime.py:667-676)."""
+        del contacts
+        cfg = self.config
+        qd = state.particle_qd
+        fl = (self.model.particle_flags & _ACTIVE) != 0
+        liquid = fl & (self.model.sph.phase >= 1)
+        speed = torch.linalg.vector_norm(qd, dim=1)
+        speed = torch.where(torch.isfinite(speed), speed, torch.full_like(speed, 1.0e30))
+        speed = torch.where(liquid, speed, torch.zeros_like(speed))
+        vmax = torch.zeros(self.world_count, dtype=torch.float32, device=self.device)
+        vmax.scatter_reduce_(0, self.model.particle_world.long().clamp(min=0), speed, reduce="amax")
+        dt = torch.where(vmax > 0.0, torch.clamp(cfg.cfl * cfg.spacing / vmax.clamp(min=1e-30), cfg.dt_min,
+                                                   cfg.dt_max), torch.full_like(vmax, cfg.dt_max))
+        out.copy_(dt)
+
+    def alloy_capacity_report(self) -> dict[str, int]:
+        a = self._world_arrays()
+        return {"neighbor_overflow": int(a["neighbor_overflow"].sum()),
+                "emitter_overflow": int(a["emitter_overflow"].sum())}
+
+    def alloy_state_arrays(self, state=None) -> dict:
+        """The solver state a snapshot must hold beside State (coupling_hooks.py:260-271)."""
+        del state
+        return {"sph.kappa_v": self._kv, "sph.kappa_d": self._kd, "sph.phase": self.model.sph.phase,
+                "particle_flags": self.model.particle_flags}
+
+    def alloy_state_worlds(self) -> dict:
+        pw = self.model.particle_world
+        return {"sph.kappa_v": pw, "sph.kappa_d": pw, "sph.phase": pw, "particle_flags": pw}
+
+    # ------------------------------------------------------------------------------------------------ emitters
+    def _spares(self, w: int) -> np.ndarray:
+        ph = _host(self.model.sph.phase)
+        wo = _host(self.model.particle_world)
+        fl = _host(self.model.particle_flags)
+        return np.nonzero((ph == PHASE_SPARE) & (wo == w) & ((fl & _ACTIVE) == 0))[0].astype(np.int32)
+
+    def _first_sph(self, world: int) -> int:
+        ws = self.world_start
+        ph = _host(self.model.sph.phase)[ws[world]:ws[world + 1]]
+        idx = np.nonzero(sph_phase(ph))[0]
+        if len(idx) == 0:
+            raise ValueError(f"world {world} has no SPH particles or spares")
+        return int(ws[world] + idx[0])
+
+    def add_emitter(self, world: int, region, half_extents, rate: float, velocity, pool=None) -> int:
+        """Emit liquid from a box region at ``rate`` [m^3/s] with ``velocity`` [m/s] by activating spares
+        (runtime.py:498-525)."""
+        if not 0 <= world < self.world_count:
+            raise ValueError(f"add_emitter: world {world} out of range")
+        if rate <= 0.0:
+            raise ValueError("add_emitter: rate must be > 0 [m^3/s]")
+        cfg = self.config
+        X = _xform7(region)
+        v_local = quat_rotate_inv(X[3:], np.asarray(velocity, np.float64))
+        offs = layer_offsets(np.asarray(half_extents, dtype=np.float64), v_local, cfg.spacing)
+        i0 = self._first_sph(world)
+        rho0 = float(_host(self.model.sph.rest_density)[i0])
+        mass = float(_host(self.model.particle_mass)[i0])
+        interval = len(offs) * (mass / rho0) / rate
+        area = len(offs) * cfg.spacing * cfg.spacing
+        speed = float(np.linalg.norm(v_local))
+        if speed > 0.0 and not 0.8 <= rate / (area * speed) <= 1.25:
+            log.warning("SPH emitter rate %.3g m^3/s vs area*|v| %.3g m^3/s: layers will over/under-pack", rate,
+                        area * speed)
+        own = pool is not None
+        pool_ids = (np.intersect1d(np.asarray(pool), self._spares(world)).astype(np.int32) if own
+                    else np.zeros(0, np.int32))
+        e = self._lib.adf_add_emitter(self._h, int(world), X.ctypes.data, offs.ctypes.data, len(offs),
+                                      np.asarray(velocity, np.float32).ctypes.data, C.c_float(interval),
+                                      pool_ids.ctypes.data, len(pool_ids))
+        _lib.check(e if e < 0 else 0, "add_emitter")
+        self._em_world.append(world)
+        self._em_pool.append(pool_ids)
+        self._em_own.append(own)
+        self._split_pools(world)
+        log.info("SPH emitter %d: world %d, %d particles per layer every %.4g s", e, world, len(offs), interval)
+        return int(e)
+
+    def _split_pools(self, world: int) -> None:
+        """Share the world's unused spares evenly among its emitters given no pool (emitters.py:225-238)."""
+        spares = self._spares(world)
+        owned = [self._em_pool[e] for e, w in enumerate(self._em_world) if w == world and self._em_own[e]]
+        free = np.setdiff1d(spares, np.concatenate(owned)) if owned else spares
+        mine = [e for e, w in enumerate(self._em_world) if w == world and not self._em_own[e]]
+        if not mine:
+            return
+        cursors = np.zeros(len(self._em_world), np.int32)
+        _lib.check(self._lib.adf_emitter_state(self._h, None, cursors.ctypes.data), "emitters")
+        new = {}
+        if any(cursors[e] > 0 for e in mine[:-1]):
+            used = np.concatenate([self._em_pool[e] for e in mine[:-1]]) if len(mine) > 1 else np.zeros(0, np.int32)
+            new[mine[-1]] = np.setdiff1d(free, used).astype(np.int32)
+        else:
+            for k, part in enumerate(np.array_split(free, len(mine))):
+                new[mine[k]] = part.astype(np.int32)
+        for e, pool in new.items():
+            pool = np.ascontiguousarray(pool, np.int32)
+            self._em_pool[e] = pool
+            _lib.check(self._lib.adf_set_emitter_pool(self._h, int(e), pool.ctypes.data, len(pool)), "emitter pool")
+
+    def set_emitter_enabled(self, e: int, on: bool) -> None:
+        _lib.check(self._lib.adf_set_emitter_enabled(self._h, int(e), int(bool(on))), "set_emitter_enabled")
+
+    def add_sink(self, world: int, region, half_extents) -> int:
+        """Retire particles that enter a box region; their mass goes to ``mass_out`` (runtime.py:557-565)."""
+        X = _xform7(region)
+        half = np.asarray(half_extents, np.float32)
+        k = self._lib.adf_add_sink(self._h, int(world), X.ctypes.data, half.ctypes.data)
+        _lib.check(k if k < 0 else 0, "add_sink")
+        return int(k)

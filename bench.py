@@ -1,0 +1,281 @@
+#!/usr/bin/env python
+# SPDX-License-Identifier: Apache-2.0
+"""Benchmark of the DFSPH liquid step: particle-steps/s of liquid particles, one JSON line on rank 0.
+
+Workload (default): the 1,048,576-particle dam break (128 x 64 x 128 block at 0.01 m, seeded +-1 % jitter) in a
+closed 4 x 2 x 2 m tank of boundary particles, dt 0.5 ms, cubic kernel, Jacobi, tolerances 1e-3, FP32 particles with
+float64 per-world residual sums. A step is one full DFSPH step over every particle; steps continue the same run
+(warm starts carried). The working set per step (~0.9 GB) is far larger than L2, so no flush is needed between steps.
+
+Arms:
+  --impl b200       this package's CUDA path (one process per GPU; N > 1 runs N replicas of the single world:
+                    the path has no data-path collective)
+  --impl reference  the reference algorithm on the host cores: the CPU oracle (a restatement of the reference's
+                    Warp kernels; Warp itself is not installed) with every host thread, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s at ≤0.1% density error, warm-started vs plain DFSPH; HBM GB/s"
+UNIT = "particle-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", choices=("large_dam_break", "dam_break"), default="large_dam_break")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_scene(name: str, device):
+    from alloy_b200.solvers.sph.testing import dam_break, large_dam_break
+
+    if name == "large_dam_break":
+        return large_dam_break(device=device)
+    return dam_break(device=device)
+
+
+def workload_config(sc, name: str) -> dict:
+    return {"workload": f"{name}: {sc.fluid_count} liquid particles + {sc.wall_count} boundary particles, "
+                        f"dt {sc.dt} s, Jacobi, tol 1e-3/1e-3, cubic h=2 spacings",
+            "liquid_particles": sc.fluid_count, "boundary_particles": sc.wall_count, "dt": sc.dt,
+            "spacing": sc.config.spacing, "l2": "inputs larger than L2 (working set > 126 MB per step)"}
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms during the timed region (clocks, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        self.f.close()
+        os.unlink(self.f.name)
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9 and r[0].strip() == str(self.idx)]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_oracle_run(sc, steps: int, warmup: int, budget_s: float | None):
+    """Steps of the CPU oracle (all host threads) on the scene from its start state: (particle-steps/s, steps, s)."""
+    from oracle.pyoracle import Oracle
+
+    orc = Oracle(sc.model.host(), sc.config)
+    for _ in range(warmup):
+        orc.step(sc.dt)
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        orc.step(sc.dt)
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
+    t = time.perf_counter() - t0
+    return sc.fluid_count * done / t, done, t
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sc = make_scene(args.workload, "cpu")
+    threads = os.cpu_count() or 1
+    value, done, t = cpu_oracle_run(sc, args.steps, args.warmup, None)
+    sample = (f"{done} full steps after {args.warmup} warm-up steps of the {args.workload} workload from its start "
+              f"state, {threads} OpenMP threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / max(done, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(sc, args.workload),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "CPU oracle: a C++/OpenMP restatement of the reference's Warp kernels (warp-lang is not installed)"}))
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from alloy_b200.solvers.sph import SolverDFSPH
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    sc = make_scene(args.workload, dev)
+    sol = SolverDFSPH(sc.model, sc.config)
+    a, b = sc.model.state(), sc.model.state()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        sol.step(a, b, None, None, sc.dt)
+        a, b = b, a
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    sol.profile(True)
+    sol.profile_read()
+    launches0 = sol.kernel_launches()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sol.step(a, b, None, None, sc.dt)
+        a, b = b, a
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    t = e0.elapsed_time(e1) * 1e-3
+    prof = sol.profile_read()
+    sol.profile(False)
+    launches = sol.kernel_launches() - launches0
+    tmax = torch.tensor([t], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    t_max = float(tmax.item())
+    value = sc.fluid_count * world * args.steps / t_max
+
+    # end to end through the public API with host buffers: H2D of the state, the step, D2H of the state and report
+    n = sc.model.particle_count
+    hq = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    hqd = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    hq.copy_(a.particle_q)
+    hqd.copy_(a.particle_qd)
+    it_den, it_div, den_err, den_max = [], [], [], []
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        a.particle_q.copy_(hq, non_blocking=True)
+        a.particle_qd.copy_(hqd, non_blocking=True)
+        sol.step(a, b, None, None, sc.dt)
+        hq.copy_(b.particle_q, non_blocking=True)
+        hqd.copy_(b.particle_qd, non_blocking=True)
+        r = sol.report()  # synchronises the stream and reads the per-world result
+        it_den.append(int(r.iters_density.max()))
+        it_div.append(int(r.iters_divergence.max()))
+        den_err.append(float(r.density_err.max()))
+    torch.cuda.synchronize(dev)
+    t_e2e = time.perf_counter() - t0
+    den_max.append(float(sol.diagnostics()["density_err_max"].max()))
+    e2e = {"value": sc.fluid_count * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
+           "d2h_bytes_per_step": 2 * n * 12 + sol.world_count * 64}
+
+    nf, entries = sol.list_stats()
+    nbar = entries / max(nf, 1)
+    pk = peaks()
+    # algorithmic bytes per liquid particle and launch (element sizes of the reference, 2-byte list entries)
+    alg = {"jacobi": 72.0 + 2.0 * nbar, "accel": 44.0 + 2.0 * nbar, "density_alpha": 52.0 + 2.0 * nbar,
+           "solve_init": 80.0 + 2.0 * nbar, "apply": 60.0 + 2.0 * nbar, "xsph": 68.0 + 2.0 * nbar,
+           "lists": 44.0 + 2.0 * nbar}
+    total_ms = sum(v[0] for v in prof.values())
+    dom = max(alg, key=lambda k: prof[k][0])
+    ms, cnt = prof[dom]
+    per_launch_s = ms * 1e-3 / max(cnt, 1)
+    achieved = alg[dom] * nf / per_launch_s / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(dom)
+    shares = {k: round(v[0] / total_ms, 4) for k, v in prof.items() if total_ms > 0}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        csc = make_scene(args.workload, "cpu")
+        threads = os.cpu_count() or 1
+        v_cpu, done, t_cpu = cpu_oracle_run(csc, 1000, 1, 20.0)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{done} full steps (after 1 warm-up step) of the same workload from its start state, "
+                         f"{t_cpu:.1f} s, CPU oracle with {threads} OpenMP threads"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {**workload_config(sc, args.workload),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                         "peak_src": pk["src"], "alg_bytes_per_particle": alg[dom], "mean_neighbours": nbar,
+                         "avg_launch_us": per_launch_s * 1e6, "launches": cnt},
+            "kernel_time_share": shares,
+            "solver_stats": {"iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean":
+                             float(np.mean(it_div)), "density_err_mean_max_over_steps": float(np.max(den_err)),
+                             "density_err_max_last_step": den_max[-1]},
+            "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,186 @@
+/* SPDX-License-Identifier: Apache-2.0
+ *
+ * alloy_dfsph.h — C ABI of the B200 DFSPH liquid step (liballoy_dfsph.so).
+ *
+ * This is the drop-in boundary for the reference's SolverDFSPH (argonrobotics-ai/alloy, alloy/solvers/sph). Each entry
+ * point names the reference interface it replaces. All particle arrays are in the caller's particle order (the
+ * Newton model's), float32 vec3 as [n][3]; device pointers are CUDA device memory of the solver's device. Calls
+ * return ADF_OK (0) or an ADF_ERR_* code; adf_last_error() gives the message of the calling thread's last failure.
+ * No C++ exception or torch type crosses this boundary. adf_step allocates nothing.
+ */
+#ifndef ALLOY_DFSPH_H
+#define ALLOY_DFSPH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ADF_OK 0
+#define ADF_ERR_VALUE 1    /* invalid argument or model layout (the reference raises ValueError) */
+#define ADF_ERR_CAPACITY 2 /* a fixed capacity is exceeded (the reference raises CapacityError) */
+#define ADF_ERR_CUDA 3     /* a CUDA runtime call failed */
+#define ADF_ERR_STATE 4    /* the call is not valid in the solver's current state */
+
+typedef struct adf_solver adf_solver;
+
+/* Solver constants. Configuration fields follow DFSPHConfig (alloy/solvers/sph/config.py:46-131); the derived host
+ * constants (sigma, n_full, tot_min, lattice_grad, wall_offset, wall_amplitude, taper0/1, reach, project_eps) are
+ * the float64 values of config.py:225-236, kernels.py:221-270, layout.py:195-244 and solver.py:94, 483. */
+typedef struct {
+  int kind;                 /* 0 cubic spline, 1 Wendland C2 */
+  double particle_radius;   /* r [m] */
+  double h;                 /* support radius [m] */
+  double sigma;             /* W(0) = 8/(pi h^3) or 21/(2 pi h^3) */
+  double n_full;            /* neighbours of an interior lattice particle */
+  double tot_min;           /* diagonal floor x lattice diagonal [1/m^2] */
+  double lattice_grad;      /* sqrt(lattice diagonal) [1/m] */
+  double wall_offset;       /* boundary fit delta [m] */
+  double wall_amplitude;    /* boundary fit A */
+  double taper0, taper1;    /* slot taper interval [m] */
+  double reach;             /* slots kept below this phi [m] */
+  double tol_den, tol_div;  /* max_density_error, max_divergence_error */
+  double max_error_factor;
+  int min_it, max_it;
+  double omega;             /* jacobi_omega */
+  double warm_den, warm_div;
+  double min_nb;            /* min_neighbors_divergence */
+  int divergence_solve, two_sided;
+  double xsph_c;            /* 0: no XSPH */
+  int capacity;             /* neighbor_capacity (8..64) */
+  double v_sep;             /* contact_separation_speed [m/s] */
+  double relief_speed;      /* compression_relief_speed [m/s]; <= 0: uncapped */
+  double project_eps;       /* wall projection skin [m] */
+  int has_bounds;           /* world_bounds given: escape box */
+  double bounds_lo[3], bounds_hi[3];
+} adf_params;
+
+/* The model's particle arrays (Newton Model + sph:* attributes), bound once at creation. */
+typedef struct {
+  int n;                         /* particle count */
+  int world_count;               /* W */
+  const int32_t* world_start;    /* host [W + 1], contiguous worlds (Model.particle_world_start) */
+  const float* q_host;           /* host [n][3] start positions: size the per-world grids (may be NULL) */
+  const float* mass;             /* device [n] particle_mass */
+  const float* rest_density;     /* device [n] sph:rest_density */
+  const float* radius;           /* device [n] particle_radius (wall particles carry volume 8 r^3) */
+  int32_t* flags;                /* device [n] particle_flags (written by emitters, sinks, the escape box) */
+  int8_t* phase;                 /* device [n] sph:phase (written likewise) */
+  const int32_t* world;          /* device [n] particle_world */
+  const float* gravity;          /* device [W][3] Model.gravity */
+} adf_model;
+
+/* Per-world host outputs of adf_get_report; any pointer may be NULL. SPHReport (types.py:11-28) and
+ * WorldStats.diagnostics (runtime.py:410-418). Masses are int64 fixed point at 2^40 per kg. */
+typedef struct {
+  float* density_err;
+  float* divergence_err;
+  int32_t* iters_density;
+  int32_t* iters_divergence;
+  int64_t* mass_in;
+  int64_t* mass_out;
+  int64_t* mass_initial;
+  int32_t* escaped;
+  int32_t* neighbor_overflow;
+  float* max_speed;
+  float* density_err_max;
+  int32_t* projected;
+  int32_t* nonfinite;
+  int32_t* emitter_overflow;
+  float* density_tol;
+} adf_report;
+
+/* Message of this thread's last failed call ("" if none). */
+const char* adf_last_error(void);
+
+/* Replaces SolverDFSPH.__init__ (solver.py:72-111): validates the layout (layout.py:47-72), binds the model arrays,
+ * allocates every work array at fixed capacity and sizes the per-world cell grids. */
+int adf_create(const adf_params* params, const adf_model* model, int device, adf_solver** out);
+
+/* Frees the solver's device memory (the model's arrays are the caller's). */
+void adf_destroy(adf_solver* solver);
+
+/* Replaces SolverDFSPH.step (solver.py:218-268): one DFSPH step of every world. q_in/qd_in may alias q_out/qd_out;
+ * f_ext (device [n][3] particle_f, N) may be NULL. Enqueued on `stream` (cudaStream_t; NULL: legacy default). */
+int adf_step(adf_solver* solver, const float* q_in, const float* qd_in, float* q_out, float* qd_out,
+             const float* f_ext, double dt, void* stream);
+
+/* Replaces SolverDFSPH.density_ratio (solver.py:386-393): density ratio and active mask of every particle of the
+ * state (device [n] outputs, 0 for non-liquid particles) from fresh lists and wall slots. */
+int adf_density_ratio(adf_solver* solver, const float* q, const float* qd, float* ratio_out, float* active_out,
+                      void* stream);
+
+/* Replaces SolverDFSPH.report (solver.py:365-367) and stats.diagnostics: synchronises `stream`, copies to host. */
+int adf_get_report(adf_solver* solver, adf_report* out, void* stream);
+
+/* Replaces WorldStats._active_mass (runtime.py:381-385): int64 fixed-point liquid mass per world, host [W]. */
+int adf_active_mass(adf_solver* solver, int64_t* out_host, void* stream);
+
+/* Warm starts k dt (divergence) and k dt^2 (density) per particle: the alloy_state_arrays keys "sph.kappa_v" and
+ * "sph.kappa_d" (coupling_hooks.py:260-271). Device [n] copies in particle order. */
+int adf_get_warm_starts(adf_solver* solver, float* kappa_v, float* kappa_d, void* stream);
+int adf_set_warm_starts(adf_solver* solver, const float* kappa_v, const float* kappa_d, void* stream);
+
+/* The solver's own warm-start storage (device [n] float32 each, particle order), for snapshot code that saves and
+ * restores "sph.kappa_v" / "sph.kappa_d" in place (coupling_hooks.py:260-271). Valid until adf_destroy. */
+int adf_state_arrays(adf_solver* solver, float** kappa_v, float** kappa_d);
+
+/* Replaces SolverDFSPH.reset (solver.py:353-362) + WorldStats.reset (runtime.py:431-449) + emitters.rewind
+ * (emitters.py:241-255): masked worlds (host [W] bytes; NULL = all) get warm starts cleared, flags and phase back to
+ * flags0/phase0 (device [n]), their counters and ledgers zeroed and their emitters rewound. */
+int adf_reset(adf_solver* solver, const uint8_t* world_mask, const int32_t* flags0, const int8_t* phase0,
+              void* stream);
+
+/* Replaces EmitterManager.add_emitter (runtime.py:498-525) after its host logic: a layer emitter with its layer
+ * offsets (host [n_off][3], region frame), transform (px py pz qx qy qz qw), velocity, interval [s] and its pool of
+ * spare particle ids (host, ascending). Returns the emitter index (>= 0) or -ADF_ERR_*. Between steps only. */
+int adf_add_emitter(adf_solver* solver, int world, const float* xform, const float* offsets, int n_off,
+                    const float* velocity, float interval, const int32_t* pool, int pool_size);
+
+/* Replaces the pool reassignment of emitters.split_pools (emitters.py:225-238): emitter `emitter` draws from `pool`
+ * (host ids, ascending) from now on; its cursor is kept. Between steps only. */
+int adf_set_emitter_pool(adf_solver* solver, int emitter, const int32_t* pool, int pool_size);
+
+/* Layer clocks [s] and cursors (particles of the pool already emitted) of every emitter, host arrays
+ * (EmitterDevice.t_acc / cursor, emitters.py:174-213); either may be NULL. */
+int adf_emitter_state(adf_solver* solver, float* t_acc, int32_t* cursor);
+
+/* Replaces SolverDFSPH.set_emitter_enabled (solver.py:438-447). */
+int adf_set_emitter_enabled(adf_solver* solver, int emitter, int enabled);
+
+/* Replaces EmitterManager.add_sink (runtime.py:557-565): retire liquid entering the box (xform, half extents). */
+int adf_add_sink(adf_solver* solver, int world, const float* xform, const float* half_extents);
+
+/* Replaces NeighborLists.global_rows (neighbors.py:285-295): the last step's lists as global particle ids, host
+ * rows [n][capacity] (entries past count are -1) and counts [n]; synchronises `stream`. */
+int adf_neighbor_rows(adf_solver* solver, int32_t* rows, int32_t* count, void* stream);
+
+/* Diagnostics for parity tests: a per-particle float field of the last step in particle order (device [n] or
+ * [n][3]): ratio alpha neff reg src kappa lower err slot_psi slot_phi (scalars), acc slot_g slot_vb slot_n (vec3). */
+int adf_debug_field(adf_solver* solver, const char* name, float* out, void* stream);
+
+/* Per-world float64 sums and maxima of a float array in the solver's tree order (reduce.py:185-227); device
+ * in/out; exported for the reducer's parity test. */
+int adf_world_sum(adf_solver* solver, const float* values, double* out_sum, float* out_max, void* stream);
+
+/* Number of kernels this library enqueued since creation (launch accounting for benchmarks). */
+int64_t adf_kernel_launches(const adf_solver* solver);
+
+/* Live kernel timing with CUDA events on the launch stream (benchmarks). Kinds, in this order: 0 sort (classify,
+ * scan, scatter), 1 neighbour rows, 2 wall slots, 3 density and factor, 4 solve start, 5 pressure acceleration,
+ * 6 Jacobi update, 7 per-world reduction and stop test, 8 apply pressure, 9 XSPH, 10 advect/project/write-back,
+ * 11 emitters. adf_profile_read synchronises, returns the summed milliseconds and launch counts per kind since the
+ * last read (host arrays of ADF_PROF_KINDS) and starts a new window. */
+#define ADF_PROF_KINDS 12
+int adf_profile_enable(adf_solver* solver, int enable);
+int adf_profile_read(adf_solver* solver, double* ms, int64_t* launches);
+
+/* Liquid particle count and neighbour-row entries of the last list build (host outputs; synchronises `stream`). */
+int adf_list_stats(adf_solver* solver, int32_t* fluid, int64_t* entries, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALLOY_DFSPH_H */

@@ -1,0 +1,1080 @@
+// TEST INFRASTRUCTURE — NOT PART OF THE PRODUCT.
+//
+// CPU oracle for the DFSPH liquid step of argonrobotics-ai/alloy (alloy/solvers/sph), restated in plain C++ from
+// the reference's Warp kernels. Only tests/, __graft_entry__.smoke() and bench.py's CPU legs may load it, and there
+// only as the checker or the timed CPU baseline; the CUDA product never links or calls it.
+//
+// What it follows (reference file:line, paths inside the alloy project):
+//   kernels.py:41-77      cubic / Wendland W and grad W              -> wf()
+//   kernels.py:80-138     projected kernel, half-space volume Psi    -> halfspace()
+//   neighbors.py:36-51    particle groups (fluid = world, wall = -2 - world)
+//   neighbors.py:160-195  id-sorted lists, lowest K kept, overflow   -> build_lists()
+//   particle_walls.py:65-119  wall colour, 30-step bisection, plane  -> wall_slot()
+//   boundary.py:241-287, 336-396  slot fill with fit and taper (one particle-wall slot)
+//   pressure.py:144-193   density and DFSPH factor                   -> density_alpha()
+//   pressure.py:196-261   density rate, solve source, warm start     -> solve_init()
+//   pressure.py:264-352   pressure acceleration, relaxed Jacobi      -> accel(), jacobi()
+//   pressure.py:355-390   per-world start and stop test              -> solve()
+//   pressure.py:393-414, 461-480  lone-particle limit, apply pressure
+//   solve_driver.py:121-186  solve orchestration (Jacobi branch)
+//   reduce.py:185-227     per-world float64 sums and max             -> world_sum() (tree order below)
+//   integrate.py:150-185, 212-326  XSPH, advection, particle-wall projection, speed
+//   particle_walls.py:131-135  wall particles advance with their own velocity
+//   emitters.py:67-164    layer emitters, sinks and escape box, int64 mass ledger
+//   solver.py:218-268     step order
+//
+// Arithmetic contract. The FP32 instantiation evaluates every expression in a fixed order with explicit fused
+// multiply-adds (std::fma) and correctly rounded sqrt and division, compiled with -ffp-contract=off, so that the
+// CUDA kernels (same order, __fmaf_rn, -fmad=false) reproduce it bit for bit. Pair distances use the unfused
+// (dx*dx + dy*dy) + dz*dz, the reference's dot. Neighbour sums run in ascending particle id (the reference's order);
+// wall-colour sums run in ascending wall-particle id (the reference sums in hash-grid visit order, which Warp does
+// not pin). Per-world float64 sums use the tree order documented at world_sum(). The FP64 instantiation runs the
+// same algorithm in double for error reports.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr int FLAG_ACTIVE = 1;  // newton ParticleFlags.ACTIVE (geometry/flags.py:14)
+constexpr int PROJECT_PASSES = 4;  // integrate.py:50
+constexpr int BISECT = 30;         // particle_walls.py:44
+constexpr double C_MIN = 1.0e-4;   // particle_walls.py:43
+
+inline float fma_(float a, float b, float c) { return std::fmaf(a, b, c); }
+inline double fma_(double a, double b, double c) { return std::fma(a, b, c); }
+template <class R> inline R maxr(R a, R b) { return a > b ? a : b; }
+template <class R> inline R minr(R a, R b) { return a < b ? a : b; }
+template <class R> inline R clampr(R x, R lo, R hi) { return minr(maxr(x, lo), hi); }
+
+template <class R> struct V3 { R x, y, z; };
+template <class R> inline V3<R> sub(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+// the reference's dot (left to right, unfused); used for pair distances
+template <class R> inline R dot_plain(V3<R> a, V3<R> b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+// fused dot used everywhere else
+template <class R> inline R dotf(V3<R> a, V3<R> b) { return fma_(a.z, b.z, fma_(a.y, b.y, a.x * b.x)); }
+
+struct OrcParams {
+  int kind;
+  double particle_radius, h, sigma;
+  double n_full, tot_min, lattice_grad;
+  double wall_offset, wall_amplitude, taper0, taper1, reach;
+  double tol_den, tol_div, max_error_factor;
+  int min_it, max_it;
+  double omega, warm_den, warm_div, min_nb;
+  int divergence_solve, two_sided;
+  double xsph_c;
+  int capacity;
+  double v_sep, relief_speed, project_eps;
+  int has_bounds;
+  double bounds_lo[3], bounds_hi[3];
+};
+
+// Kernel constants in the working precision, derived from double host values exactly as the CUDA side does.
+template <class R> struct KC {
+  int kind;
+  R h, inv_h, h2, sigma, sig_h2, m6sig_h, m20sig_h2, r_min;
+  void init(int k, double hd, double sigma_d) {
+    kind = k;
+    h = R(hd);
+    inv_h = R(1.0 / hd);
+    h2 = h * h;
+    sigma = R(sigma_d);
+    sig_h2 = R(sigma_d / (hd * hd));
+    m6sig_h = R(-6.0 * sigma_d / hd);
+    m20sig_h2 = R(-20.0 * sigma_d / (hd * hd));
+    r_min = R(1.0e-9 * hd);
+  }
+};
+
+// W(r) and F(r) = (dW/dr)/r from r^2 (kernels.py:41-77); grad W_ij = (x_i - x_j) F.
+template <class R> inline void wf(const KC<R>& k, R r2, R& W, R& F) {
+  R r = std::sqrt(r2);
+  R q = r * k.inv_h;
+  if (q >= R(1)) { W = R(0); F = R(0); return; }
+  if (k.kind == 0) {
+    if (q <= R(0.5)) {
+      W = k.sigma * fma_(R(6) * (q * q), q - R(1), R(1));
+      F = k.sig_h2 * fma_(R(18), q, R(-12));
+    } else {
+      R s = R(1) - q;
+      R s2 = s * s;
+      W = k.sigma * (R(2) * (s2 * s));
+      F = (k.m6sig_h * s2) / r;
+    }
+  } else {
+    R s = R(1) - q;
+    R s2 = s * s;
+    W = k.sigma * ((s2 * s2) * fma_(R(4), q, R(1)));
+    F = k.m20sig_h2 * (s2 * s);
+  }
+  if (r <= k.r_min) F = R(0);
+}
+
+// Psi(d) and dPsi/dd of a flat solid half-space at signed distance d (kernels.py:80-138, curvature H = 0).
+// Cubic: p(y) = 1.4 - 8y^2 + 24y^4 - 19.2y^5 (y <= 1/2), (1-y)^4 (1.6 + 6.4y) (y > 1/2);
+// G0(y) = int_0^y p = 1.4y - 8/3 y^3 + 4.8y^5 - 3.2y^6 (y <= 1/2), 1/2 - (1-y)^5 (1.6 - 16/15 (1-y)) (y > 1/2).
+// Wendland C2: p(y) = 1.5 - 10.5y^2 + 52.5y^4 - 84y^5 + 52.5y^6 - 12y^7, G0 its integral.
+template <class R> inline void halfspace(const KC<R>& k, R d, R& psi, R& dpsi) {
+  if (d >= k.h) { psi = R(0); dpsi = R(0); return; }
+  R z = clampr(-d * k.inv_h, R(-1), R(1));
+  R y = std::fabs(z);
+  R g0, p;
+  if (k.kind == 0) {
+    if (y <= R(0.5)) {
+      R y2 = y * y;
+      g0 = y * fma_(y2, fma_(y2, fma_(R(-3.2), y, R(4.8)), R(-2.66666666666666667)), R(1.4));
+      p = fma_(y2, fma_(y2, fma_(R(-19.2), y, R(24)), R(-8)), R(1.4));
+    } else {
+      R u = R(1) - y;
+      R u2 = u * u;
+      R u4 = u2 * u2;
+      g0 = R(0.5) - (u4 * u) * fma_(R(-1.06666666666666667), u, R(1.6));
+      p = u4 * fma_(R(6.4), y, R(1.6));
+    }
+  } else {
+    R y2 = y * y;
+    g0 = y * fma_(y2, fma_(y2, fma_(y, fma_(y, fma_(R(-1.5), y, R(7.5)), R(-14)), R(10.5)), R(-3.5)), R(1.5));
+    p = fma_(y2, fma_(y2, fma_(y, fma_(y, fma_(R(-12), y, R(52.5)), R(-84)), R(52.5)), R(-10.5)), R(1.5));
+  }
+  psi = (z < R(0)) ? R(0.5) - g0 : R(0.5) + g0;
+  dpsi = (d > -k.h) ? -p * k.inv_h : R(0);
+}
+
+// The distance at which a flat wall covers c of the support (particle_walls.py:87-98).
+template <class R> inline R colour_distance(const KC<R>& k, R c) {
+  R lo = -k.h, hi = k.h;
+  for (int it = 0; it < BISECT; ++it) {
+    R mid = R(0.5) * (lo + hi);
+    R psi, dpsi;
+    halfspace(k, mid, psi, dpsi);
+    if (psi > c) lo = mid; else hi = mid;
+  }
+  return R(0.5) * (lo + hi);
+}
+
+inline int64_t to_fixed(float m) { return (int64_t)std::llround((double)m * 1099511627776.0); }
+
+template <class R> inline V3<R> quat_rotate(const float* qv, V3<R> v) {
+  // v' = v (2w^2 - 1) + 2w (u x v) + 2u (u . v), u = (qx, qy, qz)
+  R ux = R(qv[0]), uy = R(qv[1]), uz = R(qv[2]), w = R(qv[3]);
+  R a = R(2) * (w * w) - R(1);
+  R cx = uy * v.z - uz * v.y, cy = uz * v.x - ux * v.z, cz = ux * v.y - uy * v.x;
+  R b = R(2) * w;
+  R d = R(2) * ((ux * v.x + uy * v.y) + uz * v.z);
+  return {(v.x * a + cx * b) + ux * d, (v.y * a + cy * b) + uy * d, (v.z * a + cz * b) + uz * d};
+}
+
+// --------------------------------------------------------------------------------------------- reductions
+// Per-world float64 sum and max of a per-particle float array over contiguous world ranges, in this fixed order:
+// chunks of 256 consecutive particles aligned to each world start; inside a chunk lane l holds v[b + l] (0 past the
+// end), each group of 32 lanes folds with offsets 16, 8, 4, 2, 1 (lane l += lane l + off), then the 8 group sums
+// fold with offsets 4, 2, 1. A world's 256 lanes then take chunks l, l + 256, ... serially and fold the same way.
+inline double fold256(double* x) {
+  for (int g = 0; g < 8; ++g) {
+    double* y = x + 32 * g;
+    for (int off = 16; off >= 1; off >>= 1)
+      for (int l = 0; l < off; ++l) y[l] = y[l] + y[l + off];
+  }
+  double s[8];
+  for (int g = 0; g < 8; ++g) s[g] = x[32 * g];
+  for (int off = 4; off >= 1; off >>= 1)
+    for (int l = 0; l < off; ++l) s[l] = s[l] + s[l + off];
+  return s[0];
+}
+
+template <class R>
+void world_sum(int W, const int* ws, const R* v, double* out, float* out_max) {
+  const int CH = 256;
+  for (int w = 0; w < W; ++w) {
+    int lo = ws[w], hi = ws[w + 1];
+    std::vector<double> part;
+    float mx = -3.4e38f;
+    for (int b = lo; b < hi; b += CH) {
+      double x[256];
+      for (int l = 0; l < CH; ++l) {
+        int i = b + l;
+        x[l] = (i < hi) ? (double)v[i] : 0.0;
+        if (i < hi) mx = maxr(mx, (float)v[i]);
+      }
+      part.push_back(fold256(x));
+    }
+    double x[256];
+    for (int l = 0; l < CH; ++l) {
+      double a = 0.0;
+      for (size_t c = l; c < part.size(); c += CH) a = a + part[c];
+      x[l] = a;
+    }
+    out[w] = fold256(x);
+    if (out_max) out_max[w] = maxr(mx, 0.0f);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ solver
+struct Emitter {
+  int world;
+  float xform[7];
+  float vel[3];
+  float interval;
+  std::vector<float> offsets;  // n_layer x 3
+  std::vector<int> pool;
+  int enabled = 1;
+  float t_acc = 0.0f;
+  int cursor = 0;
+};
+struct Sink {
+  int world;
+  float xform[7];
+  float half[3];
+};
+
+template <class R> struct Solver {
+  OrcParams P;
+  KC<R> kc;
+  int n = 0, W = 0, K = 64;
+  std::vector<int> ws;
+  std::vector<float> mass, rho0, wall_vol, gravity;
+  std::vector<int> flags, world;
+  std::vector<int8_t> phase;
+  std::vector<V3<R>> q, v, vtmp, acc;
+  std::vector<R> kv, kd;
+  // per step
+  std::vector<int> group, cnt, nbr;
+  std::vector<int> slot_on;
+  std::vector<R> slot_psi, slot_phi;
+  std::vector<V3<R>> slot_g, slot_vb, slot_xb, slot_n;
+  std::vector<R> ratio, alpha, neff, active, reg, src, kappa, lower, err;
+  // per world
+  std::vector<int> overflow, escaped, projected, nonfinite, emit_overflow;
+  std::vector<int> iters_den, iters_div, converged, iters;
+  std::vector<float> den_err, div_err, den_err_max, max_speed, err_mean, den_tol;
+  std::vector<int64_t> mass_in, mass_out, mass0;
+  std::vector<double> n_active;
+  std::vector<Emitter> emitters;
+  std::vector<Sink> sinks;
+  int nthreads = 1;
+
+  bool is_fluid(int i) const { return (flags[i] & FLAG_ACTIVE) != 0 && phase[i] >= 1; }
+
+  void init() {
+    K = P.capacity;
+    kc.init(P.kind, P.h, P.sigma);
+    auto zr = [&](std::vector<R>& a) { a.assign(n, R(0)); };
+    auto z3 = [&](std::vector<V3<R>>& a) { a.assign(n, V3<R>{R(0), R(0), R(0)}); };
+    z3(q); z3(v); z3(vtmp); z3(acc);
+    zr(kv); zr(kd);
+    group.assign(n, -1); cnt.assign(n, 0); nbr.assign((size_t)n * K, -1);
+    slot_on.assign(n, 0); zr(slot_psi); zr(slot_phi); z3(slot_g); z3(slot_vb); z3(slot_xb); z3(slot_n);
+    zr(ratio); zr(alpha); zr(neff); zr(active); zr(reg); zr(src); zr(kappa); zr(lower); zr(err);
+    auto zi = [&](std::vector<int>& a) { a.assign(W, 0); };
+    zi(overflow); zi(escaped); zi(projected); zi(nonfinite); zi(emit_overflow);
+    zi(iters_den); zi(iters_div); zi(converged); zi(iters);
+    auto zf = [&](std::vector<float>& a) { a.assign(W, 0.0f); };
+    zf(den_err); zf(div_err); zf(den_err_max); zf(max_speed); zf(err_mean); zf(den_tol);
+    mass_in.assign(W, 0); mass_out.assign(W, 0); mass0.assign(W, 0);
+    n_active.assign(W, 0.0);
+  }
+
+  void init_mass() {
+    for (int w = 0; w < W; ++w) mass0[w] = 0;
+    for (int i = 0; i < n; ++i)
+      if (is_fluid(i)) mass0[world[i]] += to_fixed(mass[i]);
+  }
+
+  // ------------------------------------------------------------------- grid (this oracle's own, per world)
+  struct Grid {
+    double lo[3];
+    int dim[3];
+    double cw;
+    std::vector<int> start, ids;  // counting sort of members by cell
+    int cell_of(const V3<R>& x, int* c) const {
+      double p[3] = {(double)x.x, (double)x.y, (double)x.z};
+      for (int a = 0; a < 3; ++a) {
+        double f = std::floor((p[a] - lo[a]) / cw);
+        int ci = (f < 0.0) ? 0 : (f > dim[a] - 1 ? dim[a] - 1 : (int)f);
+        if (!(f == f)) ci = 0;
+        c[a] = ci;
+      }
+      return (c[2] * dim[1] + c[1]) * dim[0] + c[0];
+    }
+  };
+  std::vector<Grid> fluid_grid, wall_grid;
+
+  void build_grid(Grid& g, const std::vector<int>& members, const double* lo, const int* dim, double cw) {
+    for (int a = 0; a < 3; ++a) { g.lo[a] = lo[a]; g.dim[a] = dim[a]; }
+    g.cw = cw;
+    size_t nc = (size_t)dim[0] * dim[1] * dim[2];
+    g.start.assign(nc + 1, 0);
+    std::vector<int> key(members.size());
+    for (size_t m = 0; m < members.size(); ++m) {
+      int c[3];
+      key[m] = g.cell_of(q[members[m]], c);
+      g.start[key[m] + 1]++;
+    }
+    for (size_t c = 0; c < nc; ++c) g.start[c + 1] += g.start[c];
+    g.ids.assign(members.size(), 0);
+    std::vector<int> cur(g.start.begin(), g.start.end() - 1);
+    for (size_t m = 0; m < members.size(); ++m) g.ids[cur[key[m]]++] = members[m];
+  }
+
+  void build_groups_and_grids() {
+    for (int i = 0; i < n; ++i) {
+      int g = -1;
+      if ((flags[i] & FLAG_ACTIVE) != 0 && phase[i] >= 1) g = world[i];
+      else if (wall_vol[i] > 0.0f && (flags[i] & FLAG_ACTIVE) != 0 && world[i] >= 0) g = -2 - world[i];
+      group[i] = g;
+    }
+    fluid_grid.assign(W, Grid());
+    wall_grid.assign(W, Grid());
+    const double cw = 1.01 * P.h;
+    for (int w = 0; w < W; ++w) {
+      std::vector<int> fl, wl;
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int i = ws[w]; i < ws[w + 1]; ++i) {
+        if (group[i] == w) fl.push_back(i);
+        else if (group[i] == -2 - w) wl.push_back(i);
+        else continue;
+        double p[3] = {(double)q[i].x, (double)q[i].y, (double)q[i].z};
+        for (int a = 0; a < 3; ++a)
+          if (std::isfinite(p[a])) { lo[a] = std::min(lo[a], p[a]); hi[a] = std::max(hi[a], p[a]); }
+      }
+      int dim[3];
+      double cww = cw;
+      for (;;) {  // cells never narrower than h; coarser where a world's box is huge (escaped particles)
+        double cells = 1.0;
+        for (int a = 0; a < 3; ++a) {
+          if (!(lo[a] <= hi[a])) { lo[a] = 0.0; hi[a] = 0.0; }
+          dim[a] = (int)std::floor((hi[a] - lo[a]) / cww) + 1;
+          cells *= dim[a];
+        }
+        if (cells <= 6.4e7) break;
+        cww *= 2.0;
+      }
+      build_grid(fluid_grid[w], fl, lo, dim, cww);
+      build_grid(wall_grid[w], wl, lo, dim, cww);
+    }
+  }
+
+  template <class Fn> void for_each_near(const Grid& g, const V3<R>& x, Fn fn) const {
+    int c[3];
+    g.cell_of(x, c);
+    for (int dz = -1; dz <= 1; ++dz) {
+      int z = c[2] + dz;
+      if (z < 0 || z >= g.dim[2]) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        int y = c[1] + dy;
+        if (y < 0 || y >= g.dim[1]) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          int xx = c[0] + dx;
+          if (xx < 0 || xx >= g.dim[0]) continue;
+          int cell = (z * g.dim[1] + y) * g.dim[0] + xx;
+          for (int m = g.start[cell]; m < g.start[cell + 1]; ++m) fn(g.ids[m]);
+        }
+      }
+    }
+  }
+
+  // neighbors.py:160-195: ascending ids j != i of the same group with |x_j - x_i|^2 < h^2, lowest K kept
+  void build_lists() {
+    std::vector<int> ovf(W, 0);
+#pragma omp parallel num_threads(nthreads)
+    {
+      std::vector<int> cand;
+      std::vector<int> ovf_local(W, 0);
+#pragma omp for schedule(dynamic, 256)
+      for (int i = 0; i < n; ++i) {
+        int g = group[i];
+        if (g < 0) { cnt[i] = 0; continue; }
+        cand.clear();
+        const V3<R> xi = q[i];
+        for_each_near(fluid_grid[g], xi, [&](int j) {
+          if (j == i) return;
+          V3<R> d = sub(q[j], xi);
+          if (dot_plain(d, d) < kc.h2) cand.push_back(j);
+        });
+        std::sort(cand.begin(), cand.end());
+        int total = (int)cand.size();
+        int m = std::min(total, K);
+        for (int k = 0; k < m; ++k) nbr[(size_t)i * K + k] = cand[k];
+        cnt[i] = m;
+        if (total > K) ovf_local[g]++;
+      }
+#pragma omp critical
+      for (int w = 0; w < W; ++w) ovf[w] += ovf_local[w];
+    }
+    for (int w = 0; w < W; ++w) overflow[w] += ovf[w];
+  }
+
+  // particle_walls.py:65-119 + boundary.py:241-287: the particle-wall slot of fluid particle i
+  void wall_slots() {
+    const R offset = R(P.wall_offset), amp = R(P.wall_amplitude), t0 = R(P.taper0), t1 = R(P.taper1);
+    const R reach = R(P.reach);
+#pragma omp parallel num_threads(nthreads)
+    {
+      struct C { int j; R wj, F; V3<R> d; };
+      std::vector<C> cand;
+#pragma omp for schedule(dynamic, 256)
+      for (int i = 0; i < n; ++i) {
+        slot_on[i] = 0;
+        slot_psi[i] = R(0);
+        slot_g[i] = {R(0), R(0), R(0)};
+        if (!is_fluid(i)) continue;
+        int w = world[i];
+        const V3<R> x = q[i];
+        cand.clear();
+        for_each_near(wall_grid[w], x, [&](int j) {
+          V3<R> d = sub(x, q[j]);
+          R Wv, F;
+          wf(kc, dot_plain(d, d), Wv, F);
+          R wj = R(wall_vol[j]) * Wv;
+          if (wj > R(0)) cand.push_back({j, wj, F, d});
+        });
+        if (cand.empty()) continue;
+        std::sort(cand.begin(), cand.end(), [](const C& a, const C& b) { return a.j < b.j; });
+        R c = R(0);
+        V3<R> gc{R(0), R(0), R(0)}, mv{R(0), R(0), R(0)};
+        for (const C& e : cand) {
+          R vol = R(wall_vol[e.j]);
+          c = c + e.wj;
+          gc.x = fma_(vol, e.d.x * e.F, gc.x);
+          gc.y = fma_(vol, e.d.y * e.F, gc.y);
+          gc.z = fma_(vol, e.d.z * e.F, gc.z);
+          mv.x = fma_(e.wj, v[e.j].x, mv.x);
+          mv.y = fma_(e.wj, v[e.j].y, mv.y);
+          mv.z = fma_(e.wj, v[e.j].z, mv.z);
+        }
+        mv = {mv.x / c, mv.y / c, mv.z / c};
+        R lg = std::sqrt(dot_plain(gc, gc));
+        if (c < R(C_MIN) || lg <= R(0)) continue;
+        R phi = colour_distance(kc, minr(c, R(1)));
+        if (!(phi < reach && phi + offset < kc.h)) continue;
+        V3<R> nrm{-gc.x / lg, -gc.y / lg, -gc.z / lg};
+        R psi, dpsi;
+        halfspace(kc, phi + offset, psi, dpsi);
+        psi = psi * amp;
+        dpsi = dpsi * amp;
+        if (phi > t0) {  // C1 taper between the first and second lattice layer
+          R L = t1 - t0;
+          R t = minr((phi - t0) / L, R(1));
+          R sm = R(1) - (t * t) * (R(3) - R(2) * t);
+          R dsm = ((R(6) * t) * (t - R(1))) / L;
+          R p0 = psi;
+          psi = p0 * sm;
+          dpsi = fma_(p0, dsm, dpsi * sm);
+        }
+        slot_on[i] = 1;
+        slot_psi[i] = psi;
+        slot_phi[i] = phi;
+        slot_g[i] = {dpsi * nrm.x, dpsi * nrm.y, dpsi * nrm.z};
+        slot_n[i] = nrm;
+        slot_xb[i] = {fma_(-phi, nrm.x, x.x), fma_(-phi, nrm.y, x.y), fma_(-phi, nrm.z, x.z)};
+        slot_vb[i] = mv;
+      }
+    }
+  }
+
+  // pressure.py:144-193
+  void density_alpha() {
+    const R n_full = R(P.n_full), tot_min = R(P.tot_min);
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) { ratio[i] = alpha[i] = neff[i] = active[i] = reg[i] = R(0); continue; }
+      const V3<R> xi = q[i];
+      R mi = R(mass[i]);
+      R inv_r0 = R(1) / R(rho0[i]);
+      R bi = mi * inv_r0;
+      R rho = mi * kc.sigma;
+      V3<R> G{R(0), R(0), R(0)};
+      R sq = R(0);
+      const int* row = &nbr[(size_t)i * K];
+      for (int k = 0; k < cnt[i]; ++k) {
+        int j = row[k];
+        V3<R> rv = sub(xi, q[j]);
+        R r2 = dot_plain(rv, rv);
+        R Wv, F;
+        wf(kc, r2, Wv, F);
+        R mj = R(mass[j]);
+        rho = fma_(mj, Wv, rho);
+        R a = mj * inv_r0;
+        R aF = a * F;
+        G.x = fma_(aF, rv.x, G.x);
+        G.y = fma_(aF, rv.y, G.y);
+        G.z = fma_(aF, rv.z, G.z);
+        sq = fma_(bi * a, (F * F) * r2, sq);
+      }
+      R psi = R(0);
+      if (slot_on[i]) {
+        psi = slot_psi[i];
+        G.x = G.x + slot_g[i].x;
+        G.y = G.y + slot_g[i].y;
+        G.z = G.z + slot_g[i].z;
+      }
+      R lam = R(0);
+      R tot = (dotf(G, G) + sq) + lam;
+      lam = lam + maxr(tot_min - tot, R(0));
+      tot = maxr(tot, tot_min);
+      reg[i] = lam;
+      ratio[i] = fma_(rho, inv_r0, psi);
+      alpha[i] = (tot > R(1.0e-12)) ? R(1) / tot : R(0);
+      neff[i] = fma_(psi, n_full, R(cnt[i]));
+      active[i] = R(1);
+    }
+  }
+
+  // pressure.py:196-261 (the lone-particle and two-sided branches included)
+  void solve_init(bool div, R dt, R relief) {
+    const R warm = R(div ? P.warm_div : P.warm_den), warm_den = R(P.warm_den), min_nb = R(P.min_nb);
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) { src[i] = kappa[i] = lower[i] = R(0); continue; }
+      const V3<R> xi = q[i], vi = v[i];
+      R inv_r0 = R(1) / R(rho0[i]);
+      R rate = R(0);
+      const int* row = &nbr[(size_t)i * K];
+      for (int k = 0; k < cnt[i]; ++k) {
+        int j = row[k];
+        V3<R> rv = sub(xi, q[j]);
+        R Wv, F;
+        wf(kc, dot_plain(rv, rv), Wv, F);
+        R aF = (R(mass[j]) * inv_r0) * F;
+        rate = fma_(aF, dotf(sub(vi, v[j]), rv), rate);
+      }
+      if (slot_on[i]) rate = rate + dotf(sub(vi, slot_vb[i]), slot_g[i]);
+      if (div) {
+        R kdv = R(0);
+        if (P.two_sided) kdv = maxr((warm_den * minr(kd[i], R(2.5e-4))) / (dt * dt), R(0));
+        R lb = -kdv;
+        R r = rate;
+        if (kdv <= R(0)) { r = maxr(rate, R(0)); lb = R(0); }
+        if (neff[i] < min_nb) { r = R(0); lb = R(0); }
+        src[i] = r;
+        lower[i] = lb;
+        kappa[i] = maxr((warm * minr(kv[i], R(0.5))) / dt, lb);
+      } else {
+        R rs = fma_(dt, rate, ratio[i]);
+        if (ratio[i] - R(1) > relief) rs = fma_(dt, rate, R(1) + relief);
+        src[i] = rs;
+        lower[i] = R(0);
+        kappa[i] = (warm * minr(kd[i], R(2.5e-4))) / (dt * dt);
+      }
+    }
+  }
+
+  // pressure.py:264-277: a_i = -sum_j m_j (k_i/rho0_i + k_j/rho0_j) grad W_ij - k_i sum_b dPsi_b
+  V3<R> pressure_accel(int i, const std::vector<R>& kr) const {
+    const V3<R> xi = q[i];
+    R ki = kr[i];
+    V3<R> a{R(0), R(0), R(0)};
+    const int* row = &nbr[(size_t)i * K];
+    for (int k = 0; k < cnt[i]; ++k) {
+      int j = row[k];
+      V3<R> rv = sub(xi, q[j]);
+      R Wv, F;
+      wf(kc, dot_plain(rv, rv), Wv, F);
+      R cF = (R(mass[j]) * (ki + kr[j])) * F;
+      a.x = fma_(-cF, rv.x, a.x);
+      a.y = fma_(-cF, rv.y, a.y);
+      a.z = fma_(-cF, rv.z, a.z);
+    }
+    if (slot_on[i]) {
+      R k = kappa[i];
+      a.x = fma_(-k, slot_g[i].x, a.x);
+      a.y = fma_(-k, slot_g[i].y, a.y);
+      a.z = fma_(-k, slot_g[i].z, a.z);
+    }
+    return a;
+  }
+
+  std::vector<R> kr;  // kappa / rho0, refreshed whenever kappa changes
+
+  void refresh_kr() {
+    kr.resize(n);
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) kr[i] = kappa[i] / R(rho0[i]);
+  }
+
+  // pressure.py:280-291
+  void accel_pass() {
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) { acc[i] = {R(0), R(0), R(0)}; continue; }
+      if (converged[world[i]]) continue;
+      acc[i] = pressure_accel(i, kr);
+    }
+  }
+
+  // pressure.py:294-352
+  void jacobi_pass(bool div, R dt) {
+    const R omega = R(P.omega), min_nb = R(P.min_nb);
+    const R scale = div ? R(1) / dt : R(1) / (dt * dt);
+    const R dtn = div ? dt : dt * dt;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) { err[i] = R(0); continue; }
+      if (converged[world[i]]) continue;
+      const V3<R> xi = q[i], ai = acc[i];
+      R inv_r0 = R(1) / R(rho0[i]);
+      R ar = R(0);
+      const int* row = &nbr[(size_t)i * K];
+      for (int k = 0; k < cnt[i]; ++k) {
+        int j = row[k];
+        V3<R> rv = sub(xi, q[j]);
+        R Wv, F;
+        wf(kc, dot_plain(rv, rv), Wv, F);
+        R aF = (R(mass[j]) * inv_r0) * F;
+        ar = fma_(aF, dotf(sub(ai, acc[j]), rv), ar);
+      }
+      if (slot_on[i]) ar = ar + dotf(ai, slot_g[i]);
+      ar = fma_(-reg[i], kappa[i], ar);
+      ar = ar * dtn;
+      R s = div ? -src[i] : R(1) - src[i];
+      R r = s - ar;
+      R lb = lower[i];
+      R knew = maxr(kappa[i] - ((omega * r) * alpha[i]) * scale, lb);
+      kappa[i] = knew;
+      kr[i] = knew / R(rho0[i]);
+      R e = maxr(-r, R(0));
+      if (knew > lb) e = std::fabs(r);
+      if (div) {
+        if (neff[i] < min_nb) e = R(0);
+        e = e * dt;
+      }
+      err[i] = e;
+    }
+  }
+
+  // pressure.py:355-390 + solve_driver.py:121-186 (Jacobi branch)
+  void solve(bool div, R dt, double dt_d) {
+    const double tol_d = div ? P.tol_div : P.tol_den;
+    const float tol = (float)tol_d, tol_max = (float)(tol_d * P.max_error_factor);
+    R relief = R(1.0e30);
+    if (!div && P.relief_speed > 0.0) relief = R(P.relief_speed * dt_d * P.lattice_grad);
+    solve_init(div, dt, relief);
+    refresh_kr();
+    int n_unconv = 0;
+    for (int w = 0; w < W; ++w) {
+      iters[w] = 0;
+      err_mean[w] = 0.0f;
+      if (n_active[w] > 0.0) { converged[w] = 0; n_unconv++; } else converged[w] = 1;
+    }
+    std::vector<double> esum(W);
+    std::vector<float> emax(W);
+    int guard = 0;
+    while (n_unconv > 0 && guard++ < 100000) {
+      accel_pass();
+      jacobi_pass(div, dt);
+      world_sum<R>(W, ws.data(), err.data(), esum.data(), emax.data());
+      n_unconv = 0;
+      for (int w = 0; w < W; ++w) {
+        if (converged[w]) continue;
+        int it = iters[w] + 1;
+        iters[w] = it;
+        float mean = (float)(esum[w] / std::max(n_active[w], 1.0));
+        err_mean[w] = mean;
+        const float ts = 1.0f;
+        if ((it >= P.min_it && mean <= tol * ts && emax[w] <= tol_max * ts) || it >= P.max_it) converged[w] = 1;
+        else n_unconv++;
+      }
+    }
+    contact_limit(dt);
+    apply_pressure(div, dt);
+    for (int w = 0; w < W; ++w) {
+      if (div) { iters_div[w] = iters[w]; div_err[w] = err_mean[w]; }
+      else { iters_den[w] = iters[w]; den_err[w] = err_mean[w]; }
+    }
+    if (!div) {
+      for (int w = 0; w < W; ++w) { den_err_max[w] = 0.0f; den_tol[w] = (float)tol_d; }
+      for (int i = 0; i < n; ++i)
+        if (is_fluid(i)) den_err_max[world[i]] = maxr(den_err_max[world[i]], (float)err[i]);
+    }
+  }
+
+  // pressure.py:393-414 (one particle-wall slot)
+  void contact_limit(R dt) {
+    const R v_sep = R(P.v_sep);
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i) || cnt[i] > 0 || kappa[i] <= R(0)) continue;
+      if (!slot_on[i]) continue;
+      V3<R> G = slot_g[i];
+      R ps = slot_psi[i];
+      V3<R> vb{ps * slot_vb[i].x, ps * slot_vb[i].y, ps * slot_vb[i].z};
+      R g = std::sqrt(dot_plain(G, G));
+      if (g <= R(0)) continue;
+      if (ps > R(0)) vb = {vb.x / ps, vb.y / ps, vb.z / ps};
+      V3<R> nn{-G.x / g, -G.y / g, -G.z / g};
+      R u = dotf(sub(v[i], vb), nn);
+      kappa[i] = minr(kappa[i], maxr(v_sep - u, R(0)) / (dt * g));
+    }
+  }
+
+  // pressure.py:461-480 (slot impulses are coupling output and not tracked here)
+  void apply_pressure(bool div, R dt) {
+    refresh_kr();
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) continue;
+      V3<R> a = pressure_accel(i, kr);
+      acc[i] = a;
+    }
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) continue;
+      v[i] = {fma_(dt, acc[i].x, v[i].x), fma_(dt, acc[i].y, v[i].y), fma_(dt, acc[i].z, v[i].z)};
+      if (div) kv[i] = kappa[i] * dt;
+      else kd[i] = (kappa[i] * dt) * dt;
+    }
+  }
+
+  // integrate.py:150-178
+  void nonpressure(R dt) {
+    const R c = R(P.xsph_c);
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      V3<R> vi = v[i];
+      if (!is_fluid(i)) { vtmp[i] = vi; continue; }
+      int w = world[i];
+      V3<R> g{R(gravity[3 * w]), R(gravity[3 * w + 1]), R(gravity[3 * w + 2])};
+      V3<R> vn{fma_(dt, g.x, vi.x), fma_(dt, g.y, vi.y), fma_(dt, g.z, vi.z)};
+      if (c > R(0)) {
+        const V3<R> xi = q[i];
+        V3<R> corr{R(0), R(0), R(0)};
+        R rho_i = ratio[i] * R(rho0[i]);
+        const int* row = &nbr[(size_t)i * K];
+        for (int k = 0; k < cnt[i]; ++k) {
+          int j = row[k];
+          R rho_bar = R(0.5) * (rho_i + ratio[j] * R(rho0[j]));
+          if (rho_bar > R(0)) {
+            V3<R> rv = sub(xi, q[j]);
+            R Wv, F;
+            wf(kc, dot_plain(rv, rv), Wv, F);
+            R cw = (R(mass[j]) / rho_bar) * Wv;
+            corr.x = fma_(cw, v[j].x - vi.x, corr.x);
+            corr.y = fma_(cw, v[j].y - vi.y, corr.y);
+            corr.z = fma_(cw, v[j].z - vi.z, corr.z);
+          }
+        }
+        vn = {fma_(c, corr.x, vn.x), fma_(c, corr.y, vn.y), fma_(c, corr.z, vn.z)};
+      }
+      vtmp[i] = vn;
+    }
+    v.swap(vtmp);
+  }
+
+  // integrate.py:181-185 + particle_walls.py:131-135 + integrate.py:212-309 (particle-wall slot only)
+  void advect_project(R dt) {
+    const R eps = R(P.project_eps);
+    std::vector<int> moved_w(W, 0);
+    for (int i = 0; i < n; ++i) {
+      if (is_fluid(i)) {
+        q[i] = {fma_(dt, v[i].x, q[i].x), fma_(dt, v[i].y, q[i].y), fma_(dt, v[i].z, q[i].z)};
+      } else if (wall_vol[i] > 0.0f) {
+        q[i] = {fma_(dt, v[i].x, q[i].x), fma_(dt, v[i].y, q[i].y), fma_(dt, v[i].z, q[i].z)};
+      }
+    }
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i) || !slot_on[i]) continue;
+      V3<R> x = q[i], vv = v[i];
+      const V3<R> nn = slot_n[i], vb = slot_vb[i], xb = slot_xb[i];
+      V3<R> p{fma_(dt, vb.x, xb.x), fma_(dt, vb.y, xb.y), fma_(dt, vb.z, xb.z)};
+      int moved = 0;
+      for (int pass = 0; pass < PROJECT_PASSES; ++pass) {
+        R d = dotf(sub(x, p), nn);
+        if (!(d < eps)) break;
+        R push = eps - d;
+        x = {fma_(push, nn.x, x.x), fma_(push, nn.y, x.y), fma_(push, nn.z, x.z)};
+        R vn = dotf(sub(vv, vb), nn);
+        if (vn < R(0)) vv = {fma_(-vn, nn.x, vv.x), fma_(-vn, nn.y, vv.y), fma_(-vn, nn.z, vv.z)};
+        moved = 1;
+      }
+      if (moved) { q[i] = x; v[i] = vv; moved_w[world[i]]++; }
+    }
+    for (int w = 0; w < W; ++w) projected[w] += moved_w[w];
+  }
+
+  // emitters.py:134-164
+  void retire() {
+    bool any = P.has_bounds || !sinks.empty();
+    if (!any) return;
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) continue;
+      int w = world[i];
+      V3<R> x = q[i];
+      int gone = 0;
+      for (const Sink& s : sinks) {
+        if (s.world != w) continue;
+        V3<R> d{x.x - R(s.xform[0]), x.y - R(s.xform[1]), x.z - R(s.xform[2])};
+        float inv[4] = {-s.xform[3], -s.xform[4], -s.xform[5], s.xform[6]};
+        V3<R> xl = quat_rotate(inv, d);
+        if (std::fabs(xl.x) <= R(s.half[0]) && std::fabs(xl.y) <= R(s.half[1]) && std::fabs(xl.z) <= R(s.half[2])) gone = 1;
+      }
+      if (P.has_bounds && gone == 0) {
+        bool out = x.x < R(P.bounds_lo[0]) || x.y < R(P.bounds_lo[1]) || x.z < R(P.bounds_lo[2]) ||
+                   x.x > R(P.bounds_hi[0]) || x.y > R(P.bounds_hi[1]) || x.z > R(P.bounds_hi[2]);
+        if (out || !std::isfinite((x.x + x.y) + x.z)) { gone = 2; escaped[w]++; }
+      }
+      if (gone) {
+        flags[i] &= ~FLAG_ACTIVE;
+        phase[i] = -2;
+        v[i] = {R(0), R(0), R(0)};
+        mass_out[w] += to_fixed(mass[i]);
+      }
+    }
+  }
+
+  // emitters.py:67-126
+  void emit(R dt) {
+    for (Emitter& e : emitters) {
+      int now = 0;
+      if (e.enabled) {
+        float t = e.t_acc + (float)dt;
+        if (t >= e.interval) { t -= e.interval; now = 1; }
+        e.t_acc = t;
+      }
+      if (!now) continue;
+      int nl = (int)(e.offsets.size() / 3);
+      for (int c = 0; c < nl; ++c) {
+        int slot = e.cursor + c;
+        if (slot >= (int)e.pool.size()) { emit_overflow[e.world]++; continue; }
+        int i = e.pool[slot];
+        V3<R> p{R(e.offsets[3 * c]), R(e.offsets[3 * c + 1]), R(e.offsets[3 * c + 2])};
+        V3<R> r = quat_rotate(e.xform + 3, p);
+        q[i] = {r.x + R(e.xform[0]), r.y + R(e.xform[1]), r.z + R(e.xform[2])};
+        v[i] = {R(e.vel[0]), R(e.vel[1]), R(e.vel[2])};
+        flags[i] |= FLAG_ACTIVE;
+        phase[i] = 1;
+        mass_in[e.world] += to_fixed(mass[i]);
+      }
+      e.cursor = std::min(e.cursor + nl, (int)e.pool.size());
+    }
+  }
+
+  // integrate.py:312-326
+  void speed() {
+    for (int w = 0; w < W; ++w) max_speed[w] = 0.0f;
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) continue;
+      int w = world[i];
+      R s = std::sqrt(dotf(v[i], v[i]));
+      V3<R> x = q[i];
+      if (std::isfinite(s) && std::isfinite((x.x + x.y) + x.z)) max_speed[w] = maxr(max_speed[w], (float)s);
+      else { nonfinite[w]++; max_speed[w] = maxr(max_speed[w], 1.0e30f); }
+    }
+  }
+
+  void prepare_density() {
+    build_groups_and_grids();
+    build_lists();
+    wall_slots();
+    density_alpha();
+    for (int w = 0; w < W; ++w) {
+      double a = 0.0;
+      for (int i = ws[w]; i < ws[w + 1]; ++i) a += (double)active[i];
+      n_active[w] = a;
+    }
+  }
+
+  // solver.py:218-268
+  void step(double dt_d) {
+    R dt = R(dt_d);
+    prepare_density();
+    if (P.divergence_solve) solve(true, dt, dt_d);
+    nonpressure(dt);
+    solve(false, dt, dt_d);
+    advect_project(dt);
+    retire();
+    emit(dt);
+    speed();
+  }
+};
+
+struct Handle {
+  int f64;
+  std::unique_ptr<Solver<float>> s32;
+  std::unique_ptr<Solver<double>> s64;
+};
+
+template <class R> void setup(Solver<R>& s, const OrcParams* p, int n, int W, const int* ws, const float* mass,
+                               const float* rho0, const int* flags, const int8_t* phase, const int* world,
+                               const float* wall_vol, const float* gravity) {
+  s.P = *p;
+  s.n = n;
+  s.W = W;
+  s.ws.assign(ws, ws + W + 1);
+  s.mass.assign(mass, mass + n);
+  s.rho0.assign(rho0, rho0 + n);
+  s.flags.assign(flags, flags + n);
+  s.phase.assign(phase, phase + n);
+  s.world.assign(world, world + n);
+  s.wall_vol.assign(wall_vol, wall_vol + n);
+  s.gravity.assign(gravity, gravity + 3 * W);
+  s.init();
+  s.init_mass();
+#ifdef _OPENMP
+  s.nthreads = omp_get_max_threads();
+#endif
+}
+
+template <class R, class T> void copy_out(const std::vector<R>& a, T* out) {
+  for (size_t i = 0; i < a.size(); ++i) out[i] = (T)a[i];
+}
+template <class R, class T> void copy_out3(const std::vector<V3<R>>& a, T* out) {
+  for (size_t i = 0; i < a.size(); ++i) { out[3 * i] = (T)a[i].x; out[3 * i + 1] = (T)a[i].y; out[3 * i + 2] = (T)a[i].z; }
+}
+
+}  // namespace
+
+extern "C" {
+
+typedef OrcParams orc_params;
+
+void* orc_create(const orc_params* p, int n, int W, const int* ws, const float* mass, const float* rho0,
+                 const int* flags, const int8_t* phase, const int* world, const float* wall_vol, const float* gravity,
+                 int f64) {
+  Handle* h = new Handle();
+  h->f64 = f64;
+  if (f64) { h->s64.reset(new Solver<double>()); setup(*h->s64, p, n, W, ws, mass, rho0, flags, phase, world, wall_vol, gravity); }
+  else { h->s32.reset(new Solver<float>()); setup(*h->s32, p, n, W, ws, mass, rho0, flags, phase, world, wall_vol, gravity); }
+  return h;
+}
+
+void orc_destroy(void* hp) { delete (Handle*)hp; }
+
+void orc_set_threads(void* hp, int t) {
+  Handle* h = (Handle*)hp;
+  if (h->f64) h->s64->nthreads = t; else h->s32->nthreads = t;
+}
+
+#define DISPATCH(...) do { Handle* h = (Handle*)hp; if (h->f64) { auto& s = *h->s64; __VA_ARGS__; } else { auto& s = *h->s32; __VA_ARGS__; } } while (0)
+
+void orc_set_state(void* hp, const float* q, const float* qd) {
+  DISPATCH({
+    using R = typename std::remove_reference<decltype(s.kv)>::type::value_type;
+    for (int i = 0; i < s.n; ++i) {
+      s.q[i] = {R(q[3 * i]), R(q[3 * i + 1]), R(q[3 * i + 2])};
+      s.v[i] = {R(qd[3 * i]), R(qd[3 * i + 1]), R(qd[3 * i + 2])};
+    }
+  });
+}
+void orc_get_state(void* hp, float* q, float* qd) { DISPATCH({ copy_out3(s.q, q); copy_out3(s.v, qd); }); }
+void orc_get_state_f64(void* hp, double* q, double* qd) { DISPATCH({ copy_out3(s.q, q); copy_out3(s.v, qd); }); }
+void orc_set_warm(void* hp, const float* kv, const float* kd) {
+  DISPATCH({
+    for (int i = 0; i < s.n; ++i) { s.kv[i] = kv[i]; s.kd[i] = kd[i]; }
+  });
+}
+void orc_get_warm(void* hp, float* kv, float* kd) { DISPATCH({ copy_out(s.kv, kv); copy_out(s.kd, kd); }); }
+void orc_get_flags_phase(void* hp, int* flags, int8_t* phase) {
+  DISPATCH({
+    std::memcpy(flags, s.flags.data(), sizeof(int) * s.n);
+    std::memcpy(phase, s.phase.data(), s.n);
+  });
+}
+int orc_step(void* hp, double dt) { DISPATCH(s.step(dt)); return 0; }
+void orc_prepare_density(void* hp) { DISPATCH(s.prepare_density()); }
+
+// name: ratio alpha neff active reg src kappa err slot_psi slot_phi
+int orc_get_field(void* hp, const char* name, float* out) {
+  int ok = 1;
+  DISPATCH({
+    auto pick = [&](const char* nm, const auto& a) { if (std::strcmp(name, nm) == 0) { copy_out(a, out); ok = 0; } };
+    pick("ratio", s.ratio); pick("alpha", s.alpha); pick("neff", s.neff); pick("active", s.active);
+    pick("reg", s.reg); pick("src", s.src); pick("kappa", s.kappa); pick("err", s.err);
+    pick("slot_psi", s.slot_psi); pick("slot_phi", s.slot_phi);
+    if (std::strcmp(name, "slot_g") == 0) { copy_out3(s.slot_g, out); ok = 0; }
+    if (std::strcmp(name, "slot_vb") == 0) { copy_out3(s.slot_vb, out); ok = 0; }
+    if (std::strcmp(name, "slot_n") == 0) { copy_out3(s.slot_n, out); ok = 0; }
+    if (std::strcmp(name, "acc") == 0) { copy_out3(s.acc, out); ok = 0; }
+  });
+  return ok;
+}
+
+void orc_get_slot_on(void* hp, int* out) { DISPATCH(std::memcpy(out, s.slot_on.data(), sizeof(int) * s.n)); }
+
+void orc_get_lists(void* hp, int* rows, int* count) {
+  DISPATCH({
+    std::memcpy(count, s.cnt.data(), sizeof(int) * s.n);
+    for (int i = 0; i < s.n; ++i)
+      for (int k = 0; k < s.K; ++k) rows[(size_t)i * s.K + k] = (k < s.cnt[i]) ? s.nbr[(size_t)i * s.K + k] : -1;
+  });
+}
+
+// int arrays: iters_den iters_div overflow escaped projected nonfinite emit_overflow
+// float arrays: den_err div_err den_err_max max_speed den_tol ; int64: mass_in mass_out mass0
+void orc_get_report(void* hp, int* ints /*7*W*/, float* floats /*5*W*/, int64_t* ledger /*3*W*/) {
+  DISPATCH({
+    int W = s.W;
+    const std::vector<int>* ia[7] = {&s.iters_den, &s.iters_div, &s.overflow, &s.escaped, &s.projected, &s.nonfinite, &s.emit_overflow};
+    for (int k = 0; k < 7; ++k) std::memcpy(ints + k * W, ia[k]->data(), sizeof(int) * W);
+    const std::vector<float>* fa[5] = {&s.den_err, &s.div_err, &s.den_err_max, &s.max_speed, &s.den_tol};
+    for (int k = 0; k < 5; ++k) std::memcpy(floats + k * W, fa[k]->data(), sizeof(float) * W);
+    std::memcpy(ledger, s.mass_in.data(), 8 * W);
+    std::memcpy(ledger + W, s.mass_out.data(), 8 * W);
+    std::memcpy(ledger + 2 * W, s.mass0.data(), 8 * W);
+  });
+}
+
+void orc_active_mass(void* hp, int64_t* out) {
+  DISPATCH({
+    for (int w = 0; w < s.W; ++w) out[w] = 0;
+    for (int i = 0; i < s.n; ++i) if (s.is_fluid(i)) out[s.world[i]] += to_fixed(s.mass[i]);
+  });
+}
+
+void orc_add_emitter(void* hp, int world, const float* xform, const float* offsets, int n_off, const float* vel,
+                     float interval, const int* pool, int pool_size) {
+  Emitter e;
+  e.world = world;
+  std::memcpy(e.xform, xform, sizeof(float) * 7);
+  std::memcpy(e.vel, vel, sizeof(float) * 3);
+  e.interval = interval;
+  e.offsets.assign(offsets, offsets + 3 * n_off);
+  e.pool.assign(pool, pool + pool_size);
+  DISPATCH(s.emitters.push_back(e));
+}
+
+void orc_add_sink(void* hp, int world, const float* xform, const float* half) {
+  Sink k;
+  k.world = world;
+  std::memcpy(k.xform, xform, sizeof(float) * 7);
+  std::memcpy(k.half, half, sizeof(float) * 3);
+  DISPATCH(s.sinks.push_back(k));
+}
+
+// ---- scalar primitives and the reducer, for known-answer tests
+void orc_kernel_wf(int kind, double h, double sigma, int m, const float* r2, float* Wout, float* Fout) {
+  KC<float> k;
+  k.init(kind, h, sigma);
+  for (int i = 0; i < m; ++i) wf(k, r2[i], Wout[i], Fout[i]);
+}
+void orc_kernel_wf64(int kind, double h, double sigma, int m, const double* r2, double* Wout, double* Fout) {
+  KC<double> k;
+  k.init(kind, h, sigma);
+  for (int i = 0; i < m; ++i) wf(k, r2[i], Wout[i], Fout[i]);
+}
+void orc_halfspace(int kind, double h, int m, const float* d, float* psi, float* dpsi) {
+  KC<float> k;
+  k.init(kind, h, 1.0);
+  for (int i = 0; i < m; ++i) halfspace(k, d[i], psi[i], dpsi[i]);
+}
+void orc_halfspace64(int kind, double h, int m, const double* d, double* psi, double* dpsi) {
+  KC<double> k;
+  k.init(kind, h, 1.0);
+  for (int i = 0; i < m; ++i) halfspace(k, d[i], psi[i], dpsi[i]);
+}
+void orc_colour_distance(int kind, double h, int m, const float* c, float* out) {
+  KC<float> k;
+  k.init(kind, h, 1.0);
+  for (int i = 0; i < m; ++i) out[i] = colour_distance(k, c[i]);
+}
+void orc_world_sum(int W, const int* ws, const float* v, double* out, float* out_max) {
+  world_sum<float>(W, ws, v, out, out_max);
+}
+
+}  // extern "C"
