@@ -18,6 +18,13 @@ using namespace adf;
 
 namespace {
 thread_local std::string g_err;
+}
+
+namespace adf {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace adf
+
+namespace {
 
 int fail(int code, const std::string& msg) {
   g_err = msg;

@@ -164,6 +164,22 @@ int adf_debug_field(adf_solver* solver, const char* name, float* out, void* stre
  * in/out; exported for the reducer's parity test. */
 int adf_world_sum(adf_solver* solver, const float* values, double* out_sum, float* out_max, void* stream);
 
+/* No counterpart in the reference. The per-world float64 sum and maximum of adf_world_sum, for callers that cannot
+ * allocate device memory: a host loop that must not enter the CUDA allocator (cudaMalloc may synchronise the device
+ * and has no latency bound), or a process whose device memory is already reserved by another framework's pool. It
+ * needs no solver object and allocates nothing. values: device [n]; world_start: device [W + 1], non-decreasing,
+ * world_start[W] <= n; out_sum: device [W] float64; out_max: device [W] float32, floored at 0. The result equals
+ * adf_world_sum's for the same world ranges (same chunks, same tree order). Runs on the current device.
+ * Scratch: a fixed static device array of about 0.85 MB, held by every GPU that loads the library until the process
+ * exits. Limits: W <= ADF_NOALLOC_MAX_WORLDS and n / 256 + W + 1 <= ADF_NOALLOC_MAX_CHUNKS (about 12.5 million
+ * values); larger sizes return ADF_ERR_CAPACITY with a message. The first call on a device sets up (looks up the
+ * scratch's device address once, with that device current); make it before any stream capture. All calls on a
+ * device share the scratch, so calls that overlap on the GPU (on different streams) race. */
+#define ADF_NOALLOC_MAX_WORLDS 16384
+#define ADF_NOALLOC_MAX_CHUNKS 65536
+int adf_world_sum_noalloc(const float* values, int n, const int32_t* world_start, int world_count, double* out_sum,
+                          float* out_max, void* stream);
+
 /* Number of kernels this library enqueued since creation (launch accounting for benchmarks). */
 int64_t adf_kernel_launches(const adf_solver* solver);
 
