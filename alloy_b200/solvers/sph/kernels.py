@@ -33,13 +33,22 @@ def kernel_sigma(h: float, kind: str = "cubic") -> float:
 
 
 def kernel_w_np(r: np.ndarray, h: float, kind: str = "cubic") -> np.ndarray:
+    """W(r) in float64. The polynomial forms and their evaluation order are the reference's (kernels.py:155-170):
+    the wall fit below differentiates W numerically, which would amplify any other rounding into the constants."""
     q = np.asarray(r, dtype=np.float64) / h
-    s = np.clip(1.0 - q, 0.0, None)
+    out = np.zeros_like(q)
+    h3 = h**3
     if kind == "wendland_c2":
-        return kernel_sigma(h, kind) * np.where(q < 1.0, s**4 * (1.0 + 4.0 * q), 0.0)
-    inner = 1.0 + 6.0 * q * q * (q - 1.0)
-    outer = 2.0 * s**3
-    return kernel_sigma(h, kind) * np.where(q <= 0.5, inner, np.where(q < 1.0, outer, 0.0))
+        m = q < 1.0
+        s = 1.0 - q[m]
+        out[m] = 21.0 / (2.0 * math.pi * h3) * s**4 * (1.0 + 4.0 * q[m])
+        return out
+    k = 8.0 / (math.pi * h3)
+    inner = q <= 0.5
+    outer = (q > 0.5) & (q < 1.0)
+    out[inner] = k * (6.0 * q[inner] ** 3 - 6.0 * q[inner] ** 2 + 1.0)
+    out[outer] = k * 2.0 * (1.0 - q[outer]) ** 3
+    return out
 
 
 def _offsets(spacing: float, h: float) -> np.ndarray:
@@ -78,15 +87,20 @@ def lattice_diagonal(spacing: float, h: float, kind: str = "cubic") -> float:
     return float(np.sum((vol * _dw_dr(r[m], h, kind)) ** 2))
 
 
+# G0(y) = int_0^y p(t) dt as power series in y (the integral of the projected kernel p, one piece per branch of W);
+# the same coefficient tables as the reference's kernels.py:182-186, evaluated with polyval as there.
+_G0 = {
+    "cubic": ((0.5, [0.0, 1.4, 0.0, -8.0 / 3.0, 0.0, 4.8, -3.2]),
+              (1.0, [-1.0 / 30.0, 1.6, 0.0, -16.0 / 3.0, 8.0, -4.8, 16.0 / 15.0])),
+    "wendland_c2": ((1.0, [0.0, 1.5, 0.0, -3.5, 0.0, 10.5, -14.0, 7.5, -1.5]),),
+}
+
+
 def _g0(y: float, kind: str) -> float:
-    """G0(y) = int_0^y p(t) dt, y in [0, 1]."""
-    if kind == "wendland_c2":
-        c = [0.0, 1.5, 0.0, -3.5, 0.0, 10.5, -14.0, 7.5, -1.5]
-        return float(np.polynomial.polynomial.polyval(y, c))
-    if y <= 0.5:
-        return 1.4 * y - (8.0 / 3.0) * y**3 + 4.8 * y**5 - 3.2 * y**6
-    u = 1.0 - y
-    return 0.5 - u**5 * (1.6 - (16.0 / 15.0) * u)
+    for top, coeffs in _G0[kind]:
+        if y <= top:
+            return float(np.polynomial.polynomial.polyval(y, coeffs))
+    return 0.5
 
 
 def halfspace_volume_np(d: float, h: float, kind: str = "cubic") -> float:

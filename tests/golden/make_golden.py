@@ -1,0 +1,115 @@
+# SPDX-License-Identifier: Apache-2.0
+"""Generate tests/golden/reference_kernels.json from the reference's own source (run in a container that has the
+reference checkout; the committed JSON is what the tests read).
+
+warp-lang is not installed, so ``warp`` is replaced by a minimal stand-in: decorators pass functions through and the
+few math helpers the scalar functions call (clamp, abs, min, max, vec2/vec3, length) are plain Python. The
+reference's scalar functions then evaluate in float64 Python arithmetic: these vectors pin the *mathematics* of
+the kernels, the half-space volume, the wall fit, the lattice constants and the colour inversion, not Warp's float32
+rounding. Sources used (paths inside the alloy project):
+  alloy/solvers/sph/kernels.py    kernel_w, kernel_grad, projected_p, _g0, _g1, halfspace_volume, lattice_sum,
+                                  boundary_fit, lattice_diagonal, _half_lattice
+  alloy/solvers/sph/config.py     particle_mass, full_neighbor_count (function bodies extracted with ast)
+  alloy/solvers/sph/particle_walls.py  colour_distance, pw_project (function bodies extracted with ast)
+
+Usage: python tests/golden/make_golden.py /path/to/alloy-checkout
+"""
+
+from __future__ import annotations
+
+import ast
+import importlib.util
+import json
+import math
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+OUT = Path(__file__).resolve().parent / "reference_kernels.json"
+
+
+def warp_stand_in() -> types.ModuleType:
+    wp = types.ModuleType("warp")
+    ident = lambda f=None, **kw: f if f is not None else (lambda g: g)  # noqa: E731
+    wp.func = wp.kernel = wp.struct = ident
+    wp.constant = lambda x: x
+    wp.pi = math.pi
+    wp.clamp = lambda x, lo, hi: min(max(x, lo), hi)
+    wp.abs = abs
+    wp.min = min
+    wp.max = max
+    wp.vec2 = lambda *a: np.array(a, dtype=np.float64)
+    wp.vec3 = lambda *a: np.array(a, dtype=np.float64)
+    wp.length = lambda v: float(np.linalg.norm(v))
+    wp.dot = lambda a, b: float(np.dot(a, b))
+    wp.int64 = int
+    wp.float64 = float
+    wp.round = round
+    return wp
+
+
+def load_module(path: Path, name: str):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def extract(path: Path, names: list[str], namespace: dict) -> dict:
+    """Exec the named top-level functions of ``path`` (decorators dropped) in ``namespace``."""
+    tree = ast.parse(path.read_text())
+    keep = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name in names]
+    for n in keep:
+        n.decorator_list = []
+    mod = ast.Module(body=keep, type_ignores=[])
+    exec(compile(mod, str(path), "exec"), namespace)
+    return {n: namespace[n] for n in names}
+
+
+def main(root: Path) -> None:
+    sys.modules["warp"] = warp_stand_in()
+    sph = root / "alloy" / "solvers" / "sph"
+    K = load_module(sph / "kernels.py", "ref_sph_kernels")
+    ns = {"math": math, "np": np, "kernel_w_np": K.kernel_w_np, "lattice_sum": K.lattice_sum,
+          "halfspace_volume": K.halfspace_volume, "wp": sys.modules["warp"], "BISECT": 30}
+
+    class Cfg:
+        def __init__(self, r, kind):
+            self.particle_radius, self.support_factor, self.kernel = r, 4.0, kind
+
+        h = property(lambda s: s.support_factor * s.particle_radius)
+        spacing = property(lambda s: 2.0 * s.particle_radius)
+
+    fns = extract(sph / "config.py", ["particle_mass", "full_neighbor_count"], ns)
+    pw = extract(sph / "particle_walls.py", ["colour_distance", "pw_project"], ns)
+
+    cases = []
+    for r, kind in ((0.01, "cubic"), (0.005, "cubic"), (0.001, "cubic"), (0.002, "cubic"), (0.002, "wendland_c2")):
+        cfg = Cfg(r, kind)
+        s, h = cfg.spacing, cfg.h
+        kid = K.KERNEL_IDS[kind]
+        delta, amp = K.boundary_fit(s, h, kind)
+        deficit, grad = K._half_lattice(s, h, kind)
+        rs = np.linspace(0.0, 1.1 * h, 23)
+        grads = [[0.3 * h, -0.2 * h, 0.1 * h], [0.6 * h, 0.1 * h, 0.0], [1e-12 * h, 0.0, 0.0], [0.0, 0.0, 0.95 * h]]
+        ds = list(np.linspace(-1.2 * h, 1.2 * h, 25))
+        cs = list(np.linspace(0.0002, 0.999, 21))
+        cases.append({
+            "particle_radius": r, "kind": kind, "spacing": s, "h": h,
+            "lattice_sum": K.lattice_sum(s, h, kind), "particle_mass_rho1000": fns["particle_mass"](cfg, 1000.0),
+            "full_neighbor_count": fns["full_neighbor_count"](cfg), "lattice_diagonal": K.lattice_diagonal(s, h, kind),
+            "boundary_fit": [delta, amp], "half_lattice": [deficit, grad],
+            "kernel_w": [[float(x), float(K.kernel_w(float(x), h, kid))] for x in rs],
+            "kernel_grad": [[g, [float(c) for c in K.kernel_grad(np.array(g), h, kid)]] for g in grads],
+            "halfspace": [[float(d), [float(c) for c in K.halfspace_volume(float(d), h, 0.0, kid)]] for d in ds],
+            "colour_distance": [[float(c), float(pw["colour_distance"](float(c), h, kid))] for c in cs],
+        })
+    OUT.write_text(json.dumps({"source": "alloy/solvers/sph kernels.py, config.py, particle_walls.py (float64 Python "
+                                         "evaluation with a warp stand-in)", "cases": cases}, indent=1))
+    print(f"wrote {OUT} ({len(cases)} cases)")
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))

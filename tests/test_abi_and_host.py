@@ -1,0 +1,107 @@
+# SPDX-License-Identifier: Apache-2.0
+"""CPU checks of the boundary: the library builds for sm_100a, loads without a GPU and exports every entry point
+include/alloy_dfsph.h declares (no compute calls); the host logic of SolverDFSPH (configuration, emitter layers,
+scene builders, world sharding) matches the reference's."""
+
+from __future__ import annotations
+
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from alloy_b200 import _lib
+from alloy_b200.solvers.sph import config as C
+from alloy_b200.solvers.sph.build import box_shell_points
+from alloy_b200.solvers.sph.config import DFSPHConfig
+from alloy_b200.solvers.sph.sharding import shard_worlds, sub_arrays
+from alloy_b200.solvers.sph.solver import layer_offsets, quat_rotate_inv
+from alloy_b200.solvers.sph.testing import batched_worlds, dam_break
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared() -> list[str]:
+    text = (ROOT / "include" / "alloy_dfsph.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_0-9]+\s*\**\s*(adf_[a-z_0-9]+)\(", text, re.M)))
+
+
+def test_library_builds_loads_and_exports_every_declared_entry_point():
+    from alloy_b200 import build
+
+    build.build()
+    L = _lib.lib()
+    names = _declared()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing
+    assert set(names) == set(_lib.EXPORTS)
+
+
+def test_status_codes_map_to_the_reference_exceptions():
+    L = _lib.lib()
+    # a null solver is refused on the host, before any CUDA call
+    with pytest.raises(ValueError, match="null"):
+        _lib.check(L.adf_get_report(None, None, None))
+    with pytest.raises(ValueError, match="null solver"):
+        _lib.check(L.adf_step(None, None, None, None, None, None, 1.0e-3, None))
+    with pytest.raises(_lib.CapacityError):
+        _lib.check(-_lib.ADF_ERR_CAPACITY)
+
+
+def test_config_validation_messages_follow_the_reference():
+    with pytest.raises(ValueError, match="jacobi_omega must be in"):
+        DFSPHConfig(jacobi_omega=0.8).validate()
+    with pytest.raises(ValueError, match="need 0 < min_iterations <= max_iterations"):
+        DFSPHConfig(min_iterations=5, max_iterations=4).validate()
+    with pytest.raises(ValueError, match="neighbor|support_factor"):
+        DFSPHConfig(support_factor=1.0).validate()
+    f = DFSPHConfig.fast(particle_radius=0.01)
+    assert f.rest_jitter_speed is None and f.cfl == 0.4 and f.h == pytest.approx(0.04)
+    assert DFSPHConfig(surface_tension="csf").unsupported() == ["surface_tension 'csf'"]
+    assert DFSPHConfig().unsupported(viscosity_max=0.5) == ["viscosity weiler2018 (implicit viscosity)"]
+
+
+def test_time_step_helpers():
+    cfg = DFSPHConfig(particle_radius=0.01)
+    assert C.stable_dt(cfg, 0.0) == cfg.dt_max
+    assert C.stable_dt(cfg, float("inf")) == cfg.dt_min
+    assert C.stable_dt(cfg, 10.0) == pytest.approx(0.2 * 0.02 / 10.0)
+    assert C.snap_down(3.0e-4, 0.02) == 0.02 / 128 and C.snap_down(3.2e-4, 0.02) == 0.02 / 64
+    assert C.snap_down(1e-9, 0.02) == 0.02 / 1024
+
+
+def test_emitter_layer_matches_the_reference_rule():
+    # a 0.3 m nozzle at 0.1 m spacing has 3 columns, not 2 (emitters.py:48-64)
+    pts = layer_offsets(np.array([0.15, 0.15, 0.05]), np.array([0.0, 0.0, -1.0]), 0.1)
+    assert pts.shape == (9, 3) and np.all(pts[:, 2] == 0.0)
+    assert sorted(set(np.round(pts[:, 0], 6))) == [-0.1, 0.0, 0.1]
+    v = quat_rotate_inv([0.0, 0.0, np.sin(np.pi / 4), np.cos(np.pi / 4)], [1.0, 0.0, 0.0])
+    np.testing.assert_allclose(v, [0.0, -1.0, 0.0], atol=1e-12)
+
+
+def test_particle_box_counts_and_faces():
+    pts = box_shell_points((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 0.02)
+    assert len(pts) == 52**3 - 50**3
+    assert np.isclose(pts.min(), -0.01) and np.isclose(pts.max(), 1.01)
+    open_top = box_shell_points((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 0.02, open_top=True)
+    assert len(open_top) == len(pts) - 52 * 52 and open_top[:, 2].max() < 1.0
+    sc = dam_break()
+    assert sc.fluid_count == 8000 and sc.wall_count == 52**3 - 50**3
+    h = sc.model.host()
+    assert np.all(np.abs(h["q"][:8000] - np.round(h["q"][:8000] / 0.02 - 0.5) * 0.02 - 0.01) <= 0.01 * 0.02 + 1e-7)
+
+
+def test_world_sharding_balances_and_keeps_world_order():
+    sizes = [5000, 100, 3000, 3000, 200, 7000]
+    parts = shard_worlds(sizes, 2)
+    assert sorted(w for p in parts for w in p) == list(range(6))
+    loads = [sum(sizes[w] for w in p) for p in parts]
+    assert max(loads) - min(loads) <= max(sizes) and all(p == sorted(p) for p in parts)
+    sc = batched_worlds(worlds=5, lo=300, hi=900, seed=1)
+    arr = sc.model.host()
+    sub = sub_arrays(arr, [1, 3])
+    ws = arr["world_start"]
+    np.testing.assert_array_equal(sub["q"], np.concatenate([arr["q"][ws[1]:ws[2]], arr["q"][ws[3]:ws[4]]]))
+    assert sub["world_start"].tolist() == [0, ws[2] - ws[1], ws[2] - ws[1] + ws[4] - ws[3]]
