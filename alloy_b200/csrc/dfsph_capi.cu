@@ -197,7 +197,13 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   LAUNCH(s, k_scatter, blocks(n), BLOCK, st, P);
   prof_end(s, st);
   prof_begin(s, 1, st);
-  LAUNCH(s, k_lists, blocks(n), BLOCK, st, P);
+  if (s->K <= LU_ROW) {
+    LAUNCH(s, k_lists_union, blocks(n, 32 * LU_WARPS), 32 * LU_WARPS, st, P);
+  } else {
+    const size_t smem = sizeof(int) * (size_t)s->K * LS_THREADS;
+    k_lists_smem<<<blocks(n, LS_THREADS), LS_THREADS, smem, st>>>(P);
+    ++s->launches;
+  }
   prof_end(s, st);
   prof_begin(s, 2, st);
   LAUNCH(s, k_wall_slots, blocks(n), BLOCK, st, P);
@@ -407,10 +413,12 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.vel, n);
   rc |= s->alloc(&d.vel2, n);
   rc |= s->alloc(&d.id_of, n);
+  rc |= s->alloc(&d.pos_of, n);
   rc |= s->alloc(&d.world_s, n);
   rc |= s->alloc(&d.kv_s, n);
   rc |= s->alloc(&d.kd_s, n);
   rc |= s->alloc(&d.nbr, (size_t)s->K * n);
+  rc |= s->alloc(&d.nbrF, (size_t)s->K * n);
   rc |= s->alloc(&d.cnt, n);
   rc |= s->alloc(&d.slot_g, n);
   rc |= s->alloc(&d.slot_vb, n);
@@ -512,6 +520,8 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     CKC(cudaMemset(s->mass0, 0, 8 * W));
   }
   CKC(cudaGetLastError());
+  CKC(cudaFuncSetAttribute(k_lists_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(int) * (size_t)s->K * LS_THREADS)));
   CKC(cudaHostAlloc((void**)&s->pinned, 2 * sizeof(int), cudaHostAllocDefault));
   CKC(cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming));

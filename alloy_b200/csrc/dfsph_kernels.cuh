@@ -84,10 +84,12 @@ struct DevP {
   float4* vel;   // vx vy vz, rest density
   float4* vel2;  // XSPH output
   int* id_of;
+  int* pos_of;  // caller order -> sorted position (liquid and walls; written by k_scatter)
   int* world_s;
   float* kv_s;
   float* kd_s;
-  int* nbr;  // [K][n] sorted positions, ascending original id
+  int* nbr;     // [K][n] sorted positions, ascending original id
+  float* nbrF;  // [K][n] gradient factor F(r_ij) of each row entry, written by k_density_alpha
   int* cnt;
   float4* slot_g;   // dPsi/dx (3), psi; psi < 0: no slot
   float4* slot_vb;  // wall velocity (3), phi
@@ -272,6 +274,7 @@ __global__ void k_scatter(DevP P) {
   P.pos[p] = make_float4(P.q[3 * i], P.q[3 * i + 1], P.q[3 * i + 2], m);
   P.vel[p] = make_float4(P.qd[3 * i], P.qd[3 * i + 1], P.qd[3 * i + 2], P.rho0[i]);
   P.id_of[p] = i;
+  P.pos_of[i] = p;
   P.world_s[p] = P.world[i];
   if (fluid) {
     P.kv_s[p] = P.kv[i];
@@ -324,6 +327,327 @@ __global__ void __launch_bounds__(BLOCK) k_lists(DevP P) {
   for (int k = 0; k < m; ++k) P.nbr[(size_t)k * P.n + p] = (int)(unsigned)(buf[k] & 0xffffffffull);
   P.cnt[p] = m;
   if (total > K) atomicAdd(&P.overflow[w], 1);
+}
+
+// The same rows built by a warp per 32 consecutive particles (capacity K <= LIST_STAGE): for each particle the
+// warp tests 32 candidates at a time (a cell row's candidates are contiguous in the sorted arrays), compacts the
+// ones within h into a shared-memory buffer, orders them by rank (the count of smaller keys; keys are unique), and
+// stages the row; the 32 staged rows are then written column by column, 128 contiguous bytes per row entry.
+constexpr int LIST_WARPS = 4;    // warps per block
+constexpr int LIST_STAGE = 64;   // largest capacity this kernel stages
+constexpr int LIST_CAND = 128;   // candidates buffered per particle; more take the selection path below
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w < v ? w : v;
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(32 * LIST_WARPS) k_lists_warp(DevP P) {
+  __shared__ unsigned long long cand[LIST_WARPS][LIST_CAND];
+  __shared__ int stage[LIST_WARPS][32][LIST_STAGE + 1];
+  __shared__ int stage_n[LIST_WARPS][32];
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const int p0 = (blockIdx.x * LIST_WARPS + wq) * 32;
+  const int nf = P.nfw[0];
+  if (p0 >= nf) return;
+  const int K = P.K;
+  const float h2 = P.kc.h2;
+  unsigned long long* cb = cand[wq];
+  const unsigned lt = (1u << lane) - 1u;
+  const int tend = min(32, nf - p0);
+  for (int t = 0; t < tend; ++t) {
+    const int p = p0 + t;
+    const int w = P.world_s[p];
+    const WorldGrid g = P.grid[w];
+    const float4 xi = P.pos[p];
+    int cx, cy, cz;
+    cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, g.nx - 1);
+    int T = 0;
+    for (int r = 0; r < 9; ++r) {
+      const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+      if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
+      const int row = g.base + (z * g.ny + y) * g.nx;
+      const int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
+      for (int base = b; base < e; base += 32) {
+        const int j = base + lane;
+        bool pass = false;
+        if (j < e && j != p) {
+          float4 xj = P.pos[j];
+          float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+          pass = dot_plain(dx, dy, dz, dx, dy, dz) < h2;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, pass);
+        if (pass) {
+          int at = T + __popc(m & lt);
+          if (at < LIST_CAND) cb[at] = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
+        }
+        T += __popc(m);
+      }
+    }
+    __syncwarp();
+    const int cnt = min(T, K);
+    if (T <= LIST_CAND) {
+      for (int c = lane; c < T; c += 32) {  // rank of each key among the T (unique) keys
+        const unsigned long long key = cb[c];
+        int rank = 0;
+        for (int u = 0; u < T; ++u) rank += cb[u] < key;
+        if (rank < K) stage[wq][t][rank] = (int)(unsigned)(key & 0xffffffffull);
+      }
+    } else {
+      // more candidates than the buffer holds (a pile of particles within h): select the K lowest keys one by one
+      unsigned long long last = 0;
+      for (int k = 0; k < cnt; ++k) {
+        unsigned long long best = ~0ull;
+        for (int r = 0; r < 9; ++r) {
+          const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+          if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
+          const int row = g.base + (z * g.ny + y) * g.nx;
+          const int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
+          for (int j = b + lane; j < e; j += 32) {
+            if (j == p) continue;
+            float4 xj = P.pos[j];
+            float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+              unsigned long long key = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
+              if ((k == 0 || key > last) && key < best) best = key;
+            }
+          }
+        }
+        best = warp_min_u64(best);
+        if (lane == 0) stage[wq][t][k] = (int)(unsigned)(best & 0xffffffffull);
+        last = best;
+      }
+    }
+    if (lane == 0) {
+      stage_n[wq][t] = cnt;
+      if (T > K) atomicAdd(&P.overflow[w], 1);
+    }
+    __syncwarp();
+  }
+  // write the staged rows: entry k of 32 consecutive particles is one contiguous 128-byte segment
+  const int myn = lane < tend ? stage_n[wq][lane] : 0;
+  int kmax = myn;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+  for (int k = 0; k < kmax; ++k)
+    if (k < myn) P.nbr[(size_t)k * P.n + p0 + lane] = stage[wq][lane][k];
+  if (lane < tend) P.cnt[p0 + lane] = myn;
+}
+
+// The same rows, one thread per particle with its row kept in shared memory as ascending original ids (entry k of
+// thread t at [k][t]: threads inserting at the same k use distinct banks), mapped back to sorted positions through
+// pos_of when written. 32 independent particles per warp keep many candidate loads in flight.
+constexpr int LS_THREADS = 128;
+
+__global__ void __launch_bounds__(LS_THREADS) k_lists_smem(DevP P) {
+  extern __shared__ int srow[];
+  const int p = blockIdx.x * LS_THREADS + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  int* buf = srow + threadIdx.x;
+  const int K = P.K;
+  const int w = P.world_s[p];
+  const WorldGrid g = P.grid[w];
+  const float4 xi = P.pos[p];
+  const float h2 = P.kc.h2;
+  int cx, cy, cz;
+  cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
+  const int x0 = max(cx - 1, 0), x1 = min(cx + 1, g.nx - 1);
+  int m = 0, total = 0;
+  for (int r = 0; r < 9; ++r) {
+    const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+    if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
+    const int row = g.base + (z * g.ny + y) * g.nx;
+    const int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
+    for (int j = b; j < e; ++j) {
+      if (j == p) continue;
+      float4 xj = P.pos[j];
+      float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+      if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+        ++total;
+        const int id = P.id_of[j];
+        if (m == K && id >= buf[(K - 1) * LS_THREADS]) continue;
+        int at = (m < K) ? m : K - 1;
+        while (at > 0) {
+          int prev = buf[(at - 1) * LS_THREADS];
+          if (prev <= id) break;
+          buf[at * LS_THREADS] = prev;
+          --at;
+        }
+        buf[at * LS_THREADS] = id;
+        if (m < K) ++m;
+      }
+    }
+  }
+  for (int k = 0; k < m; ++k) P.nbr[(size_t)k * P.n + p] = P.pos_of[buf[k * LS_THREADS]];
+  P.cnt[p] = m;
+  if (total > K) atomicAdd(&P.overflow[w], 1);
+}
+
+// Rows of 32 consecutive sorted particles built by one warp in lockstep (capacity K <= 64):
+//  1. scan: the union of the 32 particles' 27-cell neighbourhoods is one box of cell rows whose candidates are
+//     contiguous; 32 candidates at a time are staged in shared memory and every lane tests all of them against its
+//     own particle, appending the original id of each one within h to its row (unsorted). A warp whose particles span
+//     a large box (a row wrap, a splash) scans each lane's own 27 cells instead.
+//  2. order: rows of at most 32 entries are sorted in registers by a fully unrolled bitonic network; longer rows by
+//     insertion in shared memory; a row with more than 64 candidates selects its K lowest ids by repeated scans.
+//  3. write: entry k of the 32 rows is one contiguous 128-byte segment (ids mapped to sorted positions by pos_of).
+constexpr int LU_WARPS = 4;
+constexpr int LU_ROW = 64;         // row buffer per particle (and the largest capacity this kernel builds)
+constexpr int LU_MAX_CELLS = 108;  // largest union box scanned in lockstep
+
+__device__ __forceinline__ void sort32_registers(unsigned (&key)[32]) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const unsigned a = key[i], b = key[l];
+          const unsigned lo = min(a, b), hi = max(a, b);
+          if ((i & k) == 0) {
+            key[i] = lo;
+            key[l] = hi;
+          } else {
+            key[i] = hi;
+            key[l] = lo;
+          }
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
+  __shared__ unsigned rows[LU_WARPS][LU_ROW][32];  // [warp][entry][lane]: lanes of one entry in distinct banks
+  __shared__ float4 cpos[LU_WARPS][32];
+  __shared__ unsigned cid[LU_WARPS][32];
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const int p0 = (blockIdx.x * LU_WARPS + wq) * 32;
+  const int nf = P.nfw[0];
+  if (p0 >= nf) return;
+  const int tend = min(32, nf - p0);
+  const bool valid = lane < tend;
+  const int p = valid ? p0 + lane : p0;
+  const int w = P.world_s[p];
+  const WorldGrid g = P.grid[w];
+  const float4 xi = P.pos[p];
+  const float h2 = P.kc.h2;
+  const int K = P.K;
+  int cx, cy, cz;
+  cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
+  const unsigned full = 0xffffffffu;
+  const int w_lo = __reduce_min_sync(full, (unsigned)w), w_hi = __reduce_max_sync(full, (unsigned)w);
+  const int xlo = max((int)__reduce_min_sync(full, (unsigned)cx) - 1, 0);
+  const int xhi = min((int)__reduce_max_sync(full, (unsigned)cx) + 1, g.nx - 1);
+  const int ylo = max((int)__reduce_min_sync(full, (unsigned)cy) - 1, 0);
+  const int yhi = min((int)__reduce_max_sync(full, (unsigned)cy) + 1, g.ny - 1);
+  const int zlo = max((int)__reduce_min_sync(full, (unsigned)cz) - 1, 0);
+  const int zhi = min((int)__reduce_max_sync(full, (unsigned)cz) + 1, g.nz - 1);
+  unsigned* myrow = &rows[wq][0][lane];
+  int cnt = 0, total = 0;
+  const bool lockstep = w_lo == w_hi && (xhi - xlo + 1) * (yhi - ylo + 1) * (zhi - zlo + 1) <= LU_MAX_CELLS;
+  if (lockstep) {
+    for (int z = zlo; z <= zhi; ++z) {
+      for (int y = ylo; y <= yhi; ++y) {
+        const int row = g.base + (z * g.ny + y) * g.nx;
+        const int b = P.cell_start[row + xlo], e = P.cell_start[row + xhi + 1];
+        for (int c0 = b; c0 < e; c0 += 32) {
+          const int nc = min(32, e - c0);
+          if (lane < nc) {
+            cpos[wq][lane] = P.pos[c0 + lane];
+            cid[wq][lane] = (unsigned)P.id_of[c0 + lane];
+          }
+          __syncwarp();
+          for (int t = 0; t < nc; ++t) {
+            const float4 xj = cpos[wq][t];
+            const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            if (valid && c0 + t != p && dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+              if (cnt < LU_ROW) myrow[cnt * 32] = cid[wq][t];
+              ++cnt;
+            }
+          }
+          __syncwarp();
+        }
+      }
+    }
+  } else if (valid) {
+    for (int r = 0; r < 9; ++r) {
+      const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+      if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
+      const int row = g.base + (z * g.ny + y) * g.nx;
+      const int b = P.cell_start[row + max(cx - 1, 0)], e = P.cell_start[row + min(cx + 1, g.nx - 1) + 1];
+      for (int j = b; j < e; ++j) {
+        if (j == p) continue;
+        const float4 xj = P.pos[j];
+        const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+          if (cnt < LU_ROW) myrow[cnt * 32] = (unsigned)P.id_of[j];
+          ++cnt;
+        }
+      }
+    }
+  }
+  total = valid ? cnt : 0;
+  cnt = min(total, LU_ROW);
+  const int cmax = __reduce_max_sync(full, (unsigned)total);
+  if (cmax <= 32) {
+    unsigned key[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) key[k] = k < cnt ? myrow[k * 32] : 0xffffffffu;
+    sort32_registers(key);
+#pragma unroll
+    for (int k = 0; k < 32; ++k)
+      if (k < cnt) myrow[k * 32] = key[k];
+  } else if (total <= LU_ROW) {
+    for (int a = 1; a < cnt; ++a) {  // insertion sort of this lane's row
+      const unsigned v = myrow[a * 32];
+      int at = a;
+      while (at > 0 && myrow[(at - 1) * 32] > v) {
+        myrow[at * 32] = myrow[(at - 1) * 32];
+        --at;
+      }
+      myrow[at * 32] = v;
+    }
+  } else {
+    // more candidates than the row buffer: the K lowest ids by repeated scans of this particle's 27 cells
+    unsigned last = 0;
+    const int kk = min(total, K);
+    for (int k = 0; k < kk; ++k) {
+      unsigned best = 0xffffffffu;
+      for (int r = 0; r < 9; ++r) {
+        const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+        if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
+        const int row = g.base + (z * g.ny + y) * g.nx;
+        const int b = P.cell_start[row + max(cx - 1, 0)], e = P.cell_start[row + min(cx + 1, g.nx - 1) + 1];
+        for (int j = b; j < e; ++j) {
+          if (j == p) continue;
+          const float4 xj = P.pos[j];
+          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+          if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+            const unsigned id = (unsigned)P.id_of[j];
+            if ((k == 0 || id > last) && id < best) best = id;
+          }
+        }
+      }
+      myrow[k * 32] = best;
+      last = best;
+    }
+  }
+  const int m = min(total, K);
+  const int mmax = __reduce_max_sync(full, (unsigned)m);
+  for (int k = 0; k < mmax; ++k)
+    if (k < m) P.nbr[(size_t)k * P.n + p] = P.pos_of[myrow[k * 32]];
+  if (valid) {
+    P.cnt[p] = m;
+    if (total > K) atomicAdd(&P.overflow[w], 1);
+  }
 }
 
 // --------------------------------------------------------------------------------------- particle-wall slot
@@ -423,6 +747,30 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
   P.slot_xb[p] = make_float4(ADF_FMA(-phi, nx, xi.x), ADF_FMA(-phi, ny, xi.y), ADF_FMA(-phi, nz, xi.z), 0.0f);
 }
 
+// Neighbour loops read their rows in batches of NB: the NB row entries first, then the NB gathers they address,
+// then the arithmetic in ascending row order, so the loads of a batch overlap instead of forming one dependent
+// chain per neighbour. Entries past the row's end address the particle itself (a harmless load) and are skipped.
+constexpr int NB = 8;
+
+__device__ __forceinline__ void load_row_batch(const DevP& P, int p, int c, int k, int (&j)[NB]) {
+  const int* row = P.nbr + p;
+#pragma unroll
+  for (int u = 0; u < NB; ++u) j[u] = (k + u < c) ? __ldg(row + (size_t)(k + u) * P.n) : p;
+}
+
+// Row entries with their gradient factor F(r_ij) (the value wf() gives for the pair, stored by k_density_alpha):
+// the later loops read F instead of re-evaluating sqrt, branches and a division per pair; the value is the same.
+__device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, int k, int (&j)[NB], float (&f)[NB]) {
+  const int* row = P.nbr + p;
+  const float* rowf = P.nbrF + p;
+#pragma unroll
+  for (int u = 0; u < NB; ++u) {
+    bool in = k + u < c;
+    j[u] = in ? __ldg(row + (size_t)(k + u) * P.n) : p;
+    f[u] = in ? __ldg(rowf + (size_t)(k + u) * P.n) : 0.0f;
+  }
+}
+
 // ------------------------------------------------------------------------------------------ density, factor
 // pressure.py:144-193
 __global__ void __launch_bounds__(BLOCK) k_density_alpha(DevP P) {
@@ -435,22 +783,30 @@ __global__ void __launch_bounds__(BLOCK) k_density_alpha(DevP P) {
   float rho = mi * P.kc.sigma;
   float Gx = 0.0f, Gy = 0.0f, Gz = 0.0f, sq = 0.0f;
   int c = P.cnt[p];
-  const int* row = P.nbr + p;
-  for (int k = 0; k < c; ++k) {
-    int j = row[(size_t)k * P.n];
-    float4 xj = P.pos[j];
-    float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-    float r2 = dot_plain(rx, ry, rz, rx, ry, rz);
-    float W, F;
-    wf(P.kc, r2, W, F);
-    float mj = xj.w;
-    rho = ADF_FMA(mj, W, rho);
-    float a = mj * inv_r0;
-    float aF = a * F;
-    Gx = ADF_FMA(aF, rx, Gx);
-    Gy = ADF_FMA(aF, ry, Gy);
-    Gz = ADF_FMA(aF, rz, Gz);
-    sq = ADF_FMA(bi * a, (F * F) * r2, sq);
+  for (int k = 0; k < c; k += NB) {
+    int j[NB];
+    load_row_batch(P, p, c, k, j);
+    float4 xb[NB];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) xb[u] = P.pos[j[u]];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      if (k + u >= c) break;
+      float4 xj = xb[u];
+      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      float r2 = dot_plain(rx, ry, rz, rx, ry, rz);
+      float W, F;
+      wf(P.kc, r2, W, F);
+      P.nbrF[(size_t)(k + u) * P.n + p] = F;
+      float mj = xj.w;
+      rho = ADF_FMA(mj, W, rho);
+      float a = mj * inv_r0;
+      float aF = a * F;
+      Gx = ADF_FMA(aF, rx, Gx);
+      Gy = ADF_FMA(aF, ry, Gy);
+      Gz = ADF_FMA(aF, rz, Gz);
+      sq = ADF_FMA(bi * a, (F * F) * r2, sq);
+    }
   }
   float psi = 0.0f;
   float4 sg = P.slot_g[p];
@@ -480,16 +836,24 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   float inv_r0 = 1.0f / vi.w;
   float rate = 0.0f;
   int c = P.cnt[p];
-  const int* row = P.nbr + p;
-  for (int k = 0; k < c; ++k) {
-    int j = row[(size_t)k * P.n];
-    float4 xj = P.pos[j];
-    float4 vj = P.vel[j];
-    float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-    float W, F;
-    wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
-    float aF = (xj.w * inv_r0) * F;
-    rate = ADF_FMA(aF, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, rx, ry, rz), rate);
+  for (int k = 0; k < c; k += NB) {
+    int j[NB];
+    float fb[NB];
+    load_row_batch_f(P, p, c, k, j, fb);
+    float4 xb[NB], vb[NB];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      xb[u] = P.pos[j[u]];
+      vb[u] = P.vel[j[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      if (k + u >= c) break;
+      float4 xj = xb[u], vj = vb[u];
+      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      float aF = (xj.w * inv_r0) * fb[u];
+      rate = ADF_FMA(aF, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, rx, ry, rz), rate);
+    }
   }
   float4 sg = P.slot_g[p];
   if (sg.w >= 0.0f) {
@@ -546,18 +910,27 @@ __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, 
   float ki = P.kr[p];
   ax = ay = az = 0.0f;
   int c = P.cnt[p];
-  const int* row = P.nbr + p;
-  for (int k = 0; k < c; ++k) {
-    int j = row[(size_t)k * P.n];
-    float4 xj = P.pos[j];
-    float krj = P.kr[j];
-    float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-    float W, F;
-    wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
-    float cF = (xj.w * (ki + krj)) * F;
-    ax = ADF_FMA(-cF, rx, ax);
-    ay = ADF_FMA(-cF, ry, ay);
-    az = ADF_FMA(-cF, rz, az);
+  for (int k = 0; k < c; k += NB) {
+    int j[NB];
+    float fb[NB];
+    load_row_batch_f(P, p, c, k, j, fb);
+    float4 xb[NB];
+    float kb[NB];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      xb[u] = P.pos[j[u]];
+      kb[u] = P.kr[j[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      if (k + u >= c) break;
+      float4 xj = xb[u];
+      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      float cF = (xj.w * (ki + kb[u])) * fb[u];
+      ax = ADF_FMA(-cF, rx, ax);
+      ay = ADF_FMA(-cF, ry, ay);
+      az = ADF_FMA(-cF, rz, az);
+    }
   }
   float4 sg = P.slot_g[p];
   if (sg.w >= 0.0f) {
@@ -588,16 +961,24 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
   float inv_r0 = 1.0f / r0;
   float ar = 0.0f;
   int c = P.cnt[p];
-  const int* row = P.nbr + p;
-  for (int k = 0; k < c; ++k) {
-    int j = row[(size_t)k * P.n];
-    float4 xj = P.pos[j];
-    float4 aj = P.acc[j];
-    float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-    float W, F;
-    wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
-    float aF = (xj.w * inv_r0) * F;
-    ar = ADF_FMA(aF, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz), ar);
+  for (int k = 0; k < c; k += NB) {
+    int j[NB];
+    float fb[NB];
+    load_row_batch_f(P, p, c, k, j, fb);
+    float4 xb[NB], ab[NB];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      xb[u] = P.pos[j[u]];
+      ab[u] = P.acc[j[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      if (k + u >= c) break;
+      float4 xj = xb[u], aj = ab[u];
+      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      float aF = (xj.w * inv_r0) * fb[u];
+      ar = ADF_FMA(aF, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz), ar);
+    }
   }
   float4 sg = P.slot_g[p];
   if (sg.w >= 0.0f) ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
@@ -732,20 +1113,32 @@ __global__ void __launch_bounds__(BLOCK) k_xsph(DevP P) {
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
     float rho_i = P.ratio[p] * vi.w;
     int cn = P.cnt[p];
-    const int* row = P.nbr + p;
-    for (int k = 0; k < cn; ++k) {
-      int j = row[(size_t)k * P.n];
-      float4 vj = P.vel[j];
-      float rho_bar = 0.5f * (rho_i + P.ratio[j] * vj.w);
-      if (rho_bar > 0.0f) {
-        float4 xj = P.pos[j];
-        float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-        float W, F;
-        wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
-        float cw = (xj.w / rho_bar) * W;
-        cx = ADF_FMA(cw, vj.x - vi.x, cx);
-        cy = ADF_FMA(cw, vj.y - vi.y, cy);
-        cz = ADF_FMA(cw, vj.z - vi.z, cz);
+    for (int k = 0; k < cn; k += NB) {
+      int j[NB];
+      load_row_batch(P, p, cn, k, j);
+      float4 xb[NB], vb[NB];
+      float rb[NB];
+#pragma unroll
+      for (int u = 0; u < NB; ++u) {
+        xb[u] = P.pos[j[u]];
+        vb[u] = P.vel[j[u]];
+        rb[u] = P.ratio[j[u]];
+      }
+#pragma unroll
+      for (int u = 0; u < NB; ++u) {
+        if (k + u >= cn) break;
+        float4 vj = vb[u];
+        float rho_bar = 0.5f * (rho_i + rb[u] * vj.w);
+        if (rho_bar > 0.0f) {
+          float4 xj = xb[u];
+          float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+          float W, F;
+          wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
+          float cw = (xj.w / rho_bar) * W;
+          cx = ADF_FMA(cw, vj.x - vi.x, cx);
+          cy = ADF_FMA(cw, vj.y - vi.y, cy);
+          cz = ADF_FMA(cw, vj.z - vi.z, cz);
+        }
       }
     }
     vx = ADF_FMA(c, cx, vx);
@@ -815,6 +1208,7 @@ __global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
       atomicAdd(&P.escaped[w], 1);
     }
   }
+  int speed_bits = 0;  // float bits of a non-negative speed (their integer order is the float order)
   if (gone) {
     P.flags[i] = P.flags[i] & ~FLAG_ACTIVE;
     P.phase[i] = (int8_t)-2;
@@ -822,11 +1216,20 @@ __global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
     atomicAdd((unsigned long long*)&P.mass_out[w], (unsigned long long)to_fixed(P.mass[i]));
   } else {
     float sp = __fsqrt_rn(dotf(vx, vy, vz, vx, vy, vz));
-    if (isfinite(sp) && isfinite((x + y) + z)) atomicMax(&P.max_speed_bits[w], __float_as_int(sp));
+    if (isfinite(sp) && isfinite((x + y) + z)) speed_bits = __float_as_int(sp);
     else {
       atomicAdd(&P.nonfinite[w], 1);
-      atomicMax(&P.max_speed_bits[w], __float_as_int(1.0e30f));
+      speed_bits = __float_as_int(1.0e30f);
     }
+  }
+  // per-world maximum: one atomic per warp when the warp's liquid lanes share a world (sorted storage groups worlds)
+  const unsigned lanes = __activemask();
+  const int w0 = __shfl_sync(lanes, w, __ffs(lanes) - 1);
+  if (__all_sync(lanes, w == w0)) {
+    unsigned m = __reduce_max_sync(lanes, (unsigned)speed_bits);
+    if ((threadIdx.x & 31) == __ffs(lanes) - 1 && m) atomicMax(&P.max_speed_bits[w0], (int)m);
+  } else if (speed_bits) {
+    atomicMax(&P.max_speed_bits[w], speed_bits);
   }
   P.q[3 * i] = x;
   P.q[3 * i + 1] = y;

@@ -258,7 +258,7 @@ def run_b200(args):
                          "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
                          "peak_src": pk["src"], "alg_bytes_per_particle": alg[dom], "mean_neighbours": nbar,
                          "avg_launch_us": per_launch_s * 1e6, "launches": cnt},
-            "kernel_time_share": shares,
+            "kernel_time_share": shares, "kernel_ms_per_step": total_ms / args.steps,
             "solver_stats": {"iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean":
                              float(np.mean(it_div)), "density_err_mean_max_over_steps": float(np.max(den_err)),
                              "density_err_max_last_step": den_max[-1]},
