@@ -17,7 +17,7 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_active_mass", "adf_get_warm_starts", "adf_set_warm_starts", "adf_state_arrays", "adf_reset",
            "adf_add_emitter", "adf_set_emitter_pool", "adf_emitter_state", "adf_set_emitter_enabled", "adf_add_sink",
            "adf_neighbor_rows", "adf_debug_field", "adf_world_sum", "adf_kernel_launches", "adf_profile_enable",
-           "adf_profile_read", "adf_list_stats", "adf_world_sum_noalloc")
+           "adf_profile_read", "adf_list_stats", "adf_world_sum_noalloc", "adf_set_graphs")
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
               "apply", "xsph", "finish", "emit")
 
@@ -90,6 +90,7 @@ def lib() -> C.CDLL:
     L.adf_profile_read.argtypes = [P, vp, vp]
     L.adf_list_stats.argtypes = [P, vp, vp, vp]
     L.adf_world_sum_noalloc.argtypes = [vp, i, vp, i, vp, vp, vp]
+    L.adf_set_graphs.argtypes = [P, i]
     for name in EXPORTS:
         if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches"):
             getattr(L, name).restype = C.c_int

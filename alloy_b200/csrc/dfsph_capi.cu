@@ -86,6 +86,20 @@ struct adf_solver {
   size_t prof_used = 0;
   int prof_open = -1;
   long long* list_entries = nullptr;
+  // CUDA graphs of whole steps (one per state-pointer set and dt), rebuilt when the emitter or sink tables change
+  struct GraphEntry {
+    const void* key[5];
+    double dt;
+    unsigned version;
+    cudaGraphExec_t exec;
+  };
+  std::vector<GraphEntry> graphs;
+  unsigned table_version = 0;
+  bool use_graphs = true;
+  long long graph_kernels = 0;  // kernels a step graph launches outside its WHILE bodies
+  long long body_kernels = 0;   // kernels of one WHILE-body iteration
+  unsigned long long* body_runs = nullptr;  // device: WHILE-body iterations run so far
+  cudaStream_t cap_stream = nullptr, body_stream = nullptr;
 
   template <class T> int alloc(T** p, size_t count) {
     int rc = dalloc(p, count);
@@ -233,8 +247,45 @@ void enqueue_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   prof_end(s, st);
 }
 
+int host_iterations(adf_solver* s, DevP& P, cudaStream_t st);
+
+// The iteration loop as a WHILE node of the graph being captured on `st` (the body: one iteration plus the
+// condition update). Mirrors wp.capture_while (solve_driver.py:186): no host round trip per iteration.
+int capture_iterations(adf_solver* s, DevP& P, cudaStream_t st) {
+  cudaStreamCaptureStatus cs;
+  unsigned long long id;
+  cudaGraph_t g;
+  const cudaGraphNode_t* deps;
+  size_t nd;
+  CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) return fail(ADF_ERR_STATE, "capture_iterations: stream not capturing");
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  LAUNCH(s, k_set_cond, 1, 1, st, h, (const int*)P.n_unconv, (unsigned long long*)nullptr);
+  CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, deps, nd, &cp));
+  CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if (!s->body_stream) CK(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
+  const long long b0 = s->launches;
+  CK(cudaStreamBeginCaptureToGraph(s->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  enqueue_iteration(s, P, s->body_stream);
+  LAUNCH(s, k_set_cond, 1, 1, s->body_stream, h, (const int*)P.n_unconv, s->body_runs);
+  cudaGraph_t out;
+  CK(cudaStreamEndCapture(s->body_stream, &out));
+  s->body_kernels = s->launches - b0;  // counted per run through body_runs, not per capture
+  s->launches = b0;
+  return check_launch();
+}
+
 // pressure.py:355-390 + solve_driver.py:121-186 (Jacobi branch) + pressure.py:393-480
-int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st) {
+int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool graph) {
   set_solve_params(s, P, mode, dt);
   const int n = s->n, W = s->W;
   CK(cudaMemsetAsync(P.err_orig, 0, sizeof(float) * n, st));
@@ -245,21 +296,13 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st) {
   if (W > 0) LAUNCH(s, k_begin_solve, blocks(W), BLOCK, st, P);
   int rc = check_launch();
   if (rc) return rc;
-  const int limit = s->prm.max_it + 2;
-  enqueue_iteration(s, P, st);
-  CK(cudaMemcpyAsync(&s->pinned[0], P.n_unconv, sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(cudaEventRecord(s->ev[0], st));
-  for (int it = 1;; ++it) {
-    if (it < limit) {
-      enqueue_iteration(s, P, st);
-      CK(cudaMemcpyAsync(&s->pinned[it & 1], P.n_unconv, sizeof(int), cudaMemcpyDeviceToHost, st));
-      CK(cudaEventRecord(s->ev[it & 1], st));
-    }
-    CK(cudaEventSynchronize(s->ev[(it - 1) & 1]));
-    if (s->pinned[(it - 1) & 1] == 0 || it >= limit) break;
+  if (graph) {
+    rc = capture_iterations(s, P, st);
+    if (rc) return rc;
+  } else {
+    rc = host_iterations(s, P, st);
+    if (rc) return rc;
   }
-  rc = check_launch();
-  if (rc) return rc;
   prof_begin(s, 8, st);
   LAUNCH(s, k_apply, blocks(n), BLOCK, st, P);
   prof_end(s, st);
@@ -270,6 +313,34 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st) {
     CK(cudaMemcpyAsync(s->iters_den, P.iters, sizeof(int) * W, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s->den_err, P.err_mean, sizeof(float) * W, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s->den_err_max, P.emax, sizeof(float) * W, cudaMemcpyDeviceToDevice, st));
+  }
+  return check_launch();
+}
+
+// The iteration loop driven from the host: iteration k+1 is enqueued before the unconverged count of iteration k
+// is read, so the GPU does not idle on the read; iterations before min_iterations cannot stop a world and are not
+// checked.
+int host_iterations(adf_solver* s, DevP& P, cudaStream_t st) {
+  const int limit = s->prm.max_it + 2;  // every world stops at max_iterations
+  const bool speculate = !s->prof_on;   // profiled runs time only iterations that do work
+  int enq = 0;
+  for (; enq < s->prm.min_it - 1; ++enq) enqueue_iteration(s, P, st);  // these cannot stop a world
+  auto push = [&]() -> int {
+    const int slot = enq & 1;
+    enqueue_iteration(s, P, st);
+    CK(cudaMemcpyAsync(&s->pinned[slot], P.n_unconv, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(s->ev[slot], st));
+    ++enq;
+    return ADF_OK;
+  };
+  int rc = push();
+  if (rc) return rc;
+  for (;;) {
+    const int last = enq - 1;
+    if (speculate && enq < limit && (rc = push())) return rc;
+    CK(cudaEventSynchronize(s->ev[last & 1]));
+    if (s->pinned[last & 1] == 0 || last + 1 >= limit) break;
+    if (!speculate && (rc = push())) return rc;
   }
   return check_launch();
 }
@@ -418,7 +489,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.kv_s, n);
   rc |= s->alloc(&d.kd_s, n);
   rc |= s->alloc(&d.nbr, (size_t)s->K * n);
-  rc |= s->alloc(&d.nbrF, (size_t)s->K * n);
+  rc |= s->alloc(&d.nbrjf, (size_t)s->K * n);
   rc |= s->alloc(&d.cnt, n);
   rc |= s->alloc(&d.slot_g, n);
   rc |= s->alloc(&d.slot_vb, n);
@@ -523,6 +594,10 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   CKC(cudaFuncSetAttribute(k_lists_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(int) * (size_t)s->K * LS_THREADS)));
   CKC(cudaHostAlloc((void**)&s->pinned, 2 * sizeof(int), cudaHostAllocDefault));
+  CKC(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+  CKC(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
+  CKC(cudaMalloc(&s->body_runs, sizeof(unsigned long long)));
+  CKC(cudaMemset(s->body_runs, 0, sizeof(unsigned long long)));
   CKC(cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming));
   CKC(cudaDeviceSynchronize());
@@ -542,20 +617,22 @@ void adf_destroy(adf_solver* s) {
     if (p) cudaFree(p);
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->list_entries) cudaFree(s->list_entries);
+  if (s->body_runs) cudaFree(s->body_runs);
+  for (auto& g : s->graphs) cudaGraphExecDestroy(g.exec);
+  if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+  if (s->body_stream) cudaStreamDestroy(s->body_stream);
   for (auto& e : s->prof_pool) cudaEventDestroy(e);
   for (auto& e : s->ev)
     if (e) cudaEventDestroy(e);
   delete s;
 }
 
-int adf_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out, float* qd_out, const float* f_ext,
-             double dt, void* stream) {
-  if (!s) return fail(ADF_ERR_VALUE, "adf_step: null solver");
-  if (!(dt > 0.0)) return fail(ADF_ERR_VALUE, "SolverDFSPH.step: dt must be > 0, got " + std::to_string(dt));
-  if (s->n == 0) return ADF_OK;
-  if (!q_in || !qd_in || !q_out || !qd_out) return fail(ADF_ERR_VALUE, "adf_step: null state array");
-  cudaStream_t st = (cudaStream_t)stream;
-  CK(cudaSetDevice(s->device));
+}  // extern "C"
+
+namespace {
+// One step's work enqueued on `st`; with `graph` the stream is capturing and the solves become WHILE nodes.
+int enqueue_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out, float* qd_out,
+                 const float* f_ext, double dt, cudaStream_t st, bool graph) {
   const size_t bytes = sizeof(float) * 3 * (size_t)s->n;
   if (q_out != q_in) CK(cudaMemcpyAsync(q_out, q_in, bytes, cudaMemcpyDeviceToDevice, st));
   if (qd_out != qd_in) CK(cudaMemcpyAsync(qd_out, qd_in, bytes, cudaMemcpyDeviceToDevice, st));
@@ -570,7 +647,7 @@ int adf_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out,
   int rc = prepare(s, P, st);
   if (rc) return rc;
   if (s->prm.divergence_solve) {
-    rc = solve(s, P, 0, dt, st);
+    rc = solve(s, P, 0, dt, st, graph);
     if (rc) return rc;
   }
   P.dt = (float)dt;
@@ -578,7 +655,7 @@ int adf_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out,
   LAUNCH(s, k_xsph, blocks(s->n), BLOCK, st, P);
   prof_end(s, st);
   std::swap(P.vel, P.vel2);
-  rc = solve(s, P, 1, dt, st);
+  rc = solve(s, P, 1, dt, st, graph);
   if (rc) return rc;
   prof_begin(s, 10, st);
   LAUNCH(s, k_finish, blocks(s->n), BLOCK, st, P);
@@ -595,6 +672,74 @@ int adf_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out,
     prof_end(s, st);
   }
   return check_launch();
+}
+
+// A whole step as a CUDA graph (built once per state-pointer set, dt and emitter/sink table version).
+int graph_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out, float* qd_out, const float* f_ext,
+               double dt, cudaStream_t st) {
+  const void* key[5] = {q_in, qd_in, q_out, qd_out, f_ext};
+  for (auto& g : s->graphs) {
+    if (g.dt == dt && g.version == s->table_version && std::equal(key, key + 5, g.key)) {
+      CK(cudaGraphLaunch(g.exec, st));
+      s->launches += s->graph_kernels;
+      return ADF_OK;
+    }
+  }
+  if (!s->cap_stream) CK(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+  if (!s->body_stream) CK(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
+  const long long before = s->launches;
+  CK(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, s->cap_stream, true);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s->cap_stream, &g);
+  s->graph_kernels = s->launches - before;
+  s->launches = before;
+  if (rc || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return rc ? rc : fail(ADF_ERR_CUDA, std::string("step graph capture: ") + cudaGetErrorString(e));
+  }
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(ADF_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  if (s->graphs.size() >= 4) {
+    cudaGraphExecDestroy(s->graphs.front().exec);
+    s->graphs.erase(s->graphs.begin());
+  }
+  adf_solver::GraphEntry ge;
+  std::copy(key, key + 5, ge.key);
+  ge.dt = dt;
+  ge.version = s->table_version;
+  ge.exec = exec;
+  s->graphs.push_back(ge);
+  CK(cudaGraphLaunch(exec, st));
+  s->launches += s->graph_kernels;
+  return ADF_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int adf_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out, float* qd_out, const float* f_ext,
+             double dt, void* stream) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_step: null solver");
+  if (!(dt > 0.0)) return fail(ADF_ERR_VALUE, "SolverDFSPH.step: dt must be > 0, got " + std::to_string(dt));
+  if (s->n == 0) return ADF_OK;
+  if (!q_in || !qd_in || !q_out || !qd_out) return fail(ADF_ERR_VALUE, "adf_step: null state array");
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaSetDevice(s->device));
+  cudaStreamCaptureStatus cs;
+  CK(cudaStreamIsCapturing(st, &cs));
+  if (cs == cudaStreamCaptureStatusActive)  // the caller is capturing: the step joins its graph
+    return enqueue_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st, true);
+  if (!s->use_graphs || s->prof_on) return enqueue_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st, false);
+  return graph_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st);
+}
+
+int adf_set_graphs(adf_solver* s, int enable) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_graphs: null solver");
+  s->use_graphs = enable != 0;
+  return ADF_OK;
 }
 
 int adf_density_ratio(adf_solver* s, const float* q, const float* qd, float* ratio_out, float* active_out,
@@ -747,6 +892,7 @@ int adf_add_emitter(adf_solver* s, int world, const float* xform, const float* o
     for (int a = 0; a < 3; ++a) s->off_local_h.push_back(offsets[3 * c + a]);
   }
   s->pool_h.insert(s->pool_h.end(), pool, pool + pool_size);
+  ++s->table_version;
   int rc = upload_emitters(s, idx);
   if (rc) return -rc;
   return idx;
@@ -778,6 +924,7 @@ int adf_set_emitter_pool(adf_solver* s, int e, const int32_t* pool, int pool_siz
     s->em_h[k].pool_begin = b;
   }
   s->pool_h.swap(pools);
+  ++s->table_version;
   return upload_emitters(s, ne);
 }
 
@@ -812,6 +959,7 @@ int adf_add_sink(adf_solver* s, int world, const float* xform, const float* half
   std::memcpy(k.xform, xform, sizeof(float) * 7);
   std::memcpy(k.half, half, sizeof(float) * 3);
   s->sinks_h.push_back(k);
+  ++s->table_version;
   if (s->sinks_d) cudaFree(s->sinks_d);
   s->sinks_d = nullptr;
   if (dalloc(&s->sinks_d, s->sinks_h.size())) return -ADF_ERR_CUDA;
@@ -877,7 +1025,12 @@ int adf_world_sum(adf_solver* s, const float* values, double* out_sum, float* ou
   return check_launch();
 }
 
-int64_t adf_kernel_launches(const adf_solver* s) { return s ? s->launches : 0; }
+int64_t adf_kernel_launches(const adf_solver* s) {
+  if (!s) return 0;
+  unsigned long long runs = 0;
+  if (s->body_runs) cudaMemcpy(&runs, s->body_runs, sizeof(runs), cudaMemcpyDeviceToHost);
+  return s->launches + s->body_kernels * (long long)runs;
+}
 
 int adf_profile_enable(adf_solver* s, int enable) {
   if (!s) return fail(ADF_ERR_VALUE, "adf_profile_enable: null solver");

@@ -89,7 +89,7 @@ struct DevP {
   float* kv_s;
   float* kd_s;
   int* nbr;     // [K][n] sorted positions, ascending original id
-  float* nbrF;  // [K][n] gradient factor F(r_ij) of each row entry, written by k_density_alpha
+  int2* nbrjf;  // [K][n] (row entry, bits of its gradient factor F(r_ij)), written by k_density_alpha
   int* cnt;
   float4* slot_g;   // dPsi/dx (3), psi; psi < 0: no slot
   float4* slot_vb;  // wall velocity (3), phi
@@ -752,22 +752,23 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
 // chain per neighbour. Entries past the row's end address the particle itself (a harmless load) and are skipped.
 constexpr int NB = 8;
 
+// Rows are streamed once per kernel (evict-first loads) so that the gathered particle arrays keep L1 and L2.
 __device__ __forceinline__ void load_row_batch(const DevP& P, int p, int c, int k, int (&j)[NB]) {
   const int* row = P.nbr + p;
 #pragma unroll
-  for (int u = 0; u < NB; ++u) j[u] = (k + u < c) ? __ldg(row + (size_t)(k + u) * P.n) : p;
+  for (int u = 0; u < NB; ++u) j[u] = (k + u < c) ? __ldcs(row + (size_t)(k + u) * P.n) : p;
 }
 
-// Row entries with their gradient factor F(r_ij) (the value wf() gives for the pair, stored by k_density_alpha):
-// the later loops read F instead of re-evaluating sqrt, branches and a division per pair; the value is the same.
+// Row entries with their gradient factor F(r_ij) (the value wf() gives for the pair, stored by k_density_alpha) in
+// one 8-byte load: the later loops read F instead of re-evaluating sqrt, branches and a division; the value is the
+// same, so every sum is unchanged.
 __device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, int k, int (&j)[NB], float (&f)[NB]) {
-  const int* row = P.nbr + p;
-  const float* rowf = P.nbrF + p;
+  const int2* row = P.nbrjf + p;
 #pragma unroll
   for (int u = 0; u < NB; ++u) {
-    bool in = k + u < c;
-    j[u] = in ? __ldg(row + (size_t)(k + u) * P.n) : p;
-    f[u] = in ? __ldg(rowf + (size_t)(k + u) * P.n) : 0.0f;
+    int2 e = (k + u < c) ? __ldcs(row + (size_t)(k + u) * P.n) : make_int2(p, 0);
+    j[u] = e.x;
+    f[u] = __int_as_float(e.y);
   }
 }
 
@@ -797,7 +798,7 @@ __global__ void __launch_bounds__(BLOCK) k_density_alpha(DevP P) {
       float r2 = dot_plain(rx, ry, rz, rx, ry, rz);
       float W, F;
       wf(P.kc, r2, W, F);
-      P.nbrF[(size_t)(k + u) * P.n + p] = F;
+      __stcs(P.nbrjf + (size_t)(k + u) * P.n + p, make_int2(j[u], __float_as_int(F)));
       float mj = xj.w;
       rho = ADF_FMA(mj, W, rho);
       float a = mj * inv_r0;
@@ -889,6 +890,12 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   P.lower[p] = lb;
   P.kappa[p] = kap;
   P.kr[p] = kap / vi.w;
+}
+
+// Condition of a solve's WHILE graph node: iterate while any world is unconverged (solve_driver.py:186).
+__global__ void k_set_cond(cudaGraphConditionalHandle h, const int* n_unconv, unsigned long long* body_runs) {
+  cudaGraphSetConditional(h, *n_unconv > 0 ? 1u : 0u);
+  if (body_runs) atomicAdd(body_runs, 1ull);  // iterations run by WHILE bodies (launch accounting)
 }
 
 __global__ void k_begin_solve(DevP P) {

@@ -338,6 +338,10 @@ class SolverDFSPH:
     def kernel_launches(self) -> int:
         return int(self._lib.adf_kernel_launches(self._h))
 
+    def use_graphs(self, enable: bool) -> None:
+        """Replay each step as one CUDA graph (default) or launch its kernels one by one (include/alloy_dfsph.h)."""
+        _lib.check(self._lib.adf_set_graphs(self._h, int(bool(enable))), "use_graphs")
+
     def profile(self, enable: bool) -> None:
         """Time every kernel group with CUDA events on the launch stream (``profile_read``)."""
         _lib.check(self._lib.adf_profile_enable(self._h, int(bool(enable))), "profile")

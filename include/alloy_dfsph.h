@@ -106,6 +106,12 @@ void adf_destroy(adf_solver* solver);
 int adf_step(adf_solver* solver, const float* q_in, const float* qd_in, float* q_out, float* qd_out,
              const float* f_ext, double dt, void* stream);
 
+/* Step execution mode. enable = 1 (default): adf_step replays a CUDA graph of the whole step (built on first use per
+ * state-pointer set and dt; the pressure iterations are WHILE nodes, as wp.capture_while, solve_driver.py:186);
+ * 0: the same kernels launched one by one with the iteration count read back on the host. A step enqueued on a
+ * stream that the caller is capturing always joins that capture with WHILE nodes. */
+int adf_set_graphs(adf_solver* solver, int enable);
+
 /* Replaces SolverDFSPH.density_ratio (solver.py:386-393): density ratio and active mask of every particle of the
  * state (device [n] outputs, 0 for non-liquid particles) from fresh lists and wall slots. */
 int adf_density_ratio(adf_solver* solver, const float* q, const float* qd, float* ratio_out, float* active_out,
