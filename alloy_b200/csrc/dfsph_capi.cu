@@ -166,6 +166,7 @@ void size_grids(adf_solver* s, const float* q_host) {
       for (int a = 0; a < 3; ++a) {
         double margin = 4.0 * cw + 0.1 * (hi[a] - lo[a]);
         dim[a] = (int)std::ceil((hi[a] - lo[a] + 2.0 * margin) / cw) + 1;
+        dim[a] = (dim[a] + 3) / 4 * 4;  // whole 4 x 4 x 4 tiles
         cells *= dim[a];
       }
       if (cells <= 33554432.0) break;
@@ -181,6 +182,9 @@ void size_grids(adf_solver* s, const float* q_host) {
     g.nx = dim[0];
     g.ny = dim[1];
     g.nz = dim[2];
+    g.tnx = dim[0] / 4;
+    g.tny = dim[1] / 4;
+    g.pad0 = g.pad1 = 0;
     g.base = (int)base;
     s->grids[w] = g;
     s->world_cells_h[w] = dim[0] * dim[1] * dim[2];

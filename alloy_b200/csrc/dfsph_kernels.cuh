@@ -23,10 +23,30 @@ constexpr int FLAG_ACTIVE = 1;
 constexpr int FLAG_PROXY = 2;
 constexpr int PROJECT_PASSES = 4;  // integrate.py:50
 
+// A world's cell grid. Cells are numbered tile by tile (4 x 4 x 4 cells per tile, tiles in x-fastest order, cells
+// x-fastest inside a tile), so a run of consecutive sorted particles covers a compact brick of space and its
+// neighbourhood stays small enough for L1. Cells of one tile row with consecutive x have consecutive keys.
 struct WorldGrid {
   float ox, oy, oz, inv_cw;  // origin, 1 / cell width
-  int nx, ny, nz, base;      // cells per axis, first cell of the world in the class-0 key space
+  int nx, ny, nz, base;      // cells per axis (multiples of 4), first cell of the world in the class-0 key space
+  int tnx, tny, pad0, pad1;  // tiles per axis (x, y)
 };
+
+__device__ __forceinline__ int cell_key(const WorldGrid& g, int x, int y, int z) {
+  return g.base + ((((z >> 2) * g.tny + (y >> 2)) * g.tnx + (x >> 2)) << 6) + (((z & 3) << 4) | ((y & 3) << 2) | (x & 3));
+}
+
+// Sorted ranges [b, e) of the cells x = x0..x1 of row (y, z) of key class `cls_off` (0 liquid, total_cells walls):
+// one range per tile the row crosses.
+template <class F>
+__device__ __forceinline__ void for_row_ranges(const int* cell_start, const WorldGrid& g, int cls_off, int y, int z,
+                                               int x0, int x1, F&& f) {
+  for (int x = x0; x <= x1;) {
+    const int xe = min(x1, x | 3);
+    f(cell_start[cls_off + cell_key(g, x, y, z)], cell_start[cls_off + cell_key(g, xe, y, z) + 1]);
+    x = xe + 1;
+  }
+}
 
 struct Emit {
   int world, n_layer, pool_begin, pool_size;
@@ -163,7 +183,7 @@ __global__ void k_classify(DevP P) {
   const WorldGrid g = P.grid[w];
   int cx, cy, cz;
   cell_coords(g, P.q[3 * i], P.q[3 * i + 1], P.q[3 * i + 2], cx, cy, cz);
-  int key = cls * P.total_cells + g.base + (cz * g.ny + cy) * g.nx + cx;
+  int key = cls * P.total_cells + cell_key(g, cx, cy, cz);
   P.key_of[i] = key;
   atomicAdd(&P.counts[key], 1);
 }
@@ -285,159 +305,6 @@ __global__ void k_scatter(DevP P) {
 // ----------------------------------------------------------------------------------------- neighbour rows
 // neighbors.py:160-195: fluid neighbours j != i of the same world with |x_j - x_i|^2 < h^2, ascending original id,
 // the lowest K kept; a world's overflow counter counts particles with more than K.
-__global__ void __launch_bounds__(BLOCK) k_lists(DevP P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P.nfw[0]) return;
-  int w = P.world_s[p];
-  const WorldGrid g = P.grid[w];
-  float4 xi = P.pos[p];
-  int cx, cy, cz;
-  cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
-  unsigned long long buf[MAXCAP];
-  int m = 0, total = 0;
-  const int K = P.K;
-  for (int dz = -1; dz <= 1; ++dz) {
-    int z = cz + dz;
-    if (z < 0 || z >= g.nz) continue;
-    for (int dy = -1; dy <= 1; ++dy) {
-      int y = cy + dy;
-      if (y < 0 || y >= g.ny) continue;
-      int row = g.base + (z * g.ny + y) * g.nx;
-      int x0 = max(cx - 1, 0), x1 = min(cx + 1, g.nx - 1);
-      int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
-      for (int j = b; j < e; ++j) {
-        if (j == p) continue;
-        float4 xj = P.pos[j];
-        float r2 = dot_plain(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z, xj.x - xi.x, xj.y - xi.y, xj.z - xi.z);
-        if (r2 < P.kc.h2) {
-          ++total;
-          unsigned long long key = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
-          if (m == K && key >= buf[K - 1]) continue;
-          int at = (m < K) ? m : K - 1;
-          while (at > 0 && buf[at - 1] > key) {
-            buf[at] = buf[at - 1];
-            --at;
-          }
-          buf[at] = key;
-          if (m < K) ++m;
-        }
-      }
-    }
-  }
-  for (int k = 0; k < m; ++k) P.nbr[(size_t)k * P.n + p] = (int)(unsigned)(buf[k] & 0xffffffffull);
-  P.cnt[p] = m;
-  if (total > K) atomicAdd(&P.overflow[w], 1);
-}
-
-// The same rows built by a warp per 32 consecutive particles (capacity K <= LIST_STAGE): for each particle the
-// warp tests 32 candidates at a time (a cell row's candidates are contiguous in the sorted arrays), compacts the
-// ones within h into a shared-memory buffer, orders them by rank (the count of smaller keys; keys are unique), and
-// stages the row; the 32 staged rows are then written column by column, 128 contiguous bytes per row entry.
-constexpr int LIST_WARPS = 4;    // warps per block
-constexpr int LIST_STAGE = 64;   // largest capacity this kernel stages
-constexpr int LIST_CAND = 128;   // candidates buffered per particle; more take the selection path below
-
-__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-    v = w < v ? w : v;
-  }
-  return v;
-}
-
-__global__ void __launch_bounds__(32 * LIST_WARPS) k_lists_warp(DevP P) {
-  __shared__ unsigned long long cand[LIST_WARPS][LIST_CAND];
-  __shared__ int stage[LIST_WARPS][32][LIST_STAGE + 1];
-  __shared__ int stage_n[LIST_WARPS][32];
-  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
-  const int p0 = (blockIdx.x * LIST_WARPS + wq) * 32;
-  const int nf = P.nfw[0];
-  if (p0 >= nf) return;
-  const int K = P.K;
-  const float h2 = P.kc.h2;
-  unsigned long long* cb = cand[wq];
-  const unsigned lt = (1u << lane) - 1u;
-  const int tend = min(32, nf - p0);
-  for (int t = 0; t < tend; ++t) {
-    const int p = p0 + t;
-    const int w = P.world_s[p];
-    const WorldGrid g = P.grid[w];
-    const float4 xi = P.pos[p];
-    int cx, cy, cz;
-    cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
-    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, g.nx - 1);
-    int T = 0;
-    for (int r = 0; r < 9; ++r) {
-      const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
-      if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
-      const int row = g.base + (z * g.ny + y) * g.nx;
-      const int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
-      for (int base = b; base < e; base += 32) {
-        const int j = base + lane;
-        bool pass = false;
-        if (j < e && j != p) {
-          float4 xj = P.pos[j];
-          float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-          pass = dot_plain(dx, dy, dz, dx, dy, dz) < h2;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, pass);
-        if (pass) {
-          int at = T + __popc(m & lt);
-          if (at < LIST_CAND) cb[at] = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
-        }
-        T += __popc(m);
-      }
-    }
-    __syncwarp();
-    const int cnt = min(T, K);
-    if (T <= LIST_CAND) {
-      for (int c = lane; c < T; c += 32) {  // rank of each key among the T (unique) keys
-        const unsigned long long key = cb[c];
-        int rank = 0;
-        for (int u = 0; u < T; ++u) rank += cb[u] < key;
-        if (rank < K) stage[wq][t][rank] = (int)(unsigned)(key & 0xffffffffull);
-      }
-    } else {
-      // more candidates than the buffer holds (a pile of particles within h): select the K lowest keys one by one
-      unsigned long long last = 0;
-      for (int k = 0; k < cnt; ++k) {
-        unsigned long long best = ~0ull;
-        for (int r = 0; r < 9; ++r) {
-          const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
-          if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
-          const int row = g.base + (z * g.ny + y) * g.nx;
-          const int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
-          for (int j = b + lane; j < e; j += 32) {
-            if (j == p) continue;
-            float4 xj = P.pos[j];
-            float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-            if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
-              unsigned long long key = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
-              if ((k == 0 || key > last) && key < best) best = key;
-            }
-          }
-        }
-        best = warp_min_u64(best);
-        if (lane == 0) stage[wq][t][k] = (int)(unsigned)(best & 0xffffffffull);
-        last = best;
-      }
-    }
-    if (lane == 0) {
-      stage_n[wq][t] = cnt;
-      if (T > K) atomicAdd(&P.overflow[w], 1);
-    }
-    __syncwarp();
-  }
-  // write the staged rows: entry k of 32 consecutive particles is one contiguous 128-byte segment
-  const int myn = lane < tend ? stage_n[wq][lane] : 0;
-  int kmax = myn;
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
-  for (int k = 0; k < kmax; ++k)
-    if (k < myn) P.nbr[(size_t)k * P.n + p0 + lane] = stage[wq][lane][k];
-  if (lane < tend) P.cnt[p0 + lane] = myn;
-}
 
 // The same rows, one thread per particle with its row kept in shared memory as ascending original ids (entry k of
 // thread t at [k][t]: threads inserting at the same k use distinct banks), mapped back to sorted positions through
@@ -461,27 +328,27 @@ __global__ void __launch_bounds__(LS_THREADS) k_lists_smem(DevP P) {
   for (int r = 0; r < 9; ++r) {
     const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
     if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
-    const int row = g.base + (z * g.ny + y) * g.nx;
-    const int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
-    for (int j = b; j < e; ++j) {
-      if (j == p) continue;
-      float4 xj = P.pos[j];
-      float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-      if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
-        ++total;
-        const int id = P.id_of[j];
-        if (m == K && id >= buf[(K - 1) * LS_THREADS]) continue;
-        int at = (m < K) ? m : K - 1;
-        while (at > 0) {
-          int prev = buf[(at - 1) * LS_THREADS];
-          if (prev <= id) break;
-          buf[at * LS_THREADS] = prev;
-          --at;
+    for_row_ranges(P.cell_start, g, 0, y, z, x0, x1, [&](int b, int e) {
+      for (int j = b; j < e; ++j) {
+        if (j == p) continue;
+        float4 xj = P.pos[j];
+        float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+          ++total;
+          const int id = P.id_of[j];
+          if (m == K && id >= buf[(K - 1) * LS_THREADS]) continue;
+          int at = (m < K) ? m : K - 1;
+          while (at > 0) {
+            int prev = buf[(at - 1) * LS_THREADS];
+            if (prev <= id) break;
+            buf[at * LS_THREADS] = prev;
+            --at;
+          }
+          buf[at * LS_THREADS] = id;
+          if (m < K) ++m;
         }
-        buf[at * LS_THREADS] = id;
-        if (m < K) ++m;
       }
-    }
+    });
   }
   for (int k = 0; k < m; ++k) P.nbr[(size_t)k * P.n + p] = P.pos_of[buf[k * LS_THREADS]];
   P.cnt[p] = m;
@@ -489,16 +356,19 @@ __global__ void __launch_bounds__(LS_THREADS) k_lists_smem(DevP P) {
 }
 
 // Rows of 32 consecutive sorted particles built by one warp in lockstep (capacity K <= 64):
-//  1. scan: the union of the 32 particles' 27-cell neighbourhoods is one box of cell rows whose candidates are
-//     contiguous; 32 candidates at a time are staged in shared memory and every lane tests all of them against its
-//     own particle, appending the original id of each one within h to its row (unsorted). A warp whose particles span
-//     a large box (a row wrap, a splash) scans each lane's own 27 cells instead.
+//  1. scan: the union of the 32 particles' 27-cell neighbourhoods is one box of cells; each of its cell rows splits
+//     into at most one contiguous candidate range per 4-cell tile. The ranges are flattened into one candidate
+//     stream (offsets by a warp scan), 32 candidates at a time are staged in shared memory (the next 32 already in
+//     flight in registers) and every lane tests all of them against its own particle as a 32-bit pass mask, then
+//     appends the original ids of the passing ones to its row (unsorted). A warp whose particles span a large box
+//     (a splash, several worlds) scans each lane's own 27 cells instead.
 //  2. order: rows of at most 32 entries are sorted in registers by a fully unrolled bitonic network; longer rows by
 //     insertion in shared memory; a row with more than 64 candidates selects its K lowest ids by repeated scans.
 //  3. write: entry k of the 32 rows is one contiguous 128-byte segment (ids mapped to sorted positions by pos_of).
 constexpr int LU_WARPS = 4;
 constexpr int LU_ROW = 64;         // row buffer per particle (and the largest capacity this kernel builds)
-constexpr int LU_MAX_CELLS = 108;  // largest union box scanned in lockstep
+constexpr int LU_MAX_ROWS = 64;    // cell rows (y, z) of the warp's box scanned in lockstep
+constexpr int LU_MAX_SEGS = 160;   // candidate ranges (row x tile) scanned in lockstep
 
 __device__ __forceinline__ void sort32_registers(unsigned (&key)[32]) {
 #pragma unroll
@@ -528,6 +398,8 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
   __shared__ unsigned rows[LU_WARPS][LU_ROW][32];  // [warp][entry][lane]: lanes of one entry in distinct banks
   __shared__ float4 cpos[LU_WARPS][32];
   __shared__ unsigned cid[LU_WARPS][32];
+  __shared__ int rbeg[LU_WARPS][LU_MAX_SEGS];     // first sorted index of each candidate range
+  __shared__ int roff[LU_WARPS][LU_MAX_SEGS + 1];  // flat offset of each range in the warp's candidate stream
   const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
   const int p0 = (blockIdx.x * LU_WARPS + wq) * 32;
   const int nf = P.nfw[0];
@@ -544,54 +416,150 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
   cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
   const unsigned full = 0xffffffffu;
   const int w_lo = __reduce_min_sync(full, (unsigned)w), w_hi = __reduce_max_sync(full, (unsigned)w);
-  const int xlo = max((int)__reduce_min_sync(full, (unsigned)cx) - 1, 0);
-  const int xhi = min((int)__reduce_max_sync(full, (unsigned)cx) + 1, g.nx - 1);
   const int ylo = max((int)__reduce_min_sync(full, (unsigned)cy) - 1, 0);
   const int yhi = min((int)__reduce_max_sync(full, (unsigned)cy) + 1, g.ny - 1);
   const int zlo = max((int)__reduce_min_sync(full, (unsigned)cz) - 1, 0);
   const int zhi = min((int)__reduce_max_sync(full, (unsigned)cz) + 1, g.nz - 1);
   unsigned* myrow = &rows[wq][0][lane];
   int cnt = 0, total = 0;
-  const bool lockstep = w_lo == w_hi && (xhi - xlo + 1) * (yhi - ylo + 1) * (zhi - zlo + 1) <= LU_MAX_CELLS;
+  const int sy = yhi - ylo + 1, sz = zhi - zlo + 1, nrows = sy * sz;
+  bool lockstep = w_lo == w_hi && nrows <= LU_MAX_ROWS;
+  int T = 0;
   if (lockstep) {
-    for (int z = zlo; z <= zhi; ++z) {
-      for (int y = ylo; y <= yhi; ++y) {
-        const int row = g.base + (z * g.ny + y) * g.nx;
-        const int b = P.cell_start[row + xlo], e = P.cell_start[row + xhi + 1];
-        for (int c0 = b; c0 < e; c0 += 32) {
-          const int nc = min(32, e - c0);
-          if (lane < nc) {
-            cpos[wq][lane] = P.pos[c0 + lane];
-            cid[wq][lane] = (unsigned)P.id_of[c0 + lane];
-          }
-          __syncwarp();
-          for (int t = 0; t < nc; ++t) {
-            const float4 xj = cpos[wq][t];
-            const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-            if (valid && c0 + t != p && dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
-              if (cnt < LU_ROW) myrow[cnt * 32] = cid[wq][t];
-              ++cnt;
-            }
-          }
-          __syncwarp();
+    // rows (y, z) of the box, row-major; row j's x range is the union of [cx - 1, cx + 1] over the lanes whose cell
+    // is within one row of it (empty: x0 > x1). Lane l keeps rows l and l + 32.
+    int ax0 = 1, ax1 = 0, bx0 = 1, bx1 = 0;
+    for (int j = 0; j < nrows; ++j) {
+      const int y = ylo + j % sy, z = zlo + j / sy;
+      const bool near = abs(cy - y) <= 1 && abs(cz - z) <= 1;
+      const unsigned mn = __reduce_min_sync(full, near ? (unsigned)cx : 0xffffffffu);
+      const unsigned mx = __reduce_max_sync(full, near ? (unsigned)(cx + 1) : 0u);
+      if (lane == (j & 31) && mx != 0u) {
+        const int x0 = max((int)mn - 1, 0), x1 = min((int)mx, g.nx - 1);
+        if (j < 32) {
+          ax0 = x0;
+          ax1 = x1;
+        } else {
+          bx0 = x0;
+          bx1 = x1;
         }
       }
+    }
+    // one candidate range per tile a row's x range crosses; exclusive scan of the range counts over rows 0..63
+    const int sa = ax0 <= ax1 ? (ax1 >> 2) - (ax0 >> 2) + 1 : 0;
+    const int sb = bx0 <= bx1 ? (bx1 >> 2) - (bx0 >> 2) + 1 : 0;
+    int ia = sa, ib = sb;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int va = __shfl_up_sync(full, ia, o), vb = __shfl_up_sync(full, ib, o);
+      if (lane >= o) {
+        ia += va;
+        ib += vb;
+      }
+    }
+    const int ta = __shfl_sync(full, ia, 31);
+    const int nseg = ta + __shfl_sync(full, ib, 31);
+    if (nseg > LU_MAX_SEGS) {
+      lockstep = false;
+    } else {
+      // ranges' first sorted index into rbeg; their lengths, prefixed within the row, into roff[r + 1]
+      int na = 0, nb = 0;
+      for (int half = 0; half < 2; ++half) {
+        const int j = lane + 32 * half;
+        const int x0 = half ? bx0 : ax0, x1 = half ? bx1 : ax1;
+        const int r0 = half ? ta + ib - sb : ia - sa;
+        const int y = ylo + j % sy, z = zlo + j / sy;
+        int acc = 0;
+        for (int xs = x0, r = r0; xs <= x1; ++r) {
+          const int xe = min(x1, xs | 3);
+          const int bb = P.cell_start[cell_key(g, xs, y, z)];
+          const int ee = P.cell_start[cell_key(g, xe, y, z) + 1];
+          rbeg[wq][r] = bb;
+          acc += ee - bb;
+          roff[wq][r + 1] = acc;
+          xs = xe + 1;
+        }
+        (half ? nb : na) = acc;
+      }
+      // candidates before each row: scan of the row totals over rows 0..63, then shift each row's ranges by it
+      int ca = na, cb = nb;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int va = __shfl_up_sync(full, ca, o), vb = __shfl_up_sync(full, cb, o);
+        if (lane >= o) {
+          ca += va;
+          cb += vb;
+        }
+      }
+      const int tca = __shfl_sync(full, ca, 31);
+      T = tca + __shfl_sync(full, cb, 31);
+      for (int r = ia - sa; r < ia; ++r) roff[wq][r + 1] += ca - na;
+      for (int r = ta + ib - sb; r < ta + ib; ++r) roff[wq][r + 1] += tca + cb - nb;
+      if (lane == 0) roff[wq][0] = 0;
+      __syncwarp();
+    }
+  }
+  if (lockstep) {
+    const unsigned myid = (unsigned)P.id_of[p];
+    int rr = 0;  // range of this lane's next candidate; candidates lane, lane + 32, ... only move it forward
+    float4 nxt = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    unsigned nid = 0u;
+    auto fetch = [&](int c) {
+      if (c < T) {
+        while (roff[wq][rr + 1] <= c) ++rr;
+        const int j = rbeg[wq][rr] + (c - roff[wq][rr]);
+        nxt = P.pos[j];
+        nid = (unsigned)P.id_of[j];
+      }
+    };
+    fetch(lane);
+    for (int c0 = 0; c0 < T; c0 += 32) {
+      const int nc = min(32, T - c0);
+      cpos[wq][lane] = nxt;
+      cid[wq][lane] = nid;
+      __syncwarp();
+      fetch(c0 + 32 + lane);
+      unsigned hit = 0u;
+      if (nc == 32) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const float4 xj = cpos[wq][t];
+          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+          hit |= (dot_plain(dx, dy, dz, dx, dy, dz) < h2 ? 1u : 0u) << t;
+        }
+      } else {
+        for (int t = 0; t < nc; ++t) {
+          const float4 xj = cpos[wq][t];
+          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+          hit |= (dot_plain(dx, dy, dz, dx, dy, dz) < h2 ? 1u : 0u) << t;
+        }
+      }
+      while (hit) {
+        const int t = __ffs(hit) - 1;
+        hit &= hit - 1u;
+        const unsigned id = cid[wq][t];
+        if (id != myid) {
+          if (cnt < LU_ROW) myrow[cnt * 32] = id;
+          ++cnt;
+        }
+      }
+      __syncwarp();
     }
   } else if (valid) {
     for (int r = 0; r < 9; ++r) {
       const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
       if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
-      const int row = g.base + (z * g.ny + y) * g.nx;
-      const int b = P.cell_start[row + max(cx - 1, 0)], e = P.cell_start[row + min(cx + 1, g.nx - 1) + 1];
-      for (int j = b; j < e; ++j) {
-        if (j == p) continue;
-        const float4 xj = P.pos[j];
-        const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-        if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
-          if (cnt < LU_ROW) myrow[cnt * 32] = (unsigned)P.id_of[j];
-          ++cnt;
+      for_row_ranges(P.cell_start, g, 0, y, z, max(cx - 1, 0), min(cx + 1, g.nx - 1), [&](int b, int e) {
+        for (int j = b; j < e; ++j) {
+          if (j == p) continue;
+          const float4 xj = P.pos[j];
+          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+          if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+            if (cnt < LU_ROW) myrow[cnt * 32] = (unsigned)P.id_of[j];
+            ++cnt;
+          }
         }
-      }
+      });
     }
   }
   total = valid ? cnt : 0;
@@ -624,17 +592,17 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       for (int r = 0; r < 9; ++r) {
         const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
         if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
-        const int row = g.base + (z * g.ny + y) * g.nx;
-        const int b = P.cell_start[row + max(cx - 1, 0)], e = P.cell_start[row + min(cx + 1, g.nx - 1) + 1];
-        for (int j = b; j < e; ++j) {
-          if (j == p) continue;
-          const float4 xj = P.pos[j];
-          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-          if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
-            const unsigned id = (unsigned)P.id_of[j];
-            if ((k == 0 || id > last) && id < best) best = id;
+        for_row_ranges(P.cell_start, g, 0, y, z, max(cx - 1, 0), min(cx + 1, g.nx - 1), [&](int b, int e) {
+          for (int j = b; j < e; ++j) {
+            if (j == p) continue;
+            const float4 xj = P.pos[j];
+            const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+              const unsigned id = (unsigned)P.id_of[j];
+              if ((k == 0 || id > last) && id < best) best = id;
+            }
           }
-        }
+        });
       }
       myrow[k * 32] = best;
       last = best;
@@ -667,6 +635,20 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
   float4 xi = P.pos[p];
   int cx, cy, cz;
   cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
+  {
+    // the 27 cells lie in at most 2 tiles per axis; most liquid particles see no wall particle in any of them
+    const int x0 = max(cx - 1, 0) >> 2, x1 = min(cx + 1, g.nx - 1) >> 2;
+    const int y0 = max(cy - 1, 0) >> 2, y1 = min(cy + 1, g.ny - 1) >> 2;
+    const int z0 = max(cz - 1, 0) >> 2, z1 = min(cz + 1, g.nz - 1) >> 2;
+    int walls = 0;
+    for (int tz = z0; tz <= z1; ++tz)
+      for (int ty = y0; ty <= y1; ++ty)
+        for (int tx = x0; tx <= x1; ++tx) {
+          const int t0 = P.total_cells + g.base + (((tz * g.tny + ty) * g.tnx + tx) << 6);
+          walls |= P.cell_start[t0 + 64] - P.cell_start[t0];
+        }
+    if (walls == 0) return;
+  }
   unsigned long long buf[MAXWALL];
   int m = 0;
   for (int dz = -1; dz <= 1; ++dz) {
@@ -675,30 +657,29 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
     for (int dy = -1; dy <= 1; ++dy) {
       int y = cy + dy;
       if (y < 0 || y >= g.ny) continue;
-      int row = P.total_cells + g.base + (z * g.ny + y) * g.nx;
-      int x0 = max(cx - 1, 0), x1 = min(cx + 1, g.nx - 1);
-      int b = P.cell_start[row + x0], e = P.cell_start[row + x1 + 1];
-      for (int j = b; j < e; ++j) {
-        float4 xj = P.pos[j];
-        float dx = xi.x - xj.x, dy2 = xi.y - xj.y, dz2 = xi.z - xj.z;
-        float W, F;
-        wf(P.kc, dot_plain(dx, dy2, dz2, dx, dy2, dz2), W, F);
-        float wj = xj.w * W;
-        if (wj > 0.0f) {
-          if (m >= MAXWALL) {
-            atomicAdd(&P.wall_overflow[w], 1);
-            continue;
+      for_row_ranges(P.cell_start, g, P.total_cells, y, z, max(cx - 1, 0), min(cx + 1, g.nx - 1), [&](int b, int e) {
+        for (int j = b; j < e; ++j) {
+          float4 xj = P.pos[j];
+          float dx = xi.x - xj.x, dy2 = xi.y - xj.y, dz2 = xi.z - xj.z;
+          float W, F;
+          wf(P.kc, dot_plain(dx, dy2, dz2, dx, dy2, dz2), W, F);
+          float wj = xj.w * W;
+          if (wj > 0.0f) {
+            if (m >= MAXWALL) {
+              atomicAdd(&P.wall_overflow[w], 1);
+              continue;
+            }
+            unsigned long long key = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
+            int at = m;
+            while (at > 0 && buf[at - 1] > key) {
+              buf[at] = buf[at - 1];
+              --at;
+            }
+            buf[at] = key;
+            ++m;
           }
-          unsigned long long key = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
-          int at = m;
-          while (at > 0 && buf[at - 1] > key) {
-            buf[at] = buf[at - 1];
-            --at;
-          }
-          buf[at] = key;
-          ++m;
         }
-      }
+      });
     }
   }
   if (m == 0) return;
