@@ -396,7 +396,9 @@ __device__ __forceinline__ void sort32_registers(unsigned (&key)[32]) {
 
 __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
   __shared__ unsigned rows[LU_WARPS][LU_ROW][32];  // [warp][entry][lane]: lanes of one entry in distinct banks
-  __shared__ float4 cpos[LU_WARPS][32];
+  __shared__ __align__(8) float cxs[LU_WARPS][32];  // staged candidates, one coordinate per array so that two
+  __shared__ __align__(8) float cys[LU_WARPS][32];  // neighbouring candidates are one 8-byte broadcast load
+  __shared__ __align__(8) float czs[LU_WARPS][32];
   __shared__ unsigned cid[LU_WARPS][32];
   __shared__ int rbeg[LU_WARPS][LU_MAX_SEGS];     // first sorted index of each candidate range
   __shared__ int roff[LU_WARPS][LU_MAX_SEGS + 1];  // flat offset of each range in the warp's candidate stream
@@ -513,26 +515,33 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       }
     };
     fetch(lane);
+    const f32x2 xi2 = f2_dup(xi.x), yi2 = f2_dup(xi.y), zi2 = f2_dup(xi.z);
     for (int c0 = 0; c0 < T; c0 += 32) {
       const int nc = min(32, T - c0);
-      cpos[wq][lane] = nxt;
+      cxs[wq][lane] = nxt.x;
+      cys[wq][lane] = nxt.y;
+      czs[wq][lane] = nxt.z;
       cid[wq][lane] = nid;
       __syncwarp();
       fetch(c0 + 32 + lane);
       unsigned hit = 0u;
+      // two candidates per step: the differences in one packed f32x2 subtraction each (exactly rounded per half),
+      // squares and sums in scalar dot_plain. Packed multiplies feeding packed adds are not used: the assembler fuses
+      // a single-use packed product into the add, which changes the rounding of d^2 at the h^2 boundary.
+      auto pair_hits = [&](int t) -> unsigned {
+        const f32x2 dx = f2_sub(f2_load(&cxs[wq][t]), xi2);
+        const f32x2 dy = f2_sub(f2_load(&cys[wq][t]), yi2);
+        const f32x2 dz = f2_sub(f2_load(&czs[wq][t]), zi2);
+        const float ax = f2_lo(dx), ay = f2_lo(dy), az = f2_lo(dz);
+        const float bx = f2_hi(dx), by = f2_hi(dy), bz = f2_hi(dz);
+        return (dot_plain(ax, ay, az, ax, ay, az) < h2 ? 1u : 0u) | (dot_plain(bx, by, bz, bx, by, bz) < h2 ? 2u : 0u);
+      };
       if (nc == 32) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
-          const float4 xj = cpos[wq][t];
-          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-          hit |= (dot_plain(dx, dy, dz, dx, dy, dz) < h2 ? 1u : 0u) << t;
-        }
+        for (int t = 0; t < 32; t += 2) hit |= pair_hits(t) << t;
       } else {
-        for (int t = 0; t < nc; ++t) {
-          const float4 xj = cpos[wq][t];
-          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-          hit |= (dot_plain(dx, dy, dz, dx, dy, dz) < h2 ? 1u : 0u) << t;
-        }
+        for (int t = 0; t < nc; t += 2) hit |= pair_hits(t) << t;
+        hit &= (1u << nc) - 1u;  // nc < 32: drop the stale slot past the last candidate
       }
       while (hit) {
         const int t = __ffs(hit) - 1;
@@ -565,7 +574,9 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
   total = valid ? cnt : 0;
   cnt = min(total, LU_ROW);
   const int cmax = __reduce_max_sync(full, (unsigned)total);
-  if (cmax <= 32) {
+  // run A = entries [0, min(cnt, 32)), run B = entries [32, cnt), each sorted in registers
+  int a_end = min(cnt, 32), b_end = cnt;
+  {
     unsigned key[32];
 #pragma unroll
     for (int k = 0; k < 32; ++k) key[k] = k < cnt ? myrow[k * 32] : 0xffffffffu;
@@ -573,17 +584,17 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
 #pragma unroll
     for (int k = 0; k < 32; ++k)
       if (k < cnt) myrow[k * 32] = key[k];
-  } else if (total <= LU_ROW) {
-    for (int a = 1; a < cnt; ++a) {  // insertion sort of this lane's row
-      const unsigned v = myrow[a * 32];
-      int at = a;
-      while (at > 0 && myrow[(at - 1) * 32] > v) {
-        myrow[at * 32] = myrow[(at - 1) * 32];
-        --at;
-      }
-      myrow[at * 32] = v;
-    }
-  } else {
+  }
+  if (cmax > 32) {
+    unsigned key[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) key[k] = 32 + k < cnt ? myrow[(32 + k) * 32] : 0xffffffffu;
+    sort32_registers(key);
+#pragma unroll
+    for (int k = 0; k < 32; ++k)
+      if (32 + k < cnt) myrow[(32 + k) * 32] = key[k];
+  }
+  if (total > LU_ROW) {
     // more candidates than the row buffer: the K lowest ids by repeated scans of this particle's 27 cells
     unsigned last = 0;
     const int kk = min(total, K);
@@ -607,11 +618,27 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       myrow[k * 32] = best;
       last = best;
     }
+    a_end = kk;
+    b_end = 32;
   }
+  // write the merge of the two runs: entry k of the 32 rows is one contiguous 128-byte segment
   const int m = min(total, K);
   const int mmax = __reduce_max_sync(full, (unsigned)m);
-  for (int k = 0; k < mmax; ++k)
-    if (k < m) P.nbr[(size_t)k * P.n + p] = P.pos_of[myrow[k * 32]];
+  int ia = 0, ib = 32;
+  unsigned va = ia < a_end ? myrow[ia * 32] : 0xffffffffu;
+  unsigned vb = ib < b_end ? myrow[ib * 32] : 0xffffffffu;
+  for (int k = 0; k < mmax; ++k) {
+    const bool take_a = va < vb;
+    const unsigned v = take_a ? va : vb;
+    if (k < m) P.nbr[(size_t)k * P.n + p] = P.pos_of[v];
+    if (take_a) {
+      ++ia;
+      va = ia < a_end ? myrow[ia * 32] : 0xffffffffu;
+    } else {
+      ++ib;
+      vb = ib < b_end ? myrow[ib * 32] : 0xffffffffu;
+    }
+  }
   if (valid) {
     P.cnt[p] = m;
     if (total > K) atomicAdd(&P.overflow[w], 1);
@@ -1294,12 +1321,27 @@ __global__ void k_wall_volume(int n, const int32_t* flags, const float* radius, 
   wall_vol[i] = (flags[i] & FLAG_PROXY) ? (float)(8.0 * (double)r * (double)r * (double)r) : 0.0f;
 }
 
+// Exact int64 sum per world; a warp whose particles all belong to one world adds its shuffle-reduced total with one
+// atomic (integer addition, so the order does not matter).
 __global__ void k_active_mass(DevP P, long long* out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.n) return;
-  int w = P.world[i];
-  if (w < 0 || w >= P.W || !is_fluid_orig(P, i)) return;
-  atomicAdd((unsigned long long*)&out[w], (unsigned long long)to_fixed(P.mass[i]));
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int w = -1;
+  long long v = 0;
+  if (i < P.n) {
+    w = P.world[i];
+    if (w < 0 || w >= P.W || !is_fluid_orig(P, i)) w = -1;
+    else v = to_fixed(P.mass[i]);
+  }
+  const unsigned full = 0xffffffffu;
+  const int w0 = __shfl_sync(full, w, 0);
+  if (__all_sync(full, w == w0)) {
+    if (w0 < 0) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(full, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long*)&out[w0], (unsigned long long)v);
+  } else if (w >= 0) {
+    atomicAdd((unsigned long long*)&out[w], (unsigned long long)v);
+  }
 }
 
 __global__ void k_unsort_n(int n, const int* nfw, const int* id_of, const float* f, int stride, int comp, float* out,

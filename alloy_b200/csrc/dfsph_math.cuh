@@ -12,6 +12,45 @@ namespace adf {
 
 #define ADF_FMA(a, b, c) __fmaf_rn((a), (b), (c))
 
+// Packed pairs of floats for sm_100's two-wide FP32 instructions (add/sub/mul.rn.f32x2): each half is rounded as the
+// scalar instruction would round it. The assembler may still contract a packed multiply whose only use is a packed
+// add into a fused multiply-add (observed on sm_100a even with -fmad=false), so bit-exact code uses the packed
+// subtraction and keeps products and their sums scalar.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_dup(float a) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ f32x2 f2_load(const float* p) {  // p 8-byte aligned: p[0] low half, p[1] high half
+  return *reinterpret_cast<const f32x2*>(p);
+}
+__device__ __forceinline__ float f2_lo(f32x2 a) {
+  float lo;
+  asm("{\n\t.reg .b32 hi;\n\tmov.b64 {%0, hi}, %1;\n\t}" : "=f"(lo) : "l"(a));
+  return lo;
+}
+__device__ __forceinline__ float f2_hi(f32x2 a) {
+  float hi;
+  asm("{\n\t.reg .b32 lo;\n\tmov.b64 {lo, %0}, %1;\n\t}" : "=f"(hi) : "l"(a));
+  return hi;
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+
 struct KC {
   int kind;  // 0 cubic spline, 1 Wendland C2
   float h, inv_h, h2, sigma, sig_h2, m6sig_h, m20sig_h2, r_min;

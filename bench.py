@@ -20,9 +20,9 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
+import re
 import sys
-import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -38,7 +38,7 @@ UNIT = "particle-steps/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", choices=("large_dam_break", "dam_break"), default="large_dam_break")
@@ -70,43 +70,93 @@ def peaks() -> dict:
 
 
 class Clocks:
-    """nvidia-smi samples every 200 ms during the timed region (clocks, throttle reasons)."""
+    """SM clock, power and clock-event reasons sampled through NVML every 5 ms during the timed region (read only;
+    nothing is set). The GPU is found by the UUID CUDA reports, so the sample follows the device the bench runs on
+    whatever CUDA_VISIBLE_DEVICES maps."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    BAD = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown")
 
-    def __init__(self, gpu_index: int):
-        self.idx = gpu_index
-        self.proc = None
-        self.f = None
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.err = None
+        self.thread = None
+        self.stop_flag = threading.Event()
+
+    def _handle(self, nv):
+        import torch
+
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:  # noqa: BLE001 - older drivers or a UUID format NVML does not take
+            return nv.nvmlDeviceGetHandleByIndex(self.device.index or 0)
+
+    def _run(self, nv, h):
+        names = ((nv.nvmlClocksEventReasonHwSlowdown, "hw_slowdown"),
+                 (nv.nvmlClocksEventReasonHwThermalSlowdown, "hw_thermal_slowdown"),
+                 (nv.nvmlClocksEventReasonSwThermalSlowdown, "sw_thermal_slowdown"),
+                 (nv.nvmlClocksEventReasonSwPowerCap, "sw_power_cap"))
+        while True:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                watts = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.rows.append((sm, [n for m, n in names if bits & m], watts))
+            except Exception as e:  # noqa: BLE001
+                self.err = str(e)
+                return
+            if self.stop_flag.wait(0.005):
+                return
 
     def start(self):
         try:
-            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception as e:  # noqa: BLE001
+            self.err = f"NVML unavailable: {e}"
+            return
+        self.thread = threading.Thread(target=self._run, args=(nv, h), daemon=True)
+        self.thread.start()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        self.proc.wait(timeout=10)
-        self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
-        self.f.close()
-        os.unlink(self.f.name)
-        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9 and r[0].strip() == str(self.idx)]
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "no sampler"]}
+        self.stop_flag.set()
+        self.thread.join(timeout=10)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [self.err or "no samples"]}
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted({n for r in self.rows for n in r[1]}), "samples": len(self.rows),
+                "power_w_max": max(r[2] for r in self.rows)}
+
+    @classmethod
+    def rejected(cls, clk: dict) -> bool:
+        """A sample with a hardware or thermal slowdown, or SM clocks far under max with no reason (a clock lock)."""
+        if any(r in clk.get("reasons", []) for r in cls.BAD):
+            return True
+        sm, mx = clk.get("sm_mhz"), clk.get("sm_max_mhz")
+        return bool(sm and mx and sm < 0.6 * mx and not clk.get("reasons"))
+
+
+KERNEL_NAMES = {"k_jacobi": "jacobi", "k_accel": "accel", "k_density_alpha": "density_alpha",
+                "k_solve_init": "solve_init", "k_apply": "apply", "k_xsph": "xsph", "k_lists_union": "lists",
+                "k_wall_slots": "wall_slots", "k_finish": "finish"}
+
+
+def dram_traffic(workload: str) -> dict:
+    """DRAM bytes (read + write) per launch of each kernel from the committed ncu summary of this workload: the
+    table rows `| k_name | launches | read MB | write MB | bytes per launch |`."""
+    f = ROOT / "profiles" / f"dram_traffic_{workload}.md"
+    out = {}
+    if f.exists():
+        for m in re.finditer(r"^\|\s*(k_\w+)\s*\|[^\n]*\|\s*(\d+)\s*\|\s*$", f.read_text(), re.M):
+            if m.group(1) in KERNEL_NAMES:
+                out[KERNEL_NAMES[m.group(1)]] = int(m.group(2))
+    return out
 
 
 def cpu_oracle_run(sc, steps: int, warmup: int, budget_s: float | None):
@@ -171,18 +221,33 @@ def run_b200(args):
     if world > 1:
         dist.barrier()
     launches0 = sol.kernel_launches()
-    clocks = Clocks(local)
-    clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize(dev)
-    e0.record(stream)
-    for _ in range(args.steps):
-        sol.step(a, b, None, None, sc.dt)
-        a, b = b, a
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    clk = clocks.stop()
-    t = e0.elapsed_time(e1) * 1e-3
+
+    def timed():
+        nonlocal a, b
+        clocks = Clocks(dev)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            sol.step(a, b, None, None, sc.dt)
+            a, b = b, a
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        return e0.elapsed_time(e1) * 1e-3, clocks.stop()
+
+    t, clk = timed()
+    bad = torch.tensor([1.0 if Clocks.rejected(clk) else 0.0], device=dev)
+    if world > 1:
+        dist.all_reduce(bad, op=dist.ReduceOp.MAX)
+    if bad.item() > 0.0:  # the timed region saw a slowdown: measure once more and keep that
+        launches0 = sol.kernel_launches()
+        t, clk2 = timed()
+        clk = {**clk2, "remeasured_after": clk}
     launches = sol.kernel_launches() - launches0
     # per-kernel durations: the same number of steps again, each kernel group bracketed by CUDA events on the launch
     # stream (kernels launched one by one; the timed steps above replay one CUDA graph per step)
@@ -237,10 +302,7 @@ def run_b200(args):
     ms, cnt = prof[dom]
     per_launch_s = ms * 1e-3 / max(cnt, 1)
     achieved = alg[dom] * nf / per_launch_s / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get(dom)
+    traffic = dram_traffic(args.workload).get(dom)
     shares = {k: round(v[0] / total_ms, 4) for k, v in prof.items() if total_ms > 0}
     per_kernel = {}
     for k, b_alg in alg.items():
