@@ -178,6 +178,11 @@ class Oracle:
         self.L.orc_get_flags_phase(self.h, _p(fl, C.c_int), ph.ctypes.data)
         return fl, ph
 
+    def active_fluid(self) -> int:
+        """Active liquid particles (ACTIVE flag, phase >= 1): the count the throughput metric sums per step."""
+        fl, ph = self.flags_phase()
+        return int(np.count_nonzero(((fl & 1) != 0) & (ph >= 1)))
+
     def step(self, dt: float):
         self.L.orc_step(self.h, float(dt))
 
