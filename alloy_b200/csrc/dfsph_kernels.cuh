@@ -110,6 +110,7 @@ struct DevP {
   float* kd_s;
   int* nbr;     // [K][n] sorted positions, ascending original id
   int2* nbrjf;  // [K][n] (row entry, bits of its gradient factor F(r_ij)), written by k_density_alpha
+  float* nbrw;  // [K][n] kernel value W(r_ij) of each row entry, written by k_density_alpha, read by k_xsph
   int* cnt;
   float4* slot_g;   // dPsi/dx (3), psi; psi < 0: no slot
   float4* slot_vb;  // wall velocity (3), phi
@@ -782,7 +783,7 @@ __device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, in
 
 // ------------------------------------------------------------------------------------------ density, factor
 // pressure.py:144-193
-__global__ void __launch_bounds__(BLOCK) k_density_alpha(DevP P) {
+__global__ void __launch_bounds__(BLOCK, 3) k_density_alpha(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   float4 xi = P.pos[p];
@@ -807,6 +808,7 @@ __global__ void __launch_bounds__(BLOCK) k_density_alpha(DevP P) {
       float W, F;
       wf(P.kc, r2, W, F);
       __stcs(P.nbrjf + (size_t)(k + u) * P.n + p, make_int2(j[u], __float_as_int(F)));
+      __stcs(P.nbrw + (size_t)(k + u) * P.n + p, W);
       float mj = xj.w;
       rho = ADF_FMA(mj, W, rho);
       float a = mj * inv_r0;
@@ -1108,9 +1110,15 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
 
 // ----------------------------------------------------------------------------------------- non-pressure
 // integrate.py:150-178: gravity, external force, XSPH with Monaghan's symmetric weight m_j / rho_bar_ij.
-__global__ void __launch_bounds__(BLOCK) k_xsph(DevP P) {
+// The output array becomes the velocity array for the rest of the step (the host swaps them), so boundary
+// particles carry their own velocity across: the wall advance in k_finish reads it.
+__global__ void __launch_bounds__(BLOCK, 3) k_xsph(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P.nfw[0]) return;
+  const int nf = P.nfw[0];
+  if (p >= nf) {
+    if (p < nf + P.nfw[1]) P.vel2[p] = P.vel[p];
+    return;
+  }
   const float dt = P.dt;
   float4 vi = P.vel[p];
   int w = P.world_s[p];
@@ -1130,14 +1138,17 @@ __global__ void __launch_bounds__(BLOCK) k_xsph(DevP P) {
     int cn = P.cnt[p];
     for (int k = 0; k < cn; k += NB) {
       int j[NB];
+      float wb[NB];
       load_row_batch(P, p, cn, k, j);
-      float4 xb[NB], vb[NB];
-      float rb[NB];
+#pragma unroll
+      for (int u = 0; u < NB; ++u) wb[u] = (k + u < cn) ? __ldcs(P.nbrw + (size_t)(k + u) * P.n + p) : 0.0f;
+      float4 vb[NB];
+      float rb[NB], mb[NB];
 #pragma unroll
       for (int u = 0; u < NB; ++u) {
-        xb[u] = P.pos[j[u]];
         vb[u] = P.vel[j[u]];
         rb[u] = P.ratio[j[u]];
+        mb[u] = reinterpret_cast<const float*>(P.pos)[4 * (size_t)j[u] + 3];  // mass (pos.w) only
       }
 #pragma unroll
       for (int u = 0; u < NB; ++u) {
@@ -1145,11 +1156,7 @@ __global__ void __launch_bounds__(BLOCK) k_xsph(DevP P) {
         float4 vj = vb[u];
         float rho_bar = 0.5f * (rho_i + rb[u] * vj.w);
         if (rho_bar > 0.0f) {
-          float4 xj = xb[u];
-          float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-          float W, F;
-          wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);
-          float cw = (xj.w / rho_bar) * W;
+          float cw = (mb[u] / rho_bar) * wb[u];  // W(r_ij) as k_density_alpha evaluated it for this entry
           cx = ADF_FMA(cw, vj.x - vi.x, cx);
           cy = ADF_FMA(cw, vj.y - vi.y, cy);
           cz = ADF_FMA(cw, vj.z - vi.z, cz);
