@@ -17,7 +17,10 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_active_mass", "adf_get_warm_starts", "adf_set_warm_starts", "adf_state_arrays", "adf_reset",
            "adf_add_emitter", "adf_set_emitter_pool", "adf_emitter_state", "adf_set_emitter_enabled", "adf_add_sink",
            "adf_neighbor_rows", "adf_debug_field", "adf_world_sum", "adf_kernel_launches", "adf_profile_enable",
-           "adf_profile_read", "adf_list_stats", "adf_world_sum_noalloc", "adf_set_graphs")
+           "adf_profile_read", "adf_list_stats", "adf_world_sum_noalloc", "adf_set_graphs", "adf_mlp_create",
+           "adf_mlp_destroy", "adf_mlp_set_params", "adf_mlp_get_params", "adf_mlp_forward", "adf_mlp_gradient",
+           "adf_mlp_train_step", "adf_mlp_status")
+MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
               "apply", "xsph", "finish", "emit")
 
@@ -91,8 +94,17 @@ def lib() -> C.CDLL:
     L.adf_list_stats.argtypes = [P, vp, vp, vp]
     L.adf_world_sum_noalloc.argtypes = [vp, i, vp, i, vp, vp, vp]
     L.adf_set_graphs.argtypes = [P, i]
+    L.adf_mlp_create.argtypes = [vp, i, C.POINTER(P)]
+    L.adf_mlp_destroy.argtypes = [P]
+    L.adf_mlp_destroy.restype = None
+    L.adf_mlp_set_params.argtypes = [P, vp]
+    L.adf_mlp_get_params.argtypes = [P, vp]
+    L.adf_mlp_forward.argtypes = [P, vp, i, vp, vp]
+    L.adf_mlp_gradient.argtypes = [P, vp, vp, vp, i, vp, vp, vp]
+    L.adf_mlp_train_step.argtypes = [P, vp, vp, vp, i, C.c_float, vp, vp]
+    L.adf_mlp_status.argtypes = [P]
     for name in EXPORTS:
-        if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches"):
+        if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches", "adf_mlp_destroy"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -53,6 +53,7 @@ struct adf_solver {
   std::vector<WorldGrid> grids;
   std::vector<int> world_cells_h;
   int total_cells = 0, n_keys = 0, n_tiles = 0;
+  int max_items = 0;  // grid of the pressure iterations: an upper bound of their work items (k_worklist)
   DevP d{};
   std::vector<void*> owned;
   int* world_cells = nullptr;
@@ -235,19 +236,23 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
 
 void enqueue_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   const int n = s->n;
+  (void)n;
   prof_begin(s, 5, st);
-  LAUNCH(s, k_accel, blocks(n), BLOCK, st, P);
+  LAUNCH(s, k_accel, s->max_items, ITEM, st, P);
   prof_end(s, st);
   prof_begin(s, 6, st);
-  LAUNCH(s, k_jacobi, blocks(n), BLOCK, st, P);
+  LAUNCH(s, k_jacobi, s->max_items, ITEM, st, P);
   prof_end(s, st);
   prof_begin(s, 7, st);
   if (P.n_chunks > 0)
     LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, P.err_orig, P.chunk_begin, P.chunk_end, P.part_sum, P.part_max,
-           P.n_unconv);
+           P.n_unconv, P.chunk_world, (const int*)P.converged);
   else
     cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
-  if (s->W > 0) LAUNCH(s, k_world_check, s->W, 256, st, P, 1, (double*)nullptr, (float*)nullptr);
+  if (s->W > 0) {
+    LAUNCH(s, k_world_check, s->W, 256, st, P, 1, (double*)nullptr, (float*)nullptr);
+    LAUNCH(s, k_worklist, 1, 1024, st, P);
+  }
   prof_end(s, st);
 }
 
@@ -297,7 +302,12 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
   prof_begin(s, 4, st);
   LAUNCH(s, k_solve_init, blocks(n), BLOCK, st, P);
   prof_end(s, st);
-  if (W > 0) LAUNCH(s, k_begin_solve, blocks(W), BLOCK, st, P);
+  if (W > 0) {
+    LAUNCH(s, k_begin_solve, blocks(W), BLOCK, st, P);
+    LAUNCH(s, k_worklist, 1, 1024, st, P);
+  } else {
+    CK(cudaMemsetAsync(P.n_cw, 0, sizeof(int), st));
+  }
   int rc = check_launch();
   if (rc) return rc;
   if (graph) {
@@ -462,20 +472,23 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   d.gravity = m->gravity;
 
   // chunk table of the per-world reductions (reduce.py:167-182)
-  std::vector<int> cb, ce, cs(1, 0);
+  std::vector<int> cb, ce, cs(1, 0), cwld;
   for (int w = 0; w < s->W; ++w) {
     for (int b = s->ws_host[w]; b < s->ws_host[w + 1]; b += 256) {
       cb.push_back(b);
       ce.push_back(std::min(b + 256, s->ws_host[w + 1]));
+      cwld.push_back(w);
     }
     cs.push_back((int)cb.size());
   }
   d.n_chunks = (int)cb.size();
+  // sum over worlds of ceil(liquid_w / 256) <= n / 256 + W, whatever the worlds' sizes
+  s->max_items = (int)std::max<long long>(((long long)s->n + ITEM - 1) / ITEM + s->W, 1);
 
   int rc = 0;
   float* wall_vol = nullptr;
   WorldGrid* grid = nullptr;
-  int *chunk_begin = nullptr, *chunk_end = nullptr, *world_chunk_start = nullptr;
+  int *chunk_begin = nullptr, *chunk_end = nullptr, *world_chunk_start = nullptr, *chunk_world = nullptr;
   rc |= s->alloc(&wall_vol, n);
   rc |= s->alloc(&grid, W);
   rc |= s->alloc(&s->world_cells, W);
@@ -512,6 +525,11 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.err_orig, n);
   rc |= s->alloc(&d.kv, n);
   rc |= s->alloc(&d.kd, n);
+  rc |= s->alloc(&d.wrange, W);
+  rc |= s->alloc(&d.cw, W);
+  rc |= s->alloc(&d.cseg, (size_t)W + 1);
+  rc |= s->alloc(&d.n_cw, 1);
+  rc |= s->alloc(&chunk_world, cb.size());
   rc |= s->alloc(&d.converged, W);
   rc |= s->alloc(&d.iters, W);
   rc |= s->alloc(&d.err_mean, W);
@@ -551,6 +569,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   d.chunk_begin = chunk_begin;
   d.chunk_end = chunk_end;
   d.world_chunk_start = world_chunk_start;
+  d.chunk_world = chunk_world;
   auto fin = [&](int code) {
     if (code != ADF_OK) {
       std::string msg = g_err;
@@ -569,6 +588,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   if (!cb.empty()) {
     CKC(cudaMemcpy(chunk_begin, cb.data(), sizeof(int) * cb.size(), cudaMemcpyHostToDevice));
     CKC(cudaMemcpy(chunk_end, ce.data(), sizeof(int) * ce.size(), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(chunk_world, cwld.data(), sizeof(int) * cwld.size(), cudaMemcpyHostToDevice));
   }
   CKC(cudaMemcpy(world_chunk_start, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice));
   CKC(cudaMemset(d.counts, 0, sizeof(int) * std::max(s->n_keys, 1)));
@@ -1025,7 +1045,7 @@ int adf_world_sum(adf_solver* s, const float* values, double* out_sum, float* ou
   const DevP& P = s->d;
   if (P.n_chunks > 0)
     LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, values, P.chunk_begin, P.chunk_end, P.part_sum, P.part_max,
-           (int*)nullptr);
+           (int*)nullptr, (const int*)nullptr, (const int*)nullptr);
   LAUNCH(s, k_world_check, s->W, 256, st, P, 0, out_sum, out_max);
   return check_launch();
 }

@@ -127,6 +127,10 @@ struct DevP {
   float4* acc;
   float* err_orig;  // original order
   // per world
+  int2* wrange;     // [W] sorted liquid range of each world (k_post_scan)
+  int* cw;          // [W] worlds still iterating, ascending (k_worklist)
+  int* cseg;        // [W + 1] first work item of each listed world; cseg[n_cw] = items
+  int* n_cw;        // [1] listed worlds
   int* converged;
   int* iters;
   float* err_mean;
@@ -143,6 +147,7 @@ struct DevP {
   const int* chunk_begin;
   const int* chunk_end;
   const int* world_chunk_start;
+  const int* chunk_world;
   int n_chunks;
   double* part_sum;
   float* part_max;
@@ -280,7 +285,9 @@ __global__ void k_post_scan(DevP P, const int* world_cells) {
   }
   if (w >= P.W) return;
   int b = P.grid[w].base;
-  P.n_active[w] = (double)(P.cell_start[b + world_cells[w]] - P.cell_start[b]);
+  const int lb = P.cell_start[b], le = P.cell_start[b + world_cells[w]];
+  P.wrange[w] = make_int2(lb, le);
+  P.n_active[w] = (double)(le - lb);
 }
 
 // Place each particle in its cell's range and gather its data into the sorted arrays. The counts go back to zero.
@@ -918,7 +925,76 @@ __global__ void k_begin_solve(DevP P) {
     atomicAdd(P.n_unconv, 1);
   } else {
     P.converged[w] = 1;
+    P.emax[w] = 0.0f;  // no liquid: nothing is iterated or reduced for this world in this solve
   }
+}
+
+// Work items of the pressure iterations: 256-particle segments of the sorted liquid range of every world that is still
+// iterating. One block lists the worlds (ascending) with the running count of their segments; an iteration kernel's
+// block t finds its world by binary search. Converged worlds therefore cost the iteration kernels nothing, which is
+// what keeps a batch of uneven worlds cheap once most of them have converged.
+constexpr int ITEM = 256;
+
+__global__ void __launch_bounds__(1024) k_worklist(DevP P) {
+  __shared__ int smem[32];
+  __shared__ int carry_w, carry_s;
+  if (threadIdx.x == 0) {
+    carry_w = 0;
+    carry_s = 0;
+  }
+  __syncthreads();
+  for (int w0 = 0; w0 < P.W; w0 += blockDim.x) {
+    const int w = w0 + threadIdx.x;
+    int segs = 0;
+    if (w < P.W && !P.converged[w]) {
+      const int2 r = P.wrange[w];
+      segs = (r.y - r.x + ITEM - 1) / ITEM;
+    }
+    const int on = segs > 0 ? 1 : 0;
+    int tw, ts;
+    const int ow = block_exclusive_scan(on, smem, tw);
+    const int os = block_exclusive_scan(segs, smem, ts);
+    const int cw0 = carry_w, cs0 = carry_s;
+    if (on) {
+      P.cw[cw0 + ow] = w;
+      P.cseg[cw0 + ow] = cs0 + os;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      carry_w = cw0 + tw;
+      carry_s = cs0 + ts;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    P.cseg[carry_w] = carry_s;
+    *P.n_cw = carry_w;
+  }
+}
+
+// The sorted range [b, e) of this block's work item; false (for the whole block) past the last item.
+__device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
+  __shared__ int sb, se;
+  if (threadIdx.x == 0) {
+    const int n = *P.n_cw;
+    const int t = blockIdx.x;
+    sb = se = 0;
+    if (n > 0 && t < P.cseg[n]) {
+      int lo = 0, hi = n - 1;  // the last listed world whose first item is <= t
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.cseg[mid] <= t) lo = mid;
+        else hi = mid - 1;
+      }
+      const int2 r = P.wrange[P.cw[lo]];
+      sb = r.x + (t - P.cseg[lo]) * ITEM;
+      se = min(sb + ITEM, r.y);
+    }
+  }
+  __syncthreads();
+  b = sb;
+  e = se;
+  return b < e;
 }
 
 // ------------------------------------------------------------------------------------------ Jacobi sweep
@@ -959,19 +1035,17 @@ __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, 
 }
 
 __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P.nfw[0]) return;
-  if (P.converged[P.world_s[p]]) return;
-  float ax, ay, az;
-  pressure_accel(P, p, P.pos[p], ax, ay, az);
-  P.acc[p] = make_float4(ax, ay, az, 0.0f);
+  int b, e;
+  if (!work_item(P, b, e)) return;
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
+    float ax, ay, az;
+    pressure_accel(P, p, P.pos[p], ax, ay, az);
+    P.acc[p] = make_float4(ax, ay, az, 0.0f);
+  }
 }
 
 // pressure.py:294-352
-__global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P.nfw[0]) return;
-  if (P.converged[P.world_s[p]]) return;
+__device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
   float4 xi = P.pos[p];
   float4 ai = P.acc[p];
   float r0 = P.vel[p].w;
@@ -1021,12 +1095,21 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
   P.err_orig[P.id_of[p]] = e;
 }
 
+__global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
+  int b, e;
+  if (!work_item(P, b, e)) return;
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one(P, p);
+}
+
+// Chunk partials of the per-world sums. With `converged` given, chunks of converged worlds keep their partials (their
+// values no longer change) except chunk 0, whose block also clears the unconverged count.
 __global__ void __launch_bounds__(256) k_chunk_sum(const float* __restrict__ v, const int* chunk_begin,
                                                    const int* chunk_end, double* part_sum, float* part_max,
-                                                   int* n_unconv) {
+                                                   int* n_unconv, const int* chunk_world, const int* converged) {
   __shared__ double smd[8];
   __shared__ float smf[8];
   int c = blockIdx.x;
+  if (converged && c != 0 && converged[chunk_world[c]]) return;
   int i = chunk_begin[c] + threadIdx.x;
   bool in = i < chunk_end[c];
   float x = in ? v[i] : 0.0f;
@@ -1045,6 +1128,7 @@ __global__ void __launch_bounds__(256) k_world_check(DevP P, int check, double* 
   __shared__ double smd[8];
   __shared__ float smf[8];
   int w = blockIdx.x;
+  if (check && P.converged[w]) return;  // its error sums and maximum are those it converged with
   int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
   double a = 0.0;
   float m = -3.4e38f;
@@ -1062,7 +1146,6 @@ __global__ void __launch_bounds__(256) k_world_check(DevP P, int check, double* 
     return;
   }
   P.emax[w] = mx;
-  if (P.converged[w]) return;
   int it = P.iters[w] + 1;
   P.iters[w] = it;
   double na = P.n_active[w];

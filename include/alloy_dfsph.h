@@ -186,6 +186,33 @@ int adf_world_sum(adf_solver* solver, const float* values, double* out_sum, floa
 int adf_world_sum_noalloc(const float* values, int n, const int32_t* world_start, int world_count, double* out_sum,
                           float* out_max, void* stream);
 
+/* ------------------------------------------------------------------------------------------- warm-start network
+ * No counterpart in the reference (its warm start is the previous step's kappa scaled, pressure.py:214-261). A per-
+ * particle network 16 -> 64 -> 64 -> 2 (SiLU; BF16 weights, FP32 accumulation on the tcgen05 tensor cores) that predicts
+ * both pressure solves' warm starts. Parameters are FP32 in one packed host vector of ADF_MLP_PARAMS floats:
+ * W1[64][16], b1[64], W2[64][64], b2[64], W3[2][64], b3[2] (weights [out][in]). Feature rows are [n][16] FP32, target
+ * rows [n][2] FP32, both normalised by the caller (adf_set_warm_model takes the statistics). */
+#define ADF_MLP_PARAMS 5378
+#define ADF_MLP_FEATURES 16
+typedef struct adf_mlp adf_mlp;
+int adf_mlp_create(const float* params, int device, adf_mlp** out);
+void adf_mlp_destroy(adf_mlp* mlp);
+/* Replace the parameters (host vector) and clear the Adam moments. */
+int adf_mlp_set_params(adf_mlp* mlp, const float* params);
+int adf_mlp_get_params(adf_mlp* mlp, float* params);
+/* y[n][2] = network(x[n][16]) on the device (normalised units). */
+int adf_mlp_forward(adf_mlp* mlp, const float* x, int n, float* y, void* stream);
+/* Gradient (host [ADF_MLP_PARAMS], may be NULL) and loss (host [1], may be NULL) of L = sum (y - t)^2 / (2 batch) over
+ * the rows idx[0 .. batch) (device int32) of x and targets t (device); synchronises `stream`. */
+int adf_mlp_gradient(adf_mlp* mlp, const float* x, const float* t, const int32_t* idx, int batch, float* grad,
+                     float* loss, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) at learning rate lr on the same loss; loss (host, may be NULL: no
+ * synchronisation) receives the batch's loss before the step. */
+int adf_mlp_train_step(adf_mlp* mlp, const float* x, const float* t, const int32_t* idx, int batch, float lr,
+                       float* loss, void* stream);
+/* ADF_OK, or ADF_ERR_STATE if a tensor-core wait of this network's kernels ever expired (its results are invalid). */
+int adf_mlp_status(adf_mlp* mlp);
+
 /* Number of kernels this library enqueued since creation (launch accounting for benchmarks). */
 int64_t adf_kernel_launches(const adf_solver* solver);
 
