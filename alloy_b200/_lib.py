@@ -19,10 +19,11 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_neighbor_rows", "adf_debug_field", "adf_world_sum", "adf_kernel_launches", "adf_profile_enable",
            "adf_profile_read", "adf_list_stats", "adf_world_sum_noalloc", "adf_set_graphs", "adf_mlp_create",
            "adf_mlp_destroy", "adf_mlp_set_params", "adf_mlp_get_params", "adf_mlp_forward", "adf_mlp_gradient",
-           "adf_mlp_train_step", "adf_mlp_status")
+           "adf_mlp_train_step", "adf_mlp_status", "adf_set_warm_model", "adf_set_feature_recording",
+           "adf_warm_features", "adf_set_warm_judging")
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
-              "apply", "xsph", "finish", "emit")
+              "apply", "xsph", "finish", "emit", "warm_start")
 
 
 class Params(C.Structure):
@@ -52,7 +53,7 @@ class Report(C.Structure):
     _fields_ = [(name, C.c_void_p) for name in (
         "density_err", "divergence_err", "iters_density", "iters_divergence", "mass_in", "mass_out", "mass_initial",
         "escaped", "neighbor_overflow", "max_speed", "density_err_max", "projected", "nonfinite", "emitter_overflow",
-        "density_tol")]
+        "density_tol", "learned_divergence", "learned_density")]
 
 
 _lib = None
@@ -103,6 +104,10 @@ def lib() -> C.CDLL:
     L.adf_mlp_gradient.argtypes = [P, vp, vp, vp, i, vp, vp, vp]
     L.adf_mlp_train_step.argtypes = [P, vp, vp, vp, i, C.c_float, vp, vp]
     L.adf_mlp_status.argtypes = [P]
+    L.adf_set_warm_model.argtypes = [P, P, vp]
+    L.adf_set_feature_recording.argtypes = [P, i]
+    L.adf_warm_features.argtypes = [P, vp, vp]
+    L.adf_set_warm_judging.argtypes = [P, i]
     for name in EXPORTS:
         if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches", "adf_mlp_destroy"):
             getattr(L, name).restype = C.c_int

@@ -13,8 +13,41 @@
 
 #include "../../include/alloy_dfsph.h"
 #include "dfsph_kernels.cuh"
+#include "dfsph_mlp.cuh"
 
 using namespace adf;
+
+namespace adf {
+// The warm-start network over the liquid particles of a step: raw features from k_solve_init, predictions (kappa dt,
+// kappa dt^2) into pred_kv / pred_kd, all in sorted order.
+struct WarmSrc {
+  const float* feat;
+  float* pred_kv;
+  float* pred_kd;
+  int n;
+  __device__ int rows() const { return n; }
+  __device__ void features(int row, float (&f)[16]) const {
+    const float4* p = reinterpret_cast<const float4*>(feat + (size_t)row * 16);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 v = p[q];
+      f[4 * q] = v.x;
+      f[4 * q + 1] = v.y;
+      f[4 * q + 2] = v.z;
+      f[4 * q + 3] = v.w;
+    }
+  }
+  __device__ void output(int row, float y0, float y1) const {
+    pred_kv[row] = y0;
+    pred_kd[row] = y1;
+  }
+};
+
+__global__ void __launch_bounds__(mlp::TILE) k_mlp_warm(DevP P, mlp::Net net) {
+  WarmSrc s{P.feat, P.pred_kv, P.pred_kd, P.nfw[0]};
+  mlp::forward_rows(net, s);
+}
+}  // namespace adf
 
 namespace {
 thread_local std::string g_err;
@@ -101,6 +134,13 @@ struct adf_solver {
   long long body_kernels = 0;   // kernels of one WHILE-body iteration
   unsigned long long* body_runs = nullptr;  // device: WHILE-body iterations run so far
   cudaStream_t cap_stream = nullptr, body_stream = nullptr;
+  // learned warm start (adf_set_warm_model) and feature recording (adf_set_feature_recording)
+  bool warm_on = false, feat_rec = false, warm_alloc = false, judge = true;
+  __nv_bfloat16 *mw1 = nullptr, *mw2 = nullptr;
+  float *mparams = nullptr, *mnorm = nullptr;
+  int* merr = nullptr;
+  int mlp_grid = 1;
+  long long warm_kernels = 0;  // kernels of the dual first sweep (counted per solve, in graph_kernels)
 
   template <class T> int alloc(T** p, size_t count) {
     int rc = dalloc(p, count);
@@ -256,7 +296,7 @@ void enqueue_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   prof_end(s, st);
 }
 
-int host_iterations(adf_solver* s, DevP& P, cudaStream_t st);
+int host_iterations(adf_solver* s, DevP& P, cudaStream_t st, int done);
 
 // The iteration loop as a WHILE node of the graph being captured on `st` (the body: one iteration plus the
 // condition update). Mirrors wp.capture_while (solve_driver.py:186): no host round trip per iteration.
@@ -293,15 +333,76 @@ int capture_iterations(adf_solver* s, DevP& P, cudaStream_t st) {
   return check_launch();
 }
 
+// Iteration 1 of a solve with the learned start: one sweep from the plain start and one from the learned start, their
+// per-world residual sums, each world's choice (the learned start unless its residual is larger), the chosen state
+// copied into the solve's arrays, then the iteration's stop test as in every other iteration.
+void dual_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
+  DevP L = P;
+  L.kappa = P.kappa2;
+  L.kr = P.kr2;
+  L.acc = P.acc2;
+  L.err_orig = P.err2;
+  const int W = s->W;
+  for (int pass = 0; pass < 2; ++pass) {
+    DevP& Q = pass == 0 ? P : L;
+    prof_begin(s, 5, st);
+    LAUNCH(s, k_accel, s->max_items, ITEM, st, Q);
+    prof_end(s, st);
+    prof_begin(s, 6, st);
+    LAUNCH(s, k_jacobi, s->max_items, ITEM, st, Q);
+    prof_end(s, st);
+    prof_begin(s, 7, st);
+    if (P.n_chunks > 0)
+      LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, (const float*)Q.err_orig, P.chunk_begin, P.chunk_end, P.part_sum,
+             P.part_max, (int*)nullptr, (const int*)nullptr, (const int*)nullptr);
+    LAUNCH(s, k_world_check, W, 256, st, P, 0, pass == 0 ? P.sum_c : P.sum_l, pass == 0 ? P.max_c : P.max_l);
+    prof_end(s, st);
+  }
+  const int n = s->n;
+  LAUNCH(s, k_choose_start, blocks(W), BLOCK, st, P);
+  LAUNCH(s, k_select_start, blocks(n), BLOCK, st, P);
+  prof_begin(s, 7, st);
+  if (P.n_chunks > 0)
+    LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, P.err_orig, P.chunk_begin, P.chunk_end, P.part_sum, P.part_max,
+           P.n_unconv, P.chunk_world, (const int*)P.converged);
+  else
+    cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
+  LAUNCH(s, k_world_check, W, 256, st, P, 1, (double*)nullptr, (float*)nullptr);
+  LAUNCH(s, k_worklist, 1, 1024, st, P);
+  prof_end(s, st);
+}
+
+mlp::Net solver_net(const adf_solver* s) { return mlp::Net{s->mw1, s->mw2, s->mparams, s->mnorm, s->merr}; }
+
 // pressure.py:355-390 + solve_driver.py:121-186 (Jacobi branch) + pressure.py:393-480
 int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool graph) {
   set_solve_params(s, P, mode, dt);
   const int n = s->n, W = s->W;
+  const bool first = mode == 0 || !s->prm.divergence_solve;  // the step's first solve records the features
+  const bool warm = s->warm_on && W > 0;
   CK(cudaMemsetAsync(P.err_orig, 0, sizeof(float) * n, st));
+  if (warm) CK(cudaMemsetAsync(P.err2, 0, sizeof(float) * n, st));
   CK(cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st));
+  P.feat_on = (first && (s->warm_on || s->feat_rec)) ? 1 : 0;
   prof_begin(s, 4, st);
   LAUNCH(s, k_solve_init, blocks(n), BLOCK, st, P);
   prof_end(s, st);
+  P.feat_on = 0;
+  if (warm) {
+    prof_begin(s, 12, st);
+    if (first) {
+      k_mlp_warm<<<s->mlp_grid, mlp::TILE, mlp::FW_SMEM, st>>>(P, solver_net(s));
+      ++s->launches;
+    }
+    DevP Q = P;
+    if (!s->judge) {  // the learned start replaces the plain one outright
+      Q.kappa2 = P.kappa;
+      Q.kr2 = P.kr;
+    }
+    LAUNCH(s, k_learned_start, blocks(n), BLOCK, st, Q);
+    if (!s->judge) LAUNCH(s, k_mark_learned, blocks(W), BLOCK, st, P);
+    prof_end(s, st);
+  }
   if (W > 0) {
     LAUNCH(s, k_begin_solve, blocks(W), BLOCK, st, P);
     LAUNCH(s, k_worklist, 1, 1024, st, P);
@@ -310,11 +411,13 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
   }
   int rc = check_launch();
   if (rc) return rc;
+  const bool dual = warm && s->judge;
+  if (dual) dual_iteration(s, P, st);
   if (graph) {
     rc = capture_iterations(s, P, st);
     if (rc) return rc;
   } else {
-    rc = host_iterations(s, P, st);
+    rc = host_iterations(s, P, st, dual ? 1 : 0);
     if (rc) return rc;
   }
   prof_begin(s, 8, st);
@@ -334,10 +437,10 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
 // The iteration loop driven from the host: iteration k+1 is enqueued before the unconverged count of iteration k
 // is read, so the GPU does not idle on the read; iterations before min_iterations cannot stop a world and are not
 // checked.
-int host_iterations(adf_solver* s, DevP& P, cudaStream_t st) {
+int host_iterations(adf_solver* s, DevP& P, cudaStream_t st, int done) {
   const int limit = s->prm.max_it + 2;  // every world stops at max_iterations
   const bool speculate = !s->prof_on;   // profiled runs time only iterations that do work
-  int enq = 0;
+  int enq = done;                       // iterations already enqueued (the dual first sweep)
   for (; enq < s->prm.min_it - 1; ++enq) enqueue_iteration(s, P, st);  // these cannot stop a world
   auto push = [&]() -> int {
     const int slot = enq & 1;
@@ -452,6 +555,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   d.reach = (float)p.reach;
   d.omega = (float)p.omega;
   d.warm_den = (float)p.warm_den;
+  d.warm_div = (float)p.warm_div;
   d.min_nb = (float)p.min_nb;
   d.xsph_c = (float)p.xsph_c;
   d.v_sep = (float)p.v_sep;
@@ -816,7 +920,110 @@ int adf_get_report(adf_solver* s, adf_report* r, void* stream) {
   rc |= cp(r->nonfinite, s->d.nonfinite, 4 * W);
   rc |= cp(r->emitter_overflow, s->emit_overflow, 4 * W);
   rc |= cp(r->density_tol, s->den_tol, 4 * W);
-  return rc ? ADF_ERR_CUDA : ADF_OK;
+  if (s->warm_alloc) {
+    rc |= cp(r->learned_divergence, s->d.learned, 4 * W);
+    rc |= cp(r->learned_density, s->d.learned + W, 4 * W);
+  } else {
+    if (r->learned_divergence) std::memset(r->learned_divergence, 0, 4 * (size_t)W);
+    if (r->learned_density) std::memset(r->learned_density, 0, 4 * (size_t)W);
+  }
+  if (rc) return ADF_ERR_CUDA;
+  if (s->merr) {
+    int e = 0;
+    CK(cudaMemcpy(&e, s->merr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(ADF_ERR_STATE, "warm-start network: a tensor-core wait expired; the learned starts are invalid");
+  }
+  return ADF_OK;
+}
+
+// Buffers of the learned start and of the feature record, allocated once (outside any step).
+static int ensure_warm(adf_solver* s) {
+  if (s->warm_alloc) return ADF_OK;
+  DevP& d = s->d;
+  const size_t n = (size_t)std::max(s->n, 1), W = (size_t)std::max(s->W, 1);
+  int rc = 0;
+  rc |= s->alloc(&d.feat, 16 * n);
+  rc |= s->alloc(&d.pred_kv, n);
+  rc |= s->alloc(&d.pred_kd, n);
+  rc |= s->alloc(&d.kappa2, n);
+  rc |= s->alloc(&d.kr2, n);
+  rc |= s->alloc(&d.acc2, n);
+  rc |= s->alloc(&d.err2, n);
+  rc |= s->alloc(&d.use_l, W);
+  rc |= s->alloc(&d.learned, 2 * W);
+  rc |= s->alloc(&d.sum_c, W);
+  rc |= s->alloc(&d.sum_l, W);
+  rc |= s->alloc(&d.max_c, W);
+  rc |= s->alloc(&d.max_l, W);
+  rc |= s->alloc(&s->mw1, (size_t)mlp::NH * mlp::NF);
+  rc |= s->alloc(&s->mw2, (size_t)mlp::NH * mlp::NH);
+  rc |= s->alloc(&s->mparams, (size_t)mlp::N_PARAMS);
+  rc |= s->alloc(&s->mnorm, (size_t)36);
+  rc |= s->alloc(&s->merr, (size_t)1);
+  if (rc) return fail(ADF_ERR_CUDA, "learned warm start: " + g_err);
+  CK(cudaMemset(d.feat, 0, sizeof(float) * 16 * n));
+  CK(cudaMemset(d.learned, 0, sizeof(int) * 2 * W));
+  CK(cudaMemset(s->merr, 0, sizeof(int)));
+  CK(cudaFuncSetAttribute(k_mlp_warm, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::FW_SMEM));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+  const long long tiles = ((long long)s->n + mlp::TILE - 1) / mlp::TILE;
+  s->mlp_grid = (int)std::max<long long>(1, std::min<long long>(tiles, 4LL * sms));
+  s->warm_alloc = true;
+  return ADF_OK;
+}
+
+int adf_set_warm_model(adf_solver* s, const adf_mlp* m, const float* norm) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_warm_model: null solver");
+  CK(cudaSetDevice(s->device));
+  ++s->table_version;  // cached step graphs hold the other start
+  if (!m) {
+    s->warm_on = false;
+    return ADF_OK;
+  }
+  if (!norm) return fail(ADF_ERR_VALUE, "adf_set_warm_model: the feature and target statistics are required");
+  if (m->device != s->device) return fail(ADF_ERR_VALUE, "adf_set_warm_model: network and solver on different devices");
+  int rc = ensure_warm(s);
+  if (rc) return rc;
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(s->mw1, m->w1b, sizeof(__nv_bfloat16) * mlp::NH * mlp::NF, cudaMemcpyDeviceToDevice));
+  CK(cudaMemcpy(s->mw2, m->w2b, sizeof(__nv_bfloat16) * mlp::NH * mlp::NH, cudaMemcpyDeviceToDevice));
+  CK(cudaMemcpy(s->mparams, m->w, sizeof(float) * mlp::N_PARAMS, cudaMemcpyDeviceToDevice));
+  CK(cudaMemcpy(s->mnorm, norm, sizeof(float) * 36, cudaMemcpyHostToDevice));
+  s->warm_on = true;
+  return ADF_OK;
+}
+
+int adf_set_warm_judging(adf_solver* s, int enable) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_warm_judging: null solver");
+  if (s->judge != (enable != 0)) ++s->table_version;
+  s->judge = enable != 0;
+  return ADF_OK;
+}
+
+int adf_set_feature_recording(adf_solver* s, int enable) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_feature_recording: null solver");
+  CK(cudaSetDevice(s->device));
+  if (enable) {
+    int rc = ensure_warm(s);
+    if (rc) return rc;
+  }
+  if (s->feat_rec != (enable != 0)) ++s->table_version;
+  s->feat_rec = enable != 0;
+  return ADF_OK;
+}
+
+int adf_warm_features(adf_solver* s, float* out, void* stream) {
+  if (!s || !out) return fail(ADF_ERR_VALUE, "adf_warm_features: null argument");
+  if (!s->warm_alloc || !s->built) return fail(ADF_ERR_STATE, "adf_warm_features: no features recorded yet");
+  if (s->n == 0) return ADF_OK;
+  CK(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(out, 0, sizeof(float) * 16 * (size_t)s->n, st));
+  const DevP& d = s->d;
+  LAUNCH(s, k_unsort_n, blocks(s->n), BLOCK, st, s->n, (const int*)d.nfw, (const int*)d.id_of, (const float*)d.feat,
+         16, 0, out, 16);
+  return check_launch();
 }
 
 int adf_active_mass(adf_solver* s, int64_t* out_host, void* stream) {
@@ -1024,9 +1231,11 @@ int adf_debug_field(adf_solver* s, const char* name, float* out, void* stream) {
       {"src", d.src, 1, 0, 1}, {"kappa", d.kappa, 1, 0, 1}, {"lower", d.lower, 1, 0, 1},
       {"slot_psi", (const float*)d.slot_g, 4, 3, 1}, {"slot_phi", (const float*)d.slot_vb, 4, 3, 1},
       {"acc", (const float*)d.acc, 4, 0, 3}, {"slot_g", (const float*)d.slot_g, 4, 0, 3},
-      {"slot_vb", (const float*)d.slot_vb, 4, 0, 3}, {"slot_n", (const float*)d.slot_n, 4, 0, 3}};
+      {"slot_vb", (const float*)d.slot_vb, 4, 0, 3}, {"slot_n", (const float*)d.slot_n, 4, 0, 3},
+      {"pred_kv", d.pred_kv, 1, 0, 1}, {"pred_kd", d.pred_kd, 1, 0, 1}};
   for (const F& f : fields) {
     if (std::strcmp(f.nm, name) != 0) continue;
+    if (!f.ptr) return fail(ADF_ERR_STATE, std::string("adf_debug_field: ") + name + " is not recorded");
     CK(cudaMemsetAsync(out, 0, sizeof(float) * f.ncomp * (size_t)s->n, st));
     LAUNCH(s, k_unsort_n, blocks(s->n), BLOCK, st, s->n, d.nfw, d.id_of, f.ptr, f.stride, f.comp, out, f.ncomp);
     return check_launch();

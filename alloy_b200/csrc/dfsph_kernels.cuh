@@ -68,7 +68,7 @@ struct DevP {
   int W;
   int K;            // neighbour capacity
   int total_cells;  // cells of all worlds (one class)
-  float dt, n_full, tot_min, wall_offset, wall_amp, taper0, taper1, reach, omega, warm, warm_den, min_nb;
+  float dt, n_full, tot_min, wall_offset, wall_amp, taper0, taper1, reach, omega, warm, warm_den, warm_div, min_nb;
   float xsph_c, v_sep, relief, eps;
   int mode;  // 0 divergence, 1 density
   int two_sided;
@@ -152,6 +152,21 @@ struct DevP {
   double* part_sum;
   float* part_max;
   float* emax;
+  // learned warm start (null when off)
+  float* feat;      // [nf][16] features at the step's first solve (sorted), written by k_solve_init when feat_on
+  int feat_on;
+  float* pred_kv;   // [n] predicted kappa dt (sorted)
+  float* pred_kd;   // [n] predicted kappa dt^2 (sorted)
+  float* kappa2;    // the learned start's kappa, kappa / rho0, acceleration and residual (first sweep)
+  float* kr2;
+  float4* acc2;
+  float* err2;      // original order
+  int* use_l;       // [W] 1: this solve continues from the learned start
+  int* learned;     // [2][W] the last step's choice per solve (divergence, density)
+  double* sum_c;    // [W] first-sweep residual sums and maxima from the plain and the learned start
+  double* sum_l;
+  float* max_c;
+  float* max_l;
 };
 
 __device__ __forceinline__ bool is_fluid_orig(const DevP& P, int i) {
@@ -907,6 +922,69 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   P.lower[p] = lb;
   P.kappa[p] = kap;
   P.kr[p] = kap / vi.w;
+  if (P.feat_on) {  // warm-start network features (their order is documented in solvers/sph/warmstart.py)
+    const float ratio = P.ratio[p], al = P.alpha[p], kvp = P.kv_s[p], kdp = P.kd_s[p];
+    const float drate = dt * rate;
+    const bool on = sg.w >= 0.0f;
+    const float phi = on ? P.slot_vb[p].w : P.kc.h;
+    const float4 f0 = make_float4(ratio - 1.0f, P.neff[p] / P.n_full, drate, kvp);
+    const float4 f1 = make_float4(kdp, al, __fsqrt_rn(dotf(vi.x, vi.y, vi.z, vi.x, vi.y, vi.z)), phi);
+    const float4 f2 = make_float4(on ? sg.w : 0.0f, (ratio + drate) - 1.0f, P.warm_div * minr(kvp, 0.5f),
+                                  P.warm_den * minr(kdp, (float)(2.5e-4)));
+    const float4 f3 = make_float4(vi.z, on ? __fsqrt_rn(dotf(sg.x, sg.y, sg.z, sg.x, sg.y, sg.z)) : 0.0f,
+                                  (ratio - 1.0f) * al, drate * al);
+    float4* fr = reinterpret_cast<float4*>(P.feat + (size_t)p * 16);
+    fr[0] = f0;
+    fr[1] = f1;
+    fr[2] = f2;
+    fr[3] = f3;
+  }
+}
+
+// The learned start of this solve: the plain start (the previous warm start scaled, in dt-free units) plus the
+// network's correction, capped like the stored warm start and kept above the solve's lower bound (a non-finite
+// correction ends at the cap). kv_s / kd_s still hold the previous step's values when each solve starts.
+__global__ void __launch_bounds__(BLOCK) k_learned_start(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const float dt = P.dt;
+  float kap;
+  if (P.mode == 0) {
+    const float base = P.warm_div * minr(P.kv_s[p], 0.5f);
+    kap = maxr(minr(base + P.pred_kv[p], 0.5f) / dt, P.lower[p]);
+  } else {
+    const float base = P.warm_den * minr(P.kd_s[p], (float)(2.5e-4));
+    kap = maxr(minr(base + P.pred_kd[p], (float)(2.5e-4)) / (dt * dt), P.lower[p]);
+  }
+  P.kappa2[p] = kap;
+  P.kr2[p] = kap / P.vel[p].w;
+}
+
+// Without the first-sweep judge every world with liquid takes the learned start.
+__global__ void k_mark_learned(DevP P) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W) return;
+  P.learned[P.mode * P.W + w] = P.n_active[w] > 0.0 ? 1 : 0;
+}
+
+// After the first sweep from both starts: a world keeps the learned start unless its residual sum exceeds the plain
+// start's (equal liquid counts, so the sums order the mean errors).
+__global__ void k_choose_start(DevP P) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W) return;
+  const int use = (P.n_active[w] > 0.0 && !(P.sum_l[w] > P.sum_c[w])) ? 1 : 0;
+  P.use_l[w] = use;
+  P.learned[P.mode * P.W + w] = use;
+}
+
+__global__ void __launch_bounds__(BLOCK) k_select_start(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  if (!P.use_l[P.world_s[p]]) return;
+  P.kappa[p] = P.kappa2[p];
+  P.kr[p] = P.kr2[p];
+  const int i = P.id_of[p];
+  P.err_orig[i] = P.err2[i];
 }
 
 // Condition of a solve's WHILE graph node: iterate while any world is unconverged (solve_driver.py:186).

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "../../include/alloy_dfsph.h"
+#define ADF_MLP_STANDALONE
 #include "dfsph_mlp.cuh"
 
 namespace adf {
@@ -14,21 +15,6 @@ void set_last_error(const std::string& msg);
 }
 
 using namespace adf::mlp;
-
-struct adf_mlp {
-  int device = 0;
-  int sms = 148;
-  float* w = nullptr;  // FP32 master parameters [N_PARAMS]
-  float* m = nullptr;  // Adam first moments
-  float* v = nullptr;  // Adam second moments
-  __nv_bfloat16* w1b = nullptr;
-  __nv_bfloat16* w2b = nullptr;
-  float* part = nullptr;  // [sms][N_PARAMS + 1] per-CTA gradients
-  float* grad = nullptr;  // [N_PARAMS]
-  float* loss = nullptr;  // [1]
-  int* error = nullptr;   // bounded-wait expiry flag
-  int step = 0;
-};
 
 namespace {
 

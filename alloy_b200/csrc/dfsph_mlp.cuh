@@ -131,12 +131,34 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 64 consecutive FP32 columns of this thread's TMEM lane: two 32-column loads in flight, one completion wait.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%64];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%65];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr), "r"(taddr + 32u)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // TMEM address of column `col` in the lanes of this thread's warp (warp w may access lanes 32 (w % 4) ...).
 __device__ __forceinline__ uint32_t tmem_row(uint32_t base, int col) {
   return base + ((uint32_t)((threadIdx.x >> 5) & 3) * 32u << 16) + (uint32_t)col;
 }
 
-__device__ __forceinline__ float sigmoid(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// Logistic sigmoid through the identity s(z) = (1 + tanh(z / 2)) / 2 with the hardware tanh approximation (one MUFU
+// instruction, relative error about 2^-11, below the BF16 rounding the activations get next): the library is built
+// with IEEE division, which would make a 1 / (1 + e^-z) form several times slower.
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sigmoid(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
 
 __device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, float v) {
   *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16_rn(v);
@@ -257,17 +279,16 @@ __device__ void forward_rows(const Net& net, Src& src) {
     phase ^= 1;
     --committed;
     tc_after();
+    {
+      float v[64];
+      tmem_ld64(tmem_row(tm, 0), v);
 #pragma unroll
-    for (int c = 0; c < NH; c += 16) {
-      float v[16];
-      tmem_ld16(tmem_row(tm, c), v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const float z = v[i] + b1[c + i];
+      for (int i = 0; i < 64; ++i) {
+        const float z = v[i] + b1[i];
         v[i] = z * sigmoid(z);
       }
-      st_row8(sH, kmaj(t, c, NH), v);
-      st_row8(sH, kmaj(t, c + 8, NH), v + 8);
+#pragma unroll
+      for (int c = 0; c < NH; c += 8) st_row8(sH, kmaj(t, c, NH), v + c);
     }
     fence_async_smem();
     tc_before();
@@ -285,16 +306,15 @@ __device__ void forward_rows(const Net& net, Src& src) {
     --committed;
     tc_after();
     float y0 = b3[0], y1 = b3[1];
+    {
+      float v[64];
+      tmem_ld64(tmem_row(tm, 64), v);
 #pragma unroll
-    for (int c = 0; c < NH; c += 16) {
-      float v[16];
-      tmem_ld16(tmem_row(tm, 64 + c), v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const float z = v[i] + b2[c + i];
+      for (int i = 0; i < 64; ++i) {
+        const float z = v[i] + b2[i];
         const float h = z * sigmoid(z);
-        y0 = fmaf(w3[c + i], h, y0);
-        y1 = fmaf(w3[64 + c + i], h, y1);
+        y0 = fmaf(w3[i], h, y0);
+        y1 = fmaf(w3[64 + i], h, y1);
       }
     }
     if (valid) src.output(row, fmaf(y0, nrm[34], nrm[32]), fmaf(y1, nrm[35], nrm[33]));
@@ -312,6 +332,9 @@ __device__ void forward_rows(const Net& net, Src& src) {
   tc_after();
   if (t < 32) tmem_dealloc(tm, FW_TMEM_COLS);
 }
+
+// The standalone kernels below are compiled only in the translation unit of the adf_mlp_* entry points.
+#ifdef ADF_MLP_STANDALONE
 
 // Standalone inference: x [n][16] features (FP32), y [n][2] outputs; normalised units when net.norm is null.
 struct RowsSrc {
@@ -645,5 +668,23 @@ __global__ void k_mlp_to_bf16(const float* w, __nv_bfloat16* w1b, __nv_bfloat16*
   if (i < NH * NH) w2b[i] = __float2bfloat16_rn(w[OFF_W2 + i]);
 }
 
+#endif  // ADF_MLP_STANDALONE
+
 }  // namespace mlp
 }  // namespace adf
+
+// The network object behind the adf_mlp_* entry points (shared by the solver, which copies a trained network).
+struct adf_mlp {
+  int device = 0;
+  int sms = 148;
+  float* w = nullptr;  // FP32 master parameters [N_PARAMS]
+  float* m = nullptr;  // Adam first moments
+  float* v = nullptr;  // Adam second moments
+  __nv_bfloat16* w1b = nullptr;
+  __nv_bfloat16* w2b = nullptr;
+  float* part = nullptr;  // [sms][N_PARAMS + 1] per-CTA gradients
+  float* grad = nullptr;  // [N_PARAMS]
+  float* loss = nullptr;  // [1]
+  int* error = nullptr;   // bounded-wait expiry flag
+  int step = 0;
+};

@@ -273,7 +273,8 @@ class SolverDFSPH:
                 "neighbor_overflow": np.zeros(W, np.int32), "max_speed": np.zeros(W, np.float32),
                 "density_err_max": np.zeros(W, np.float32), "projected": np.zeros(W, np.int32),
                 "nonfinite": np.zeros(W, np.int32), "emitter_overflow": np.zeros(W, np.int32),
-                "density_tol": np.zeros(W, np.float32)}
+                "density_tol": np.zeros(W, np.float32), "learned_divergence": np.zeros(W, np.int32),
+                "learned_density": np.zeros(W, np.int32)}
         r = _lib.Report(**{k: v.ctypes.data for k, v in arrs.items()})
         _lib.check(self._lib.adf_get_report(self._h, C.byref(r), self._stream()), "report")
         return {k: v[: self.world_count] for k, v in arrs.items()}
@@ -301,7 +302,8 @@ class SolverDFSPH:
         a = self._world_arrays()
         return {"density_err_max": a["density_err_max"].astype(np.float64), "projected": a["projected"],
                 "nonfinite": a["nonfinite"], "emitter_overflow": a["emitter_overflow"],
-                "swept": np.zeros(self.world_count, np.int32), "cavitating": np.zeros(self.world_count, np.int32)}
+                "swept": np.zeros(self.world_count, np.int32), "cavitating": np.zeros(self.world_count, np.int32),
+                "learned_divergence": a["learned_divergence"], "learned_density": a["learned_density"]}
 
     def mass_ledger(self) -> dict[str, np.ndarray]:
         """Exact int64 fixed-point ledger per world: initial, in, out, active (active + out == initial + in)."""
@@ -327,6 +329,36 @@ class SolverDFSPH:
         _lib.check(self._lib.adf_neighbor_rows(self._h, rows.ctypes.data, cnt.ctypes.data, self._stream()),
                    "neighbor_rows")
         return rows, cnt
+
+    # ------------------------------------------------------------------------------------------ learned start
+    def set_warm_model(self, model) -> None:
+        """Start both pressure solves from the warm-start network ``model`` (a ``warmstart.WarmModel``; None: the
+        reference's plain start). Each world keeps the plain start whenever the learned one's first sweep leaves
+        the larger residual, and every world iterates to the same tolerance (include/alloy_dfsph.h)."""
+        if model is None:
+            _lib.check(self._lib.adf_set_warm_model(self._h, None, None), "set_warm_model")
+            return
+        from .warmstart import Network
+
+        net = Network(model.params, self.device.index or 0)
+        norm = np.ascontiguousarray(model.norm_vector(), np.float32)
+        _lib.check(self._lib.adf_set_warm_model(self._h, net.handle, norm.ctypes.data), "set_warm_model")
+        del net  # the solver holds its own copy of the weights
+
+    def warm_judging(self, enable: bool = True) -> None:
+        """Judge the learned start by one sweep from both starts (default). Off: the learned start is taken outright
+        (a measurement of the network alone; every world still iterates to the same tolerance)."""
+        _lib.check(self._lib.adf_set_warm_judging(self._h, int(bool(enable))), "warm_judging")
+
+    def record_features(self, enable: bool = True) -> None:
+        """Record the network's features of every liquid particle at the start of each step's first solve."""
+        _lib.check(self._lib.adf_set_feature_recording(self._h, int(bool(enable))), "record_features")
+
+    def warm_features(self) -> torch.Tensor:
+        """The last step's recorded features, [n, 16] float32 on the device (zero rows for non-liquid particles)."""
+        out = torch.empty((self.n, 16), dtype=torch.float32, device=self.device)
+        _lib.check(self._lib.adf_warm_features(self._h, out.data_ptr(), self._stream()), "warm_features")
+        return out
 
     def debug_field(self, name: str) -> np.ndarray:
         """A per-particle field of the last step in particle order (parity tests)."""

@@ -26,7 +26,9 @@ Features (raw values, written by the solver at the start of each step's first so
  13 |grad psi|         boundary gradient magnitude
  14 (ratio - 1) alpha
  15 dt rate alpha
-Targets: the converged kappa dt (divergence) and kappa dt^2 (density) the solver stores after the step.
+Targets: corrections to the plain starts, in the dt-free units the solver stores: the converged kappa dt of the
+divergence solve minus feature 10, and the converged kappa dt^2 of the density solve minus feature 11. A network
+that outputs zero therefore reproduces the reference's start exactly.
 """
 
 from __future__ import annotations
@@ -151,6 +153,16 @@ class WarmModel:
         return cls(*(np.asarray(d[k], np.float32) for k in ("params", "f_mean", "f_std", "t_mean", "t_std")))
 
 
+DEFAULT_MODEL = __import__("pathlib").Path(__file__).resolve().parent / "data" / "warm_model.npz"
+
+
+def default_model() -> WarmModel:
+    """The network shipped with the package: trained by ``python -m alloy_b200.solvers.sph.warmstart --out
+    alloy_b200/solvers/sph/data/warm_model.npz`` (2,000,000 pairs from seed-1 runs of the 1,048,576-particle dam break
+    and of the 256 batched worlds, 200 steps each, Adam at 1e-3, batch 65,536, 20 epochs)."""
+    return WarmModel.load(DEFAULT_MODEL)
+
+
 def statistics(x: np.ndarray, floor: float = 1e-12) -> tuple[np.ndarray, np.ndarray]:
     """Per-column mean and deviation (float64 accumulation); constant columns get deviation 1."""
     x = np.asarray(x, np.float64)
@@ -185,3 +197,90 @@ def train(features: np.ndarray, targets: np.ndarray, *, epochs: int = 20, batch:
             log(f"epoch {ep}: loss {np.mean(losses):.4e}")
     net.status()
     return WarmModel(net.params(), f_mean, f_std, t_mean, t_std)
+
+
+def collect_pairs(solver, state_a, state_b, dt: float, steps: int, every: int = 1, per_record: int | None = None,
+                  seed: int = 0):
+    """Run ``steps`` steps of ``solver`` (the plain start unless a model is set) and gather (features, corrections of
+    the converged warm starts to the plain starts) of the liquid particles every ``every`` steps; ``per_record`` rows drawn without replacement per
+    record (all when None). Returns float32 arrays [N][16] and [N][2] and the final (state_a, state_b)."""
+    import torch
+
+    solver.record_features(True)
+    rng = np.random.default_rng(seed)
+    feats, targs = [], []
+    model = solver.model
+    for k in range(steps):
+        live = None
+        if k % every == 0:
+            live = ((model.particle_flags & 1) != 0) & (model.sph.phase >= 1)
+        solver.step(state_a, state_b, None, None, dt)
+        state_a, state_b = state_b, state_a
+        if live is None:
+            continue
+        idx = torch.nonzero(live).squeeze(1)
+        if per_record is not None and idx.numel() > per_record:
+            pick = rng.choice(idx.numel(), per_record, replace=False)
+            idx = idx[torch.from_numpy(np.sort(pick)).to(idx.device)]
+        f = solver.warm_features()[idx]
+        arr = solver.alloy_state_arrays()
+        t = torch.stack([arr["sph.kappa_v"][idx] - f[:, 10], arr["sph.kappa_d"][idx] - f[:, 11]], dim=1)
+        feats.append(f.cpu().numpy())
+        targs.append(t.cpu().numpy())
+    solver.record_features(False)
+    return np.concatenate(feats).astype(np.float32), np.concatenate(targs).astype(np.float32), state_a, state_b
+
+
+def generate_pairs(device=None, pairs: int = 2_000_000, seed: int = 1, steps: int = 200, log=None):
+    """Training pairs from seeded runs of the two plain workloads (half each): the 1,048,576-particle dam break and
+    the 256 batched worlds with spouts, ``steps`` steps each, a record every 4 steps."""
+    import torch
+
+    from .solver import SolverDFSPH, layer_offsets
+    from .testing import batched_worlds, large_dam_break
+
+    dev = device or torch.device("cuda", 0)
+    every = 4
+    per = int(np.ceil(pairs / 2 / (steps // every)))
+    out_f, out_t = [], []
+    for make in (large_dam_break, batched_worlds):
+        sc = make(device=dev, seed=seed)
+        sol = SolverDFSPH(sc.model, sc.config)
+        host = sc.model.host()
+        for e in sc.emitters:
+            i0 = int(host["world_start"][e["world"]])
+            vol = float(host["mass"][i0]) / float(host["rest_density"][i0])
+            offs = layer_offsets(np.asarray(e["half"], np.float64), np.asarray(e["velocity"], np.float64),
+                                 sc.config.spacing)
+            sol.add_emitter(e["world"], e["centre"], e["half"], len(offs) * vol / (10.0 * sc.dt), e["velocity"],
+                            pool=e["pool"])
+        a, b = sc.model.state(), sc.model.state()
+        f, t, _, _ = collect_pairs(sol, a, b, sc.dt, steps, every=every, per_record=per, seed=seed)
+        if log is not None:
+            log(f"{sc.name}: {len(f)} pairs")
+        out_f.append(f)
+        out_t.append(t)
+        del sol
+    return np.concatenate(out_f)[:pairs], np.concatenate(out_t)[:pairs]
+
+
+def main(argv=None) -> None:
+    """python -m alloy_b200.solvers.sph.warmstart --out model.npz: pairs from the plain solver, then training."""
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--pairs", type=int, default=2_000_000)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=1)
+    a = ap.parse_args(argv)
+    f, t = generate_pairs(pairs=a.pairs, seed=a.seed, log=print)
+    m = train(f, t, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, log=print)
+    m.save(a.out)
+    print(f"saved {a.out}: {len(f)} pairs")
+
+
+if __name__ == "__main__":
+    main()

@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--workload", choices=("large_dam_break", "dam_break", "batched_worlds"),
                     default="large_dam_break")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-warm", action="store_true", help="skip the learned warm-start arms")
     return ap.parse_args()
 
 
@@ -246,6 +247,56 @@ def run_reference(args):
         "note": "CPU oracle: a C++/OpenMP restatement of the reference's Warp kernels (warp-lang is not installed)"}))
 
 
+def warm_arm(args, dev, judge: bool, rank: int, world: int) -> dict:
+    """The same workload from its start state with the shipped warm-start network: W warm-up steps, K steps timed
+    with CUDA events (graph replay), then 20 steps read back for iterations and the share of solves that kept the
+    learned start. Particle-steps/s at the same tolerances (every world iterates to the same stop test)."""
+    import torch
+
+    from alloy_b200.solvers.sph import SolverDFSPH
+    from alloy_b200.solvers.sph.warmstart import DEFAULT_MODEL, default_model
+
+    full = make_scene(args.workload, dev)
+    sc = rank_scene(full, args.workload, rank, world, dev)
+    sol = SolverDFSPH(sc.model, sc.config)
+    for w, centre, half, rate, vel, pool, _, _ in spouts(sc):
+        sol.add_emitter(w, centre, half, rate, vel, pool=pool)
+    sol.set_warm_model(default_model())
+    sol.warm_judging(judge)
+    a, b = sc.model.state(), sc.model.state()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        sol.step(a, b, None, None, sc.dt)
+        a, b = b, a
+    torch.cuda.synchronize(dev)
+    nf0 = sol.list_stats()[0]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sol.step(a, b, None, None, sc.dt)
+        a, b = b, a
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    t = e0.elapsed_time(e1) * 1e-3
+    nf1 = sol.list_stats()[0]
+    it_den, it_div, err, kept = [], [], [], []
+    for _ in range(20):
+        sol.step(a, b, None, None, sc.dt)
+        a, b = b, a
+        r = sol.report()
+        d = sol.diagnostics()
+        it_den.append(int(r.iters_density.max()))
+        it_div.append(int(r.iters_divergence.max()))
+        err.append(float(r.density_err.max()))
+        kept.append(0.5 * float(d["learned_density"].mean() + d["learned_divergence"].mean()))
+    ps = 0.5 * (nf0 + nf1) * args.steps
+    return {"value": ps / t, "ms_per_step": 1e3 * t / args.steps, "judge": judge,
+            "model": str(DEFAULT_MODEL.relative_to(ROOT)),
+            "iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean": float(np.mean(it_div)),
+            "density_err_mean_max_over_steps": float(np.max(err)), "learned_start_kept": float(np.mean(kept)),
+            "particle_steps": ps, "seconds": t}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -383,6 +434,22 @@ def run_b200(args):
                              "alg_bytes_per_particle": round(b_alg, 2), "achieved_gbs": round(gbs, 1),
                              "frac": round(gbs / pk["hbm_gbs"], 4)}
 
+    warm = {}
+    if not args.no_warm:
+        del sol
+        for judge in (True, False):
+            r = warm_arm(args, dev, judge, rank, world)
+            tw = torch.tensor([r["seconds"]], dtype=torch.float64, device=dev)
+            pw = torch.tensor([r["particle_steps"]], dtype=torch.float64, device=dev)
+            if world > 1:
+                dist.all_reduce(tw, op=dist.ReduceOp.MAX)
+                dist.all_reduce(pw, op=dist.ReduceOp.SUM)
+            r["value"] = float(pw.item()) / float(tw.item())
+            r["vs_plain"] = r["value"] / value
+            for k in ("particle_steps", "seconds"):
+                r.pop(k)
+            warm["warm_started" if judge else "warm_started_unjudged"] = r
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         csc = make_scene(args.workload, "cpu")
@@ -409,7 +476,7 @@ def run_b200(args):
             "solver_stats": {"iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean":
                              float(np.mean(it_div)), "density_err_mean_max_over_steps": float(np.max(den_err)),
                              "density_err_max_last_step": den_max[-1]},
-            "cpu_baseline": cpu, "clocks": clk}
+            **warm, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

@@ -89,6 +89,8 @@ typedef struct {
   int32_t* nonfinite;
   int32_t* emitter_overflow;
   float* density_tol;
+  int32_t* learned_divergence; /* 1: the last step's divergence solve kept the learned start (adf_set_warm_model) */
+  int32_t* learned_density;    /* the same for the density solve */
 } adf_report;
 
 /* Message of this thread's last failed call ("" if none). */
@@ -163,7 +165,8 @@ int adf_add_sink(adf_solver* solver, int world, const float* xform, const float*
 int adf_neighbor_rows(adf_solver* solver, int32_t* rows, int32_t* count, void* stream);
 
 /* Diagnostics for parity tests: a per-particle float field of the last step in particle order (device [n] or
- * [n][3]): ratio alpha neff reg src kappa lower err slot_psi slot_phi (scalars), acc slot_g slot_vb slot_n (vec3). */
+ * [n][3]): ratio alpha neff reg src kappa lower err slot_psi slot_phi pred_kv pred_kd (scalars; pred_*: the
+ * warm-start network's predictions), acc slot_g slot_vb slot_n (vec3). */
 int adf_debug_field(adf_solver* solver, const char* name, float* out, void* stream);
 
 /* Per-world float64 sums and maxima of a float array in the solver's tree order (reduce.py:185-227); device
@@ -213,15 +216,40 @@ int adf_mlp_train_step(adf_mlp* mlp, const float* x, const float* t, const int32
 /* ADF_OK, or ADF_ERR_STATE if a tensor-core wait of this network's kernels ever expired (its results are invalid). */
 int adf_mlp_status(adf_mlp* mlp);
 
+/* Learned warm start (no counterpart in the reference; its starts are the previous kappa scaled, pressure.py:214-261).
+ * With a network set, each step evaluates it once per liquid particle at the start of its first solve and both
+ * solves begin from its predictions: the first Jacobi sweep runs from the plain and from the learned start, and a
+ * world continues from the learned one unless its residual is larger (then the solve is exactly the plain one).
+ * The network's weights are copied (the adf_mlp may be destroyed afterwards); norm is host [36]: feature mean[16],
+ * 1 / feature deviation[16], target mean[2], target deviation[2]. model = NULL switches the learned start off.
+ * Between steps only; the first call allocates the buffers of the learned start. */
+int adf_set_warm_model(adf_solver* solver, const adf_mlp* model, const float* norm);
+/* The network's two outputs are corrections, in the dt-free units of the stored warm starts (kappa dt and
+ * kappa dt^2), to the plain starts 0.5 min(kappa_v, 0.5) and 0.9 min(kappa_d, 2.5e-4) (warm_div / warm_den); the
+ * learned start is the plain start plus the correction, capped at 0.5 and 2.5e-4 and kept above the solve's lower
+ * bound. */
+
+/* First-sweep judging of the learned start (default 1, as described above). 0 measures the network alone: every world
+ * starts from the learned kappa without the plain start's sweep; every world still iterates to the same tolerance. */
+int adf_set_warm_judging(adf_solver* solver, int enable);
+
+/* Record the network's 16 raw features of every liquid particle at the start of each step's first solve (always on
+ * while a network is set); adf_warm_features copies the last step's record to out (device [n][16], particle order,
+ * zero rows for other particles). Used to build training pairs with the converged warm starts (adf_get_warm_starts
+ * after the step). */
+int adf_set_feature_recording(adf_solver* solver, int enable);
+int adf_warm_features(adf_solver* solver, float* out, void* stream);
+
 /* Number of kernels this library enqueued since creation (launch accounting for benchmarks). */
 int64_t adf_kernel_launches(const adf_solver* solver);
 
 /* Live kernel timing with CUDA events on the launch stream (benchmarks). Kinds, in this order: 0 sort (classify,
  * scan, scatter), 1 neighbour rows, 2 wall slots, 3 density and factor, 4 solve start, 5 pressure acceleration,
  * 6 Jacobi update, 7 per-world reduction and stop test, 8 apply pressure, 9 XSPH, 10 advect/project/write-back,
- * 11 emitters. adf_profile_read synchronises, returns the summed milliseconds and launch counts per kind since the
- * last read (host arrays of ADF_PROF_KINDS) and starts a new window. */
-#define ADF_PROF_KINDS 12
+ * 11 emitters, 12 warm-start network and learned start. adf_profile_read synchronises, returns the summed
+ * milliseconds and launch counts per kind since the last read (host arrays of ADF_PROF_KINDS) and starts a new
+ * window. */
+#define ADF_PROF_KINDS 13
 int adf_profile_enable(adf_solver* solver, int enable);
 int adf_profile_read(adf_solver* solver, double* ms, int64_t* launches);
 

@@ -2,9 +2,9 @@
 """The warm-start network's tensor-core kernels (tcgen05) against a plain PyTorch FP32 reference of the same network.
 
 The kernels round the MMA operands to BF16 (features, hidden activations, weights and, in training, the
-back-propagated dZ) and accumulate in FP32; the reference rounds the same operands at the same places, so forward
-outputs agree to FP32 accumulation-order differences (rtol 1e-3 of the output scale) and gradients to the BF16
-rounding of the back-propagated terms (2e-2 of each block's largest entry)."""
+back-propagated dZ) and accumulate in FP32; the reference rounds the same operands at the same places. The kernels'
+SiLU uses the hardware tanh approximation (relative error about 2^-11), so forward outputs agree to 3e-3 of the
+output scale and gradients to the BF16 rounding of the back-propagated terms (2e-2 of each block's largest entry)."""
 
 from __future__ import annotations
 
@@ -45,7 +45,7 @@ def test_forward_matches_reference(cuda, n):
     ref = ref.detach()
     scale = float(ref.abs().max()) + 1e-6
     assert torch.isfinite(y).all()
-    np.testing.assert_allclose(y.numpy(), ref.numpy(), rtol=0, atol=1e-3 * scale)
+    np.testing.assert_allclose(y.numpy(), ref.numpy(), rtol=0, atol=3e-3 * scale)
 
 
 @pytest.mark.parametrize("batch", [64, 300, 5000])
