@@ -20,7 +20,8 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_profile_read", "adf_list_stats", "adf_world_sum_noalloc", "adf_set_graphs", "adf_mlp_create",
            "adf_mlp_destroy", "adf_mlp_set_params", "adf_mlp_get_params", "adf_mlp_forward", "adf_mlp_gradient",
            "adf_mlp_train_step", "adf_mlp_status", "adf_set_warm_model", "adf_set_feature_recording",
-           "adf_warm_features", "adf_set_warm_judging")
+           "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs")
+TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
               "apply", "xsph", "finish", "emit", "warm_start")
@@ -108,6 +109,8 @@ def lib() -> C.CDLL:
     L.adf_set_feature_recording.argtypes = [P, i]
     L.adf_warm_features.argtypes = [P, vp, vp]
     L.adf_set_warm_judging.argtypes = [P, i]
+    L.adf_set_autotune.argtypes = [P, i]
+    L.adf_tuned_configs.argtypes = [P, vp, vp, vp]
     for name in EXPORTS:
         if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches", "adf_mlp_destroy"):
             getattr(L, name).restype = C.c_int

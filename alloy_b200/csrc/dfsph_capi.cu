@@ -47,6 +47,16 @@ __global__ void __launch_bounds__(mlp::TILE) k_mlp_warm(DevP P, mlp::Net net) {
   WarmSrc s{P.feat, P.pred_kv, P.pred_kd, P.nfw[0]};
   mlp::forward_rows(net, s);
 }
+
+// Kernels the autotuner configures (k_apply runs the acceleration loop and takes TK_ACCEL's choice), and the choices:
+// threads per block and the neighbour gathers each thread keeps in flight (NB).
+enum TuneKernel { TK_DENSITY = 0, TK_SOLVE_INIT, TK_ACCEL, TK_JACOBI, TK_XSPH, TK_COUNT };
+struct TuneCfg {
+  int block = BLOCK;
+  int nb = NB_DEFAULT;
+};
+constexpr int TUNE_BLOCKS[] = {128, 256};
+constexpr int TUNE_NB[] = {4, 8, 16};
 }  // namespace adf
 
 namespace {
@@ -140,7 +150,13 @@ struct adf_solver {
   float *mparams = nullptr, *mnorm = nullptr;
   int* merr = nullptr;
   int mlp_grid = 1;
-  long long warm_kernels = 0;  // kernels of the dual first sweep (counted per solve, in graph_kernels)
+  // autotuner: block size and gathers in flight per neighbour-loop kernel (adf_set_autotune)
+  adf::TuneCfg tune[adf::TK_COUNT];
+  float tune_ms[adf::TK_COUNT] = {};
+  bool tuned[adf::TK_COUNT] = {};
+  bool tune_pending = true, tuning = false;
+  float *snap_kappa = nullptr, *snap_kr = nullptr, *snap_err = nullptr;
+  cudaEvent_t tev[2] = {nullptr, nullptr};
 
   template <class T> int alloc(T** p, size_t count) {
     int rc = dalloc(p, count);
@@ -170,6 +186,84 @@ void prof_end(adf_solver* s, cudaStream_t st) {
   if (s->prof_open < 0) return;
   cudaEventRecord(s->prof_pool[s->prof_open + 1], st);
   s->prof_open = -1;
+}
+
+#define NB_DISPATCH(kern, nb, grid, block, st, ...)                      \
+  do {                                                                   \
+    switch (nb) {                                                        \
+      case 4: kern<4><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;   \
+      case 16: kern<16><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break; \
+      default: kern<8><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;  \
+    }                                                                    \
+  } while (0)
+
+// One launch of a tuned kernel with configuration c (the pressure iterations' grid is the work-item bound, each block
+// covering one 256-particle item whatever its size; the others one particle per thread).
+void launch_tk(adf_solver* s, int id, const TuneCfg& c, cudaStream_t st, const DevP& P) {
+  const int n = s->n;
+  switch (id) {
+    case TK_DENSITY: NB_DISPATCH(k_density_alpha, c.nb, blocks(n, c.block), c.block, st, P); break;
+    case TK_SOLVE_INIT: NB_DISPATCH(k_solve_init, c.nb, blocks(n, c.block), c.block, st, P); break;
+    case TK_ACCEL: NB_DISPATCH(k_accel, c.nb, s->max_items, c.block, st, P); break;
+    case TK_JACOBI: NB_DISPATCH(k_jacobi, c.nb, s->max_items, c.block, st, P); break;
+    default: NB_DISPATCH(k_xsph, c.nb, blocks(n, c.block), c.block, st, P); break;
+  }
+  ++s->launches;
+}
+
+// Autotuning (the first step after adf_set_autotune, outside any capture): every block size x NB candidate of the
+// kernel runs three times on the step's real inputs, timed with CUDA events on the launch stream, and the fastest
+// is kept. The tuned kernels are idempotent on their inputs except the Jacobi update, whose kappa, kappa / rho0 and
+// residual are restored before every trial and after the last, so the tuning step computes exactly an ordinary step.
+void tune_kernel(adf_solver* s, int id, cudaStream_t st, const DevP& P) {
+  if (!s->tuning || s->tuned[id]) return;
+  const bool restore = id == TK_JACOBI;
+  const size_t nb = sizeof(float) * (size_t)s->n;
+  auto copy = [&](bool save) {
+    if (!restore) return;
+    if (save) {
+      cudaMemcpyAsync(s->snap_kappa, P.kappa, nb, cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(s->snap_kr, P.kr, nb, cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(s->snap_err, P.err_orig, nb, cudaMemcpyDeviceToDevice, st);
+    } else {
+      cudaMemcpyAsync(P.kappa, s->snap_kappa, nb, cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(P.kr, s->snap_kr, nb, cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(P.err_orig, s->snap_err, nb, cudaMemcpyDeviceToDevice, st);
+    }
+  };
+  copy(true);
+  float best = 3.0e38f;
+  TuneCfg pick = s->tune[id];
+  for (int block : TUNE_BLOCKS) {
+    for (int nbv : TUNE_NB) {
+      const TuneCfg c{block, nbv};
+      float t = 3.0e38f;
+      for (int r = 0; r < 3; ++r) {
+        copy(false);
+        cudaEventRecord(s->tev[0], st);
+        launch_tk(s, id, c, st, P);
+        cudaEventRecord(s->tev[1], st);
+        float ms = 0.0f;
+        if (cudaEventSynchronize(s->tev[1]) == cudaSuccess && cudaEventElapsedTime(&ms, s->tev[0], s->tev[1]) ==
+            cudaSuccess)
+          t = std::min(t, ms);
+      }
+      if (t < best) {
+        best = t;
+        pick = c;
+      }
+    }
+  }
+  copy(false);
+  s->tune[id] = pick;
+  s->tune_ms[id] = best;
+  s->tuned[id] = true;
+}
+
+// A tuned kernel's launch at its place in the step (tuning it first when this is the tuning step).
+void run_tk(adf_solver* s, int id, cudaStream_t st, const DevP& P) {
+  tune_kernel(s, id, st, P);
+  launch_tk(s, id, s->tune[id], st, P);
 }
 
 int check_launch() {
@@ -268,7 +362,7 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   LAUNCH(s, k_wall_slots, blocks(n), BLOCK, st, P);
   prof_end(s, st);
   prof_begin(s, 3, st);
-  LAUNCH(s, k_density_alpha, blocks(n), BLOCK, st, P);
+  run_tk(s, TK_DENSITY, st, P);
   prof_end(s, st);
   s->built = true;
   return check_launch();
@@ -278,10 +372,10 @@ void enqueue_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   const int n = s->n;
   (void)n;
   prof_begin(s, 5, st);
-  LAUNCH(s, k_accel, s->max_items, ITEM, st, P);
+  run_tk(s, TK_ACCEL, st, P);
   prof_end(s, st);
   prof_begin(s, 6, st);
-  LAUNCH(s, k_jacobi, s->max_items, ITEM, st, P);
+  run_tk(s, TK_JACOBI, st, P);
   prof_end(s, st);
   prof_begin(s, 7, st);
   if (P.n_chunks > 0)
@@ -346,10 +440,10 @@ void dual_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   for (int pass = 0; pass < 2; ++pass) {
     DevP& Q = pass == 0 ? P : L;
     prof_begin(s, 5, st);
-    LAUNCH(s, k_accel, s->max_items, ITEM, st, Q);
+    run_tk(s, TK_ACCEL, st, Q);
     prof_end(s, st);
     prof_begin(s, 6, st);
-    LAUNCH(s, k_jacobi, s->max_items, ITEM, st, Q);
+    run_tk(s, TK_JACOBI, st, Q);
     prof_end(s, st);
     prof_begin(s, 7, st);
     if (P.n_chunks > 0)
@@ -385,7 +479,7 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
   CK(cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st));
   P.feat_on = (first && (s->warm_on || s->feat_rec)) ? 1 : 0;
   prof_begin(s, 4, st);
-  LAUNCH(s, k_solve_init, blocks(n), BLOCK, st, P);
+  run_tk(s, TK_SOLVE_INIT, st, P);
   prof_end(s, st);
   P.feat_on = 0;
   if (warm) {
@@ -421,7 +515,11 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
     if (rc) return rc;
   }
   prof_begin(s, 8, st);
-  LAUNCH(s, k_apply, blocks(n), BLOCK, st, P);
+  {
+    const TuneCfg& c = s->tune[TK_ACCEL];
+    NB_DISPATCH(k_apply, c.nb, blocks(n, c.block), c.block, st, P);
+    ++s->launches;
+  }
   prof_end(s, st);
   if (mode == 0) {
     CK(cudaMemcpyAsync(s->iters_div, P.iters, sizeof(int) * W, cudaMemcpyDeviceToDevice, st));
@@ -727,6 +825,11 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   CKC(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
   CKC(cudaMalloc(&s->body_runs, sizeof(unsigned long long)));
   CKC(cudaMemset(s->body_runs, 0, sizeof(unsigned long long)));
+  CKC(cudaEventCreate(&s->tev[0]));
+  CKC(cudaEventCreate(&s->tev[1]));
+  CKC(cudaMalloc(&s->snap_kappa, sizeof(float) * n));
+  CKC(cudaMalloc(&s->snap_kr, sizeof(float) * n));
+  CKC(cudaMalloc(&s->snap_err, sizeof(float) * n));
   CKC(cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming));
   CKC(cudaDeviceSynchronize());
@@ -753,6 +856,10 @@ void adf_destroy(adf_solver* s) {
   for (auto& e : s->prof_pool) cudaEventDestroy(e);
   for (auto& e : s->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : s->tev)
+    if (e) cudaEventDestroy(e);
+  for (float* p : {s->snap_kappa, s->snap_kr, s->snap_err})
+    if (p) cudaFree(p);
   delete s;
 }
 
@@ -781,7 +888,7 @@ int enqueue_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_
   }
   P.dt = (float)dt;
   prof_begin(s, 9, st);
-  LAUNCH(s, k_xsph, blocks(s->n), BLOCK, st, P);
+  run_tk(s, TK_XSPH, st, P);
   prof_end(s, st);
   std::swap(P.vel, P.vel2);
   rc = solve(s, P, 1, dt, st, graph);
@@ -861,6 +968,14 @@ int adf_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out,
   CK(cudaStreamIsCapturing(st, &cs));
   if (cs == cudaStreamCaptureStatusActive)  // the caller is capturing: the step joins its graph
     return enqueue_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st, true);
+  if (s->tune_pending) {  // the tuning step: kernels one by one, each tuned kernel timed on this step's inputs
+    s->tuning = true;
+    int rc = enqueue_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st, false);
+    s->tuning = false;
+    s->tune_pending = false;
+    ++s->table_version;  // graphs recorded before hold the previous configurations
+    return rc;
+  }
   if (!s->use_graphs || s->prof_on) return enqueue_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st, false);
   return graph_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st);
 }
@@ -991,6 +1106,28 @@ int adf_set_warm_model(adf_solver* s, const adf_mlp* m, const float* norm) {
   CK(cudaMemcpy(s->mparams, m->w, sizeof(float) * mlp::N_PARAMS, cudaMemcpyDeviceToDevice));
   CK(cudaMemcpy(s->mnorm, norm, sizeof(float) * 36, cudaMemcpyHostToDevice));
   s->warm_on = true;
+  return ADF_OK;
+}
+
+int adf_set_autotune(adf_solver* s, int enable) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_autotune: null solver");
+  for (int k = 0; k < TK_COUNT; ++k) {
+    s->tune[k] = TuneCfg{};
+    s->tuned[k] = false;
+    s->tune_ms[k] = 0.0f;
+  }
+  s->tune_pending = enable != 0;
+  ++s->table_version;
+  return ADF_OK;
+}
+
+int adf_tuned_configs(adf_solver* s, int32_t* block, int32_t* nb, float* ms) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_tuned_configs: null solver");
+  for (int k = 0; k < TK_COUNT; ++k) {
+    if (block) block[k] = s->tune[k].block;
+    if (nb) nb[k] = s->tune[k].nb;
+    if (ms) ms[k] = s->tuned[k] ? s->tune_ms[k] : -1.0f;
+  }
   return ADF_OK;
 }
 

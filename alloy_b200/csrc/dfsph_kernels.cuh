@@ -781,9 +781,12 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
 // Neighbour loops read their rows in batches of NB: the NB row entries first, then the NB gathers they address,
 // then the arithmetic in ascending row order, so the loads of a batch overlap instead of forming one dependent
 // chain per neighbour. Entries past the row's end address the particle itself (a harmless load) and are skipped.
-constexpr int NB = 8;
+// NB is a template parameter of every neighbour loop (the gathers a thread keeps in flight); the autotuner picks it
+// per kernel among NB_CHOICES, NB_DEFAULT otherwise.
+constexpr int NB_DEFAULT = 8;
 
 // Rows are streamed once per kernel (evict-first loads) so that the gathered particle arrays keep L1 and L2.
+template <int NB>
 __device__ __forceinline__ void load_row_batch(const DevP& P, int p, int c, int k, int (&j)[NB]) {
   const int* row = P.nbr + p;
 #pragma unroll
@@ -793,6 +796,7 @@ __device__ __forceinline__ void load_row_batch(const DevP& P, int p, int c, int 
 // Row entries with their gradient factor F(r_ij) (the value wf() gives for the pair, stored by k_density_alpha) in
 // one 8-byte load: the later loops read F instead of re-evaluating sqrt, branches and a division; the value is the
 // same, so every sum is unchanged.
+template <int NB>
 __device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, int k, int (&j)[NB], float (&f)[NB]) {
   const int2* row = P.nbrjf + p;
 #pragma unroll
@@ -805,6 +809,7 @@ __device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, in
 
 // ------------------------------------------------------------------------------------------ density, factor
 // pressure.py:144-193
+template <int NB>
 __global__ void __launch_bounds__(BLOCK, 3) k_density_alpha(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
@@ -861,6 +866,7 @@ __global__ void __launch_bounds__(BLOCK, 3) k_density_alpha(DevP P) {
 
 // --------------------------------------------------------------------------------------------- solve start
 // pressure.py:196-261
+template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
@@ -1077,6 +1083,7 @@ __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
 
 // ------------------------------------------------------------------------------------------ Jacobi sweep
 // pressure.py:264-291: a_i = -sum_j m_j (k_i/rho0_i + k_j/rho0_j) grad W_ij - k_i sum_b dPsi_b
+template <int NB>
 __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, float& ax, float& ay, float& az) {
   float ki = P.kr[p];
   ax = ay = az = 0.0f;
@@ -1112,17 +1119,19 @@ __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, 
   }
 }
 
+template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
   int b, e;
   if (!work_item(P, b, e)) return;
   for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
     float ax, ay, az;
-    pressure_accel(P, p, P.pos[p], ax, ay, az);
+    pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
     P.acc[p] = make_float4(ax, ay, az, 0.0f);
   }
 }
 
 // pressure.py:294-352
+template <int NB>
 __device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
   float4 xi = P.pos[p];
   float4 ai = P.acc[p];
@@ -1173,10 +1182,11 @@ __device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
   P.err_orig[P.id_of[p]] = e;
 }
 
+template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
   int b, e;
   if (!work_item(P, b, e)) return;
-  for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one(P, p);
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one<NB>(P, p);
 }
 
 // Chunk partials of the per-world sums. With `converged` given, chunks of converged worlds keep their partials (their
@@ -1236,6 +1246,7 @@ __global__ void __launch_bounds__(256) k_world_check(DevP P, int check, double* 
 // ---------------------------------------------------------------------------------------- apply pressure
 // pressure.py:393-414 (lone particles: a push limited like a rigid contact's depenetration) and 461-480
 // (v += dt a, warm start stored dt-free). A lone particle has no neighbours, so no other particle reads its kappa.
+template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
@@ -1262,7 +1273,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
     }
   }
   float ax, ay, az;
-  pressure_accel(P, p, P.pos[p], ax, ay, az);
+  pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
   P.acc[p] = make_float4(ax, ay, az, 0.0f);
   P.vel[p] = make_float4(ADF_FMA(dt, ax, vi.x), ADF_FMA(dt, ay, vi.y), ADF_FMA(dt, az, vi.z), vi.w);
   if (P.mode == 0) P.kv_s[p] = kap * dt;
@@ -1273,6 +1284,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
 // integrate.py:150-178: gravity, external force, XSPH with Monaghan's symmetric weight m_j / rho_bar_ij.
 // The output array becomes the velocity array for the rest of the step (the host swaps them), so boundary
 // particles carry their own velocity across: the wall advance in k_finish reads it.
+template <int NB>
 __global__ void __launch_bounds__(BLOCK, 3) k_xsph(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = P.nfw[0];

@@ -345,6 +345,19 @@ class SolverDFSPH:
         _lib.check(self._lib.adf_set_warm_model(self._h, net.handle, norm.ctypes.data), "set_warm_model")
         del net  # the solver holds its own copy of the weights
 
+    def autotune(self, enable: bool = True) -> None:
+        """Tune block size and gathers in flight of the neighbour-loop kernels at the next step (on by default;
+        include/alloy_dfsph.h adf_set_autotune). Off: the default configuration."""
+        _lib.check(self._lib.adf_set_autotune(self._h, int(bool(enable))), "autotune")
+
+    def tuned_configs(self) -> dict[str, dict]:
+        """{kernel: {"block", "nb", "ms"}} of the configuration in use (ms < 0: not tuned)."""
+        k = len(_lib.TUNE_KERNELS)
+        blk, nb, ms = np.zeros(k, np.int32), np.zeros(k, np.int32), np.zeros(k, np.float32)
+        _lib.check(self._lib.adf_tuned_configs(self._h, blk.ctypes.data, nb.ctypes.data, ms.ctypes.data), "tuned")
+        return {name: {"block": int(blk[i]), "nb": int(nb[i]), "ms": float(ms[i])}
+                for i, name in enumerate(_lib.TUNE_KERNELS)}
+
     def warm_judging(self, enable: bool = True) -> None:
         """Judge the learned start by one sweep from both starts (default). Off: the learned start is taken outright
         (a measurement of the network alone; every world still iterates to the same tolerance)."""

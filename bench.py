@@ -412,6 +412,7 @@ def run_b200(args):
 
     nf, entries = sol.list_stats()
     nbar = entries / max(nf, 1)
+    tuned = sol.tuned_configs()  # chosen in the first warm-up step
     pk = peaks()
     # algorithmic bytes per liquid particle and launch (element sizes of the reference, 2-byte list entries)
     alg = {"jacobi": 72.0 + 2.0 * nbar, "accel": 44.0 + 2.0 * nbar, "density_alpha": 52.0 + 2.0 * nbar,
@@ -476,7 +477,7 @@ def run_b200(args):
             "solver_stats": {"iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean":
                              float(np.mean(it_div)), "density_err_mean_max_over_steps": float(np.max(den_err)),
                              "density_err_max_last_step": den_max[-1]},
-            **warm, "cpu_baseline": cpu, "clocks": clk}
+            **warm, "autotuned": tuned, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

@@ -114,6 +114,18 @@ int adf_step(adf_solver* solver, const float* q_in, const float* qd_in, float* q
  * stream that the caller is capturing always joins that capture with WHILE nodes. */
 int adf_set_graphs(adf_solver* solver, int enable);
 
+/* Autotuner (no counterpart in the reference; Warp picks its own launch shapes). enable = 1 (the default at creation):
+ * the next adf_step on a stream that is not capturing is a tuning step: it launches its kernels one by one and, the
+ * first time each neighbour-loop kernel (density and factor, solve start, pressure acceleration and its application,
+ * Jacobi update, XSPH) runs, times every candidate of threads per block {128, 256} x neighbour gathers in flight
+ * {4, 8, 16} three times on that step's inputs and keeps the fastest; it synchronises the stream while it does and
+ * its results equal an ordinary step's bit for bit. 0: the default configuration (256 threads, 8 gathers). */
+#define ADF_TUNE_KERNELS 5 /* density and factor, solve start, acceleration (and apply), Jacobi, XSPH */
+int adf_set_autotune(adf_solver* solver, int enable);
+/* The configuration in use per tuned kernel (host [ADF_TUNE_KERNELS] each, any may be NULL): threads per block,
+ * gathers in flight, and the winning trial's milliseconds (-1 if not tuned). */
+int adf_tuned_configs(adf_solver* solver, int32_t* block, int32_t* nb, float* ms);
+
 /* Replaces SolverDFSPH.density_ratio (solver.py:386-393): density ratio and active mask of every particle of the
  * state (device [n] outputs, 0 for non-liquid particles) from fresh lists and wall slots. */
 int adf_density_ratio(adf_solver* solver, const float* q, const float* qd, float* ratio_out, float* active_out,
