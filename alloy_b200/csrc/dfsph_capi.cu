@@ -1234,16 +1234,21 @@ int adf_reset(adf_solver* s, const uint8_t* world_mask, const int32_t* flags0, c
   return check_launch();
 }
 
-int adf_add_emitter(adf_solver* s, int world, const float* xform, const float* offsets, int n_off,
-                    const float* velocity, float interval, const int32_t* pool, int pool_size) {
-  if (!s || !xform || !velocity || (n_off > 0 && !offsets) || (pool_size > 0 && !pool))
-    return -fail(ADF_ERR_VALUE, "adf_add_emitter: null argument");
-  if (world < 0 || world >= s->W) return -fail(ADF_ERR_VALUE, "add_emitter: world " + std::to_string(world) +
-                                                                 " out of range");
-  if (!(interval > 0.0f)) return -fail(ADF_ERR_VALUE, "add_emitter: interval must be > 0");
+static int check_emitter(const adf_solver* s, int world, const float* xform, const float* offsets, int n_off,
+                         const float* velocity, float interval, const int32_t* pool, int pool_size) {
+  if (!xform || !velocity || (n_off > 0 && !offsets) || (pool_size > 0 && !pool) || n_off < 0 || pool_size < 0)
+    return fail(ADF_ERR_VALUE, "adf_add_emitter: null argument or negative size");
+  if (world < 0 || world >= s->W) return fail(ADF_ERR_VALUE, "add_emitter: world " + std::to_string(world) +
+                                                             " out of range");
+  if (!(interval > 0.0f)) return fail(ADF_ERR_VALUE, "add_emitter: interval must be > 0");
   for (int k = 0; k < pool_size; ++k)
     if (pool[k] < s->ws_host[world] || pool[k] >= s->ws_host[world + 1])
-      return -fail(ADF_ERR_VALUE, "add_emitter: pool particle outside the emitter's world");
+      return fail(ADF_ERR_VALUE, "add_emitter: pool particle outside the emitter's world");
+  return ADF_OK;
+}
+
+static int append_emitter(adf_solver* s, int world, const float* xform, const float* offsets, int n_off,
+                          const float* velocity, float interval, const int32_t* pool, int pool_size) {
   Emit e{};
   e.world = world;
   e.n_layer = n_off;
@@ -1261,10 +1266,46 @@ int adf_add_emitter(adf_solver* s, int world, const float* xform, const float* o
     for (int a = 0; a < 3; ++a) s->off_local_h.push_back(offsets[3 * c + a]);
   }
   s->pool_h.insert(s->pool_h.end(), pool, pool + pool_size);
+  return idx;
+}
+
+int adf_add_emitter(adf_solver* s, int world, const float* xform, const float* offsets, int n_off,
+                    const float* velocity, float interval, const int32_t* pool, int pool_size) {
+  if (!s) return -fail(ADF_ERR_VALUE, "adf_add_emitter: null solver");
+  int rc = check_emitter(s, world, xform, offsets, n_off, velocity, interval, pool, pool_size);
+  if (rc) return -rc;
+  const int idx = append_emitter(s, world, xform, offsets, n_off, velocity, interval, pool, pool_size);
   ++s->table_version;
-  int rc = upload_emitters(s, idx);
+  rc = upload_emitters(s, idx);
   if (rc) return -rc;
   return idx;
+}
+
+int adf_add_emitters(adf_solver* s, int count, const int32_t* world, const float* xform, const int32_t* n_off,
+                     const float* offsets, const float* velocity, const float* interval, const int32_t* pool_size,
+                     const int32_t* pool) {
+  if (!s || count < 0 || (count > 0 && (!world || !xform || !n_off || !velocity || !interval || !pool_size)))
+    return -fail(ADF_ERR_VALUE, "adf_add_emitters: null argument");
+  size_t oo = 0, po = 0;
+  for (int k = 0; k < count; ++k) {  // every emitter is checked before any is added
+    int rc = check_emitter(s, world[k], xform + 7 * (size_t)k, offsets ? offsets + 3 * oo : nullptr, n_off[k],
+                           velocity + 3 * (size_t)k, interval[k], pool ? pool + po : nullptr, pool_size[k]);
+    if (rc) return -fail(rc, "add_emitters[" + std::to_string(k) + "]: " + g_err);
+    oo += (size_t)std::max(n_off[k], 0);
+    po += (size_t)std::max(pool_size[k], 0);
+  }
+  const int first = (int)s->em_h.size();
+  oo = po = 0;
+  for (int k = 0; k < count; ++k) {
+    append_emitter(s, world[k], xform + 7 * (size_t)k, offsets + 3 * oo, n_off[k], velocity + 3 * (size_t)k,
+                   interval[k], pool + po, pool_size[k]);
+    oo += (size_t)n_off[k];
+    po += (size_t)pool_size[k];
+  }
+  ++s->table_version;
+  int rc = upload_emitters(s, first);
+  if (rc) return -rc;
+  return first;
 }
 
 int adf_state_arrays(adf_solver* s, float** kv, float** kd) {

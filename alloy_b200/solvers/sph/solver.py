@@ -473,36 +473,71 @@ class SolverDFSPH:
     def add_emitter(self, world: int, region, half_extents, rate: float, velocity, pool=None) -> int:
         """Emit liquid from a box region at ``rate`` [m^3/s] with ``velocity`` [m/s] by activating spares
         (runtime.py:498-525)."""
-        if not 0 <= world < self.world_count:
-            raise ValueError(f"add_emitter: world {world} out of range")
-        if rate <= 0.0:
-            raise ValueError("add_emitter: rate must be > 0 [m^3/s]")
+        return self.add_emitters([(world, region, half_extents, rate, velocity, pool)])[0]
+
+    def add_emitters(self, specs) -> list[int]:
+        """Several emitters at once, each ``(world, region, half_extents, rate, velocity, pool)`` as in
+        ``add_emitter``: the host arrays are read once and the library uploads its emitter tables once."""
         cfg = self.config
-        X = _xform7(region)
-        v_local = quat_rotate_inv(X[3:], np.asarray(velocity, np.float64))
-        offs = layer_offsets(np.asarray(half_extents, dtype=np.float64), v_local, cfg.spacing)
-        i0 = self._first_sph(world)
-        rho0 = float(_host(self.model.sph.rest_density)[i0])
-        mass = float(_host(self.model.particle_mass)[i0])
-        interval = len(offs) * (mass / rho0) / rate
-        area = len(offs) * cfg.spacing * cfg.spacing
-        speed = float(np.linalg.norm(v_local))
-        if speed > 0.0 and not 0.8 <= rate / (area * speed) <= 1.25:
-            log.warning("SPH emitter rate %.3g m^3/s vs area*|v| %.3g m^3/s: layers will over/under-pack", rate,
-                        area * speed)
-        own = pool is not None
-        pool_ids = (np.intersect1d(np.asarray(pool), self._spares(world)).astype(np.int32) if own
-                    else np.zeros(0, np.int32))
-        e = self._lib.adf_add_emitter(self._h, int(world), X.ctypes.data, offs.ctypes.data, len(offs),
-                                      np.asarray(velocity, np.float32).ctypes.data, C.c_float(interval),
-                                      pool_ids.ctypes.data, len(pool_ids))
-        _lib.check(e if e < 0 else 0, "add_emitter")
-        self._em_world.append(world)
-        self._em_pool.append(pool_ids)
-        self._em_own.append(own)
-        self._split_pools(world)
-        log.info("SPH emitter %d: world %d, %d particles per layer every %.4g s", e, world, len(offs), interval)
-        return int(e)
+        ph = _host(self.model.sph.phase)
+        fl = _host(self.model.particle_flags)
+        mass = _host(self.model.particle_mass)
+        rho = _host(self.model.sph.rest_density)
+        ws = self.world_start
+        sph_ids = np.nonzero(sph_phase(ph))[0]
+        spare_ids = np.nonzero((ph == PHASE_SPARE) & ((fl & _ACTIVE) == 0))[0].astype(np.int32)
+        rows = []
+        packing = []
+        for world, region, half_extents, rate, velocity, pool in specs:
+            if not 0 <= world < self.world_count:
+                raise ValueError(f"add_emitter: world {world} out of range")
+            if rate <= 0.0:
+                raise ValueError("add_emitter: rate must be > 0 [m^3/s]")
+            X = _xform7(region)
+            v_local = quat_rotate_inv(X[3:], np.asarray(velocity, np.float64))
+            offs = layer_offsets(np.asarray(half_extents, dtype=np.float64), v_local, cfg.spacing)
+            k = np.searchsorted(sph_ids, ws[world])
+            if k >= len(sph_ids) or sph_ids[k] >= ws[world + 1]:
+                raise ValueError(f"world {world} has no SPH particles or spares")
+            i0 = int(sph_ids[k])
+            interval = len(offs) * (float(mass[i0]) / float(rho[i0])) / rate
+            speed = float(np.linalg.norm(v_local))
+            if speed > 0.0:
+                packing.append(rate / (len(offs) * cfg.spacing * cfg.spacing * speed))
+            own = pool is not None
+            if own:
+                lo_, hi_ = np.searchsorted(spare_ids, [ws[world], ws[world + 1]])
+                pool_ids = np.intersect1d(np.asarray(pool), spare_ids[lo_:hi_]).astype(np.int32)
+            else:
+                pool_ids = np.zeros(0, np.int32)
+            rows.append((int(world), X, offs, np.asarray(velocity, np.float32), interval, pool_ids, own))
+        bad = [r for r in packing if not 0.8 <= r <= 1.25]
+        if bad:
+            log.warning("SPH emitters: %d of %d have rate / (area |v|) outside [0.8, 1.25] (e.g. %.3g): layers will "
+                        "over/under-pack", len(bad), len(packing), bad[0])
+        if not rows:
+            return []
+        cnt = len(rows)
+        world_a = np.array([r[0] for r in rows], np.int32)
+        xform = np.ascontiguousarray(np.stack([r[1] for r in rows]), np.float32)
+        n_off = np.array([len(r[2]) for r in rows], np.int32)
+        offsets = np.ascontiguousarray(np.concatenate([r[2] for r in rows]).reshape(-1, 3), np.float32)
+        vel = np.ascontiguousarray(np.stack([r[3] for r in rows]), np.float32)
+        interval = np.array([r[4] for r in rows], np.float32)
+        psize = np.array([len(r[5]) for r in rows], np.int32)
+        pools = np.ascontiguousarray(np.concatenate([r[5] for r in rows]), np.int32)
+        first = self._lib.adf_add_emitters(self._h, cnt, world_a.ctypes.data, xform.ctypes.data, n_off.ctypes.data,
+                                           offsets.ctypes.data, vel.ctypes.data, interval.ctypes.data,
+                                           psize.ctypes.data, pools.ctypes.data)
+        _lib.check(first if first < 0 else 0, "add_emitter")
+        for r in rows:
+            self._em_world.append(r[0])
+            self._em_pool.append(r[5])
+            self._em_own.append(r[6])
+        for w in sorted({r[0] for r in rows if not r[6]}):
+            self._split_pools(w)
+        log.info("SPH emitters %d..%d added", first, first + cnt - 1)
+        return list(range(int(first), int(first) + cnt))
 
     def _split_pools(self, world: int) -> None:
         """Share the world's unused spares evenly among its emitters given no pool (emitters.py:225-238)."""

@@ -6,6 +6,8 @@
   1,048,576-particle case: 128 x 64 x 128 at 0.01 m in a 4 x 2 x 2 m tank.
 - ``batched_worlds``: many uneven worlds (particle count log-uniform by seed), each a cuboid block in an open box of
   boundary particles 1.5x its extent, with spares for a spout emitter.
+- ``pour_bowls``: thousands of worlds, each a hemisphere bowl of boundary particles moving on a seeded sinusoid
+  (``BowlMotion`` drives the wall velocities between steps) with liquid resting in it and a spout pouring in.
 Config: cubic kernel, h = 4r = 2 spacings, rho0 1000, XSPH 0.01, Jacobi, tolerances 1e-3, resting-jitter rule off.
 """
 
@@ -15,7 +17,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .build import add_fluid_block, add_particle_box, add_spares, box_shell_points, add_wall_particles
+from .build import (add_fluid_block, add_fluid_points, add_particle_box, add_spares, add_wall_particles,
+                    box_shell_points, jittered)
 from .config import DFSPHConfig
 from .model import Model, ModelBuilder
 
@@ -37,6 +40,7 @@ class Scene:
     wall_count: int
     emitters: list[dict] = field(default_factory=list)
     name: str = ""
+    motion: object = None  # BowlMotion of kinematic walls, if any
 
 
 def dam_break(counts=(20, 20, 20), box=(1.0, 1.0, 1.0), spacing: float = 0.02, jitter: float = 0.01, seed: int = 0,
@@ -97,5 +101,111 @@ def batched_worlds(worlds: int = 256, lo: int = 2000, hi: int = 32000, spacing: 
     return Scene(b.finalize(device), cfg, dt, steps, fluid, wall, emit, name=f"batched_{worlds}")
 
 
-__all__ = ["Scene", "benchmark_config", "dam_break", "large_dam_break", "batched_worlds", "world_sizes",
-           "box_shell_points", "add_wall_particles"]
+def hemisphere_shell_points(centre, radius: float, spacing: float) -> np.ndarray:
+    """One layer of wall-particle centres on the lower half of the sphere of radius ``radius + spacing / 2`` about
+    ``centre``: rings of constant latitude one spacing apart along the meridian, each with its circumference / spacing
+    points (the innermost face of the layer is then the bowl surface, as for the box walls)."""
+    rr = radius + 0.5 * spacing
+    rings = max(int(np.ceil(0.5 * np.pi * rr / spacing)), 1)
+    pts = []
+    for k in range(rings + 1):
+        th = 0.5 * np.pi + 0.5 * np.pi * k / rings  # equator (rim) ... bottom pole
+        ring_r = rr * np.sin(th)
+        m = max(int(round(2.0 * np.pi * ring_r / spacing)), 1)
+        ph = 2.0 * np.pi * (np.arange(m) + 0.5 * (k % 2)) / m
+        pts.append(np.stack([ring_r * np.cos(ph), ring_r * np.sin(ph), np.full(m, rr * np.cos(th))], axis=1))
+    return np.concatenate(pts) + np.asarray(centre, np.float64)
+
+
+def bowl_interior_points(centre, radius: float, spacing: float) -> np.ndarray:
+    """Lattice cell centres inside the bowl (at least half a spacing from its surface, below the rim), lowest first."""
+    n = int(np.ceil(radius / spacing)) + 1
+    ax = (np.arange(-n, n) + 0.5) * spacing
+    g = np.stack(np.meshgrid(ax, ax, ax, indexing="ij"), -1).reshape(-1, 3)
+    keep = (np.linalg.norm(g, axis=1) <= radius - 0.5 * spacing) & (g[:, 2] <= 0.0)
+    g = g[keep]
+    g = g[np.lexsort((g[:, 1], g[:, 0], g[:, 2]))]
+    return g + np.asarray(centre, np.float64)
+
+
+@dataclass
+class BowlMotion:
+    """Kinematic bowls: every wall particle of world w moves with the bowl's velocity
+    v_w(t) = A (2 pi / T) cos(2 pi t / T + phase_w) d_w (horizontal unit direction d_w), the derivative of a
+    sinusoidal path of amplitude A and period T. ``apply`` writes the velocity at the step's midpoint time into the
+    state's wall particles before a step (the caller's role for kinematic bodies)."""
+
+    wall_index: np.ndarray   # [n_wall] particle ids
+    wall_world: np.ndarray   # [n_wall] world of each
+    direction: np.ndarray    # [W, 3]
+    phase: np.ndarray        # [W]
+    amplitude: float
+    period: float
+    _dev: dict = field(default_factory=dict)
+
+    def velocities(self, t: float) -> np.ndarray:
+        w = 2.0 * np.pi / self.period
+        return (self.amplitude * w * np.cos(w * t + self.phase))[:, None] * self.direction
+
+    def apply(self, state, t: float, dt: float) -> None:
+        import torch
+
+        qd = state.particle_qd
+        key = str(qd.device)
+        if key not in self._dev:
+            self._dev[key] = (torch.as_tensor(self.wall_index, dtype=torch.int64, device=qd.device),
+                              torch.as_tensor(self.wall_world, dtype=torch.int64, device=qd.device))
+        idx, wof = self._dev[key]
+        v = torch.as_tensor(self.velocities(t + 0.5 * dt).astype(np.float32), device=qd.device)
+        qd[idx] = v[wof]
+
+    def host_velocities(self, t: float, dt: float) -> np.ndarray:
+        """The same per-particle velocities as float32 host rows (for the CPU oracle)."""
+        return self.velocities(t + 0.5 * dt).astype(np.float32)[self.wall_world]
+
+
+def pour_bowls(worlds: int = 4096, lo: int = 4096, hi: int = 16384, spacing: float = 0.005, radius: float = 0.08,
+               amplitude: float = 0.05, period: float = 1.0, spout_speed: float = 1.0, seed: int = 0,
+               jitter: float = 0.01, dt: float = 1.0e-3, steps: int = 2000, device="cpu", **cfg_kw) -> Scene:
+    """Batched pour: per world n_w SPH particles (log-uniform in [lo, hi] by seed), half of them (at most 80 % of the
+    bowl) resting as a jittered lattice in a hemisphere bowl of boundary particles of ``radius``, the rest spares for
+    a 4 x 4 spout at ``spout_speed`` downward into the bowl's centre. Every bowl moves on its own seeded sinusoid
+    (``BowlMotion``); liquid that leaves the escape box is retired. Spacing 0.005 m lets a 0.08 m bowl hold the
+    thousands of particles per world the workload names (at 0.01 m it holds about 1,000)."""
+    cfg = benchmark_config(spacing, world_bounds=((-0.3, -0.3, -0.2), (0.3, 0.3, 0.5)), **cfg_kw)
+    sizes = world_sizes(worlds, lo, hi, seed)
+    rng = np.random.default_rng(seed + 7)
+    ang = rng.uniform(0.0, 2.0 * np.pi, worlds)
+    phase = rng.uniform(0.0, 2.0 * np.pi, worlds)
+    direction = np.stack([np.cos(ang), np.sin(ang), np.zeros(worlds)], axis=1)
+    centre = (0.0, 0.0, radius)
+    shell = hemisphere_shell_points(centre, radius, spacing)
+    inside = bowl_interior_points(centre, radius, spacing)
+    b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    emit, wall_index, wall_world = [], [], []
+    fluid = wall = 0
+    v0 = BowlMotion(np.zeros(0), np.zeros(0), direction, phase, amplitude, period).velocities(0.5 * dt)
+    for w, n_w in enumerate(sizes):
+        b.begin_world()
+        n_liq = int(min(n_w // 2, int(0.8 * len(inside))))
+        pts = jittered(inside[:n_liq], spacing, jitter, seed * 100003 + w)
+        fl = add_fluid_points(b, cfg, pts)
+        wl = add_wall_particles(b, cfg, shell, velocity=tuple(float(c) for c in v0[w]))
+        spares = add_spares(b, cfg, int(n_w) - n_liq, park=(0.0, 0.0, radius + 0.05))
+        b.end_world()
+        fluid += len(fl)
+        wall += len(wl)
+        wall_index.append(np.arange(wl.start, wl.stop))
+        wall_world.append(np.full(len(wl), w))
+        emit.append({"world": w, "centre": (0.0, 0.0, radius + 0.02), "half": (2.0 * spacing, 2.0 * spacing,
+                                                                             0.5 * spacing),
+                     "velocity": (0.0, 0.0, -spout_speed), "pool": np.arange(spares.start, spares.stop),
+                     "layer_every": spacing / spout_speed})
+    motion = BowlMotion(np.concatenate(wall_index), np.concatenate(wall_world), direction, phase, amplitude, period)
+    sc = Scene(b.finalize(device), cfg, dt, steps, fluid, wall, emit, name=f"pour_{worlds}")
+    sc.motion = motion
+    return sc
+
+
+__all__ = ["Scene", "benchmark_config", "dam_break", "large_dam_break", "batched_worlds", "pour_bowls", "BowlMotion",
+           "world_sizes", "box_shell_points", "add_wall_particles", "hemisphere_shell_points", "bowl_interior_points"]

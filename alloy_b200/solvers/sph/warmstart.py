@@ -247,13 +247,15 @@ def generate_pairs(device=None, pairs: int = 2_000_000, seed: int = 1, steps: in
         sc = make(device=dev, seed=seed)
         sol = SolverDFSPH(sc.model, sc.config)
         host = sc.model.host()
+        specs = []
         for e in sc.emitters:
             i0 = int(host["world_start"][e["world"]])
             vol = float(host["mass"][i0]) / float(host["rest_density"][i0])
             offs = layer_offsets(np.asarray(e["half"], np.float64), np.asarray(e["velocity"], np.float64),
                                  sc.config.spacing)
-            sol.add_emitter(e["world"], e["centre"], e["half"], len(offs) * vol / (10.0 * sc.dt), e["velocity"],
-                            pool=e["pool"])
+            rate = len(offs) * vol / e.get("layer_every", 10.0 * sc.dt)
+            specs.append((e["world"], e["centre"], e["half"], rate, e["velocity"], e["pool"]))
+        sol.add_emitters(specs)
         a, b = sc.model.state(), sc.model.state()
         f, t, _, _ = collect_pairs(sol, a, b, sc.dt, steps, every=every, per_record=per, seed=seed)
         if log is not None:

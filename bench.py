@@ -7,6 +7,10 @@ closed 4 x 2 x 2 m tank of boundary particles, dt 0.5 ms, cubic kernel, Jacobi, 
 float64 per-world residual sums. A step is one full DFSPH step over every particle; steps continue the same run
 (warm starts carried). The working set per step (~0.9 GB) is far larger than L2, so no flush is needed between steps.
 
+Other workloads (--workload): dam_break (8,000 particles, 1 world), batched_worlds (256 uneven worlds with spouts,
+world shards across ranks), pour_bowls (4,096 worlds of 4,096-16,384 particles, each a moving hemisphere bowl of
+boundary particles with a spout; the bowls' velocities are set before every step, inside the timed region).
+
 Arms:
   --impl b200       this package's CUDA path (one process per GPU; N > 1 runs N replicas of the single world:
                     the path has no data-path collective)
@@ -41,26 +45,53 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--workload", choices=("large_dam_break", "dam_break", "batched_worlds"),
+    ap.add_argument("--workload", choices=("large_dam_break", "dam_break", "batched_worlds", "pour_bowls"),
                     default="large_dam_break")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-warm", action="store_true", help="skip the learned warm-start arms")
     return ap.parse_args()
 
 
-def make_scene(name: str, device):
-    from alloy_b200.solvers.sph.testing import batched_worlds, dam_break, large_dam_break
+MULTI_WORLD = ("batched_worlds", "pour_bowls")
+
+
+def make_scene(name: str, device, cpu_sample: bool = False):
+    """The workload's scene; ``cpu_sample``: the bounded share the CPU oracle runs (the first 256 of the 4,096 pour
+    worlds, whose sizes, seeds and paths are those of the full workload)."""
+    from alloy_b200.solvers.sph.testing import batched_worlds, dam_break, large_dam_break, pour_bowls
 
     if name == "large_dam_break":
         return large_dam_break(device=device)
     if name == "batched_worlds":
         return batched_worlds(device=device)
+    if name == "pour_bowls":
+        return pour_bowls(worlds=256 if cpu_sample else 4096, device=device)
     return dam_break(device=device)
+
+
+class Stepper:
+    """Steps of one solver over a pair of states, with the scene's kinematic walls (if any) driven before each step
+    as a caller drives kinematic bodies."""
+
+    def __init__(self, sol, sc, a, b):
+        self.sol, self.sc, self.a, self.b, self.k = sol, sc, a, b, 0
+
+    def drive(self, state):
+        if self.sc.motion is not None:
+            self.sc.motion.apply(state, self.k * self.sc.dt, self.sc.dt)
+
+    def __call__(self, n: int = 1):
+        for _ in range(n):
+            self.drive(self.a)
+            self.sol.step(self.a, self.b, None, None, self.sc.dt)
+            self.a, self.b = self.b, self.a
+            self.k += 1
 
 
 def spouts(sc):
     """(world, centre, half extents, rate, velocity, pool, layer offsets, interval) of each spout of a scene: one layer
-    every 10 steps (the 256-world benchmark's 64 particles per 10 steps at 1.5 m/s)."""
+    every ``layer_every`` seconds (default 10 steps: the 256-world benchmark's 64 particles per 10 steps at 1.5 m/s;
+    the pour's 16 particles every 5 ms at 1 m/s)."""
     from alloy_b200.solvers.sph.solver import layer_offsets
 
     arr = sc.model.host()
@@ -71,7 +102,7 @@ def spouts(sc):
         vol = float(arr["mass"][i0]) / float(arr["rest_density"][i0])
         offs = layer_offsets(np.asarray(e["half"], np.float64), np.asarray(e["velocity"], np.float64),
                              sc.config.spacing)
-        rate = len(offs) * vol / (10.0 * sc.dt)
+        rate = len(offs) * vol / e.get("layer_every", 10.0 * sc.dt)
         out.append((w, e["centre"], e["half"], rate, e["velocity"], np.sort(e["pool"]), offs,
                     float(np.float32(len(offs) * vol / rate))))
     return out
@@ -80,7 +111,7 @@ def spouts(sc):
 def rank_scene(sc, name: str, rank: int, world: int, device):
     """The share of the workload one rank steps: a replica of a single-world scene, or the rank's shard of whole
     worlds (longest-processing-time by particle count; no data-path collective) with its spouts renumbered."""
-    if name != "batched_worlds" or world == 1:
+    if name not in MULTI_WORLD or world == 1:
         return sc
     from alloy_b200.solvers.sph.sharding import shard_worlds, sub_model
     from alloy_b200.solvers.sph.testing import Scene
@@ -95,14 +126,31 @@ def rank_scene(sc, name: str, rank: int, world: int, device):
             k = mine.index(e["world"])
             ems.append({**e, "world": k, "pool": np.asarray(e["pool"]) - ws[e["world"]] + sws[k]})
     fl = int(sum(np.sum(sub.host()["phase"][sws[k]:sws[k + 1]] >= 1) for k in range(len(mine))))
-    return Scene(sub, sc.config, sc.dt, sc.steps, fl, 0, ems, name=f"{sc.name}_shard{rank}")
+    out = Scene(sub, sc.config, sc.dt, sc.steps, fl, 0, ems, name=f"{sc.name}_shard{rank}")
+    if sc.motion is not None:  # the shard's bowls, renumbered into the sub-model
+        from alloy_b200.solvers.sph.testing import BowlMotion
+
+        m = sc.motion
+        idx, wof = [], []
+        for k, w in enumerate(mine):
+            sel = m.wall_world == w
+            idx.append(m.wall_index[sel] - ws[w] + sws[k])
+            wof.append(np.full(int(sel.sum()), k))
+        out.motion = BowlMotion(np.concatenate(idx), np.concatenate(wof), m.direction[mine], m.phase[mine],
+                                m.amplitude, m.period)
+    return out
 
 
 def workload_config(sc, name: str) -> dict:
-    W = len(sc.model.host()["world_start"]) - 1 if name == "batched_worlds" else 1
+    W = len(sc.model.host()["world_start"]) - 1 if name in MULTI_WORLD else 1
+    extra = ""
+    if name == "batched_worlds":
+        extra = ", one spout per world (64 particles per 10 steps)"
+    elif name == "pour_bowls":
+        extra = (", a hemisphere bowl (r 0.08 m) of boundary particles per world on a seeded sinusoid (0.05 m, 1 s), "
+                 "one spout per world (16 particles per 5 ms at 1 m/s), escape box")
     return {"workload": f"{name}: {sc.fluid_count} liquid particles + {sc.wall_count} boundary particles in {W} "
-                        f"world(s), dt {sc.dt} s, Jacobi, tol 1e-3/1e-3, cubic h=2 spacings"
-                        + (", one spout per world (64 particles per 10 steps)" if W > 1 else ""),
+                        f"world(s), dt {sc.dt} s, Jacobi, tol 1e-3/1e-3, cubic h=2 spacings" + extra,
             "liquid_particles": sc.fluid_count, "boundary_particles": sc.wall_count, "worlds": W, "dt": sc.dt,
             "spacing": sc.config.spacing, "l2": "inputs larger than L2 (working set > 126 MB per step)"}
 
@@ -214,11 +262,20 @@ def cpu_oracle_run(sc, steps: int, warmup: int, budget_s: float | None):
     orc = Oracle(sc.model.host(), sc.config)
     for w, centre, _, _, vel, pool, offs, interval in spouts(sc):
         orc.add_emitter(w, _xform7(centre), offs, vel, interval, pool)
-    for _ in range(warmup):
+    k = 0
+
+    def step():
+        nonlocal k
+        if sc.motion is not None:  # the bowls' velocities, as the GPU arm drives them
+            orc.set_velocity(sc.motion.wall_index, sc.motion.host_velocities(k * sc.dt, sc.dt))
         orc.step(sc.dt)
+        k += 1
+
+    for _ in range(warmup):
+        step()
     done, t0, ps = 0, time.perf_counter(), 0
     while done < steps:
-        orc.step(sc.dt)
+        step()
         done += 1
         ps += int(orc.active_fluid())
         if budget_s is not None and time.perf_counter() - t0 > budget_s:
@@ -231,17 +288,18 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sc = make_scene(args.workload, "cpu")
+    sc = make_scene(args.workload, "cpu", cpu_sample=True)
     threads = os.cpu_count() or 1
     warm = min(args.warmup, 2)
     value, done, t = cpu_oracle_run(sc, args.steps, warm, 90.0)
+    share = " (its first 256 worlds)" if args.workload == "pour_bowls" else ""
     sample = (f"{done} of {args.steps} full steps (90 s budget) after {warm} warm-up steps of the {args.workload} "
-              f"workload from its start state, {threads} OpenMP threads")
+              f"workload{share} from its start state, {threads} OpenMP threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / max(done, 1), "higher_is_better": True,
-        "scaling": "strong" if args.workload == "batched_worlds" else "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": workload_config(sc, args.workload),
+        "scaling": "strong" if args.workload in MULTI_WORLD else "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(make_scene(args.workload, "cpu"), args.workload),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "CPU oracle: a C++/OpenMP restatement of the reference's Warp kernels (warp-lang is not installed)"}))
@@ -259,30 +317,24 @@ def warm_arm(args, dev, judge: bool, rank: int, world: int) -> dict:
     full = make_scene(args.workload, dev)
     sc = rank_scene(full, args.workload, rank, world, dev)
     sol = SolverDFSPH(sc.model, sc.config)
-    for w, centre, half, rate, vel, pool, _, _ in spouts(sc):
-        sol.add_emitter(w, centre, half, rate, vel, pool=pool)
+    sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
     sol.set_warm_model(default_model())
     sol.warm_judging(judge)
-    a, b = sc.model.state(), sc.model.state()
+    run = Stepper(sol, sc, sc.model.state(), sc.model.state())
     stream = torch.cuda.current_stream(dev)
-    for _ in range(args.warmup):
-        sol.step(a, b, None, None, sc.dt)
-        a, b = b, a
+    run(args.warmup)
     torch.cuda.synchronize(dev)
     nf0 = sol.list_stats()[0]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        sol.step(a, b, None, None, sc.dt)
-        a, b = b, a
+    run(args.steps)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     t = e0.elapsed_time(e1) * 1e-3
     nf1 = sol.list_stats()[0]
     it_den, it_div, err, kept = [], [], [], []
     for _ in range(20):
-        sol.step(a, b, None, None, sc.dt)
-        a, b = b, a
+        run()
         r = sol.report()
         d = sol.diagnostics()
         it_den.append(int(r.iters_density.max()))
@@ -295,6 +347,14 @@ def warm_arm(args, dev, judge: bool, rank: int, world: int) -> dict:
             "iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean": float(np.mean(it_div)),
             "density_err_mean_max_over_steps": float(np.max(err)), "learned_start_kept": float(np.mean(kept)),
             "particle_steps": ps, "seconds": t}
+
+
+T_START = time.perf_counter()
+
+
+def note(msg: str) -> None:
+    """Progress of the phases on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - T_START:7.1f} s] {msg}", file=sys.stderr, flush=True)
 
 
 def run_b200(args):
@@ -312,23 +372,24 @@ def run_b200(args):
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    note("building the scene")
     full = make_scene(args.workload, dev)
     sc = rank_scene(full, args.workload, rank, world, dev)
+    note(f"solver for {sc.model.particle_count} particles")
     sol = SolverDFSPH(sc.model, sc.config)
-    for w, centre, half, rate, vel, pool, _, _ in spouts(sc):
-        sol.add_emitter(w, centre, half, rate, vel, pool=pool)
-    a, b = sc.model.state(), sc.model.state()
+    sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
+    run = Stepper(sol, sc, sc.model.state(), sc.model.state())
     stream = torch.cuda.current_stream(dev)
-    for _ in range(args.warmup):
-        sol.step(a, b, None, None, sc.dt)
-        a, b = b, a
+    note("warm-up steps (the first one tunes)")
+    run(args.warmup)
+    torch.cuda.synchronize(dev)
+    note("timed steps")
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
     launches0 = sol.kernel_launches()
 
     def timed():
-        nonlocal a, b
         clocks = Clocks(dev)
         clocks.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -336,9 +397,7 @@ def run_b200(args):
             dist.barrier()
         torch.cuda.synchronize(dev)
         e0.record(stream)
-        for _ in range(args.steps):
-            sol.step(a, b, None, None, sc.dt)
-            a, b = b, a
+        run(args.steps)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         if world > 1:
@@ -362,11 +421,10 @@ def run_b200(args):
     launches = sol.kernel_launches() - launches0
     # per-kernel durations: the same number of steps again, each kernel group bracketed by CUDA events on the launch
     # stream (kernels launched one by one; the timed steps above replay one CUDA graph per step)
+    note("per-kernel timing pass")
     sol.profile(True)
     sol.profile_read()
-    for _ in range(args.steps):
-        sol.step(a, b, None, None, sc.dt)
-        a, b = b, a
+    run(args.steps)
     prof = sol.profile_read()
     sol.profile(False)
     psteps = 0.5 * (nf0 + nf1) * args.steps
@@ -380,7 +438,9 @@ def run_b200(args):
     value = float(ptot.item()) / t_max
 
     # end to end through the public API with host buffers: H2D of the state, the step, D2H of the state and report
+    note("end-to-end pass")
     n = sc.model.particle_count
+    a, b = run.a, run.b
     hq = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
     hqd = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
     hq.copy_(a.particle_q)
@@ -391,7 +451,9 @@ def run_b200(args):
     for _ in range(args.steps):
         a.particle_q.copy_(hq, non_blocking=True)
         a.particle_qd.copy_(hqd, non_blocking=True)
+        run.drive(a)
         sol.step(a, b, None, None, sc.dt)
+        run.k += 1
         hq.copy_(b.particle_q, non_blocking=True)
         hqd.copy_(b.particle_qd, non_blocking=True)
         r = sol.report()  # synchronises the stream and reads the per-world result
@@ -438,7 +500,9 @@ def run_b200(args):
     warm = {}
     if not args.no_warm:
         del sol
+        run = None  # the plain solver's memory goes back before the warm-start arms build theirs
         for judge in (True, False):
+            note(f"warm-start arm (judge {judge})")
             r = warm_arm(args, dev, judge, rank, world)
             tw = torch.tensor([r["seconds"]], dtype=torch.float64, device=dev)
             pw = torch.tensor([r["particle_steps"]], dtype=torch.float64, device=dev)
@@ -453,20 +517,22 @@ def run_b200(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        csc = make_scene(args.workload, "cpu")
+        note("CPU baseline")
+        csc = make_scene(args.workload, "cpu", cpu_sample=True)
         threads = os.cpu_count() or 1
         v_cpu, done, t_cpu = cpu_oracle_run(csc, 1000, 1, 20.0)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{done} full steps (after 1 warm-up step) of the same workload from its start state, "
+               "sample": f"{done} full steps (after 1 warm-up step) of the same workload"
+                         f"{' (its first 256 worlds)' if args.workload == 'pour_bowls' else ''} from its start state, "
                          f"{t_cpu:.1f} s, CPU oracle with {threads} OpenMP threads"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "strong" if args.workload == "batched_worlds" else "weak", "vs_baseline": None,
+            "scaling": "strong" if args.workload in MULTI_WORLD else "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {**workload_config(full, args.workload),
-                       "parallelism": ("world shards" if args.workload == "batched_worlds" else "replicas")
+                       "parallelism": ("world shards" if args.workload in MULTI_WORLD else "replicas")
                        if world > 1 else "single GPU"},
             "e2e": e2e, "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",

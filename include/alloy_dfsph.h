@@ -158,6 +158,14 @@ int adf_reset(adf_solver* solver, const uint8_t* world_mask, const int32_t* flag
 int adf_add_emitter(adf_solver* solver, int world, const float* xform, const float* offsets, int n_off,
                     const float* velocity, float interval, const int32_t* pool, int pool_size);
 
+/* Many emitters in one call, with one upload of the emitter tables (adding them one by one re-uploads the tables each
+ * time): emitter k has world[k], xform[k][7], n_off[k] offsets (the next n_off[k] rows of offsets[][3]), velocity[k][3],
+ * interval[k] and pool_size[k] pool ids (the next pool_size[k] of pool). All are checked before any is added. Returns
+ * the first new emitter's index (>= 0) or -ADF_ERR_*. Between steps only. */
+int adf_add_emitters(adf_solver* solver, int count, const int32_t* world, const float* xform, const int32_t* n_off,
+                     const float* offsets, const float* velocity, const float* interval, const int32_t* pool_size,
+                     const int32_t* pool);
+
 /* Replaces the pool reassignment of emitters.split_pools (emitters.py:225-238): emitter `emitter` draws from `pool`
  * (host ids, ascending) from now on; its cursor is kept. Between steps only. */
 int adf_set_emitter_pool(adf_solver* solver, int emitter, const int32_t* pool, int pool_size);

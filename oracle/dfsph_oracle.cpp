@@ -962,6 +962,13 @@ void orc_set_state(void* hp, const float* q, const float* qd) {
     }
   });
 }
+// Velocities of m particles (kinematic walls driven by the caller between steps), in the working precision.
+void orc_set_velocity(void* hp, int m, const int* idx, const float* v) {
+  DISPATCH({
+    using R = typename std::remove_reference<decltype(s.kv)>::type::value_type;
+    for (int k = 0; k < m; ++k) s.v[idx[k]] = {R(v[3 * k]), R(v[3 * k + 1]), R(v[3 * k + 2])};
+  });
+}
 void orc_get_state(void* hp, float* q, float* qd) { DISPATCH({ copy_out3(s.q, q); copy_out3(s.v, qd); }); }
 void orc_get_state_f64(void* hp, double* q, double* qd) { DISPATCH({ copy_out3(s.q, q); copy_out3(s.v, qd); }); }
 void orc_set_warm(void* hp, const float* kv, const float* kd) {

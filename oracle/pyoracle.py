@@ -86,6 +86,7 @@ def lib():
             getattr(L, name).argtypes = [P]
         L.orc_set_threads.argtypes = [P, C.c_int]
         L.orc_set_state.argtypes = [P, fp, fp]
+        L.orc_set_velocity.argtypes = [P, C.c_int, ip, fp]
         L.orc_get_state.argtypes = [P, fp, fp]
         L.orc_get_state_f64.argtypes = [P, dp, dp]
         L.orc_set_warm.argtypes = [P, fp, fp]
@@ -148,6 +149,12 @@ class Oracle:
         q = np.ascontiguousarray(q, np.float32).reshape(-1)
         qd = np.ascontiguousarray(qd, np.float32).reshape(-1)
         self.L.orc_set_state(self.h, _p(q, C.c_float), _p(qd, C.c_float))
+
+    def set_velocity(self, idx, v):
+        """Velocities of the particles ``idx`` (kinematic walls), keeping the rest of the state's precision."""
+        idx = np.ascontiguousarray(idx, np.int32)
+        v = np.ascontiguousarray(v, np.float32).reshape(-1)
+        self.L.orc_set_velocity(self.h, len(idx), _p(idx, C.c_int), _p(v, C.c_float))
 
     def state(self):
         q = np.zeros((self.n, 3), np.float32)
