@@ -38,7 +38,7 @@ class Params(C.Structure):
                 ("divergence_solve", C.c_int), ("two_sided", C.c_int), ("xsph_c", C.c_double),
                 ("capacity", C.c_int), ("v_sep", C.c_double), ("relief_speed", C.c_double),
                 ("project_eps", C.c_double), ("has_bounds", C.c_int), ("bounds_lo", C.c_double * 3),
-                ("bounds_hi", C.c_double * 3)]
+                ("bounds_hi", C.c_double * 3), ("cg", C.c_int)]
 
 
 class ModelDesc(C.Structure):

@@ -146,6 +146,7 @@ struct adf_solver {
   cudaStream_t cap_stream = nullptr, body_stream = nullptr;
   // learned warm start (adf_set_warm_model) and feature recording (adf_set_feature_recording)
   bool warm_on = false, feat_rec = false, warm_alloc = false, judge = true;
+  bool cg = false;  // projected preconditioned CG pressure solve (adf_params.cg)
   __nv_bfloat16 *mw1 = nullptr, *mw2 = nullptr;
   float *mparams = nullptr, *mnorm = nullptr;
   int* merr = nullptr;
@@ -368,9 +369,61 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   return check_launch();
 }
 
+// One CG product out (+)= A vec (- b): the pressure acceleration of vec, then its divergence (krylov.py:254-261).
+void cg_product(adf_solver* s, DevP& P, cudaStream_t st, const float* vec, const float* vr, float* out, int gated,
+                int bias, int accumulate) {
+  const int n = s->n;
+  const TuneCfg& ca = s->tune[TK_ACCEL];
+  const TuneCfg& cj = s->tune[TK_JACOBI];
+  prof_begin(s, 5, st);
+  NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, vec, vr, gated);
+  ++s->launches;
+  prof_end(s, st);
+  prof_begin(s, 6, st);
+  NB_DISPATCH(k_cg_apply, cj.nb, blocks(n, cj.block), cj.block, st, P, vec, out, gated, bias, accumulate);
+  ++s->launches;
+  prof_end(s, st);
+}
+
+void cg_sums(adf_solver* s, DevP& P, cudaStream_t st, int with_max) {
+  prof_begin(s, 7, st);
+  if (P.n_chunks > 0) LAUNCH(s, k_chunk_sum2, P.n_chunks, 256, st, P);
+  LAUNCH(s, k_world_sum2, s->W, 256, st, P, with_max);
+  prof_end(s, st);
+}
+
+// krylov.py:278-285: w = A k - b from the warm start, the active set, z, p and r.z
+void cg_init(adf_solver* s, DevP& P, cudaStream_t st) {
+  const int n = s->n;
+  cudaMemsetAsync(P.cg_restart, 0, sizeof(int) * std::max(s->W, 1), st);
+  cudaMemsetAsync(P.cg_pair, 0, sizeof(float2) * std::max(n, 1), st);
+  cg_product(s, P, st, P.kappa, P.kr, P.cg_w, 0, 1, 0);
+  LAUNCH(s, k_cg_init, blocks(n), BLOCK, st, P);
+  cg_sums(s, P, st, 0);
+  LAUNCH(s, k_cg_first_rz, blocks(s->W), BLOCK, st, P);
+}
+
+// krylov.py:287-297: one projected PCG iteration of every unconverged world, with its stop test
+void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
+  const int n = s->n;
+  cg_product(s, P, st, P.cg_pd, P.cg_pdr, P.cg_ap, 0, 0, 0);
+  cg_sums(s, P, st, 0);
+  LAUNCH(s, k_cg_step, blocks(n), BLOCK, st, P);
+  cg_product(s, P, st, P.cg_corr, P.cg_corrr, P.cg_w, 1, 0, 1);
+  LAUNCH(s, k_cg_finish, blocks(n), BLOCK, st, P);
+  cg_sums(s, P, st, 1);
+  cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
+  LAUNCH(s, k_cg_beta, blocks(s->W), BLOCK, st, P);
+  LAUNCH(s, k_cg_direction, blocks(n), BLOCK, st, P);
+}
+
 void enqueue_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   const int n = s->n;
   (void)n;
+  if (s->cg) {
+    cg_iteration(s, P, st);
+    return;
+  }
   prof_begin(s, 5, st);
   run_tk(s, TK_ACCEL, st, P);
   prof_end(s, st);
@@ -489,12 +542,13 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
       ++s->launches;
     }
     DevP Q = P;
-    if (!s->judge) {  // the learned start replaces the plain one outright
+    const bool take = !s->judge || s->cg;
+    if (take) {  // the learned start replaces the plain one outright
       Q.kappa2 = P.kappa;
       Q.kr2 = P.kr;
     }
     LAUNCH(s, k_learned_start, blocks(n), BLOCK, st, Q);
-    if (!s->judge) LAUNCH(s, k_mark_learned, blocks(W), BLOCK, st, P);
+    if (take) LAUNCH(s, k_mark_learned, blocks(W), BLOCK, st, P);
     prof_end(s, st);
   }
   if (W > 0) {
@@ -505,8 +559,9 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
   }
   int rc = check_launch();
   if (rc) return rc;
-  const bool dual = warm && s->judge;
+  const bool dual = warm && s->judge && !s->cg;  // the first-sweep judge is a Jacobi sweep
   if (dual) dual_iteration(s, P, st);
+  if (s->cg && W > 0) cg_init(s, P, st);
   if (graph) {
     rc = capture_iterations(s, P, st);
     if (rc) return rc;
@@ -732,6 +787,23 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.cseg, (size_t)W + 1);
   rc |= s->alloc(&d.n_cw, 1);
   rc |= s->alloc(&chunk_world, cb.size());
+  s->cg = p.cg != 0;
+  if (s->cg) {
+    rc |= s->alloc(&d.cg_pd, n);
+    rc |= s->alloc(&d.cg_pdr, n);
+    rc |= s->alloc(&d.cg_z, n);
+    rc |= s->alloc(&d.cg_w, n);
+    rc |= s->alloc(&d.cg_ap, n);
+    rc |= s->alloc(&d.cg_corr, n);
+    rc |= s->alloc(&d.cg_corrr, n);
+    rc |= s->alloc(&d.cg_act, n);
+    rc |= s->alloc(&d.cg_pair, n);
+    rc |= s->alloc(&d.cg_rz, W);
+    rc |= s->alloc(&d.cg_step, W);
+    rc |= s->alloc(&d.cg_sums, W);
+    rc |= s->alloc(&d.cg_restart, W);
+    rc |= s->alloc(&d.part2, std::max<size_t>(cb.size(), 1));
+  }
   rc |= s->alloc(&d.converged, W);
   rc |= s->alloc(&d.iters, W);
   rc |= s->alloc(&d.err_mean, W);

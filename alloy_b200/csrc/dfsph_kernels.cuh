@@ -167,6 +167,21 @@ struct DevP {
   double* sum_l;
   float* max_c;
   float* max_l;
+  // projected preconditioned CG (krylov.py; null unless the CG pressure solver is selected)
+  float* cg_pd;     // search direction p, and p / rho0 (sorted)
+  float* cg_pdr;
+  float* cg_z;      // M^-1 r on the active set
+  float* cg_w;      // w = A k - b
+  float* cg_ap;     // A p
+  float* cg_corr;   // clamped part of the step, and / rho0
+  float* cg_corrr;
+  int* cg_act;      // 1: in the active set F
+  float2* cg_pair;  // original order: (dot-product term, error) for the per-world sums
+  double* cg_rz;    // [W] r.z
+  double* cg_step;  // [W] beta
+  double2* cg_sums; // [W] (sum of pair.x, sum of pair.y)
+  int* cg_restart;  // [W] active-set changes this iteration
+  double2* part2;   // [chunks] partial sums of pairs
 };
 
 __device__ __forceinline__ bool is_fluid_orig(const DevP& P, int i) {
@@ -1131,12 +1146,11 @@ __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
 }
 
 // pressure.py:294-352
+// pressure.py:294-310: Ar_i of the accelerations in P.acc (the matrix-free product, before the compliance term)
 template <int NB>
-__device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
+__device__ __forceinline__ float accel_divergence(const DevP& P, int p, float inv_r0) {
   float4 xi = P.pos[p];
   float4 ai = P.acc[p];
-  float r0 = P.vel[p].w;
-  float inv_r0 = 1.0f / r0;
   float ar = 0.0f;
   int c = P.cnt[p];
   for (int k = 0; k < c; k += NB) {
@@ -1160,6 +1174,14 @@ __device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
   }
   float4 sg = P.slot_g[p];
   if (sg.w >= 0.0f) ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
+  return ar;
+}
+
+template <int NB>
+__device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
+  float r0 = P.vel[p].w;
+  float inv_r0 = 1.0f / r0;
+  float ar = accel_divergence<NB>(P, p, inv_r0);
   float kap = P.kappa[p];
   ar = ADF_FMA(-P.reg[p], kap, ar);
   const float dt = P.dt;
@@ -1187,6 +1209,194 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
   int b, e;
   if (!work_item(P, b, e)) return;
   for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one<NB>(P, p);
+}
+
+// ------------------------------------------------------------------------------------ projected CG (krylov.py)
+// One CG per world on w = A k - b, k >= k_lo (krylov.py:1-17), A k = -dt^n (Ar(k) - reg k). Each kernel follows
+// the reference kernel of the same name (krylov.py:71-246); a + b c updates are fused (the oracle fuses the same
+// ones), per-world dot products are the float64 sums of k_chunk_sum2 / k_world_sum2 in the caller's order.
+__device__ __forceinline__ bool cg_skip(const DevP& P, int w, int gated) {
+  return P.converged[w] != 0 || (gated && P.cg_restart[w] == 0);
+}
+
+// krylov.py:71-80: acc = pressure acceleration of the field vec (vr = vec / rho0)
+template <int NB>
+__global__ void __launch_bounds__(BLOCK) k_cg_accel(DevP P, const float* vec, const float* vr, int gated) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
+  DevP Q = P;
+  Q.kappa = const_cast<float*>(vec);
+  Q.kr = const_cast<float*>(vr);
+  float ax, ay, az;
+  pressure_accel<NB>(Q, p, P.pos[p], ax, ay, az);
+  P.acc[p] = make_float4(ax, ay, az, 0.0f);
+}
+
+// krylov.py:83-101: out (+)= A vec (- b); pair.x = vec_i (A vec)_i
+template <int NB>
+__global__ void __launch_bounds__(BLOCK) k_cg_apply(DevP P, const float* vec, float* out, int gated, int bias,
+                                                    int accumulate) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
+  const float dt = P.dt;
+  const bool div = P.mode == 0;
+  const float scale = div ? dt : dt * dt;
+  const float inv_r0 = 1.0f / P.vel[p].w;
+  const float t = ADF_FMA(-P.reg[p], vec[p], accel_divergence<NB>(P, p, inv_r0));
+  float v = -(scale * t);
+  P.cg_pair[P.id_of[p]] = make_float2(vec[p] * v, 0.0f);
+  if (bias) v = v - (div ? P.src[p] : P.src[p] - 1.0f);
+  if (accumulate) v = v + out[p];
+  out[p] = v;
+}
+
+// krylov.py:104-133: active set, z = M^-1 r on F (r = -w), first direction p = z; pair.x = r.z
+__global__ void __launch_bounds__(BLOCK) k_cg_init(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const float dt = P.dt;
+  const float scale = P.mode == 0 ? dt : dt * dt;
+  const float w = P.cg_w[p];
+  const bool a = P.kappa[p] > P.lower[p] || w < 0.0f;
+  const float zi = a ? ((-w) * P.alpha[p]) / scale : 0.0f;
+  P.cg_act[p] = a ? 1 : 0;
+  P.cg_z[p] = zi;
+  P.cg_pd[p] = zi;
+  P.cg_pdr[p] = zi / P.vel[p].w;
+  P.cg_pair[P.id_of[p]] = make_float2(-w * zi, 0.0f);
+}
+
+__global__ void k_cg_first_rz(DevP P) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W) return;
+  P.cg_rz[w] = P.cg_sums[w].x;
+  P.cg_restart[w] = 0;
+}
+
+// krylov.py:146-170: k += a p on F, projected onto k >= k_lo (the clamped part into corr); w += a A p
+__global__ void __launch_bounds__(BLOCK) k_cg_step(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const int w = P.world_s[p];
+  if (P.converged[w]) return;
+  const double pap = P.cg_sums[w].x;
+  const float a = (float)(pap > 1.0e-30 ? P.cg_rz[w] / pap : 0.0);
+  const float r0 = P.vel[p].w;
+  float c = 0.0f;
+  if (P.cg_act[p]) {
+    float k = ADF_FMA(a, P.cg_pd[p], P.kappa[p]);
+    const float lb = P.lower[p];
+    if (k < lb) {
+      c = lb - k;
+      k = lb;
+      P.cg_act[p] = 0;
+      atomicAdd(&P.cg_restart[w], 1);
+    }
+    P.kappa[p] = k;
+    P.kr[p] = k / r0;
+  }
+  P.cg_corr[p] = c;
+  P.cg_corrr[p] = c / r0;
+  P.cg_w[p] = ADF_FMA(a, P.cg_ap[p], P.cg_w[p]);
+}
+
+// krylov.py:173-204: activation of compressed bound variables, z = M^-1 r on F, (r.z, error) per particle
+__global__ void __launch_bounds__(BLOCK) k_cg_finish(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const int w = P.world_s[p];
+  if (P.converged[w]) return;
+  const float dt = P.dt;
+  const bool div = P.mode == 0;
+  const float scale = div ? dt : dt * dt;
+  const float wv = P.cg_w[p];
+  int act = P.cg_act[p];
+  if (!act && wv < 0.0f) {
+    act = 1;
+    P.cg_act[p] = 1;
+    atomicAdd(&P.cg_restart[w], 1);
+  }
+  const float zi = act ? ((-wv) * P.alpha[p]) / scale : 0.0f;
+  P.cg_z[p] = zi;
+  float e = maxr(-wv, 0.0f);
+  if (P.kappa[p] > P.lower[p]) e = fabsf(wv);
+  if (div) {
+    if (P.neff[p] < P.min_nb) e = 0.0f;
+    e = e * dt;
+  }
+  const int i = P.id_of[p];
+  P.err_orig[i] = e;
+  P.cg_pair[i] = make_float2(-wv * zi, e);
+}
+
+// krylov.py:207-233: per world the stop test (as k_world_check), then beta = r.z_new / r.z (0 after a set change)
+__global__ void k_cg_beta(DevP P) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W || P.converged[w]) return;
+  const int it = P.iters[w] + 1;
+  P.iters[w] = it;
+  const double2 sm = P.cg_sums[w];
+  const double na = P.n_active[w];
+  const float mean = (float)(sm.y / (na > 1.0 ? na : 1.0));
+  P.err_mean[w] = mean;
+  double beta = 0.0;
+  if (P.cg_restart[w] == 0 && P.cg_rz[w] > 1.0e-30) beta = sm.x / P.cg_rz[w];
+  P.cg_restart[w] = 0;
+  P.cg_rz[w] = sm.x;
+  P.cg_step[w] = beta;
+  if ((it >= P.min_it && mean <= P.tol && P.emax[w] <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+  else atomicAdd(P.n_unconv, 1);
+}
+
+// krylov.py:236-246: p = z + beta p on F, 0 elsewhere
+__global__ void __launch_bounds__(BLOCK) k_cg_direction(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const int w = P.world_s[p];
+  if (P.converged[w]) return;
+  const float pd = P.cg_act[p] ? ADF_FMA((float)P.cg_step[w], P.cg_pd[p], P.cg_z[p]) : 0.0f;
+  P.cg_pd[p] = pd;
+  P.cg_pdr[p] = pd / P.vel[p].w;
+}
+
+// Per-world (sum x, sum y, max y) of the CG pairs: chunk partials (chunks of converged worlds skipped), then one
+// block per world in the fixed tree order of k_world_check; the maximum floored at 0 goes to emax when asked.
+__global__ void __launch_bounds__(256) k_chunk_sum2(DevP P) {
+  __shared__ double smd[8];
+  __shared__ float smf[8];
+  const int c = blockIdx.x;
+  if (P.converged[P.chunk_world[c]]) return;
+  const int i = P.chunk_begin[c] + threadIdx.x;
+  const bool in = i < P.chunk_end[c];
+  const float2 v = in ? P.cg_pair[i] : make_float2(0.0f, 0.0f);
+  const double sx = fold256(in ? (double)v.x : 0.0, smd);
+  const double sy = fold256(in ? (double)v.y : 0.0, smd);
+  const float m = block_max256(in ? v.y : -3.4e38f, smf);
+  if (threadIdx.x == 0) {
+    P.part2[c] = make_double2(sx, sy);
+    P.part_max[c] = m;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_world_sum2(DevP P, int with_max) {
+  __shared__ double smd[8];
+  __shared__ float smf[8];
+  const int w = blockIdx.x;
+  if (P.converged[w]) return;
+  const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
+  double ax = 0.0, ay = 0.0;
+  float m = -3.4e38f;
+  for (int c = c0 + threadIdx.x; c < c1; c += 256) {
+    ax = ax + P.part2[c].x;
+    ay = ay + P.part2[c].y;
+    m = fmaxf(m, P.part_max[c]);
+  }
+  const double sx = fold256(ax, smd);
+  const double sy = fold256(ay, smd);
+  const float mx = block_max256(m, smf);
+  if (threadIdx.x != 0) return;
+  P.cg_sums[w] = make_double2(sx, sy);
+  if (with_max) P.emax[w] = maxr(mx, 0.0f);
 }
 
 // Chunk partials of the per-world sums. With `converged` given, chunks of converged worlds keep their partials (their

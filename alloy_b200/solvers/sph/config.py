@@ -8,6 +8,8 @@ which of them it cannot honour (``unsupported``) when it is constructed.
 
 from __future__ import annotations
 
+import numpy as np
+
 import math
 from dataclasses import dataclass
 from typing import Literal
@@ -199,3 +201,16 @@ def host_constants(cfg: DFSPHConfig) -> HostConstants:
         tot_min=cfg.diagonal_floor * diag, lattice_grad=math.sqrt(diag), wall_offset=delta, wall_amplitude=amp,
         taper0=0.5 * s, taper1=1.5 * s, reach=reach, project_eps=PROJECT_EPS * cfg.particle_radius,
     )
+
+
+def uniform_layout(mass: np.ndarray, rest_density: np.ndarray, rel: float = 1.0e-6) -> bool:
+    """One particle mass and one rest density among the SPH particles (layout.py:97-100): the DFSPH operator is then
+    symmetric, which the projected CG pressure solve needs; otherwise the reference falls back to Jacobi."""
+    if len(mass) == 0:
+        return True
+
+    def spread(a):
+        a = np.asarray(a, np.float64)
+        return float(np.ptp(a)) / max(float(np.max(np.abs(a))), 1.0e-30)
+
+    return spread(mass) <= rel and spread(rest_density) <= rel

@@ -8,10 +8,11 @@ reset, emitter and protocol methods and the ``alloy_state_arrays`` keys. Everyth
 library's sm_100a kernels; this module holds host logic only (validation, constants, emitter tables) and has no CPU
 fallback: without a CUDA device or the library it raises.
 
-Scope of the CUDA path: cubic or Wendland kernel, relaxed Jacobi pressure solves, XSPH, particle walls (boundary
-particles flagged PROXY), emitters, sinks and the escape box. Settings outside it are refused in the constructor
-(``DFSPHConfig.unsupported``); ``pressure_solver="cg"`` and the resting-jitter rule fall back with a warning, as
-the reference itself falls back from CG (solver.py:89-91).
+Scope of the CUDA path: cubic or Wendland kernel, projected preconditioned CG (the reference's default, krylov.py)
+or relaxed Jacobi pressure solves, XSPH, particle walls (boundary particles flagged PROXY), emitters, sinks and the
+escape box. Settings outside it are refused in the constructor (``DFSPHConfig.unsupported``); CG falls back to Jacobi
+with a warning when particle masses or rest densities differ, as the reference does (solver.py:89-91), and the
+resting-jitter rule falls back to the base tolerance with a warning.
 """
 
 from __future__ import annotations
@@ -24,7 +25,7 @@ import numpy as np
 import torch
 
 from ... import _lib
-from .config import (PHASE_HELD, PHASE_SPARE, DFSPHConfig, host_constants, snap_down, stable_dt)
+from .config import (PHASE_HELD, PHASE_SPARE, DFSPHConfig, host_constants, snap_down, stable_dt, uniform_layout)
 from .model import ParticleFlags
 from .types import SPHReport
 
@@ -155,9 +156,13 @@ class SolverDFSPH:
         if missing:
             raise ValueError("SolverDFSPH (B200 build): not implemented on the CUDA path: " + ", ".join(missing))
         self.pressure_solver = cfg.pressure_solver
-        if self.pressure_solver == "cg":
-            log.warning("SolverDFSPH: pressure_solver 'cg' is not in this build's CUDA path; using 'jacobi'")
-            self.pressure_solver = "jacobi"
+        if self.pressure_solver == "cg" and n:
+            m_all = _host(model.particle_mass)
+            r_all = _host(ns.rest_density)
+            if not uniform_layout(m_all[sph], r_all[sph]):  # solver.py:89-91
+                log.warning("SolverDFSPH: pressure_solver 'cg' needs one particle mass and rest density; using "
+                            "'jacobi'")
+                self.pressure_solver = "jacobi"
         if cfg.rest_jitter_speed:
             log.warning("SolverDFSPH: the resting-jitter tolerance rule is not in this build's CUDA path; the density"
                         " solve runs at max_density_error")
@@ -168,6 +173,7 @@ class SolverDFSPH:
             torch.device("cuda", 0)
         self.hc = host_constants(cfg)
         self._params = self._make_params(cfg, self.hc)
+        self._params.cg = int(self.pressure_solver == "cg")
         q_host = np.ascontiguousarray(_host(model.particle_q), np.float32).reshape(-1) if n else np.zeros(0, np.float32)
         md = _lib.ModelDesc()
         md.n, md.world_count = n, W

@@ -24,8 +24,8 @@ from .model import Model, ModelBuilder
 
 
 def benchmark_config(spacing: float, **overrides) -> DFSPHConfig:
-    cfg = DFSPHConfig(particle_radius=0.5 * spacing, pressure_solver="jacobi", rest_jitter_speed=None,
-                      xsph_c=0.01, viscosity="xsph", **overrides)
+    kw = {"pressure_solver": "jacobi", "rest_jitter_speed": None, "xsph_c": 0.01, "viscosity": "xsph", **overrides}
+    cfg = DFSPHConfig(particle_radius=0.5 * spacing, **kw)
     cfg.validate()
     return cfg
 

@@ -48,25 +48,26 @@ def parse():
     ap.add_argument("--workload", choices=("large_dam_break", "dam_break", "batched_worlds", "pour_bowls"),
                     default="large_dam_break")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-warm", action="store_true", help="skip the learned warm-start arms")
+    ap.add_argument("--no-warm", action="store_true", help="skip the learned warm-start and CG arms")
     return ap.parse_args()
 
 
 MULTI_WORLD = ("batched_worlds", "pour_bowls")
 
 
-def make_scene(name: str, device, cpu_sample: bool = False):
+def make_scene(name: str, device, cpu_sample: bool = False, **cfg_kw):
     """The workload's scene; ``cpu_sample``: the bounded share the CPU oracle runs (the first 256 of the 4,096 pour
-    worlds, whose sizes, seeds and paths are those of the full workload)."""
+    worlds, whose sizes, seeds and paths are those of the full workload); ``cfg_kw``: solver settings (the pressure
+    solver of an arm)."""
     from alloy_b200.solvers.sph.testing import batched_worlds, dam_break, large_dam_break, pour_bowls
 
     if name == "large_dam_break":
-        return large_dam_break(device=device)
+        return large_dam_break(device=device, **cfg_kw)
     if name == "batched_worlds":
-        return batched_worlds(device=device)
+        return batched_worlds(device=device, **cfg_kw)
     if name == "pour_bowls":
-        return pour_bowls(worlds=256 if cpu_sample else 4096, device=device)
-    return dam_break(device=device)
+        return pour_bowls(worlds=256 if cpu_sample else 4096, device=device, **cfg_kw)
+    return dam_break(device=device, **cfg_kw)
 
 
 class Stepper:
@@ -305,21 +306,24 @@ def run_reference(args):
         "note": "CPU oracle: a C++/OpenMP restatement of the reference's Warp kernels (warp-lang is not installed)"}))
 
 
-def warm_arm(args, dev, judge: bool, rank: int, world: int) -> dict:
-    """The same workload from its start state with the shipped warm-start network: W warm-up steps, K steps timed
-    with CUDA events (graph replay), then 20 steps read back for iterations and the share of solves that kept the
-    learned start. Particle-steps/s at the same tolerances (every world iterates to the same stop test)."""
+def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **cfg_kw) -> dict:
+    """The same workload from its start state with one change: the shipped warm-start network (``judge`` not None:
+    with or without the first-sweep judge) or other solver settings (``cfg_kw``, e.g. the CG pressure solve). W
+    warm-up steps, K steps timed with CUDA events (graph replay), then 20 steps read back for iterations (and the
+    share of solves that kept the learned start). Particle-steps/s at the same tolerances (every world iterates to
+    the same stop test)."""
     import torch
 
     from alloy_b200.solvers.sph import SolverDFSPH
     from alloy_b200.solvers.sph.warmstart import DEFAULT_MODEL, default_model
 
-    full = make_scene(args.workload, dev)
+    full = make_scene(args.workload, dev, **cfg_kw)
     sc = rank_scene(full, args.workload, rank, world, dev)
     sol = SolverDFSPH(sc.model, sc.config)
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
-    sol.set_warm_model(default_model())
-    sol.warm_judging(judge)
+    if judge is not None:
+        sol.set_warm_model(default_model())
+        sol.warm_judging(judge)
     run = Stepper(sol, sc, sc.model.state(), sc.model.state())
     stream = torch.cuda.current_stream(dev)
     run(args.warmup)
@@ -342,11 +346,13 @@ def warm_arm(args, dev, judge: bool, rank: int, world: int) -> dict:
         err.append(float(r.density_err.max()))
         kept.append(0.5 * float(d["learned_density"].mean() + d["learned_divergence"].mean()))
     ps = 0.5 * (nf0 + nf1) * args.steps
-    return {"value": ps / t, "ms_per_step": 1e3 * t / args.steps, "judge": judge,
-            "model": str(DEFAULT_MODEL.relative_to(ROOT)),
-            "iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean": float(np.mean(it_div)),
-            "density_err_mean_max_over_steps": float(np.max(err)), "learned_start_kept": float(np.mean(kept)),
-            "particle_steps": ps, "seconds": t}
+    out = {"value": ps / t, "ms_per_step": 1e3 * t / args.steps, "pressure_solver": sol.pressure_solver,
+           "iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean": float(np.mean(it_div)),
+           "density_err_mean_max_over_steps": float(np.max(err)), "particle_steps": ps, "seconds": t}
+    if judge is not None:
+        out.update({"judge": judge, "model": str(DEFAULT_MODEL.relative_to(ROOT)),
+                    "learned_start_kept": float(np.mean(kept))})
+    return out
 
 
 T_START = time.perf_counter()
@@ -500,10 +506,12 @@ def run_b200(args):
     warm = {}
     if not args.no_warm:
         del sol
-        run = None  # the plain solver's memory goes back before the warm-start arms build theirs
-        for judge in (True, False):
-            note(f"warm-start arm (judge {judge})")
-            r = warm_arm(args, dev, judge, rank, world)
+        run = None  # the plain solver's memory goes back before the other arms build theirs
+        arms = [("warm_started", {"judge": True}), ("warm_started_unjudged", {"judge": False}),
+                ("cg", {"pressure_solver": "cg"})]
+        for key, kw in arms:
+            note(f"arm {key}")
+            r = variant_arm(args, dev, rank, world, **kw)
             tw = torch.tensor([r["seconds"]], dtype=torch.float64, device=dev)
             pw = torch.tensor([r["particle_steps"]], dtype=torch.float64, device=dev)
             if world > 1:
@@ -513,7 +521,7 @@ def run_b200(args):
             r["vs_plain"] = r["value"] / value
             for k in ("particle_steps", "seconds"):
                 r.pop(k)
-            warm["warm_started" if judge else "warm_started_unjudged"] = r
+            warm[key] = r
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

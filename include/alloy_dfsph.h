@@ -54,6 +54,9 @@ typedef struct {
   double project_eps;       /* wall projection skin [m] */
   int has_bounds;           /* world_bounds given: escape box */
   double bounds_lo[3], bounds_hi[3];
+  int cg;                   /* pressure iteration: 1 projected preconditioned CG per world (krylov.py:77-318; the
+                               caller sets it only for one particle mass and rest density, solver.py:89-91),
+                               0 relaxed Jacobi */
 } adf_params;
 
 /* The model's particle arrays (Newton Model + sph:* attributes), bound once at creation. */

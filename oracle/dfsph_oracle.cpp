@@ -74,6 +74,7 @@ struct OrcParams {
   double v_sep, relief_speed, project_eps;
   int has_bounds;
   double bounds_lo[3], bounds_hi[3];
+  int cg;  // pressure iteration: 1 projected preconditioned CG (krylov.py), 0 relaxed Jacobi
 };
 
 // Kernel constants in the working precision, derived from double host values exactly as the CUDA side does.
@@ -567,7 +568,10 @@ template <class R> struct Solver {
   }
 
   // pressure.py:264-277: a_i = -sum_j m_j (k_i/rho0_i + k_j/rho0_j) grad W_ij - k_i sum_b dPsi_b
-  V3<R> pressure_accel(int i, const std::vector<R>& kr) const {
+  V3<R> pressure_accel(int i, const std::vector<R>& kr) const { return pressure_accel(i, kr, kappa); }
+
+  // a_i of the pressure field whose kappa / rho0 is kr and whose kappa is kvec (slot term)
+  V3<R> pressure_accel(int i, const std::vector<R>& kr, const std::vector<R>& kvec) const {
     const V3<R> xi = q[i];
     R ki = kr[i];
     V3<R> a{R(0), R(0), R(0)};
@@ -583,7 +587,7 @@ template <class R> struct Solver {
       a.z = fma_(-cF, rv.z, a.z);
     }
     if (slot_on[i]) {
-      R k = kappa[i];
+      R k = kvec[i];
       a.x = fma_(-k, slot_g[i].x, a.x);
       a.y = fma_(-k, slot_g[i].y, a.y);
       a.z = fma_(-k, slot_g[i].z, a.z);
@@ -609,6 +613,24 @@ template <class R> struct Solver {
     }
   }
 
+  // pressure.py:294-310: Ar_i of the accelerations in acc (the matrix-free product, before the compliance term)
+  R accel_divergence(int i) const {
+    const V3<R> xi = q[i], ai = acc[i];
+    R inv_r0 = R(1) / R(rho0[i]);
+    R ar = R(0);
+    const int* row = &nbr[(size_t)i * K];
+    for (int k = 0; k < cnt[i]; ++k) {
+      int j = row[k];
+      V3<R> rv = sub(xi, q[j]);
+      R Wv, F;
+      wf(kc, dot_plain(rv, rv), Wv, F);
+      R aF = (R(mass[j]) * inv_r0) * F;
+      ar = fma_(aF, dotf(sub(ai, acc[j]), rv), ar);
+    }
+    if (slot_on[i]) ar = ar + dotf(ai, slot_g[i]);
+    return ar;
+  }
+
   // pressure.py:294-352
   void jacobi_pass(bool div, R dt) {
     const R omega = R(P.omega), min_nb = R(P.min_nb);
@@ -618,19 +640,7 @@ template <class R> struct Solver {
     for (int i = 0; i < n; ++i) {
       if (!is_fluid(i)) { err[i] = R(0); continue; }
       if (converged[world[i]]) continue;
-      const V3<R> xi = q[i], ai = acc[i];
-      R inv_r0 = R(1) / R(rho0[i]);
-      R ar = R(0);
-      const int* row = &nbr[(size_t)i * K];
-      for (int k = 0; k < cnt[i]; ++k) {
-        int j = row[k];
-        V3<R> rv = sub(xi, q[j]);
-        R Wv, F;
-        wf(kc, dot_plain(rv, rv), Wv, F);
-        R aF = (R(mass[j]) * inv_r0) * F;
-        ar = fma_(aF, dotf(sub(ai, acc[j]), rv), ar);
-      }
-      if (slot_on[i]) ar = ar + dotf(ai, slot_g[i]);
+      R ar = accel_divergence(i);
       ar = fma_(-reg[i], kappa[i], ar);
       ar = ar * dtn;
       R s = div ? -src[i] : R(1) - src[i];
@@ -646,6 +656,159 @@ template <class R> struct Solver {
         e = e * dt;
       }
       err[i] = e;
+    }
+  }
+
+  // ---------------------------------------------------------------- projected preconditioned CG (krylov.py)
+  // One CG per world on the bound-constrained DFSPH system w = A k - b, k >= k_lo (krylov.py:1-17). Operations
+  // follow krylov.py:77-318 kernel by kernel; a + b c updates are fused (fma), dot products are the per-world
+  // float64 sums of world_sum in particle order.
+  std::vector<R> cg_pd, cg_pdr, cg_z, cg_w, cg_ap, cg_corr, cg_corrr, pair_x, pair_y;
+  std::vector<int> cg_act, cg_restart;
+  std::vector<double> cg_rz, cg_step, sum_x, sum_y;
+  std::vector<float> cg_emax;
+
+  bool cg_skip(int i, bool gated) const {
+    const int w = world[i];
+    return converged[w] != 0 || (gated && cg_restart[w] == 0);
+  }
+
+  // krylov.py:71-80: acc = pressure acceleration of the field vec (vr = vec / rho0)
+  void cg_accel(const std::vector<R>& vec, const std::vector<R>& vr, bool gated) {
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) { acc[i] = {R(0), R(0), R(0)}; continue; }
+      if (cg_skip(i, gated)) continue;
+      acc[i] = pressure_accel(i, vr, vec);
+    }
+  }
+
+  // krylov.py:83-101: out (+)= A vec (- b); pair.x = vec_i (A vec)_i
+  void cg_apply(bool div, R dt, const std::vector<R>& vec, std::vector<R>& out, bool gated, bool bias,
+                bool accumulate) {
+    const R scale = div ? dt : dt * dt;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) { out[i] = R(0); pair_x[i] = R(0); pair_y[i] = R(0); continue; }
+      if (cg_skip(i, gated)) continue;
+      R t = fma_(-reg[i], vec[i], accel_divergence(i));
+      R v = -(scale * t);
+      pair_x[i] = vec[i] * v;
+      pair_y[i] = R(0);
+      if (bias) v = v - (div ? src[i] : src[i] - R(1));
+      if (accumulate) v = v + out[i];
+      out[i] = v;
+    }
+  }
+
+  void cg_sums(bool with_max) {
+    world_sum<R>(W, ws.data(), pair_x.data(), sum_x.data(), nullptr);
+    world_sum<R>(W, ws.data(), pair_y.data(), sum_y.data(), with_max ? cg_emax.data() : nullptr);
+  }
+
+  void cg_solve(bool div, R dt, float tol, float tol_max, int& n_unconv) {
+    const R scale = div ? dt : dt * dt;
+    const R min_nb = R(P.min_nb);
+    auto zr = [&](std::vector<R>& a) { a.assign(n, R(0)); };
+    zr(cg_pd); zr(cg_pdr); zr(cg_z); zr(cg_w); zr(cg_ap); zr(cg_corr); zr(cg_corrr); zr(pair_x); zr(pair_y);
+    cg_act.assign(n, 0);
+    cg_restart.assign(W, 0);
+    cg_rz.assign(W, 0.0); cg_step.assign(W, 0.0); sum_x.assign(W, 0.0); sum_y.assign(W, 0.0);
+    cg_emax.assign(W, 0.0f);
+    // krylov.py:278-285 init: w = A k - b, active set, z = M^-1 r, p = z, r.z
+    cg_accel(kappa, kr, false);
+    cg_apply(div, dt, kappa, cg_w, false, true, false);
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i)) continue;
+      const bool a = kappa[i] > lower[i] || cg_w[i] < R(0);
+      const R zi = a ? ((-cg_w[i]) * alpha[i]) / scale : R(0);
+      cg_act[i] = a ? 1 : 0;
+      cg_z[i] = zi;
+      cg_pd[i] = zi;
+      cg_pdr[i] = zi / R(rho0[i]);
+      pair_x[i] = -cg_w[i] * zi;
+      pair_y[i] = R(0);
+    }
+    cg_sums(false);
+    for (int w = 0; w < W; ++w) { cg_rz[w] = sum_x[w]; cg_restart[w] = 0; }
+    int guard = 0;
+    while (n_unconv > 0 && guard++ < 100000) {
+      // krylov.py:287-290: Ap and p.Ap
+      cg_accel(cg_pd, cg_pdr, false);
+      cg_apply(div, dt, cg_pd, cg_ap, false, false, false);
+      cg_sums(false);
+      // krylov.py:146-170: k += a p on F, projected; w += a Ap
+      for (int i = 0; i < n; ++i) {
+        if (!is_fluid(i)) { cg_corr[i] = R(0); cg_corrr[i] = R(0); continue; }
+        const int w = world[i];
+        if (converged[w]) continue;
+        double pap = sum_x[w];
+        const R a = R(pap > 1.0e-30 ? cg_rz[w] / pap : 0.0);
+        R c = R(0);
+        if (cg_act[i]) {
+          R k = fma_(a, cg_pd[i], kappa[i]);
+          if (k < lower[i]) {
+            c = lower[i] - k;
+            k = lower[i];
+            cg_act[i] = 0;
+            cg_restart[w] += 1;
+          }
+          kappa[i] = k;
+          kr[i] = k / R(rho0[i]);
+        }
+        cg_corr[i] = c;
+        cg_corrr[i] = c / R(rho0[i]);
+        cg_w[i] = fma_(a, cg_ap[i], cg_w[i]);
+      }
+      // krylov.py:292: w += A c in worlds where something was clamped
+      cg_accel(cg_corr, cg_corrr, true);
+      cg_apply(div, dt, cg_corr, cg_w, true, false, true);
+      // krylov.py:173-204: activation, z, error
+      for (int i = 0; i < n; ++i) {
+        if (!is_fluid(i)) { pair_x[i] = R(0); pair_y[i] = R(0); err[i] = R(0); continue; }
+        const int w = world[i];
+        if (converged[w]) continue;
+        const R wv = cg_w[i];
+        if (!cg_act[i] && wv < R(0)) { cg_act[i] = 1; cg_restart[w] += 1; }
+        const R zi = cg_act[i] ? ((-wv) * alpha[i]) / scale : R(0);
+        cg_z[i] = zi;
+        R e = maxr(-wv, R(0));
+        if (kappa[i] > lower[i]) e = std::fabs(wv);
+        if (div) {
+          if (neff[i] < min_nb) e = R(0);
+          e = e * dt;
+        }
+        err[i] = e;
+        pair_x[i] = -wv * zi;
+        pair_y[i] = e;
+      }
+      cg_sums(true);
+      // krylov.py:207-233: stop test, beta
+      n_unconv = 0;
+      for (int w = 0; w < W; ++w) {
+        if (converged[w]) continue;
+        int it = iters[w] + 1;
+        iters[w] = it;
+        const double rz_new = sum_x[w];
+        float mean = (float)(sum_y[w] / std::max(n_active[w], 1.0));
+        err_mean[w] = mean;
+        double beta = 0.0;
+        if (cg_restart[w] == 0 && cg_rz[w] > 1.0e-30) beta = rz_new / cg_rz[w];
+        cg_restart[w] = 0;
+        cg_rz[w] = rz_new;
+        cg_step[w] = beta;
+        if ((it >= P.min_it && mean <= tol && cg_emax[w] <= tol_max) || it >= P.max_it) converged[w] = 1;
+        else n_unconv++;
+      }
+      // krylov.py:236-246: p = z + beta p on F
+      for (int i = 0; i < n; ++i) {
+        if (!is_fluid(i)) continue;
+        const int w = world[i];
+        if (converged[w]) continue;
+        const R pd = cg_act[i] ? fma_(R(cg_step[w]), cg_pd[i], cg_z[i]) : R(0);
+        cg_pd[i] = pd;
+        cg_pdr[i] = pd / R(rho0[i]);
+      }
     }
   }
 
@@ -666,7 +829,8 @@ template <class R> struct Solver {
     std::vector<double> esum(W);
     std::vector<float> emax(W);
     int guard = 0;
-    while (n_unconv > 0 && guard++ < 100000) {
+    if (P.cg) cg_solve(div, dt, tol, tol_max, n_unconv);
+    while (!P.cg && n_unconv > 0 && guard++ < 100000) {
       accel_pass();
       jacobi_pass(div, dt);
       world_sum<R>(W, ws.data(), err.data(), esum.data(), emax.data());

@@ -40,7 +40,7 @@ class OrcParams(C.Structure):
                 ("divergence_solve", C.c_int), ("two_sided", C.c_int), ("xsph_c", C.c_double),
                 ("capacity", C.c_int), ("v_sep", C.c_double), ("relief_speed", C.c_double),
                 ("project_eps", C.c_double), ("has_bounds", C.c_int), ("bounds_lo", C.c_double * 3),
-                ("bounds_hi", C.c_double * 3)]
+                ("bounds_hi", C.c_double * 3), ("cg", C.c_int)]
 
 
 def params_from_config(cfg) -> OrcParams:
@@ -133,6 +133,10 @@ class Oracle:
                       self.wall_vol, np.ascontiguousarray(a["gravity"], np.float32).reshape(-1)]
         ws, m, r0, fl, ph, wo, wv, g = self._keep
         self.params = params_from_config(cfg)
+        from alloy_b200.solvers.sph.config import PHASE_HELD, PHASE_SPARE, uniform_layout
+
+        sph = (a["phase"] >= PHASE_SPARE) | (a["phase"] == PHASE_HELD)
+        self.params.cg = int(cfg.pressure_solver == "cg" and uniform_layout(a["mass"][sph], a["rest_density"][sph]))
         self.h = self.L.orc_create(C.byref(self.params), n, W, _p(ws, C.c_int), _p(m, C.c_float), _p(r0, C.c_float),
                                    _p(fl, C.c_int), ph.ctypes.data, _p(wo, C.c_int), _p(wv, C.c_float),
                                    _p(g, C.c_float), int(f64))

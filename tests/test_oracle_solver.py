@@ -185,3 +185,24 @@ def test_seeded_blowup_reaches_speed_fail():
     assert peak > 20.0
     with pytest.raises(ValueError, match="jacobi_omega"):
         cfg.validate()
+
+
+def test_cg_needs_far_fewer_iterations_than_jacobi_on_a_deep_column():
+    """krylov.py:1-9: relaxed Jacobi needs O(N^2) iterations for N layers, CG O(N). A 40-layer column at a tight
+    tolerance: every CG solve converges, in far fewer iterations than Jacobi (which hits max_iterations)."""
+    totals = {}
+    for solver in ("jacobi", "cg"):
+        sc = dam_break(counts=(6, 6, 40), box=(0.12, 0.12, 1.0), pressure_solver=solver, max_density_error=1e-4,
+                       max_divergence_error=1e-4, max_iterations=200)
+        o = Oracle(sc.model.host(), sc.config, threads=4)
+        assert o.params.cg == (solver == "cg")
+        its = []
+        for _ in range(10):
+            o.step(sc.dt)
+            r = o.report()
+            its.append(int(r["iters_divergence"][0]) + int(r["iters_density"][0]))
+            if solver == "cg":
+                assert r["iters_divergence"][0] < 200 and r["iters_density"][0] < 200
+                assert r["density_err"][0] <= 1e-4
+        totals[solver] = sum(its)
+    assert totals["cg"] * 3 < totals["jacobi"], totals
