@@ -20,7 +20,8 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_profile_read", "adf_list_stats", "adf_world_sum_noalloc", "adf_set_graphs", "adf_mlp_create",
            "adf_mlp_destroy", "adf_mlp_set_params", "adf_mlp_get_params", "adf_mlp_forward", "adf_mlp_gradient",
            "adf_mlp_train_step", "adf_mlp_status", "adf_set_warm_model", "adf_set_feature_recording",
-           "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs", "adf_add_emitters")
+           "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs", "adf_add_emitters",
+           "adf_prime")
 TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
@@ -84,6 +85,7 @@ def lib() -> C.CDLL:
     L.adf_add_emitter.argtypes = [P, i, vp, vp, i, vp, C.c_float, vp, i]
     L.adf_set_emitter_pool.argtypes = [P, i, vp, i]
     L.adf_add_emitters.argtypes = [P, i, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.adf_prime.argtypes = [P, vp, vp, C.c_double, C.c_double, i, vp, vp]
     L.adf_emitter_state.argtypes = [P, vp, vp]
     L.adf_set_emitter_enabled.argtypes = [P, i, i]
     L.adf_add_sink.argtypes = [P, i, vp, vp]

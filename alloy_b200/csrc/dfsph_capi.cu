@@ -1181,6 +1181,51 @@ int adf_set_warm_model(adf_solver* s, const adf_mlp* m, const float* norm) {
   return ADF_OK;
 }
 
+int adf_prime(adf_solver* s, const float* q, const float* qd, double dt, double tol, int max_it, int32_t* iters,
+              void* stream) {
+  if (!s || !q || !qd) return fail(ADF_ERR_VALUE, "adf_prime: null argument");
+  if (!(dt > 0.0) || !(tol > 0.0) || max_it < 1) return fail(ADF_ERR_VALUE, "adf_prime: dt, tol and max_it must be > 0");
+  if (iters) *iters = 0;
+  if (s->n == 0) return ADF_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaSetDevice(s->device));
+  DevP P = s->d;
+  P.q = const_cast<float*>(q);  // read only: the sort gathers from them; nothing is written back
+  P.qd = const_cast<float*>(qd);
+  P.f_ext = nullptr;
+  P.dt = (float)dt;
+  P.n_sinks = 0;
+  P.min_nb = 0.0f;
+  P.max_it = max_it;
+  int rc = prepare(s, P, st);
+  if (rc) return rc;
+  run_tk(s, TK_XSPH, st, P);  // the velocity one gravity step adds (no pressure guess yet)
+  std::swap(P.vel, P.vel2);
+  const adf_params saved = s->prm;
+  const bool warm = s->warm_on, rec = s->feat_rec;
+  s->prm.tol_div = tol;
+  s->prm.max_it = max_it;
+  s->prm.warm_div = 1.0;
+  s->prm.max_error_factor = 1.0e9;
+  s->warm_on = s->feat_rec = false;
+  rc = solve(s, P, 0, dt, st, false);
+  s->prm = saved;
+  s->warm_on = warm;
+  s->feat_rec = rec;
+  if (rc) return rc;
+  LAUNCH(s, k_prime_gather, blocks(s->n), BLOCK, st, P);
+  LAUNCH(s, k_prime_store, blocks(s->n), BLOCK, st, s->n, (float)dt, P.kv, P.kd);
+  rc = check_launch();
+  if (rc) return rc;
+  if (iters) {
+    std::vector<int> it(std::max(s->W, 1), 0);
+    CK(cudaMemcpyAsync(it.data(), s->iters_div, sizeof(int) * s->W, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int w = 0; w < s->W; ++w) *iters = std::max(*iters, it[w]);
+  }
+  return ADF_OK;
+}
+
 int adf_set_autotune(adf_solver* s, int enable) {
   if (!s) return fail(ADF_ERR_VALUE, "adf_set_autotune: null solver");
   for (int k = 0; k < TK_COUNT; ++k) {

@@ -1703,6 +1703,21 @@ __global__ void k_emit_cursor(const Emit* em, int n_e, const int* emit_now, int*
   if (emit_now[e] != 0) cursor[e] = min(cursor[e] + em[e].n_layer, em[e].pool_size);
 }
 
+// prime.py:80-85: the solved divergence warm starts back in the caller's order, then kd = kv dt and kv = 0 for every
+// particle (the density solve of the first step starts from the hydrostatic pressure).
+__global__ void k_prime_gather(DevP P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  P.kv[P.id_of[p]] = P.kv_s[p];
+}
+
+__global__ void k_prime_store(int n, float dt, float* kv, float* kd) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  kd[i] = kv[i] * dt;
+  kv[i] = 0.0f;
+}
+
 // ------------------------------------------------------------------------------------------------- misc
 __global__ void k_wall_volume(int n, const int32_t* flags, const float* radius, float* wall_vol) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -110,6 +110,37 @@ def _xform7(region) -> np.ndarray:
     return x
 
 
+def hydrostatic_guess(solver, state) -> np.ndarray:
+    """k_i = |g| (z_top - z_i + r) per (world, horizontal 2r bin) column of active liquid, measured along gravity: the
+    initial guess ``prime`` refines (prime.py:20-49; k = p / rho0 [m^2/s^2]). Host float64, float32 result."""
+    n = solver.n
+    out = np.zeros(max(n, 1), dtype=np.float32)
+    m = solver.model
+    q = _host(state.particle_q).astype(np.float64).reshape(-1, 3)
+    act = (_host(m.sph.phase) >= 1) & ((_host(m.particle_flags) & _ACTIVE) != 0)
+    world = _host(m.particle_world)
+    grav = _host(m.gravity).astype(np.float64).reshape(-1, 3)
+    sp = solver.config.spacing
+    for w in np.unique(world[act]):
+        g = grav[w]
+        gn = float(np.linalg.norm(g))
+        if gn == 0.0:
+            continue
+        up = -g / gn
+        sel = np.nonzero(act & (world == w))[0]
+        z = q[sel] @ up
+        e1 = np.cross(up, [1.0, 0.0, 0.0] if abs(up[0]) < 0.9 else [0.0, 1.0, 0.0])
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(up, e1)
+        key = np.stack([np.floor(q[sel] @ e1 / sp), np.floor(q[sel] @ e2 / sp)], 1).astype(np.int64)
+        _, inv = np.unique(key, axis=0, return_inverse=True)
+        inv = inv.reshape(-1)
+        top = np.full(inv.max() + 1, -np.inf)
+        np.maximum.at(top, inv, z)
+        out[sel] = (gn * np.maximum(top[inv] - z + 0.5 * sp, 0.0)).astype(np.float32)
+    return out[:n]
+
+
 class SolverDFSPH:
     """Divergence-free SPH (Bender & Koschier 2017) on B200: sorted-cell neighbour lists, particle walls,
     per-world float64 convergence (module doc)."""
@@ -412,6 +443,22 @@ class SolverDFSPH:
         return int(nf[0]), int(ne[0])
 
     # ------------------------------------------------------------------------------------------------- control
+    def prime(self, state, dt: float, tol: float = 1.0e-6, max_iterations: int = 2000) -> int:
+        """Give a fluid at rest its hydrostatic pressure before the first step (solver.py:369-372, prime.py:52-87):
+        the hydrostatic guess per liquid column, refined by one divergence solve of the velocity a gravity step
+        adds, becomes the first density solve's warm start. ``state`` is not changed. Returns the iterations."""
+        if self.n == 0:
+            return 0
+        guess = hydrostatic_guess(self, state)
+        kv = torch.as_tensor(guess * np.float32(dt), dtype=torch.float32, device=self.device)
+        _lib.check(self._lib.adf_set_warm_starts(self._h, kv.data_ptr(), self._kd.data_ptr(), self._stream()),
+                   "prime")
+        it = np.zeros(1, np.int32)
+        _lib.check(self._lib.adf_prime(self._h, _ptr(state.particle_q, torch.float32, self.n, "particle_q"),
+                                       _ptr(state.particle_qd, torch.float32, self.n, "particle_qd"), float(dt),
+                                       float(tol), int(max_iterations), it.ctypes.data, self._stream()), "prime")
+        return int(it[0])
+
     def reset(self, state=None, world_mask=None, flags: int | None = None) -> None:
         """Masked worlds (all when None) back to their build-time SPH configuration (solver.py:353-362)."""
         del state, flags

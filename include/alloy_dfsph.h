@@ -129,6 +129,14 @@ int adf_set_autotune(adf_solver* solver, int enable);
  * gathers in flight, and the winning trial's milliseconds (-1 if not tuned). */
 int adf_tuned_configs(adf_solver* solver, int32_t* block, int32_t* nb, float* ms);
 
+/* Replaces SolverDFSPH.prime (solver.py:369-372, prime.py:52-87): with the divergence warm starts holding the
+ * hydrostatic guess x dt (adf_set_warm_starts), one divergence solve of the velocity a gravity step adds to the
+ * state (tolerance tol, up to max_it iterations, plain start 1 x the guess, no neighbour floor, no max-error test);
+ * the state is not changed; afterwards the density warm start is kd = kv dt and kv = 0. iters (host, may be NULL)
+ * receives the largest per-world iteration count; synchronises `stream` when iters is given. Not capturable. */
+int adf_prime(adf_solver* solver, const float* q, const float* qd, double dt, double tol, int max_it, int32_t* iters,
+              void* stream);
+
 /* Replaces SolverDFSPH.density_ratio (solver.py:386-393): density ratio and active mask of every particle of the
  * state (device [n] outputs, 0 for non-liquid particles) from fresh lists and wall slots. */
 int adf_density_ratio(adf_solver* solver, const float* q, const float* qd, float* ratio_out, float* active_out,

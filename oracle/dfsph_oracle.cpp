@@ -1044,6 +1044,33 @@ template <class R> struct Solver {
     }
   }
 
+  // prime.py:52-87: the hydrostatic pressure of a fluid at rest. The caller stores the hydrostatic guess as the
+  // divergence warm start (kv = guess dt); one divergence solve (tolerance tol, up to max_it iterations, plain
+  // start 1 x kv, no neighbour floor, no max-error test) of the velocity one gravity step adds; velocities are left
+  // unchanged; the density warm start becomes kd = kv dt and kv is cleared. Returns the iterations used.
+  int prime(double dt_d, double tol, int max_it) {
+    R dt = R(dt_d);
+    const std::vector<V3<R>> v_saved = v;
+    const OrcParams saved = P;
+    prepare_density();
+    nonpressure(dt);
+    P.tol_div = tol;
+    P.max_it = max_it;
+    P.warm_div = 1.0;
+    P.min_nb = 0.0;
+    P.max_error_factor = 1.0e9;
+    solve(true, dt, dt_d);
+    P = saved;
+    v = v_saved;
+    for (int i = 0; i < n; ++i) {
+      kd[i] = kv[i] * dt;
+      kv[i] = R(0);
+    }
+    int it = 0;
+    for (int w = 0; w < W; ++w) it = std::max(it, iters_div[w]);
+    return it;
+  }
+
   // solver.py:218-268
   void step(double dt_d) {
     R dt = R(dt_d);
@@ -1148,6 +1175,11 @@ void orc_get_flags_phase(void* hp, int* flags, int8_t* phase) {
   });
 }
 int orc_step(void* hp, double dt) { DISPATCH(s.step(dt)); return 0; }
+int orc_prime(void* hp, double dt, double tol, int max_it) {
+  int it = 0;
+  DISPATCH(it = s.prime(dt, tol, max_it));
+  return it;
+}
 void orc_prepare_density(void* hp) { DISPATCH(s.prepare_density()); }
 
 // name: ratio alpha neff active reg src kappa err slot_psi slot_phi

@@ -93,6 +93,7 @@ def lib():
         L.orc_get_warm.argtypes = [P, fp, fp]
         L.orc_get_flags_phase.argtypes = [P, ip, C.c_void_p]
         L.orc_step.argtypes = [P, C.c_double]
+        L.orc_prime.argtypes = [P, C.c_double, C.c_double, C.c_int]
         L.orc_get_field.argtypes = [P, C.c_char_p, fp]
         L.orc_get_slot_on.argtypes = [P, ip]
         L.orc_get_lists.argtypes = [P, ip, ip]
@@ -196,6 +197,10 @@ class Oracle:
 
     def step(self, dt: float):
         self.L.orc_step(self.h, float(dt))
+
+    def prime(self, dt: float, tol: float = 1.0e-6, max_iterations: int = 2000) -> int:
+        """prime.py:52-87 after the caller set kv to the hydrostatic guess x dt; returns the iterations."""
+        return int(self.L.orc_prime(self.h, float(dt), float(tol), int(max_iterations)))
 
     def prepare_density(self):
         self.L.orc_prepare_density(self.h)

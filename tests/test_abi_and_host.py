@@ -105,3 +105,20 @@ def test_world_sharding_balances_and_keeps_world_order():
     ws = arr["world_start"]
     np.testing.assert_array_equal(sub["q"], np.concatenate([arr["q"][ws[1]:ws[2]], arr["q"][ws[3]:ws[4]]]))
     assert sub["world_start"].tolist() == [0, ws[2] - ws[1], ws[2] - ws[1] + ws[4] - ws[3]]
+
+
+def test_hydrostatic_guess_is_gravity_times_depth():
+    """prime.py:20-49: k_i = |g| (z_top - z_i + r) per horizontal 2r column of liquid (here every column is full, so
+    z_top is the block's top layer)."""
+    import types
+
+    from alloy_b200.solvers.sph.solver import hydrostatic_guess
+    from alloy_b200.solvers.sph.testing import dam_break
+
+    sc = dam_break(counts=(4, 3, 10), box=(0.2, 0.2, 0.4), jitter=0.0)
+    fake = types.SimpleNamespace(n=sc.model.particle_count, model=sc.model, config=sc.config)
+    g = hydrostatic_guess(fake, sc.model.state())
+    q = sc.model.host()["q"][: sc.fluid_count].astype(np.float64)
+    expect = 9.81 * (q[:, 2].max() - q[:, 2] + 0.5 * sc.config.spacing)
+    np.testing.assert_allclose(g[: sc.fluid_count], expect, rtol=1e-6)
+    assert (g[sc.fluid_count:] == 0).all()
