@@ -786,6 +786,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.cw, W);
   rc |= s->alloc(&d.cseg, (size_t)W + 1);
   rc |= s->alloc(&d.n_cw, 1);
+  rc |= s->alloc(&d.iter_work, 1);
   rc |= s->alloc(&chunk_world, cb.size());
   s->cg = p.cg != 0;
   if (s->cg) {
@@ -875,6 +876,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
                     s->den_err_max, d.emax};
   for (void* z : zero_w) CKC(cudaMemset(z, 0, 4 * W));
   CKC(cudaMemset(d.mass_out, 0, 8 * W));
+  CKC(cudaMemset(d.iter_work, 0, sizeof(unsigned long long)));
   CKC(cudaMemset(s->mass_in, 0, 8 * W));
   CKC(cudaMemset(d.n_active, 0, 8 * W));
   std::vector<float> tol(W, (float)p.tol_den);
@@ -1223,6 +1225,16 @@ int adf_prime(adf_solver* s, const float* q, const float* qd, double dt, double 
     CK(cudaStreamSynchronize(st));
     for (int w = 0; w < s->W; ++w) *iters = std::max(*iters, it[w]);
   }
+  return ADF_OK;
+}
+
+int adf_iteration_work(adf_solver* s, int64_t* particles, void* stream) {
+  if (!s || !particles) return fail(ADF_ERR_VALUE, "adf_iteration_work: null argument");
+  CK(cudaSetDevice(s->device));
+  unsigned long long v = 0;
+  CK(cudaMemcpyAsync(&v, s->d.iter_work, sizeof(v), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  *particles = (int64_t)v;
   return ADF_OK;
 }
 

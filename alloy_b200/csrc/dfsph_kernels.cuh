@@ -131,6 +131,7 @@ struct DevP {
   int* cw;          // [W] worlds still iterating, ascending (k_worklist)
   int* cseg;        // [W + 1] first work item of each listed world; cseg[n_cw] = items
   int* n_cw;        // [1] listed worlds
+  unsigned long long* iter_work;  // [1] liquid particles covered by the pressure iterations' work lists so far
   int* converged;
   int* iters;
   float* err_mean;
@@ -1042,17 +1043,21 @@ __global__ void __launch_bounds__(1024) k_worklist(DevP P) {
     carry_s = 0;
   }
   __syncthreads();
+  unsigned long long work = 0;
   for (int w0 = 0; w0 < P.W; w0 += blockDim.x) {
     const int w = w0 + threadIdx.x;
-    int segs = 0;
+    int segs = 0, parts = 0;
     if (w < P.W && !P.converged[w]) {
       const int2 r = P.wrange[w];
       segs = (r.y - r.x + ITEM - 1) / ITEM;
+      parts = r.y - r.x;
     }
     const int on = segs > 0 ? 1 : 0;
-    int tw, ts;
+    int tw, ts, tp;
     const int ow = block_exclusive_scan(on, smem, tw);
     const int os = block_exclusive_scan(segs, smem, ts);
+    block_exclusive_scan(parts, smem, tp);
+    work += (unsigned long long)tp;
     const int cw0 = carry_w, cs0 = carry_s;
     if (on) {
       P.cw[cw0 + ow] = w;
@@ -1068,6 +1073,7 @@ __global__ void __launch_bounds__(1024) k_worklist(DevP P) {
   if (threadIdx.x == 0) {
     P.cseg[carry_w] = carry_s;
     *P.n_cw = carry_w;
+    if (P.iter_work && work) atomicAdd(P.iter_work, work);  // the iteration this list drives, if it runs
   }
 }
 

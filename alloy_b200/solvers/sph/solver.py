@@ -435,6 +435,13 @@ class SolverDFSPH:
         _lib.check(self._lib.adf_profile_read(self._h, ms.ctypes.data, cnt.ctypes.data), "profile_read")
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.PROF_KINDS)}
 
+    def iteration_work(self) -> int:
+        """Liquid particles processed by the Jacobi iterations so far (their work lists cover the worlds still
+        iterating)."""
+        v = np.zeros(1, np.int64)
+        _lib.check(self._lib.adf_iteration_work(self._h, v.ctypes.data, self._stream()), "iteration_work")
+        return int(v[0])
+
     def list_stats(self) -> tuple[int, int]:
         """(liquid particles, neighbour-row entries) of the last list build."""
         nf = np.zeros(1, np.int32)

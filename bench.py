@@ -48,11 +48,17 @@ def parse():
     ap.add_argument("--workload", choices=("large_dam_break", "dam_break", "batched_worlds", "pour_bowls"),
                     default="large_dam_break")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--worlds", type=int, default=None,
+                    help="worlds of batched_worlds / pour_bowls (default: the workload's 256 / 4,096; fewer only for "
+                         "profiling a smaller instance of the same worlds)")
     ap.add_argument("--no-warm", action="store_true", help="skip the learned warm-start and CG arms")
     return ap.parse_args()
 
 
 MULTI_WORLD = ("batched_worlds", "pour_bowls")
+
+
+WORLDS = None  # --worlds
 
 
 def make_scene(name: str, device, cpu_sample: bool = False, **cfg_kw):
@@ -64,9 +70,9 @@ def make_scene(name: str, device, cpu_sample: bool = False, **cfg_kw):
     if name == "large_dam_break":
         return large_dam_break(device=device, **cfg_kw)
     if name == "batched_worlds":
-        return batched_worlds(device=device, **cfg_kw)
+        return batched_worlds(worlds=WORLDS or 256, device=device, **cfg_kw)
     if name == "pour_bowls":
-        return pour_bowls(worlds=256 if cpu_sample else 4096, device=device, **cfg_kw)
+        return pour_bowls(worlds=256 if cpu_sample else (WORLDS or 4096), device=device, **cfg_kw)
     return dam_break(device=device, **cfg_kw)
 
 
@@ -358,6 +364,11 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
 T_START = time.perf_counter()
 
 
+def pcg_off(sol) -> bool:
+    """The Jacobi path (whose iterations the library's work counter covers)."""
+    return sol.pressure_solver == "jacobi"
+
+
 def note(msg: str) -> None:
     """Progress of the phases on stderr (the JSON line alone goes to stdout)."""
     print(f"[bench {time.perf_counter() - T_START:7.1f} s] {msg}", file=sys.stderr, flush=True)
@@ -430,8 +441,10 @@ def run_b200(args):
     note("per-kernel timing pass")
     sol.profile(True)
     sol.profile_read()
+    work0 = sol.iteration_work()
     run(args.steps)
     prof = sol.profile_read()
+    iter_work = sol.iteration_work() - work0  # liquid particles the pressure iterations processed
     sol.profile(False)
     psteps = 0.5 * (nf0 + nf1) * args.steps
     tmax = torch.tensor([t], dtype=torch.float64, device=dev)
@@ -487,10 +500,16 @@ def run_b200(args):
            "solve_init": 80.0 + 2.0 * nbar, "apply": 60.0 + 2.0 * nbar, "xsph": 68.0 + 2.0 * nbar,
            "lists": 44.0 + 2.0 * nbar}
     total_ms = sum(v[0] for v in prof.values())
+    # liquid particles per launch: every liquid particle, except the pressure iterations', whose work lists cover
+    # only the worlds still iterating (counted by the library for the timing pass)
+    per_launch = {k: float(nf) for k in alg}
+    if prof["jacobi"][1] and pcg_off(sol):
+        for k in ("jacobi", "accel"):
+            per_launch[k] = iter_work / prof[k][1]
     dom = max(alg, key=lambda k: prof[k][0])
     ms, cnt = prof[dom]
     per_launch_s = ms * 1e-3 / max(cnt, 1)
-    achieved = alg[dom] * nf / per_launch_s / 1e9
+    achieved = alg[dom] * per_launch[dom] / per_launch_s / 1e9
     traffic = dram_traffic(args.workload).get(dom)
     shares = {k: round(v[0] / total_ms, 4) for k, v in prof.items() if total_ms > 0}
     per_kernel = {}
@@ -498,10 +517,10 @@ def run_b200(args):
         kms, kn = prof[k]
         if kn:
             us = kms * 1e3 / kn
-            gbs = b_alg * nf / (us * 1e-6) / 1e9
+            gbs = b_alg * per_launch[k] / (us * 1e-6) / 1e9
             per_kernel[k] = {"launches_per_step": kn / args.steps, "avg_launch_us": round(us, 2),
-                             "alg_bytes_per_particle": round(b_alg, 2), "achieved_gbs": round(gbs, 1),
-                             "frac": round(gbs / pk["hbm_gbs"], 4)}
+                             "alg_bytes_per_particle": round(b_alg, 2), "particles_per_launch": round(per_launch[k]),
+                             "achieved_gbs": round(gbs, 1), "frac": round(gbs / pk["hbm_gbs"], 4)}
 
     warm = {}
     if not args.no_warm:
@@ -546,6 +565,7 @@ def run_b200(args):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
                          "peak_src": pk["src"], "alg_bytes_per_particle": alg[dom], "mean_neighbours": nbar,
+                         "particles_per_launch": per_launch[dom],
                          "avg_launch_us": per_launch_s * 1e6, "launches": cnt},
             "kernel_time_share": shares, "kernel_ms_per_step": total_ms / args.steps, "kernels": per_kernel,
             "solver_stats": {"iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean":
@@ -559,7 +579,9 @@ def run_b200(args):
 
 
 def main():
+    global WORLDS
     args = parse()
+    WORLDS = args.worlds
     if args.impl == "reference":
         run_reference(args)
     else:

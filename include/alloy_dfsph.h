@@ -284,6 +284,11 @@ int64_t adf_kernel_launches(const adf_solver* solver);
 int adf_profile_enable(adf_solver* solver, int enable);
 int adf_profile_read(adf_solver* solver, double* ms, int64_t* launches);
 
+/* Liquid particles covered by the Jacobi iterations' work lists since creation (each iteration's acceleration and
+ * update kernels process the liquid of the worlds still iterating; benchmarks divide by launches for the particles
+ * per launch). Host output; synchronises `stream`. */
+int adf_iteration_work(adf_solver* solver, int64_t* particles, void* stream);
+
 /* Liquid particle count and neighbour-row entries of the last list build (host outputs; synchronises `stream`). */
 int adf_list_stats(adf_solver* solver, int32_t* fluid, int64_t* entries, void* stream);
 
