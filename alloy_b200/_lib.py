@@ -21,8 +21,8 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_mlp_destroy", "adf_mlp_set_params", "adf_mlp_get_params", "adf_mlp_forward", "adf_mlp_gradient",
            "adf_mlp_train_step", "adf_mlp_status", "adf_set_warm_model", "adf_set_feature_recording",
            "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs", "adf_add_emitters",
-           "adf_prime", "adf_iteration_work")
-TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph")  # ADF_TUNE_KERNELS, in order
+           "adf_prime", "adf_iteration_work", "adf_set_tuned_config")
+TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph", "lists")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
               "apply", "xsph", "finish", "emit", "warm_start")
@@ -87,6 +87,7 @@ def lib() -> C.CDLL:
     L.adf_add_emitters.argtypes = [P, i, vp, vp, vp, vp, vp, vp, vp, vp]
     L.adf_prime.argtypes = [P, vp, vp, C.c_double, C.c_double, i, vp, vp]
     L.adf_iteration_work.argtypes = [P, vp, vp]
+    L.adf_set_tuned_config.argtypes = [P, i, i, i]
     L.adf_emitter_state.argtypes = [P, vp, vp]
     L.adf_set_emitter_enabled.argtypes = [P, i, i]
     L.adf_add_sink.argtypes = [P, i, vp, vp]

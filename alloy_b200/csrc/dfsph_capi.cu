@@ -50,13 +50,17 @@ __global__ void __launch_bounds__(mlp::TILE) k_mlp_warm(DevP P, mlp::Net net) {
 
 // Kernels the autotuner configures (k_apply runs the acceleration loop and takes TK_ACCEL's choice), and the choices:
 // threads per block and the neighbour gathers each thread keeps in flight (NB).
-enum TuneKernel { TK_DENSITY = 0, TK_SOLVE_INIT, TK_ACCEL, TK_JACOBI, TK_XSPH, TK_COUNT };
+// For the list build the "gathers" field holds the particles per warp (32 or 16) and the block is fixed.
+enum TuneKernel { TK_DENSITY = 0, TK_SOLVE_INIT, TK_ACCEL, TK_JACOBI, TK_XSPH, TK_LISTS, TK_COUNT };
 struct TuneCfg {
   int block = BLOCK;
   int nb = NB_DEFAULT;
 };
 constexpr int TUNE_BLOCKS[] = {128, 256};
 constexpr int TUNE_NB[] = {4, 8, 16};
+constexpr TuneCfg LISTS_DEFAULT{32 * LU_WARPS, 32};
+constexpr int TUNE_PPW[] = {32, 16};
+inline TuneCfg default_cfg(int id) { return id == TK_LISTS ? LISTS_DEFAULT : TuneCfg{}; }
 }  // namespace adf
 
 namespace {
@@ -157,6 +161,7 @@ struct adf_solver {
   bool tuned[adf::TK_COUNT] = {};
   bool tune_pending = true, tuning = false;
   float *snap_kappa = nullptr, *snap_kr = nullptr, *snap_err = nullptr;
+  int* snap_ovf = nullptr;
   cudaEvent_t tev[2] = {nullptr, nullptr};
 
   template <class T> int alloc(T** p, size_t count) {
@@ -207,6 +212,10 @@ void launch_tk(adf_solver* s, int id, const TuneCfg& c, cudaStream_t st, const D
     case TK_SOLVE_INIT: NB_DISPATCH(k_solve_init, c.nb, blocks(n, c.block), c.block, st, P); break;
     case TK_ACCEL: NB_DISPATCH(k_accel, c.nb, s->max_items, c.block, st, P); break;
     case TK_JACOBI: NB_DISPATCH(k_jacobi, c.nb, s->max_items, c.block, st, P); break;
+    case TK_LISTS:
+      if (c.nb == 16) k_lists_union<16><<<blocks(n, 16 * LU_WARPS), 32 * LU_WARPS, 0, st>>>(P);
+      else k_lists_union<32><<<blocks(n, 32 * LU_WARPS), 32 * LU_WARPS, 0, st>>>(P);
+      break;
     default: NB_DISPATCH(k_xsph, c.nb, blocks(n, c.block), c.block, st, P); break;
   }
   ++s->launches;
@@ -218,10 +227,16 @@ void launch_tk(adf_solver* s, int id, const TuneCfg& c, cudaStream_t st, const D
 // residual are restored before every trial and after the last, so the tuning step computes exactly an ordinary step.
 void tune_kernel(adf_solver* s, int id, cudaStream_t st, const DevP& P) {
   if (!s->tuning || s->tuned[id]) return;
-  const bool restore = id == TK_JACOBI;
+  const bool restore = id == TK_JACOBI || id == TK_LISTS;
   const size_t nb = sizeof(float) * (size_t)s->n;
   auto copy = [&](bool save) {
     if (!restore) return;
+    if (id == TK_LISTS) {  // the rows are rewritten whole; only the overflow counters accumulate
+      const size_t wb = sizeof(int) * (size_t)std::max(s->W, 1);
+      if (save) cudaMemcpyAsync(s->snap_ovf, P.overflow, wb, cudaMemcpyDeviceToDevice, st);
+      else cudaMemcpyAsync(P.overflow, s->snap_ovf, wb, cudaMemcpyDeviceToDevice, st);
+      return;
+    }
     if (save) {
       cudaMemcpyAsync(s->snap_kappa, P.kappa, nb, cudaMemcpyDeviceToDevice, st);
       cudaMemcpyAsync(s->snap_kr, P.kr, nb, cudaMemcpyDeviceToDevice, st);
@@ -235,9 +250,15 @@ void tune_kernel(adf_solver* s, int id, cudaStream_t st, const DevP& P) {
   copy(true);
   float best = 3.0e38f;
   TuneCfg pick = s->tune[id];
-  for (int block : TUNE_BLOCKS) {
-    for (int nbv : TUNE_NB) {
-      const TuneCfg c{block, nbv};
+  std::vector<TuneCfg> cands;
+  if (id == TK_LISTS) {
+    for (int g : TUNE_PPW) cands.push_back(TuneCfg{32 * LU_WARPS, g});
+  } else {
+    for (int block : TUNE_BLOCKS)
+      for (int nbv : TUNE_NB) cands.push_back(TuneCfg{block, nbv});
+  }
+  {
+    for (const TuneCfg& c : cands) {
       float t = 3.0e38f;
       for (int r = 0; r < 3; ++r) {
         copy(false);
@@ -352,7 +373,7 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   prof_end(s, st);
   prof_begin(s, 1, st);
   if (s->K <= LU_ROW) {
-    LAUNCH(s, k_lists_union, blocks(n, 32 * LU_WARPS), 32 * LU_WARPS, st, P);
+    run_tk(s, TK_LISTS, st, P);
   } else {
     const size_t smem = sizeof(int) * (size_t)s->K * LS_THREADS;
     k_lists_smem<<<blocks(n, LS_THREADS), LS_THREADS, smem, st>>>(P);
@@ -904,6 +925,8 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   CKC(cudaMalloc(&s->snap_kappa, sizeof(float) * n));
   CKC(cudaMalloc(&s->snap_kr, sizeof(float) * n));
   CKC(cudaMalloc(&s->snap_err, sizeof(float) * n));
+  CKC(cudaMalloc(&s->snap_ovf, sizeof(int) * W));
+  s->tune[TK_LISTS] = LISTS_DEFAULT;
   CKC(cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming));
   CKC(cudaDeviceSynchronize());
@@ -934,6 +957,7 @@ void adf_destroy(adf_solver* s) {
     if (e) cudaEventDestroy(e);
   for (float* p : {s->snap_kappa, s->snap_kr, s->snap_err})
     if (p) cudaFree(p);
+  if (s->snap_ovf) cudaFree(s->snap_ovf);
   delete s;
 }
 
@@ -1241,11 +1265,24 @@ int adf_iteration_work(adf_solver* s, int64_t* particles, void* stream) {
 int adf_set_autotune(adf_solver* s, int enable) {
   if (!s) return fail(ADF_ERR_VALUE, "adf_set_autotune: null solver");
   for (int k = 0; k < TK_COUNT; ++k) {
-    s->tune[k] = TuneCfg{};
+    s->tune[k] = default_cfg(k);
     s->tuned[k] = false;
     s->tune_ms[k] = 0.0f;
   }
   s->tune_pending = enable != 0;
+  ++s->table_version;
+  return ADF_OK;
+}
+
+int adf_set_tuned_config(adf_solver* s, int kernel, int block, int nb) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_tuned_config: null solver");
+  if (kernel < 0 || kernel >= TK_COUNT) return fail(ADF_ERR_VALUE, "adf_set_tuned_config: kernel out of range");
+  const bool ok = kernel == TK_LISTS ? (block == 32 * LU_WARPS && (nb == 16 || nb == 32))
+                                     : ((block == 128 || block == 256) && (nb == 4 || nb == 8 || nb == 16));
+  if (!ok) return fail(ADF_ERR_VALUE, "adf_set_tuned_config: not one of the tuner's candidates");
+  s->tune[kernel] = TuneCfg{block, nb};
+  s->tuned[kernel] = true;
+  s->tune_ms[kernel] = 0.0f;
   ++s->table_version;
   return ADF_OK;
 }

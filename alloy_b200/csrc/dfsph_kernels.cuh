@@ -433,6 +433,34 @@ __device__ __forceinline__ void sort32_registers(unsigned (&key)[32]) {
   }
 }
 
+__device__ __forceinline__ void sort16_registers(unsigned (&key)[16]) {
+#pragma unroll
+  for (int k = 2; k <= 16; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const unsigned a = key[i], b = key[l];
+          const unsigned lo = min(a, b), hi = max(a, b);
+          if ((i & k) == 0) {
+            key[i] = lo;
+            key[l] = hi;
+          } else {
+            key[i] = hi;
+            key[l] = lo;
+          }
+        }
+      }
+    }
+  }
+}
+
+// G particles per warp: 32 (one lane per particle), or 16 (lanes l and l + 16 share particle l: the warp's union of
+// neighbourhoods is about a third smaller and each lane tests half of each staged batch; the two halves' sorted runs
+// are merged on write by lane l). The rows are the same either way.
+template <int G>
 __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
   __shared__ unsigned rows[LU_WARPS][LU_ROW][32];  // [warp][entry][lane]: lanes of one entry in distinct banks
   __shared__ __align__(8) float cxs[LU_WARPS][32];  // staged candidates, one coordinate per array so that two
@@ -441,13 +469,15 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
   __shared__ unsigned cid[LU_WARPS][32];
   __shared__ int rbeg[LU_WARPS][LU_MAX_SEGS];     // first sorted index of each candidate range
   __shared__ int roff[LU_WARPS][LU_MAX_SEGS + 1];  // flat offset of each range in the warp's candidate stream
+  static_assert(G == 32 || G == 16, "particles per warp");
   const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
-  const int p0 = (blockIdx.x * LU_WARPS + wq) * 32;
+  const int sub = lane % G, half = lane / G;
+  const int p0 = (blockIdx.x * LU_WARPS + wq) * G;
   const int nf = P.nfw[0];
   if (p0 >= nf) return;
-  const int tend = min(32, nf - p0);
-  const bool valid = lane < tend;
-  const int p = valid ? p0 + lane : p0;
+  const int tend = min(G, nf - p0);
+  const bool valid = sub < tend;
+  const int p = valid ? p0 + sub : p0;
   const int w = P.world_s[p];
   const WorldGrid g = P.grid[w];
   const float4 xi = P.pos[p];
@@ -575,11 +605,12 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
         const float bx = f2_hi(dx), by = f2_hi(dy), bz = f2_hi(dz);
         return (dot_plain(ax, ay, az, ax, ay, az) < h2 ? 1u : 0u) | (dot_plain(bx, by, bz, bx, by, bz) < h2 ? 2u : 0u);
       };
+      const int t0 = half * G;  // this lane's share of the staged batch
       if (nc == 32) {
 #pragma unroll
-        for (int t = 0; t < 32; t += 2) hit |= pair_hits(t) << t;
+        for (int t = 0; t < G; t += 2) hit |= pair_hits(t0 + t) << (t0 + t);
       } else {
-        for (int t = 0; t < nc; t += 2) hit |= pair_hits(t) << t;
+        for (int t = t0; t < min(nc, t0 + G); t += 2) hit |= pair_hits(t) << t;
         hit &= (1u << nc) - 1u;  // nc < 32: drop the stale slot past the last candidate
       }
       while (hit) {
@@ -593,7 +624,7 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       }
       __syncwarp();
     }
-  } else if (valid) {
+  } else if (valid && half == 0) {
     for (int r = 0; r < 9; ++r) {
       const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
       if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
@@ -610,12 +641,30 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       });
     }
   }
-  total = valid ? cnt : 0;
-  cnt = min(total, LU_ROW);
-  const int cmax = __reduce_max_sync(full, (unsigned)total);
-  // run A = entries [0, min(cnt, 32)), run B = entries [32, cnt), each sorted in registers
-  int a_end = min(cnt, 32), b_end = cnt;
-  {
+  const int own = valid ? cnt : 0;                                       // this lane's hits
+  const int other = G == 16 ? __shfl_xor_sync(full, own, 16) : 0;       // its partner lane's (G = 16)
+  total = own + other;
+  const bool writer = valid && half == 0;
+  cnt = min(own, LU_ROW);
+  const int cmax = __reduce_max_sync(full, (unsigned)cnt);
+  // G = 32: run A = entries [0, min(cnt, 32)), run B = entries [32, cnt) of this lane's column; G = 16: run A = this
+  // lane's column, run B = the partner's; each run sorted in registers
+  const bool sel = total > LU_ROW || (G == 16 && (own > 32 || other > 32));
+  int a_end = min(cnt, 32), b_end = cnt, b_begin = 32;
+  if (G == 16) {
+    a_end = min(own, 32);
+    b_end = min(other, 32);
+    b_begin = 0;
+  }
+  if (G == 16 && cmax <= 16) {
+    unsigned key[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) key[k] = k < cnt ? myrow[k * 32] : 0xffffffffu;
+    sort16_registers(key);
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      if (k < cnt) myrow[k * 32] = key[k];
+  } else {
     unsigned key[32];
 #pragma unroll
     for (int k = 0; k < 32; ++k) key[k] = k < cnt ? myrow[k * 32] : 0xffffffffu;
@@ -624,7 +673,7 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
     for (int k = 0; k < 32; ++k)
       if (k < cnt) myrow[k * 32] = key[k];
   }
-  if (cmax > 32) {
+  if (G == 32 && cmax > 32) {
     unsigned key[32];
 #pragma unroll
     for (int k = 0; k < 32; ++k) key[k] = 32 + k < cnt ? myrow[(32 + k) * 32] : 0xffffffffu;
@@ -633,7 +682,8 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
     for (int k = 0; k < 32; ++k)
       if (32 + k < cnt) myrow[(32 + k) * 32] = key[k];
   }
-  if (total > LU_ROW) {
+  __syncwarp();  // the partner's sorted run is read below (G = 16)
+  if (sel && writer) {
     // more candidates than the row buffer: the K lowest ids by repeated scans of this particle's 27 cells
     unsigned last = 0;
     const int kk = min(total, K);
@@ -658,14 +708,15 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       last = best;
     }
     a_end = kk;
-    b_end = 32;
+    b_begin = b_end = 0;
   }
-  // write the merge of the two runs: entry k of the 32 rows is one contiguous 128-byte segment
-  const int m = min(total, K);
+  // write the merge of the two runs: entry k of the rows is one contiguous segment
+  const unsigned* rowb = G == 16 ? &rows[wq][0][lane ^ 16] : myrow;
+  const int m = writer ? min(total, K) : 0;
   const int mmax = __reduce_max_sync(full, (unsigned)m);
-  int ia = 0, ib = 32;
+  int ia = 0, ib = b_begin;
   unsigned va = ia < a_end ? myrow[ia * 32] : 0xffffffffu;
-  unsigned vb = ib < b_end ? myrow[ib * 32] : 0xffffffffu;
+  unsigned vb = ib < b_end ? rowb[ib * 32] : 0xffffffffu;
   for (int k = 0; k < mmax; ++k) {
     const bool take_a = va < vb;
     const unsigned v = take_a ? va : vb;
@@ -675,10 +726,10 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       va = ia < a_end ? myrow[ia * 32] : 0xffffffffu;
     } else {
       ++ib;
-      vb = ib < b_end ? myrow[ib * 32] : 0xffffffffu;
+      vb = ib < b_end ? rowb[ib * 32] : 0xffffffffu;
     }
   }
-  if (valid) {
+  if (writer) {
     P.cnt[p] = m;
     if (total > K) atomicAdd(&P.overflow[w], 1);
   }

@@ -395,6 +395,11 @@ class SolverDFSPH:
         return {name: {"block": int(blk[i]), "nb": int(nb[i]), "ms": float(ms[i])}
                 for i, name in enumerate(_lib.TUNE_KERNELS)}
 
+    def set_tuned_config(self, kernel: str, block: int, nb: int) -> None:
+        """Pin one kernel's launch configuration (a tuner candidate; for "lists", nb = particles per warp)."""
+        _lib.check(self._lib.adf_set_tuned_config(self._h, _lib.TUNE_KERNELS.index(kernel), int(block), int(nb)),
+                   "set_tuned_config")
+
     def warm_judging(self, enable: bool = True) -> None:
         """Judge the learned start by one sweep from both starts (default). Off: the learned start is taken outright
         (a measurement of the network alone; every world still iterates to the same tolerance)."""

@@ -120,11 +120,15 @@ int adf_set_graphs(adf_solver* solver, int enable);
 /* Autotuner (no counterpart in the reference; Warp picks its own launch shapes). enable = 1 (the default at creation):
  * the next adf_step on a stream that is not capturing is a tuning step: it launches its kernels one by one and, the
  * first time each neighbour-loop kernel (density and factor, solve start, pressure acceleration and its application,
- * Jacobi update, XSPH) runs, times every candidate of threads per block {128, 256} x neighbour gathers in flight
- * {4, 8, 16} three times on that step's inputs and keeps the fastest; it synchronises the stream while it does and
+ * Jacobi update, XSPH, list build) runs, times every candidate (threads per block {128, 256} x neighbour gathers in
+ * flight {4, 8, 16}; for the list build 32 or 16 particles per warp) three times on that step's inputs and keeps the
+ * fastest; it synchronises the stream while it does and
  * its results equal an ordinary step's bit for bit. 0: the default configuration (256 threads, 8 gathers). */
-#define ADF_TUNE_KERNELS 5 /* density and factor, solve start, acceleration (and apply), Jacobi, XSPH */
+#define ADF_TUNE_KERNELS 6 /* density and factor, solve start, acceleration (and apply), Jacobi, XSPH, list build */
 int adf_set_autotune(adf_solver* solver, int enable);
+/* Pin one kernel's configuration (one of the tuner's candidates; for the list build block 128 and nb = particles per
+ * warp, 32 or 16); the tuner then leaves it as set. */
+int adf_set_tuned_config(adf_solver* solver, int kernel, int block, int nb);
 /* The configuration in use per tuned kernel (host [ADF_TUNE_KERNELS] each, any may be NULL): threads per block,
  * gathers in flight, and the winning trial's milliseconds (-1 if not tuned). */
 int adf_tuned_configs(adf_solver* solver, int32_t* block, int32_t* nb, float* ms);
