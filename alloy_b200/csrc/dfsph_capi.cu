@@ -763,6 +763,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   // sum over worlds of ceil(liquid_w / 256) <= n / 256 + W, whatever the worlds' sizes
   s->max_items = (int)std::max<long long>(((long long)s->n + ITEM - 1) / ITEM + s->W, 1);
 
+
   int rc = 0;
   float* wall_vol = nullptr;
   WorldGrid* grid = nullptr;

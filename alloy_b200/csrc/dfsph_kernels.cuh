@@ -740,33 +740,14 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
 // wall id), its gradient and mean velocity; the distance phi with Psi(phi) = c; the slot filled as a flat wall at phi
 // with the fitted amplitude, offset and C1 taper. One slot per particle (no SDF shapes), so the inclusion-exclusion
 // combine of boundary.py:336-396 is the identity.
-__global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  int nf = P.nfw[0];
-  if (p >= nf) return;
-  int nw = P.nfw[1];
-  P.slot_g[p] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-  if (nw == 0) return;
-  int w = P.world_s[p];
+// One listed liquid particle's wall slot (a tile of its 27 cells holds boundary particles).
+__device__ __forceinline__ void wall_slot_one(const DevP& P, int p) {
+  const int w = P.world_s[p];
   const WorldGrid g = P.grid[w];
-  float4 xi = P.pos[p];
+  const float4 xi = P.pos[p];
   int cx, cy, cz;
   cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
-  {
-    // the 27 cells lie in at most 2 tiles per axis; most liquid particles see no wall particle in any of them
-    const int x0 = max(cx - 1, 0) >> 2, x1 = min(cx + 1, g.nx - 1) >> 2;
-    const int y0 = max(cy - 1, 0) >> 2, y1 = min(cy + 1, g.ny - 1) >> 2;
-    const int z0 = max(cz - 1, 0) >> 2, z1 = min(cz + 1, g.nz - 1) >> 2;
-    int walls = 0;
-    for (int tz = z0; tz <= z1; ++tz)
-      for (int ty = y0; ty <= y1; ++ty)
-        for (int tx = x0; tx <= x1; ++tx) {
-          const int t0 = P.total_cells + g.base + (((tz * g.tny + ty) * g.tnx + tx) << 6);
-          walls |= P.cell_start[t0 + 64] - P.cell_start[t0];
-        }
-    if (walls == 0) return;
-  }
-  unsigned long long buf[MAXWALL];
+  unsigned buf[MAXWALL];  // original ids of the wall particles within h, kept ascending
   int m = 0;
   for (int dz = -1; dz <= 1; ++dz) {
     int z = cz + dz;
@@ -786,7 +767,7 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
               atomicAdd(&P.wall_overflow[w], 1);
               continue;
             }
-            unsigned long long key = ((unsigned long long)(unsigned)P.id_of[j] << 32) | (unsigned)j;
+            const unsigned key = (unsigned)P.id_of[j];
             int at = m;
             while (at > 0 && buf[at - 1] > key) {
               buf[at] = buf[at - 1];
@@ -802,7 +783,7 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
   if (m == 0) return;
   float c = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
   for (int k = 0; k < m; ++k) {
-    int j = (int)(unsigned)(buf[k] & 0xffffffffull);
+    const int j = P.pos_of[buf[k]];
     float4 xj = P.pos[j];
     float4 vj = P.vel[j];
     float dx = xi.x - xj.x, dy2 = xi.y - xj.y, dz2 = xi.z - xj.z;
@@ -845,6 +826,52 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
   P.slot_xb[p] = make_float4(ADF_FMA(-phi, nx, xi.x), ADF_FMA(-phi, ny, xi.y), ADF_FMA(-phi, nz, xi.z), 0.0f);
 }
 
+
+// Every liquid particle's slot starts empty; those whose 27 cells reach a tile holding boundary particles are
+// compacted within the block, in order (warp ballots, then the warps' counts scanned), and handed to the block's
+// first threads, so that the colour sums and bisections run in full warps: most liquid particles see no wall
+// particle, and the near-wall ones of a block are usually a minority of it.
+__global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
+  __shared__ int list[BLOCK];
+  __shared__ int wcount[BLOCK / 32];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nf = P.nfw[0];
+  bool near = false;
+  if (p < nf) {
+    P.slot_g[p] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+    if (P.nfw[1] > 0) {
+      const WorldGrid g = P.grid[P.world_s[p]];
+      const float4 xi = P.pos[p];
+      int cx, cy, cz;
+      cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
+      // the 27 cells lie in at most 2 tiles per axis
+      const int x0 = max(cx - 1, 0) >> 2, x1 = min(cx + 1, g.nx - 1) >> 2;
+      const int y0 = max(cy - 1, 0) >> 2, y1 = min(cy + 1, g.ny - 1) >> 2;
+      const int z0 = max(cz - 1, 0) >> 2, z1 = min(cz + 1, g.nz - 1) >> 2;
+      int walls = 0;
+      for (int tz = z0; tz <= z1; ++tz)
+        for (int ty = y0; ty <= y1; ++ty)
+          for (int tx = x0; tx <= x1; ++tx) {
+            const int t0 = P.total_cells + g.base + (((tz * g.tny + ty) * g.tnx + tx) << 6);
+            walls |= P.cell_start[t0 + 64] - P.cell_start[t0];
+          }
+      near = walls != 0;
+    }
+  }
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const unsigned m = __ballot_sync(0xffffffffu, near);
+  if (lane == 0) wcount[wq] = __popc(m);
+  __syncthreads();
+  int base = 0, total = 0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+    if (k < wq) base += wcount[k];
+    total += wcount[k];
+  }
+  if (near) list[base + __popc(m & ((1u << lane) - 1u))] = p;
+  __syncthreads();
+  if ((int)threadIdx.x < total) wall_slot_one(P, list[threadIdx.x]);
+}
+
 // Neighbour loops read their rows in batches of NB: the NB row entries first, then the NB gathers they address,
 // then the arithmetic in ascending row order, so the loads of a batch overlap instead of forming one dependent
 // chain per neighbour. Entries past the row's end address the particle itself (a harmless load) and are skipped.
@@ -877,7 +904,7 @@ __device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, in
 // ------------------------------------------------------------------------------------------ density, factor
 // pressure.py:144-193
 template <int NB>
-__global__ void __launch_bounds__(BLOCK, 3) k_density_alpha(DevP P) {
+__global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   float4 xi = P.pos[p];
