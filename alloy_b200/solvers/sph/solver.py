@@ -147,8 +147,16 @@ class SolverDFSPH:
 
     plugin_name: ClassVar[str] = "sph"
     routes: ClassVar[frozenset[str]] = frozenset({"liquid_sph"})
+    determinism: ClassVar[str] = "native"  # bitwise repeatable, independent of batch composition (D9)
     alloy_clock_safety: ClassVar[float] = 1.0
     Config = DFSPHConfig
+
+    @staticmethod
+    def register_custom_attributes(builder) -> None:
+        """solver.py:60-70; see plugin.register_custom_attributes."""
+        from .plugin import register_custom_attributes
+
+        register_custom_attributes(builder)
 
     def __init__(self, model, config: DFSPHConfig | None = None, *, capacity_per_world: int | None = None,
                  soft_particles=None, soft_half_thickness: float = 0.0, soft_inertia: bool = True):

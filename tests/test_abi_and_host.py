@@ -122,3 +122,30 @@ def test_hydrostatic_guess_is_gravity_times_depth():
     expect = 9.81 * (q[:, 2].max() - q[:, 2] + 0.5 * sc.config.spacing)
     np.testing.assert_allclose(g[: sc.fluid_count], expect, rtol=1e-6)
     assert (g[sc.fluid_count:] == 0).all()
+
+
+def test_plugin_factory_contract():
+    """plugin.py:36-61: config or DFSPHConfig fields as kwargs, unknown kwargs raise TypeError, the escape box comes
+    from the scene's content (padded by max(0.25 m, the largest extent)) unless world_bounds or a config is given."""
+    from alloy_b200.solvers.sph.config import DFSPHConfig
+    from alloy_b200.solvers.sph.plugin import CAPABILITY, config_from_kwargs, register, REGISTRY
+    from alloy_b200.solvers.sph.testing import dam_break
+
+    sc = dam_break(counts=(4, 4, 4), box=(0.2, 0.2, 0.2))
+    with pytest.raises(TypeError):
+        config_from_kwargs(sc.model, {"no_such_field": 1})
+    cfg, cap, auto = config_from_kwargs(sc.model, {"particle_radius": 0.01, "capacity_per_world": 10})
+    assert cap == 10 and cfg.particle_radius == 0.01
+    lo, hi = (np.array(v) for v in cfg.world_bounds)
+    q = sc.model.host()["q"]
+    ext = (q.max(0) - q.min(0)).max()
+    pad = max(0.25, float(ext))
+    np.testing.assert_allclose(lo, q.min(0) - pad, rtol=1e-6)
+    np.testing.assert_allclose(hi, q.max(0) + pad, rtol=1e-6)
+    assert auto[1] == pytest.approx(pad)
+    base = DFSPHConfig(particle_radius=0.02)
+    cfg, _, auto = config_from_kwargs(sc.model, {"config": base, "xsph_c": 0.05})
+    assert cfg.particle_radius == 0.02 and cfg.xsph_c == 0.05 and cfg.world_bounds is None and auto is None
+    assert CAPABILITY.name == "sph" and CAPABILITY.routes == frozenset({"liquid_sph"})
+    register()
+    assert REGISTRY["sph"]["capability"] is CAPABILITY

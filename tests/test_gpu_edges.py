@@ -115,3 +115,20 @@ def test_sink_ledger_and_reset(cuda):
     assert live() == sc.fluid_count
     assert int(sol.mass_ledger()["out"][0]) == 0
     assert (sol.alloy_state_arrays()["sph.kappa_d"] == 0).all()
+
+
+def test_capability_factory_builds_a_working_solver(cuda):
+    """The router's path (plugin.py:36-61): the sph capability's factory from config fields, with the automatic
+    escape box, steps like a solver built directly."""
+    from alloy_b200.solvers.sph.plugin import CAPABILITY
+
+    sc = dam_break(counts=(6, 6, 6), box=(0.3, 0.3, 0.3), device=cuda)
+    sol = CAPABILITY.factory(sc.model, {"particle_radius": 0.01, "pressure_solver": "jacobi", "rest_jitter_speed": None,
+                                        "xsph_c": 0.01, "viscosity": "xsph"})
+    assert sol.config.world_bounds is not None and sol.escape_box_pad >= 0.25
+    a, b = sc.model.state(), sc.model.state()
+    for _ in range(3):
+        sol.step(a, b, None, None, sc.dt)
+        a, b = b, a
+    r = sol.report()
+    assert r.iters_density[0] >= 2 and r.escaped[0] == 0
