@@ -6,6 +6,8 @@
   1,048,576-particle case: 128 x 64 x 128 at 0.01 m in a 4 x 2 x 2 m tank.
 - ``batched_worlds``: many uneven worlds (particle count log-uniform by seed), each a cuboid block in an open box of
   boundary particles 1.5x its extent, with spares for a spout emitter.
+- ``water_column``: the reference's resting column (its own speed harness, tests/solvers/sph/test_speed_gpu.py), one
+  world or many, primed before stepping; ``tank_dam_break`` is the same harness's 30k-particle dam break.
 - ``pour_bowls``: thousands of worlds, each a hemisphere bowl of boundary particles moving on a seeded sinusoid
   (``BowlMotion`` drives the wall velocities between steps) with liquid resting in it and a spout pouring in.
 Config: cubic kernel, h = 4r = 2 spacings, rho0 1000, XSPH 0.01, Jacobi, tolerances 1e-3, resting-jitter rule off.
@@ -19,7 +21,7 @@ import numpy as np
 
 from .build import (add_fluid_block, add_fluid_points, add_particle_box, add_spares, add_wall_particles,
                     box_shell_points, jittered)
-from .config import DFSPHConfig
+from .config import DFSPHConfig, snap_down, stable_dt
 from .model import Model, ModelBuilder
 
 
@@ -57,6 +59,45 @@ def dam_break(counts=(20, 20, 20), box=(1.0, 1.0, 1.0), spacing: float = 0.02, j
 def large_dam_break(device="cpu", **kw) -> Scene:
     return dam_break(counts=(128, 64, 128), box=(4.0, 2.0, 2.0), spacing=0.01, dt=5.0e-4, steps=500,
                      device=device, **kw)
+
+
+def water_column(nx: int = 6, ny: int = 6, nz: int = 20, *, worlds: int = 1, r: float = 1.0e-3, headroom: int = 8,
+                 dt: float = 1.25e-3, steps: int = 400, device="cpu", **cfg_kw) -> Scene:
+    """A resting column nx x ny x nz on the 2r lattice filling the floor of a box tank per world (the reference's
+    ``alloy.testing.sph.water_column``, alloy/testing/sph.py:49-73), with the tank made of one layer of boundary
+    particles instead of the reference's SDF box. Config: the reference's ``fast`` preset (projected CG, the
+    resting-jitter rule off, config.py:146-157); dt = dt_max."""
+    cfg = DFSPHConfig.fast(particle_radius=r, **cfg_kw)
+    cfg.validate()
+    s = cfg.spacing
+    b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    fluid = wall = 0
+    for _ in range(worlds):
+        b.begin_world()
+        fl = add_fluid_block(b, cfg, (0.0, 0.0, 0.0), (nx, ny, nz))
+        wl = add_particle_box(b, cfg, (0.0, 0.0, 0.0), (nx * s, ny * s, (nz + headroom) * s))
+        b.end_world()
+        fluid += len(fl)
+        wall += len(wl)
+    return Scene(b.finalize(device), cfg, dt, steps, fluid, wall, name=f"water_column_{worlds}x{nx}x{ny}x{nz}")
+
+
+def tank_dam_break(width: int = 32, height: int = 30, depth: int = 32, tank: int = 96, *, r: float = 2.0e-3,
+                   steps: int = 400, device="cpu", **cfg_kw) -> Scene:
+    """The reference harness's dam break (alloy/testing/sph.py:101-115): a width x depth x height lattice block
+    against the x_lo wall of a tank (tank x depth x (height + 10)) spacings, here a box of boundary particles. The
+    reference's default config (projected CG, CFL 0.2) with the resting-jitter rule off; dt is the CFL step at the
+    Ritter front speed 2 sqrt(g H), snapped down to 0.02 s / 2^j (test_speed_gpu.py:30-31)."""
+    cfg = DFSPHConfig(particle_radius=r, **{"rest_jitter_speed": None, **cfg_kw})
+    cfg.validate()
+    s = cfg.spacing
+    dt = snap_down(stable_dt(cfg, 2.0 * (9.81 * height * s) ** 0.5), 0.02)
+    b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    b.begin_world()
+    fl = add_fluid_block(b, cfg, (0.0, 0.0, 0.0), (width, depth, height))
+    wl = add_particle_box(b, cfg, (0.0, 0.0, 0.0), (tank * s, depth * s, (height + 10) * s))
+    b.end_world()
+    return Scene(b.finalize(device), cfg, dt, steps, len(fl), len(wl), name=f"tank_dam_break_{width}x{depth}x{height}")
 
 
 def world_sizes(count: int, lo: int, hi: int, seed: int) -> np.ndarray:
@@ -208,4 +249,5 @@ def pour_bowls(worlds: int = 4096, lo: int = 4096, hi: int = 16384, spacing: flo
 
 
 __all__ = ["Scene", "benchmark_config", "dam_break", "large_dam_break", "batched_worlds", "pour_bowls", "BowlMotion",
+           "water_column", "tank_dam_break",
            "world_sizes", "box_shell_points", "add_wall_particles", "hemisphere_shell_points", "bowl_interior_points"]

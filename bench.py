@@ -45,7 +45,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--workload", choices=("large_dam_break", "dam_break", "batched_worlds", "pour_bowls"),
+    ap.add_argument("--workload", choices=("large_dam_break", "dam_break", "batched_worlds", "pour_bowls",
+                                           "column_30k", "dam_break_30k", "columns_256x4k"),
                     default="large_dam_break")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--worlds", type=int, default=None,
@@ -55,7 +56,12 @@ def parse():
     return ap.parse_args()
 
 
-MULTI_WORLD = ("batched_worlds", "pour_bowls")
+MULTI_WORLD = ("batched_worlds", "pour_bowls", "columns_256x4k")
+# the reference's own speed harness (tests/solvers/sph/test_speed_gpu.py, LIQ-9): resting columns at r = 2 mm,
+# dt_max, primed before the warm-up steps; the reference publishes 4.6 ms per step for the 30k column on an L4 with
+# the fast preset (alloy/solvers/sph/config.py:151-152)
+LIQ9 = ("column_30k", "dam_break_30k", "columns_256x4k")
+LIQ9_PUBLISHED = {"column_30k": 30720 / 4.6e-3}  # particle-steps/s, NVIDIA L4, fast preset
 
 
 WORLDS = None  # --worlds
@@ -65,7 +71,8 @@ def make_scene(name: str, device, cpu_sample: bool = False, **cfg_kw):
     """The workload's scene; ``cpu_sample``: the bounded share the CPU oracle runs (the first 256 of the 4,096 pour
     worlds, whose sizes, seeds and paths are those of the full workload); ``cfg_kw``: solver settings (the pressure
     solver of an arm)."""
-    from alloy_b200.solvers.sph.testing import batched_worlds, dam_break, large_dam_break, pour_bowls
+    from alloy_b200.solvers.sph.testing import (batched_worlds, dam_break, large_dam_break, pour_bowls,
+                                                 tank_dam_break, water_column)
 
     if name == "large_dam_break":
         return large_dam_break(device=device, **cfg_kw)
@@ -73,6 +80,12 @@ def make_scene(name: str, device, cpu_sample: bool = False, **cfg_kw):
         return batched_worlds(worlds=WORLDS or 256, device=device, **cfg_kw)
     if name == "pour_bowls":
         return pour_bowls(worlds=256 if cpu_sample else (WORLDS or 4096), device=device, **cfg_kw)
+    if name == "column_30k":
+        return water_column(32, 32, 30, r=2.0e-3, device=device, **cfg_kw)
+    if name == "dam_break_30k":
+        return tank_dam_break(32, 30, 32, 96, r=2.0e-3, device=device, **cfg_kw)
+    if name == "columns_256x4k":
+        return water_column(16, 16, 16, worlds=WORLDS or 256, r=2.0e-3, steps=200, device=device, **cfg_kw)
     return dam_break(device=device, **cfg_kw)
 
 
@@ -151,13 +164,21 @@ def rank_scene(sc, name: str, rank: int, world: int, device):
 def workload_config(sc, name: str) -> dict:
     W = len(sc.model.host()["world_start"]) - 1 if name in MULTI_WORLD else 1
     extra = ""
+    if name in LIQ9 and name != "dam_break_30k":
+        extra = (", resting column(s) at r = 2 mm primed before stepping, dt_max 1.25 ms, projected CG, fast preset "
+                 "(the reference's LIQ-9 speed harness), box tank of boundary particles")
+    if name == "dam_break_30k":
+        extra = (", 32 x 32 x 30 block against the wall of a 96-spacing tank at r = 2 mm, primed before stepping, "
+                 "default config (projected CG, CFL 0.2) with the resting-jitter rule off, dt the CFL step at the "
+                 "Ritter front speed (the reference's LIQ-9 speed harness), box tank of boundary particles")
     if name == "batched_worlds":
         extra = ", one spout per world (64 particles per 10 steps)"
     elif name == "pour_bowls":
         extra = (", a hemisphere bowl (r 0.08 m) of boundary particles per world on a seeded sinusoid (0.05 m, 1 s), "
                  "one spout per world (16 particles per 5 ms at 1 m/s), escape box")
+    solver = "projected CG" if sc.config.pressure_solver == "cg" else "Jacobi"
     return {"workload": f"{name}: {sc.fluid_count} liquid particles + {sc.wall_count} boundary particles in {W} "
-                        f"world(s), dt {sc.dt} s, Jacobi, tol 1e-3/1e-3, cubic h=2 spacings" + extra,
+                        f"world(s), dt {sc.dt} s, {solver}, tol 1e-3/1e-3, cubic h=2 spacings" + extra,
             "liquid_particles": sc.fluid_count, "boundary_particles": sc.wall_count, "worlds": W, "dt": sc.dt,
             "spacing": sc.config.spacing, "l2": "inputs larger than L2 (working set > 126 MB per step)"}
 
@@ -269,6 +290,15 @@ def cpu_oracle_run(sc, steps: int, warmup: int, budget_s: float | None):
     orc = Oracle(sc.model.host(), sc.config)
     for w, centre, _, _, vel, pool, offs, interval in spouts(sc):
         orc.add_emitter(w, _xform7(centre), offs, vel, interval, pool)
+    if sc.name.startswith(("water_column", "tank_dam_break")):  # primed like the GPU arm: the hydrostatic guess refined in place
+        from types import SimpleNamespace
+
+        from alloy_b200.solvers.sph.solver import hydrostatic_guess
+
+        guess = hydrostatic_guess(SimpleNamespace(n=sc.model.particle_count, model=sc.model, config=sc.config),
+                                  sc.model.state())
+        orc.set_warm(guess * np.float32(sc.dt), orc.warm()[1])
+        orc.prime(sc.dt)
     k = 0
 
     def step():
@@ -332,6 +362,8 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
         sol.warm_judging(judge)
     run = Stepper(sol, sc, sc.model.state(), sc.model.state())
     stream = torch.cuda.current_stream(dev)
+    if args.workload in LIQ9:
+        sol.prime(run.a, sc.dt)
     run(args.warmup)
     torch.cuda.synchronize(dev)
     nf0 = sol.list_stats()[0]
@@ -362,6 +394,19 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
 
 
 T_START = time.perf_counter()
+
+
+def liq9_fields(workload: str, sc, step_s: float) -> dict:
+    """The reference harness's own figures for its workloads (test_speed_gpu.py:24-39): the real-time factor of one
+    world and the world-seconds per wall-second of many (its targets on an L4: >= 0.5 and >= 50)."""
+    if workload == "column_30k":
+        return {"rt_factor": sc.dt / step_s, "published_l4": "4.6 ms per step, fast preset (config.py:151-152)"}
+    if workload == "dam_break_30k":
+        return {"rt_factor": sc.dt / step_s, "target_l4": ">= 0.5x real time (LIQ-9 target)"}
+    if workload == "columns_256x4k":
+        W = int(sc.model.world_count)
+        return {"world_s_per_wall_s": W * sc.dt / step_s, "target_l4": ">= 50 world-s per wall-s (LIQ-9 target)"}
+    return {}
 
 
 def pcg_off(sol) -> bool:
@@ -397,6 +442,8 @@ def run_b200(args):
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
     run = Stepper(sol, sc, sc.model.state(), sc.model.state())
     stream = torch.cuda.current_stream(dev)
+    if args.workload in LIQ9:  # the reference's harness primes its columns (alloy/testing/sph.py:334-343)
+        sol.prime(run.a, sc.dt)
     note("warm-up steps (the first one tunes)")
     run(args.warmup)
     torch.cuda.synchronize(dev)
@@ -526,8 +573,9 @@ def run_b200(args):
     if not args.no_warm:
         del sol
         run = None  # the plain solver's memory goes back before the other arms build theirs
+        other = "jacobi" if args.workload in LIQ9 else "cg"  # the other pressure solve beside the workload's own
         arms = [("warm_started", {"judge": True}), ("warm_started_unjudged", {"judge": False}),
-                ("cg", {"pressure_solver": "cg"})]
+                (other, {"pressure_solver": other})]
         for key, kw in arms:
             note(f"arm {key}")
             r = variant_arm(args, dev, rank, world, **kw)
@@ -556,8 +604,9 @@ def run_b200(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "strong" if args.workload in MULTI_WORLD else "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
+            "scaling": "strong" if args.workload in MULTI_WORLD else "weak",
+            "vs_baseline": (value / LIQ9_PUBLISHED[args.workload]) if args.workload in LIQ9_PUBLISHED else None,
+            "dtype": "f32", "data": "synthetic", **liq9_fields(args.workload, full, t_max / args.steps),
             "config": {**workload_config(full, args.workload),
                        "parallelism": ("world shards" if args.workload in MULTI_WORLD else "replicas")
                        if world > 1 else "single GPU"},

@@ -58,3 +58,27 @@ def test_primed_pressure_grows_with_depth(cuda):
     depth = z.max() - z
     deep, shallow = kd[depth > 0.38].mean(), kd[depth < 0.1].mean()
     assert (kd >= 0.0).all() and deep > 5.0 * shallow, (deep, shallow)
+
+
+def test_primed_resting_columns_bit_exact(cuda):
+    """The reference's speed-harness scene (alloy/testing/sph.py:49-73) at a small size: several resting columns in
+    box tanks, fast preset with the projected CG solve, primed, then stepped at dt_max beside the oracle."""
+    from alloy_b200.solvers.sph.testing import water_column
+
+    sc = water_column(8, 8, 12, worlds=3, r=2.0e-3, device=cuda)
+    sol = SolverDFSPH(sc.model, sc.config)
+    assert sol.pressure_solver == "cg"
+    orc = Oracle(sc.model.host(), sc.config)
+    a, b = sc.model.state(), sc.model.state()
+    guess = hydrostatic_guess(sol, a)
+    it = sol.prime(a, sc.dt)
+    orc.set_warm(guess * np.float32(sc.dt), orc.warm()[1])
+    assert it == orc.prime(sc.dt)
+    for k in range(10):
+        sol.step(a, b, None, None, sc.dt)
+        a, b = b, a
+        orc.step(sc.dt)
+        q, qd = orc.state()
+        np.testing.assert_array_equal(a.particle_q.cpu().numpy(), q, err_msg=f"q step {k}")
+        np.testing.assert_array_equal(a.particle_qd.cpu().numpy(), qd, err_msg=f"qd step {k}")
+        np.testing.assert_array_equal(sol.report().iters_density, orc.report()["iters_density"], err_msg=f"step {k}")
