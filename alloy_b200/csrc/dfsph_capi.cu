@@ -146,7 +146,7 @@ struct adf_solver {
   bool use_graphs = true;
   long long graph_kernels = 0;  // kernels a step graph launches outside its WHILE bodies
   long long body_kernels = 0;   // kernels of one WHILE-body iteration
-  unsigned long long* body_runs = nullptr;  // device: WHILE-body iterations run so far
+  unsigned long long* body_runs = nullptr;  // device [2]: WHILE-body iterations run so far, those of the running loop
   cudaStream_t cap_stream = nullptr, body_stream = nullptr;
   // learned warm start (adf_set_warm_model) and feature recording (adf_set_feature_recording)
   bool warm_on = false, feat_rec = false, warm_alloc = false, judge = true;
@@ -408,8 +408,8 @@ void cg_product(adf_solver* s, DevP& P, cudaStream_t st, const float* vec, const
 
 void cg_sums(adf_solver* s, DevP& P, cudaStream_t st, int with_max) {
   prof_begin(s, 7, st);
-  if (P.n_chunks > 0) LAUNCH(s, k_chunk_sum2, P.n_chunks, 256, st, P);
-  LAUNCH(s, k_world_sum2, s->W, 256, st, P, with_max);
+  if (P.n_chunks > 0) LAUNCH(s, k_sums2_fused, P.n_chunks, 256, st, P, with_max, 0);
+  else LAUNCH(s, k_world_sum2, s->W, 256, st, P, with_max);
   prof_end(s, st);
 }
 
@@ -432,10 +432,26 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   LAUNCH(s, k_cg_step, blocks(n), BLOCK, st, P);
   cg_product(s, P, st, P.cg_corr, P.cg_corrr, P.cg_w, 1, 0, 1);
   LAUNCH(s, k_cg_finish, blocks(n), BLOCK, st, P);
-  cg_sums(s, P, st, 1);
-  cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
-  LAUNCH(s, k_cg_beta, blocks(s->W), BLOCK, st, P);
+  if (P.n_chunks > 0) {  // sums with the maximum, stop test and beta per world, unconverged count: one launch
+    prof_begin(s, 7, st);
+    LAUNCH(s, k_sums2_fused, P.n_chunks, 256, st, P, 1, 1);
+    prof_end(s, st);
+  } else {
+    cg_sums(s, P, st, 1);
+    cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
+    LAUNCH(s, k_cg_beta, blocks(s->W), BLOCK, st, P);
+  }
   LAUNCH(s, k_cg_direction, blocks(n), BLOCK, st, P);
+}
+
+// The stop test of an iteration and the next iteration's work list (one launch: k_check_fused).
+void check_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
+  if (P.n_chunks > 0) {
+    LAUNCH(s, k_check_fused, P.n_chunks, 256, st, P);
+  } else {
+    cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
+    if (s->W > 0) LAUNCH(s, k_worklist, 1, 1024, st, P);
+  }
 }
 
 void enqueue_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
@@ -452,15 +468,7 @@ void enqueue_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   run_tk(s, TK_JACOBI, st, P);
   prof_end(s, st);
   prof_begin(s, 7, st);
-  if (P.n_chunks > 0)
-    LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, P.err_orig, P.chunk_begin, P.chunk_end, P.part_sum, P.part_max,
-           P.n_unconv, P.chunk_world, (const int*)P.converged);
-  else
-    cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
-  if (s->W > 0) {
-    LAUNCH(s, k_world_check, s->W, 256, st, P, 1, (double*)nullptr, (float*)nullptr);
-    LAUNCH(s, k_worklist, 1, 1024, st, P);
-  }
+  check_iteration(s, P, st);
   prof_end(s, st);
 }
 
@@ -478,7 +486,7 @@ int capture_iterations(adf_solver* s, DevP& P, cudaStream_t st) {
   if (cs != cudaStreamCaptureStatusActive) return fail(ADF_ERR_STATE, "capture_iterations: stream not capturing");
   cudaGraphConditionalHandle h;
   CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-  LAUNCH(s, k_set_cond, 1, 1, st, h, (const int*)P.n_unconv, (unsigned long long*)nullptr);
+  LAUNCH(s, k_set_cond, 1, 1, st, h, (const int*)P.n_unconv, s->body_runs, -1);
   CK(cudaStreamGetCaptureInfo(st, &cs, &id, &g, &deps, &nd));
   cudaGraphNodeParams cp{};
   cp.type = cudaGraphNodeTypeConditional;
@@ -493,7 +501,7 @@ int capture_iterations(adf_solver* s, DevP& P, cudaStream_t st) {
   const long long b0 = s->launches;
   CK(cudaStreamBeginCaptureToGraph(s->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
   enqueue_iteration(s, P, s->body_stream);
-  LAUNCH(s, k_set_cond, 1, 1, s->body_stream, h, (const int*)P.n_unconv, s->body_runs);
+  LAUNCH(s, k_set_cond, 1, 1, s->body_stream, h, (const int*)P.n_unconv, s->body_runs, P.max_it + 2);
   cudaGraph_t out;
   CK(cudaStreamEndCapture(s->body_stream, &out));
   s->body_kernels = s->launches - b0;  // counted per run through body_runs, not per capture
@@ -530,13 +538,7 @@ void dual_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   LAUNCH(s, k_choose_start, blocks(W), BLOCK, st, P);
   LAUNCH(s, k_select_start, blocks(n), BLOCK, st, P);
   prof_begin(s, 7, st);
-  if (P.n_chunks > 0)
-    LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, P.err_orig, P.chunk_begin, P.chunk_end, P.part_sum, P.part_max,
-           P.n_unconv, P.chunk_world, (const int*)P.converged);
-  else
-    cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
-  LAUNCH(s, k_world_check, W, 256, st, P, 1, (double*)nullptr, (float*)nullptr);
-  LAUNCH(s, k_worklist, 1, 1024, st, P);
+  check_iteration(s, P, st);
   prof_end(s, st);
 }
 
@@ -760,6 +762,8 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     cs.push_back((int)cb.size());
   }
   d.n_chunks = (int)cb.size();
+  d.n_chunk_worlds = 0;
+  for (size_t k = 0; k + 1 < cs.size(); ++k) d.n_chunk_worlds += cs[k + 1] > cs[k] ? 1 : 0;
   // sum over worlds of ceil(liquid_w / 256) <= n / 256 + W, whatever the worlds' sizes
   s->max_items = (int)std::max<long long>(((long long)s->n + ITEM - 1) / ITEM + s->W, 1);
 
@@ -831,6 +835,8 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.iters, W);
   rc |= s->alloc(&d.err_mean, W);
   rc |= s->alloc(&d.n_unconv, 1);
+  rc |= s->alloc(&d.wdone, W);
+  rc |= s->alloc(&d.gdone, 1);
   rc |= s->alloc(&d.n_active, W);
   rc |= s->alloc(&d.overflow, W);
   rc |= s->alloc(&d.escaped, W);
@@ -898,6 +904,8 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
                     s->den_err_max, d.emax};
   for (void* z : zero_w) CKC(cudaMemset(z, 0, 4 * W));
   CKC(cudaMemset(d.mass_out, 0, 8 * W));
+  CKC(cudaMemset(d.wdone, 0, sizeof(int) * std::max(W, 1)));
+  CKC(cudaMemset(d.gdone, 0, sizeof(unsigned)));
   CKC(cudaMemset(d.iter_work, 0, sizeof(unsigned long long)));
   CKC(cudaMemset(s->mass_in, 0, 8 * W));
   CKC(cudaMemset(d.n_active, 0, 8 * W));
@@ -919,8 +927,8 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   CKC(cudaHostAlloc((void**)&s->pinned, 2 * sizeof(int), cudaHostAllocDefault));
   CKC(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
   CKC(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
-  CKC(cudaMalloc(&s->body_runs, sizeof(unsigned long long)));
-  CKC(cudaMemset(s->body_runs, 0, sizeof(unsigned long long)));
+  CKC(cudaMalloc(&s->body_runs, 2 * sizeof(unsigned long long)));
+  CKC(cudaMemset(s->body_runs, 0, 2 * sizeof(unsigned long long)));
   CKC(cudaEventCreate(&s->tev[0]));
   CKC(cudaEventCreate(&s->tev[1]));
   CKC(cudaMalloc(&s->snap_kappa, sizeof(float) * n));

@@ -136,6 +136,9 @@ struct DevP {
   int* iters;
   float* err_mean;
   int* n_unconv;
+  int* wdone;        // [W] chunk blocks of the world finished in the running reduction launch (reset by its last)
+  unsigned* gdone;   // worlds of the running reduction launch finished (reset by its last)
+  int n_chunk_worlds;  // worlds with at least one chunk
   double* n_active;
   int* overflow;
   int* escaped;
@@ -400,7 +403,7 @@ __global__ void __launch_bounds__(LS_THREADS) k_lists_smem(DevP P) {
 //     stream (offsets by a warp scan), 32 candidates at a time are staged in shared memory (the next 32 already in
 //     flight in registers) and every lane tests all of them against its own particle as a 32-bit pass mask, then
 //     appends the original ids of the passing ones to its row (unsorted). A warp whose particles span a large box
-//     (a splash, several worlds) scans each lane's own 27 cells instead.
+//     (a splash, several worlds) runs the same scan once per compact group of its lanes.
 //  2. order: rows of at most 32 entries are sorted in registers by a fully unrolled bitonic network; longer rows by
 //     insertion in shared memory; a row with more than 64 candidates selects its K lowest ids by repeated scans.
 //  3. write: entry k of the 32 rows is one contiguous 128-byte segment (ids mapped to sorted positions by pos_of).
@@ -458,8 +461,8 @@ __device__ __forceinline__ void sort16_registers(unsigned (&key)[16]) {
 }
 
 // G particles per warp: 32 (one lane per particle), or 16 (lanes l and l + 16 share particle l: the warp's union of
-// neighbourhoods is about a third smaller and each lane tests half of each staged batch; the two halves' sorted runs
-// are merged on write by lane l). The rows are the same either way.
+// neighbourhoods is about a third smaller and each lane tests every other candidate pair of each staged batch; the
+// two lanes' sorted runs are merged on write by lane l). The rows are the same either way.
 template <int G>
 __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
   __shared__ unsigned rows[LU_WARPS][LU_ROW][32];  // [warp][entry][lane]: lanes of one entry in distinct banks
@@ -486,27 +489,40 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
   int cx, cy, cz;
   cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
   const unsigned full = 0xffffffffu;
-  const int w_lo = __reduce_min_sync(full, (unsigned)w), w_hi = __reduce_max_sync(full, (unsigned)w);
-  const int ylo = max((int)__reduce_min_sync(full, (unsigned)cy) - 1, 0);
-  const int yhi = min((int)__reduce_max_sync(full, (unsigned)cy) + 1, g.ny - 1);
-  const int zlo = max((int)__reduce_min_sync(full, (unsigned)cz) - 1, 0);
-  const int zhi = min((int)__reduce_max_sync(full, (unsigned)cz) + 1, g.nz - 1);
   unsigned* myrow = &rows[wq][0][lane];
   int cnt = 0, total = 0;
-  const int sy = yhi - ylo + 1, sz = zhi - zlo + 1, nrows = sy * sz;
-  bool lockstep = w_lo == w_hi && nrows <= LU_MAX_ROWS;
-  int T = 0;
-  if (lockstep) {
-    // rows (y, z) of the box, row-major; row j's x range is the union of [cx - 1, cx + 1] over the lanes whose cell
-    // is within one row of it (empty: x0 > x1). Lane l keeps rows l and l + 32.
+  const unsigned myid = (unsigned)P.id_of[p];
+  const f32x2 xi2 = f2_dup(xi.x), yi2 = f2_dup(xi.y), zi2 = f2_dup(xi.z);
+  // One lockstep scan of the lanes with `in` set; false (before any candidate is read) when they span more than one
+  // world or their box needs more rows or tile segments than the tables hold. The whole warp is scanned at once when
+  // it can be; otherwise (a splash, a sparse tile, a world boundary in the sorted order) its lanes are scanned in
+  // groups, each the pending lanes of the lowest pending lane's world within 2 cells of its cell per axis: a box of at
+  // most 7 x 7 x 7 cells, 49 cell rows of at most 3 tile segments, which the tables always hold.
+  auto scan = [&](const bool in) -> bool {
+    const int w_lo = __reduce_min_sync(full, in ? (unsigned)w : 0xffffffffu);
+    const int w_hi = __reduce_max_sync(full, in ? (unsigned)w : 0u);
+    if (w_lo != w_hi) {  // only the whole warp: a group's lanes share the leader's world
+      return false;
+    }
+    const WorldGrid gw = P.grid[w_lo];  // the group's world: every lane computes its cell rows and ranges in it
+    const int ylo = max((int)__reduce_min_sync(full, in ? (unsigned)cy : 0xffffffffu) - 1, 0);
+    const int yhi = min((int)__reduce_max_sync(full, in ? (unsigned)cy : 0u) + 1, gw.ny - 1);
+    const int zlo = max((int)__reduce_min_sync(full, in ? (unsigned)cz : 0xffffffffu) - 1, 0);
+    const int zhi = min((int)__reduce_max_sync(full, in ? (unsigned)cz : 0u) + 1, gw.nz - 1);
+    const int sy = yhi - ylo + 1, sz = zhi - zlo + 1, nrows = sy * sz;
+    if (nrows > LU_MAX_ROWS) {  // likewise: a group spans at most 7 x 7 cell rows
+      return false;
+    }
+    // rows (y, z) of the box, row-major; row j's x range is the union of [cx - 1, cx + 1] over the group's lanes
+    // whose cell is within one row of it (empty: x0 > x1). Lane l keeps rows l and l + 32.
     int ax0 = 1, ax1 = 0, bx0 = 1, bx1 = 0;
     for (int j = 0; j < nrows; ++j) {
       const int y = ylo + j % sy, z = zlo + j / sy;
-      const bool near = abs(cy - y) <= 1 && abs(cz - z) <= 1;
+      const bool near = in && abs(cy - y) <= 1 && abs(cz - z) <= 1;
       const unsigned mn = __reduce_min_sync(full, near ? (unsigned)cx : 0xffffffffu);
       const unsigned mx = __reduce_max_sync(full, near ? (unsigned)(cx + 1) : 0u);
       if (lane == (j & 31) && mx != 0u) {
-        const int x0 = max((int)mn - 1, 0), x1 = min((int)mx, g.nx - 1);
+        const int x0 = max((int)mn - 1, 0), x1 = min((int)mx, gw.nx - 1);
         if (j < 32) {
           ax0 = x0;
           ax1 = x1;
@@ -530,48 +546,44 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
     }
     const int ta = __shfl_sync(full, ia, 31);
     const int nseg = ta + __shfl_sync(full, ib, 31);
-    if (nseg > LU_MAX_SEGS) {
-      lockstep = false;
-    } else {
-      // ranges' first sorted index into rbeg; their lengths, prefixed within the row, into roff[r + 1]
-      int na = 0, nb = 0;
-      for (int half = 0; half < 2; ++half) {
-        const int j = lane + 32 * half;
-        const int x0 = half ? bx0 : ax0, x1 = half ? bx1 : ax1;
-        const int r0 = half ? ta + ib - sb : ia - sa;
-        const int y = ylo + j % sy, z = zlo + j / sy;
-        int acc = 0;
-        for (int xs = x0, r = r0; xs <= x1; ++r) {
-          const int xe = min(x1, xs | 3);
-          const int bb = P.cell_start[cell_key(g, xs, y, z)];
-          const int ee = P.cell_start[cell_key(g, xe, y, z) + 1];
-          rbeg[wq][r] = bb;
-          acc += ee - bb;
-          roff[wq][r + 1] = acc;
-          xs = xe + 1;
-        }
-        (half ? nb : na) = acc;
-      }
-      // candidates before each row: scan of the row totals over rows 0..63, then shift each row's ranges by it
-      int ca = na, cb = nb;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int va = __shfl_up_sync(full, ca, o), vb = __shfl_up_sync(full, cb, o);
-        if (lane >= o) {
-          ca += va;
-          cb += vb;
-        }
-      }
-      const int tca = __shfl_sync(full, ca, 31);
-      T = tca + __shfl_sync(full, cb, 31);
-      for (int r = ia - sa; r < ia; ++r) roff[wq][r + 1] += ca - na;
-      for (int r = ta + ib - sb; r < ta + ib; ++r) roff[wq][r + 1] += tca + cb - nb;
-      if (lane == 0) roff[wq][0] = 0;
-      __syncwarp();
+    if (nseg > LU_MAX_SEGS) {  // only the whole warp: a group has at most 49 rows x 3 segments
+      return false;
     }
-  }
-  if (lockstep) {
-    const unsigned myid = (unsigned)P.id_of[p];
+    // ranges' first sorted index into rbeg; their lengths, prefixed within the row, into roff[r + 1]
+    int na = 0, nb = 0;
+    for (int hf = 0; hf < 2; ++hf) {
+      const int j = lane + 32 * hf;
+      const int x0 = hf ? bx0 : ax0, x1 = hf ? bx1 : ax1;
+      const int r0 = hf ? ta + ib - sb : ia - sa;
+      const int y = ylo + j % sy, z = zlo + j / sy;
+      int acc = 0;
+      for (int xs = x0, r = r0; xs <= x1; ++r) {
+        const int xe = min(x1, xs | 3);
+        const int bb = P.cell_start[cell_key(gw, xs, y, z)];
+        const int ee = P.cell_start[cell_key(gw, xe, y, z) + 1];
+        rbeg[wq][r] = bb;
+        acc += ee - bb;
+        roff[wq][r + 1] = acc;
+        xs = xe + 1;
+      }
+      (hf ? nb : na) = acc;
+    }
+    // candidates before each row: scan of the row totals over rows 0..63, then shift each row's ranges by it
+    int ca = na, cb = nb;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int va = __shfl_up_sync(full, ca, o), vb = __shfl_up_sync(full, cb, o);
+      if (lane >= o) {
+        ca += va;
+        cb += vb;
+      }
+    }
+    const int tca = __shfl_sync(full, ca, 31);
+    const int T = tca + __shfl_sync(full, cb, 31);
+    for (int r = ia - sa; r < ia; ++r) roff[wq][r + 1] += ca - na;
+    for (int r = ta + ib - sb; r < ta + ib; ++r) roff[wq][r + 1] += tca + cb - nb;
+    if (lane == 0) roff[wq][0] = 0;
+    __syncwarp();
     int rr = 0;  // range of this lane's next candidate; candidates lane, lane + 32, ... only move it forward
     float4 nxt = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     unsigned nid = 0u;
@@ -584,7 +596,6 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       }
     };
     fetch(lane);
-    const f32x2 xi2 = f2_dup(xi.x), yi2 = f2_dup(xi.y), zi2 = f2_dup(xi.z);
     for (int c0 = 0; c0 < T; c0 += 32) {
       const int nc = min(32, T - c0);
       cxs[wq][lane] = nxt.x;
@@ -605,14 +616,20 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
         const float bx = f2_hi(dx), by = f2_hi(dy), bz = f2_hi(dz);
         return (dot_plain(ax, ay, az, ax, ay, az) < h2 ? 1u : 0u) | (dot_plain(bx, by, bz, bx, by, bz) < h2 ? 2u : 0u);
       };
-      const int t0 = half * G;  // this lane's share of the staged batch
+      // this lane's share of the staged batch: every pair (G = 32), or every other pair (G = 16: pairs 0, 2, 4, ... for
+      // the first lane of a particle, 1, 3, 5, ... for the second), so that a particle's hits, which come in runs of
+      // the same few cells, split about evenly between its two lanes (halves of the batch did not: on a settled
+      // column one lane could get all 37 hits of a row, more than its sorted run holds)
+      constexpr int STEP = G == 32 ? 2 : 4;
+      const int t0 = G == 32 ? 0 : 2 * half;
       if (nc == 32) {
 #pragma unroll
-        for (int t = 0; t < G; t += 2) hit |= pair_hits(t0 + t) << (t0 + t);
+        for (int t = t0; t < 32; t += STEP) hit |= pair_hits(t) << t;
       } else {
-        for (int t = t0; t < min(nc, t0 + G); t += 2) hit |= pair_hits(t) << t;
+        for (int t = t0; t < nc; t += STEP) hit |= pair_hits(t) << t;
         hit &= (1u << nc) - 1u;  // nc < 32: drop the stale slot past the last candidate
       }
+      if (!in) hit = 0u;
       while (hit) {
         const int t = __ffs(hit) - 1;
         hit &= hit - 1u;
@@ -624,21 +641,18 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
       }
       __syncwarp();
     }
-  } else if (valid && half == 0) {
-    for (int r = 0; r < 9; ++r) {
-      const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
-      if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
-      for_row_ranges(P.cell_start, g, 0, y, z, max(cx - 1, 0), min(cx + 1, g.nx - 1), [&](int b, int e) {
-        for (int j = b; j < e; ++j) {
-          if (j == p) continue;
-          const float4 xj = P.pos[j];
-          const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-          if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
-            if (cnt < LU_ROW) myrow[cnt * 32] = (unsigned)P.id_of[j];
-            ++cnt;
-          }
-        }
-      });
+    return true;
+  };
+  if (!scan(true)) {
+    unsigned pending = __ballot_sync(full, valid);
+    while (pending) {
+      const int ld = __ffs(pending) - 1;
+      const int lw = __shfl_sync(full, w, ld), lx = __shfl_sync(full, cx, ld), ly = __shfl_sync(full, cy, ld),
+                lz = __shfl_sync(full, cz, ld);
+      const bool in =
+          ((pending >> lane) & 1u) && w == lw && abs(cx - lx) <= 2 && abs(cy - ly) <= 2 && abs(cz - lz) <= 2;
+      scan(in);
+      pending &= ~__ballot_sync(full, in);
     }
   }
   const int own = valid ? cnt : 0;                                       // this lane's hits
@@ -827,10 +841,10 @@ __device__ __forceinline__ void wall_slot_one(const DevP& P, int p) {
 }
 
 
-// Every liquid particle's slot starts empty; those whose 27 cells reach a tile holding boundary particles are
-// compacted within the block, in order (warp ballots, then the warps' counts scanned), and handed to the block's
-// first threads, so that the colour sums and bisections run in full warps: most liquid particles see no wall
-// particle, and the near-wall ones of a block are usually a minority of it.
+// Every liquid particle's slot starts empty; those whose 27 cells hold boundary particles (tiles checked first, then
+// the cells) are compacted within the block, in order (warp ballots, then the warps' counts scanned), and handed to
+// the block's first threads, so that the colour sums and bisections run in full warps: most liquid particles see no
+// wall particle, and the near-wall ones of a block are usually a minority of it.
 __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
   __shared__ int list[BLOCK];
   __shared__ int wcount[BLOCK / 32];
@@ -855,6 +869,15 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
             const int t0 = P.total_cells + g.base + (((tz * g.tny + ty) * g.tnx + tx) << 6);
             walls |= P.cell_start[t0 + 64] - P.cell_start[t0];
           }
+      if (walls != 0) {  // then the 27 cells themselves (their 9 rows, one range per tile crossed)
+        walls = 0;
+        for (int r = 0; r < 9 && walls == 0; ++r) {
+          const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+          if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
+          for_row_ranges(P.cell_start, g, P.total_cells, y, z, max(cx - 1, 0), min(cx + 1, g.nx - 1),
+                         [&](int b, int e) { walls |= e - b; });
+        }
+      }
       near = walls != 0;
     }
   }
@@ -1087,10 +1110,20 @@ __global__ void __launch_bounds__(BLOCK) k_select_start(DevP P) {
   P.err_orig[i] = P.err2[i];
 }
 
-// Condition of a solve's WHILE graph node: iterate while any world is unconverged (solve_driver.py:186).
-__global__ void k_set_cond(cudaGraphConditionalHandle h, const int* n_unconv, unsigned long long* body_runs) {
-  cudaGraphSetConditional(h, *n_unconv > 0 ? 1u : 0u);
-  if (body_runs) atomicAdd(body_runs, 1ull);  // iterations run by WHILE bodies (launch accounting)
+// Condition of a solve's WHILE graph node: iterate while any world is unconverged (solve_driver.py:186). runs[0]
+// counts the iterations run by WHILE bodies (launch accounting), runs[1] those of the running loop: the call before
+// the loop (cap < 0) resets it, and a loop stops after `cap` iterations whatever the unconverged count says (every
+// world stops at max_iterations before that, so the cap only guards the loop against a count that never drops).
+__global__ void k_set_cond(cudaGraphConditionalHandle h, const int* n_unconv, unsigned long long* runs, int cap) {
+  bool more = *n_unconv > 0;
+  if (cap < 0) {
+    runs[1] = 0ull;
+  } else {
+    runs[0] += 1ull;
+    runs[1] += 1ull;
+    more = more && runs[1] < (unsigned long long)cap;
+  }
+  cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 __global__ void k_begin_solve(DevP P) {
@@ -1113,7 +1146,9 @@ __global__ void k_begin_solve(DevP P) {
 // what keeps a batch of uneven worlds cheap once most of them have converged.
 constexpr int ITEM = 256;
 
-__global__ void __launch_bounds__(1024) k_worklist(DevP P) {
+// The block that builds the list: any multiple of 32 threads. `fresh`: the converged flags were written by other
+// blocks of the same launch, so they are read from L2.
+__device__ __forceinline__ int build_worklist(const DevP& P, bool fresh) {
   __shared__ int smem[32];
   __shared__ int carry_w, carry_s;
   if (threadIdx.x == 0) {
@@ -1125,7 +1160,7 @@ __global__ void __launch_bounds__(1024) k_worklist(DevP P) {
   for (int w0 = 0; w0 < P.W; w0 += blockDim.x) {
     const int w = w0 + threadIdx.x;
     int segs = 0, parts = 0;
-    if (w < P.W && !P.converged[w]) {
+    if (w < P.W && !(fresh ? __ldcg(&P.converged[w]) : P.converged[w])) {
       const int2 r = P.wrange[w];
       segs = (r.y - r.x + ITEM - 1) / ITEM;
       parts = r.y - r.x;
@@ -1148,12 +1183,16 @@ __global__ void __launch_bounds__(1024) k_worklist(DevP P) {
     }
     __syncthreads();
   }
+  const int listed = carry_w;
   if (threadIdx.x == 0) {
     P.cseg[carry_w] = carry_s;
     *P.n_cw = carry_w;
     if (P.iter_work && work) atomicAdd(P.iter_work, work);  // the iteration this list drives, if it runs
   }
+  return listed;
 }
+
+__global__ void __launch_bounds__(1024) k_worklist(DevP P) { build_worklist(P, false); }
 
 // The sorted range [b, e) of this block's work item; false (for the whole block) past the last item.
 __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
@@ -1414,9 +1453,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_finish(DevP P) {
 }
 
 // krylov.py:207-233: per world the stop test (as k_world_check), then beta = r.z_new / r.z (0 after a set change)
-__global__ void k_cg_beta(DevP P) {
-  int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= P.W || P.converged[w]) return;
+__device__ __forceinline__ void cg_beta_world(const DevP& P, int w) {
   const int it = P.iters[w] + 1;
   P.iters[w] = it;
   const double2 sm = P.cg_sums[w];
@@ -1429,7 +1466,13 @@ __global__ void k_cg_beta(DevP P) {
   P.cg_rz[w] = sm.x;
   P.cg_step[w] = beta;
   if ((it >= P.min_it && mean <= P.tol && P.emax[w] <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
-  else atomicAdd(P.n_unconv, 1);
+}
+
+__global__ void k_cg_beta(DevP P) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W || P.converged[w]) return;
+  cg_beta_world(P, w);
+  if (!P.converged[w]) atomicAdd(P.n_unconv, 1);
 }
 
 // krylov.py:236-246: p = z + beta p on F, 0 elsewhere
@@ -1535,6 +1578,140 @@ __global__ void __launch_bounds__(256) k_world_check(DevP P, int check, double* 
   P.err_mean[w] = mean;
   if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
   else atomicAdd(P.n_unconv, 1);
+}
+
+// Tickets of the one-launch reductions below: thread 0 of a block that has stored its partials takes a ticket of its
+// world (true for the world's last block, which resets the counter for the next launch).
+__device__ __forceinline__ bool world_ticket(const DevP& P, int w, int chunks) {
+  __threadfence();
+  const bool last = atomicAdd(&P.wdone[w], 1) == chunks - 1;
+  if (last) P.wdone[w] = 0;
+  return last;
+}
+
+// The grid's ticket is taken once per world that has chunks: by its last block when the world iterates, by its first
+// chunk's block when it had converged before the launch; the last of the n_chunk_worlds tickets is the grid's last.
+__device__ __forceinline__ bool grid_ticket(const DevP& P) {
+  __threadfence();
+  const bool last = atomicAdd(P.gdone, 1u) == (unsigned)P.n_chunk_worlds - 1u;
+  if (last) *P.gdone = 0u;
+  return last;
+}
+
+// The Jacobi iteration's stop test in one launch (k_chunk_sum, k_world_check and k_worklist fused): block c folds
+// chunk c (chunks of converged worlds keep their partials); the last block of a world to finish folds the world's
+// partials in the same fixed tree order as k_world_check and runs its stop test (pressure.py:370-390); the last block
+// of the grid lists the worlds still iterating for the next iteration and stores their count as the unconverged
+// count. The sums are those of the separate kernels bit for bit; only the launches are fewer.
+__global__ void __launch_bounds__(256) k_check_fused(DevP P) {
+  __shared__ double smd[8];
+  __shared__ float smf[8];
+  __shared__ bool wlast, glast;
+  const int c = blockIdx.x;
+  const int w = P.chunk_world[c];
+  const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
+  bool ticket = c == c0;  // the world's grid ticket: its first chunk's block if it had converged, else its last block
+  if (!P.converged[w]) {
+    const int i = P.chunk_begin[c] + threadIdx.x;
+    const bool in = i < P.chunk_end[c];
+    const float x = in ? P.err_orig[i] : 0.0f;
+    const double s = fold256(in ? (double)x : 0.0, smd);
+    const float m = block_max256(in ? x : -3.4e38f, smf);
+    if (threadIdx.x == 0) {
+      P.part_sum[c] = s;
+      P.part_max[c] = m;
+      wlast = world_ticket(P, w, c1 - c0);
+    }
+    __syncthreads();
+    if (wlast) {
+      __threadfence();
+      double a = 0.0;
+      float mm = -3.4e38f;
+      for (int k = c0 + threadIdx.x; k < c1; k += 256) {
+        a = a + __ldcg(&P.part_sum[k]);
+        mm = fmaxf(mm, __ldcg(&P.part_max[k]));
+      }
+      const double sw = fold256(a, smd);
+      const float mx = maxr(block_max256(mm, smf), 0.0f);
+      if (threadIdx.x == 0) {
+        P.emax[w] = mx;
+        const int it = P.iters[w] + 1;
+        P.iters[w] = it;
+        const double na = P.n_active[w];
+        const float mean = (float)(sw / (na > 1.0 ? na : 1.0));
+        P.err_mean[w] = mean;
+        if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+      }
+    }
+    ticket = wlast;
+  }
+  if (!ticket) return;
+  if (threadIdx.x == 0) glast = grid_ticket(P);
+  __syncthreads();
+  if (glast) {
+    __threadfence();
+    const int listed = build_worklist(P, true);
+    if (threadIdx.x == 0) *P.n_unconv = listed;
+  }
+}
+
+// The CG reductions in one launch (k_chunk_sum2 and k_world_sum2 fused, same partials and tree order); with `beta`
+// the world's last block also runs k_cg_beta's stop test and beta for its world, and the grid's last block stores the
+// count of worlds still iterating as the unconverged count.
+__global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int beta) {
+  __shared__ double smd[8];
+  __shared__ float smf[8];
+  __shared__ int smi[32];
+  __shared__ bool wlast, glast;
+  const int c = blockIdx.x;
+  const int w = P.chunk_world[c];
+  const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
+  bool ticket = c == c0;  // as in k_check_fused
+  if (!P.converged[w]) {
+    const int i = P.chunk_begin[c] + threadIdx.x;
+    const bool in = i < P.chunk_end[c];
+    const float2 v = in ? P.cg_pair[i] : make_float2(0.0f, 0.0f);
+    const double sx = fold256(in ? (double)v.x : 0.0, smd);
+    const double sy = fold256(in ? (double)v.y : 0.0, smd);
+    const float m = block_max256(in ? v.y : -3.4e38f, smf);
+    if (threadIdx.x == 0) {
+      P.part2[c] = make_double2(sx, sy);
+      P.part_max[c] = m;
+      wlast = world_ticket(P, w, c1 - c0);
+    }
+    __syncthreads();
+    if (wlast) {
+      __threadfence();
+      double ax = 0.0, ay = 0.0;
+      float mm = -3.4e38f;
+      for (int k = c0 + threadIdx.x; k < c1; k += 256) {
+        const double2 pk = __ldcg(&P.part2[k]);
+        ax = ax + pk.x;
+        ay = ay + pk.y;
+        mm = fmaxf(mm, __ldcg(&P.part_max[k]));
+      }
+      const double wx = fold256(ax, smd);
+      const double wy = fold256(ay, smd);
+      const float mx = block_max256(mm, smf);
+      if (threadIdx.x == 0) {
+        P.cg_sums[w] = make_double2(wx, wy);
+        if (with_max) P.emax[w] = maxr(mx, 0.0f);
+        if (beta) cg_beta_world(P, w);
+      }
+    }
+    ticket = wlast;
+  }
+  if (!beta || !ticket) return;
+  if (threadIdx.x == 0) glast = grid_ticket(P);
+  __syncthreads();
+  if (glast) {
+    __threadfence();
+    int open = 0;
+    for (int k = threadIdx.x; k < P.W; k += 256) open += __ldcg(&P.converged[k]) ? 0 : 1;
+    int tot;
+    block_exclusive_scan(open, smi, tot);
+    if (threadIdx.x == 0) *P.n_unconv = tot;
+  }
 }
 
 // ---------------------------------------------------------------------------------------- apply pressure
