@@ -417,6 +417,7 @@ void cg_sums(adf_solver* s, DevP& P, cudaStream_t st, int with_max) {
 void cg_init(adf_solver* s, DevP& P, cudaStream_t st) {
   const int n = s->n;
   cudaMemsetAsync(P.cg_restart, 0, sizeof(int) * std::max(s->W, 1), st);
+  cudaMemsetAsync(P.cg_act_new, 0, sizeof(int) * std::max(s->W, 1), st);
   cudaMemsetAsync(P.cg_pair, 0, sizeof(float2) * std::max(n, 1), st);
   cg_product(s, P, st, P.kappa, P.kr, P.cg_w, 0, 1, 0);
   LAUNCH(s, k_cg_init, blocks(n), BLOCK, st, P);
@@ -430,8 +431,19 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   cg_product(s, P, st, P.cg_pd, P.cg_pdr, P.cg_ap, 0, 0, 0);
   cg_sums(s, P, st, 0);
   LAUNCH(s, k_cg_step, blocks(n), BLOCK, st, P);
-  cg_product(s, P, st, P.cg_corr, P.cg_corrr, P.cg_w, 1, 0, 1);
-  LAUNCH(s, k_cg_finish, blocks(n), BLOCK, st, P);
+  {  // the correction product (worlds where the step clamped a variable) with the finish of the iteration
+    const TuneCfg& ca = s->tune[TK_ACCEL];
+    const TuneCfg& cj = s->tune[TK_JACOBI];
+    prof_begin(s, 5, st);
+    NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, (const float*)P.cg_corr,
+                (const float*)P.cg_corrr, 1);
+    ++s->launches;
+    prof_end(s, st);
+    prof_begin(s, 6, st);
+    NB_DISPATCH(k_cg_apply_finish, cj.nb, blocks(n, cj.block), cj.block, st, P);
+    ++s->launches;
+    prof_end(s, st);
+  }
   if (P.n_chunks > 0) {  // sums with the maximum, stop test and beta per world, unconverged count: one launch
     prof_begin(s, 7, st);
     LAUNCH(s, k_sums2_fused, P.n_chunks, 256, st, P, 1, 1);
@@ -829,6 +841,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     rc |= s->alloc(&d.cg_step, W);
     rc |= s->alloc(&d.cg_sums, W);
     rc |= s->alloc(&d.cg_restart, W);
+    rc |= s->alloc(&d.cg_act_new, W);
     rc |= s->alloc(&d.part2, std::max<size_t>(cb.size(), 1));
   }
   rc |= s->alloc(&d.converged, W);

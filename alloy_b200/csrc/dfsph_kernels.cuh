@@ -184,7 +184,8 @@ struct DevP {
   double* cg_rz;    // [W] r.z
   double* cg_step;  // [W] beta
   double2* cg_sums; // [W] (sum of pair.x, sum of pair.y)
-  int* cg_restart;  // [W] active-set changes this iteration
+  int* cg_restart;  // [W] variables clamped onto their bound this iteration (k_cg_step)
+  int* cg_act_new;  // [W] set when a bound variable was activated this iteration (k_cg_apply_finish)
   double2* part2;   // [chunks] partial sums of pairs
 };
 
@@ -1394,6 +1395,7 @@ __global__ void k_cg_first_rz(DevP P) {
   if (w >= P.W) return;
   P.cg_rz[w] = P.cg_sums[w].x;
   P.cg_restart[w] = 0;
+  P.cg_act_new[w] = 0;
 }
 
 // krylov.py:146-170: k += a p on F, projected onto k >= k_lo (the clamped part into corr); w += a A p
@@ -1423,8 +1425,13 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(DevP P) {
   P.cg_w[p] = ADF_FMA(a, P.cg_ap[p], P.cg_w[p]);
 }
 
-// krylov.py:173-204: activation of compressed bound variables, z = M^-1 r on F, (r.z, error) per particle
-__global__ void __launch_bounds__(BLOCK) k_cg_finish(DevP P) {
+// krylov.py:148-204 after the step: in worlds where k_cg_step clamped a variable, w += A corr (the correction
+// product of k_cg_apply: its acceleration field comes from k_cg_accel, launched for the same worlds); then in every
+// iterating world the activation of compressed bound variables, z = M^-1 r on F and (r.z, error) per particle. One
+// kernel: the finish needs only the particle's own w. Activations are flagged in cg_act_new, not in cg_restart,
+// which decides here which worlds take the product.
+template <int NB>
+__global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
@@ -1432,12 +1439,18 @@ __global__ void __launch_bounds__(BLOCK) k_cg_finish(DevP P) {
   const float dt = P.dt;
   const bool div = P.mode == 0;
   const float scale = div ? dt : dt * dt;
-  const float wv = P.cg_w[p];
+  float wv = P.cg_w[p];
+  if (P.cg_restart[w] != 0) {
+    const float inv_r0 = 1.0f / P.vel[p].w;
+    const float t = ADF_FMA(-P.reg[p], P.cg_corr[p], accel_divergence<NB>(P, p, inv_r0));
+    wv = -(scale * t) + wv;
+    P.cg_w[p] = wv;
+  }
   int act = P.cg_act[p];
   if (!act && wv < 0.0f) {
     act = 1;
     P.cg_act[p] = 1;
-    atomicAdd(&P.cg_restart[w], 1);
+    P.cg_act_new[w] = 1;
   }
   const float zi = act ? ((-wv) * P.alpha[p]) / scale : 0.0f;
   P.cg_z[p] = zi;
@@ -1461,8 +1474,9 @@ __device__ __forceinline__ void cg_beta_world(const DevP& P, int w) {
   const float mean = (float)(sm.y / (na > 1.0 ? na : 1.0));
   P.err_mean[w] = mean;
   double beta = 0.0;
-  if (P.cg_restart[w] == 0 && P.cg_rz[w] > 1.0e-30) beta = sm.x / P.cg_rz[w];
+  if (P.cg_restart[w] == 0 && P.cg_act_new[w] == 0 && P.cg_rz[w] > 1.0e-30) beta = sm.x / P.cg_rz[w];
   P.cg_restart[w] = 0;
+  P.cg_act_new[w] = 0;
   P.cg_rz[w] = sm.x;
   P.cg_step[w] = beta;
   if ((it >= P.min_it && mean <= P.tol && P.emax[w] <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
