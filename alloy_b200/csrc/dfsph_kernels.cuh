@@ -18,6 +18,8 @@ namespace adf {
 
 constexpr int BLOCK = 256;
 constexpr int MAXCAP = 128;      // largest neighbor_capacity
+constexpr int WT = 4;            // lanes per near-wall particle in k_wall_slots
+constexpr int WT_CAP = 48;       // wall particles within h a team sorts in shared memory (more: one lane does it)
 constexpr int MAXWALL = 160;     // wall particles within h of one fluid particle (far above any lattice wall)
 constexpr int FLAG_ACTIVE = 1;
 constexpr int FLAG_PROXY = 2;
@@ -755,7 +757,10 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
 // wall id), its gradient and mean velocity; the distance phi with Psi(phi) = c; the slot filled as a flat wall at phi
 // with the fitted amplitude, offset and C1 taper. One slot per particle (no SDF shapes), so the inclusion-exclusion
 // combine of boundary.py:336-396 is the identity.
-// One listed liquid particle's wall slot (a tile of its 27 cells holds boundary particles).
+__device__ __forceinline__ void wall_slot_fill(const DevP& P, int p, float4 xi, float c, float gx, float gy, float gz,
+                                               float mx, float my, float mz);
+
+// One listed liquid particle's wall slot, by one lane (a cell of its 27 holds boundary particles).
 __device__ __forceinline__ void wall_slot_one(const DevP& P, int p) {
   const int w = P.world_s[p];
   const WorldGrid g = P.grid[w];
@@ -814,6 +819,13 @@ __device__ __forceinline__ void wall_slot_one(const DevP& P, int p) {
     my = ADF_FMA(wj, vj.y, my);
     mz = ADF_FMA(wj, vj.z, mz);
   }
+  wall_slot_fill(P, p, xi, c, gx, gy, gz, mx, my, mz);
+}
+
+// The slot of liquid particle p from its colour sums over the wall particles within h (ascending wall id): mean wall
+// velocity, distance by bisection, amplitude, taper, and the four slot records.
+__device__ __forceinline__ void wall_slot_fill(const DevP& P, int p, float4 xi, float c, float gx, float gy, float gz,
+                                               float mx, float my, float mz) {
   mx = mx / c;
   my = my / c;
   mz = mz / c;
@@ -844,8 +856,8 @@ __device__ __forceinline__ void wall_slot_one(const DevP& P, int p) {
 
 // Every liquid particle's slot starts empty; those whose 27 cells hold boundary particles (tiles checked first, then
 // the cells) are compacted within the block, in order (warp ballots, then the warps' counts scanned), and handed to
-// the block's first threads, so that the colour sums and bisections run in full warps: most liquid particles see no
-// wall particle, and the near-wall ones of a block are usually a minority of it.
+// teams of the block's lanes: most liquid particles see no wall particle, and the near-wall ones of a block are
+// usually a minority of it.
 __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
   __shared__ int list[BLOCK];
   __shared__ int wcount[BLOCK / 32];
@@ -893,7 +905,106 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
   }
   if (near) list[base + __popc(m & ((1u << lane) - 1u))] = p;
   __syncthreads();
-  if ((int)threadIdx.x < total) wall_slot_one(P, list[threadIdx.x]);
+  // WT lanes per listed particle (a team; BLOCK / WT particles per round): the team's lanes take the 9 cell rows in
+  // turn, append the wall particles within h (vol W > 0) to the team's buffer, rank them by original id, then compute
+  // the terms of the colour sums WT at a time while the team's first lane adds them in ascending id order, exactly as
+  // one lane does. A particle with more than WT_CAP such wall particles is done by its first lane alone.
+  __shared__ unsigned t_id[BLOCK / WT][WT_CAP];
+  __shared__ int t_j[BLOCK / WT][WT_CAP];
+  __shared__ int t_sorted[BLOCK / WT][WT_CAP];
+  __shared__ int t_cnt[BLOCK / WT];
+  const int tm = threadIdx.x / WT, t = threadIdx.x % WT;
+  const int t0 = lane - t;  // the team's first lane
+  for (int r0 = 0; r0 < total; r0 += BLOCK / WT) {
+    const int k = r0 + tm;
+    const bool act = k < total;
+    const int q = act ? list[k] : 0;
+    if (t == 0) t_cnt[tm] = 0;
+    __syncwarp();
+    float4 xi = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (act) {
+      const WorldGrid g = P.grid[P.world_s[q]];
+      xi = P.pos[q];
+      int cx, cy, cz;
+      cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
+      for (int r = t; r < 9; r += WT) {
+        const int z = cz + r / 3 - 1, y = cy + r % 3 - 1;
+        if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
+        for_row_ranges(P.cell_start, g, P.total_cells, y, z, max(cx - 1, 0), min(cx + 1, g.nx - 1),
+                       [&](int b, int e) {
+                         for (int j = b; j < e; ++j) {
+                           const float4 xj = P.pos[j];
+                           const float dx = xi.x - xj.x, dy2 = xi.y - xj.y, dz2 = xi.z - xj.z;
+                           float W, F;
+                           wf(P.kc, dot_plain(dx, dy2, dz2, dx, dy2, dz2), W, F);
+                           if (xj.w * W > 0.0f) {
+                             const int slot = atomicAdd(&t_cnt[tm], 1);
+                             if (slot < WT_CAP) {
+                               t_id[tm][slot] = (unsigned)P.id_of[j];
+                               t_j[tm][slot] = j;
+                             }
+                           }
+                         }
+                       });
+      }
+    }
+    __syncwarp();
+    const int mt = act ? t_cnt[tm] : 0;
+    const bool team = mt <= WT_CAP;  // else the one-lane path below
+    if (team) {
+      for (int h = t; h < mt; h += WT) {  // rank by original id (ids are distinct)
+        const unsigned id = t_id[tm][h];
+        int rank = 0;
+        for (int u = 0; u < mt; ++u) rank += t_id[tm][u] < id ? 1 : 0;
+        t_sorted[tm][rank] = t_j[tm][h];
+      }
+    }
+    __syncwarp();
+    const int mrun = __reduce_max_sync(0xffffffffu, team ? (unsigned)mt : 0u);
+    float c = 0.0f, gx = 0.0f, gy = 0.0f, gz = 0.0f, mx = 0.0f, my = 0.0f, mz = 0.0f;
+    for (int k0 = 0; k0 < mrun; k0 += WT) {
+      // lane t: the terms of entry k0 + t (the same expressions as the one-lane sum)
+      float wj = 0.0f, vol = 0.0f, ax = 0.0f, ay = 0.0f, az = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+      if (team && k0 + t < mt) {
+        const int j = t_sorted[tm][k0 + t];
+        const float4 xj = P.pos[j];
+        const float4 vj = P.vel[j];
+        const float dx = xi.x - xj.x, dy2 = xi.y - xj.y, dz2 = xi.z - xj.z;
+        float W, F;
+        wf(P.kc, dot_plain(dx, dy2, dz2, dx, dy2, dz2), W, F);
+        vol = xj.w;
+        wj = vol * W;
+        ax = dx * F;
+        ay = dy2 * F;
+        az = dz2 * F;
+        vx = vj.x;
+        vy = vj.y;
+        vz = vj.z;
+      }
+#pragma unroll
+      for (int u = 0; u < WT; ++u) {  // the first lane adds entries k0, k0 + 1, ... in order
+        const int src = t0 + u;
+        const float swj = __shfl_sync(0xffffffffu, wj, src), svol = __shfl_sync(0xffffffffu, vol, src);
+        const float sax = __shfl_sync(0xffffffffu, ax, src), say = __shfl_sync(0xffffffffu, ay, src);
+        const float saz = __shfl_sync(0xffffffffu, az, src), svx = __shfl_sync(0xffffffffu, vx, src);
+        const float svy = __shfl_sync(0xffffffffu, vy, src), svz = __shfl_sync(0xffffffffu, vz, src);
+        if (team && t == 0 && k0 + u < mt) {
+          c = c + swj;
+          gx = ADF_FMA(svol, sax, gx);
+          gy = ADF_FMA(svol, say, gy);
+          gz = ADF_FMA(svol, saz, gz);
+          mx = ADF_FMA(swj, svx, mx);
+          my = ADF_FMA(swj, svy, my);
+          mz = ADF_FMA(swj, svz, mz);
+        }
+      }
+    }
+    if (act && t == 0) {
+      if (!team) wall_slot_one(P, q);
+      else if (mt > 0) wall_slot_fill(P, q, xi, c, gx, gy, gz, mx, my, mz);
+    }
+    __syncwarp();
+  }
 }
 
 // Neighbour loops read their rows in batches of NB: the NB row entries first, then the NB gathers they address,
