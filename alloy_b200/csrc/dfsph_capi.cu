@@ -86,6 +86,10 @@ int fail(int code, const std::string& msg) {
 
 inline int blocks(long long n, int b = BLOCK) { return (int)((n + b - 1) / b); }
 
+// Models up to this many particles take the CG products by teams of TL lanes per particle: below it one lane per
+// particle fills less than a wave or two of the GPU (148 SMs x 2048 threads) and each lane's row is a chain of gathers.
+constexpr int CG_TEAM_MAX = 131072;
+
 template <class T> int dalloc(T** p, size_t count) {
   cudaError_t e = cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(count, 1));
   if (e != cudaSuccess) return fail(ADF_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
@@ -151,6 +155,7 @@ struct adf_solver {
   // learned warm start (adf_set_warm_model) and feature recording (adf_set_feature_recording)
   bool warm_on = false, feat_rec = false, warm_alloc = false, judge = true;
   bool cg = false;  // projected preconditioned CG pressure solve (adf_params.cg)
+  bool cg_team = false;  // CG products by teams of TL lanes per particle (models of at most CG_TEAM_MAX particles)
   __nv_bfloat16 *mw1 = nullptr, *mw2 = nullptr;
   float *mparams = nullptr, *mnorm = nullptr;
   int* merr = nullptr;
@@ -397,11 +402,13 @@ void cg_product(adf_solver* s, DevP& P, cudaStream_t st, const float* vec, const
   const TuneCfg& ca = s->tune[TK_ACCEL];
   const TuneCfg& cj = s->tune[TK_JACOBI];
   prof_begin(s, 5, st);
-  NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, vec, vr, gated);
+  if (s->cg_team) k_cg_accel_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, vec, vr, gated);
+  else NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, vec, vr, gated);
   ++s->launches;
   prof_end(s, st);
   prof_begin(s, 6, st);
-  NB_DISPATCH(k_cg_apply, cj.nb, blocks(n, cj.block), cj.block, st, P, vec, out, gated, bias, accumulate);
+  if (s->cg_team) k_cg_apply_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, vec, out, gated, bias, accumulate);
+  else NB_DISPATCH(k_cg_apply, cj.nb, blocks(n, cj.block), cj.block, st, P, vec, out, gated, bias, accumulate);
   ++s->launches;
   prof_end(s, st);
 }
@@ -435,12 +442,17 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
     const TuneCfg& ca = s->tune[TK_ACCEL];
     const TuneCfg& cj = s->tune[TK_JACOBI];
     prof_begin(s, 5, st);
-    NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, (const float*)P.cg_corr,
-                (const float*)P.cg_corrr, 1);
+    if (s->cg_team)
+      k_cg_accel_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, (const float*)P.cg_corr, (const float*)P.cg_corrr,
+                                                                   1);
+    else
+      NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, (const float*)P.cg_corr,
+                  (const float*)P.cg_corrr, 1);
     ++s->launches;
     prof_end(s, st);
     prof_begin(s, 6, st);
-    NB_DISPATCH(k_cg_apply_finish, cj.nb, blocks(n, cj.block), cj.block, st, P);
+    if (s->cg_team) k_cg_apply_finish_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P);
+    else NB_DISPATCH(k_cg_apply_finish, cj.nb, blocks(n, cj.block), cj.block, st, P);
     ++s->launches;
     prof_end(s, st);
   }
@@ -827,6 +839,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.iter_work, 1);
   rc |= s->alloc(&chunk_world, cb.size());
   s->cg = p.cg != 0;
+  s->cg_team = s->cg && n <= CG_TEAM_MAX;
   if (s->cg) {
     rc |= s->alloc(&d.cg_pd, n);
     rc |= s->alloc(&d.cg_pdr, n);

@@ -1485,6 +1485,142 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply(DevP P, const float* vec, fl
   out[p] = v;
 }
 
+// Team variants of the CG products for worlds too small to fill the GPU with one lane per particle (a 30k-particle
+// world is less than one wave, and each lane's row is a chain of dependent gathers): TL lanes share one particle,
+// lane t gathers row entries t, t + TL, ... (TB of them per round) and computes their terms, and the team's first
+// lane adds the terms in row order with the one-lane loop's own operations, so the results are bit-identical.
+constexpr int TL = 4;  // lanes per particle
+constexpr int TB = 4;  // row entries per lane per round
+
+struct Team {
+  int t, t0;       // this lane's rank in the team, the team's first lane (in the warp)
+  unsigned mask;   // the team's lanes
+};
+
+__device__ __forceinline__ Team team_of(int& p) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  p = g / TL;
+  Team tm;
+  tm.t = g % TL;
+  tm.t0 = (threadIdx.x & 31) - tm.t;
+  tm.mask = ((1u << TL) - 1u) << tm.t0;
+  return tm;
+}
+
+__device__ __forceinline__ int2 row_entry(const DevP& P, int p, int k) { return __ldcs(P.nbrjf + p + (size_t)k * P.n); }
+
+// pressure_accel with the fields of Q (kappa, kr), valid in the team's first lane
+__device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, float4 xi, const Team& tm, float& ax, float& ay,
+                                                    float& az) {
+  const float ki = Q.kr[p];
+  ax = ay = az = 0.0f;
+  const int c = Q.cnt[p];
+  for (int k0 = 0; k0 < c; k0 += TL * TB) {
+    float cf[TB], rx[TB], ry[TB], rz[TB];
+#pragma unroll
+    for (int u = 0; u < TB; ++u) {
+      const int k = k0 + u * TL + tm.t;
+      cf[u] = rx[u] = ry[u] = rz[u] = 0.0f;
+      if (k < c) {
+        const int2 e = row_entry(Q, p, k);
+        const float4 xj = Q.pos[e.x];
+        const float kj = Q.kr[e.x];
+        rx[u] = xi.x - xj.x;
+        ry[u] = xi.y - xj.y;
+        rz[u] = xi.z - xj.z;
+        cf[u] = (xj.w * (ki + kj)) * __int_as_float(e.y);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < TB; ++u) {
+#pragma unroll
+      for (int s = 0; s < TL; ++s) {
+        const float a = __shfl_sync(tm.mask, cf[u], tm.t0 + s), x = __shfl_sync(tm.mask, rx[u], tm.t0 + s);
+        const float y = __shfl_sync(tm.mask, ry[u], tm.t0 + s), z = __shfl_sync(tm.mask, rz[u], tm.t0 + s);
+        if (tm.t == 0 && k0 + u * TL + s < c) {
+          ax = ADF_FMA(-a, x, ax);
+          ay = ADF_FMA(-a, y, ay);
+          az = ADF_FMA(-a, z, az);
+        }
+      }
+    }
+  }
+  const float4 sg = Q.slot_g[p];
+  if (sg.w >= 0.0f) {
+    const float kk = Q.kappa[p];
+    ax = ADF_FMA(-kk, sg.x, ax);
+    ay = ADF_FMA(-kk, sg.y, ay);
+    az = ADF_FMA(-kk, sg.z, az);
+  }
+}
+
+// accel_divergence, valid in the team's first lane
+__device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, float inv_r0, const Team& tm) {
+  const float4 xi = P.pos[p];
+  const float4 ai = P.acc[p];
+  float ar = 0.0f;
+  const int c = P.cnt[p];
+  for (int k0 = 0; k0 < c; k0 += TL * TB) {
+    float af[TB], d[TB];
+#pragma unroll
+    for (int u = 0; u < TB; ++u) {
+      const int k = k0 + u * TL + tm.t;
+      af[u] = d[u] = 0.0f;
+      if (k < c) {
+        const int2 e = row_entry(P, p, k);
+        const float4 xj = P.pos[e.x], aj = P.acc[e.x];
+        const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+        af[u] = (xj.w * inv_r0) * __int_as_float(e.y);
+        d[u] = dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < TB; ++u) {
+#pragma unroll
+      for (int s = 0; s < TL; ++s) {
+        const float a = __shfl_sync(tm.mask, af[u], tm.t0 + s), b = __shfl_sync(tm.mask, d[u], tm.t0 + s);
+        if (tm.t == 0 && k0 + u * TL + s < c) ar = ADF_FMA(a, b, ar);
+      }
+    }
+  }
+  const float4 sg = P.slot_g[p];
+  if (sg.w >= 0.0f) ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
+  return ar;
+}
+
+// k_cg_accel by teams (grid: TL threads per particle)
+__global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* vec, const float* vr, int gated) {
+  int p;
+  const Team tm = team_of(p);
+  if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
+  DevP Q = P;
+  Q.kappa = const_cast<float*>(vec);
+  Q.kr = const_cast<float*>(vr);
+  float ax, ay, az;
+  pressure_accel_team(Q, p, P.pos[p], tm, ax, ay, az);
+  if (tm.t == 0) P.acc[p] = make_float4(ax, ay, az, 0.0f);
+}
+
+// k_cg_apply by teams
+__global__ void __launch_bounds__(BLOCK) k_cg_apply_team(DevP P, const float* vec, float* out, int gated, int bias,
+                                                         int accumulate) {
+  int p;
+  const Team tm = team_of(p);
+  if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
+  const float inv_r0 = 1.0f / P.vel[p].w;
+  const float ar = accel_divergence_team(P, p, inv_r0, tm);
+  if (tm.t != 0) return;
+  const float dt = P.dt;
+  const bool div = P.mode == 0;
+  const float scale = div ? dt : dt * dt;
+  const float t = ADF_FMA(-P.reg[p], vec[p], ar);
+  float v = -(scale * t);
+  P.cg_pair[P.id_of[p]] = make_float2(vec[p] * v, 0.0f);
+  if (bias) v = v - (div ? P.src[p] : P.src[p] - 1.0f);
+  if (accumulate) v = v + out[p];
+  out[p] = v;
+}
+
 // krylov.py:104-133: active set, z = M^-1 r on F (r = -w), first direction p = z; pair.x = r.z
 __global__ void __launch_bounds__(BLOCK) k_cg_init(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1541,6 +1677,27 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(DevP P) {
 // iterating world the activation of compressed bound variables, z = M^-1 r on F and (r.z, error) per particle. One
 // kernel: the finish needs only the particle's own w. Activations are flagged in cg_act_new, not in cg_restart,
 // which decides here which worlds take the product.
+// The finish of one particle after its w update (activation, z, r.z and error).
+__device__ __forceinline__ void cg_finish_one(const DevP& P, int p, int w, float wv, float scale, bool div) {
+  int act = P.cg_act[p];
+  if (!act && wv < 0.0f) {
+    act = 1;
+    P.cg_act[p] = 1;
+    P.cg_act_new[w] = 1;
+  }
+  const float zi = act ? ((-wv) * P.alpha[p]) / scale : 0.0f;
+  P.cg_z[p] = zi;
+  float e = maxr(-wv, 0.0f);
+  if (P.kappa[p] > P.lower[p]) e = fabsf(wv);
+  if (div) {
+    if (P.neff[p] < P.min_nb) e = 0.0f;
+    e = e * P.dt;
+  }
+  const int i = P.id_of[p];
+  P.err_orig[i] = e;
+  P.cg_pair[i] = make_float2(-wv * zi, e);
+}
+
 template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1557,23 +1714,30 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
     wv = -(scale * t) + wv;
     P.cg_w[p] = wv;
   }
-  int act = P.cg_act[p];
-  if (!act && wv < 0.0f) {
-    act = 1;
-    P.cg_act[p] = 1;
-    P.cg_act_new[w] = 1;
+  cg_finish_one(P, p, w, wv, scale, div);
+}
+
+// k_cg_apply_finish by teams
+__global__ void __launch_bounds__(BLOCK) k_cg_apply_finish_team(DevP P) {
+  int p;
+  const Team tm = team_of(p);
+  if (p >= P.nfw[0]) return;
+  const int w = P.world_s[p];
+  if (P.converged[w]) return;
+  const float dt = P.dt;
+  const bool div = P.mode == 0;
+  const float scale = div ? dt : dt * dt;
+  float wv = P.cg_w[p];
+  if (P.cg_restart[w] != 0) {
+    const float inv_r0 = 1.0f / P.vel[p].w;
+    const float ar = accel_divergence_team(P, p, inv_r0, tm);
+    if (tm.t == 0) {
+      const float t = ADF_FMA(-P.reg[p], P.cg_corr[p], ar);
+      wv = -(scale * t) + wv;
+      P.cg_w[p] = wv;
+    }
   }
-  const float zi = act ? ((-wv) * P.alpha[p]) / scale : 0.0f;
-  P.cg_z[p] = zi;
-  float e = maxr(-wv, 0.0f);
-  if (P.kappa[p] > P.lower[p]) e = fabsf(wv);
-  if (div) {
-    if (P.neff[p] < P.min_nb) e = 0.0f;
-    e = e * dt;
-  }
-  const int i = P.id_of[p];
-  P.err_orig[i] = e;
-  P.cg_pair[i] = make_float2(-wv * zi, e);
+  if (tm.t == 0) cg_finish_one(P, p, w, wv, scale, div);
 }
 
 // krylov.py:207-233: per world the stop test (as k_world_check), then beta = r.z_new / r.z (0 after a set change)
