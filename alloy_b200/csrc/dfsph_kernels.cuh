@@ -1449,7 +1449,7 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
 // ------------------------------------------------------------------------------------ projected CG (krylov.py)
 // One CG per world on w = A k - b, k >= k_lo (krylov.py:1-17), A k = -dt^n (Ar(k) - reg k). Each kernel follows
 // the reference kernel of the same name (krylov.py:71-246); a + b c updates are fused (the oracle fuses the same
-// ones), per-world dot products are the float64 sums of k_chunk_sum2 / k_world_sum2 in the caller's order.
+// ones), per-world dot products are the float64 sums of k_sums2_fused in the caller's order.
 __device__ __forceinline__ bool cg_skip(const DevP& P, int w, int gated) {
   return P.converged[w] != 0 || (gated && P.cg_restart[w] == 0);
 }
@@ -1775,25 +1775,8 @@ __global__ void __launch_bounds__(BLOCK) k_cg_direction(DevP P) {
   P.cg_pdr[p] = pd / P.vel[p].w;
 }
 
-// Per-world (sum x, sum y, max y) of the CG pairs: chunk partials (chunks of converged worlds skipped), then one
-// block per world in the fixed tree order of k_world_check; the maximum floored at 0 goes to emax when asked.
-__global__ void __launch_bounds__(256) k_chunk_sum2(DevP P) {
-  __shared__ double smd[8];
-  __shared__ float smf[8];
-  const int c = blockIdx.x;
-  if (P.converged[P.chunk_world[c]]) return;
-  const int i = P.chunk_begin[c] + threadIdx.x;
-  const bool in = i < P.chunk_end[c];
-  const float2 v = in ? P.cg_pair[i] : make_float2(0.0f, 0.0f);
-  const double sx = fold256(in ? (double)v.x : 0.0, smd);
-  const double sy = fold256(in ? (double)v.y : 0.0, smd);
-  const float m = block_max256(in ? v.y : -3.4e38f, smf);
-  if (threadIdx.x == 0) {
-    P.part2[c] = make_double2(sx, sy);
-    P.part_max[c] = m;
-  }
-}
-
+// Per-world (sum x, sum y, max y) of the CG pairs for models without chunks (no particles): one block per world in
+// the fixed tree order of k_world_check; k_sums2_fused does it in one launch otherwise.
 __global__ void __launch_bounds__(256) k_world_sum2(DevP P, int with_max) {
   __shared__ double smd[8];
   __shared__ float smf[8];
@@ -1944,7 +1927,7 @@ __global__ void __launch_bounds__(256) k_check_fused(DevP P) {
   }
 }
 
-// The CG reductions in one launch (k_chunk_sum2 and k_world_sum2 fused, same partials and tree order); with `beta`
+// The CG reductions in one launch (chunk partials and k_world_sum2's world fold, same tree order); with `beta`
 // the world's last block also runs k_cg_beta's stop test and beta for its world, and the grid's last block stores the
 // count of worlds still iterating as the unconverged count.
 __global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int beta) {
