@@ -9,11 +9,14 @@ float64 per-world residual sums. A step is one full DFSPH step over every partic
 
 Other workloads (--workload): dam_break (8,000 particles, 1 world), batched_worlds (256 uneven worlds with spouts,
 world shards across ranks), pour_bowls (4,096 worlds of 4,096-16,384 particles, each a moving hemisphere bowl of
-boundary particles with a spout; the bowls' velocities are set before every step, inside the timed region).
+boundary particles with a spout; the bowls' velocities are set before every step, inside the timed region), and the
+reference's own speed-harness scenes at r = 2 mm, primed before stepping: column_30k (a resting 32 x 32 x 30 column,
+fast preset, CG), dam_break_30k (32 x 32 x 30 against the wall of a 96-spacing tank, default config) and
+columns_256x4k (256 resting 16 x 16 x 16 columns).
 
 Arms:
   --impl b200       this package's CUDA path (one process per GPU; N > 1 runs N replicas of the single world:
-                    the path has no data-path collective, see DESIGN.md)
+                    the path has no data-path collective)
   --impl reference  the reference algorithm on the host cores: the CPU oracle (a restatement of the reference's
                     Warp kernels; Warp itself is not installed) with every host thread, rank 0 only.
 """
