@@ -88,3 +88,13 @@ def test_cg_falls_back_to_jacobi_for_unequal_masses(cuda):
     sc.model.particle_mass[: sc.fluid_count // 2] *= 1.01
     sol = SolverDFSPH(sc.model, sc.config)
     assert sol.pressure_solver == "jacobi"
+
+
+def test_cg_one_lane_products_in_a_large_model_bit_exact(cuda):
+    """Models of more than 131,072 particles take the CG products with one lane per particle (smaller ones by teams of
+    four lanes, which every other test here exercises): a 139,776-particle dam break against the oracle."""
+    sc = dam_break(counts=(56, 48, 52), box=(0.8, 0.6, 0.8), spacing=0.01, device=cuda, pressure_solver="cg")
+    assert sc.model.particle_count > 131072
+    sol = SolverDFSPH(sc.model, sc.config)
+    orc = Oracle(sc.model.host(), sc.config)
+    _compare(sc, sol, orc, 8)

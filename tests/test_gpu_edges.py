@@ -1,8 +1,9 @@
 # SPDX-License-Identifier: Apache-2.0
 """Edge cases of the CUDA path against the oracle, bit for bit: worlds without liquid (walls only, spares only) beside
 a liquid world, a model without particles, neighbour rows that overflow a small capacity (lowest ids kept, overflow
-counted, neighbors.py:131-195), the shared-memory list path of capacities above 64, the Wendland C2 kernel, and a sink
-emptying liquid into the ledger; then reset restores flags, phase and warm starts of the masked worlds."""
+counted, neighbors.py:131-195), the shared-memory list path of capacities above 64, the Wendland C2 kernel, a sink
+emptying liquid into the ledger (then reset restores flags, phase and warm starts of the masked worlds), and walls dense
+enough that some liquid particles' wall slots are done by one lane instead of a team of four."""
 
 from __future__ import annotations
 
@@ -11,7 +12,7 @@ import pytest
 import torch
 
 from alloy_b200.solvers.sph import SolverDFSPH
-from alloy_b200.solvers.sph.build import add_fluid_block, add_particle_box, add_spares
+from alloy_b200.solvers.sph.build import add_fluid_block, add_particle_box, add_spares, add_wall_particles, box_shell_points
 from alloy_b200.solvers.sph.model import ModelBuilder
 from alloy_b200.solvers.sph.solver import _xform7
 from alloy_b200.solvers.sph.testing import benchmark_config, dam_break
@@ -132,3 +133,22 @@ def test_capability_factory_builds_a_working_solver(cuda):
         a, b = b, a
     r = sol.report()
     assert r.iters_density[0] >= 2 and r.escaped[0] == 0
+
+
+def test_dense_walls_take_the_one_lane_wall_slot_path(cuda):
+    """Walls of boundary particles at half the liquid spacing: liquid particles near an edge or corner see more than 48
+    wall particles within h, which the four-lane wall-slot teams leave to one lane; both paths agree with the oracle."""
+    cfg = benchmark_config(0.02)
+    s = cfg.spacing
+    b = ModelBuilder()
+    b.begin_world()
+    add_fluid_block(b, cfg, (0.0, 0.0, 0.0), (6, 6, 6), jitter=0.01, seed=3)
+    add_wall_particles(b, cfg, box_shell_points((0.0, 0.0, 0.0), (8 * s, 8 * s, 10 * s), 0.5 * s), spacing=0.5 * s)
+    b.end_world()
+    model = b.finalize(cuda)
+    host = model.host()
+    q = host["q"].reshape(-1, 3)
+    fl, wl = host["phase"] >= 1, host["phase"] == -1
+    d2 = ((q[fl][:, None, :] - q[wl][None, :, :]) ** 2).sum(-1)
+    assert ((d2 < cfg.h * cfg.h).sum(1) > 48).any()  # some liquid particle takes the one-lane path
+    _lockstep(model, cfg, 1.0e-3, 8)
