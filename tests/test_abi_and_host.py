@@ -149,3 +149,41 @@ def test_plugin_factory_contract():
     assert CAPABILITY.name == "sph" and CAPABILITY.routes == frozenset({"liquid_sph"})
     register()
     assert REGISTRY["sph"]["capability"] is CAPABILITY
+
+
+def test_speed_harness_scenes_follow_the_reference_harness():
+    """The reference's own speed scenes (tests/solvers/sph/test_speed_gpu.py:24-39, alloy/testing/sph.py:49-115):
+    sizes, config and dt; the tanks are boundary-particle boxes on the same inner box."""
+    from alloy_b200.solvers.sph.testing import tank_dam_break, water_column
+
+    col = water_column(32, 32, 30, r=2.0e-3)
+    cfg = col.config
+    assert col.fluid_count == 30720 and col.model.world_count == 1
+    assert cfg.pressure_solver == "cg" and cfg.cfl == 0.4 and cfg.rest_jitter_speed is None  # the fast preset
+    assert col.dt == cfg.dt_max == 1.25e-3
+    q = col.model.host()["q"].reshape(-1, 3)
+    wall = col.model.host()["phase"] == -1
+    s = cfg.spacing
+    assert np.isclose(q[wall][:, 2].max(), (30 + 8) * s + 0.5 * s)  # headroom of 8 layers, closed top
+    many = water_column(16, 16, 16, worlds=3, r=2.0e-3)
+    assert many.fluid_count == 3 * 4096 and many.model.world_count == 3
+    dam = tank_dam_break(32, 30, 32, 96, r=2.0e-3)
+    assert dam.fluid_count == 30720 and dam.config.pressure_solver == "cg" and dam.config.cfl == 0.2
+    assert dam.dt == C.snap_down(C.stable_dt(dam.config, 2.0 * (9.81 * 30 * s) ** 0.5), 0.02) == 0.02 / 64
+    qd = dam.model.host()["q"].reshape(-1, 3)
+    assert np.isclose(qd[dam.model.host()["phase"] == -1][:, 0].max(), 96 * s + 0.5 * s)
+
+
+def test_bench_reports_the_harness_figures():
+    """rt_factor = dt / wall time per step; world-s per wall-s = worlds x dt / wall time per step
+    (test_speed_gpu.py:28-39); vs_baseline on the resting column against the published 4.6 ms per step."""
+    import bench
+    from alloy_b200.solvers.sph.testing import water_column
+
+    sc = water_column(8, 8, 8, worlds=4, r=2.0e-3)
+    f = bench.liq9_fields("columns_256x4k", sc, 2.0e-3)
+    assert f["world_s_per_wall_s"] == pytest.approx(4 * 1.25e-3 / 2.0e-3)
+    col = water_column(8, 8, 8, r=2.0e-3)
+    assert bench.liq9_fields("column_30k", col, 1.0e-3)["rt_factor"] == pytest.approx(1.25)
+    assert bench.liq9_fields("large_dam_break", col, 1.0e-3) == {}
+    assert bench.LIQ9_PUBLISHED["column_30k"] == pytest.approx(30720 / 4.6e-3)
