@@ -5,7 +5,9 @@
 Workload (default): the 1,048,576-particle dam break (128 x 64 x 128 block at 0.01 m, seeded +-1 % jitter) in a
 closed 4 x 2 x 2 m tank of boundary particles, dt 0.5 ms, cubic kernel, Jacobi, tolerances 1e-3, FP32 particles with
 float64 per-world residual sums. A step is one full DFSPH step over every particle; steps continue the same run
-(warm starts carried). The working set per step (~0.9 GB) is far larger than L2, so no flush is needed between steps.
+(warm starts carried). The working set per step (~1.4 GB) is far larger than L2, so no flush is needed between steps;
+workloads whose working set could stay in L2 (the 30k scenes) get a 256 MB write between timed steps, outside the
+per-step CUDA events.
 
 Other workloads (--workload): dam_break (8,000 particles, 1 world), batched_worlds (256 uneven worlds with spouts,
 world shards across ranks), pour_bowls (4,096 worlds of 4,096-16,384 particles, each a moving hemisphere bowl of
@@ -183,7 +185,29 @@ def workload_config(sc, name: str) -> dict:
     return {"workload": f"{name}: {sc.fluid_count} liquid particles + {sc.wall_count} boundary particles in {W} "
                         f"world(s), dt {sc.dt} s, {solver}, tol 1e-3/1e-3, cubic h=2 spacings" + extra,
             "liquid_particles": sc.fluid_count, "boundary_particles": sc.wall_count, "worlds": W, "dt": sc.dt,
-            "spacing": sc.config.spacing, "l2": "inputs larger than L2 (working set > 126 MB per step)"}
+            "spacing": sc.config.spacing, "l2": l2_note(sc)}
+
+
+L2_BYTES = 126 << 20  # B200 L2
+FLUSH_BYTES = 256 << 20  # written between timed steps when a workload's working set could stay in L2
+
+
+def working_set(sc) -> int:
+    """Device bytes a step touches, estimated from the particle count: the neighbour rows (K entries of a 4-byte
+    index and an 8-byte (index, F) pair) and about 200 bytes of per-particle arrays."""
+    return int(sc.model.particle_count) * (12 * int(sc.config.neighbor_capacity) + 200)
+
+
+def l2_resident(sc) -> bool:
+    return working_set(sc) < 2 * L2_BYTES
+
+
+def l2_note(sc) -> str:
+    mb = working_set(sc) / 2**20
+    if l2_resident(sc):
+        return (f"working set ~{mb:.0f} MB fits in L2 (126 MB): L2 flushed between timed steps by a 256 MB write "
+                "outside the per-step CUDA events; the end-to-end pass runs its steps back to back")
+    return f"inputs larger than L2 (working set ~{mb:.0f} MB per step)"
 
 
 def peaks() -> dict:
@@ -456,6 +480,9 @@ def run_b200(args):
         dist.barrier()
     launches0 = sol.kernel_launches()
 
+    # a working set that fits in L2 is flushed before every timed step (outside the step's events)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev) if l2_resident(sc) else None
+
     def timed():
         clocks = Clocks(dev)
         clocks.start()
@@ -463,13 +490,26 @@ def run_b200(args):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
-        e0.record(stream)
-        run(args.steps)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
+        if flush is None:
+            e0.record(stream)
+            run(args.steps)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            seconds = e0.elapsed_time(e1) * 1e-3
+        else:
+            marks = []
+            for _ in range(args.steps):
+                flush.fill_(1)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                run(1)
+                b.record(stream)
+                marks.append((a, b))
+            torch.cuda.synchronize(dev)
+            seconds = sum(a.elapsed_time(b) for a, b in marks) * 1e-3
         if world > 1:
             dist.barrier()
-        return e0.elapsed_time(e1) * 1e-3, clocks.stop()
+        return seconds, clocks.stop()
 
     nf0 = sol.list_stats()[0]
     t, clk = timed()
