@@ -112,4 +112,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) < 2:
+        raise SystemExit(__doc__)
+    main(Path(sys.argv[1]))

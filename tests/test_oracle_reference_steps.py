@@ -1,0 +1,116 @@
+# SPDX-License-Identifier: Apache-2.0
+"""The CPU oracle against the reference's OWN kernels at step level.
+
+The fixtures ``tests/golden/reference_steps_<case>.npz`` hold DFSPH steps computed by the reference's Warp kernels and
+solve driver (alloy/solvers/sph: neighbors.py:160-195, boundary.py:190-396, particle_walls.py:65-135,
+pressure.py:144-480, krylov.py, solve_driver.py:121-186, integrate.py:150-326) run under a float32 warp stand-in
+(``tests/golden/make_step_golden.py``, ``tests/golden/refrun.py``). Two comparisons per case:
+
+- anchored: every step starts the oracle from the reference's own start state and warm starts, so each step's
+  differences are that step's alone;
+- free running: the oracle steps from the initial state on its own, as a user's run would.
+
+Bit for bit: neighbour rows and counts (integer ids), per-solve iteration counts (every step, both comparisons).
+Within tolerance (the reference's Warp code generation may contract multiply-adds and its wall-colour sums follow
+Warp's hash order, neither pinned; the oracle fixes both orders and spells its fused multiply-adds out), each
+relative to the field's largest magnitude over the liquid unless it says otherwise: ``TOL`` below.
+"""
+
+from __future__ import annotations
+
+import ast
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from alloy_b200.solvers.sph.testing import dam_break
+from oracle.pyoracle import Oracle
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+CASES = ("dam_break_jacobi", "dam_break_cg", "column_jacobi_tight")
+# Largest differences measured over the three cases, for scale: ratio 3.6e-6, alpha 1.4e-5, neff 4.7e-6, slot psi
+# 6.5e-6, slot phi 4.9e-7, kv 2.3e-5, kd 1.8e-3, q 4.5e-8 m (1.3e-7 m free running), qd 4.8e-5, mean errors 1.9e-3.
+TOL = {"ratio": 1e-4, "alpha": 1e-4, "neff": 1e-4, "reg": 1e-4, "slot_psi": 1e-4, "slot_phi": 1e-5, "kv": 2e-4,
+       "kd": 1e-2, "qd": 5e-4, "q_abs_m": 1e-6, "err_rel": 1e-2}
+
+
+def load(case: str):
+    g = np.load(GOLDEN / f"reference_steps_{case}.npz")
+    c = ast.literal_eval(str(g["scene"]))
+    sc = dam_break(device="cpu", **c["scene"], **c["config"])
+    return g, c, sc
+
+
+def rel(x, y, m) -> float:
+    return float(np.max(np.abs(x[m] - y[m])) / (np.max(np.abs(y[m])) + 1e-30))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fixture_matches_scene(case):
+    """The fixture was made from the scene the test builds: same start state, same particle count."""
+    g, c, sc = load(case)
+    a = sc.model.host()
+    np.testing.assert_array_equal(g["q0"][0], a["q"])
+    np.testing.assert_array_equal(g["qd0"][0], a["qd"])
+    assert int(g["steps"]) == c["steps"] >= 10
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_anchored_steps_match_reference_kernels(case):
+    g, c, sc = load(case)
+    a = sc.model.host()
+    fluid = a["phase"] >= 1
+    dt = c["scene"]["dt"]
+    orc = Oracle(a, sc.config)
+    for s in range(int(g["steps"])):
+        orc.set_state(g["q0"][s], g["qd0"][s])
+        orc.set_warm(g["kv0"][s], g["kd0"][s])
+        orc.step(dt)
+        rows, cnt = orc.lists()
+        np.testing.assert_array_equal(cnt[fluid], g["count"][s][fluid], err_msg=f"{case} step {s} counts")
+        for i in np.flatnonzero(fluid):
+            np.testing.assert_array_equal(rows[i, :cnt[i]], g["rows"][s][i, :cnt[i]], err_msg=f"{case} step {s} row {i}")
+        rep = orc.report()
+        assert rep["iters_divergence"][0] == g["iters_div"][s][0], (case, s)
+        assert rep["iters_density"][0] == g["iters_den"][s][0], (case, s)
+        for name in ("ratio", "alpha", "neff", "reg", "slot_psi"):
+            assert rel(orc.field(name), g[name][s], fluid) <= TOL[name], \
+                (case, s, name)
+        on = fluid & (g["slot_shape"][s] >= 0)
+        assert on.any() or s > 0
+        if on.any():
+            assert rel(orc.field("slot_phi"), g["slot_phi"][s], on) <= TOL["slot_phi"], (case, s)
+        kv, kd = orc.warm()
+        assert rel(kv, g["kv"][s], fluid) <= TOL["kv"], (case, s)
+        assert rel(kd, g["kd"][s], fluid) <= TOL["kd"], (case, s)
+        q, qd = orc.state()
+        assert float(np.max(np.abs(q - g["q1"][s])[fluid])) <= TOL["q_abs_m"], (case, s)
+        assert rel(qd, g["qd1"][s], fluid) <= TOL["qd"], (case, s)
+        for ours, ref in (("density_err", "den_err"), ("divergence_err", "div_err")):
+            r = float(g[ref][s][0])
+            assert abs(float(rep[ours][0]) - r) <= TOL["err_rel"] * r + 1e-9, (case, s, ours)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_free_run_matches_reference_kernels(case):
+    g, c, sc = load(case)
+    a = sc.model.host()
+    fluid = a["phase"] >= 1
+    orc = Oracle(a, sc.config)
+    for s in range(int(g["steps"])):
+        orc.step(c["scene"]["dt"])
+        q, qd = orc.state()
+        rep = orc.report()
+        assert rep["iters_divergence"][0] == g["iters_div"][s][0], (case, s)
+        assert rep["iters_density"][0] == g["iters_den"][s][0], (case, s)
+        assert float(np.max(np.abs(q - g["q1"][s])[fluid])) <= TOL["q_abs_m"], (case, s)
+        assert rel(qd, g["qd1"][s], fluid) <= TOL["qd"], (case, s)
+
+
+def test_cases_cover_both_solvers_and_the_iteration_cap():
+    """The fixtures exercise relaxed Jacobi, projected CG, multi-iteration solves and the 50-iteration cap."""
+    its = {case: (load(case)[0]["iters_div"][:, 0], load(case)[0]["iters_den"][:, 0]) for case in CASES}
+    assert load("dam_break_cg")[1]["config"]["pressure_solver"] == "cg"
+    div, den = its["column_jacobi_tight"]
+    assert div.max() == 50 and den.max() > 2
