@@ -21,7 +21,8 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_mlp_destroy", "adf_mlp_set_params", "adf_mlp_get_params", "adf_mlp_forward", "adf_mlp_gradient",
            "adf_mlp_train_step", "adf_mlp_status", "adf_set_warm_model", "adf_set_feature_recording",
            "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs", "adf_add_emitters",
-           "adf_prime", "adf_iteration_work", "adf_set_tuned_config")
+           "adf_prime", "adf_iteration_work", "adf_set_tuned_config", "adf_get_state_storage", "adf_port_take",
+           "adf_port_emit", "adf_energy", "adf_stable_dt")
 TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph", "lists")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
@@ -56,6 +57,15 @@ class Report(C.Structure):
         "density_err", "divergence_err", "iters_density", "iters_divergence", "mass_in", "mass_out", "mass_initial",
         "escaped", "neighbor_overflow", "max_speed", "density_err_max", "projected", "nonfinite", "emitter_overflow",
         "density_tol", "learned_divergence", "learned_density")]
+
+
+class StateStorage(C.Structure):
+    """adf_state_storage"""
+    _fields_ = [("mass_in", C.c_void_p), ("mass_out", C.c_void_p), ("escaped", C.c_void_p), ("emit_t", C.c_void_p),
+                ("emit_cursor", C.c_void_p), ("emit_world", C.c_void_p), ("n_emitters", C.c_int32),
+                ("port_stack", C.c_void_p), ("port_top", C.c_void_p), ("port_absorbed", C.c_void_p),
+                ("port_emitted", C.c_void_p), ("port_retired", C.c_void_p), ("port_taken", C.c_void_p),
+                ("port_granted", C.c_void_p)]
 
 
 _lib = None
@@ -116,6 +126,11 @@ def lib() -> C.CDLL:
     L.adf_set_warm_judging.argtypes = [P, i]
     L.adf_set_autotune.argtypes = [P, i]
     L.adf_tuned_configs.argtypes = [P, vp, vp, vp]
+    L.adf_get_state_storage.argtypes = [P, C.POINTER(StateStorage)]
+    L.adf_port_take.argtypes = [P, vp, vp, i, vp]
+    L.adf_port_emit.argtypes = [P, vp, vp, vp, vp, i, vp, vp]
+    L.adf_energy.argtypes = [P, vp, vp, vp, vp, vp]
+    L.adf_stable_dt.argtypes = [P, vp, C.c_double, C.c_double, C.c_double, vp, vp]
     for name in EXPORTS:
         if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches", "adf_mlp_destroy"):
             getattr(L, name).restype = C.c_int

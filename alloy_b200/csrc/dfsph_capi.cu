@@ -14,6 +14,7 @@
 #include "../../include/alloy_dfsph.h"
 #include "dfsph_kernels.cuh"
 #include "dfsph_mlp.cuh"
+#include "dfsph_port.cuh"
 
 using namespace adf;
 
@@ -124,8 +125,17 @@ struct adf_solver {
   int *off_emitter_d = nullptr, *off_rank_d = nullptr, *pool_d = nullptr, *enabled_d = nullptr;
   int *cursor_d = nullptr, *emit_now_d = nullptr;
   float* t_acc_d = nullptr;
+  int* em_world_d = nullptr;  // [E] world of each emitter (the snapshot keys' item -> world map)
   std::vector<Sink> sinks_h;
   Sink* sinks_d = nullptr;
+  // the port (ports.py): world w's held particles are a stack in its own index range [ws[w], ws[w + 1])
+  int* ws_d = nullptr;  // [W + 1] world starts
+  int *port_stack = nullptr, *port_stack0 = nullptr, *port_top = nullptr, *port_top0 = nullptr;
+  int *port_taken = nullptr, *port_granted = nullptr, *port_absorbed = nullptr, *port_emitted = nullptr;
+  int* port_retired = nullptr;
+  // scratch of the between-step calls (adf_energy, adf_stable_dt)
+  float* energy_max = nullptr;
+  int* speed_bits = nullptr;
   // host side of the iteration loop
   int* pinned = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -676,15 +686,19 @@ int upload_emitters(adf_solver* s, int n_carry) {
       CK(cudaMemcpy(c_old.data(), s->cursor_d, sizeof(int) * n_old, cudaMemcpyDeviceToHost));
     }
     void* olds[] = {s->em_d, s->off_local_d, s->off_emitter_d, s->off_rank_d, s->pool_d, s->enabled_d, s->cursor_d,
-                    s->emit_now_d, s->t_acc_d};
+                    s->emit_now_d, s->t_acc_d, s->em_world_d};
     for (void* p : olds) cudaFree(p);
   }
   int ne = (int)s->em_h.size();
   int no = (int)s->off_emitter_h.size();
   int rc = dalloc(&s->em_d, ne) | dalloc(&s->off_local_d, 3 * (size_t)no) | dalloc(&s->off_emitter_d, no) |
            dalloc(&s->off_rank_d, no) | dalloc(&s->pool_d, s->pool_h.size()) | dalloc(&s->enabled_d, ne) |
-           dalloc(&s->cursor_d, ne) | dalloc(&s->emit_now_d, ne) | dalloc(&s->t_acc_d, ne);
+           dalloc(&s->cursor_d, ne) | dalloc(&s->emit_now_d, ne) | dalloc(&s->t_acc_d, ne) |
+           dalloc(&s->em_world_d, ne);
   if (rc) return fail(ADF_ERR_CUDA, "emitter tables: cudaMalloc failed");
+  std::vector<int> em_world(ne);
+  for (int e = 0; e < ne; ++e) em_world[e] = s->em_h[e].world;
+  if (ne) CK(cudaMemcpy(s->em_world_d, em_world.data(), sizeof(int) * ne, cudaMemcpyHostToDevice));
   std::vector<float> t(ne, 0.0f);
   std::vector<int> c(ne, 0);
   for (int e = 0; e < n_old; ++e) { t[e] = t_old[e]; c[e] = c_old[e]; }
@@ -888,6 +902,13 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&s->mass0, W);
   rc |= s->alloc(&s->tmp_mass, W);
   rc |= s->alloc(&s->mask_d, W);
+  rc |= s->alloc(&s->ws_d, (size_t)W + 1);
+  rc |= s->alloc(&s->port_stack, n);
+  rc |= s->alloc(&s->port_stack0, n);
+  for (int** a : {&s->port_top, &s->port_top0, &s->port_taken, &s->port_granted, &s->port_absorbed,
+                  &s->port_emitted, &s->port_retired, &s->speed_bits})
+    rc |= s->alloc(a, W);
+  rc |= s->alloc(&s->energy_max, W);
   if (rc) {
     std::string msg = g_err;
     adf_destroy(s);
@@ -920,6 +941,25 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     CKC(cudaMemcpy(chunk_world, cwld.data(), sizeof(int) * cwld.size(), cudaMemcpyHostToDevice));
   }
   CKC(cudaMemcpy(world_chunk_start, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice));
+  CKC(cudaMemcpy(s->ws_d, s->ws_host.data(), sizeof(int) * s->ws_host.size(), cudaMemcpyHostToDevice));
+  {  // the port's reservoir: each world's build-time held particles, popped in ascending id order (ports.py:124-133)
+    std::vector<int8_t> ph(s->n);
+    if (s->n > 0) CKC(cudaMemcpy(ph.data(), m->phase, s->n, cudaMemcpyDeviceToHost));
+    std::vector<int> stack0(n, 0), top0(W, 0);
+    for (int w = 0; w < s->W; ++w) {
+      std::vector<int> ids;
+      for (int i = s->ws_host[w]; i < s->ws_host[w + 1]; ++i)
+        if (ph[i] == PH_HELD) ids.push_back(i);
+      for (size_t j = 0; j < ids.size(); ++j) stack0[s->ws_host[w] + j] = ids[ids.size() - 1 - j];
+      top0[w] = (int)ids.size();
+    }
+    CKC(cudaMemcpy(s->port_stack0, stack0.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(s->port_stack, stack0.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(s->port_top0, top0.data(), sizeof(int) * W, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(s->port_top, top0.data(), sizeof(int) * W, cudaMemcpyHostToDevice));
+    for (int* a : {s->port_taken, s->port_granted, s->port_absorbed, s->port_emitted, s->port_retired})
+      CKC(cudaMemset(a, 0, sizeof(int) * W));
+  }
   CKC(cudaMemset(d.counts, 0, sizeof(int) * std::max(s->n_keys, 1)));
   CKC(cudaMemset(d.nfw, 0, sizeof(int) * 2));
   CKC(cudaMemset(d.kv, 0, sizeof(float) * n));
@@ -976,7 +1016,7 @@ void adf_destroy(adf_solver* s) {
   cudaDeviceSynchronize();
   for (void* p : s->owned) cudaFree(p);
   void* em[] = {s->em_d, s->off_local_d, s->off_emitter_d, s->off_rank_d, s->pool_d, s->enabled_d, s->cursor_d,
-                s->emit_now_d, s->t_acc_d, s->sinks_d};
+                s->emit_now_d, s->t_acc_d, s->sinks_d, s->em_world_d};
   for (void* p : em)
     if (p) cudaFree(p);
   if (s->pinned) cudaFreeHost(s->pinned);
@@ -1417,6 +1457,9 @@ int adf_reset(adf_solver* s, const uint8_t* world_mask, const int32_t* flags0, c
     rc |= zero_masked(s->d.nonfinite, 4) | zero_masked(s->emit_overflow, 4) | zero_masked(s->mass_in, 8);
     rc |= zero_masked(s->d.mass_out, 8);
     if (rc) return rc;
+    LAUNCH(s, k_port_reset, W, 256, st, W, s->ws_d, s->mask_d, s->port_stack0, s->port_top0, s->port_stack,
+           s->port_top, s->port_absorbed, s->port_emitted, s->port_retired, s->port_taken, s->port_granted);
+    CK(cudaStreamSynchronize(st));
   }
   const int ne = (int)s->em_h.size();
   if (ne > 0) {  // emitters.rewind: layer clock and cursor of the masked worlds' emitters back to 0
@@ -1686,6 +1729,66 @@ int adf_list_stats(adf_solver* s, int32_t* fluid, int64_t* entries, void* stream
   CK(cudaMemcpy(&e, s->list_entries, sizeof(e), cudaMemcpyDeviceToHost));
   *fluid = nfw[0];
   *entries = e;
+  return check_launch();
+}
+
+int adf_get_state_storage(adf_solver* s, adf_state_storage* out) {
+  if (!s || !out) return fail(ADF_ERR_VALUE, "adf_get_state_storage: null argument");
+  out->mass_in = (int64_t*)s->mass_in;
+  out->mass_out = (int64_t*)s->d.mass_out;
+  out->escaped = s->d.escaped;
+  const int ne = (int)s->em_h.size();
+  out->n_emitters = ne;
+  out->emit_t = ne ? s->t_acc_d : nullptr;
+  out->emit_cursor = ne ? s->cursor_d : nullptr;
+  out->emit_world = ne ? s->em_world_d : nullptr;
+  out->port_stack = s->port_stack;
+  out->port_top = s->port_top;
+  out->port_absorbed = s->port_absorbed;
+  out->port_emitted = s->port_emitted;
+  out->port_retired = s->port_retired;
+  out->port_taken = s->port_taken;
+  out->port_granted = s->port_granted;
+  return ADF_OK;
+}
+
+int adf_port_take(adf_solver* s, float* qd, const int32_t* mask, int keep, void* stream) {
+  if (!s || (s->n > 0 && (!qd || !mask))) return fail(ADF_ERR_VALUE, "adf_port_take: null argument");
+  if (s->W == 0 || s->n == 0) return ADF_OK;
+  LAUNCH(s, k_port_take, s->W, 256, stream, s->ws_d, mask, keep ? 1 : 0, s->d.flags, s->d.phase, s->d.mass, qd,
+         s->port_stack, s->port_top, s->port_taken, keep ? s->port_absorbed : s->port_retired, s->d.mass_out);
+  return check_launch();
+}
+
+int adf_port_emit(adf_solver* s, float* q, float* qd, const float* pos, const float* vel, int R,
+                  const int32_t* n_req, void* stream) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_port_emit: null solver");
+  if (R < 0) return fail(ADF_ERR_VALUE, "adf_port_emit: negative request capacity");
+  if (s->W == 0 || s->n == 0) return ADF_OK;
+  if (!q || !qd || !n_req || (R > 0 && (!pos || !vel))) return fail(ADF_ERR_VALUE, "adf_port_emit: null argument");
+  LAUNCH(s, k_port_emit, s->W, 256, stream, s->ws_d, pos, vel, R, n_req, q, qd, s->d.flags, s->d.phase, s->d.mass,
+         s->port_stack, s->port_top, s->port_granted, s->port_emitted, s->mass_in);
+  return check_launch();
+}
+
+int adf_energy(adf_solver* s, const float* q, const float* qd, const double* z_ref, double* out, void* stream) {
+  if (!s || !z_ref || !out || (s->n > 0 && (!q || !qd))) return fail(ADF_ERR_VALUE, "adf_energy: null argument");
+  if (s->W == 0) return ADF_OK;
+  const DevP& P = s->d;
+  if (P.n_chunks > 0) LAUNCH(s, k_energy_chunk, P.n_chunks, 256, stream, P, q, qd, z_ref);
+  LAUNCH(s, k_world_check, s->W, 256, stream, P, 0, out, s->energy_max);
+  return check_launch();
+}
+
+int adf_stable_dt(adf_solver* s, const float* qd, double cfl, double dt_min, double dt_max, float* out,
+                  void* stream) {
+  if (!s || !out || (s->n > 0 && !qd)) return fail(ADF_ERR_VALUE, "adf_stable_dt: null argument");
+  if (s->W == 0) return ADF_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(s->speed_bits, 0, sizeof(int) * s->W, st));
+  if (s->n > 0) LAUNCH(s, k_speed_max, blocks(s->n), BLOCK, st, s->d, qd, s->speed_bits);
+  LAUNCH(s, k_stable_dt, blocks(s->W), BLOCK, st, s->W, s->speed_bits, (float)cfl,
+         (float)(2.0 * s->prm.particle_radius), (float)dt_min, (float)dt_max, out);
   return check_launch();
 }
 

@@ -89,3 +89,136 @@ def add_wall_particles(b: ModelBuilder, cfg: DFSPHConfig, points: np.ndarray, sp
 def add_particle_box(b: ModelBuilder, cfg: DFSPHConfig, inner_lo: Vec3, inner_hi: Vec3,
                      open_top: bool = False) -> range:
     return add_wall_particles(b, cfg, box_shell_points(inner_lo, inner_hi, cfg.spacing, open_top))
+
+
+BOUNDARY_SDF = 1  # sph:shape_boundary (config.py:41-44)
+
+
+def wall_box(builder: ModelBuilder, center: Vec3, half: Vec3, mu: float = 1.0) -> int:
+    """One static wall the liquid sees through its signed distance field: a box shape (build.py:104-110)."""
+    return builder.add_shape_box(-1, tuple(center), *half, mu=mu, sph_boundary=BOUNDARY_SDF)
+
+
+def add_box_tank(builder: ModelBuilder, inner_lo: Vec3, inner_hi: Vec3, wall: float, *, open_top: bool = True,
+                 floor: bool = True, mu: float = 1.0) -> dict[str, int]:
+    """A static axis-aligned tank of box walls ``wall`` thick around the inner box (build.py:113-137): the floor spans
+    the full footprint, the x walls the full y extent, the y walls sit between them, so every solid point belongs to
+    exactly one box. Returns the shape ids by name (floor, x_lo, x_hi, y_lo, y_hi[, lid])."""
+    lo, hi = np.asarray(inner_lo, np.float64), np.asarray(inner_hi, np.float64)
+    c = 0.5 * (lo + hi)
+    hx, hy, hz = 0.5 * (hi - lo)
+    t = 0.5 * wall
+    ids = {}
+    if floor:
+        ids["floor"] = wall_box(builder, (c[0], c[1], lo[2] - t), (hx + wall, hy + wall, t), mu)
+    for name, sx in (("x_lo", -1.0), ("x_hi", 1.0)):
+        ids[name] = wall_box(builder, (c[0] + sx * (hx + t), c[1], c[2]), (t, hy + wall, hz), mu)
+    for name, sy in (("y_lo", -1.0), ("y_hi", 1.0)):
+        ids[name] = wall_box(builder, (c[0], c[1] + sy * (hy + t), c[2]), (hx, t, hz), mu)
+    if not open_top:
+        ids["lid"] = wall_box(builder, (c[0], c[1], hi[2] + t), (hx + wall, hy + wall, t), mu)
+    return ids
+
+
+# ------------------------------------------------------------------------------------------------ scene assembly emit
+DISK_CLEAR = 0.375  # a cylinder's outer ring of particles stays this many spacings inside its side (build.py:226)
+
+
+def inside_primitive(pts: np.ndarray, kind: str, size) -> np.ndarray:
+    """Points inside a primitive centred at the origin (cylinder and capsule along z; build.py:181-197)."""
+    r2 = pts[:, 0] ** 2 + pts[:, 1] ** 2
+    if kind == "box":
+        return np.all(np.abs(pts) <= np.asarray(size[:3], np.float64), axis=1)
+    if kind == "sphere":
+        return r2 + pts[:, 2] ** 2 <= size[0] ** 2
+    if kind == "cylinder":
+        return (r2 <= size[0] ** 2) & (np.abs(pts[:, 2]) <= size[1])
+    if kind == "capsule":
+        over = np.maximum(np.abs(pts[:, 2]) - size[1], 0.0)
+        return r2 + over ** 2 <= size[0] ** 2
+    if kind == "ellipsoid":
+        return np.sum((pts / np.asarray(size[:3], np.float64)) ** 2, axis=1) <= 1.0
+    raise ValueError(f"SPH emit: no liquid volume for primitive {kind!r}")
+
+
+def disk_rings(pts: np.ndarray, radius: float, spacing: float) -> np.ndarray:
+    """A cylinder's lattice points out to the ring of equal axis distance whose per-layer count comes closest to the
+    disk's area / spacing^2 without exceeding it, that ring at least ``DISK_CLEAR`` spacings inside the side
+    (build.py:229-246): a square lattice in a small disk can hold more points than its area, which starts the liquid
+    compressed."""
+    if len(pts) == 0:
+        return pts
+    dist = np.round(np.hypot(pts[:, 0], pts[:, 1]), 9)
+    layer = np.sort(dist[pts[:, 2] == pts[0, 2]])
+    rings = np.unique(layer)
+    within = np.searchsorted(layer, rings, side="right")
+    area = np.pi * radius ** 2 / spacing ** 2
+    fits = (within <= area + 1.0e-9) & (rings <= radius - DISK_CLEAR * spacing + 1.0e-9)
+    miss = np.where(fits, np.abs(within - area), np.inf)
+    pick = int(np.argmin(miss)) if np.isfinite(miss).any() else 0
+    return pts[dist <= rings[pick]]
+
+
+def column_layers(pts: np.ndarray, radius: float, half_height: float, spacing: float) -> np.ndarray:
+    """``disk_rings``' column topped up with whole layers until its count is closest to the cylinder's volume /
+    spacing^3; the bottom layer stays (build.py:249-262)."""
+    if len(pts) == 0:
+        return pts
+    top = float(pts[:, 2].max())
+    layer = pts[np.isclose(pts[:, 2], top)]
+    have = len(pts) // len(layer)
+    want = np.pi * radius ** 2 * 2.0 * half_height / spacing ** 3
+    extra = max(int(np.floor(want / len(layer) + 0.5)) - have, 0)
+    more = [layer + np.array([0.0, 0.0, k * spacing]) for k in range(1, extra + 1)]
+    return np.concatenate([pts, *more]) if more else pts
+
+
+def liquid_points(shape, spacing: float) -> np.ndarray:
+    """Lattice points (spacing 2r) filling a particle-source region (``shape.region`` = (lo, hi)) or a closed
+    primitive (``shape.kind``, ``shape.size``; Newton's half-extent conventions), centred so the lattice sits
+    symmetrically in the volume (build.py:200-223). Object frame."""
+    region = getattr(shape, "region", None)
+    kind = getattr(shape, "kind", None)
+    if region is not None:
+        lo, hi = np.asarray(region[0], np.float64), np.asarray(region[1], np.float64)
+    elif kind is not None and kind != "plane":
+        size = tuple(float(v) for v in shape.size)
+        ext = {"box": size[:3], "sphere": (size[0],) * 3, "ellipsoid": size[:3],
+               "cylinder": (size[0], size[0], size[1]) if len(size) > 1 else None,
+               "capsule": (size[0], size[0], size[1] + size[0]) if len(size) > 1 else None}.get(kind)
+        if ext is None:
+            raise ValueError(f"SPH emit: no liquid volume for primitive {kind!r}")
+        lo, hi = -np.asarray(ext, np.float64), np.asarray(ext, np.float64)
+    else:
+        raise ValueError(f"SPH emit: liquid needs a particle-source region or a closed primitive, got {type(shape)}")
+    counts = np.maximum(np.floor((hi - lo) / spacing + 1.0e-9).astype(int), 1)
+    start = 0.5 * (lo + hi) - 0.5 * counts * spacing
+    pts = lattice_points(tuple(start), tuple(int(c) for c in counts), spacing)
+    if region is None:
+        size = tuple(float(v) for v in shape.size)
+        pts = pts[inside_primitive(pts, kind, size)]
+        if kind == "cylinder":
+            pts = column_layers(disk_rings(pts, size[0], spacing), size[0], size[1], spacing)
+    return pts
+
+
+def emit_object(builder: ModelBuilder, obj, decision) -> range:
+    """The plug-in's emit (build.py:265-285): a liquid object -> active lattice particles at the router's particle
+    radius (``decision.numbers["particle_radius"]``), mass rho0 / S, the material's viscosity, in ``builder``'s current
+    world (object frame). ``obj`` carries ``card.name``, ``card.shape``, ``card.budget.particles`` and
+    ``material.density.value`` / ``material.fluid.viscosity.value`` (fluid may be None: 1e-3 Pa s). Raises
+    CapacityError over the particle budget."""
+    from ... import _lib
+
+    r = float(decision.numbers.get("particle_radius", 0.0))
+    if not r > 0.0:
+        raise ValueError(f"{obj.card.name}: liquid_sph decision without particle_radius")
+    cfg = DFSPHConfig(particle_radius=r)
+    pts = liquid_points(obj.card.shape, cfg.spacing)
+    budget = obj.card.budget.particles
+    if len(pts) > budget:
+        raise _lib.CapacityError(f"{obj.card.name}: {len(pts)} SPH particles at r = {r:.3g} m > budget {budget}")
+    fluid = obj.material.fluid
+    mu = float(fluid.viscosity.value) if fluid is not None else 1.0e-3
+    return add_fluid_points(b=builder, cfg=cfg, points=pts, rest_density=float(obj.material.density.value),
+                            viscosity=mu)

@@ -27,6 +27,29 @@ class ParticleFlags(IntEnum):
     PROXY = 1 << 1
 
 
+class ShapeFlags(IntEnum):
+    """newton ShapeFlags (geometry/flags.py:27-45): the liquid sees shapes that collide with particles."""
+
+    VISIBLE = 1 << 0
+    COLLIDE_SHAPES = 1 << 1
+    COLLIDE_PARTICLES = 1 << 2
+
+
+class GeoType(IntEnum):
+    """newton GeoType (geometry/types.py:73-118)."""
+
+    PLANE = 1
+    HFIELD = 2
+    SPHERE = 3
+    CAPSULE = 4
+    ELLIPSOID = 5
+    CYLINDER = 6
+    BOX = 7
+    MESH = 8
+    CONE = 9
+    CONVEX_MESH = 10
+
+
 @dataclass
 class State:
     particle_q: torch.Tensor
@@ -40,7 +63,7 @@ class Model:
     """Finalized particle model (see module doc)."""
 
     def __init__(self, q, qd, mass, radius, flags, world, world_start, gravity, phase, rest_density, viscosity,
-                 device):
+                 device, shapes: dict | None = None):
         dev = torch.device(device)
         t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)  # noqa: E731
         self.device = dev
@@ -56,7 +79,18 @@ class Model:
         self.gravity = t(np.asarray(gravity, np.float32).reshape(-1, 3), torch.float32)
         self.sph = SimpleNamespace(phase=t(phase, torch.int8), rest_density=t(rest_density, torch.float32),
                                    viscosity=t(viscosity, torch.float32))
-        self.shape_count = 0
+        sh = shapes or {}
+        S = len(sh.get("type", ()))
+        self.shape_count = S
+        self.shape_type = t(np.asarray(sh.get("type", np.zeros(0)), np.int32), torch.int32)
+        self.shape_scale = t(np.asarray(sh.get("scale", np.zeros((0, 3))), np.float32).reshape(-1, 3), torch.float32)
+        self.shape_transform = t(np.asarray(sh.get("xform", np.zeros((0, 7))), np.float32).reshape(-1, 7),
+                                 torch.float32)
+        self.shape_world = t(np.asarray(sh.get("world", np.zeros(0)), np.int32), torch.int32)
+        self.shape_flags = t(np.asarray(sh.get("flags", np.zeros(0)), np.int32), torch.int32)
+        self.shape_body = t(np.asarray(sh.get("body", np.zeros(0)), np.int32), torch.int32)
+        self.shape_material_mu = t(np.asarray(sh.get("mu", np.zeros(0)), np.float32), torch.float32)
+        self.sph.shape_boundary = t(np.asarray(sh.get("boundary", np.zeros(0)), np.int8), torch.int8)
         self.body_count = 0
 
     def state(self) -> State:
@@ -68,7 +102,11 @@ class Model:
         return {"q": c(self.particle_q), "qd": c(self.particle_qd), "mass": c(self.particle_mass),
                 "radius": c(self.particle_radius), "flags": c(self.particle_flags), "world": c(self.particle_world),
                 "world_start": c(self.particle_world_start), "gravity": c(self.gravity), "phase": c(self.sph.phase),
-                "rest_density": c(self.sph.rest_density)}
+                "rest_density": c(self.sph.rest_density), "shape_type": c(self.shape_type),
+                "shape_scale": c(self.shape_scale), "shape_transform": c(self.shape_transform),
+                "shape_world": c(self.shape_world), "shape_flags": c(self.shape_flags),
+                "shape_body": c(self.shape_body), "shape_mu": c(self.shape_material_mu),
+                "shape_boundary": c(self.sph.shape_boundary)}
 
 
 class ModelBuilder:
@@ -82,6 +120,34 @@ class ModelBuilder:
         self._world = -1
         self._world_count = 0
         self._world_gravity: list[tuple[float, float, float]] = []
+        self._shapes: dict[str, list] = {k: [] for k in ("type", "scale", "xform", "world", "flags", "body", "mu",
+                                                          "boundary")}
+
+    @property
+    def shape_count(self) -> int:
+        return len(self._shapes["type"])
+
+    def add_shape_box(self, body: int = -1, xform=None, hx: float = 0.5, hy: float = 0.5, hz: float = 0.5,
+                      mu: float = 1.0, collide_particles: bool = True, sph_boundary: int = 0) -> int:
+        """A box shape (half extents hx, hy, hz) at ``xform`` = (px, py, pz[, qx, qy, qz, qw]) in the current world
+        (global, world -1, when no world is open), as newton.ModelBuilder.add_shape_box; ``sph_boundary`` is the
+        sph:shape_boundary attribute (0 auto, 1 sdf, 2 akinci, 3 ignore). Returns the shape id."""
+        x = np.zeros(7, np.float32)
+        x[6] = 1.0
+        if xform is not None:
+            v = np.asarray(tuple(xform), np.float32).reshape(-1)
+            x[: v.size] = v
+        sh = self._shapes
+        sh["type"].append(int(GeoType.BOX))
+        sh["scale"].append((float(hx), float(hy), float(hz)))
+        sh["xform"].append(x)
+        sh["world"].append(self._world)
+        sh["flags"].append(int(ShapeFlags.VISIBLE | ShapeFlags.COLLIDE_SHAPES |
+                               (ShapeFlags.COLLIDE_PARTICLES if collide_particles else 0)))
+        sh["body"].append(int(body))
+        sh["mu"].append(float(mu))
+        sh["boundary"].append(int(sph_boundary))
+        return len(sh["type"]) - 1
 
     @property
     def particle_count(self) -> int:
@@ -132,4 +198,5 @@ class ModelBuilder:
         return Model(cat("q", np.float32, (0, 3)), cat("qd", np.float32, (0, 3)), cat("mass", np.float32),
                      cat("radius", np.float32), cat("flags", np.int32), world, ws,
                      np.asarray(self._world_gravity or [self.gravity], np.float32).reshape(-1, 3),
-                     cat("phase", np.int8), cat("rho0", np.float32), cat("mu", np.float32), device)
+                     cat("phase", np.int8), cat("rho0", np.float32), cat("mu", np.float32), device,
+                     shapes=self._shapes if self.shape_count else None)

@@ -206,6 +206,11 @@ class SolverDFSPH:
             log.warning("SolverDFSPH: the resting-jitter tolerance rule is not in this build's CUDA path; the density"
                         " solve runs at max_density_error")
         self._check_capacity(capacity_per_world, phase, ws)
+        from .shapes import shape_table
+
+        self.shapes = shape_table(model)  # refuses shape walls this path does not evaluate
+        if self.shapes.count and len(self.shapes.ids):
+            raise ValueError("SolverDFSPH (B200 build): box-shape walls are not yet on this build's CUDA path")
         if n and isinstance(model.particle_mass, torch.Tensor) and not model.particle_mass.is_cuda:
             raise ValueError("SolverDFSPH: the model must live on a CUDA device (Model.finalize(device='cuda'))")
         self.device = model.particle_mass.device if isinstance(model.particle_mass, torch.Tensor) else \
@@ -242,6 +247,10 @@ class SolverDFSPH:
         self._em_own: list[bool] = []
         self._sinks = 0
         self.bounds = None if cfg.world_bounds is None else cfg.world_bounds
+        from .ports import SPHPort
+
+        self.port = SPHPort(self)  # absorb / emit / retire between steps (ports.py)
+        self._saved: dict[str, torch.Tensor] = {}  # coupling restarts (coupling_notify_input_state_update)
         log.info("SolverDFSPH (B200): %d particles in %d worlds, r=%g m, h=%g m, kernel=%s", n, W,
                  cfg.particle_radius, cfg.h, cfg.kernel)
 
@@ -498,35 +507,156 @@ class SolverDFSPH:
         return snap_down(stable_dt(self.config, v), control_dt)
 
     def alloy_stable_dt(self, state, contacts, out) -> None:
-        """out[w] = clamp(cfl 2r / |v|max, dt_min, dt_max) over the state's liquid (runtime.py:667-676)."""
+        """out[w] (device float32 [W]) = clamp(cfl 2r / |v|max, dt_min, dt_max) over the state's liquid, dt_max at
+        rest (runtime.py:411-421); one pass over the particles on the device, nothing allocated."""
         del contacts
+        if self.world_count == 0:
+            return
         cfg = self.config
-        qd = state.particle_qd
-        fl = (self.model.particle_flags & _ACTIVE) != 0
-        liquid = fl & (self.model.sph.phase >= 1)
-        speed = torch.linalg.vector_norm(qd, dim=1)
-        speed = torch.where(torch.isfinite(speed), speed, torch.full_like(speed, 1.0e30))
-        speed = torch.where(liquid, speed, torch.zeros_like(speed))
-        vmax = torch.zeros(self.world_count, dtype=torch.float32, device=self.device)
-        vmax.scatter_reduce_(0, self.model.particle_world.long().clamp(min=0), speed, reduce="amax")
-        dt = torch.where(vmax > 0.0, torch.clamp(cfg.cfl * cfg.spacing / vmax.clamp(min=1e-30), cfg.dt_min,
-                                                   cfg.dt_max), torch.full_like(vmax, cfg.dt_max))
-        out.copy_(dt)
+        _lib.check(self._lib.adf_stable_dt(self._h, _ptr(state.particle_qd, torch.float32, self.n, "particle_qd"),
+                                           float(cfg.cfl), float(cfg.dt_min), float(cfg.dt_max),
+                                           _ptr(out, torch.float32, self.world_count, "out"), self._stream()),
+                   "alloy_stable_dt")
+
+    def alloy_energy(self, state, z_ref, out) -> None:
+        """Kinetic + gravity energy [J] of each world's liquid about (0, 0, z_ref[w]) into ``out`` (device float64
+        [W]); float64 per-world sums in a fixed order (runtime.py:66-79, 423-430)."""
+        if self.world_count == 0:
+            return
+        W = self.world_count
+        _lib.check(self._lib.adf_energy(self._h, _ptr(state.particle_q, torch.float32, self.n, "particle_q"),
+                                        _ptr(state.particle_qd, torch.float32, self.n, "particle_qd"),
+                                        _ptr(z_ref, torch.float64, W, "z_ref"), _ptr(out, torch.float64, W, "out"),
+                                        self._stream()), "alloy_energy")
 
     def alloy_capacity_report(self) -> dict[str, int]:
         a = self._world_arrays()
         return {"neighbor_overflow": int(a["neighbor_overflow"].sum()),
                 "emitter_overflow": int(a["emitter_overflow"].sum())}
 
+    def _storage(self) -> dict[str, torch.Tensor]:
+        """Views of the library's own device arrays behind the snapshot keys (include/alloy_dfsph.h
+        adf_state_storage). The emitter views change when emitters are added."""
+        st = _lib.StateStorage()
+        _lib.check(self._lib.adf_get_state_storage(self._h, C.byref(st)), "state storage")
+        W, n = self.world_count, self.n
+
+        def view(ptr, count, typestr):
+            return torch.as_tensor(_DevView(ptr, (max(count, 1),), typestr), device=self.device)[:count]
+
+        out = {"mass_in": view(st.mass_in, W, "<i8"), "mass_out": view(st.mass_out, W, "<i8"),
+               "escaped": view(st.escaped, W, "<i4"), "port_stack": view(st.port_stack, n, "<i4"),
+               "port_top": view(st.port_top, W, "<i4"), "port_absorbed": view(st.port_absorbed, W, "<i4"),
+               "port_emitted": view(st.port_emitted, W, "<i4"), "port_retired": view(st.port_retired, W, "<i4"),
+               "taken": view(st.port_taken, W, "<i4"), "granted": view(st.port_granted, W, "<i4")}
+        E = int(st.n_emitters)
+        if E:
+            out.update({"emit_t": view(st.emit_t, E, "<f4"), "emit_cursor": view(st.emit_cursor, E, "<i4"),
+                        "emit_world": view(st.emit_world, E, "<i4")})
+        return out
+
     def alloy_state_arrays(self, state=None) -> dict:
-        """The solver state a snapshot must hold beside State (coupling_hooks.py:260-271)."""
+        """The solver state a snapshot must hold beside State (coupling_hooks.py:115-126): warm starts, phase and
+        flags, the mass ledger (runtime.py:173-174), the emitters' clocks and cursors (runtime.py:389-393) and the
+        port (ports.py:201-203). Every value is the library's own storage: a snapshot copies it out and back in
+        place between steps."""
         del state
-        return {"sph.kappa_v": self._kv, "sph.kappa_d": self._kd, "sph.phase": self.model.sph.phase,
-                "particle_flags": self.model.particle_flags}
+        a = self._storage()
+        arrays = {"sph.kappa_v": self._kv, "sph.kappa_d": self._kd, "sph.phase": self.model.sph.phase,
+                  "particle_flags": self.model.particle_flags, "sph.mass_in": a["mass_in"],
+                  "sph.mass_out": a["mass_out"], "sph.escaped": a["escaped"]}
+        if "emit_t" in a:
+            arrays.update({"sph.emit_t": a["emit_t"], "sph.emit_cursor": a["emit_cursor"]})
+        arrays.update(self.port.state_arrays())
+        return arrays
 
     def alloy_state_worlds(self) -> dict:
+        """Item -> world maps of the per-item arrays in ``alloy_state_arrays`` (coupling_hooks.py:128-138); per-world
+        arrays are world-major and need none. The port stack holds world w's particles in that world's own index
+        range, so its map is the particles' world."""
         pw = self.model.particle_world
-        return {"sph.kappa_v": pw, "sph.kappa_d": pw, "sph.phase": pw, "particle_flags": pw}
+        maps = {"sph.kappa_v": pw, "sph.kappa_d": pw, "sph.phase": pw, "particle_flags": pw, "sph.port_stack": pw}
+        a = self._storage()
+        if "emit_world" in a:
+            maps.update({"sph.emit_t": a["emit_world"], "sph.emit_cursor": a["emit_world"]})
+        return maps
+
+    # ------------------------------------------------------------------------------------------------ port
+    def retire(self, state, mask) -> None:
+        """Retire the masked liquid particles for good (``mask [n]`` int32; one launch, capture-safe): their mass
+        leaves the ledger as at a sink; ``port.taken[w]`` counts them (solver.py:428-431, ports.py:187-189)."""
+        self.port.retire(state, mask)
+
+    # ------------------------------------------------------------------------------------------------ model
+    def notify_model_changed(self, flags: int) -> None:
+        """solver.py:343-351. The reference re-derives its body modes when body properties change and rebuilds its
+        shape table when shape properties change. This path has neither (the constructor refuses bodies and SDF
+        shapes; particle walls are particles), and every step reads the particle arrays, masses, rest densities and
+        gravity live from the model, so no flag leaves anything to rebuild."""
+        int(flags)
+
+    @staticmethod
+    def emit(builder, obj, decision) -> None:
+        """Scene assembly's emit (solver.py:475-479, build.py:265-285): a liquid object -> active lattice particles
+        in ``builder``'s current world (``build.emit_object``)."""
+        from .build import emit_object
+
+        emit_object(builder, obj, decision)
+
+    # ------------------------------------------------------------------------------------------------ coupling
+    def coupling_notify_input_state_update(self, state, flags: int, *, iteration_restart: bool = False,
+                                           dt: float = 0.0) -> None:
+        """coupling_hooks.py:41-72: every pass of one exchange starts from the same solver state. A restart copies
+        back the warm starts, flags, phase, ledgers and emitter clocks saved at the exchange's first pass; any other
+        notification saves them."""
+        del state, flags, dt
+        if self.n == 0:
+            return
+        live = {"kv": self._kv, "kd": self._kd, "flags": self.model.particle_flags, "phase": self.model.sph.phase}
+        live.update({k: v for k, v in self._storage().items() if k in ("mass_in", "mass_out", "escaped", "emit_t",
+                                                                          "emit_cursor")})
+        if iteration_restart:
+            for k, a in live.items():
+                if k in self._saved and self._saved[k].shape == a.shape:
+                    a.copy_(self._saved[k])
+        else:
+            self._saved = {k: a.clone() for k, a in live.items()}
+
+    def coupling_prepare_proxy_contacts(self, state, contacts, *, contacts_freshly_detected: bool = False):
+        del state, contacts_freshly_detected
+        return contacts  # the liquid reads no contact rows: its walls are particle walls
+
+    def coupling_supports_full_surface_soft_contacts(self) -> bool:
+        return True  # contacts are ignored, so any soft-contact layout is acceptable
+
+    def coupling_supports_inertial_property_refresh(self) -> bool:
+        return False
+
+    def coupling_harvest_proxy_wrenches(self, body_local_to_proxy_global, out_body_f, **kwargs) -> None:
+        """This path has no proxy bodies (coupling_hooks.py:74-86 integrates them): only an empty mapping is valid."""
+        del out_body_f, kwargs
+        if len(body_local_to_proxy_global):
+            raise ValueError("SolverDFSPH (B200 build): proxy bodies are not part of this build's CUDA path")
+
+    def coupling_rewind_proxy_particle(self, particle_local_to_proxy_global, state, coupling_forces,
+                                       particle_gravity_acceleration, dt: float) -> None:
+        """coupling_hooks.py:88-95: lagged particle proxies are refused beside walls."""
+        del state, coupling_forces, particle_gravity_acceleration, dt
+        if len(particle_local_to_proxy_global):
+            raise ValueError("SolverDFSPH particle walls need a staggered proxy pair (PairPolicy / Proxy mode "
+                             "'staggered' with Aitken relaxation); lagged proxies diverge for a liquid-wall pair")
+
+    def coupling_harvest_proxy_particle_forces(self, particle_local_to_proxy_global, out_particle_f, *, dt: float,
+                                               **kwargs) -> None:
+        """coupling_hooks.py:97-105 returns the liquid's force on two-way particle walls. This path's walls are
+        one-way (prescribed): the wall reactions are not accumulated, so a non-empty mapping is refused."""
+        del out_particle_f, kwargs
+        if len(particle_local_to_proxy_global) == 0:
+            return
+        if not dt > 0.0:
+            raise ValueError("SolverDFSPH harvest requires dt > 0")
+        raise ValueError("SolverDFSPH (B200 build): two-way particle walls (reaction forces on proxies) are not part "
+                         "of this build's CUDA path")
 
     # ------------------------------------------------------------------------------------------------ emitters
     def _spares(self, w: int) -> np.ndarray:

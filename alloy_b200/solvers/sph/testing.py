@@ -19,8 +19,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .build import (add_fluid_block, add_fluid_points, add_particle_box, add_spares, add_wall_particles,
-                    box_shell_points, jittered)
+from .build import (add_box_tank, add_fluid_block, add_fluid_points, add_particle_box, add_spares,
+                    add_wall_particles, box_shell_points, jittered)
 from .config import DFSPHConfig, snap_down, stable_dt
 from .model import Model, ModelBuilder
 
@@ -46,14 +46,41 @@ class Scene:
 
 
 def dam_break(counts=(20, 20, 20), box=(1.0, 1.0, 1.0), spacing: float = 0.02, jitter: float = 0.01, seed: int = 0,
-              dt: float = 1.0e-3, steps: int = 200, open_top: bool = False, device="cpu", **cfg_kw) -> Scene:
+              dt: float = 1.0e-3, steps: int = 200, open_top: bool = False, walls: str = "particles", device="cpu",
+              **cfg_kw) -> Scene:
+    """``walls``: "particles" (one layer of boundary particles) or "sdf" (the reference's box tank, walls h thick,
+    alloy/testing/sph.py:101-115)."""
     cfg = benchmark_config(spacing, **cfg_kw)
     b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
     b.begin_world()
     fl = add_fluid_block(b, cfg, (0.0, 0.0, 0.0), counts, jitter=jitter, seed=seed)
-    wl = add_particle_box(b, cfg, (0.0, 0.0, 0.0), box, open_top=open_top)
+    if walls == "sdf":
+        add_box_tank(b, (0.0, 0.0, 0.0), box, wall=cfg.h, open_top=open_top)
+        nw = 0
+    else:
+        nw = len(add_particle_box(b, cfg, (0.0, 0.0, 0.0), box, open_top=open_top))
     b.end_world()
-    return Scene(b.finalize(device), cfg, dt, steps, len(fl), len(wl), name=f"dam_break_{counts}")
+    return Scene(b.finalize(device), cfg, dt, steps, len(fl), nw, name=f"dam_break_{counts}_{walls}")
+
+
+def tank_impacts(spacing: float = 0.02, dt: float = 1.0e-3, steps: int = 10, device="cpu", **cfg_kw) -> Scene:
+    """Walls hit hard (a parity scene for the projection, wall friction and sweep paths): the 6 x 6 x 8 jittered block
+    thrown at 1 m/s into the corner of an open box tank (the reference's box shapes, walls h thick) and eight lone
+    particles: four at 30 m/s, far past the CFL step, towards the floor and the x and y walls (swept), four at
+    0.5-2 m/s grazing the walls (pushed out, lone-particle limit and friction)."""
+    cfg = benchmark_config(spacing, **cfg_kw)
+    b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    b.begin_world()
+    fl = add_fluid_block(b, cfg, (0.0, 0.0, 0.0), (6, 6, 8), jitter=0.01, seed=3, velocity=(-1.0, -0.6, -0.4))
+    lone = [((0.17, 0.06, 0.05), (30.0, 0.0, -4.0)), ((0.15, 0.17, 0.12), (0.0, 30.0, 2.0)),
+            ((0.16, 0.09, 0.06), (3.0, 1.0, -30.0)), ((0.18, 0.15, 0.20), (-9.0, 28.0, -6.0)),
+            ((0.19, 0.05, 0.16), (2.0, -0.5, 0.3)), ((0.14, 0.19, 0.02), (0.7, 1.5, -1.0)),
+            ((0.185, 0.185, 0.09), (0.5, 0.5, -0.2)), ((0.15, 0.012, 0.011), (-0.3, -0.8, -1.2))]
+    for x, v in lone:
+        add_fluid_points(b, cfg, np.asarray([x]), velocity=v)
+    add_box_tank(b, (0.0, 0.0, 0.0), (0.2, 0.2, 0.24), wall=cfg.h, open_top=True)
+    b.end_world()
+    return Scene(b.finalize(device), cfg, dt, steps, len(fl) + len(lone), 0, name="tank_impacts")
 
 
 def large_dam_break(device="cpu", **kw) -> Scene:
@@ -215,9 +242,9 @@ def pour_bowls(worlds: int = 4096, lo: int = 4096, hi: int = 16384, spacing: flo
     thousands of particles per world the workload names (at 0.01 m it holds about 1,000)."""
     cfg = benchmark_config(spacing, world_bounds=((-0.3, -0.3, -0.2), (0.3, 0.3, 0.5)), **cfg_kw)
     sizes = world_sizes(worlds, lo, hi, seed)
-    rng = np.random.default_rng(seed + 7)
-    ang = rng.uniform(0.0, 2.0 * np.pi, worlds)
-    phase = rng.uniform(0.0, 2.0 * np.pi, worlds)
+    # one stream per quantity, so the first k worlds of any build are the same worlds (sizes, paths, phases)
+    ang = np.random.default_rng(seed + 7).uniform(0.0, 2.0 * np.pi, worlds)
+    phase = np.random.default_rng(seed + 8).uniform(0.0, 2.0 * np.pi, worlds)
     direction = np.stack([np.cos(ang), np.sin(ang), np.zeros(worlds)], axis=1)
     centre = (0.0, 0.0, radius)
     shell = hemisphere_shell_points(centre, radius, spacing)
@@ -248,6 +275,6 @@ def pour_bowls(worlds: int = 4096, lo: int = 4096, hi: int = 16384, spacing: flo
     return sc
 
 
-__all__ = ["Scene", "benchmark_config", "dam_break", "large_dam_break", "batched_worlds", "pour_bowls", "BowlMotion",
+__all__ = ["Scene", "benchmark_config", "dam_break", "tank_impacts", "large_dam_break", "batched_worlds", "pour_bowls", "BowlMotion",
            "water_column", "tank_dam_break",
            "world_sizes", "box_shell_points", "add_wall_particles", "hemisphere_shell_points", "bowl_interior_points"]

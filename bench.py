@@ -2,23 +2,29 @@
 # SPDX-License-Identifier: Apache-2.0
 """Benchmark of the DFSPH liquid step: particle-steps/s of liquid particles, one JSON line on rank 0.
 
-Workload (default): the 1,048,576-particle dam break (128 x 64 x 128 block at 0.01 m, seeded +-1 % jitter) in a
-closed 4 x 2 x 2 m tank of boundary particles, dt 0.5 ms, cubic kernel, Jacobi, tolerances 1e-3, FP32 particles with
-float64 per-world residual sums. A step is one full DFSPH step over every particle; steps continue the same run
-(warm starts carried). The working set per step (~1.4 GB) is far larger than L2, so no flush is needed between steps;
+Workload (default): the batched + learned pour, 4,096 worlds of 4,096-16,384 particles (seeded log-uniform), each a
+hemisphere bowl (r 0.08 m) of boundary particles moving on a seeded sinusoid (0.05 m, 1 s; the bowls' velocities
+are set before every step, inside the timed region) with a 1 m/s spout and an escape box, dt 1 ms, cubic kernel,
+Jacobi, tolerances 1e-3, FP32 particles with float64 per-world residual sums. The headline ``value`` is the
+warm-started solve: the shipped network predicts both pressure solves' starts and the first sweep judges them against
+the plain start per world, every world iterating to the same tolerance. Beside it: the plain solve of the same
+batched worlds (``plain``, and ``warm_started.vs_plain``), the same worlds stepped one world per solver
+(``plain_per_world``, a timed sample), the learned start without the judge, the CG solve, and the first 16 worlds
+against the FP64 oracle (``fp64_check``). A step is one full DFSPH step over every world; steps continue the same run
+(warm starts carried). The working set per step (~40 GB) is far larger than L2, so no flush is needed between steps;
 workloads whose working set could stay in L2 (the 30k scenes) get a 256 MB write between timed steps, outside the
 per-step CUDA events.
 
-Other workloads (--workload): dam_break (8,000 particles, 1 world), batched_worlds (256 uneven worlds with spouts,
-world shards across ranks), pour_bowls (4,096 worlds of 4,096-16,384 particles, each a moving hemisphere bowl of
-boundary particles with a spout; the bowls' velocities are set before every step, inside the timed region), and the
-reference's own speed-harness scenes at r = 2 mm, primed before stepping: column_30k (a resting 32 x 32 x 30 column,
-fast preset, CG), dam_break_30k (32 x 32 x 30 against the wall of a 96-spacing tank, default config) and
-columns_256x4k (256 resting 16 x 16 x 16 columns).
+Other workloads (--workload): large_dam_break (1,048,576 particles in a 4 x 2 x 2 m tank, dt 0.5 ms, one world: the
+HBM-roofline and neighbour-list case), dam_break (8,000 particles, 1 world), batched_worlds (256 uneven worlds with
+spouts, world shards across ranks), and the reference's own speed-harness scenes at r = 2 mm, primed before
+stepping: column_30k (a resting 32 x 32 x 30 column, fast preset, CG), dam_break_30k (32 x 32 x 30 against the wall
+of a 96-spacing tank, default config) and columns_256x4k (256 resting 16 x 16 x 16 columns). --plain makes the plain
+solve the headline (``warm_started`` then becomes the arm).
 
 Arms:
-  --impl b200       this package's CUDA path (one process per GPU; N > 1 runs N replicas of the single world:
-                    the path has no data-path collective)
+  --impl b200       this package's CUDA path (one process per GPU; N > 1 shards whole worlds across ranks, or runs
+                    N replicas of a single-world scene: the path has no data-path collective)
   --impl reference  the reference algorithm on the host cores: the CPU oracle (a restatement of the reference's
                     Warp kernels; Warp itself is not installed) with every host thread, rank 0 only.
 """
@@ -52,12 +58,14 @@ def parse():
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", choices=("large_dam_break", "dam_break", "batched_worlds", "pour_bowls",
                                            "column_30k", "dam_break_30k", "columns_256x4k"),
-                    default="large_dam_break")
+                    default="pour_bowls")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--worlds", type=int, default=None,
                     help="worlds of batched_worlds / pour_bowls (default: the workload's 256 / 4,096; fewer only for "
                          "profiling a smaller instance of the same worlds)")
-    ap.add_argument("--no-warm", action="store_true", help="skip the learned warm-start and CG arms")
+    ap.add_argument("--no-warm", action="store_true", help="skip the arms beside the headline (plain or learned, CG, "
+                                                              "per-world, FP64 check)")
+    ap.add_argument("--plain", action="store_true", help="headline the plain solve instead of the warm-started one")
     return ap.parse_args()
 
 
@@ -138,11 +146,19 @@ def rank_scene(sc, name: str, rank: int, world: int, device):
     worlds (longest-processing-time by particle count; no data-path collective) with its spouts renumbered."""
     if name not in MULTI_WORLD or world == 1:
         return sc
-    from alloy_b200.solvers.sph.sharding import shard_worlds, sub_model
+    from alloy_b200.solvers.sph.sharding import shard_worlds
+
+    ws = sc.model.host()["world_start"]
+    return worlds_scene(sc, shard_worlds(np.diff(ws), world)[rank], device, f"{sc.name}_shard{rank}")
+
+
+def worlds_scene(sc, mine: list[int], device, name: str):
+    """The scene of the worlds ``mine`` of a multi-world scene, renumbered 0.. in that order: their particles, spouts
+    and kinematic bowls."""
+    from alloy_b200.solvers.sph.sharding import sub_model
     from alloy_b200.solvers.sph.testing import Scene
 
     ws = sc.model.host()["world_start"]
-    mine = shard_worlds(np.diff(ws), world)[rank]
     sub = sub_model(sc.model, mine, device)
     sws = np.concatenate([[0], np.cumsum([ws[w + 1] - ws[w] for w in mine])])
     ems = []
@@ -151,8 +167,8 @@ def rank_scene(sc, name: str, rank: int, world: int, device):
             k = mine.index(e["world"])
             ems.append({**e, "world": k, "pool": np.asarray(e["pool"]) - ws[e["world"]] + sws[k]})
     fl = int(sum(np.sum(sub.host()["phase"][sws[k]:sws[k + 1]] >= 1) for k in range(len(mine))))
-    out = Scene(sub, sc.config, sc.dt, sc.steps, fl, 0, ems, name=f"{sc.name}_shard{rank}")
-    if sc.motion is not None:  # the shard's bowls, renumbered into the sub-model
+    out = Scene(sub, sc.config, sc.dt, sc.steps, fl, 0, ems, name=name)
+    if sc.motion is not None:  # the worlds' bowls, renumbered into the sub-model
         from alloy_b200.solvers.sph.testing import BowlMotion
 
         m = sc.motion
@@ -296,16 +312,20 @@ KERNEL_NAMES = {"k_jacobi": "jacobi", "k_accel": "accel", "k_density_alpha": "de
                 "k_wall_slots": "wall_slots", "k_finish": "finish"}
 
 
-def dram_traffic(workload: str) -> dict:
-    """DRAM bytes (read + write) per launch of each kernel from the committed ncu summary of this workload: the
-    table rows `| k_name | launches | read MB | write MB | bytes per launch |`."""
+def dram_traffic(workload: str, kernel: str) -> tuple[int | None, str | None]:
+    """DRAM bytes (read + write) per launch of ``kernel`` from the committed ncu summary of this workload (its table
+    rows `| k_name | launches | read MB | write MB | bytes per launch |`), with the summary's file name and capture
+    date: a figure measured by ncu on an earlier build, not in this run. (None, None) without a summary."""
     f = ROOT / "profiles" / f"dram_traffic_{workload}.md"
-    out = {}
-    if f.exists():
-        for m in re.finditer(r"^\|\s*(k_\w+)\s*\|[^\n]*\|\s*(\d+)\s*\|\s*$", f.read_text(), re.M):
-            if m.group(1) in KERNEL_NAMES:
-                out[KERNEL_NAMES[m.group(1)]] = int(m.group(2))
-    return out
+    if not f.exists():
+        return None, None
+    text = f.read_text()
+    date = re.search(r"[Cc]aptured[^\n]*?(\d{4}-\d{2}-\d{2})", text)
+    for m in re.finditer(r"^\|\s*(k_\w+)\s*\|[^\n]*\|\s*(\d+)\s*\|\s*$", text, re.M):
+        if KERNEL_NAMES.get(m.group(1)) == kernel:
+            src = f"profiles/{f.name}" + (f" (ncu, {date.group(1)})" if date else " (ncu)")
+            return int(m.group(2)), src
+    return None, None
 
 
 def cpu_oracle_run(sc, steps: int, warmup: int, budget_s: float | None):
@@ -420,6 +440,110 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
     return out
 
 
+def per_world_arm(args, dev, batched_value: float, worlds: int = 32, steps: int = 20) -> dict:
+    """Plain DFSPH without batching: the workload's first ``worlds`` worlds (the same worlds as the full build's),
+    each in its own solver with its own launches and step graph, stepped in turn (plain start). Particle-steps/s of
+    that sample, timed with CUDA events around the round-robin of ``steps`` steps after 3 warm-up steps, and how many
+    times the batched plain solve's throughput over every world exceeds it."""
+    import torch
+
+    from alloy_b200.solvers.sph import SolverDFSPH
+
+    global WORLDS
+    keep, WORLDS = WORLDS, worlds
+    try:
+        small = make_scene(args.workload, dev)
+    finally:
+        WORLDS = keep
+    runs = []
+    for w in range(worlds):
+        sc = worlds_scene(small, [w], dev, f"{small.name}_world{w}")
+        sol = SolverDFSPH(sc.model, sc.config)
+        sol.add_emitters([(0, c, h, r, v, p) for _, c, h, r, v, p, _, _ in spouts(sc)])
+        runs.append(Stepper(sol, sc, sc.model.state(), sc.model.state()))
+    for r in runs:
+        r(3)
+    torch.cuda.synchronize(dev)
+    nf0 = sum(r.sol.list_stats()[0] for r in runs)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        for r in runs:
+            r()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    t = e0.elapsed_time(e1) * 1e-3
+    nf1 = sum(r.sol.list_stats()[0] for r in runs)
+    value = 0.5 * (nf0 + nf1) * steps / t
+    return {"value": value, "ms_per_world_step": 1e3 * t / (steps * worlds), "batched_plain_vs_this": batched_value
+            / value, "sample": f"the first {worlds} worlds, one solver each, {steps} steps round-robin after 3 warm-up "
+            "steps, plain start"}
+
+
+def _fp64_compression(sc, q, qd) -> np.ndarray:
+    """Per world: mean over the liquid of max(rho / rho0 - 1, 0) of a state, evaluated by the FP64 oracle."""
+    from oracle.pyoracle import Oracle
+
+    orc = Oracle(sc.model.host(), sc.config, f64=True)
+    orc.set_state(q, qd)
+    orc.prepare_density()
+    ratio, act = orc.field("ratio").astype(np.float64), orc.field("active") > 0
+    world = sc.model.host()["world"]
+    W = len(sc.model.host()["world_start"]) - 1
+    return np.array([np.maximum(ratio[act & (world == w)] - 1.0, 0.0).mean() if (act & (world == w)).any() else 0.0
+                     for w in range(W)])
+
+
+def fp64_check(args, dev, warm: bool, worlds: int = 16, steps: int = 30) -> dict:
+    """The workload's first 16 worlds (the full build's worlds: sizes, particles, bowl paths, spouts) for 30 steps on
+    the CUDA path (FP32 particles; with the headline's learned start and with the plain start) and on the oracle in
+    FP64 throughout (plain start). Reported: each run's largest per-world solver density error (the mean compression
+    its density solve stopped at) over the steps, the compression of each run's end state measured in FP64, and the
+    largest per-world difference of that compression from the FP64 run's."""
+    from oracle.pyoracle import Oracle
+
+    from alloy_b200.solvers.sph import SolverDFSPH
+    from alloy_b200.solvers.sph.solver import _xform7
+    from alloy_b200.solvers.sph.warmstart import default_model
+
+    global WORLDS
+    keep, WORLDS = WORLDS, worlds
+    try:
+        sc = make_scene(args.workload, dev)
+    finally:
+        WORLDS = keep
+    orc = Oracle(sc.model.host(), sc.config, f64=True)
+    for w, centre, _, _, vel, pool, offs, interval in spouts(sc):
+        orc.add_emitter(w, _xform7(centre), offs, vel, interval, pool)
+    err = {"fp64_oracle": 0.0}
+    for k in range(steps):
+        if sc.motion is not None:
+            orc.set_velocity(sc.motion.wall_index, sc.motion.host_velocities(k * sc.dt, sc.dt))
+        orc.step(sc.dt)
+        err["fp64_oracle"] = max(err["fp64_oracle"], float(orc.report()["density_err"].max()))
+    q64, v64 = orc.state64()
+    comp = {"fp64_oracle": _fp64_compression(sc, q64.astype(np.float32), v64.astype(np.float32))}
+    for key, learned in (("gpu_learned", True), ("gpu_plain", False)) if warm else (("gpu_plain", False),):
+        sol = SolverDFSPH(sc.model, sc.config)
+        sol.add_emitters([(w, c, h, r, v, p) for w, c, h, r, v, p, _, _ in spouts(sc)])
+        if learned:
+            sol.set_warm_model(default_model())
+            sol.warm_judging(True)
+        run = Stepper(sol, sc, sc.model.state(), sc.model.state())
+        err[key] = 0.0
+        for _ in range(steps):
+            run()
+            err[key] = max(err[key], float(sol.report().density_err.max()))
+        comp[key] = _fp64_compression(sc, run.a.particle_q.cpu().numpy(), run.a.particle_qd.cpu().numpy())
+        del sol, run
+    return {"worlds": worlds, "steps": steps, "tolerance": sc.config.max_density_error,
+            "max_world_density_err": err,
+            "end_state_compression_fp64_measured": {k: float(v.max()) for k, v in comp.items()},
+            "max_world_compression_diff_vs_fp64": {k: float(np.abs(v - comp["fp64_oracle"]).max())
+                                                   for k, v in comp.items() if k != "fp64_oracle"}}
+
+
 T_START = time.perf_counter()
 
 
@@ -467,6 +591,12 @@ def run_b200(args):
     note(f"solver for {sc.model.particle_count} particles")
     sol = SolverDFSPH(sc.model, sc.config)
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
+    headline_warm = not args.plain
+    if headline_warm:  # the shipped network's starts, judged by the first sweep against the plain start per world
+        from alloy_b200.solvers.sph.warmstart import DEFAULT_MODEL, default_model
+
+        sol.set_warm_model(default_model())
+        sol.warm_judging(True)
     run = Stepper(sol, sc, sc.model.state(), sc.model.state())
     stream = torch.cuda.current_stream(dev)
     if args.workload in LIQ9:  # the reference's harness primes its columns (alloy/testing/sph.py:334-343)
@@ -575,6 +705,12 @@ def run_b200(args):
     t_e2e = time.perf_counter() - t0
     den_max.append(float(sol.diagnostics()["density_err_max"].max()))
     nf2 = sol.list_stats()[0]
+    kept = []
+    if headline_warm:  # share of solves whose world kept the learned start (outside every timed region)
+        for _ in range(10):
+            run()
+            d = sol.diagnostics()
+            kept.append(0.5 * float(d["learned_density"].mean() + d["learned_divergence"].mean()))
     te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
     pe = torch.tensor([0.5 * (nf1 + nf2) * args.steps], dtype=torch.float64, device=dev)
     if world > 1:  # wall clock of each rank's own loop, the slowest rank's; particle-steps of all ranks
@@ -602,7 +738,7 @@ def run_b200(args):
     ms, cnt = prof[dom]
     per_launch_s = ms * 1e-3 / max(cnt, 1)
     achieved = alg[dom] * per_launch[dom] / per_launch_s / 1e9
-    traffic = dram_traffic(args.workload).get(dom)
+    traffic, traffic_src = dram_traffic(args.workload, dom)
     shares = {k: round(v[0] / total_ms, 4) for k, v in prof.items() if total_ms > 0}
     per_kernel = {}
     for k, b_alg in alg.items():
@@ -619,8 +755,8 @@ def run_b200(args):
         del sol
         run = None  # the plain solver's memory goes back before the other arms build theirs
         other = "jacobi" if args.workload in LIQ9 else "cg"  # the other pressure solve beside the workload's own
-        arms = [("warm_started", {"judge": True}), ("warm_started_unjudged", {"judge": False}),
-                (other, {"pressure_solver": other})]
+        arms = [("plain" if headline_warm else "warm_started", {} if headline_warm else {"judge": True}),
+                ("warm_started_unjudged", {"judge": False}), (other, {"pressure_solver": other})]
         for key, kw in arms:
             note(f"arm {key}")
             r = variant_arm(args, dev, rank, world, **kw)
@@ -630,10 +766,25 @@ def run_b200(args):
                 dist.all_reduce(tw, op=dist.ReduceOp.MAX)
                 dist.all_reduce(pw, op=dist.ReduceOp.SUM)
             r["value"] = float(pw.item()) / float(tw.item())
-            r["vs_plain"] = r["value"] / value
+            warm[key] = r
+        plain_value = warm["plain"]["value"] if headline_warm else value
+        for key, r in warm.items():
+            r["vs_plain"] = r["value"] / plain_value
             for k in ("particle_steps", "seconds"):
                 r.pop(k)
-            warm[key] = r
+        if headline_warm:
+            warm["warm_started"] = {"value": value, "vs_plain": value / plain_value, "judge": True,
+                                    "model": str(DEFAULT_MODEL.relative_to(ROOT)),
+                                    "learned_start_kept": float(np.mean(kept)) if kept else None,
+                                    "iters_density_mean": float(np.mean(it_den)),
+                                    "iters_divergence_mean": float(np.mean(it_div)),
+                                    "density_err_mean_max_over_steps": float(np.max(den_err))}
+        if world == 1 and args.workload in MULTI_WORLD:
+            note("arm plain_per_world")
+            warm["plain_per_world"] = per_world_arm(args, dev, plain_value)
+        if rank == 0 and args.workload == "pour_bowls":
+            note("FP64 check (first 16 worlds)")
+            warm["fp64_check"] = fp64_check(args, dev, headline_warm)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -652,12 +803,13 @@ def run_b200(args):
             "scaling": "strong" if args.workload in MULTI_WORLD else "weak",
             "vs_baseline": (value / LIQ9_PUBLISHED[args.workload]) if args.workload in LIQ9_PUBLISHED else None,
             "dtype": "f32", "data": "synthetic", **liq9_fields(args.workload, full, t_max / args.steps),
-            "config": {**workload_config(full, args.workload),
-                       "parallelism": ("world shards" if args.workload in MULTI_WORLD else "replicas")
-                       if world > 1 else "single GPU"},
+            "config": workload_config(full, args.workload),
+            "parallelism": ("world shards" if args.workload in MULTI_WORLD else "replicas") if world > 1
+            else "single GPU",
+            "headline": "warm_started (learned start, judged)" if headline_warm else "plain",
             "e2e": e2e, "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                         "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "traffic_src": traffic_src,
                          "peak_src": pk["src"], "alg_bytes_per_particle": alg[dom], "mean_neighbours": nbar,
                          "particles_per_launch": per_launch[dom],
                          "avg_launch_us": per_launch_s * 1e6, "launches": cnt},

@@ -161,9 +161,61 @@ int adf_set_warm_starts(adf_solver* solver, const float* kappa_v, const float* k
  * restores "sph.kappa_v" / "sph.kappa_d" in place (coupling_hooks.py:260-271). Valid until adf_destroy. */
 int adf_state_arrays(adf_solver* solver, float** kappa_v, float** kappa_d);
 
+/* The rest of a snapshot's solver state, beside the warm starts: the keys that WorldStats.state_arrays
+ * (runtime.py:173-174), EmitterManager.state_arrays (runtime.py:389-399) and SPHPort.state_arrays (ports.py:201-203)
+ * add to alloy_state_arrays (coupling_hooks.py:115-138). Every pointer is the solver's own device storage, for
+ * snapshot code that copies the arrays out and back in place between steps; the emitter pointers change when
+ * emitters are added (adf_add_emitter(s)), all end with adf_destroy. */
+typedef struct {
+  int64_t* mass_in;       /* [W] "sph.mass_in": liquid mass emitted, int64 fixed point at 2^40 per kg */
+  int64_t* mass_out;      /* [W] "sph.mass_out": liquid mass retired (sinks, escape box, port) */
+  int32_t* escaped;       /* [W] "sph.escaped" */
+  float* emit_t;          /* [E] "sph.emit_t": layer clocks [s]; NULL without emitters */
+  int32_t* emit_cursor;   /* [E] "sph.emit_cursor": pool particles already emitted */
+  int32_t* emit_world;    /* [E] each emitter's world: alloy_state_worlds' map of the two emitter keys */
+  int32_t n_emitters;     /* E */
+  int32_t* port_stack;    /* [n] "sph.port_stack": world w's held particles, a stack in its index range
+                             [world_start[w], world_start[w + 1]) (the reference's [W][depth] stack, world by world) */
+  int32_t* port_top;      /* [W] "sph.port_top": held particles per world */
+  int32_t* port_absorbed; /* [W] "sph.port_absorbed" (cumulative since creation or reset) */
+  int32_t* port_emitted;  /* [W] "sph.port_emitted" */
+  int32_t* port_retired;  /* [W] "sph.port_retired" */
+  int32_t* port_taken;    /* [W] the last absorb / retire call's count per world (SPHPort.taken) */
+  int32_t* port_granted;  /* [W] the last port emit's count per world (SPHPort.granted) */
+} adf_state_storage;
+int adf_get_state_storage(adf_solver* solver, adf_state_storage* out);
+
+/* Replaces SPHPort.absorb and SPHPort.retire (ports.py:101-122, 183-189; SolverDFSPH.retire, solver.py:428-431): the
+ * masked liquid particles (mask: device int32 [n], non-zero = take) leave the liquid in one launch: ACTIVE cleared,
+ * their velocity in qd (device [n][3], the state's) zeroed, their mass booked to mass_out. keep = 1 holds them for
+ * adf_port_emit (phase -3, pushed on the world's stack in ascending id order), keep = 0 retires them for good (phase
+ * -2). Counts go to port_taken and the cumulative port_absorbed / port_retired. Capture-safe; no host work. The port
+ * books no flux energy (the reference's emitter energy export, emitters.flux_add, is not on this path). */
+int adf_port_take(adf_solver* solver, float* qd, const int32_t* mask, int keep, void* stream);
+
+/* Replaces SPHPort.emit (ports.py:191-199): per world the first min(n_req[w], R) requests (n_req: device int32 [W])
+ * pop held particles (fewer when the world's reservoir runs out), which become liquid at pos [W][R][3] with velocity
+ * vel [W][R][3] (device, world frame), written into q / qd (device [n][3], the state's), their mass booked into
+ * mass_in; port_granted[w] says how many. Capture-safe. */
+int adf_port_emit(adf_solver* solver, float* q, float* qd, const float* pos, const float* vel, int R,
+                  const int32_t* n_req, void* stream);
+
+/* Replaces SolverDFSPH.alloy_energy (solver.py:469-470; runtime.py:66-79, 423-430): kinetic plus gravity energy [J]
+ * of each world's liquid about (0, 0, z_ref[w]) (z_ref: device float64 [W]) into out (device float64 [W]): per
+ * particle m (v.v / 2 - g.(x - z_ref e_z)) in float64 from float32 dot products, summed in the per-world reductions'
+ * fixed chunk and tree order. Allocates nothing; capture-safe. */
+int adf_energy(adf_solver* solver, const float* q, const float* qd, const double* z_ref, double* out, void* stream);
+
+/* Replaces SolverDFSPH.alloy_stable_dt (solver.py:465-467; runtime.py:55-62, 82-90, 411-421): out[w] (device float32
+ * [W]) = dt_max for a world whose liquid is at rest, else clamp(cfl 2r / |v|max, dt_min, dt_max) over the state's
+ * liquid (qd: device [n][3]; a non-finite speed counts as 1e30). Allocates nothing; capture-safe. */
+int adf_stable_dt(adf_solver* solver, const float* qd, double cfl, double dt_min, double dt_max, float* out,
+                  void* stream);
+
 /* Replaces SolverDFSPH.reset (solver.py:353-362) + WorldStats.reset (runtime.py:431-449) + emitters.rewind
- * (emitters.py:241-255): masked worlds (host [W] bytes; NULL = all) get warm starts cleared, flags and phase back to
- * flags0/phase0 (device [n]), their counters and ledgers zeroed and their emitters rewound. */
+ * (emitters.py:241-255) + SPHPort.reset (ports.py:205-216): masked worlds (host [W] bytes; NULL = all) get warm
+ * starts cleared, flags and phase back to flags0/phase0 (device [n]), their counters and ledgers zeroed, their
+ * emitters rewound and their port reservoir back to its build-time particles. */
 int adf_reset(adf_solver* solver, const uint8_t* world_mask, const int32_t* flags0, const int8_t* phase0,
               void* stream);
 

@@ -9,16 +9,18 @@
 //   kernels.py:80-138     projected kernel, half-space volume Psi    -> halfspace()
 //   neighbors.py:36-51    particle groups (fluid = world, wall = -2 - world)
 //   neighbors.py:160-195  id-sorted lists, lowest K kept, overflow   -> build_lists()
-//   particle_walls.py:65-119  wall colour, 30-step bisection, plane  -> wall_slot()
-//   boundary.py:241-287, 336-396  slot fill with fit and taper (one particle-wall slot)
+//   particle_walls.py:65-119  wall colour, 30-step bisection, plane  -> wall_slots()
+//   boundary.py:190-396, boundary_slots.py:13-108  up to four slots per particle: static box walls (newton
+//                          geometry/kernels.py:310-370 box SDF) and the particle wall, nearest first, duplicate
+//                          eviction, fit and taper, inclusion-exclusion            -> wall_slots()
 //   pressure.py:144-193   density and DFSPH factor                   -> density_alpha()
 //   pressure.py:196-261   density rate, solve source, warm start     -> solve_init()
 //   pressure.py:264-352   pressure acceleration, relaxed Jacobi      -> accel(), jacobi()
 //   pressure.py:355-390   per-world start and stop test              -> solve()
-//   pressure.py:393-414, 461-480  lone-particle limit, apply pressure
+//   pressure.py:393-480   lone-particle limit, apply pressure, lone-particle wall friction
 //   solve_driver.py:121-186  solve orchestration (Jacobi branch)
 //   reduce.py:185-227     per-world float64 sums and max             -> world_sum() (tree order below)
-//   integrate.py:150-185, 212-326  XSPH, advection, particle-wall projection, speed
+//   integrate.py:60-326   XSPH, advection, projection onto walls and particle walls, sweep past fast steps, speed
 //   particle_walls.py:131-135  wall particles advance with their own velocity
 //   emitters.py:67-164    layer emitters, sinks and escape box, int64 mass ledger
 //   solver.py:218-268     step order
@@ -33,6 +35,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -44,6 +47,8 @@ namespace {
 
 constexpr int FLAG_ACTIVE = 1;  // newton ParticleFlags.ACTIVE (geometry/flags.py:14)
 constexpr int PROJECT_PASSES = 4;  // integrate.py:50
+constexpr int NS = 4;              // boundary slots per particle (boundary.py:36)
+constexpr float COS_SAME = 0.85f;  // boundary_slots.py:9
 constexpr int BISECT = 30;         // particle_walls.py:44
 constexpr double C_MIN = 1.0e-4;   // particle_walls.py:43
 
@@ -75,6 +80,7 @@ struct OrcParams {
   int has_bounds;
   double bounds_lo[3], bounds_hi[3];
   int cg;  // pressure iteration: 1 projected preconditioned CG (krylov.py), 0 relaxed Jacobi
+  int wall_friction;  // Config.wall_friction: Coulomb friction of lone particles and projections on shape walls
 };
 
 // Kernel constants in the working precision, derived from double host values exactly as the CUDA side does.
@@ -247,9 +253,18 @@ template <class R> struct Solver {
   std::vector<R> kv, kd;
   // per step
   std::vector<int> group, cnt, nbr;
-  std::vector<int> slot_on;
-  std::vector<R> slot_psi, slot_phi;
-  std::vector<V3<R>> slot_g, slot_vb, slot_xb, slot_n;
+  // boundary slots, [i * NS + k]: shape id (-1 empty; S = the particle wall), Psi, phi, grad Psi, wall velocity, and
+  // the start-of-step plane (closest point, outward normal; world frame for the particle wall, shape frame for a box)
+  std::vector<int> s_cnt, s_shape;
+  std::vector<R> s_psi, s_phi;
+  std::vector<V3<R>> s_g, s_vb, s_xbl, s_nbl;
+  // the liquid's static axis-aligned box walls (layout.py:207-246): per-world CSR of shape ids, centre, half extents,
+  // bounding radius and friction
+  int S = 0;
+  std::vector<int> sh_start, sh_ids;
+  std::vector<float> sh_pos, sh_half, sh_radius, sh_mu;
+  double sweep_len = 1.0e30;
+  std::vector<int> swept;
   std::vector<R> ratio, alpha, neff, active, reg, src, kappa, lower, err;
   // per world
   std::vector<int> overflow, escaped, projected, nonfinite, emit_overflow;
@@ -271,10 +286,17 @@ template <class R> struct Solver {
     z3(q); z3(v); z3(vtmp); z3(acc);
     zr(kv); zr(kd);
     group.assign(n, -1); cnt.assign(n, 0); nbr.assign((size_t)n * K, -1);
-    slot_on.assign(n, 0); zr(slot_psi); zr(slot_phi); z3(slot_g); z3(slot_vb); z3(slot_xb); z3(slot_n);
+    s_cnt.assign(n, 0);
+    s_shape.assign((size_t)n * NS, -1);
+    s_psi.assign((size_t)n * NS, R(0)); s_phi.assign((size_t)n * NS, R(0));
+    const V3<R> z0{R(0), R(0), R(0)};
+    s_g.assign((size_t)n * NS, z0); s_vb.assign((size_t)n * NS, z0); s_xbl.assign((size_t)n * NS, z0);
+    s_nbl.assign((size_t)n * NS, z0);
+    sweep_len = 0.5 * P.h;
+    sh_start.assign(W + 1, 0);
     zr(ratio); zr(alpha); zr(neff); zr(active); zr(reg); zr(src); zr(kappa); zr(lower); zr(err);
     auto zi = [&](std::vector<int>& a) { a.assign(W, 0); };
-    zi(overflow); zi(escaped); zi(projected); zi(nonfinite); zi(emit_overflow);
+    zi(overflow); zi(escaped); zi(projected); zi(nonfinite); zi(emit_overflow); zi(swept);
     zi(iters_den); zi(iters_div); zi(converged); zi(iters);
     auto zf = [&](std::vector<float>& a) { a.assign(W, 0.0f); };
     zf(den_err); zf(div_err); zf(den_err_max); zf(max_speed); zf(err_mean); zf(den_tol);
@@ -412,22 +434,144 @@ template <class R> struct Solver {
     for (int w = 0; w < W; ++w) overflow[w] += ovf[w];
   }
 
-  // particle_walls.py:65-119 + boundary.py:241-287: the particle-wall slot of fluid particle i
-  void wall_slots() {
+  // newton geometry/kernels.py:310-370 (sdf_box, sdf_box_grad): signed distance of the axis-aligned box of half
+  // extents hx at shape-local p, and its outward unit gradient
+  static R box_sdf(const V3<R>& p, const float* hx) {
+    R qx = std::fabs(p.x) - R(hx[0]), qy = std::fabs(p.y) - R(hx[1]), qz = std::fabs(p.z) - R(hx[2]);
+    V3<R> e{maxr(qx, R(0)), maxr(qy, R(0)), maxr(qz, R(0))};
+    return std::sqrt(dot_plain(e, e)) + minr(maxr(qx, maxr(qy, qz)), R(0));
+  }
+  static V3<R> normalized(const V3<R>& a) {
+    R l = std::sqrt(dot_plain(a, a));
+    if (l > R(0)) return {a.x / l, a.y / l, a.z / l};
+    return {R(0), R(0), R(0)};
+  }
+  static V3<R> box_grad(const V3<R>& p, const float* hx) {
+    const R h0 = R(hx[0]), h1 = R(hx[1]), h2 = R(hx[2]);
+    R qx = std::fabs(p.x) - h0, qy = std::fabs(p.y) - h1, qz = std::fabs(p.z) - h2;
+    if (qx > R(0) || qy > R(0) || qz > R(0)) {
+      V3<R> c{clampr(p.x, -h0, h0), clampr(p.y, -h1, h1), clampr(p.z, -h2, h2)};
+      return normalized(sub(p, c));
+    }
+    R sx = p.x < R(0) ? R(-1) : R(1), sy = p.y < R(0) ? R(-1) : R(1), sz = p.z < R(0) ? R(-1) : R(1);
+    if ((qx > qy && qx > qz) || (qy == R(0) && qz == R(0))) return {sx, R(0), R(0)};
+    if ((qy > qx && qy > qz) || (qx == R(0) && qz == R(0))) return {R(0), sy, R(0)};
+    return {R(0), R(0), sz};
+  }
+  V3<R> shape_local(int sh, const V3<R>& x) const {  // static axis-aligned box: the frame is its centre
+    return {x.x - R(sh_pos[3 * sh]), x.y - R(sh_pos[3 * sh + 1]), x.z - R(sh_pos[3 * sh + 2])};
+  }
+  V3<R> shape_world(int sh, const V3<R>& l) const {
+    return {l.x + R(sh_pos[3 * sh]), l.y + R(sh_pos[3 * sh + 1]), l.z + R(sh_pos[3 * sh + 2])};
+  }
+
+  // boundary_slots.py:13-37: (sh, phi) into particle i's phi-ascending row of n_ slots; the slot used, or -1
+  int slot_insert(int i, int n_, int sh, R phi) {
+    int* shp = &s_shape[(size_t)i * NS];
+    R* ph = &s_phi[(size_t)i * NS];
+    int pos = n_, k = n_ - 1;
+    while (k >= 0) {
+      if (ph[k] <= phi) break;
+      pos = k;
+      --k;
+    }
+    if (pos >= NS) return -1;
+    for (k = n_ >= NS ? NS - 1 : n_; k > pos; --k) {
+      shp[k] = shp[k - 1];
+      ph[k] = ph[k - 1];
+    }
+    shp[pos] = sh;
+    ph[pos] = phi;
+    return pos;
+  }
+
+  // boundary_slots.py:59-102: a wall (sh, phi, world normal nrm) into the row; a full row drops the farthest
+  // same-facing duplicate (cos > COS_SAME) of its four slots and the new wall, never one nearer than `near`, with
+  // none the farthest of the five. nr holds the slots' normals. 1 if the wall was kept.
+  int shape_insert(int i, int n_, int sh, R phi, const V3<R>& nrm, V3<R>* nr, R near) {
+    if (n_ < NS) {
+      const int r = slot_insert(i, n_, sh, phi);
+      if (r < 0) return 0;
+      for (int k = n_; k > r; --k) nr[k] = nr[k - 1];
+      nr[r] = nrm;
+      return 1;
+    }
+    int* shp = &s_shape[(size_t)i * NS];
+    R* ph = &s_phi[(size_t)i * NS];
+    const R cs = R(COS_SAME);
+    int ev = -1;
+    R ev_phi = R(-1);
+    for (int m = 0; m < NS; ++m)
+      if (phi >= near && ph[m] <= phi && dot_plain(nr[m], nrm) > cs) { ev = 4; ev_phi = phi; }
+    for (int k = 0; k < NS; ++k) {
+      const R pk = ph[k];
+      int dup = 0;
+      for (int m = 0; m < NS; ++m)
+        if (m != k && ph[m] <= pk && dot_plain(nr[m], nr[k]) > cs) dup = 1;
+      if (phi <= pk && dot_plain(nrm, nr[k]) > cs) dup = 1;
+      if (dup == 1 && pk >= near && pk > ev_phi) { ev = k; ev_phi = pk; }
+    }
+    if (ev < 0 && phi < ph[3]) ev = 3;
+    if (ev < 0 || ev == 4) return 0;
+    for (int k = ev; k < NS - 1; ++k) { shp[k] = shp[k + 1]; ph[k] = ph[k + 1]; nr[k] = nr[k + 1]; }
+    int pos = NS - 1;
+    while (pos > 0 && ph[pos - 1] > phi) { shp[pos] = shp[pos - 1]; ph[pos] = ph[pos - 1]; nr[pos] = nr[pos - 1]; --pos; }
+    shp[pos] = sh;
+    ph[pos] = phi;
+    nr[pos] = nrm;
+    return 1;
+  }
+
+  // (Psi, dPsi) of a wall at distance phi: A Psi(phi + delta) with the C1 taper (boundary.py:241-251, kernels.py)
+  void wall_volume(R phi, R& psi, R& dpsi) const {
     const R offset = R(P.wall_offset), amp = R(P.wall_amplitude), t0 = R(P.taper0), t1 = R(P.taper1);
-    const R reach = R(P.reach);
+    halfspace(kc, phi + offset, psi, dpsi);
+    psi = psi * amp;
+    dpsi = dpsi * amp;
+    if (phi > t0) {  // C1 taper between the first and second lattice layer
+      R L = t1 - t0;
+      R t = minr((phi - t0) / L, R(1));
+      R sm = R(1) - (t * t) * (R(3) - R(2) * t);
+      R dsm = ((R(6) * t) * (t - R(1))) / L;
+      R p0 = psi;
+      psi = p0 * sm;
+      dpsi = fma_(p0, dsm, dpsi * sm);
+    }
+  }
+
+  // boundary.py:190-238 (find), 254-396 (fill, combine) with particle_walls.py:65-119: fluid particle i's slots
+  void wall_slots() {
+    const R reach = R(P.reach), offset = R(P.wall_offset), near = R(0.1) * kc.h;
 #pragma omp parallel num_threads(nthreads)
     {
       struct C { int j; R wj, F; V3<R> d; };
       std::vector<C> cand;
 #pragma omp for schedule(dynamic, 256)
       for (int i = 0; i < n; ++i) {
-        slot_on[i] = 0;
-        slot_psi[i] = R(0);
-        slot_g[i] = {R(0), R(0), R(0)};
+        s_cnt[i] = 0;
+        for (int k = 0; k < NS; ++k) {
+          s_shape[(size_t)i * NS + k] = -1;
+          s_psi[(size_t)i * NS + k] = R(0);
+          s_g[(size_t)i * NS + k] = {R(0), R(0), R(0)};
+        }
         if (!is_fluid(i)) continue;
-        int w = world[i];
+        const int w = world[i];
         const V3<R> x = q[i];
+        int ns = 0;
+        V3<R> nr[NS];
+        // the world's box walls within the reach (boundary.py:211-222)
+        for (int c = sh_start[w]; c < sh_start[w + 1]; ++c) {
+          const int sh = sh_ids[c];
+          const V3<R> d{x.x - R(sh_pos[3 * sh]), x.y - R(sh_pos[3 * sh + 1]), x.z - R(sh_pos[3 * sh + 2])};
+          if (std::sqrt(dot_plain(d, d)) > R(sh_radius[sh]) + kc.h) continue;
+          const V3<R> xl = shape_local(sh, x);
+          const R phi = box_sdf(xl, &sh_half[3 * sh]);
+          if (phi < reach && phi + offset < kc.h) {
+            const V3<R> nw = normalized(box_grad(xl, &sh_half[3 * sh]));
+            if (shape_insert(i, ns, sh, phi, nw, nr, near) > 0 && ns < NS) ++ns;
+          }
+        }
+        // the particle wall: colour sums in ascending wall-particle id (particle_walls.py:65-107)
         cand.clear();
         for_each_near(wall_grid[w], x, [&](int j) {
           V3<R> d = sub(x, q[j]);
@@ -436,46 +580,88 @@ template <class R> struct Solver {
           R wj = R(wall_vol[j]) * Wv;
           if (wj > R(0)) cand.push_back({j, wj, F, d});
         });
-        if (cand.empty()) continue;
-        std::sort(cand.begin(), cand.end(), [](const C& a, const C& b) { return a.j < b.j; });
-        R c = R(0);
-        V3<R> gc{R(0), R(0), R(0)}, mv{R(0), R(0), R(0)};
-        for (const C& e : cand) {
-          R vol = R(wall_vol[e.j]);
-          c = c + e.wj;
-          gc.x = fma_(vol, e.d.x * e.F, gc.x);
-          gc.y = fma_(vol, e.d.y * e.F, gc.y);
-          gc.z = fma_(vol, e.d.z * e.F, gc.z);
-          mv.x = fma_(e.wj, v[e.j].x, mv.x);
-          mv.y = fma_(e.wj, v[e.j].y, mv.y);
-          mv.z = fma_(e.wj, v[e.j].z, mv.z);
+        R pw_phi = R(0);
+        V3<R> pw_n{R(0), R(0), R(0)}, pw_v{R(0), R(0), R(0)};
+        bool pw = false;
+        if (!cand.empty()) {
+          std::sort(cand.begin(), cand.end(), [](const C& a, const C& b) { return a.j < b.j; });
+          R c = R(0);
+          V3<R> gc{R(0), R(0), R(0)}, mv{R(0), R(0), R(0)};
+          for (const C& e : cand) {
+            R vol = R(wall_vol[e.j]);
+            c = c + e.wj;
+            gc.x = fma_(vol, e.d.x * e.F, gc.x);
+            gc.y = fma_(vol, e.d.y * e.F, gc.y);
+            gc.z = fma_(vol, e.d.z * e.F, gc.z);
+            mv.x = fma_(e.wj, v[e.j].x, mv.x);
+            mv.y = fma_(e.wj, v[e.j].y, mv.y);
+            mv.z = fma_(e.wj, v[e.j].z, mv.z);
+          }
+          mv = {mv.x / c, mv.y / c, mv.z / c};
+          R lg = std::sqrt(dot_plain(gc, gc));
+          if (!(c < R(C_MIN) || lg <= R(0))) {
+            R phi = colour_distance(kc, minr(c, R(1)));
+            if (phi < reach && phi + offset < kc.h) {
+              if (slot_insert(i, ns, S, phi) >= 0 && ns < NS) ++ns;
+              pw = true;
+              pw_phi = phi;
+              pw_n = {-gc.x / lg, -gc.y / lg, -gc.z / lg};
+              pw_v = mv;
+            }
+          }
         }
-        mv = {mv.x / c, mv.y / c, mv.z / c};
-        R lg = std::sqrt(dot_plain(gc, gc));
-        if (c < R(C_MIN) || lg <= R(0)) continue;
-        R phi = colour_distance(kc, minr(c, R(1)));
-        if (!(phi < reach && phi + offset < kc.h)) continue;
-        V3<R> nrm{-gc.x / lg, -gc.y / lg, -gc.z / lg};
-        R psi, dpsi;
-        halfspace(kc, phi + offset, psi, dpsi);
-        psi = psi * amp;
-        dpsi = dpsi * amp;
-        if (phi > t0) {  // C1 taper between the first and second lattice layer
-          R L = t1 - t0;
-          R t = minr((phi - t0) / L, R(1));
-          R sm = R(1) - (t * t) * (R(3) - R(2) * t);
-          R dsm = ((R(6) * t) * (t - R(1))) / L;
-          R p0 = psi;
-          psi = p0 * sm;
-          dpsi = fma_(p0, dsm, dpsi * sm);
+        (void)pw;
+        s_cnt[i] = ns;
+        // fill (boundary.py:254-334): a box's slot from its SDF, the particle wall's from its plane
+        for (int k = 0; k < ns; ++k) {
+          const size_t o = (size_t)i * NS + k;
+          const int sh = s_shape[o];
+          R phi, psi, dpsi;
+          V3<R> nrm;
+          if (sh == S) {
+            phi = pw_phi;
+            nrm = pw_n;
+            s_vb[o] = pw_v;
+            s_xbl[o] = {fma_(-phi, nrm.x, x.x), fma_(-phi, nrm.y, x.y), fma_(-phi, nrm.z, x.z)};
+            s_nbl[o] = nrm;
+          } else {
+            const V3<R> xl = shape_local(sh, x);
+            phi = box_sdf(xl, &sh_half[3 * sh]);
+            const V3<R> gl = box_grad(xl, &sh_half[3 * sh]);
+            nrm = normalized(gl);
+            s_nbl[o] = nrm;
+            s_xbl[o] = {fma_(-phi, nrm.x, xl.x), fma_(-phi, nrm.y, xl.y), fma_(-phi, nrm.z, xl.z)};
+            s_vb[o] = {R(0), R(0), R(0)};
+          }
+          wall_volume(phi, psi, dpsi);
+          s_phi[o] = phi;
+          s_psi[o] = psi;
+          s_g[o] = {dpsi * nrm.x, dpsi * nrm.y, dpsi * nrm.z};
         }
-        slot_on[i] = 1;
-        slot_psi[i] = psi;
-        slot_phi[i] = phi;
-        slot_g[i] = {dpsi * nrm.x, dpsi * nrm.y, dpsi * nrm.z};
-        slot_n[i] = nrm;
-        slot_xb[i] = {fma_(-phi, nrm.x, x.x), fma_(-phi, nrm.y, x.y), fma_(-phi, nrm.z, x.z)};
-        slot_vb[i] = mv;
+        // boundary.py:354-396: overlapping walls by inclusion-exclusion (psi as filled, gradients as they are
+        // rewritten slot by slot)
+        if (ns > 1) {
+          R ps[NS];
+          for (int k = 0; k < NS; ++k) ps[k] = s_psi[(size_t)i * NS + k];
+          for (int b = 0; b < ns; ++b) {
+            const size_t ob_i = (size_t)i * NS + b;
+            const V3<R> gb = s_g[ob_i];
+            R ob = R(0), sb = R(0);
+            for (int c = 0; c < ns; ++c) {
+              if (c == b) continue;
+              const V3<R> gcv = s_g[(size_t)i * NS + c];
+              const R lb = std::sqrt(dot_plain(gb, gb)), lc = std::sqrt(dot_plain(gcv, gcv));
+              R cbc = R(0);
+              if (lb > R(0) && lc > R(0)) cbc = clampr(dot_plain(gb, gcv) / (lb * lc), R(-1), R(1));
+              ob = ob + (R(1) - std::fabs(cbc)) * ps[c];
+              if (cbc > R(0) && (ps[c] > ps[b] || (ps[c] == ps[b] && c < b))) sb = sb + cbc;
+            }
+            ob = minr(ob, R(1));
+            s_psi[ob_i] = ps[b] * maxr((R(1) - R(0.5) * ob) - sb, R(0));
+            const R f = maxr((R(1) - ob) - sb, R(0));
+            s_g[ob_i] = {gb.x * f, gb.y * f, gb.z * f};
+          }
+        }
       }
     }
   }
@@ -509,14 +695,16 @@ template <class R> struct Solver {
         G.z = fma_(aF, rv.z, G.z);
         sq = fma_(bi * a, (F * F) * r2, sq);
       }
-      R psi = R(0);
-      if (slot_on[i]) {
-        psi = slot_psi[i];
-        G.x = G.x + slot_g[i].x;
-        G.y = G.y + slot_g[i].y;
-        G.z = G.z + slot_g[i].z;
+      R psi = R(0), lam = R(0);  // boundary slots, nearest first; lam: the opposing-wall compliance
+      for (int b = 0; b < s_cnt[i]; ++b) {
+        const size_t o = (size_t)i * NS + b;
+        psi = psi + s_psi[o];
+        G.x = G.x + s_g[o].x;
+        G.y = G.y + s_g[o].y;
+        G.z = G.z + s_g[o].z;
+        for (int c = b + 1; c < s_cnt[i]; ++c)
+          lam = lam + maxr(R(-2) * dot_plain(s_g[o], s_g[(size_t)i * NS + c]), R(0));
       }
-      R lam = R(0);
       R tot = (dotf(G, G) + sq) + lam;
       lam = lam + maxr(tot_min - tot, R(0));
       tot = maxr(tot, tot_min);
@@ -546,7 +734,10 @@ template <class R> struct Solver {
         R aF = (R(mass[j]) * inv_r0) * F;
         rate = fma_(aF, dotf(sub(vi, v[j]), rv), rate);
       }
-      if (slot_on[i]) rate = rate + dotf(sub(vi, slot_vb[i]), slot_g[i]);
+      for (int b = 0; b < s_cnt[i]; ++b) {
+        const size_t o = (size_t)i * NS + b;
+        rate = rate + dotf(sub(vi, s_vb[o]), s_g[o]);
+      }
       if (div) {
         R kdv = R(0);
         if (P.two_sided) kdv = maxr((warm_den * minr(kd[i], R(2.5e-4))) / (dt * dt), R(0));
@@ -586,11 +777,12 @@ template <class R> struct Solver {
       a.y = fma_(-cF, rv.y, a.y);
       a.z = fma_(-cF, rv.z, a.z);
     }
-    if (slot_on[i]) {
-      R k = kvec[i];
-      a.x = fma_(-k, slot_g[i].x, a.x);
-      a.y = fma_(-k, slot_g[i].y, a.y);
-      a.z = fma_(-k, slot_g[i].z, a.z);
+    for (int b = 0; b < s_cnt[i]; ++b) {
+      const R k = kvec[i];
+      const V3<R> g = s_g[(size_t)i * NS + b];
+      a.x = fma_(-k, g.x, a.x);
+      a.y = fma_(-k, g.y, a.y);
+      a.z = fma_(-k, g.z, a.z);
     }
     return a;
   }
@@ -627,7 +819,7 @@ template <class R> struct Solver {
       R aF = (R(mass[j]) * inv_r0) * F;
       ar = fma_(aF, dotf(sub(ai, acc[j]), rv), ar);
     }
-    if (slot_on[i]) ar = ar + dotf(ai, slot_g[i]);
+    for (int b = 0; b < s_cnt[i]; ++b) ar = ar + dotf(ai, s_g[(size_t)i * NS + b]);
     return ar;
   }
 
@@ -848,6 +1040,7 @@ template <class R> struct Solver {
     }
     contact_limit(dt);
     apply_pressure(div, dt);
+    lone_friction(dt);
     for (int w = 0; w < W; ++w) {
       if (div) { iters_div[w] = iters[w]; div_err[w] = err_mean[w]; }
       else { iters_den[w] = iters[w]; den_err[w] = err_mean[w]; }
@@ -859,22 +1052,62 @@ template <class R> struct Solver {
     }
   }
 
-  // pressure.py:393-414 (one particle-wall slot)
+  // pressure.py:393-414: a lone particle's push may stop its approach and separate it at most v_sep from its walls
   void contact_limit(R dt) {
     const R v_sep = R(P.v_sep);
 #pragma omp parallel for num_threads(nthreads) schedule(static)
     for (int i = 0; i < n; ++i) {
       if (!is_fluid(i) || cnt[i] > 0 || kappa[i] <= R(0)) continue;
-      if (!slot_on[i]) continue;
-      V3<R> G = slot_g[i];
-      R ps = slot_psi[i];
-      V3<R> vb{ps * slot_vb[i].x, ps * slot_vb[i].y, ps * slot_vb[i].z};
+      if (s_cnt[i] == 0) continue;
+      V3<R> G{R(0), R(0), R(0)}, vb{R(0), R(0), R(0)};
+      R ps = R(0);
+      for (int b = 0; b < s_cnt[i]; ++b) {
+        const size_t o = (size_t)i * NS + b;
+        G = {G.x + s_g[o].x, G.y + s_g[o].y, G.z + s_g[o].z};
+        vb = {fma_(s_psi[o], s_vb[o].x, vb.x), fma_(s_psi[o], s_vb[o].y, vb.y), fma_(s_psi[o], s_vb[o].z, vb.z)};
+        ps = ps + s_psi[o];
+      }
       R g = std::sqrt(dot_plain(G, G));
       if (g <= R(0)) continue;
       if (ps > R(0)) vb = {vb.x / ps, vb.y / ps, vb.z / ps};
       V3<R> nn{-G.x / g, -G.y / g, -G.z / g};
       R u = dotf(sub(v[i], vb), nn);
       kappa[i] = minr(kappa[i], maxr(v_sep - u, R(0)) / (dt * g));
+    }
+  }
+
+  // pressure.py:417-458: Coulomb friction of a lone particle on its walls, after the solve's velocity update: the
+  // wall's push dv_n = dt k |G| takes up to mu dv_n of its tangential speed relative to the walls, never reversing
+  // it; mu is that of the wall in its largest-Psi slot (a particle wall has none)
+  void lone_friction(R dt) {
+    if (!P.wall_friction || S == 0) return;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < n; ++i) {
+      if (!is_fluid(i) || cnt[i] > 0 || kappa[i] <= R(0) || s_cnt[i] == 0) continue;
+      V3<R> G{R(0), R(0), R(0)}, vb{R(0), R(0), R(0)};
+      R ws = R(0), pbest = R(0);
+      int best = -1;
+      for (int b = 0; b < s_cnt[i]; ++b) {
+        const size_t o = (size_t)i * NS + b;
+        G = {G.x + s_g[o].x, G.y + s_g[o].y, G.z + s_g[o].z};
+        vb = {fma_(s_psi[o], s_vb[o].x, vb.x), fma_(s_psi[o], s_vb[o].y, vb.y), fma_(s_psi[o], s_vb[o].z, vb.z)};
+        ws = ws + s_psi[o];
+        if (s_psi[o] > pbest) { pbest = s_psi[o]; best = b; }
+      }
+      R g = std::sqrt(dot_plain(G, G));
+      if (g <= R(0) || ws <= R(0) || best < 0) continue;
+      const int sh = s_shape[(size_t)i * NS + best];
+      if (sh >= S) continue;
+      const R mu = R(sh_mu[sh]);
+      if (mu <= R(0)) continue;
+      const V3<R> nn{-G.x / g, -G.y / g, -G.z / g};
+      const V3<R> u = sub(v[i], V3<R>{vb.x / ws, vb.y / ws, vb.z / ws});
+      const R un = dotf(u, nn);
+      const V3<R> vt{fma_(-un, nn.x, u.x), fma_(-un, nn.y, u.y), fma_(-un, nn.z, u.z)};
+      const R lt = std::sqrt(dot_plain(vt, vt));
+      if (lt <= R(0)) continue;
+      const R f = minr(R(1), (((mu * dt) * kappa[i]) * g) / lt);
+      v[i] = {fma_(-f, vt.x, v[i].x), fma_(-f, vt.y, v[i].y), fma_(-f, vt.z, v[i].z)};
     }
   }
 
@@ -931,10 +1164,49 @@ template <class R> struct Solver {
     v.swap(vtmp);
   }
 
-  // integrate.py:181-185 + particle_walls.py:131-135 + integrate.py:212-309 (particle-wall slot only)
+  // integrate.py:75-95 (box_span) and 98-126 (path_entry) for a static box: the last outside parameter of the path
+  // l0 -> l1 (its frame) before it first enters box sh, by the exact slab test; 2 when it stays outside or starts
+  // inside
+  R box_entry(int sh, const V3<R>& l0, const V3<R>& l1) const {
+    const float* hx = &sh_half[3 * sh];
+    if (box_sdf(l0, hx) < R(0)) return R(2);
+    R lo = R(-1.0e30), hi = R(1.0e30);
+    const R d[3] = {l1.x - l0.x, l1.y - l0.y, l1.z - l0.z}, o[3] = {l0.x, l0.y, l0.z};
+    for (int a = 0; a < 3; ++a) {
+      const R h = R(hx[a]);
+      if (std::fabs(d[a]) > R(0)) {
+        const R ta = (-h - o[a]) / d[a], tb = (h - o[a]) / d[a];
+        lo = maxr(lo, minr(ta, tb));
+        hi = minr(hi, maxr(ta, tb));
+      } else if (std::fabs(o[a]) > h) {
+        lo = R(2.0e30);
+      }
+    }
+    if (lo <= hi && lo <= R(1) && hi >= R(0)) return maxr(lo, R(0));
+    return R(2);
+  }
+
+  // integrate.py:192-205: Coulomb friction of a projection (Config.wall_friction) after the inward speed -vn went
+  V3<R> wall_friction_v(V3<R> vv, const V3<R>& vb, const V3<R>& nn, R vn, int sh) const {
+    if (!P.wall_friction) return vv;
+    const R mu = R(sh_mu[sh]);
+    if (mu <= R(0)) return vv;
+    const V3<R> u = sub(vv, vb);
+    const R un = dotf(u, nn);
+    const V3<R> vt{fma_(-un, nn.x, u.x), fma_(-un, nn.y, u.y), fma_(-un, nn.z, u.z)};
+    const R lt = std::sqrt(dot_plain(vt, vt));
+    if (lt <= R(0)) return vv;
+    const R f = minr(R(1), (mu * (-vn)) / lt);
+    return {fma_(-f, vt.x, vv.x), fma_(-f, vt.y, vv.y), fma_(-f, vt.z, vv.z)};
+  }
+
+  // integrate.py:181-185 + particle_walls.py:131-135 + integrate.py:212-309: advection, then each liquid particle
+  // that moved further than the sweep length is swept along its path against its world's walls, and its slots'
+  // walls push it out in up to PROJECT_PASSES passes (the particle wall onto its start plane advanced with the wall;
+  // a box through its SDF at the new place, onto its start-of-step tangent plane when that holds it)
   void advect_project(R dt) {
-    const R eps = R(P.project_eps);
-    std::vector<int> moved_w(W, 0);
+    const R eps = R(P.project_eps), r = R(P.particle_radius), sweep = R(sweep_len);
+    std::vector<int> moved_w(W, 0), swept_w(W, 0);
     for (int i = 0; i < n; ++i) {
       if (is_fluid(i)) {
         q[i] = {fma_(dt, v[i].x, q[i].x), fma_(dt, v[i].y, q[i].y), fma_(dt, v[i].z, q[i].z)};
@@ -943,23 +1215,89 @@ template <class R> struct Solver {
       }
     }
     for (int i = 0; i < n; ++i) {
-      if (!is_fluid(i) || !slot_on[i]) continue;
+      if (!is_fluid(i)) continue;
+      const int w = world[i];
       V3<R> x = q[i], vv = v[i];
-      const V3<R> nn = slot_n[i], vb = slot_vb[i], xb = slot_xb[i];
-      V3<R> p{fma_(dt, vb.x, xb.x), fma_(dt, vb.y, xb.y), fma_(dt, vb.z, xb.z)};
       int moved = 0;
-      for (int pass = 0; pass < PROJECT_PASSES; ++pass) {
-        R d = dotf(sub(x, p), nn);
-        if (!(d < eps)) break;
-        R push = eps - d;
-        x = {fma_(push, nn.x, x.x), fma_(push, nn.y, x.y), fma_(push, nn.z, x.z)};
-        R vn = dotf(sub(vv, vb), nn);
-        if (vn < R(0)) vv = {fma_(-vn, nn.x, vv.x), fma_(-vn, nn.y, vv.y), fma_(-vn, nn.z, vv.z)};
-        moved = 1;
+      const V3<R> step{dt * vv.x, dt * vv.y, dt * vv.z};
+      if (sh_start[w + 1] > sh_start[w] && std::sqrt(dot_plain(step, step)) > sweep) {
+        const V3<R> x0{x.x - step.x, x.y - step.y, x.z - step.z};
+        const V3<R> span = sub(x, x0);
+        const R reach = std::sqrt(dot_plain(span, span)) + r;
+        R best = R(2);
+        int hit = -1;
+        V3<R> lh{R(0), R(0), R(0)};
+        for (int c = sh_start[w]; c < sh_start[w + 1]; ++c) {
+          const int sh = sh_ids[c];
+          const V3<R> d0{x0.x - R(sh_pos[3 * sh]), x0.y - R(sh_pos[3 * sh + 1]), x0.z - R(sh_pos[3 * sh + 2])};
+          if (!(std::sqrt(dot_plain(d0, d0)) <= R(sh_radius[sh]) + reach)) continue;
+          const V3<R> l0 = shape_local(sh, x0), l1 = shape_local(sh, x);
+          const R t = box_entry(sh, l0, l1);
+          if (t < best) {
+            best = t;
+            hit = sh;
+            lh = {fma_(t, l1.x - l0.x, l0.x), fma_(t, l1.y - l0.y, l0.y), fma_(t, l1.z - l0.z, l0.z)};
+          }
+        }
+        if (hit >= 0) {
+          const R phi = box_sdf(lh, &sh_half[3 * hit]);
+          const V3<R> nn = normalized(box_grad(lh, &sh_half[3 * hit]));
+          const V3<R> xw = shape_world(hit, lh);
+          const R push = maxr(eps - phi, R(0));
+          x = {fma_(push, nn.x, xw.x), fma_(push, nn.y, xw.y), fma_(push, nn.z, xw.z)};
+          const R vn = dotf(vv, nn);
+          if (vn < R(0)) {
+            vv = {fma_(-vn, nn.x, vv.x), fma_(-vn, nn.y, vv.y), fma_(-vn, nn.z, vv.z)};
+            vv = wall_friction_v(vv, V3<R>{R(0), R(0), R(0)}, nn, vn, hit);
+          }
+          moved = 1;
+          swept_w[w]++;
+        }
       }
-      if (moved) { q[i] = x; v[i] = vv; moved_w[world[i]]++; }
+      int busy = 1;
+      for (int pass = 0; pass < PROJECT_PASSES && busy; ++pass) {
+        busy = 0;
+        for (int b = 0; b < s_cnt[i]; ++b) {
+          const size_t o = (size_t)i * NS + b;
+          const int sh = s_shape[o];
+          if (sh == S) {  // the particle wall's plane at its end-of-step place
+            const V3<R> nn = s_nbl[o], vb = s_vb[o], xb = s_xbl[o];
+            const V3<R> pp{fma_(dt, vb.x, xb.x), fma_(dt, vb.y, xb.y), fma_(dt, vb.z, xb.z)};
+            const R d = dotf(sub(x, pp), nn);
+            if (d < eps) {
+              const R push = eps - d;
+              x = {fma_(push, nn.x, x.x), fma_(push, nn.y, x.y), fma_(push, nn.z, x.z)};
+              const R vn = dotf(sub(vv, vb), nn);
+              if (vn < R(0)) vv = {fma_(-vn, nn.x, vv.x), fma_(-vn, nn.y, vv.y), fma_(-vn, nn.z, vv.z)};
+              moved = busy = 1;
+            }
+          } else if (sh >= 0) {  // a static box: its SDF at the new place, its start plane when that holds it
+            const V3<R> xl = shape_local(sh, x);
+            const R phi = box_sdf(xl, &sh_half[3 * sh]);
+            if (phi < eps) {
+              V3<R> nn = normalized(box_grad(xl, &sh_half[3 * sh]));
+              R push = eps - phi;
+              if (s_phi[o] >= R(0)) {
+                const V3<R> ns = s_nbl[o];
+                const R push_s = eps - dotf(ns, sub(x, shape_world(sh, s_xbl[o])));
+                if (push_s > R(0)) { nn = ns; push = push_s; }
+              }
+              if (push > R(0)) {
+                x = {fma_(push, nn.x, x.x), fma_(push, nn.y, x.y), fma_(push, nn.z, x.z)};
+                const R vn = dotf(vv, nn);
+                if (vn < R(0)) {
+                  vv = {fma_(-vn, nn.x, vv.x), fma_(-vn, nn.y, vv.y), fma_(-vn, nn.z, vv.z)};
+                  vv = wall_friction_v(vv, V3<R>{R(0), R(0), R(0)}, nn, vn, sh);
+                }
+                moved = busy = 1;
+              }
+            }
+          }
+        }
+      }
+      if (moved) { q[i] = x; v[i] = vv; moved_w[w]++; }
     }
-    for (int w = 0; w < W; ++w) projected[w] += moved_w[w];
+    for (int w = 0; w < W; ++w) { projected[w] += moved_w[w]; swept[w] += swept_w[w]; }
   }
 
   // emitters.py:134-164
@@ -1182,23 +1520,60 @@ int orc_prime(void* hp, double dt, double tol, int max_it) {
 }
 void orc_prepare_density(void* hp) { DISPATCH(s.prepare_density()); }
 
-// name: ratio alpha neff active reg src kappa err slot_psi slot_phi
+// name: ratio alpha neff active reg src kappa err, and slot k's (k = 0 when the name has no suffix, else the digit
+// after a colon, e.g. "slot_psi:1") slot_psi slot_phi slot_g slot_vb slot_n
 int orc_get_field(void* hp, const char* name, float* out) {
   int ok = 1;
   DISPATCH({
     auto pick = [&](const char* nm, const auto& a) { if (std::strcmp(name, nm) == 0) { copy_out(a, out); ok = 0; } };
     pick("ratio", s.ratio); pick("alpha", s.alpha); pick("neff", s.neff); pick("active", s.active);
     pick("reg", s.reg); pick("src", s.src); pick("kappa", s.kappa); pick("err", s.err);
-    pick("slot_psi", s.slot_psi); pick("slot_phi", s.slot_phi);
-    if (std::strcmp(name, "slot_g") == 0) { copy_out3(s.slot_g, out); ok = 0; }
-    if (std::strcmp(name, "slot_vb") == 0) { copy_out3(s.slot_vb, out); ok = 0; }
-    if (std::strcmp(name, "slot_n") == 0) { copy_out3(s.slot_n, out); ok = 0; }
     if (std::strcmp(name, "acc") == 0) { copy_out3(s.acc, out); ok = 0; }
+    const char* colon = std::strchr(name, ':');
+    const size_t base = colon ? (size_t)(colon - name) : std::strlen(name);
+    const int k = colon ? std::atoi(colon + 1) : 0;
+    auto is = [&](const char* nm) { return std::strlen(nm) == base && std::strncmp(name, nm, base) == 0; };
+    if (k >= 0 && k < NS) {
+      for (int i = 0; i < s.n; ++i) {
+        const size_t o = (size_t)i * NS + k;
+        if (is("slot_psi")) out[i] = (float)s.s_psi[o];
+        if (is("slot_phi")) out[i] = (float)s.s_phi[o];
+        const auto* v3 = is("slot_g") ? &s.s_g : is("slot_vb") ? &s.s_vb : is("slot_n") ? &s.s_nbl : nullptr;
+        if (v3) {
+          out[3 * i] = (float)(*v3)[o].x;
+          out[3 * i + 1] = (float)(*v3)[o].y;
+          out[3 * i + 2] = (float)(*v3)[o].z;
+        }
+      }
+      if (is("slot_psi") || is("slot_phi") || is("slot_g") || is("slot_vb") || is("slot_n")) ok = 0;
+    }
   });
   return ok;
 }
 
-void orc_get_slot_on(void* hp, int* out) { DISPATCH(std::memcpy(out, s.slot_on.data(), sizeof(int) * s.n)); }
+// per particle: its slot count (0: none), and with shapes != NULL its slots' wall ids [n][4] (-1 empty; the
+// particle wall is the shape count)
+void orc_get_slot_on(void* hp, int* out) { DISPATCH(std::memcpy(out, s.s_cnt.data(), sizeof(int) * s.n)); }
+void orc_get_slot_shapes(void* hp, int* out) {
+  DISPATCH(std::memcpy(out, s.s_shape.data(), sizeof(int) * (size_t)s.n * NS));
+}
+
+// The liquid's static axis-aligned box walls (layout.py:207-246): S shapes, per-world CSR start[W + 1] / ids, each
+// box's centre pos[S][3], half extents half[S][3], bounding radius[S] and friction mu[S]; sweep length
+// min(h / 2, thinnest / 2) (integrate.py:42-49).
+void orc_set_shapes(void* hp, int S, const int* start, const int* ids, const float* pos, const float* half,
+                    const float* radius, const float* mu, double thinnest) {
+  DISPATCH({
+    s.S = S;
+    s.sh_start.assign(start, start + s.W + 1);
+    s.sh_ids.assign(ids, ids + start[s.W]);
+    s.sh_pos.assign(pos, pos + 3 * S);
+    s.sh_half.assign(half, half + 3 * S);
+    s.sh_radius.assign(radius, radius + S);
+    s.sh_mu.assign(mu, mu + S);
+    s.sweep_len = std::min(0.5 * s.P.h, 0.5 * thinnest);
+  });
+}
 
 void orc_get_lists(void* hp, int* rows, int* count) {
   DISPATCH({
@@ -1208,13 +1583,14 @@ void orc_get_lists(void* hp, int* rows, int* count) {
   });
 }
 
-// int arrays: iters_den iters_div overflow escaped projected nonfinite emit_overflow
+// int arrays: iters_den iters_div overflow escaped projected nonfinite emit_overflow swept
 // float arrays: den_err div_err den_err_max max_speed den_tol ; int64: mass_in mass_out mass0
-void orc_get_report(void* hp, int* ints /*7*W*/, float* floats /*5*W*/, int64_t* ledger /*3*W*/) {
+void orc_get_report(void* hp, int* ints /*8*W*/, float* floats /*5*W*/, int64_t* ledger /*3*W*/) {
   DISPATCH({
     int W = s.W;
-    const std::vector<int>* ia[7] = {&s.iters_den, &s.iters_div, &s.overflow, &s.escaped, &s.projected, &s.nonfinite, &s.emit_overflow};
-    for (int k = 0; k < 7; ++k) std::memcpy(ints + k * W, ia[k]->data(), sizeof(int) * W);
+    const std::vector<int>* ia[8] = {&s.iters_den, &s.iters_div, &s.overflow, &s.escaped, &s.projected, &s.nonfinite,
+                                     &s.emit_overflow, &s.swept};
+    for (int k = 0; k < 8; ++k) std::memcpy(ints + k * W, ia[k]->data(), sizeof(int) * W);
     const std::vector<float>* fa[5] = {&s.den_err, &s.div_err, &s.den_err_max, &s.max_speed, &s.den_tol};
     for (int k = 0; k < 5; ++k) std::memcpy(floats + k * W, fa[k]->data(), sizeof(float) * W);
     std::memcpy(ledger, s.mass_in.data(), 8 * W);

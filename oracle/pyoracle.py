@@ -40,7 +40,7 @@ class OrcParams(C.Structure):
                 ("divergence_solve", C.c_int), ("two_sided", C.c_int), ("xsph_c", C.c_double),
                 ("capacity", C.c_int), ("v_sep", C.c_double), ("relief_speed", C.c_double),
                 ("project_eps", C.c_double), ("has_bounds", C.c_int), ("bounds_lo", C.c_double * 3),
-                ("bounds_hi", C.c_double * 3), ("cg", C.c_int)]
+                ("bounds_hi", C.c_double * 3), ("cg", C.c_int), ("wall_friction", C.c_int)]
 
 
 def params_from_config(cfg) -> OrcParams:
@@ -63,6 +63,7 @@ def params_from_config(cfg) -> OrcParams:
     p.v_sep = cfg.contact_separation_speed
     p.relief_speed = cfg.compression_relief_speed or 0.0
     p.project_eps = hc.project_eps
+    p.wall_friction = int(bool(cfg.wall_friction))
     if cfg.world_bounds is not None:
         p.has_bounds = 1
         for a in range(3):
@@ -96,6 +97,8 @@ def lib():
         L.orc_prime.argtypes = [P, C.c_double, C.c_double, C.c_int]
         L.orc_get_field.argtypes = [P, C.c_char_p, fp]
         L.orc_get_slot_on.argtypes = [P, ip]
+        L.orc_get_slot_shapes.argtypes = [P, ip]
+        L.orc_set_shapes.argtypes = [P, C.c_int, ip, ip, fp, fp, fp, fp, C.c_double]
         L.orc_get_lists.argtypes = [P, ip, ip]
         L.orc_get_report.argtypes = [P, ip, fp, C.POINTER(C.c_int64)]
         L.orc_active_mass.argtypes = [P, C.POINTER(C.c_int64)]
@@ -144,6 +147,31 @@ class Oracle:
         if threads is not None:
             self.L.orc_set_threads(self.h, int(threads))
         self.set_state(a["q"], a["qd"])
+        if "shape_type" in a and len(a["shape_type"]):
+            self.set_shapes(a)
+
+    def set_shapes(self, a: dict):
+        """The model's static box walls (``alloy_b200.solvers.sph.shapes.shape_table`` of the same arrays)."""
+        from types import SimpleNamespace
+
+        import torch
+
+        from alloy_b200.solvers.sph.shapes import shape_table
+
+        t = lambda k: torch.from_numpy(np.ascontiguousarray(a[k]))  # noqa: E731
+        m = SimpleNamespace(world_count=self.W, shape_count=len(a["shape_type"]), shape_type=t("shape_type"),
+                            shape_flags=t("shape_flags"), shape_world=t("shape_world"), shape_body=t("shape_body"),
+                            shape_scale=t("shape_scale"), shape_transform=t("shape_transform"),
+                            shape_material_mu=t("shape_mu"), sph=SimpleNamespace(shape_boundary=t("shape_boundary")))
+        tab = shape_table(m)
+        keep = [np.ascontiguousarray(tab.start, np.int32), np.ascontiguousarray(tab.ids if len(tab.ids) else
+                                                                                np.zeros(1, np.int32), np.int32),
+                np.ascontiguousarray(tab.xform[:, :3], np.float32), np.ascontiguousarray(tab.scale, np.float32),
+                np.ascontiguousarray(tab.radius, np.float32), np.ascontiguousarray(tab.mu, np.float32)]
+        self._shape_keep = keep
+        self.L.orc_set_shapes(self.h, tab.count, _p(keep[0], C.c_int), _p(keep[1], C.c_int), _p(keep[2], C.c_float),
+                              _p(keep[3], C.c_float), _p(keep[4], C.c_float), _p(keep[5], C.c_float),
+                              float(tab.thinnest))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -206,15 +234,22 @@ class Oracle:
         self.L.orc_prepare_density(self.h)
 
     def field(self, name: str) -> np.ndarray:
-        three = name in ("slot_g", "slot_vb", "slot_n", "acc")
+        three = name.split(":")[0] in ("slot_g", "slot_vb", "slot_n", "acc")
         out = np.zeros((self.n, 3) if three else self.n, np.float32)
         if self.L.orc_get_field(self.h, name.encode(), _p(out, C.c_float)) != 0:
             raise KeyError(name)
         return out
 
     def slot_on(self) -> np.ndarray:
+        """Boundary slots per particle (0: none)."""
         out = np.zeros(self.n, np.int32)
         self.L.orc_get_slot_on(self.h, _p(out, C.c_int))
+        return out
+
+    def slot_shapes(self) -> np.ndarray:
+        """[n, 4] wall id of each slot (-1 empty; the particle wall's id is the shape count)."""
+        out = np.zeros((self.n, 4), np.int32)
+        self.L.orc_get_slot_shapes(self.h, _p(out, C.c_int))
         return out
 
     def lists(self):
@@ -226,12 +261,12 @@ class Oracle:
 
     def report(self) -> dict:
         W = self.W
-        ints = np.zeros((7, W), np.int32)
+        ints = np.zeros((8, W), np.int32)
         fl = np.zeros((5, W), np.float32)
         led = np.zeros((3, W), np.int64)
         self.L.orc_get_report(self.h, _p(ints, C.c_int), _p(fl, C.c_float), _p(led, C.c_int64))
         names_i = ("iters_density", "iters_divergence", "neighbor_overflow", "escaped", "projected", "nonfinite",
-                   "emitter_overflow")
+                   "emitter_overflow", "swept")
         names_f = ("density_err", "divergence_err", "density_err_max", "max_speed", "density_tol")
         out = {k: ints[i].copy() for i, k in enumerate(names_i)}
         out.update({k: fl[i].copy() for i, k in enumerate(names_f)})

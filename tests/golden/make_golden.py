@@ -106,6 +106,39 @@ def main(root: Path) -> None:
             "halfspace": [[float(d), [float(c) for c in K.halfspace_volume(float(d), h, 0.0, kid)]] for d in ds],
             "colour_distance": [[float(c), float(pw["colour_distance"](float(c), h, kid))] for c in cs],
         })
+    # build.py's liquid volume fill (emit_object's points): the reference's liquid_points with stand-ins for the card
+    # types it tests with isinstance (alloy/cards/types.py ParticleSource and Primitive)
+    cards = types.ModuleType("alloy.cards.types")
+
+    class ParticleSource:
+        def __init__(self, region):
+            self.region = region
+
+    class Primitive:
+        def __init__(self, kind, size):
+            self.kind, self.size = kind, size
+
+    cards.ParticleSource, cards.Primitive = ParticleSource, Primitive
+    for name in ("alloy", "alloy.cards"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.modules["alloy.cards.types"] = cards
+    bns = {"np": np, "math": math}
+    bfn = extract(sph / "build.py", ["lattice_points", "_inside_primitive", "disk_rings", "column_layers",
+                                     "liquid_points"], {**bns, "DISK_CLEAR": 0.375})
+    bns.update(bfn)
+    for f in bfn.values():
+        f.__globals__.update(bfn)
+    shapes = [("region", ((0.0, 0.0, 0.0), (0.1, 0.06, 0.05)), 0.01), ("box", (0.011, 0.02, 0.013), 0.004),
+              ("sphere", (0.02, 0.0, 0.0), 0.004), ("ellipsoid", (0.02, 0.012, 0.016), 0.004), ("cylinder", (0.02, 0.01, 0.0), 0.004),
+              ("cylinder", (0.006, 0.01, 0.0), 0.002), ("capsule", (0.01, 0.015, 0.0), 0.004)]
+    fills = []
+    for kind, size, sp in shapes:
+        shape = ParticleSource(size) if kind == "region" else Primitive(kind, size)
+        pts = bfn["liquid_points"](shape, sp)
+        fills.append({"kind": kind, "size": size, "spacing": sp, "points": np.asarray(pts, np.float64).tolist()})
+    (OUT.parent / "reference_liquid_points.json").write_text(json.dumps(
+        {"source": "alloy/solvers/sph/build.py liquid_points (float64 numpy, card types stood in)", "cases": fills}))
+
     OUT.write_text(json.dumps({"source": "alloy/solvers/sph kernels.py, config.py, particle_walls.py (float64 Python "
                                          "evaluation with a warp stand-in)", "cases": cases}, indent=1))
     print(f"wrote {OUT} ({len(cases)} cases)")

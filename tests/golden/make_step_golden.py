@@ -20,7 +20,12 @@ corner, dt 1 ms, the plain settings (resting-jitter rule off, XSPH 0.01):
   break) in a 0.2 x 0.2 x 0.24 m box, relaxed Jacobi, tolerances 1e-3;
 - ``dam_break_cg``: the same with the projected CG solve (krylov.py, the reference's default);
 - ``column_jacobi_tight``: a 4 x 4 x 16 column in a 0.08 x 0.08 x 0.4 m box at tolerances 1e-4, which takes
-  several Jacobi iterations per solve.
+  several Jacobi iterations per solve;
+- ``tank_impacts``: the block thrown into a corner of that tank and eight lone particles, four of them beyond the
+  CFL step (testing.tank_impacts): projections onto the walls, lone-particle limits and friction, the sweep;
+- ``tank_sdf_jacobi`` / ``tank_sdf_cg``: the dam-break block in the reference's own open box tank of five box shapes,
+  walls h thick (build.py:113-137), seen through their signed distance fields: up to four boundary slots per
+  particle at the tank's edges and corners, the pressure and projection passes of the shape branch, wall friction.
 Recorded per step: the start state and warm starts, the neighbour rows, the particle-wall slot, density ratio,
 factor, effective neighbour count, per-solve iterations and mean errors, the warm starts each solve stores and the
 end state. One file per case: tests/golden/reference_steps_<case>.npz.
@@ -51,6 +56,12 @@ CASES = {
     "dam_break_cg": {"scene": _BLOCK, "config": {"pressure_solver": "cg"}, "steps": 10},
     "column_jacobi_tight": {"scene": _COLUMN, "config": {"pressure_solver": "jacobi", "max_density_error": 1.0e-4,
                                                          "max_divergence_error": 1.0e-4}, "steps": 10},
+    "tank_sdf_jacobi": {"scene": {**_BLOCK, "walls": "sdf", "open_top": True}, "config": {"pressure_solver": "jacobi"},
+                        "steps": 12},
+    "tank_sdf_cg": {"scene": {**_BLOCK, "walls": "sdf", "open_top": True}, "config": {"pressure_solver": "cg"},
+                    "steps": 12},
+    "tank_impacts": {"scene": {"dt": 1.0e-3}, "builder": "tank_impacts", "config": {"pressure_solver": "jacobi"},
+                     "steps": 10},
 }
 PROJECT_EPS = 1.0e-3  # solver.py:483
 
@@ -64,7 +75,12 @@ def scene_arrays(case: str) -> tuple[dict, object]:
     from alloy_b200.solvers.sph.testing import dam_break
 
     c = CASES[case]
-    sc = dam_break(device="cpu", **c["scene"], **c["config"])
+    if c.get("builder") == "tank_impacts":
+        from alloy_b200.solvers.sph.testing import tank_impacts
+
+        sc = tank_impacts(device="cpu", dt=c["scene"]["dt"], **c["config"])
+    else:
+        sc = dam_break(device="cpu", **c["scene"], **c["config"])
     return sc.model.host(), sc.config
 
 
@@ -125,19 +141,41 @@ class RefStep:
         # particle_walls.py:224-247, coupling_hooks.py:156-168)
         sh = R.boundary.ShapeArrays()
         z32 = lambda: wp.zeros(1, dtype=wp.int32)  # noqa: E731
-        sh.start, sh.ids = wp.zeros(W + 1, dtype=wp.int32), z32()
-        sh.geo, sh.body, sh.sdf_index, sh.bvh = z32(), z32(), z32(), z32()
-        sh.mesh, sh.scale, sh.radius, sh.mu = (wp.zeros(1, dtype=wp.uint64), wp.zeros(1, dtype=wp.vec3),
-                                               wp.zeros(1, dtype=wp.float32), wp.zeros(1, dtype=wp.float32))
-        sh.xform, sh.tex = wp.zeros(1, dtype=wp.transform), None
+        S = int(len(a.get("shape_type", ())))
+        self.S = S
+        if S:  # the model's shapes (layout.py:207-230): Newton's box radius |half extents| (geometry/utils.py:83-84)
+            start, ids = R.boundary.world_shape_table(a["shape_world"], a["shape_flags"], a["shape_type"], W,
+                                                      a["shape_boundary"] == 3)
+            sh.start = wp.array(start, dtype=wp.int32)
+            sh.ids = wp.array(ids if len(ids) else np.zeros(1, np.int32), dtype=wp.int32)
+            sh.geo = wp.array(a["shape_type"], dtype=wp.int32)
+            sh.scale = wp.array(a["shape_scale"], dtype=wp.vec3)
+            sh.xform = refrun.TfArray(a["shape_transform"])
+            sh.body = wp.array(a["shape_body"], dtype=wp.int32)
+            sh.radius = wp.array(np.linalg.norm(np.abs(a["shape_scale"].astype(np.float64)), axis=1)
+                                 .astype(np.float32), dtype=wp.float32)
+            sh.mu = wp.array(a["shape_mu"], dtype=wp.float32)
+            sh.sdf_index = wp.full(S, -1, dtype=wp.int32)
+            sh.bvh = wp.zeros(S, dtype=wp.int32)
+            sh.mesh = wp.zeros(S, dtype=wp.uint64)
+            self.thinnest = float(2.0 * a["shape_scale"][np.unique(ids)].astype(np.float64).min()) if len(ids) \
+                else float("inf")  # layout.py:135-148 (boxes)
+        else:
+            sh.start, sh.ids = wp.zeros(W + 1, dtype=wp.int32), z32()
+            sh.geo, sh.body, sh.sdf_index, sh.bvh = z32(), z32(), z32(), z32()
+            sh.mesh, sh.scale, sh.radius, sh.mu = (wp.zeros(1, dtype=wp.uint64), wp.zeros(1, dtype=wp.vec3),
+                                                   wp.zeros(1, dtype=wp.float32), wp.zeros(1, dtype=wp.float32))
+            sh.xform = refrun.TfArray(np.array([[0, 0, 0, 0, 0, 0, 1]], np.float32))
+            self.thinnest = float("inf")
+        sh.tex = None
         sh.curvature = int(cfg.boundary_curvature_order)
         off, amp = R.kernels.boundary_fit(cfg.spacing, cfg.h, cfg.kernel)
         sh.offset, sh.amplitude = np.float32(off), np.float32(amp)
         sh.taper0, sh.taper1 = np.float32(0.5 * cfg.spacing), np.float32(1.5 * cfg.spacing)
         sh.reach = np.float32(1.5 * cfg.spacing)
         sh.bvh_dist = np.float32(2.0 * cfg.h)
-        sh.soft = R.soft_walls.empty_soft(0, "cpu")
-        pw = R.particle_walls.empty_walls(0, cfg.h, cfg.kernel_id, "cpu")
+        sh.soft = R.soft_walls.empty_soft(S, "cpu")  # soft faces would follow the shapes; none here
+        pw = R.particle_walls.empty_walls(S, cfg.h, cfg.kernel_id, "cpu")  # the particle wall's id: soft.base + 0
         vid = np.flatnonzero((a["flags"] & 2) != 0)
         r64 = a["radius"].astype(np.float64)
         vol, mask = np.zeros(n, np.float32), np.zeros(n, np.int32)
@@ -203,6 +241,9 @@ class RefStep:
         rec["slot_psi"] = self._slots.psi.numpy()[:, 0].copy()
         rec["slot_phi"] = self._slots.phi.numpy()[:, 0].copy()
         rec["slot_g"] = self._slots.gpsi.numpy()[:, 0].copy()
+        rec["slot_shapes"] = self._slots.shape.numpy().copy()  # [n, 4]
+        rec["slot_psi4"] = self._slots.psi.numpy().copy()
+        rec["slot_g4"] = self._slots.gpsi.numpy().copy()
         self.launch(pr.density_alpha_kernel, [p, sl, self._h, self._kind, self._n_full, self._tot_min, w.ratio,
                                               w.alpha, w.neff, w.active])
         rec["ratio"], rec["alpha"], rec["neff"] = (np.asarray(w.ratio).copy(), np.asarray(w.alpha).copy(),
@@ -224,7 +265,7 @@ class RefStep:
                        inputs=[self.vid, dt, self.q, self.qd])  # ParticleWalls.advance
         s_ = self._slots
         r = float(cfg.particle_radius)
-        sweep = R.integrate.sweep_length(self._h, float("inf"))
+        sweep = R.integrate.sweep_length(self._h, self.thinnest)
         self.launch(R.integrate.project_kernel, [p, s_.shape, s_.phi, s_.xbl, s_.nbl, s_.face, s_.vb, self.sa,
                                                  self.bq, self.bqd, self.com, PROJECT_EPS * r, self.projected,
                                                  self.bq, dt, sweep, r, self.swept, self.shape_work])
@@ -235,6 +276,7 @@ class RefStep:
         rec["div_err"], rec["den_err"], rec["den_err_max"] = st.div_err.copy(), st.den_err.copy(), st.den_err_max.copy()
         rec["max_speed"] = np.asarray(self.max_speed).copy()
         rec["projected"] = np.asarray(self.projected).copy()
+        rec["swept"] = np.asarray(self.swept).copy()
 
 
 def _Solves(host: RefStep):

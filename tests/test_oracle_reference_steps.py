@@ -28,18 +28,29 @@ from alloy_b200.solvers.sph.testing import dam_break
 from oracle.pyoracle import Oracle
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-CASES = ("dam_break_jacobi", "dam_break_cg", "column_jacobi_tight")
-# Largest differences measured over the three cases, for scale: ratio 3.6e-6, alpha 1.4e-5, neff 4.7e-6, slot psi
-# 6.5e-6, slot phi 4.9e-7, kv 2.3e-5, kd 1.8e-3, q 4.5e-8 m (1.3e-7 m free running), qd 4.8e-5, mean errors 1.9e-3.
-TOL = {"ratio": 1e-4, "alpha": 1e-4, "neff": 1e-4, "reg": 1e-4, "slot_psi": 1e-4, "slot_phi": 1e-5, "kv": 2e-4,
-       "kd": 1e-2, "qd": 5e-4, "q_abs_m": 1e-6, "err_rel": 1e-2}
+CASES = ("dam_break_jacobi", "dam_break_cg", "column_jacobi_tight", "tank_sdf_jacobi", "tank_sdf_cg", "tank_impacts")
+SDF_CASES = ("tank_sdf_jacobi", "tank_sdf_cg", "tank_impacts")
+# Largest differences measured over the six cases, for scale: ratio 7.3e-6, alpha 4.3e-5, neff 4.7e-6, reg 1.5e-6,
+# slot psi 3.9e-5 (every slot), slot phi 4.9e-7, kv 2.3e-5, kd 6.5e-3 (CG in the box tank), q 8.8e-8 m (1.3e-7 m free
+# running), qd 5.9e-4 (box tank; 3.6e-3 free running with CG, which amplifies last-bit differences), mean errors
+# 1.9e-3.
+TOL = {"ratio": 1e-4, "alpha": 2e-4, "neff": 1e-4, "reg": 1e-4, "slot_psi": 2e-4, "slot_phi": 1e-5, "kv": 2e-4,
+       "kd": 2e-2, "qd": 2e-3, "q_abs_m": 1e-6, "err_rel": 1e-2,
+       "err_abs": 1e-7, "qd_free": 1e-2}  # per-world mean errors: 1 % of the value plus 1e-4 of the 1e-3 solver tolerance
+
+
+def scene(c: dict, device="cpu"):
+    if c.get("builder") == "tank_impacts":
+        from alloy_b200.solvers.sph.testing import tank_impacts
+
+        return tank_impacts(device=device, dt=c["scene"]["dt"], **c["config"])
+    return dam_break(device=device, **c["scene"], **c["config"])
 
 
 def load(case: str):
     g = np.load(GOLDEN / f"reference_steps_{case}.npz")
     c = ast.literal_eval(str(g["scene"]))
-    sc = dam_break(device="cpu", **c["scene"], **c["config"])
-    return g, c, sc
+    return g, c, scene(c)
 
 
 def rel(x, y, m) -> float:
@@ -81,6 +92,10 @@ def test_anchored_steps_match_reference_kernels(case):
         assert on.any() or s > 0
         if on.any():
             assert rel(orc.field("slot_phi"), g["slot_phi"][s], on) <= TOL["slot_phi"], (case, s)
+        if "slot_shapes" in g.files:  # every slot: the same walls in the same order, Psi within tolerance
+            np.testing.assert_array_equal(orc.slot_shapes()[fluid], g["slot_shapes"][s][fluid], err_msg=f"{case} {s}")
+            psi4 = np.stack([orc.field(f"slot_psi:{k}") for k in range(4)], 1)
+            assert rel(psi4, g["slot_psi4"][s], fluid) <= TOL["slot_psi"], (case, s)
         kv, kd = orc.warm()
         assert rel(kv, g["kv"][s], fluid) <= TOL["kv"], (case, s)
         assert rel(kd, g["kd"][s], fluid) <= TOL["kd"], (case, s)
@@ -89,7 +104,7 @@ def test_anchored_steps_match_reference_kernels(case):
         assert rel(qd, g["qd1"][s], fluid) <= TOL["qd"], (case, s)
         for ours, ref in (("density_err", "den_err"), ("divergence_err", "div_err")):
             r = float(g[ref][s][0])
-            assert abs(float(rep[ours][0]) - r) <= TOL["err_rel"] * r + 1e-9, (case, s, ours)
+            assert abs(float(rep[ours][0]) - r) <= TOL["err_rel"] * r + TOL["err_abs"], (case, s, ours)
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -105,12 +120,29 @@ def test_free_run_matches_reference_kernels(case):
         assert rep["iters_divergence"][0] == g["iters_div"][s][0], (case, s)
         assert rep["iters_density"][0] == g["iters_den"][s][0], (case, s)
         assert float(np.max(np.abs(q - g["q1"][s])[fluid])) <= TOL["q_abs_m"], (case, s)
-        assert rel(qd, g["qd1"][s], fluid) <= TOL["qd"], (case, s)
+        assert rel(qd, g["qd1"][s], fluid) <= TOL["qd_free"], (case, s)
 
 
-def test_cases_cover_both_solvers_and_the_iteration_cap():
-    """The fixtures exercise relaxed Jacobi, projected CG, multi-iteration solves and the 50-iteration cap."""
+@pytest.mark.parametrize("case", SDF_CASES)
+def test_wall_counters_match_reference(case):
+    """Projections onto walls and sweeps past fast steps happen at the same steps as in the reference."""
+    g, c, sc = load(case)
+    orc = Oracle(sc.model.host(), sc.config)
+    for s in range(int(g["steps"])):
+        orc.set_state(g["q0"][s], g["qd0"][s])
+        orc.set_warm(g["kv0"][s], g["kd0"][s])
+        orc.step(c["scene"]["dt"])
+        rep = orc.report()
+        assert rep["projected"][0] == g["projected"][s][0] and rep["swept"][0] == g["swept"][s][0], (case, s)
+
+
+def test_cases_cover_both_solvers_walls_and_the_iteration_cap():
+    """The fixtures exercise relaxed Jacobi, projected CG, multi-iteration solves and the 50-iteration cap, particle
+    walls and box walls with two and three slots per particle, projections and sweeps."""
     its = {case: (load(case)[0]["iters_div"][:, 0], load(case)[0]["iters_den"][:, 0]) for case in CASES}
     assert load("dam_break_cg")[1]["config"]["pressure_solver"] == "cg"
     div, den = its["column_jacobi_tight"]
     assert div.max() == 50 and den.max() > 2
+    g = load("tank_impacts")[0]
+    assert ((g["slot_shapes"] >= 0).sum(-1) >= 3).any()
+    assert g["projected"][-1][0] > 0 and g["swept"][-1][0] > 0
