@@ -40,7 +40,7 @@ class Params(C.Structure):
                 ("divergence_solve", C.c_int), ("two_sided", C.c_int), ("xsph_c", C.c_double),
                 ("capacity", C.c_int), ("v_sep", C.c_double), ("relief_speed", C.c_double),
                 ("project_eps", C.c_double), ("has_bounds", C.c_int), ("bounds_lo", C.c_double * 3),
-                ("bounds_hi", C.c_double * 3), ("cg", C.c_int)]
+                ("bounds_hi", C.c_double * 3), ("cg", C.c_int), ("wall_friction", C.c_int)]
 
 
 class ModelDesc(C.Structure):
@@ -48,7 +48,8 @@ class ModelDesc(C.Structure):
     _fields_ = [("n", C.c_int), ("world_count", C.c_int), ("world_start", C.POINTER(C.c_int32)),
                 ("q_host", C.POINTER(C.c_float)), ("mass", C.c_void_p), ("rest_density", C.c_void_p),
                 ("radius", C.c_void_p), ("flags", C.c_void_p), ("phase", C.c_void_p), ("world", C.c_void_p),
-                ("gravity", C.c_void_p)]
+                ("gravity", C.c_void_p), ("n_shapes", C.c_int), ("shape_start", C.POINTER(C.c_int32)),
+                ("shape_ids", C.POINTER(C.c_int32)), ("shape_box", C.POINTER(C.c_float)), ("sweep_len", C.c_double)]
 
 
 class Report(C.Structure):
@@ -56,7 +57,7 @@ class Report(C.Structure):
     _fields_ = [(name, C.c_void_p) for name in (
         "density_err", "divergence_err", "iters_density", "iters_divergence", "mass_in", "mass_out", "mass_initial",
         "escaped", "neighbor_overflow", "max_speed", "density_err_max", "projected", "nonfinite", "emitter_overflow",
-        "density_tol", "learned_divergence", "learned_density")]
+        "density_tol", "learned_divergence", "learned_density", "swept")]
 
 
 class StateStorage(C.Structure):

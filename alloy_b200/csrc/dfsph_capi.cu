@@ -397,6 +397,7 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   prof_end(s, st);
   prof_begin(s, 2, st);
   LAUNCH(s, k_wall_slots, blocks(n), BLOCK, st, P);
+  if (P.slot_cap > 1) LAUNCH(s, k_shape_slots, blocks(n), BLOCK, st, P);
   prof_end(s, st);
   prof_begin(s, 3, st);
   run_tk(s, TK_DENSITY, st, P);
@@ -740,6 +741,21 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     return fail(ADF_ERR_VALUE, "world_start out of range");
   if (m->n > 0 && (!m->mass || !m->rest_density || !m->radius || !m->flags || !m->phase || !m->world || !m->gravity))
     return fail(ADF_ERR_VALUE, "adf_create: a model array is null");
+  if (m->n_shapes < 0) return fail(ADF_ERR_VALUE, "adf_create: negative n_shapes");
+  if (m->n_shapes > 0) {
+    if (!m->shape_start || !m->shape_box) return fail(ADF_ERR_VALUE, "adf_create: shape_start and shape_box needed");
+    if (m->world_count > 0 && m->shape_start[0] != 0) return fail(ADF_ERR_VALUE, "shape_start[0] must be 0");
+    for (int w = 0; w < m->world_count; ++w)
+      if (m->shape_start[w + 1] < m->shape_start[w]) return fail(ADF_ERR_VALUE, "shape_start must not decrease");
+    const int total = m->world_count > 0 ? m->shape_start[m->world_count] : 0;
+    if (total > 0 && !m->shape_ids) return fail(ADF_ERR_VALUE, "adf_create: shape_ids needed");
+    for (int c = 0; c < total; ++c)
+      if (m->shape_ids[c] < 0 || m->shape_ids[c] >= m->n_shapes)
+        return fail(ADF_ERR_VALUE, "shape_ids out of range [0, n_shapes)");
+    for (int k = 0; k < m->n_shapes; ++k)
+      for (int a = 0; a < 8; ++a)
+        if (!std::isfinite(m->shape_box[8 * k + a])) return fail(ADF_ERR_VALUE, "shape_box holds a non-finite value");
+  }
   CK(cudaSetDevice(device));
   adf_solver* s = new adf_solver();
   s->prm = p;
@@ -782,6 +798,12 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     d.blo[a] = (float)p.bounds_lo[a];
     d.bhi[a] = (float)p.bounds_hi[a];
   }
+  const int n_box_refs = (m->n_shapes > 0 && m->world_count > 0) ? m->shape_start[m->world_count] : 0;
+  d.slot_cap = n_box_refs > 0 ? 4 : 1;
+  d.n_shapes = m->n_shapes;
+  d.sweep_len = (float)m->sweep_len;
+  d.prad = (float)p.particle_radius;
+  d.wall_friction = p.wall_friction != 0;
   d.mass = m->mass;
   d.rho0 = m->rest_density;
   d.flags = m->flags;
@@ -830,10 +852,20 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.nbrjf, (size_t)s->K * n);
   rc |= s->alloc(&d.nbrw, (size_t)s->K * n);
   rc |= s->alloc(&d.cnt, n);
-  rc |= s->alloc(&d.slot_g, n);
-  rc |= s->alloc(&d.slot_vb, n);
-  rc |= s->alloc(&d.slot_n, n);
-  rc |= s->alloc(&d.slot_xb, n);
+  rc |= s->alloc(&d.slot_g, (size_t)d.slot_cap * n);
+  rc |= s->alloc(&d.slot_vb, (size_t)d.slot_cap * n);
+  rc |= s->alloc(&d.slot_n, (size_t)d.slot_cap * n);
+  rc |= s->alloc(&d.slot_xb, (size_t)d.slot_cap * n);
+  int *sh_start = nullptr, *sh_ids = nullptr;
+  float4 *sh_pos = nullptr, *sh_half = nullptr;
+  if (d.slot_cap > 1) {
+    rc |= s->alloc(&d.slot_cnt, n);
+    rc |= s->alloc(&sh_start, (size_t)W + 1);
+    rc |= s->alloc(&sh_ids, (size_t)n_box_refs);
+    rc |= s->alloc(&sh_pos, (size_t)m->n_shapes);
+    rc |= s->alloc(&sh_half, (size_t)m->n_shapes);
+  }
+  rc |= s->alloc(&d.swept, W);
   rc |= s->alloc(&d.ratio, n);
   rc |= s->alloc(&d.alpha, n);
   rc |= s->alloc(&d.neff, n);
@@ -916,6 +948,10 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   }
   d.wall_vol = wall_vol;
   d.grid = grid;
+  d.sh_start = sh_start;
+  d.sh_ids = sh_ids;
+  d.sh_pos = sh_pos;
+  d.sh_half = sh_half;
   d.chunk_begin = chunk_begin;
   d.chunk_end = chunk_end;
   d.world_chunk_start = world_chunk_start;
@@ -942,6 +978,18 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   }
   CKC(cudaMemcpy(world_chunk_start, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice));
   CKC(cudaMemcpy(s->ws_d, s->ws_host.data(), sizeof(int) * s->ws_host.size(), cudaMemcpyHostToDevice));
+  if (d.slot_cap > 1) {  // the box walls: per-world id lists, (centre, radius) and (half extents, mu) per shape
+    std::vector<float4> bp(m->n_shapes), bh(m->n_shapes);
+    for (int k = 0; k < m->n_shapes; ++k) {
+      const float* b = m->shape_box + 8 * (size_t)k;
+      bp[k] = make_float4(b[0], b[1], b[2], b[3]);
+      bh[k] = make_float4(b[4], b[5], b[6], b[7]);
+    }
+    CKC(cudaMemcpy(sh_start, m->shape_start, sizeof(int) * (s->W + 1), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(sh_ids, m->shape_ids, sizeof(int) * n_box_refs, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(sh_pos, bp.data(), sizeof(float4) * bp.size(), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(sh_half, bh.data(), sizeof(float4) * bh.size(), cudaMemcpyHostToDevice));
+  }
   {  // the port's reservoir: each world's build-time held particles, popped in ascending id order (ports.py:124-133)
     std::vector<int8_t> ph(s->n);
     if (s->n > 0) CKC(cudaMemcpy(ph.data(), m->phase, s->n, cudaMemcpyDeviceToHost));
@@ -965,7 +1013,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   CKC(cudaMemset(d.kv, 0, sizeof(float) * n));
   CKC(cudaMemset(d.kd, 0, sizeof(float) * n));
   CKC(cudaMemset(d.err_orig, 0, sizeof(float) * n));
-  void* zero_w[] = {d.overflow, d.escaped, d.projected, d.nonfinite, d.wall_overflow, d.max_speed_bits, d.converged,
+  void* zero_w[] = {d.overflow, d.escaped, d.projected, d.swept, d.nonfinite, d.wall_overflow, d.max_speed_bits, d.converged,
                     d.iters, d.err_mean, s->iters_den, s->iters_div, s->emit_overflow, s->den_err, s->div_err,
                     s->den_err_max, d.emax};
   for (void* z : zero_w) CKC(cudaMemset(z, 0, 4 * W));
@@ -1208,6 +1256,7 @@ int adf_get_report(adf_solver* s, adf_report* r, void* stream) {
   rc |= cp(r->nonfinite, s->d.nonfinite, 4 * W);
   rc |= cp(r->emitter_overflow, s->emit_overflow, 4 * W);
   rc |= cp(r->density_tol, s->den_tol, 4 * W);
+  rc |= cp(r->swept, s->d.swept, 4 * W);
   if (s->warm_alloc) {
     rc |= cp(r->learned_divergence, s->d.learned, 4 * W);
     rc |= cp(r->learned_density, s->d.learned + W, 4 * W);
@@ -1454,6 +1503,7 @@ int adf_reset(adf_solver* s, const uint8_t* world_mask, const int32_t* flags0, c
   if (W > 0) {
     int rc = 0;
     rc |= zero_masked(s->d.escaped, 4) | zero_masked(s->d.projected, 4) | zero_masked(s->d.overflow, 4);
+    rc |= zero_masked(s->d.swept, 4);
     rc |= zero_masked(s->d.nonfinite, 4) | zero_masked(s->emit_overflow, 4) | zero_masked(s->mass_in, 8);
     rc |= zero_masked(s->d.mass_out, 8);
     if (rc) return rc;
@@ -1647,16 +1697,36 @@ int adf_debug_field(adf_solver* s, const char* name, float* out, void* stream) {
   if (!s || !name || !out) return fail(ADF_ERR_VALUE, "adf_debug_field: null argument");
   cudaStream_t st = (cudaStream_t)stream;
   const DevP& d = s->d;
+  // "name:k" reads slot k of a slot field (k = 0 without a suffix)
+  std::string base(name);
+  int slot = 0;
+  const size_t colon = base.find(':');
+  if (colon != std::string::npos) {
+    const std::string suffix = base.substr(colon + 1);
+    base = base.substr(0, colon);
+    if (suffix.empty() || suffix.size() > 1 || suffix[0] < '0' || suffix[0] > '9' || base.rfind("slot_", 0) != 0)
+      return fail(ADF_ERR_VALUE, std::string("adf_debug_field: bad slot suffix in ") + name);
+    slot = suffix[0] - '0';
+    if (slot >= d.slot_cap)
+      return fail(ADF_ERR_VALUE, std::string("adf_debug_field: ") + name + ": this model has " +
+                                     std::to_string(d.slot_cap) + " slot(s) per particle");
+  }
+  if (base == "slot_shape" || base == "slot_count") {
+    CK(cudaMemsetAsync(out, 0, sizeof(float) * (size_t)s->n, st));
+    LAUNCH(s, k_slot_info, blocks(s->n), BLOCK, st, d, base == "slot_count" ? -1 : slot, out);
+    return check_launch();
+  }
+  const size_t so = (size_t)slot * s->n * 4;  // floats to slot k of a float4 slot array
   struct F { const char* nm; const float* ptr; int stride, comp, ncomp; };
   const F fields[] = {
       {"ratio", d.ratio, 1, 0, 1}, {"alpha", d.alpha, 1, 0, 1}, {"neff", d.neff, 1, 0, 1}, {"reg", d.reg, 1, 0, 1},
       {"src", d.src, 1, 0, 1}, {"kappa", d.kappa, 1, 0, 1}, {"lower", d.lower, 1, 0, 1},
-      {"slot_psi", (const float*)d.slot_g, 4, 3, 1}, {"slot_phi", (const float*)d.slot_vb, 4, 3, 1},
-      {"acc", (const float*)d.acc, 4, 0, 3}, {"slot_g", (const float*)d.slot_g, 4, 0, 3},
-      {"slot_vb", (const float*)d.slot_vb, 4, 0, 3}, {"slot_n", (const float*)d.slot_n, 4, 0, 3},
+      {"slot_psi", (const float*)d.slot_g + so, 4, 3, 1}, {"slot_phi", (const float*)d.slot_vb + so, 4, 3, 1},
+      {"acc", (const float*)d.acc, 4, 0, 3}, {"slot_g", (const float*)d.slot_g + so, 4, 0, 3},
+      {"slot_vb", (const float*)d.slot_vb + so, 4, 0, 3}, {"slot_n", (const float*)d.slot_n + so, 4, 0, 3},
       {"pred_kv", d.pred_kv, 1, 0, 1}, {"pred_kd", d.pred_kd, 1, 0, 1}};
   for (const F& f : fields) {
-    if (std::strcmp(f.nm, name) != 0) continue;
+    if (base != f.nm) continue;
     if (!f.ptr) return fail(ADF_ERR_STATE, std::string("adf_debug_field: ") + name + " is not recorded");
     CK(cudaMemsetAsync(out, 0, sizeof(float) * f.ncomp * (size_t)s->n, st));
     LAUNCH(s, k_unsort_n, blocks(s->n), BLOCK, st, s->n, d.nfw, d.id_of, f.ptr, f.stride, f.comp, out, f.ncomp);

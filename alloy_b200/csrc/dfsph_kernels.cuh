@@ -114,10 +114,23 @@ struct DevP {
   int2* nbrjf;  // [K][n] (row entry, bits of its gradient factor F(r_ij)), written by k_density_alpha
   float* nbrw;  // [K][n] kernel value W(r_ij) of each row entry, written by k_density_alpha, read by k_xsph
   int* cnt;
-  float4* slot_g;   // dPsi/dx (3), psi; psi < 0: no slot
+  // Boundary slots (boundary.py:36): slot b of sorted particle p at b * n + p of each array, nearest wall first.
+  float4* slot_g;   // dPsi/dx (3), psi; with slot_cap 1, psi < 0: no slot
   float4* slot_vb;  // wall velocity (3), phi
-  float4* slot_n;   // outward normal (3), 0
-  float4* slot_xb;  // surface point (3), 0
+  float4* slot_n;   // outward normal (3), the wall's id as int bits (the particle wall's is n_shapes)
+  float4* slot_xb;  // start-of-step surface point (3; world frame for the particle wall, the box's frame for a box), 0
+  int slot_cap;      // 1: the particle wall only; 4: static box walls too (boundary.py:36 NUM_SLOTS)
+  int8_t* slot_cnt;  // [n] slots in use (slot_cap 4)
+  // the liquid's static axis-aligned box walls (layout.py:207-246), ids into the model's shape table
+  int n_shapes;
+  const int* sh_start;    // [W + 1]: world w's walls are sh_ids[sh_start[w] .. sh_start[w + 1])
+  const int* sh_ids;
+  const float4* sh_pos;   // centre (3), bounding radius
+  const float4* sh_half;  // half extents (3), Coulomb friction mu
+  float sweep_len;        // a step longer than this is swept against the world's boxes (integrate.py:42-49)
+  float prad;             // particle radius
+  int wall_friction;      // Config.wall_friction
+  int* swept;             // [W] particles swept onto a box this step
   float* ratio;
   float* alpha;
   float* neff;
@@ -190,6 +203,12 @@ struct DevP {
   int* cg_act_new;  // [W] set when a bound variable was activated this iteration (k_cg_apply_finish)
   double2* part2;   // [chunks] partial sums of pairs
 };
+
+// Slots in use by sorted liquid particle p, and the index of its slot b.
+__device__ __forceinline__ int slot_count(const DevP& P, int p) {
+  return P.slot_cap > 1 ? (int)P.slot_cnt[p] : (P.slot_g[p].w >= 0.0f ? 1 : 0);
+}
+__device__ __forceinline__ size_t slot_at(const DevP& P, int b, int p) { return (size_t)b * P.n + p; }
 
 __device__ __forceinline__ bool is_fluid_orig(const DevP& P, int i) {
   return (P.flags[i] & FLAG_ACTIVE) != 0 && P.phase[i] >= 1;
@@ -755,8 +774,26 @@ __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
 // --------------------------------------------------------------------------------------- particle-wall slot
 // particle_walls.py:65-119 + boundary.py:241-287: colour c = sum V_j W over the world's wall particles (ascending
 // wall id), its gradient and mean velocity; the distance phi with Psi(phi) = c; the slot filled as a flat wall at phi
-// with the fitted amplitude, offset and C1 taper. One slot per particle (no SDF shapes), so the inclusion-exclusion
-// combine of boundary.py:336-396 is the identity.
+// with the fitted amplitude, offset and C1 taper. Without box walls this is the particle's one slot; with them
+// k_shape_slots merges it with the boxes' (slot_cap 4).
+
+// (Psi, dPsi) of a wall at distance phi: A Psi(phi + delta) with the C1 taper between the first and second lattice
+// layer (boundary.py:241-251)
+__device__ __forceinline__ void wall_volume(const DevP& P, float phi, float& psi, float& dpsi) {
+  halfspace(P.kc, phi + P.wall_offset, psi, dpsi);
+  psi = psi * P.wall_amp;
+  dpsi = dpsi * P.wall_amp;
+  if (phi > P.taper0) {
+    float L = P.taper1 - P.taper0;
+    float t = minr((phi - P.taper0) / L, 1.0f);
+    float sm = 1.0f - (t * t) * (3.0f - 2.0f * t);
+    float dsm = ((6.0f * t) * (t - 1.0f)) / L;
+    float p0 = psi;
+    psi = p0 * sm;
+    dpsi = ADF_FMA(p0, dsm, dpsi * sm);
+  }
+}
+
 __device__ __forceinline__ void wall_slot_fill(const DevP& P, int p, float4 xi, float c, float gx, float gy, float gz,
                                                float mx, float my, float mz);
 
@@ -835,21 +872,10 @@ __device__ __forceinline__ void wall_slot_fill(const DevP& P, int p, float4 xi, 
   if (!(phi < P.reach && phi + P.wall_offset < P.kc.h)) return;
   float nx = -gx / lg, ny = -gy / lg, nz = -gz / lg;
   float psi, dpsi;
-  halfspace(P.kc, phi + P.wall_offset, psi, dpsi);
-  psi = psi * P.wall_amp;
-  dpsi = dpsi * P.wall_amp;
-  if (phi > P.taper0) {
-    float L = P.taper1 - P.taper0;
-    float t = minr((phi - P.taper0) / L, 1.0f);
-    float sm = 1.0f - (t * t) * (3.0f - 2.0f * t);
-    float dsm = ((6.0f * t) * (t - 1.0f)) / L;
-    float p0 = psi;
-    psi = p0 * sm;
-    dpsi = ADF_FMA(p0, dsm, dpsi * sm);
-  }
+  wall_volume(P, phi, psi, dpsi);
   P.slot_g[p] = make_float4(dpsi * nx, dpsi * ny, dpsi * nz, psi);
   P.slot_vb[p] = make_float4(mx, my, mz, phi);
-  P.slot_n[p] = make_float4(nx, ny, nz, 0.0f);
+  P.slot_n[p] = make_float4(nx, ny, nz, __int_as_float(P.n_shapes));
   P.slot_xb[p] = make_float4(ADF_FMA(-phi, nx, xi.x), ADF_FMA(-phi, ny, xi.y), ADF_FMA(-phi, nz, xi.z), 0.0f);
 }
 
@@ -1007,6 +1033,255 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
   }
 }
 
+// ------------------------------------------------------------------------------------------- box-shape walls
+constexpr float COS_SAME = 0.85f;  // boundary_slots.py:9: walls whose normals agree this much face the same way
+
+// newton geometry/kernels.py:310-370 (sdf_box, sdf_box_grad): signed distance of the axis-aligned box of half extents
+// h.xyz at box-frame point (x, y, z), and its outward unit gradient.
+__device__ __forceinline__ float box_sdf(float x, float y, float z, const float4& h) {
+  const float qx = fabsf(x) - h.x, qy = fabsf(y) - h.y, qz = fabsf(z) - h.z;
+  const float ex = maxr(qx, 0.0f), ey = maxr(qy, 0.0f), ez = maxr(qz, 0.0f);
+  return __fsqrt_rn(dot_plain(ex, ey, ez, ex, ey, ez)) + minr(maxr(qx, maxr(qy, qz)), 0.0f);
+}
+
+__device__ __forceinline__ void normalized3(float& x, float& y, float& z) {
+  const float l = __fsqrt_rn(dot_plain(x, y, z, x, y, z));
+  if (l > 0.0f) {
+    x = x / l;
+    y = y / l;
+    z = z / l;
+  } else {
+    x = y = z = 0.0f;
+  }
+}
+
+__device__ __forceinline__ void box_grad(float x, float y, float z, const float4& h, float& gx, float& gy, float& gz) {
+  const float qx = fabsf(x) - h.x, qy = fabsf(y) - h.y, qz = fabsf(z) - h.z;
+  if (qx > 0.0f || qy > 0.0f || qz > 0.0f) {  // outside: towards the closest point
+    gx = x - minr(maxr(x, -h.x), h.x);
+    gy = y - minr(maxr(y, -h.y), h.y);
+    gz = z - minr(maxr(z, -h.z), h.z);
+    normalized3(gx, gy, gz);
+    return;
+  }
+  const float sx = x < 0.0f ? -1.0f : 1.0f, sy = y < 0.0f ? -1.0f : 1.0f, sz = z < 0.0f ? -1.0f : 1.0f;
+  gx = gy = gz = 0.0f;
+  if ((qx > qy && qx > qz) || (qy == 0.0f && qz == 0.0f)) gx = sx;
+  else if ((qy > qx && qy > qz) || (qx == 0.0f && qz == 0.0f)) gy = sy;
+  else gz = sz;
+}
+
+// The box's outward unit normal at box-frame point (x, y, z): its SDF gradient, normalised again as the reference's
+// slot code does (boundary.py:226-231).
+__device__ __forceinline__ void box_normal(float x, float y, float z, const float4& h, float& nx, float& ny, float& nz) {
+  box_grad(x, y, z, h, nx, ny, nz);
+  normalized3(nx, ny, nz);
+}
+
+// boundary_slots.py:13-37: (sh, phi) into a phi-ascending row of n_ slots; the slot used, or -1
+__device__ __forceinline__ int slot_insert(int (&shp)[4], float (&ph)[4], int n_, int sh, float phi) {
+  int pos = n_, k = n_ - 1;
+  while (k >= 0) {
+    if (ph[k] <= phi) break;
+    pos = k;
+    --k;
+  }
+  if (pos >= 4) return -1;
+  for (k = n_ >= 4 ? 3 : n_; k > pos; --k) {
+    shp[k] = shp[k - 1];
+    ph[k] = ph[k - 1];
+  }
+  shp[pos] = sh;
+  ph[pos] = phi;
+  return pos;
+}
+
+// boundary_slots.py:59-102: a wall (sh, phi, normal nrm) into the row; a full row drops the farthest same-facing
+// duplicate (cos > COS_SAME) among its four walls and the new one, never one nearer than `near`, and when there is
+// none the farthest of the five. nr holds the slots' normals. 1 if the wall was kept.
+__device__ __forceinline__ int shape_insert(int (&shp)[4], float (&ph)[4], float3 (&nr)[4], int n_, int sh, float phi,
+                                            float3 nrm, float near) {
+  if (n_ < 4) {
+    const int r = slot_insert(shp, ph, n_, sh, phi);
+    if (r < 0) return 0;
+    for (int k = n_; k > r; --k) nr[k] = nr[k - 1];
+    nr[r] = nrm;
+    return 1;
+  }
+  auto dot3 = [](const float3& a, const float3& b) { return dot_plain(a.x, a.y, a.z, b.x, b.y, b.z); };
+  int ev = -1;
+  float ev_phi = -1.0f;
+  for (int m = 0; m < 4; ++m)
+    if (phi >= near && ph[m] <= phi && dot3(nr[m], nrm) > COS_SAME) {
+      ev = 4;
+      ev_phi = phi;
+    }
+  for (int k = 0; k < 4; ++k) {
+    const float pk = ph[k];
+    int dup = 0;
+    for (int m = 0; m < 4; ++m)
+      if (m != k && ph[m] <= pk && dot3(nr[m], nr[k]) > COS_SAME) dup = 1;
+    if (phi <= pk && dot3(nrm, nr[k]) > COS_SAME) dup = 1;
+    if (dup == 1 && pk >= near && pk > ev_phi) {
+      ev = k;
+      ev_phi = pk;
+    }
+  }
+  if (ev < 0 && phi < ph[3]) ev = 3;
+  if (ev < 0 || ev == 4) return 0;
+  for (int k = ev; k < 3; ++k) {
+    shp[k] = shp[k + 1];
+    ph[k] = ph[k + 1];
+    nr[k] = nr[k + 1];
+  }
+  int pos = 3;
+  while (pos > 0 && ph[pos - 1] > phi) {
+    shp[pos] = shp[pos - 1];
+    ph[pos] = ph[pos - 1];
+    nr[pos] = nr[pos - 1];
+    --pos;
+  }
+  shp[pos] = sh;
+  ph[pos] = phi;
+  nr[pos] = nrm;
+  return 1;
+}
+
+// boundary.py:190-238 (find), 254-334 (fill) and 336-396 (combine), after k_wall_slots, when the model has box walls:
+// every liquid particle's slots from its world's boxes within reach (in the world's shape order) and the particle
+// wall's slot k_wall_slots left in slot 0, nearest first; each box's slot filled from its SDF (the box-frame
+// start-of-step plane kept for the projection), then overlapping walls combined by inclusion-exclusion (Psi as
+// filled, gradients as rewritten slot by slot). Empty slots are zero with wall id -1.
+__global__ void __launch_bounds__(BLOCK) k_shape_slots(DevP P) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const int w = P.world_s[p];
+  const float4 xi = P.pos[p];
+  const int S = P.n_shapes;
+  const float h = P.kc.h, near = 0.1f * h;
+  const float4 g0 = P.slot_g[p], vb0 = P.slot_vb[p], n0 = P.slot_n[p], xb0 = P.slot_xb[p];
+  int shp[4] = {-1, -1, -1, -1};
+  float ph[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  float3 nr[4];
+  int ns = 0;
+  for (int c = P.sh_start[w]; c < P.sh_start[w + 1]; ++c) {
+    const int sh = P.sh_ids[c];
+    const float4 cp = P.sh_pos[sh];
+    const float lx = xi.x - cp.x, ly = xi.y - cp.y, lz = xi.z - cp.z;
+    if (__fsqrt_rn(dot_plain(lx, ly, lz, lx, ly, lz)) > cp.w + h) continue;
+    const float4 hx = P.sh_half[sh];
+    const float phi = box_sdf(lx, ly, lz, hx);
+    if (phi < P.reach && phi + P.wall_offset < h) {
+      float nx, ny, nz;
+      box_normal(lx, ly, lz, hx, nx, ny, nz);
+      if (shape_insert(shp, ph, nr, ns, sh, phi, make_float3(nx, ny, nz), near) > 0 && ns < 4) ++ns;
+    }
+  }
+  if (g0.w >= 0.0f && slot_insert(shp, ph, ns, S, vb0.w) >= 0 && ns < 4) ++ns;
+  float4 sg[4], sv[4], sn[4], sx[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    sg[k] = sv[k] = sx[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    sn[k] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+    if (k >= ns) continue;
+    const int sh = shp[k];
+    if (sh == S) {
+      sg[k] = g0;
+      sv[k] = vb0;
+      sn[k] = n0;
+      sx[k] = xb0;
+    } else {
+      const float4 cp = P.sh_pos[sh], hx = P.sh_half[sh];
+      const float lx = xi.x - cp.x, ly = xi.y - cp.y, lz = xi.z - cp.z;
+      const float phi = box_sdf(lx, ly, lz, hx);
+      float nx, ny, nz, psi, dpsi;
+      box_normal(lx, ly, lz, hx, nx, ny, nz);
+      wall_volume(P, phi, psi, dpsi);
+      sg[k] = make_float4(dpsi * nx, dpsi * ny, dpsi * nz, psi);
+      sv[k] = make_float4(0.0f, 0.0f, 0.0f, phi);
+      sn[k] = make_float4(nx, ny, nz, __int_as_float(sh));
+      sx[k] = make_float4(ADF_FMA(-phi, nx, lx), ADF_FMA(-phi, ny, ly), ADF_FMA(-phi, nz, lz), 0.0f);
+    }
+  }
+  if (ns > 1) {
+    float ps[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ps[k] = sg[k].w;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      if (b >= ns) break;
+      const float gbx = sg[b].x, gby = sg[b].y, gbz = sg[b].z;
+      float ob = 0.0f, sb = 0.0f;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (c >= ns) break;
+        if (c == b) continue;
+        const float gcx = sg[c].x, gcy = sg[c].y, gcz = sg[c].z;
+        const float lb = __fsqrt_rn(dot_plain(gbx, gby, gbz, gbx, gby, gbz));
+        const float lc = __fsqrt_rn(dot_plain(gcx, gcy, gcz, gcx, gcy, gcz));
+        float cbc = 0.0f;
+        if (lb > 0.0f && lc > 0.0f) cbc = minr(maxr(dot_plain(gbx, gby, gbz, gcx, gcy, gcz) / (lb * lc), -1.0f), 1.0f);
+        ob = ob + (1.0f - fabsf(cbc)) * ps[c];
+        if (cbc > 0.0f && (ps[c] > ps[b] || (ps[c] == ps[b] && c < b))) sb = sb + cbc;
+      }
+      ob = minr(ob, 1.0f);
+      sg[b].w = ps[b] * maxr((1.0f - 0.5f * ob) - sb, 0.0f);
+      const float f = maxr((1.0f - ob) - sb, 0.0f);
+      sg[b].x = gbx * f;
+      sg[b].y = gby * f;
+      sg[b].z = gbz * f;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const size_t o = slot_at(P, k, p);
+    P.slot_g[o] = sg[k];
+    P.slot_vb[o] = sv[k];
+    P.slot_n[o] = sn[k];
+    P.slot_xb[o] = sx[k];
+  }
+  P.slot_cnt[p] = (int8_t)ns;
+}
+
+// integrate.py:75-95 (box_span) and 98-126 (path_entry) for a static box of half extents h: the last outside parameter
+// of the box-frame path o -> e before it first enters the box, by the exact slab test; 2 when the path stays outside or
+// starts inside.
+__device__ __forceinline__ float box_entry(const float4& h, float ox, float oy, float oz, float ex, float ey, float ez) {
+  if (box_sdf(ox, oy, oz, h) < 0.0f) return 2.0f;
+  float lo = -1.0e30f, hi = 1.0e30f;
+  const float d[3] = {ex - ox, ey - oy, ez - oz}, o[3] = {ox, oy, oz}, hh[3] = {h.x, h.y, h.z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (fabsf(d[a]) > 0.0f) {
+      const float ta = (-hh[a] - o[a]) / d[a], tb = (hh[a] - o[a]) / d[a];
+      lo = maxr(lo, minr(ta, tb));
+      hi = minr(hi, maxr(ta, tb));
+    } else if (fabsf(o[a]) > hh[a]) {
+      lo = 2.0e30f;
+    }
+  }
+  if (lo <= hi && lo <= 1.0f && hi >= 0.0f) return maxr(lo, 0.0f);
+  return 2.0f;
+}
+
+// integrate.py:192-205: Coulomb friction of a projection onto box sh (Config.wall_friction), after the inward speed
+// -vn went: the tangential velocity relative to the wall (velocity b) loses up to mu (-vn), never reversing.
+__device__ __forceinline__ void wall_friction(const DevP& P, float& vx, float& vy, float& vz, float bx, float by,
+                                              float bz, float nx, float ny, float nz, float vn, int sh) {
+  if (!P.wall_friction) return;
+  const float mu = P.sh_half[sh].w;
+  if (mu <= 0.0f) return;
+  const float ux = vx - bx, uy = vy - by, uz = vz - bz;
+  const float un = dotf(ux, uy, uz, nx, ny, nz);
+  const float tx = ADF_FMA(-un, nx, ux), ty = ADF_FMA(-un, ny, uy), tz = ADF_FMA(-un, nz, uz);
+  const float lt = __fsqrt_rn(dot_plain(tx, ty, tz, tx, ty, tz));
+  if (lt <= 0.0f) return;
+  const float f = minr(1.0f, (mu * (-vn)) / lt);
+  vx = ADF_FMA(-f, tx, vx);
+  vy = ADF_FMA(-f, ty, vy);
+  vz = ADF_FMA(-f, tz, vz);
+}
+
 // Neighbour loops read their rows in batches of NB: the NB row entries first, then the NB gathers they address,
 // then the arithmetic in ascending row order, so the loads of a batch overlap instead of forming one dependent
 // chain per neighbour. Entries past the row's end address the particle itself (a harmless load) and are skipped.
@@ -1075,15 +1350,19 @@ __global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
       sq = ADF_FMA(bi * a, (F * F) * r2, sq);
     }
   }
-  float psi = 0.0f;
-  float4 sg = P.slot_g[p];
-  if (sg.w >= 0.0f) {
-    psi = sg.w;
+  float psi = 0.0f, lam = 0.0f;  // boundary slots, nearest first; lam: the opposing-wall compliance
+  const int ns = slot_count(P, p);
+  for (int b = 0; b < ns; ++b) {
+    const float4 sg = P.slot_g[slot_at(P, b, p)];
+    psi = psi + sg.w;
     Gx = Gx + sg.x;
     Gy = Gy + sg.y;
     Gz = Gz + sg.z;
+    for (int c = b + 1; c < ns; ++c) {
+      const float4 gc = P.slot_g[slot_at(P, c, p)];
+      lam = lam + maxr(-2.0f * dot_plain(sg.x, sg.y, sg.z, gc.x, gc.y, gc.z), 0.0f);
+    }
   }
-  float lam = 0.0f;
   float tot = (dotf(Gx, Gy, Gz, Gx, Gy, Gz) + sq) + lam;
   lam = lam + maxr(P.tot_min - tot, 0.0f);
   tot = maxr(tot, P.tot_min);
@@ -1123,9 +1402,10 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
       rate = ADF_FMA(aF, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, rx, ry, rz), rate);
     }
   }
-  float4 sg = P.slot_g[p];
-  if (sg.w >= 0.0f) {
-    float4 vb = P.slot_vb[p];
+  const int ns = slot_count(P, p);
+  for (int b = 0; b < ns; ++b) {
+    const size_t o = slot_at(P, b, p);
+    const float4 sg = P.slot_g[o], vb = P.slot_vb[o];
     rate = rate + dotf(vi.x - vb.x, vi.y - vb.y, vi.z - vb.z, sg.x, sg.y, sg.z);
   }
   const float dt = P.dt;
@@ -1160,7 +1440,8 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   if (P.feat_on) {  // warm-start network features (their order is documented in solvers/sph/warmstart.py)
     const float ratio = P.ratio[p], al = P.alpha[p], kvp = P.kv_s[p], kdp = P.kd_s[p];
     const float drate = dt * rate;
-    const bool on = sg.w >= 0.0f;
+    const bool on = ns > 0;  // the nearest wall's slot
+    const float4 sg = P.slot_g[p];
     const float phi = on ? P.slot_vb[p].w : P.kc.h;
     const float4 f0 = make_float4(ratio - 1.0f, P.neff[p] / P.n_full, drate, kvp);
     const float4 f1 = make_float4(kdp, al, __fsqrt_rn(dotf(vi.x, vi.y, vi.z, vi.x, vi.y, vi.z)), phi);
@@ -1360,9 +1641,10 @@ __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, 
       az = ADF_FMA(-cF, rz, az);
     }
   }
-  float4 sg = P.slot_g[p];
-  if (sg.w >= 0.0f) {
-    float kk = P.kappa[p];
+  const int ns = slot_count(P, p);
+  for (int b = 0; b < ns; ++b) {
+    const float4 sg = P.slot_g[slot_at(P, b, p)];
+    const float kk = P.kappa[p];
     ax = ADF_FMA(-kk, sg.x, ax);
     ay = ADF_FMA(-kk, sg.y, ay);
     az = ADF_FMA(-kk, sg.z, az);
@@ -1407,8 +1689,11 @@ __device__ __forceinline__ float accel_divergence(const DevP& P, int p, float in
       ar = ADF_FMA(aF, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz), ar);
     }
   }
-  float4 sg = P.slot_g[p];
-  if (sg.w >= 0.0f) ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
+  const int ns = slot_count(P, p);
+  for (int b = 0; b < ns; ++b) {
+    const float4 sg = P.slot_g[slot_at(P, b, p)];
+    ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
+  }
   return ar;
 }
 
@@ -1545,8 +1830,9 @@ __device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, float4
       }
     }
   }
-  const float4 sg = Q.slot_g[p];
-  if (sg.w >= 0.0f) {
+  const int ns = slot_count(Q, p);
+  for (int b = 0; b < ns; ++b) {
+    const float4 sg = Q.slot_g[slot_at(Q, b, p)];
     const float kk = Q.kappa[p];
     ax = ADF_FMA(-kk, sg.x, ax);
     ay = ADF_FMA(-kk, sg.y, ay);
@@ -1583,8 +1869,11 @@ __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, flo
       }
     }
   }
-  const float4 sg = P.slot_g[p];
-  if (sg.w >= 0.0f) ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
+  const int ns = slot_count(P, p);
+  for (int b = 0; b < ns; ++b) {
+    const float4 sg = P.slot_g[slot_at(P, b, p)];
+    ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
+  }
   return ar;
 }
 
@@ -1996,20 +2285,37 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
   const float dt = P.dt;
   float4 vi = P.vel[p];
   float kap = P.kappa[p];
-  float4 sg = P.slot_g[p];
-  if (P.cnt[p] == 0 && kap > 0.0f && sg.w >= 0.0f) {
-    float ps = sg.w;
-    float4 vbs = P.slot_vb[p];
-    float vbx = ps * vbs.x, vby = ps * vbs.y, vbz = ps * vbs.z;
-    float g = __fsqrt_rn(dot_plain(sg.x, sg.y, sg.z, sg.x, sg.y, sg.z));
-    if (g > 0.0f) {
-      if (ps > 0.0f) {
-        vbx = vbx / ps;
-        vby = vby / ps;
-        vbz = vbz / ps;
+  const int ns = slot_count(P, p);
+  const bool lone = P.cnt[p] == 0 && kap > 0.0f && ns > 0;
+  // the walls' summed gradient, the Psi-weighted wall velocity, the Psi sum and the largest-Psi slot
+  float Gx = 0.0f, Gy = 0.0f, Gz = 0.0f, vbx = 0.0f, vby = 0.0f, vbz = 0.0f, ps = 0.0f, pbest = 0.0f;
+  int best = -1;
+  if (lone) {
+    for (int b = 0; b < ns; ++b) {
+      const size_t o = slot_at(P, b, p);
+      const float4 sg = P.slot_g[o], vbs = P.slot_vb[o];
+      Gx = Gx + sg.x;
+      Gy = Gy + sg.y;
+      Gz = Gz + sg.z;
+      vbx = ADF_FMA(sg.w, vbs.x, vbx);
+      vby = ADF_FMA(sg.w, vbs.y, vby);
+      vbz = ADF_FMA(sg.w, vbs.z, vbz);
+      ps = ps + sg.w;
+      if (sg.w > pbest) {
+        pbest = sg.w;
+        best = b;
       }
-      float nx = -sg.x / g, ny = -sg.y / g, nz = -sg.z / g;
-      float u = dotf(vi.x - vbx, vi.y - vby, vi.z - vbz, nx, ny, nz);
+    }
+    const float g = __fsqrt_rn(dot_plain(Gx, Gy, Gz, Gx, Gy, Gz));
+    if (g > 0.0f) {
+      float ux = vbx, uy = vby, uz = vbz;
+      if (ps > 0.0f) {
+        ux = ux / ps;
+        uy = uy / ps;
+        uz = uz / ps;
+      }
+      const float nx = -Gx / g, ny = -Gy / g, nz = -Gz / g;
+      const float u = dotf(vi.x - ux, vi.y - uy, vi.z - uz, nx, ny, nz);
       kap = minr(kap, maxr(P.v_sep - u, 0.0f) / (dt * g));
       P.kappa[p] = kap;
       P.kr[p] = kap / vi.w;
@@ -2018,7 +2324,29 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
   float ax, ay, az;
   pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
   P.acc[p] = make_float4(ax, ay, az, 0.0f);
-  P.vel[p] = make_float4(ADF_FMA(dt, ax, vi.x), ADF_FMA(dt, ay, vi.y), ADF_FMA(dt, az, vi.z), vi.w);
+  float vx = ADF_FMA(dt, ax, vi.x), vy = ADF_FMA(dt, ay, vi.y), vz = ADF_FMA(dt, az, vi.z);
+  // pressure.py:417-458: Coulomb friction of a lone particle on its walls after the update: the walls' push
+  // dv_n = dt k |G| takes up to mu dv_n of its tangential speed relative to them, never reversing it; mu is that of
+  // the wall in its largest-Psi slot (a particle wall has none)
+  if (lone && P.wall_friction && P.n_shapes > 0 && kap > 0.0f && best >= 0) {
+    const float g = __fsqrt_rn(dot_plain(Gx, Gy, Gz, Gx, Gy, Gz));
+    const int sh = P.slot_cap > 1 ? __float_as_int(P.slot_n[slot_at(P, best, p)].w) : P.n_shapes;
+    if (g > 0.0f && ps > 0.0f && sh >= 0 && sh < P.n_shapes && P.sh_half[sh].w > 0.0f) {
+      const float mu = P.sh_half[sh].w;
+      const float nx = -Gx / g, ny = -Gy / g, nz = -Gz / g;
+      const float ux = vx - vbx / ps, uy = vy - vby / ps, uz = vz - vbz / ps;
+      const float un = dotf(ux, uy, uz, nx, ny, nz);
+      const float tx = ADF_FMA(-un, nx, ux), ty = ADF_FMA(-un, ny, uy), tz = ADF_FMA(-un, nz, uz);
+      const float lt = __fsqrt_rn(dot_plain(tx, ty, tz, tx, ty, tz));
+      if (lt > 0.0f) {
+        const float f = minr(1.0f, (((mu * dt) * kap) * g) / lt);
+        vx = ADF_FMA(-f, tx, vx);
+        vy = ADF_FMA(-f, ty, vy);
+        vz = ADF_FMA(-f, tz, vz);
+      }
+    }
+  }
+  P.vel[p] = make_float4(vx, vy, vz, vi.w);
   if (P.mode == 0) P.kv_s[p] = kap * dt;
   else P.kd_s[p] = (kap * dt) * dt;
 }
@@ -2087,14 +2415,126 @@ __global__ void __launch_bounds__(BLOCK, 3) k_xsph(DevP P) {
 }
 
 // ------------------------------------------------------------------------------------------------ finish
-// integrate.py:181-185 advection, particle_walls.py:131-135 wall advance, integrate.py:212-309 projection out of the
-// particle wall's advected slot plane (no SDF shapes: the sweep finds none), emitters.py:134-164 sinks and escape
-// box, integrate.py:312-326 speed; results written back to the caller's order.
+// integrate.py:181-185 advection, particle_walls.py:131-135 wall advance, integrate.py:212-309 sweep and projection
+// (finish_walls with box walls; else out of the particle wall's advected slot plane), emitters.py:134-164 sinks and
+// escape box, integrate.py:312-326 speed; results written back to the caller's order.
 __device__ __forceinline__ bool in_box(const Sink& s, float x, float y, float z) {
   float inv[4] = {-s.xform[3], -s.xform[4], -s.xform[5], s.xform[6]};
   float lx, ly, lz;
   quat_rotate(inv, x - s.xform[0], y - s.xform[1], z - s.xform[2], lx, ly, lz);
   return fabsf(lx) <= s.half[0] && fabsf(ly) <= s.half[1] && fabsf(lz) <= s.half[2];
+}
+
+// integrate.py:212-309 with box walls: a liquid particle that moved further than the sweep length is swept along its
+// path against its world's boxes (the first box entered, the particle put on its surface plus the skin, the inward
+// speed removed with friction); then its slots' walls push it out in up to PROJECT_PASSES passes: the particle wall
+// onto its start plane advanced with the wall, a box through its SDF at the new place, onto its start-of-step tangent
+// plane when that holds it.
+__device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float dt, float& x, float& y, float& z,
+                                             float& vx, float& vy, float& vz) {
+  int moved = 0;
+  const int c0 = P.sh_start[w], c1 = P.sh_start[w + 1];
+  const float stx = dt * vx, sty = dt * vy, stz = dt * vz;
+  if (c1 > c0 && __fsqrt_rn(dot_plain(stx, sty, stz, stx, sty, stz)) > P.sweep_len) {
+    const float x0 = x - stx, y0 = y - sty, z0 = z - stz;
+    const float spx = x - x0, spy = y - y0, spz = z - z0;
+    const float reach = __fsqrt_rn(dot_plain(spx, spy, spz, spx, spy, spz)) + P.prad;
+    float best = 2.0f, lhx = 0.0f, lhy = 0.0f, lhz = 0.0f;
+    int hit = -1;
+    for (int c = c0; c < c1; ++c) {
+      const int sh = P.sh_ids[c];
+      const float4 cp = P.sh_pos[sh];
+      const float ox = x0 - cp.x, oy = y0 - cp.y, oz = z0 - cp.z;
+      if (!(__fsqrt_rn(dot_plain(ox, oy, oz, ox, oy, oz)) <= cp.w + reach)) continue;
+      const float ex = x - cp.x, ey = y - cp.y, ez = z - cp.z;
+      const float t = box_entry(P.sh_half[sh], ox, oy, oz, ex, ey, ez);
+      if (t < best) {
+        best = t;
+        hit = sh;
+        lhx = ADF_FMA(t, ex - ox, ox);
+        lhy = ADF_FMA(t, ey - oy, oy);
+        lhz = ADF_FMA(t, ez - oz, oz);
+      }
+    }
+    if (hit >= 0) {
+      const float4 cp = P.sh_pos[hit], hx = P.sh_half[hit];
+      const float phi = box_sdf(lhx, lhy, lhz, hx);
+      float nx, ny, nz;
+      box_normal(lhx, lhy, lhz, hx, nx, ny, nz);
+      const float push = maxr(P.eps - phi, 0.0f);
+      x = ADF_FMA(push, nx, lhx + cp.x);
+      y = ADF_FMA(push, ny, lhy + cp.y);
+      z = ADF_FMA(push, nz, lhz + cp.z);
+      const float vn = dotf(vx, vy, vz, nx, ny, nz);
+      if (vn < 0.0f) {
+        vx = ADF_FMA(-vn, nx, vx);
+        vy = ADF_FMA(-vn, ny, vy);
+        vz = ADF_FMA(-vn, nz, vz);
+        wall_friction(P, vx, vy, vz, 0.0f, 0.0f, 0.0f, nx, ny, nz, vn, hit);
+      }
+      moved = 1;
+      atomicAdd(&P.swept[w], 1);
+    }
+  }
+  const int ns = slot_count(P, p);
+  int busy = 1;
+  for (int pass = 0; pass < PROJECT_PASSES && busy; ++pass) {
+    busy = 0;
+    for (int b = 0; b < ns; ++b) {
+      const size_t o = slot_at(P, b, p);
+      const float4 nn = P.slot_n[o], vb = P.slot_vb[o], xb = P.slot_xb[o];
+      const int sh = __float_as_int(nn.w);
+      if (sh == P.n_shapes) {  // the particle wall's plane at its end-of-step place
+        const float px = ADF_FMA(dt, vb.x, xb.x), py = ADF_FMA(dt, vb.y, xb.y), pz = ADF_FMA(dt, vb.z, xb.z);
+        const float d = dotf(x - px, y - py, z - pz, nn.x, nn.y, nn.z);
+        if (d < P.eps) {
+          const float push = P.eps - d;
+          x = ADF_FMA(push, nn.x, x);
+          y = ADF_FMA(push, nn.y, y);
+          z = ADF_FMA(push, nn.z, z);
+          const float vn = dotf(vx - vb.x, vy - vb.y, vz - vb.z, nn.x, nn.y, nn.z);
+          if (vn < 0.0f) {
+            vx = ADF_FMA(-vn, nn.x, vx);
+            vy = ADF_FMA(-vn, nn.y, vy);
+            vz = ADF_FMA(-vn, nn.z, vz);
+          }
+          moved = busy = 1;
+        }
+      } else if (sh >= 0) {  // a static box: its SDF at the new place, its start plane when that holds it
+        const float4 cp = P.sh_pos[sh], hx = P.sh_half[sh];
+        const float lx = x - cp.x, ly = y - cp.y, lz = z - cp.z;
+        const float phi = box_sdf(lx, ly, lz, hx);
+        if (phi < P.eps) {
+          float nx, ny, nz;
+          box_normal(lx, ly, lz, hx, nx, ny, nz);
+          float push = P.eps - phi;
+          if (vb.w >= 0.0f) {
+            const float push_s = P.eps - dotf(nn.x, nn.y, nn.z, x - (xb.x + cp.x), y - (xb.y + cp.y), z - (xb.z + cp.z));
+            if (push_s > 0.0f) {
+              nx = nn.x;
+              ny = nn.y;
+              nz = nn.z;
+              push = push_s;
+            }
+          }
+          if (push > 0.0f) {
+            x = ADF_FMA(push, nx, x);
+            y = ADF_FMA(push, ny, y);
+            z = ADF_FMA(push, nz, z);
+            const float vn = dotf(vx, vy, vz, nx, ny, nz);
+            if (vn < 0.0f) {
+              vx = ADF_FMA(-vn, nx, vx);
+              vy = ADF_FMA(-vn, ny, vy);
+              vz = ADF_FMA(-vn, nz, vz);
+              wall_friction(P, vx, vy, vz, 0.0f, 0.0f, 0.0f, nx, ny, nz, vn, sh);
+            }
+            moved = busy = 1;
+          }
+        }
+      }
+    }
+  }
+  if (moved) atomicAdd(&P.projected[w], 1);
 }
 
 __global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
@@ -2114,8 +2554,9 @@ __global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
   }
   int w = P.world_s[p];
   float vx = vi.x, vy = vi.y, vz = vi.z;
-  float4 sg = P.slot_g[p];
-  if (sg.w >= 0.0f) {
+  if (P.slot_cap > 1) {
+    finish_walls(P, p, w, dt, x, y, z, vx, vy, vz);
+  } else if (P.slot_g[p].w >= 0.0f) {
     float4 nn = P.slot_n[p], vb = P.slot_vb[p], xb = P.slot_xb[p];
     float px = ADF_FMA(dt, vb.x, xb.x), py = ADF_FMA(dt, vb.y, xb.y), pz = ADF_FMA(dt, vb.z, xb.z);
     int moved = 0;
@@ -2302,6 +2743,17 @@ __global__ void k_count_entries(int n, const int* nfw, const int* cnt, long long
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd((unsigned long long*)out, (unsigned long long)c);
+}
+
+// Diagnostics: slot k's wall id (-1 empty; the particle wall's id is n_shapes) or, with k < 0, the number of slots in
+// use, of each liquid particle, written as floats at its caller index.
+__global__ void k_slot_info(DevP P, int k, float* out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nfw[0]) return;
+  const int ns = slot_count(P, p);
+  int v = ns;
+  if (k >= 0) v = k >= ns ? -1 : (P.slot_cap > 1 ? __float_as_int(P.slot_n[slot_at(P, k, p)].w) : P.n_shapes);
+  out[P.id_of[p]] = (float)v;
 }
 
 __global__ void k_reset(DevP P, const uint8_t* mask, const int32_t* flags0, const int8_t* phase0) {

@@ -9,8 +9,9 @@ library's sm_100a kernels; this module holds host logic only (validation, consta
 fallback: without a CUDA device or the library it raises.
 
 Scope of the CUDA path: cubic or Wendland kernel, projected preconditioned CG (the reference's default, krylov.py)
-or relaxed Jacobi pressure solves, XSPH, particle walls (boundary particles flagged PROXY), emitters, sinks and the
-escape box. Settings outside it are refused in the constructor (``DFSPHConfig.unsupported``); CG falls back to Jacobi
+or relaxed Jacobi pressure solves, XSPH, particle walls (boundary particles flagged PROXY), static axis-aligned box
+walls evaluated through their SDF (up to four wall slots per particle, projection and the sweep past fast steps, wall
+friction), emitters, sinks and the escape box. Settings outside it are refused in the constructor (``DFSPHConfig.unsupported``); CG falls back to Jacobi
 with a warning when particle masses or rest densities differ, as the reference does (solver.py:89-91), and the
 resting-jitter rule falls back to the base tolerance with a warning.
 """
@@ -209,8 +210,6 @@ class SolverDFSPH:
         from .shapes import shape_table
 
         self.shapes = shape_table(model)  # refuses shape walls this path does not evaluate
-        if self.shapes.count and len(self.shapes.ids):
-            raise ValueError("SolverDFSPH (B200 build): box-shape walls are not yet on this build's CUDA path")
         if n and isinstance(model.particle_mass, torch.Tensor) and not model.particle_mass.is_cuda:
             raise ValueError("SolverDFSPH: the model must live on a CUDA device (Model.finalize(device='cuda'))")
         self.device = model.particle_mass.device if isinstance(model.particle_mass, torch.Tensor) else \
@@ -230,6 +229,20 @@ class SolverDFSPH:
         md.phase = _ptr(ns.phase, torch.int8, n, "sph.phase")
         md.world = _ptr(model.particle_world, torch.int32, n, "particle_world")
         md.gravity = _ptr(model.gravity, torch.float32, None, "gravity")
+        tab = self.shapes  # static box walls (layout.py:207-246), kept alive for the create call
+        box = np.zeros((max(tab.count, 1), 8), np.float32)
+        if tab.count:
+            box[:, 0:3] = tab.xform[:, 0:3]
+            box[:, 3] = tab.radius
+            box[:, 4:7] = tab.scale
+            box[:, 7] = tab.mu
+        sh_start = np.ascontiguousarray(tab.start, np.int32)
+        sh_ids = np.ascontiguousarray(tab.ids if len(tab.ids) else np.zeros(1, np.int32), np.int32)
+        md.n_shapes = tab.count
+        md.shape_start = sh_start.ctypes.data_as(C.POINTER(C.c_int32))
+        md.shape_ids = sh_ids.ctypes.data_as(C.POINTER(C.c_int32))
+        md.shape_box = box.ctypes.data_as(C.POINTER(C.c_float))
+        md.sweep_len = min(0.5 * cfg.h, 0.5 * tab.thinnest)  # integrate.py:42-49
         handle = C.c_void_p()
         with torch.cuda.device(self.device):
             _lib.check(self._lib.adf_create(C.byref(self._params), C.byref(md), self.device.index or 0,
@@ -274,6 +287,7 @@ class SolverDFSPH:
         p.v_sep = cfg.contact_separation_speed
         p.relief_speed = cfg.compression_relief_speed or 0.0
         p.project_eps = hc.project_eps
+        p.wall_friction = int(bool(cfg.wall_friction))
         if cfg.world_bounds is not None:
             p.has_bounds = 1
             for a in range(3):
@@ -328,7 +342,7 @@ class SolverDFSPH:
                 "density_err_max": np.zeros(W, np.float32), "projected": np.zeros(W, np.int32),
                 "nonfinite": np.zeros(W, np.int32), "emitter_overflow": np.zeros(W, np.int32),
                 "density_tol": np.zeros(W, np.float32), "learned_divergence": np.zeros(W, np.int32),
-                "learned_density": np.zeros(W, np.int32)}
+                "learned_density": np.zeros(W, np.int32), "swept": np.zeros(W, np.int32)}
         r = _lib.Report(**{k: v.ctypes.data for k, v in arrs.items()})
         _lib.check(self._lib.adf_get_report(self._h, C.byref(r), self._stream()), "report")
         return {k: v[: self.world_count] for k, v in arrs.items()}
@@ -356,7 +370,7 @@ class SolverDFSPH:
         a = self._world_arrays()
         return {"density_err_max": a["density_err_max"].astype(np.float64), "projected": a["projected"],
                 "nonfinite": a["nonfinite"], "emitter_overflow": a["emitter_overflow"],
-                "swept": np.zeros(self.world_count, np.int32), "cavitating": np.zeros(self.world_count, np.int32),
+                "swept": a["swept"], "cavitating": np.zeros(self.world_count, np.int32),
                 "learned_divergence": a["learned_divergence"], "learned_density": a["learned_density"]}
 
     def mass_ledger(self) -> dict[str, np.ndarray]:
@@ -433,8 +447,9 @@ class SolverDFSPH:
         return out
 
     def debug_field(self, name: str) -> np.ndarray:
-        """A per-particle field of the last step in particle order (parity tests)."""
-        three = name in ("acc", "slot_g", "slot_vb", "slot_n")
+        """A per-particle field of the last step in particle order (parity tests); slot fields take ``:k`` for slot k
+        (include/alloy_dfsph.h adf_debug_field)."""
+        three = name.split(":")[0] in ("acc", "slot_g", "slot_vb", "slot_n")
         out = torch.zeros((self.n, 3) if three else self.n, dtype=torch.float32, device=self.device)
         _lib.check(self._lib.adf_debug_field(self._h, name.encode(), out.data_ptr(), self._stream()), "debug_field")
         return out.cpu().numpy()
@@ -590,9 +605,9 @@ class SolverDFSPH:
     # ------------------------------------------------------------------------------------------------ model
     def notify_model_changed(self, flags: int) -> None:
         """solver.py:343-351. The reference re-derives its body modes when body properties change and rebuilds its
-        shape table when shape properties change. This path has neither (the constructor refuses bodies and SDF
-        shapes; particle walls are particles), and every step reads the particle arrays, masses, rest densities and
-        gravity live from the model, so no flag leaves anything to rebuild."""
+        shape table when shape properties change. This path has no bodies, its box walls are static (the constructor
+        refuses moving or rotated shapes, and their table is fixed at construction), and every step reads the particle
+        arrays, masses, rest densities and gravity live from the model, so no flag leaves anything to rebuild."""
         int(flags)
 
     @staticmethod

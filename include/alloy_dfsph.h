@@ -57,6 +57,7 @@ typedef struct {
   int cg;                   /* pressure iteration: 1 projected preconditioned CG per world (krylov.py:77-318; the
                                caller sets it only for one particle mass and rest density, solver.py:89-91),
                                0 relaxed Jacobi */
+  int wall_friction;        /* Config.wall_friction: Coulomb friction of box walls on projected and lone particles */
 } adf_params;
 
 /* The model's particle arrays (Newton Model + sph:* attributes), bound once at creation. */
@@ -72,6 +73,14 @@ typedef struct {
   int8_t* phase;                 /* device [n] sph:phase (written likewise) */
   const int32_t* world;          /* device [n] particle_world */
   const float* gravity;          /* device [W][3] Model.gravity */
+  /* The liquid's static axis-aligned box walls (layout.py:207-246 shape_table; boundary.py:70-87 per world: the
+   * world's own shapes, then the global ones). n_shapes = 0: particle walls only, and the rest may be NULL. */
+  int n_shapes;                  /* S: size of the model's shape table (ids index it; the particle wall's id is S) */
+  const int32_t* shape_start;    /* host [W + 1]: world w's walls are shape_ids[shape_start[w] .. shape_start[w + 1]) */
+  const int32_t* shape_ids;      /* host [shape_start[W]] */
+  const float* shape_box;        /* host [S][8]: centre xyz, bounding radius, half extents xyz, Coulomb friction */
+  double sweep_len;              /* [m] a step longer than this is swept against the boxes: min(h, thinnest) / 2
+                                    (integrate.py:42-49) */
 } adf_model;
 
 /* Per-world host outputs of adf_get_report; any pointer may be NULL. SPHReport (types.py:11-28) and
@@ -94,6 +103,7 @@ typedef struct {
   float* density_tol;
   int32_t* learned_divergence; /* 1: the last step's divergence solve kept the learned start (adf_set_warm_model) */
   int32_t* learned_density;    /* the same for the density solve */
+  int32_t* swept;              /* particles swept onto a box wall past a fast step (integrate.py:212-250), cumulative */
 } adf_report;
 
 /* Message of this thread's last failed call ("" if none). */
@@ -253,7 +263,9 @@ int adf_neighbor_rows(adf_solver* solver, int32_t* rows, int32_t* count, void* s
 
 /* Diagnostics for parity tests: a per-particle float field of the last step in particle order (device [n] or
  * [n][3]): ratio alpha neff reg src kappa lower err slot_psi slot_phi pred_kv pred_kd (scalars; pred_*: the
- * warm-start network's predictions), acc slot_g slot_vb slot_n (vec3). */
+ * warm-start network's predictions), acc slot_g slot_vb slot_n (vec3). A slot field takes a ":k" suffix for slot k
+ * (0..3 with box walls, nearest first; 0 without a suffix). slot_shape:k gives slot k's wall id (-1 empty; the particle
+ * wall's id is n_shapes) and slot_count the slots in use, as floats, for liquid particles (0 elsewhere). */
 int adf_debug_field(adf_solver* solver, const char* name, float* out, void* stream);
 
 /* Per-world float64 sums and maxima of a float array in the solver's tree order (reduce.py:185-227); device
