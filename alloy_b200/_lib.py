@@ -22,7 +22,7 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_mlp_train_step", "adf_mlp_status", "adf_set_warm_model", "adf_set_feature_recording",
            "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs", "adf_add_emitters",
            "adf_prime", "adf_iteration_work", "adf_set_tuned_config", "adf_get_state_storage", "adf_port_take",
-           "adf_port_emit", "adf_energy", "adf_stable_dt")
+           "adf_port_emit", "adf_energy", "adf_stable_dt", "adf_skin_flags")
 TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph", "lists")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
@@ -40,7 +40,8 @@ class Params(C.Structure):
                 ("divergence_solve", C.c_int), ("two_sided", C.c_int), ("xsph_c", C.c_double),
                 ("capacity", C.c_int), ("v_sep", C.c_double), ("relief_speed", C.c_double),
                 ("project_eps", C.c_double), ("has_bounds", C.c_int), ("bounds_lo", C.c_double * 3),
-                ("bounds_hi", C.c_double * 3), ("cg", C.c_int), ("wall_friction", C.c_int)]
+                ("bounds_hi", C.c_double * 3), ("cg", C.c_int), ("wall_friction", C.c_int), ("skin", C.c_double),
+                ("skin_cap", C.c_int)]
 
 
 class ModelDesc(C.Structure):
@@ -132,6 +133,7 @@ def lib() -> C.CDLL:
     L.adf_port_emit.argtypes = [P, vp, vp, vp, vp, i, vp, vp]
     L.adf_energy.argtypes = [P, vp, vp, vp, vp, vp]
     L.adf_stable_dt.argtypes = [P, vp, C.c_double, C.c_double, C.c_double, vp, vp]
+    L.adf_skin_flags.argtypes = [P, vp, vp]
     for name in EXPORTS:
         if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches", "adf_mlp_destroy"):
             getattr(L, name).restype = C.c_int

@@ -15,6 +15,7 @@
 #include "dfsph_kernels.cuh"
 #include "dfsph_mlp.cuh"
 #include "dfsph_port.cuh"
+#include "dfsph_skin.cuh"
 
 using namespace adf;
 
@@ -379,6 +380,10 @@ void set_solve_params(adf_solver* s, DevP& P, int mode, double dt) {
 int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   const int n = s->n;
   prof_begin(s, 0, st);
+  if (P.skin_on) {  // which worlds rebuild their superset rows (dfsph_skin.cuh)
+    LAUNCH(s, k_skin_seed, blocks(std::max(s->W, 1)), BLOCK, st, P);
+    LAUNCH(s, k_skin_check, blocks(n), BLOCK, st, P);
+  }
   LAUNCH(s, k_classify, blocks(n), BLOCK, st, P);
   LAUNCH(s, k_scan_tiles, s->n_tiles, SCAN_THREADS, st, P.counts, s->n_keys, s->tile_sums);
   LAUNCH(s, k_scan_tile_sums, 1, SCAN_THREADS, st, s->tile_sums, s->n_tiles);
@@ -387,7 +392,11 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   LAUNCH(s, k_scatter, blocks(n), BLOCK, st, P);
   prof_end(s, st);
   prof_begin(s, 1, st);
-  if (s->K <= LU_ROW) {
+  if (P.skin_on) {
+    LAUNCH(s, k_skin_ref, blocks(n), BLOCK, st, P);
+    LAUNCH(s, k_skin_build, blocks(n, 128), 128, st, P);
+    LAUNCH(s, k_skin_filter, blocks(n), BLOCK, st, P);
+  } else if (s->K <= LU_ROW) {
     run_tk(s, TK_LISTS, st, P);
   } else {
     const size_t smem = sizeof(int) * (size_t)s->K * LS_THREADS;
@@ -741,6 +750,9 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     return fail(ADF_ERR_VALUE, "world_start out of range");
   if (m->n > 0 && (!m->mass || !m->rest_density || !m->radius || !m->flags || !m->phase || !m->world || !m->gravity))
     return fail(ADF_ERR_VALUE, "adf_create: a model array is null");
+  if (!(p.skin >= 0.0) || p.skin > p.h) return fail(ADF_ERR_VALUE, "skin must be in [0, h]");
+  if (p.skin > 0.0 && (p.skin_cap < 1 || p.skin_cap > 4096))
+    return fail(ADF_ERR_VALUE, "skin_cap must be in [1, 4096] when skin > 0");
   if (m->n_shapes < 0) return fail(ADF_ERR_VALUE, "adf_create: negative n_shapes");
   if (m->n_shapes > 0) {
     if (!m->shape_start || !m->shape_box) return fail(ADF_ERR_VALUE, "adf_create: shape_start and shape_box needed");
@@ -866,6 +878,23 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     rc |= s->alloc(&sh_half, (size_t)m->n_shapes);
   }
   rc |= s->alloc(&d.swept, W);
+  d.skin_on = p.skin > 0.0;
+  if (d.skin_on) {
+    d.sup_cap = p.skin_cap;
+    const double hs = p.h + p.skin;
+    int reach = 1;
+    for (const WorldGrid& g : s->grids) reach = std::max(reach, (int)std::floor(hs * (double)g.inv_cw * (1.0 + 1.0e-5)) + 1);
+    d.skin_reach = reach;
+    d.skin_r2 = (float)hs * (float)hs;
+    d.skin_half2 = (float)((0.49 * p.skin) * (0.49 * p.skin));
+    rc |= s->alloc(&d.sup, (size_t)d.sup_cap * n);
+    rc |= s->alloc(&d.sup_cnt, n);
+    rc |= s->alloc(&d.skin_slot, n);
+    rc |= s->alloc(&d.skin_qref, n);
+    rc |= s->alloc(&d.skin_gref, n);
+    rc |= s->alloc(&d.skin_flag, W);
+    rc |= s->alloc(&d.skin_force, W);
+  }
   rc |= s->alloc(&d.ratio, n);
   rc |= s->alloc(&d.alpha, n);
   rc |= s->alloc(&d.neff, n);
@@ -948,6 +977,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   }
   d.wall_vol = wall_vol;
   d.grid = grid;
+  d.skin_ws = s->ws_d;
   d.sh_start = sh_start;
   d.sh_ids = sh_ids;
   d.sh_pos = sh_pos;
@@ -978,6 +1008,14 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   }
   CKC(cudaMemcpy(world_chunk_start, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice));
   CKC(cudaMemcpy(s->ws_d, s->ws_host.data(), sizeof(int) * s->ws_host.size(), cudaMemcpyHostToDevice));
+  if (d.skin_on) {  // nothing built yet: every world builds its superset rows on the first step
+    std::vector<int> never(n, -2);
+    CKC(cudaMemcpy(d.skin_gref, never.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    CKC(cudaMemset(d.skin_slot, 0, sizeof(int) * n));
+    CKC(cudaMemset(d.sup_cnt, 0, sizeof(int) * n));
+    CKC(cudaMemset(d.skin_flag, 0, sizeof(int) * W));
+    CKC(cudaMemset(d.skin_force, 0, sizeof(int) * W));
+  }
   if (d.slot_cap > 1) {  // the box walls: per-world id lists, (centre, radius) and (half extents, mu) per shape
     std::vector<float4> bp(m->n_shapes), bh(m->n_shapes);
     for (int k = 0; k < m->n_shapes; ++k) {
@@ -1737,6 +1775,15 @@ int adf_debug_field(adf_solver* s, const char* name, float* out, void* stream) {
     return ADF_OK;
   }
   return fail(ADF_ERR_VALUE, std::string("adf_debug_field: unknown field ") + name);
+}
+
+int adf_skin_flags(adf_solver* s, int32_t* flags, void* stream) {
+  if (!s || !flags) return fail(ADF_ERR_VALUE, "adf_skin_flags: null argument");
+  if (!s->d.skin_on) return fail(ADF_ERR_STATE, "adf_skin_flags: the solver has no skin (params.skin = 0)");
+  CK(cudaSetDevice(s->device));
+  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  if (s->W > 0) CK(cudaMemcpy(flags, s->d.skin_flag, sizeof(int) * s->W, cudaMemcpyDeviceToHost));
+  return ADF_OK;
 }
 
 int adf_world_sum(adf_solver* s, const float* values, double* out_sum, float* out_max, void* stream) {

@@ -131,6 +131,20 @@ struct DevP {
   float prad;             // particle radius
   int wall_friction;      // Config.wall_friction
   int* swept;             // [W] particles swept onto a box this step
+  // Verlet-skin reuse of the rows (dfsph_skin.cuh; skin_on 0: rows built every step)
+  int skin_on;
+  int sup_cap;          // superset row capacity
+  int skin_reach;       // cells scanned on each side for radius h + s
+  float skin_r2;        // (h + s)^2
+  float skin_half2;     // (0.49 s)^2
+  int* sup;             // [sup_cap][n] superset rows (particle ids, ascending) by slot
+  int* sup_cnt;         // [n] by slot: entries, or -1 for a plain row written by this step's rebuild
+  int* skin_slot;       // [n] caller order: the particle's slot at its world's last build
+  float4* skin_qref;    // [n] caller order: position at its world's last build
+  int* skin_gref;       // [n] caller order: group at its world's last build (-2: never built)
+  int* skin_flag;       // [W] world rebuilt this step
+  int* skin_force;      // [W] world rebuilds next step (an overfull superset row)
+  const int* skin_ws;   // [W + 1] first particle index of each world
   float* ratio;
   float* alpha;
   float* neff;

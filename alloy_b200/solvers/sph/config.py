@@ -140,11 +140,24 @@ class DFSPHConfig:
             out.append(f"surface_tension {self.surface_tension!r}")
         if self.ambient_pressure is not None:
             out.append("ambient_pressure")
-        if self.reneighbor_skin:
-            out.append("reneighbor_skin")
         if self.kernel != "cubic" and self.kernel != "wendland_c2":
             out.append(f"kernel {self.kernel!r}")
         return out
+
+
+SKIN_FILL_MARGIN = 1.75  # superset row capacity / rest fill within h + s (neighbors_skin.py:152)
+
+
+def skin_capacity(h: float, spacing: float, skin: float) -> int:
+    """Superset row capacity of the Verlet skin (neighbors_skin.py:155-166): 1.75 x the neighbours of an interior
+    lattice particle within h + skin, at least 16. A fuller row is built plain for its step and its world rebuilds
+    the next step, so a small capacity costs reuse, never exactness."""
+    rad = (h + skin) / spacing
+    m = int(math.ceil(rad)) + 1
+    ax = np.arange(-m, m + 1, dtype=np.float64)
+    d2 = ax[:, None, None] ** 2 + ax[None, :, None] ** 2 + ax[None, None, :] ** 2
+    fill = int(np.count_nonzero(d2 < rad * rad)) - 1
+    return max(16, int(math.ceil(SKIN_FILL_MARGIN * fill)))
 
 
 def resolve_viscosity(cfg: DFSPHConfig, mu_max: float) -> str:

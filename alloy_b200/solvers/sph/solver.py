@@ -26,7 +26,8 @@ import numpy as np
 import torch
 
 from ... import _lib
-from .config import (PHASE_HELD, PHASE_SPARE, DFSPHConfig, host_constants, snap_down, stable_dt, uniform_layout)
+from .config import (PHASE_HELD, PHASE_SPARE, DFSPHConfig, host_constants, skin_capacity, snap_down, stable_dt,
+                     uniform_layout)
 from .model import ParticleFlags
 from .types import SPHReport
 
@@ -160,7 +161,8 @@ class SolverDFSPH:
         register_custom_attributes(builder)
 
     def __init__(self, model, config: DFSPHConfig | None = None, *, capacity_per_world: int | None = None,
-                 soft_particles=None, soft_half_thickness: float = 0.0, soft_inertia: bool = True):
+                 soft_particles=None, soft_half_thickness: float = 0.0, soft_inertia: bool = True,
+                 skin_rows: int | None = None):
         self.model = model
         self.config = cfg = config or DFSPHConfig()
         cfg.validate()
@@ -210,12 +212,17 @@ class SolverDFSPH:
         from .shapes import shape_table
 
         self.shapes = shape_table(model)  # refuses shape walls this path does not evaluate
+        if cfg.reneighbor_skin and n and np.any((_host(model.particle_flags) & int(ParticleFlags.PROXY)) != 0):
+            raise ValueError("SolverDFSPH: particle walls need the grid rebuilt every step (reneighbor_skin off)")
         if n and isinstance(model.particle_mass, torch.Tensor) and not model.particle_mass.is_cuda:
             raise ValueError("SolverDFSPH: the model must live on a CUDA device (Model.finalize(device='cuda'))")
         self.device = model.particle_mass.device if isinstance(model.particle_mass, torch.Tensor) else \
             torch.device("cuda", 0)
         self.hc = host_constants(cfg)
         self._params = self._make_params(cfg, self.hc)
+        if cfg.reneighbor_skin:  # Verlet-skin reuse (solver.py:130-133)
+            self._params.skin = float(cfg.reneighbor_skin) * self.hc.h
+            self._params.skin_cap = skin_rows or skin_capacity(self.hc.h, cfg.spacing, self._params.skin)
         self._params.cg = int(self.pressure_solver == "cg")
         q_host = np.ascontiguousarray(_host(model.particle_q), np.float32).reshape(-1) if n else np.zeros(0, np.float32)
         md = _lib.ModelDesc()
@@ -453,6 +460,15 @@ class SolverDFSPH:
         out = torch.zeros((self.n, 3) if three else self.n, dtype=torch.float32, device=self.device)
         _lib.check(self._lib.adf_debug_field(self._h, name.encode(), out.data_ptr(), self._stream()), "debug_field")
         return out.cpu().numpy()
+
+    def skin_flags(self) -> np.ndarray:
+        """Per-world rebuild flags of the last step's Verlet-skin update (neighbors_skin.py:206-208
+        ``rebuilt_worlds``); ValueError without ``reneighbor_skin``."""
+        if not self._params.skin:
+            raise ValueError("SolverDFSPH.skin_flags: reneighbor_skin is off")
+        out = np.zeros(max(self.world_count, 1), np.int32)
+        _lib.check(self._lib.adf_skin_flags(self._h, out.ctypes.data, self._stream()), "skin_flags")
+        return out[:self.world_count].astype(bool)
 
     def kernel_launches(self) -> int:
         return int(self._lib.adf_kernel_launches(self._h))

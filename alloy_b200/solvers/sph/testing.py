@@ -89,42 +89,49 @@ def large_dam_break(device="cpu", **kw) -> Scene:
 
 
 def water_column(nx: int = 6, ny: int = 6, nz: int = 20, *, worlds: int = 1, r: float = 1.0e-3, headroom: int = 8,
-                 dt: float = 1.25e-3, steps: int = 400, device="cpu", **cfg_kw) -> Scene:
-    """A resting column nx x ny x nz on the 2r lattice filling the floor of a box tank per world (the reference's
-    ``alloy.testing.sph.water_column``, alloy/testing/sph.py:49-73), with the tank made of one layer of boundary
-    particles instead of the reference's SDF box. Config: the reference's ``fast`` preset (projected CG, the
-    resting-jitter rule off, config.py:146-157); dt = dt_max."""
+                 dt: float = 1.25e-3, steps: int = 400, walls: str = "sdf", device="cpu", **cfg_kw) -> Scene:
+    """A resting column nx x ny x nz on the 2r lattice filling the floor of an open box tank per world (the
+    reference's ``alloy.testing.sph.water_column``, alloy/testing/sph.py:49-73): ``walls`` "sdf" the reference's tank
+    of box shapes h thick, "particles" one layer of boundary particles (closed top) on the same inner box. Config: the
+    reference's ``fast`` preset (projected CG, the resting-jitter rule off, config.py:146-157); dt = dt_max."""
     cfg = DFSPHConfig.fast(particle_radius=r, **cfg_kw)
     cfg.validate()
     s = cfg.spacing
     b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
     fluid = wall = 0
+    inner_hi = (nx * s, ny * s, (nz + headroom) * s)
     for _ in range(worlds):
         b.begin_world()
+        if walls == "sdf":
+            add_box_tank(b, (0.0, 0.0, 0.0), inner_hi, wall=cfg.h)
         fl = add_fluid_block(b, cfg, (0.0, 0.0, 0.0), (nx, ny, nz))
-        wl = add_particle_box(b, cfg, (0.0, 0.0, 0.0), (nx * s, ny * s, (nz + headroom) * s))
+        if walls != "sdf":
+            wall += len(add_particle_box(b, cfg, (0.0, 0.0, 0.0), inner_hi))
         b.end_world()
         fluid += len(fl)
-        wall += len(wl)
     return Scene(b.finalize(device), cfg, dt, steps, fluid, wall, name=f"water_column_{worlds}x{nx}x{ny}x{nz}")
 
 
 def tank_dam_break(width: int = 32, height: int = 30, depth: int = 32, tank: int = 96, *, r: float = 2.0e-3,
-                   steps: int = 400, device="cpu", **cfg_kw) -> Scene:
+                   steps: int = 400, walls: str = "sdf", device="cpu", **cfg_kw) -> Scene:
     """The reference harness's dam break (alloy/testing/sph.py:101-115): a width x depth x height lattice block
-    against the x_lo wall of a tank (tank x depth x (height + 10)) spacings, here a box of boundary particles. The
-    reference's default config (projected CG, CFL 0.2) with the resting-jitter rule off; dt is the CFL step at the
-    Ritter front speed 2 sqrt(g H), snapped down to 0.02 s / 2^j (test_speed_gpu.py:30-31)."""
+    against the x_lo wall of an open tank (tank x depth x (height + 10)) spacings, of box shapes h thick (``walls``
+    "sdf", the reference's) or one layer of boundary particles ("particles"). The reference's default config
+    (projected CG, CFL 0.2) with the resting-jitter rule off; dt is the CFL step at the Ritter front speed
+    2 sqrt(g H), snapped down to 0.02 s / 2^j (test_speed_gpu.py:30-31)."""
     cfg = DFSPHConfig(particle_radius=r, **{"rest_jitter_speed": None, **cfg_kw})
     cfg.validate()
     s = cfg.spacing
     dt = snap_down(stable_dt(cfg, 2.0 * (9.81 * height * s) ** 0.5), 0.02)
     b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+    inner_hi = (tank * s, depth * s, (height + 10) * s)
     b.begin_world()
+    if walls == "sdf":
+        add_box_tank(b, (0.0, 0.0, 0.0), inner_hi, wall=cfg.h)
     fl = add_fluid_block(b, cfg, (0.0, 0.0, 0.0), (width, depth, height))
-    wl = add_particle_box(b, cfg, (0.0, 0.0, 0.0), (tank * s, depth * s, (height + 10) * s))
+    nw = 0 if walls == "sdf" else len(add_particle_box(b, cfg, (0.0, 0.0, 0.0), inner_hi))
     b.end_world()
-    return Scene(b.finalize(device), cfg, dt, steps, len(fl), len(wl), name=f"tank_dam_break_{width}x{depth}x{height}")
+    return Scene(b.finalize(device), cfg, dt, steps, len(fl), nw, name=f"tank_dam_break_{width}x{depth}x{height}")
 
 
 def world_sizes(count: int, lo: int, hi: int, seed: int) -> np.ndarray:

@@ -58,6 +58,10 @@ typedef struct {
                                caller sets it only for one particle mass and rest density, solver.py:89-91),
                                0 relaxed Jacobi */
   int wall_friction;        /* Config.wall_friction: Coulomb friction of box walls on projected and lone particles */
+  double skin;              /* [m] Verlet skin s = reneighbor_skin x h (neighbors_skin.py); 0: rows built every step.
+                               Superset rows within h + s are reused per world until a particle of the world moves
+                               more than s / 2 or the world's liquid set changes; the rows equal a plain build's */
+  int skin_cap;             /* superset row capacity (neighbors_skin.py:155-166 skin_capacity) when skin > 0 */
 } adf_params;
 
 /* The model's particle arrays (Newton Model + sph:* attributes), bound once at creation. */
@@ -267,6 +271,10 @@ int adf_neighbor_rows(adf_solver* solver, int32_t* rows, int32_t* count, void* s
  * (0..3 with box walls, nearest first; 0 without a suffix). slot_shape:k gives slot k's wall id (-1 empty; the particle
  * wall's id is n_shapes) and slot_count the slots in use, as floats, for liquid particles (0 elsewhere). */
 int adf_debug_field(adf_solver* solver, const char* name, float* out, void* stream);
+
+/* Replaces SkinState.rebuilt_worlds (neighbors_skin.py:206-208): host [W], 1 where the last step (or density_ratio)
+ * rebuilt the world's superset rows; synchronises `stream`. ADF_ERR_STATE without a skin. */
+int adf_skin_flags(adf_solver* solver, int32_t* flags, void* stream);
 
 /* Per-world float64 sums and maxima of a float array in the solver's tree order (reduce.py:185-227); device
  * in/out; exported for the reducer's parity test. */

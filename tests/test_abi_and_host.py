@@ -153,7 +153,7 @@ def test_plugin_factory_contract():
 
 def test_speed_harness_scenes_follow_the_reference_harness():
     """The reference's own speed scenes (tests/solvers/sph/test_speed_gpu.py:24-39, alloy/testing/sph.py:49-115):
-    sizes, config and dt; the tanks are boundary-particle boxes on the same inner box."""
+    sizes, config and dt, in the reference's open tanks of box shapes h thick (build.py:113-137)."""
     from alloy_b200.solvers.sph.testing import tank_dam_break, water_column
 
     col = water_column(32, 32, 30, r=2.0e-3)
@@ -161,17 +161,20 @@ def test_speed_harness_scenes_follow_the_reference_harness():
     assert col.fluid_count == 30720 and col.model.world_count == 1
     assert cfg.pressure_solver == "cg" and cfg.cfl == 0.4 and cfg.rest_jitter_speed is None  # the fast preset
     assert col.dt == cfg.dt_max == 1.25e-3
-    q = col.model.host()["q"].reshape(-1, 3)
-    wall = col.model.host()["phase"] == -1
     s = cfg.spacing
-    assert np.isclose(q[wall][:, 2].max(), (30 + 8) * s + 0.5 * s)  # headroom of 8 layers, closed top
+    hs = col.model.host()
+    assert len(hs["shape_type"]) == 5 and not (hs["phase"] == -1).any()  # floor and four walls, open top
+    top = hs["shape_transform"][:, 2] + hs["shape_scale"][:, 2]
+    assert np.isclose(top.max(), (30 + 8) * s)  # headroom of 8 layers
+    assert np.isclose(hs["shape_scale"][:, 2].min(), 0.5 * cfg.h)  # the floor, h thick
     many = water_column(16, 16, 16, worlds=3, r=2.0e-3)
     assert many.fluid_count == 3 * 4096 and many.model.world_count == 3
     dam = tank_dam_break(32, 30, 32, 96, r=2.0e-3)
     assert dam.fluid_count == 30720 and dam.config.pressure_solver == "cg" and dam.config.cfl == 0.2
     assert dam.dt == C.snap_down(C.stable_dt(dam.config, 2.0 * (9.81 * 30 * s) ** 0.5), 0.02) == 0.02 / 64
-    qd = dam.model.host()["q"].reshape(-1, 3)
-    assert np.isclose(qd[dam.model.host()["phase"] == -1][:, 0].max(), 96 * s + 0.5 * s)
+    hd = dam.model.host()
+    inner_x = hd["shape_transform"][:, 0] - hd["shape_scale"][:, 0]
+    assert np.isclose(inner_x.max(), 96 * s)  # the x_hi wall's inner face
 
 
 def test_bench_reports_the_harness_figures():

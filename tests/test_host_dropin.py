@@ -57,3 +57,29 @@ def test_emit_object_checks_budget_and_radius():
         emit_object(b, _obj(N(kind="box", size=(0.02, 0.02, 0.02))), N(numbers={}))
     with pytest.raises(ValueError):
         emit_object(b, _obj(N(kind="plane", size=(1.0, 1.0, 0.0))), N(numbers={"particle_radius": 0.002}))
+
+
+def test_skin_capacity_is_the_padded_rest_fill():
+    """neighbors_skin.py:155-166: 1.75 x the lattice neighbours within h + s, at least 16 (counted here by brute
+    force over the lattice)."""
+    import itertools
+    import math
+
+    from alloy_b200.solvers.sph.config import skin_capacity
+
+    for h, sp, s in ((0.004, 0.002, 0.0004), (0.04, 0.02, 0.004), (0.01, 0.005, 0.005), (0.002, 0.002, 0.0)):
+        rad = (h + s) / sp
+        m = int(math.ceil(rad)) + 1
+        fill = sum(1 for x, y, z in itertools.product(range(-m, m + 1), repeat=3)
+                   if x * x + y * y + z * z < rad * rad) - 1
+        assert skin_capacity(h, sp, s) == max(16, math.ceil(1.75 * fill))
+
+
+def test_skin_refuses_particle_walls():
+    """neighbors.py:248-253: particle walls need the grid every step, so the skin is refused with them."""
+    from alloy_b200.solvers.sph import SolverDFSPH
+    from alloy_b200.solvers.sph.testing import dam_break
+
+    sc = dam_break(counts=(4, 4, 4), box=(0.1, 0.1, 0.1), reneighbor_skin=0.1)
+    with pytest.raises(ValueError, match="reneighbor_skin off"):
+        SolverDFSPH(sc.model, sc.config)
