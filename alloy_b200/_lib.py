@@ -22,7 +22,8 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_mlp_train_step", "adf_mlp_status", "adf_set_warm_model", "adf_set_feature_recording",
            "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs", "adf_add_emitters",
            "adf_prime", "adf_iteration_work", "adf_set_tuned_config", "adf_get_state_storage", "adf_port_take",
-           "adf_port_emit", "adf_energy", "adf_stable_dt", "adf_skin_flags")
+           "adf_port_emit", "adf_energy", "adf_stable_dt", "adf_skin_flags",
+           "adf_add_patch_emitter", "adf_trigger")
 TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph", "lists")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
@@ -67,7 +68,8 @@ class StateStorage(C.Structure):
                 ("emit_cursor", C.c_void_p), ("emit_world", C.c_void_p), ("n_emitters", C.c_int32),
                 ("port_stack", C.c_void_p), ("port_top", C.c_void_p), ("port_absorbed", C.c_void_p),
                 ("port_emitted", C.c_void_p), ("port_retired", C.c_void_p), ("port_taken", C.c_void_p),
-                ("port_granted", C.c_void_p)]
+                ("port_granted", C.c_void_p), ("n_patch_entries", C.c_int32), ("patch_pending", C.c_void_p),
+                ("patch_fired", C.c_void_p), ("patch_world", C.c_void_p)]
 
 
 _lib = None
@@ -134,6 +136,8 @@ def lib() -> C.CDLL:
     L.adf_energy.argtypes = [P, vp, vp, vp, vp, vp]
     L.adf_stable_dt.argtypes = [P, vp, C.c_double, C.c_double, C.c_double, vp, vp]
     L.adf_skin_flags.argtypes = [P, vp, vp]
+    L.adf_add_patch_emitter.argtypes = [P, C.c_int, vp, vp, vp, vp, vp]
+    L.adf_trigger.argtypes = [P, C.c_int, vp, C.c_int, vp]
     for name in EXPORTS:
         if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches", "adf_mlp_destroy"):
             getattr(L, name).restype = C.c_int

@@ -86,6 +86,12 @@ int fail(int code, const std::string& msg) {
     if (e_ != cudaSuccess) return fail(ADF_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+#define CK_NEG(x)                                                                           \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) return -fail(ADF_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
 inline int blocks(long long n, int b = BLOCK) { return (int)((n + b - 1) / b); }
 
 // Models up to this many particles take the CG products by teams of TL lanes per particle: below it one lane per
@@ -134,6 +140,12 @@ struct adf_solver {
   int *port_stack = nullptr, *port_stack0 = nullptr, *port_top = nullptr, *port_top0 = nullptr;
   int *port_taken = nullptr, *port_granted = nullptr, *port_absorbed = nullptr, *port_emitted = nullptr;
   int* port_retired = nullptr;
+  // patch emitters (patch.py): every registration's entries in one table (an entry = one world of one group)
+  std::vector<int> pe_world_h, pe_count_h, pe_begin_h, pe_group_h, pg_first_h{0}, pp_pool_h;
+  std::vector<float> pp_points_h, pg_vel_h;
+  int *pe_world_d = nullptr, *pe_count_d = nullptr, *pe_begin_d = nullptr, *pe_group_d = nullptr;
+  int *pe_pending_d = nullptr, *pe_fired_d = nullptr, *pp_pool_d = nullptr;
+  float *pp_points_d = nullptr, *pg_vel_d = nullptr;
   // scratch of the between-step calls (adf_energy, adf_stable_dt)
   float* energy_max = nullptr;
   int* speed_bits = nullptr;
@@ -1105,6 +1117,10 @@ void adf_destroy(adf_solver* s) {
                 s->emit_now_d, s->t_acc_d, s->sinks_d, s->em_world_d};
   for (void* p : em)
     if (p) cudaFree(p);
+  for (void* p : {(void*)s->pe_world_d, (void*)s->pe_count_d, (void*)s->pe_begin_d, (void*)s->pe_group_d,
+                  (void*)s->pe_pending_d, (void*)s->pe_fired_d, (void*)s->pp_pool_d, (void*)s->pp_points_d,
+                  (void*)s->pg_vel_d})
+    if (p) cudaFree(p);
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->list_entries) cudaFree(s->list_entries);
   if (s->body_runs) cudaFree(s->body_runs);
@@ -1164,6 +1180,14 @@ int enqueue_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_
       LAUNCH(s, k_emit, blocks(no), BLOCK, st, P, s->em_d, no, s->off_emitter_d, s->off_rank_d, s->off_local_d,
              s->emit_now_d, s->cursor_d, s->pool_d, s->mass_in, s->emit_overflow);
     LAUNCH(s, k_emit_cursor, blocks(ne), BLOCK, st, s->em_d, ne, s->emit_now_d, s->cursor_d);
+    prof_end(s, st);
+  }
+  const int npe = (int)s->pe_world_h.size();
+  if (npe > 0) {  // patch emitters after the box emitters (runtime.py:318-326)
+    prof_begin(s, 11, st);
+    LAUNCH(s, k_patch_emit, npe, 256, st, P, npe, s->pe_world_d, s->pe_count_d, s->pe_pending_d, s->pe_fired_d,
+           s->pe_begin_d, s->pp_pool_d, s->pp_points_d, s->pe_group_d, s->pg_vel_d, s->mass_in);
+    LAUNCH(s, k_patch_fire, blocks(npe), BLOCK, st, npe, s->pe_pending_d, s->pe_fired_d);
     prof_end(s, st);
   }
   return check_launch();
@@ -1547,6 +1571,9 @@ int adf_reset(adf_solver* s, const uint8_t* world_mask, const int32_t* flags0, c
     if (rc) return rc;
     LAUNCH(s, k_port_reset, W, 256, st, W, s->ws_d, s->mask_d, s->port_stack0, s->port_top0, s->port_stack,
            s->port_top, s->port_absorbed, s->port_emitted, s->port_retired, s->port_taken, s->port_granted);
+    const int npe = (int)s->pe_world_h.size();
+    if (npe > 0)
+      LAUNCH(s, k_patch_reset, blocks(npe), BLOCK, st, npe, s->pe_world_d, s->mask_d, s->pe_pending_d, s->pe_fired_d);
     CK(cudaStreamSynchronize(st));
   }
   const int ne = (int)s->em_h.size();
@@ -1849,8 +1876,82 @@ int adf_list_stats(adf_solver* s, int32_t* fluid, int64_t* entries, void* stream
   return check_launch();
 }
 
+int adf_add_patch_emitter(adf_solver* s, int entries, const int32_t* world, const int32_t* count,
+                          const int32_t* pool_ids, const float* points, const float* velocity) {
+  if (!s || entries < 0 || !velocity || (entries > 0 && (!world || !count)))
+    return -fail(ADF_ERR_VALUE, "adf_add_patch_emitter: null argument");
+  CK_NEG(cudaSetDevice(s->device));
+  long long total = 0;
+  for (int e = 0; e < entries; ++e) {
+    if (world[e] < 0 || world[e] >= s->W) return -fail(ADF_ERR_VALUE, "add_patch_emitter: world out of range");
+    if (count[e] < 0) return -fail(ADF_ERR_VALUE, "add_patch_emitter: negative point count");
+    total += count[e];
+  }
+  if (total > 0 && (!pool_ids || !points)) return -fail(ADF_ERR_VALUE, "adf_add_patch_emitter: null argument");
+  for (long long k = 0; k < total; ++k)
+    if (pool_ids[k] < 0 || pool_ids[k] >= s->n) return -fail(ADF_ERR_VALUE, "add_patch_emitter: pool id out of range");
+  const int E0 = (int)s->pe_world_h.size(), gid = (int)s->pg_first_h.size() - 1;
+  std::vector<int> pend(E0, 0), fired(E0, 0);
+  if (E0 > 0) {  // the earlier groups keep their armed / fired state
+    CK_NEG(cudaMemcpy(pend.data(), s->pe_pending_d, sizeof(int) * E0, cudaMemcpyDeviceToHost));
+    CK_NEG(cudaMemcpy(fired.data(), s->pe_fired_d, sizeof(int) * E0, cudaMemcpyDeviceToHost));
+  }
+  for (int e = 0; e < entries; ++e) {
+    s->pe_world_h.push_back(world[e]);
+    s->pe_count_h.push_back(count[e]);
+    s->pe_begin_h.push_back((int)s->pp_pool_h.size());
+    s->pe_group_h.push_back(gid);
+    for (int k = 0; k < count[e]; ++k) {
+      s->pp_pool_h.push_back(pool_ids[0]);
+      pool_ids += 1;
+      for (int a = 0; a < 3; ++a) s->pp_points_h.push_back(points[a]);
+      points += 3;
+    }
+    pend.push_back(0);
+    fired.push_back(0);
+  }
+  s->pg_first_h.push_back((int)s->pe_world_h.size());
+  for (int a = 0; a < 3; ++a) s->pg_vel_h.push_back(velocity[a]);
+  for (void* q : {(void*)s->pe_world_d, (void*)s->pe_count_d, (void*)s->pe_begin_d, (void*)s->pe_group_d,
+                  (void*)s->pe_pending_d, (void*)s->pe_fired_d, (void*)s->pp_pool_d, (void*)s->pp_points_d,
+                  (void*)s->pg_vel_d})
+    if (q) cudaFree(q);
+  const size_t E = s->pe_world_h.size(), NP = s->pp_pool_h.size(), G = s->pg_first_h.size() - 1;
+  int rc = dalloc(&s->pe_world_d, E) | dalloc(&s->pe_count_d, E) | dalloc(&s->pe_begin_d, E) |
+           dalloc(&s->pe_group_d, E) | dalloc(&s->pe_pending_d, E) | dalloc(&s->pe_fired_d, E) |
+           dalloc(&s->pp_pool_d, NP) | dalloc(&s->pp_points_d, 3 * NP) | dalloc(&s->pg_vel_d, 3 * G);
+  if (rc) return -fail(ADF_ERR_CUDA, "patch emitter tables: cudaMalloc failed");
+  auto up = [&](void* d, const void* h, size_t bytes) -> int {
+    if (bytes) CK(cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice));
+    return ADF_OK;
+  };
+  rc = up(s->pe_world_d, s->pe_world_h.data(), 4 * E) | up(s->pe_count_d, s->pe_count_h.data(), 4 * E) |
+       up(s->pe_begin_d, s->pe_begin_h.data(), 4 * E) | up(s->pe_group_d, s->pe_group_h.data(), 4 * E) |
+       up(s->pe_pending_d, pend.data(), 4 * E) | up(s->pe_fired_d, fired.data(), 4 * E) |
+       up(s->pp_pool_d, s->pp_pool_h.data(), 4 * NP) | up(s->pp_points_d, s->pp_points_h.data(), 12 * NP) |
+       up(s->pg_vel_d, s->pg_vel_h.data(), 12 * G);
+  if (rc) return -ADF_ERR_CUDA;
+  ++s->table_version;  // step graphs recorded before lack the patch launches
+  return gid;
+}
+
+int adf_trigger(adf_solver* s, int pid, const void* world_flags, int flags_bool, void* stream) {
+  if (!s || !world_flags) return fail(ADF_ERR_VALUE, "adf_trigger: null argument");
+  if (pid < 0 || pid >= (int)s->pg_first_h.size() - 1)
+    return fail(ADF_ERR_VALUE, "trigger: no patch emitter " + std::to_string(pid));
+  const int e0 = s->pg_first_h[pid], e1 = s->pg_first_h[pid + 1];
+  if (e1 == e0) return ADF_OK;
+  LAUNCH(s, k_patch_trigger, blocks(e1 - e0), BLOCK, (cudaStream_t)stream, e0, e1, world_flags, flags_bool ? 1 : 0,
+         s->pe_world_d, s->pe_fired_d, s->pe_pending_d);
+  return check_launch();
+}
+
 int adf_get_state_storage(adf_solver* s, adf_state_storage* out) {
   if (!s || !out) return fail(ADF_ERR_VALUE, "adf_get_state_storage: null argument");
+  out->n_patch_entries = (int)s->pe_world_h.size();
+  out->patch_pending = s->pe_pending_d;
+  out->patch_fired = s->pe_fired_d;
+  out->patch_world = s->pe_world_d;
   out->mass_in = (int64_t*)s->mass_in;
   out->mass_out = (int64_t*)s->d.mass_out;
   out->escaped = s->d.escaped;

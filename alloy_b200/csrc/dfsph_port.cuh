@@ -198,4 +198,65 @@ __global__ void k_stable_dt(int W, const int* __restrict__ speed_bits, float cfl
   out[w] = dt;
 }
 
+// Patch emitters (patch.py): triggered one-shot emitters. An entry is one world of one registration: count[e] points
+// (world frame: this path has no bodies) and as many spares reserved at registration, pool[begin[e] ..].
+
+// patch.py:65-79: arm the entries [e0, e1) whose world is flagged (int32 or bool flags [W]) and has not fired yet.
+__global__ void k_patch_trigger(int e0, int e1, const void* __restrict__ flags, int is_bool,
+                                const int* __restrict__ world, const int* __restrict__ fired, int* pending) {
+  const int e = e0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= e1) return;
+  const int w = world[e];
+  const bool on = is_bool ? reinterpret_cast<const uint8_t*>(flags)[w] != 0
+                          : reinterpret_cast<const int32_t*>(flags)[w] != 0;
+  if (on && fired[e] == 0) pending[e] = 1;
+}
+
+// patch.py:82-107 at the end of a step, one block per entry: an armed entry's spares become liquid at its points with
+// its registration's velocity (plus the zero point velocity of the world frame), their mass into the world's mass_in.
+__global__ void __launch_bounds__(256) k_patch_emit(DevP P, int E, const int* __restrict__ world,
+                                                    const int* __restrict__ count, const int* __restrict__ pending,
+                                                    const int* __restrict__ fired, const int* __restrict__ begin,
+                                                    const int* __restrict__ pool, const float* __restrict__ points,
+                                                    const int* __restrict__ group, const float* __restrict__ vel,
+                                                    long long* mass_in) {
+  __shared__ long long sml[8];
+  const int e = blockIdx.x;
+  if (e >= E || pending[e] == 0 || fired[e] != 0) return;
+  const float* v = vel + 3 * (size_t)group[e];
+  long long in = 0;
+  for (int k = threadIdx.x; k < count[e]; k += blockDim.x) {
+    const size_t b = (size_t)begin[e] + k;
+    const int i = pool[b];
+    P.q[3 * (size_t)i] = points[3 * b];
+    P.q[3 * (size_t)i + 1] = points[3 * b + 1];
+    P.q[3 * (size_t)i + 2] = points[3 * b + 2];
+    P.qd[3 * (size_t)i] = v[0] + 0.0f;
+    P.qd[3 * (size_t)i + 1] = v[1] + 0.0f;
+    P.qd[3 * (size_t)i + 2] = v[2] + 0.0f;
+    P.flags[i] |= FLAG_ACTIVE;
+    P.phase[i] = PH_LIQUID;
+    in += to_fixed(P.mass[i]);
+  }
+  const long long sum = block_sum256_ll(in, sml);
+  if (threadIdx.x == 0) atomicAdd((unsigned long long*)&mass_in[world[e]], (unsigned long long)sum);
+}
+
+// patch.py:110-115: an armed entry has fired; every entry is disarmed.
+__global__ void k_patch_fire(int E, int* pending, int* fired) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  if (pending[e] != 0 && fired[e] == 0) fired[e] = 1;
+  pending[e] = 0;
+}
+
+// patch.py:225-234 (reset): the masked worlds' entries re-armed (pending and fired cleared).
+__global__ void k_patch_reset(int E, const int* __restrict__ world, const uint8_t* __restrict__ mask, int* pending,
+                              int* fired) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E || !mask[world[e]]) return;
+  pending[e] = 0;
+  fired[e] = 0;
+}
+
 }  // namespace adf

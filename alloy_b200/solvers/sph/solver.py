@@ -265,6 +265,7 @@ class SolverDFSPH:
         self._em_world: list[int] = []
         self._em_pool: list[np.ndarray] = []
         self._em_own: list[bool] = []
+        self._patches: list[dict[int, np.ndarray]] = []  # per patch group: world -> reserved spare ids
         self._sinks = 0
         self.bounds = None if cfg.world_bounds is None else cfg.world_bounds
         from .ports import SPHPort
@@ -580,6 +581,10 @@ class SolverDFSPH:
                "port_top": view(st.port_top, W, "<i4"), "port_absorbed": view(st.port_absorbed, W, "<i4"),
                "port_emitted": view(st.port_emitted, W, "<i4"), "port_retired": view(st.port_retired, W, "<i4"),
                "taken": view(st.port_taken, W, "<i4"), "granted": view(st.port_granted, W, "<i4")}
+        P_ = int(st.n_patch_entries)
+        if P_:
+            out.update({"patch_pending": view(st.patch_pending, P_, "<i4"),
+                        "patch_fired": view(st.patch_fired, P_, "<i4"), "patch_world": view(st.patch_world, P_, "<i4")})
         E = int(st.n_emitters)
         if E:
             out.update({"emit_t": view(st.emit_t, E, "<f4"), "emit_cursor": view(st.emit_cursor, E, "<i4"),
@@ -599,7 +604,18 @@ class SolverDFSPH:
         if "emit_t" in a:
             arrays.update({"sph.emit_t": a["emit_t"], "sph.emit_cursor": a["emit_cursor"]})
         arrays.update(self.port.state_arrays())
+        arrays.update(self._patch_views(a, "patch_pending", "patch_fired"))  # patch.py:236-241
         return arrays
+
+    def _patch_views(self, a: dict, pending: str, fired: str) -> dict:
+        """Group k's slices of the patch entry arrays under the reference's keys sph.patch_pending{k} / fired{k}."""
+        out, e = {}, 0
+        for k, g in enumerate(self._patches):
+            if g:
+                out[f"sph.patch_pending{k}"] = a[pending][e:e + len(g)]
+                out[f"sph.patch_fired{k}"] = a[fired][e:e + len(g)]
+            e += len(g)
+        return out
 
     def alloy_state_worlds(self) -> dict:
         """Item -> world maps of the per-item arrays in ``alloy_state_arrays`` (coupling_hooks.py:128-138); per-world
@@ -610,6 +626,8 @@ class SolverDFSPH:
         a = self._storage()
         if "emit_world" in a:
             maps.update({"sph.emit_t": a["emit_world"], "sph.emit_cursor": a["emit_world"]})
+        if self._patches and "patch_world" in a:
+            maps.update(self._patch_views(a, "patch_world", "patch_world"))
         return maps
 
     # ------------------------------------------------------------------------------------------------ port
@@ -691,10 +709,83 @@ class SolverDFSPH:
 
     # ------------------------------------------------------------------------------------------------ emitters
     def _spares(self, w: int) -> np.ndarray:
+        """Inactive spares of world w not reserved by a patch emitter, ascending (runtime.py:215-219)."""
         ph = _host(self.model.sph.phase)
         wo = _host(self.model.particle_world)
         fl = _host(self.model.particle_flags)
-        return np.nonzero((ph == PHASE_SPARE) & (wo == w) & ((fl & _ACTIVE) == 0))[0].astype(np.int32)
+        ids = np.nonzero((ph == PHASE_SPARE) & (wo == w) & ((fl & _ACTIVE) == 0))[0].astype(np.int32)
+        held = [g[w] for g in self._patches if w in g]
+        return np.setdiff1d(ids, np.concatenate(held)).astype(np.int32) if held else ids
+
+    def _unowned_spares(self, w: int) -> np.ndarray:
+        """``_spares`` minus the pools emitters own, for patch emitters to reserve (runtime.py:221-226)."""
+        owned = [self._em_pool[e] for e, w2 in enumerate(self._em_world) if w2 == w and self._em_own[e]]
+        sp = self._spares(w)
+        return np.setdiff1d(sp, np.concatenate(owned)).astype(np.int32) if owned else sp
+
+    def add_patch_emitter(self, world_mask, body, local_points, velocity=(0.0, 0.0, 0.0)) -> int:
+        """Triggered one-shot emitter (solver.py:449-453, patch.py): for each masked world w, ``local_points[w]``
+        (N_w, 3) in the world frame (``body`` -1: this path has no bodies), emitted with ``velocity`` once a
+        ``trigger`` armed the world; N_w spares are reserved now (CapacityError if short), and the world's box
+        emitters re-split the rest, so they must not have emitted yet (runtime.py:228-241). Returns the id."""
+        W = self.world_count
+        mask = np.asarray(world_mask, bool)
+        if mask.shape != (W,) or len(local_points) != W:
+            raise ValueError(f"add_patch_emitter: world_mask and local_points need one entry per world ({W})")
+        bodies = np.full(W, int(body), np.int32) if np.ndim(body) == 0 else np.asarray(body, np.int32)
+        if bodies.shape != (W,):
+            raise ValueError(f"add_patch_emitter: body must be one index or one per world ({W})")
+        body_count = int(getattr(self.model, "body_count", 0) or 0)
+        if np.any((bodies < -1) | (bodies >= body_count)):
+            raise ValueError("add_patch_emitter: body indices must be in [-1, body_count)")
+        for w in np.nonzero(mask)[0]:
+            a = np.asarray(local_points[w])
+            if a.size and a.reshape(-1, 3).shape[1] != 3:
+                raise ValueError(f"add_patch_emitter: local_points[{w}] must be (N, 3)")
+        worlds = [w for w in range(W) if mask[w] and len(local_points[w])]
+        box = [e for e, w in enumerate(self._em_world) if w in set(worlds)]
+        if box:
+            cursors = np.zeros(len(self._em_world), np.int32)
+            _lib.check(self._lib.adf_emitter_state(self._h, None, cursors.ctypes.data), "emitters")
+            if np.any(cursors[box] > 0):
+                raise ValueError("add_patch_emitter: a box emitter of these worlds has emitted; add patch emitters "
+                                 "first")
+        pts = [np.asarray(local_points[w], np.float32).reshape(-1, 3) for w in worlds]
+        reserved = {}
+        for w, q in zip(worlds, pts, strict=True):
+            free = self._unowned_spares(w)
+            if len(free) < len(q):
+                raise _lib.CapacityError(f"add_patch_emitter: world {w} has {len(free)} free spares, needs {len(q)}")
+            reserved[w] = free[:len(q)].astype(np.int32)
+        wa = np.asarray(worlds if worlds else [0], np.int32)
+        counts = np.asarray([len(q) for q in pts] if worlds else [0], np.int32)
+        pool = np.ascontiguousarray(np.concatenate([reserved[w] for w in worlds]) if worlds else np.zeros(1, np.int32))
+        flat = np.ascontiguousarray(np.concatenate(pts) if worlds else np.zeros((1, 3), np.float32), np.float32)
+        vel = np.ascontiguousarray(np.asarray(velocity, np.float32).reshape(3))
+        pid = self._lib.adf_add_patch_emitter(self._h, len(worlds), wa.ctypes.data, counts.ctypes.data,
+                                              pool.ctypes.data, flat.ctypes.data, vel.ctypes.data)
+        _lib.check(pid if pid < 0 else 0, "add_patch_emitter")
+        self._patches.append(reserved)
+        for w in sorted({self._em_world[e] for e in box}):
+            self._split_pools(w)
+        log.info("SPH patch emitter %d: %d worlds, up to %d particles each", pid, len(worlds),
+                 int(counts.max()) if worlds else 0)
+        return int(pid)
+
+    def trigger(self, pid: int, world_flags) -> None:
+        """Arm patch emitter ``pid`` in the worlds where ``world_flags`` (device int32 or bool, one per world) is
+        set; the next step emits there once (solver.py:455-458; one launch, capture-safe)."""
+        if not 0 <= pid < len(self._patches):
+            raise ValueError(f"trigger: no patch emitter {pid}")
+        if not self._patches[pid]:
+            return
+        if world_flags.shape[0] < self.world_count:
+            raise ValueError(f"trigger: world_flags needs >= {self.world_count} entries")
+        is_bool = world_flags.dtype == torch.bool
+        if not is_bool and world_flags.dtype != torch.int32:
+            raise ValueError("trigger: world_flags must be int32 or bool")
+        _lib.check(self._lib.adf_trigger(self._h, int(pid), _ptr(world_flags), int(is_bool), self._stream()),
+                   "trigger")
 
     def _first_sph(self, world: int) -> int:
         ws = self.world_start

@@ -196,8 +196,26 @@ typedef struct {
   int32_t* port_retired;  /* [W] "sph.port_retired" */
   int32_t* port_taken;    /* [W] the last absorb / retire call's count per world (SPHPort.taken) */
   int32_t* port_granted;  /* [W] the last port emit's count per world (SPHPort.granted) */
+  int32_t n_patch_entries;  /* entries of all patch emitters (adf_add_patch_emitter), group after group */
+  int32_t* patch_pending;   /* [entries] "sph.patch_pending{k}" (group k's slice) */
+  int32_t* patch_fired;     /* [entries] "sph.patch_fired{k}" */
+  int32_t* patch_world;     /* [entries] world of each entry (alloy_state_worlds) */
 } adf_state_storage;
 int adf_get_state_storage(adf_solver* solver, adf_state_storage* out);
+
+/* Replaces SolverDFSPH.add_patch_emitter (solver.py:449-453, patch.py:146-187): a triggered one-shot emitter. One
+ * entry per world e < entries: world[e], count[e] points (host float [sum count][3], world frame: this path has no
+ * bodies) and as many spare particle ids (host int32 [sum count], reserved by the caller, patch.py:189-196), entry
+ * after entry; velocity (host [3]) is the group's. Returns the group id (>= 0) or -ADF_ERR_*. Step graphs are
+ * re-recorded on the next step. */
+int adf_add_patch_emitter(adf_solver* solver, int entries, const int32_t* world, const int32_t* count,
+                          const int32_t* pool_ids, const float* points, const float* velocity);
+
+/* Replaces SolverDFSPH.trigger (solver.py:455-458, patch.py:199-210): arm group pid's entries whose world is set in
+ * world_flags (device [W]; int32, or bool bytes when flags_bool = 1) and has not fired; at the end of the next step
+ * each armed entry emits its particles once (liquid at its points with the group's velocity, mass into mass_in) and
+ * fires. One launch, capture-safe. adf_reset re-arms the masked worlds' entries. */
+int adf_trigger(adf_solver* solver, int pid, const void* world_flags, int flags_bool, void* stream);
 
 /* Replaces SPHPort.absorb and SPHPort.retire (ports.py:101-122, 183-189; SolverDFSPH.retire, solver.py:428-431): the
  * masked liquid particles (mask: device int32 [n], non-zero = take) leave the liquid in one launch: ACTIVE cleared,
@@ -289,8 +307,11 @@ int adf_world_sum(adf_solver* solver, const float* values, double* out_sum, floa
  * Scratch: a fixed static device array of about 0.85 MB, held by every GPU that loads the library until the process
  * exits. Limits: W <= ADF_NOALLOC_MAX_WORLDS and n / 256 + W + 1 <= ADF_NOALLOC_MAX_CHUNKS (about 12.5 million
  * values); larger sizes return ADF_ERR_CAPACITY with a message. The first call on a device sets up (looks up the
- * scratch's device address once, with that device current); make it before any stream capture. All calls on a
- * device share the scratch, so calls that overlap on the GPU (on different streams) race. */
+ * scratch's device address once, with that device current); make it before any stream capture. The address is kept
+ * for the life of the process: it assumes the device's context does too (after a cudaDeviceReset or a torn-down
+ * primary context it would be stale). All calls on a device share the scratch, so calls that overlap on the GPU (on
+ * different streams) race. A world_start that decreases, or exceeds n, gives unspecified sums: every index is
+ * clamped, so nothing is read or written outside the arrays, but chunks past the scratch's count are dropped. */
 #define ADF_NOALLOC_MAX_WORLDS 16384
 #define ADF_NOALLOC_MAX_CHUNKS 65536
 int adf_world_sum_noalloc(const float* values, int n, const int32_t* world_start, int world_count, double* out_sum,

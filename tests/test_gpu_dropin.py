@@ -225,3 +225,67 @@ def test_coupling_restart_and_model_notification(cuda):
     assert sol.coupling_prepare_proxy_contacts(x2, None) is None
     with pytest.raises(ValueError):
         sol.coupling_harvest_proxy_particle_forces(torch.zeros(3, dtype=torch.int32), None, dt=sc.dt)
+
+
+def _patch_scene(device):
+    cfg = benchmark_config(0.02)
+    b = ModelBuilder()
+    for w in range(3):
+        b.begin_world()
+        add_fluid_block(b, cfg, (0.0, 0.0, 0.0), (5, 5, 4), jitter=0.01, seed=w)
+        add_spares(b, cfg, 12)
+        add_particle_box(b, cfg, (0.0, 0.0, 0.0), (0.2, 0.2, 0.3))
+        b.end_world()
+    return b.finalize(device), cfg
+
+
+def test_patch_emitter_trigger_fire_reset(cuda):
+    """patch.py: spares reserved at registration (the lowest free ids), nothing before a trigger, one emission per
+    armed world at the end of the next step (points, velocity, ACTIVE, liquid, ledger), later triggers of a fired
+    world ignored, reset re-arms; the pending and fired flags are snapshot keys."""
+    m, cfg = _patch_scene(cuda)
+    sol = SolverDFSPH(m, cfg)
+    W = 3
+    ws = m.particle_world_start.cpu().numpy()
+    ph0 = m.sph.phase.cpu().numpy().copy()
+    spare = [np.flatnonzero(ph0[ws[w]:ws[w + 1]] == 0) + ws[w] for w in range(W)]
+    pts = [np.array([[0.05 + 0.02 * k, 0.1, 0.2] for k in range(5)], np.float32), np.zeros((0, 3), np.float32),
+           np.array([[0.1, 0.05 + 0.02 * k, 0.22] for k in range(3)], np.float32)]
+    pid = sol.add_patch_emitter([True, True, True], -1, pts, velocity=(0.0, 0.1, -0.5))
+    assert pid == 0
+    with pytest.raises(ValueError, match="body indices"):
+        sol.add_patch_emitter([True, False, False], 0, pts)
+    with pytest.raises(Exception, match="free spares"):
+        sol.add_patch_emitter([True, False, False], -1, [np.zeros((8, 3), np.float32), [], []])
+    a, b = m.state(), m.state()
+    a, b = _run(sol, a, b, 2, 1.0e-3)
+    np.testing.assert_array_equal(m.sph.phase.cpu().numpy()[spare[0]], 0)  # not triggered: nothing emitted
+    led0 = sol.mass_ledger()
+    sol.trigger(pid, torch.tensor([1, 1, 0], dtype=torch.int32, device=cuda))
+    keys = sol.alloy_state_arrays()
+    np.testing.assert_array_equal(keys["sph.patch_pending0"].cpu().numpy(), [1, 0])  # entries: worlds 0 and 2
+    a, b = _run(sol, a, b, 1, 1.0e-3)
+    ph, fl = m.sph.phase.cpu().numpy(), m.particle_flags.cpu().numpy()
+    got = spare[0][:5]
+    assert np.all(ph[got] == 1) and np.all((fl[got] & 1) == 1) and np.all(ph[spare[0][5:]] == 0)
+    np.testing.assert_array_equal(a.particle_q.cpu().numpy()[got], pts[0])
+    np.testing.assert_array_equal(a.particle_qd.cpu().numpy()[got], np.tile(np.float32([0.0, 0.1, -0.5]), (5, 1)))
+    mass = m.particle_mass.cpu().numpy()
+    led1 = sol.mass_ledger()
+    assert int(led1["in"][0] - led0["in"][0]) == sum(int(round(float(mass[i]) * 2.0 ** 40)) for i in got)
+    np.testing.assert_array_equal(led1["in"][1:], led0["in"][1:])
+    keys = sol.alloy_state_arrays()
+    np.testing.assert_array_equal(keys["sph.patch_pending0"].cpu().numpy(), [0, 0])
+    np.testing.assert_array_equal(keys["sph.patch_fired0"].cpu().numpy(), [1, 0])
+    np.testing.assert_array_equal(sol.alloy_state_worlds()["sph.patch_fired0"].cpu().numpy(), [0, 2])
+    sol.trigger(pid, torch.tensor([True, False, True], device=cuda))  # world 0 fired already: ignored
+    a, b = _run(sol, a, b, 1, 1.0e-3)
+    ph = m.sph.phase.cpu().numpy()
+    assert np.all(ph[spare[2][:3]] == 1) and np.all(ph[spare[2][3:]] == 0)
+    led2 = sol.mass_ledger()
+    np.testing.assert_array_equal(led2["in"][0], led1["in"][0])
+    np.testing.assert_array_equal(led2["active"] + led2["out"], led2["initial"] + led2["in"])
+    sol.reset(a, torch.tensor([1, 0, 0], dtype=torch.uint8))
+    np.testing.assert_array_equal(sol.alloy_state_arrays()["sph.patch_fired0"].cpu().numpy(), [0, 1])
+    with pytest.raises(ValueError, match="no patch emitter"):
+        sol.trigger(5, torch.zeros(3, dtype=torch.int32, device=cuda))
