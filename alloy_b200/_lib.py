@@ -69,7 +69,8 @@ class StateStorage(C.Structure):
                 ("port_stack", C.c_void_p), ("port_top", C.c_void_p), ("port_absorbed", C.c_void_p),
                 ("port_emitted", C.c_void_p), ("port_retired", C.c_void_p), ("port_taken", C.c_void_p),
                 ("port_granted", C.c_void_p), ("n_patch_entries", C.c_int32), ("patch_pending", C.c_void_p),
-                ("patch_fired", C.c_void_p), ("patch_world", C.c_void_p)]
+                ("patch_fired", C.c_void_p), ("patch_world", C.c_void_p), ("warm_probe_gap", C.c_void_p),
+                ("warm_probe_wait", C.c_void_p)]
 
 
 _lib = None

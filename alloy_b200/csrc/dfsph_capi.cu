@@ -148,6 +148,7 @@ struct adf_solver {
   float *pp_points_d = nullptr, *pg_vel_d = nullptr;
   // scratch of the between-step calls (adf_energy, adf_stable_dt)
   float* energy_max = nullptr;
+  int *cw2 = nullptr, *cseg2 = nullptr, *n_cw2 = nullptr;  // work list of the learned start's first sweep
   int* speed_bits = nullptr;
   // host side of the iteration loop
   int* pinned = nullptr;
@@ -575,6 +576,13 @@ void dual_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   L.acc = P.acc2;
   L.err_orig = P.err2;
   const int W = s->W;
+  // the learned start's sweep covers the worlds its schedule evaluates in this solve (their own work list)
+  L.converged = P.probe_skip;
+  L.cw = s->cw2;
+  L.cseg = s->cseg2;
+  L.n_cw = s->n_cw2;
+  LAUNCH(s, k_probe_plan, blocks(W), BLOCK, st, P);
+  LAUNCH(s, k_worklist, 1, 1024, st, L);
   for (int pass = 0; pass < 2; ++pass) {
     DevP& Q = pass == 0 ? P : L;
     prof_begin(s, 5, st);
@@ -1350,6 +1358,12 @@ static int ensure_warm(adf_solver* s) {
   rc |= s->alloc(&d.err2, n);
   rc |= s->alloc(&d.use_l, W);
   rc |= s->alloc(&d.learned, 2 * W);
+  rc |= s->alloc(&d.probe_skip, W);
+  rc |= s->alloc(&d.probe_gap, 2 * W);
+  rc |= s->alloc(&d.probe_wait, 2 * W);
+  rc |= s->alloc(&s->cw2, W);
+  rc |= s->alloc(&s->cseg2, (size_t)W + 1);
+  rc |= s->alloc(&s->n_cw2, 1);
   rc |= s->alloc(&d.sum_c, W);
   rc |= s->alloc(&d.sum_l, W);
   rc |= s->alloc(&d.max_c, W);
@@ -1362,6 +1376,12 @@ static int ensure_warm(adf_solver* s) {
   if (rc) return fail(ADF_ERR_CUDA, "learned warm start: " + g_err);
   CK(cudaMemset(d.feat, 0, sizeof(float) * 16 * n));
   CK(cudaMemset(d.learned, 0, sizeof(int) * 2 * W));
+  {
+    std::vector<int> ones(2 * (size_t)W, 1);
+    CK(cudaMemcpy(d.probe_gap, ones.data(), sizeof(int) * 2 * W, cudaMemcpyHostToDevice));
+    CK(cudaMemset(d.probe_wait, 0, sizeof(int) * 2 * W));
+    CK(cudaMemset(d.probe_skip, 0, sizeof(int) * W));
+  }
   CK(cudaMemset(s->merr, 0, sizeof(int)));
   CK(cudaFuncSetAttribute(k_mlp_warm, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::FW_SMEM));
   int sms = 148;
@@ -1571,6 +1591,8 @@ int adf_reset(adf_solver* s, const uint8_t* world_mask, const int32_t* flags0, c
     if (rc) return rc;
     LAUNCH(s, k_port_reset, W, 256, st, W, s->ws_d, s->mask_d, s->port_stack0, s->port_top0, s->port_stack,
            s->port_top, s->port_absorbed, s->port_emitted, s->port_retired, s->port_taken, s->port_granted);
+    if (s->warm_alloc)
+      LAUNCH(s, k_probe_reset, blocks(W), BLOCK, st, W, s->mask_d, s->d.probe_gap, s->d.probe_wait);
     const int npe = (int)s->pe_world_h.size();
     if (npe > 0)
       LAUNCH(s, k_patch_reset, blocks(npe), BLOCK, st, npe, s->pe_world_d, s->mask_d, s->pe_pending_d, s->pe_fired_d);
@@ -1948,6 +1970,8 @@ int adf_trigger(adf_solver* s, int pid, const void* world_flags, int flags_bool,
 
 int adf_get_state_storage(adf_solver* s, adf_state_storage* out) {
   if (!s || !out) return fail(ADF_ERR_VALUE, "adf_get_state_storage: null argument");
+  out->warm_probe_gap = s->warm_alloc ? s->d.probe_gap : nullptr;
+  out->warm_probe_wait = s->warm_alloc ? s->d.probe_wait : nullptr;
   out->n_patch_entries = (int)s->pe_world_h.size();
   out->patch_pending = s->pe_pending_d;
   out->patch_fired = s->pe_fired_d;

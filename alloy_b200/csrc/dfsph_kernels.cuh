@@ -200,6 +200,10 @@ struct DevP {
   double* sum_l;
   float* max_c;
   float* max_l;
+  // evaluation schedule of the learned start under the judge (k_probe_plan)
+  int* probe_skip;  // [W] 1: this solve does not evaluate the learned start in the world
+  int* probe_gap;   // [2][W] solves between evaluations (per solve kind)
+  int* probe_wait;  // [2][W] solves of this kind left before the next evaluation
   // projected preconditioned CG (krylov.py; null unless the CG pressure solver is selected)
   float* cg_pd;     // search direction p, and p / rho0 (sorted)
   float* cg_pdr;
@@ -1497,14 +1501,45 @@ __global__ void k_mark_learned(DevP P) {
   P.learned[P.mode * P.W + w] = P.n_active[w] > 0.0 ? 1 : 0;
 }
 
-// After the first sweep from both starts: a world keeps the learned start unless its residual sum exceeds the plain
-// start's (equal liquid counts, so the sums order the mean errors).
+// The learned start's evaluation schedule under the judge, per world and solve kind: a world whose last evaluated
+// learned start lost to the plain start waits gap - 1 solves of this kind before the next evaluation, the gap doubling
+// up to PROBE_GAP_MAX; a kept start is evaluated again at the next solve. A world that is not evaluated continues from
+// the plain start exactly as when the judge rejects the learned one, so the schedule changes which solves pay for the
+// second first sweep, and nothing else. It follows each world's own history only (batch-invariant).
+constexpr int PROBE_GAP_MAX = 16;
+
+__global__ void k_probe_plan(DevP P) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W) return;
+  const int o = P.mode * P.W + w;
+  const int wait = P.probe_wait[o];
+  P.probe_skip[w] = (wait > 0 || !(P.n_active[w] > 0.0)) ? 1 : 0;
+  if (wait > 0) P.probe_wait[o] = wait - 1;
+}
+
+// After the first sweep from both starts: an evaluated world keeps the learned start unless its residual sum exceeds
+// the plain start's (equal liquid counts, so the sums order the mean errors); its schedule is updated.
 __global__ void k_choose_start(DevP P) {
   int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W) return;
-  const int use = (P.n_active[w] > 0.0 && !(P.sum_l[w] > P.sum_c[w])) ? 1 : 0;
+  const bool probed = P.probe_skip[w] == 0;
+  const int use = (probed && P.n_active[w] > 0.0 && !(P.sum_l[w] > P.sum_c[w])) ? 1 : 0;
   P.use_l[w] = use;
   P.learned[P.mode * P.W + w] = use;
+  if (probed) {
+    const int o = P.mode * P.W + w;
+    const int gap = use ? 1 : min(2 * max(P.probe_gap[o], 1), PROBE_GAP_MAX);
+    P.probe_gap[o] = gap;
+    P.probe_wait[o] = gap - 1;
+  }
+}
+
+// The masked worlds' schedules back to "evaluate at the next solve".
+__global__ void k_probe_reset(int W, const uint8_t* __restrict__ mask, int* gap, int* wait) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W || !mask[w]) return;
+  gap[w] = gap[W + w] = 1;
+  wait[w] = wait[W + w] = 0;
 }
 
 __global__ void __launch_bounds__(BLOCK) k_select_start(DevP P) {

@@ -581,6 +581,9 @@ class SolverDFSPH:
                "port_top": view(st.port_top, W, "<i4"), "port_absorbed": view(st.port_absorbed, W, "<i4"),
                "port_emitted": view(st.port_emitted, W, "<i4"), "port_retired": view(st.port_retired, W, "<i4"),
                "taken": view(st.port_taken, W, "<i4"), "granted": view(st.port_granted, W, "<i4")}
+        if st.warm_probe_gap:
+            out.update({"warm_probe_gap": view(st.warm_probe_gap, 2 * W, "<i4"),
+                        "warm_probe_wait": view(st.warm_probe_wait, 2 * W, "<i4")})
         P_ = int(st.n_patch_entries)
         if P_:
             out.update({"patch_pending": view(st.patch_pending, P_, "<i4"),
@@ -605,6 +608,8 @@ class SolverDFSPH:
             arrays.update({"sph.emit_t": a["emit_t"], "sph.emit_cursor": a["emit_cursor"]})
         arrays.update(self.port.state_arrays())
         arrays.update(self._patch_views(a, "patch_pending", "patch_fired"))  # patch.py:236-241
+        if "warm_probe_gap" in a:  # the learned start's evaluation schedule (no counterpart in the reference)
+            arrays.update({"sph.warm_probe_gap": a["warm_probe_gap"], "sph.warm_probe_wait": a["warm_probe_wait"]})
         return arrays
 
     def _patch_views(self, a: dict, pending: str, fired: str) -> dict:
@@ -628,6 +633,9 @@ class SolverDFSPH:
             maps.update({"sph.emit_t": a["emit_world"], "sph.emit_cursor": a["emit_world"]})
         if self._patches and "patch_world" in a:
             maps.update(self._patch_views(a, "patch_world", "patch_world"))
+        if "warm_probe_gap" in a:  # [2][W]: divergence then density, world-major within each
+            two = torch.arange(2 * self.world_count, dtype=torch.int32, device=self.device) % max(self.world_count, 1)
+            maps.update({"sph.warm_probe_gap": two, "sph.warm_probe_wait": two})
         return maps
 
     # ------------------------------------------------------------------------------------------------ port

@@ -757,6 +757,8 @@ def run_b200(args):
         other = "jacobi" if args.workload in LIQ9 else "cg"  # the other pressure solve beside the workload's own
         arms = [("plain" if headline_warm else "warm_started", {} if headline_warm else {"judge": True}),
                 ("warm_started_unjudged", {"judge": False}), (other, {"pressure_solver": other})]
+        if args.workload in LIQ9:  # Verlet-skin reuse of the rows (reneighbor_skin 0.1 h, config.py:78-80)
+            arms.append(("reneighbor_skin_0.1", {"reneighbor_skin": 0.1}))
         for key, kw in arms:
             note(f"arm {key}")
             r = variant_arm(args, dev, rank, world, **kw)

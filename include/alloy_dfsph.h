@@ -200,6 +200,9 @@ typedef struct {
   int32_t* patch_pending;   /* [entries] "sph.patch_pending{k}" (group k's slice) */
   int32_t* patch_fired;     /* [entries] "sph.patch_fired{k}" */
   int32_t* patch_world;     /* [entries] world of each entry (alloy_state_worlds) */
+  int32_t* warm_probe_gap;  /* [2][W] with a warm-start network under the judge (NULL before adf_set_warm_model): solves
+                               between evaluations of the learned start per solve kind (divergence, density) */
+  int32_t* warm_probe_wait; /* [2][W] solves left before the next evaluation */
 } adf_state_storage;
 int adf_get_state_storage(adf_solver* solver, adf_state_storage* out);
 

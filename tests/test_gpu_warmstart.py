@@ -1,6 +1,7 @@
 # SPDX-License-Identifier: Apache-2.0
 """The learned warm start inside the solver: feature recording leaves the step bit-exact, a network that predicts
-badly is rejected by the first-sweep judge in every world (so the step stays bit-exact against the oracle), the
+badly is rejected by the first-sweep judge in every world (so the step stays bit-exact against the oracle) and is then
+evaluated at doubling intervals, the
 solver's in-step predictions equal the standalone tensor-core inference on the same features, and a trained network
 keeps every step at the solver's tolerance."""
 
@@ -64,6 +65,10 @@ def test_a_bad_network_is_rejected_and_the_step_stays_plain(cuda):
     _run_against_oracle(sc, sol, 10)
     d = sol.diagnostics()
     assert d["learned_divergence"].sum() == 0 and d["learned_density"].sum() == 0
+    # rejected at steps 1, 3 and 7 (gaps 2, 4, 8 between evaluations), not evaluated at the other steps
+    keys = sol.alloy_state_arrays()
+    np.testing.assert_array_equal(keys["sph.warm_probe_gap"].cpu().numpy(), [8, 8])
+    np.testing.assert_array_equal(keys["sph.warm_probe_wait"].cpu().numpy(), [4, 4])
     pk = sol.debug_field("pred_kd")
     assert (pk[: sc.fluid_count] > 1.0).all()  # the predictions really were at the cap
 
