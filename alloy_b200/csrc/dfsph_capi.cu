@@ -606,7 +606,9 @@ void dual_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   prof_end(s, st);
 }
 
-mlp::Net solver_net(const adf_solver* s) { return mlp::Net{s->mw1, s->mw2, s->mparams, s->mnorm, s->merr}; }
+mlp::Net solver_net(const adf_solver* s) {
+  return mlp::Net{s->mw1, s->mw2, s->mparams, s->mnorm, s->merr, mlp::WAIT_LIMIT};
+}
 
 // pressure.py:355-390 + solve_driver.py:121-186 (Jacobi branch) + pressure.py:393-480
 int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool graph) {

@@ -29,7 +29,7 @@ int fail(int code, const std::string& msg) {
     if (e_ != cudaSuccess) return fail(ADF_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-Net net_of(const adf_mlp* m) { return Net{m->w1b, m->w2b, m->w, nullptr, m->error}; }
+Net net_of(const adf_mlp* m) { return Net{m->w1b, m->w2b, m->w, nullptr, m->error, m->wait_limit}; }
 
 int set_params(adf_mlp* m, const float* host) {
   CKM(cudaMemcpy(m->w, host, sizeof(float) * N_PARAMS, cudaMemcpyHostToDevice));
@@ -162,6 +162,20 @@ int adf_mlp_train_step(adf_mlp* m, const float* x, const float* y, const int32_t
     CKM(cudaMemcpyAsync(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, st));
     CKM(cudaStreamSynchronize(st));
   }
+  return ADF_OK;
+}
+
+int adf_mlp_set_wait_limit(adf_mlp* m, uint32_t polls) {
+  if (!m) return fail(ADF_ERR_VALUE, "adf_mlp_set_wait_limit: null argument");
+  m->wait_limit = polls;
+  return ADF_OK;
+}
+
+int adf_mlp_clear_status(adf_mlp* m) {
+  if (!m) return fail(ADF_ERR_VALUE, "adf_mlp_clear_status: null argument");
+  CKM(cudaSetDevice(m->device));
+  CKM(cudaDeviceSynchronize());
+  CKM(cudaMemset(m->error, 0, sizeof(int)));
   return ADF_OK;
 }
 

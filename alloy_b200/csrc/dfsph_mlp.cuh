@@ -47,6 +47,7 @@ struct Net {
   const float* p;           // packed FP32 parameters (N_PARAMS): b1, b2, w3, b3 are read from here
   const float* norm;        // fmu[16], finv[16], tmu[2], tsig[2] (may be null: identity)
   int* error;               // set to 1 when a bounded wait expires
+  unsigned wait_limit;      // polls a tensor-core step's wait may take before giving up (WAIT_LIMIT; adf_mlp_set_wait_limit)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -274,7 +275,7 @@ __device__ void forward_rows(const Net& net, Src& src) {
       mma_commit(bar);
     }
     ++committed;
-    failed = !mbar_wait(bar, phase, WAIT_LIMIT);
+    failed = !mbar_wait(bar, phase, net.wait_limit);
     if (any_failed(failed)) break;
     phase ^= 1;
     --committed;
@@ -300,7 +301,7 @@ __device__ void forward_rows(const Net& net, Src& src) {
       mma_commit(bar);
     }
     ++committed;
-    failed = !mbar_wait(bar, phase, WAIT_LIMIT);
+    failed = !mbar_wait(bar, phase, net.wait_limit);
     if (any_failed(failed)) break;
     phase ^= 1;
     --committed;
@@ -445,7 +446,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_grad(Net net, const float* __restr
   float sq = 0.0f;
   auto wait = [&]() -> bool {
     ++committed;
-    failed = !mbar_wait(bar, phase, WAIT_LIMIT);
+    failed = !mbar_wait(bar, phase, net.wait_limit);
     if (any_failed(failed)) return false;
     phase ^= 1;
     --committed;
@@ -687,4 +688,5 @@ struct adf_mlp {
   float* loss = nullptr;  // [1]
   int* error = nullptr;   // bounded-wait expiry flag
   int step = 0;
+  unsigned wait_limit = adf::mlp::WAIT_LIMIT;  // the tensor-core waits' poll limit (the drain after an expiry keeps WAIT_LIMIT)
 };

@@ -346,6 +346,12 @@ int adf_mlp_train_step(adf_mlp* mlp, const float* x, const float* t, const int32
                        float* loss, void* stream);
 /* ADF_OK, or ADF_ERR_STATE if a tensor-core wait of this network's kernels ever expired (its results are invalid). */
 int adf_mlp_status(adf_mlp* mlp);
+/* Test hooks of the bounded waits. A tensor-core step's wait on its MMA's mbarrier gives up after `polls` polls
+ * (default 2^22, far above a normal wait's few): the kernel then sets the status, waits (at most 2^22 polls) for the
+ * MMAs it committed, frees its tensor memory and returns. polls = 0 makes every such wait give up at once, which runs
+ * that path without any fault. adf_mlp_clear_status resets the status after a synchronisation. */
+int adf_mlp_set_wait_limit(adf_mlp* mlp, uint32_t polls);
+int adf_mlp_clear_status(adf_mlp* mlp);
 
 /* Learned warm start (no counterpart in the reference; its starts are the previous kappa scaled, pressure.py:214-261).
  * With a network set, each step evaluates it once per liquid particle at the start of its first solve and both

@@ -95,3 +95,36 @@ def test_adam_training_fits_a_smooth_map(cuda):
     assert losses[-1] < 0.1 * losses[0], losses
     assert losses[-1] < 0.1, losses
     assert all(b < a * 1.05 for a, b in zip(losses, losses[1:])), losses
+
+
+def test_an_expired_tensor_core_wait_sets_the_status_and_the_context_survives(cuda):
+    """The MMA waits give up after a poll limit; a limit of 0 polls makes every one give up at once. Each kernel then
+    waits for the MMAs it committed, frees its tensor memory and returns: the status reports the expiry (ADF_ERR_STATE,
+    a RuntimeError here), and after the status is cleared and the limit restored the same network computes the
+    reference's outputs again on the same context."""
+    from alloy_b200 import _lib
+
+    L = _lib.lib()
+    rng = np.random.default_rng(7)
+    p = init_params(seed=7)
+    net = Network(p)
+    x = torch.from_numpy(rng.normal(0.0, 1.0, (3000, 16)).astype(np.float32))
+    t = torch.from_numpy(rng.normal(0.0, 1.0, (3000, 2)).astype(np.float32))
+    idx = torch.arange(3000, dtype=torch.int32)
+    _lib.check(L.adf_mlp_set_wait_limit(net.handle, 0))
+    net.forward(x.to(cuda))
+    torch.cuda.synchronize()
+    with pytest.raises(RuntimeError, match="tensor-core wait expired"):
+        net.status()
+    _lib.check(L.adf_mlp_clear_status(net.handle))
+    net.gradient(x.to(cuda), t.to(cuda), idx.to(cuda))  # the gradient kernel's waits expire the same way
+    with pytest.raises(RuntimeError, match="tensor-core wait expired"):
+        net.status()
+    _lib.check(L.adf_mlp_clear_status(net.handle))
+    _lib.check(L.adf_mlp_set_wait_limit(net.handle, 1 << 22))
+    y = net.forward(x.to(cuda)).cpu()
+    torch.cuda.synchronize()
+    net.status()
+    ref, _ = _reference(p, x)
+    ref = ref.detach()
+    np.testing.assert_allclose(y.numpy(), ref.numpy(), rtol=0, atol=3e-3 * (float(ref.abs().max()) + 1e-6))
