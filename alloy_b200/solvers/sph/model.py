@@ -102,7 +102,8 @@ class Model:
         return {"q": c(self.particle_q), "qd": c(self.particle_qd), "mass": c(self.particle_mass),
                 "radius": c(self.particle_radius), "flags": c(self.particle_flags), "world": c(self.particle_world),
                 "world_start": c(self.particle_world_start), "gravity": c(self.gravity), "phase": c(self.sph.phase),
-                "rest_density": c(self.sph.rest_density), "shape_type": c(self.shape_type),
+                "rest_density": c(self.sph.rest_density), "viscosity": c(self.sph.viscosity),
+                "shape_type": c(self.shape_type),
                 "shape_scale": c(self.shape_scale), "shape_transform": c(self.shape_transform),
                 "shape_world": c(self.shape_world), "shape_flags": c(self.shape_flags),
                 "shape_body": c(self.shape_body), "shape_mu": c(self.shape_material_mu),

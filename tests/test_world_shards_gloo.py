@@ -20,17 +20,31 @@ from alloy_b200.solvers.sph.testing import batched_worlds
 STEPS = 8
 
 
-def _scene():
+def _scene(kind: str = "particles"):
+    if kind == "sdf":  # box-tank columns of different heights and a global box every world sees
+        from alloy_b200.solvers.sph.build import add_box_tank, add_fluid_block, wall_box
+        from alloy_b200.solvers.sph.model import ModelBuilder
+        from alloy_b200.solvers.sph.testing import Scene, benchmark_config
+
+        cfg = benchmark_config(0.02)
+        b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
+        for w in range(5):
+            b.begin_world()
+            add_box_tank(b, (0.0, 0.0, 0.0), (0.12, 0.12, 0.3), wall=cfg.h)
+            add_fluid_block(b, cfg, (0.0, 0.0, 0.0), (6, 6, 4 + w), jitter=0.01, seed=w)
+            b.end_world()
+        wall_box(b, (0.06, 0.06, 0.0), (0.01, 0.01, 0.01), mu=0.5)
+        return Scene(b.finalize("cpu"), cfg, 1.0e-3, STEPS, 0, 0, name="sdf_columns")
     return batched_worlds(worlds=6, lo=150, hi=700, seed=5)
 
 
-def _rank(rank: int, world: int, port: int, out: str):
+def _rank(rank: int, world: int, port: int, out: str, kind: str = "particles"):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         from oracle.pyoracle import Oracle
 
-        sc = _scene()
+        sc = _scene(kind)
         arr = sc.model.host()
         ws = arr["world_start"]
         parts = shard_worlds(np.diff(ws), world)
@@ -60,14 +74,16 @@ def _free_port() -> int:
 
 
 @pytest.mark.timeout(300)
-def test_two_gloo_ranks_step_disjoint_world_shards_bitwise(tmp_path):
+@pytest.mark.parametrize("kind", ["particles", "sdf"])
+def test_two_gloo_ranks_step_disjoint_world_shards_bitwise(tmp_path, kind):
+    """Particle-wall worlds, and box-tank worlds whose shards carry their own boxes and the global one."""
     out = str(tmp_path / "merged.pkl")
-    mp.start_processes(_rank, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
+    mp.start_processes(_rank, args=(2, _free_port(), out, kind), nprocs=2, join=True, start_method="spawn")
     with open(out, "rb") as f:
         merged = pickle.load(f)
     from oracle.pyoracle import Oracle
 
-    sc = _scene()
+    sc = _scene(kind)
     arr = sc.model.host()
     o = Oracle(arr, sc.config, threads=1)
     for _ in range(STEPS):
