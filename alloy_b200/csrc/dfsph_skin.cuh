@@ -148,13 +148,24 @@ __global__ void __launch_bounds__(BLOCK) k_skin_filter(DevP P) {
   const float h2 = P.kc.h2;
   const int K = P.K;
   int m = 0, total = 0;
-  for (int k = 0; k < sc; ++k) {
-    const int j = P.pos_of[P.sup[(size_t)k * P.n + s]];
-    const float4 xj = P.pos[j];
-    const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-    if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
-      ++total;
-      if (m < K) P.nbr[(size_t)m++ * P.n + p] = j;
+  constexpr int SB = 8;  // superset entries in flight: their ids, then their sorted positions, then the positions
+  for (int k0 = 0; k0 < sc; k0 += SB) {
+    int j[SB];
+#pragma unroll
+    for (int u = 0; u < SB; ++u) j[u] = k0 + u < sc ? P.sup[(size_t)(k0 + u) * P.n + s] : -1;
+#pragma unroll
+    for (int u = 0; u < SB; ++u) j[u] = j[u] >= 0 ? P.pos_of[j[u]] : p;
+    float4 xj[SB];
+#pragma unroll
+    for (int u = 0; u < SB; ++u) xj[u] = P.pos[j[u]];
+#pragma unroll
+    for (int u = 0; u < SB; ++u) {
+      if (k0 + u >= sc) break;
+      const float dx = xj[u].x - xi.x, dy = xj[u].y - xi.y, dz = xj[u].z - xi.z;
+      if (dot_plain(dx, dy, dz, dx, dy, dz) < h2) {
+        ++total;
+        if (m < K) P.nbr[(size_t)m++ * P.n + p] = j[u];
+      }
     }
   }
   P.cnt[p] = m;

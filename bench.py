@@ -421,7 +421,11 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
     torch.cuda.synchronize(dev)
     t = e0.elapsed_time(e1) * 1e-3
     nf1 = sol.list_stats()[0]
-    it_den, it_div, err, kept = [], [], [], []
+    it_den, it_div, err, kept, rebuilt = [], [], [], [], []
+    skin = bool(sc.config.reneighbor_skin)
+    if skin:  # the 20 read-back steps also time each kernel group (launched one by one, outside the timed steps)
+        sol.profile(True)
+        sol.profile_read()
     for _ in range(20):
         run()
         r = sol.report()
@@ -430,10 +434,17 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
         it_div.append(int(r.iters_divergence.max()))
         err.append(float(r.density_err.max()))
         kept.append(0.5 * float(d["learned_density"].mean() + d["learned_divergence"].mean()))
+        if skin:
+            rebuilt.append(float(sol.skin_flags().mean()))
     ps = 0.5 * (nf0 + nf1) * args.steps
     out = {"value": ps / t, "ms_per_step": 1e3 * t / args.steps, "pressure_solver": sol.pressure_solver,
            "iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean": float(np.mean(it_div)),
            "density_err_mean_max_over_steps": float(np.max(err)), "particle_steps": ps, "seconds": t}
+    if skin:
+        prof = sol.profile_read()
+        sol.profile(False)
+        out.update({"rebuilt_world_share": float(np.mean(rebuilt)),
+                    "sort_and_rows_ms_per_step": {k: round(prof[k][0] / 20.0, 4) for k in ("sort", "lists")}})
     if judge is not None:
         out.update({"judge": judge, "model": str(DEFAULT_MODEL.relative_to(ROOT)),
                     "learned_start_kept": float(np.mean(kept))})
