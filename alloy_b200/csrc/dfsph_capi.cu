@@ -501,10 +501,10 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   LAUNCH(s, k_cg_direction, blocks(n), BLOCK, st, P);
 }
 
-// The stop test of an iteration and the next iteration's work list (one launch: k_check_fused).
+// The stop test of an iteration and the next iteration's work list (one launch: k_check_warps).
 void check_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   if (P.n_chunks > 0) {
-    LAUNCH(s, k_check_fused, P.n_chunks, 256, st, P);
+    LAUNCH(s, k_check_warps, (P.n_chunks + CHECK_WARPS - 1) / CHECK_WARPS, 32 * CHECK_WARPS, st, P);
   } else {
     cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
     if (s->W > 0) LAUNCH(s, k_worklist, 1, 1024, st, P);
@@ -883,7 +883,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.kv_s, n);
   rc |= s->alloc(&d.kd_s, n);
   rc |= s->alloc(&d.nbr, (size_t)s->K * n);
-  rc |= s->alloc(&d.nbrjf, (size_t)s->K * n);
+  rc |= s->alloc(&d.nbrg, (size_t)s->K * n);
   rc |= s->alloc(&d.nbrw, (size_t)s->K * n);
   rc |= s->alloc(&d.cnt, n);
   rc |= s->alloc(&d.slot_g, (size_t)d.slot_cap * n);

@@ -111,7 +111,7 @@ struct DevP {
   float* kv_s;
   float* kd_s;
   int* nbr;     // [K][n] sorted positions, ascending original id
-  int2* nbrjf;  // [K][n] (row entry, bits of its gradient factor F(r_ij)), written by k_density_alpha
+  float4* nbrg;  // [K][n] (m_j grad W_ij = m_j F(r_ij) r_ij, bits of the row entry), written by k_density_alpha
   float* nbrw;  // [K][n] kernel value W(r_ij) of each row entry, written by k_density_alpha, read by k_xsph
   int* cnt;
   // Boundary slots (boundary.py:36): slot b of sorted particle p at b * n + p of each array, nearest wall first.
@@ -1315,24 +1315,30 @@ __device__ __forceinline__ void load_row_batch(const DevP& P, int p, int c, int 
   for (int u = 0; u < NB; ++u) j[u] = (k + u < c) ? __ldcs(row + (size_t)(k + u) * P.n) : p;
 }
 
-// Row entries with their gradient factor F(r_ij) (the value wf() gives for the pair, stored by k_density_alpha) in
-// one 8-byte load: the later loops read F instead of re-evaluating sqrt, branches and a division; the value is the
-// same, so every sum is unchanged.
+// m_j grad W_ij = (m_j F(r)) r_ij for r_ij = x_i - x_j, F = W'(r) / r (kernels.py:59-77 gives grad W = r_ij F; the
+// mass is folded in once per pair). The oracle's mass_grad is the same expression.
+__device__ __forceinline__ float4 mass_grad(float mj, float F, float rx, float ry, float rz, int j) {
+  const float s = mj * F;
+  return make_float4(s * rx, s * ry, s * rz, __int_as_float(j));
+}
+
+// Row entries with their pair gradient m_j grad W_ij (stored by k_density_alpha) in one 16-byte load: the pressure
+// loops then gather only the neighbour's field they combine (velocity, kappa / rho0 or acceleration), not its
+// position and mass, and the values are those of the formula, so every sum is unchanged.
 template <int NB>
-__device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, int k, int (&j)[NB], float (&f)[NB]) {
-  const int2* row = P.nbrjf + p;
+__device__ __forceinline__ void load_row_batch_g(const DevP& P, int p, int c, int k, int (&j)[NB], float4 (&g)[NB]) {
+  const float4* row = P.nbrg + p;
 #pragma unroll
   for (int u = 0; u < NB; ++u) {
-    int2 e = (k + u < c) ? __ldcs(row + (size_t)(k + u) * P.n) : make_int2(p, 0);
-    j[u] = e.x;
-    f[u] = __int_as_float(e.y);
+    g[u] = (k + u < c) ? __ldcs(row + (size_t)(k + u) * P.n) : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(p));
+    j[u] = __float_as_int(g[u].w);
   }
 }
 
 // ------------------------------------------------------------------------------------------ density, factor
 // pressure.py:144-193
 template <int NB>
-__global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
+__global__ void __launch_bounds__(BLOCK, 3) k_density_alpha(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   float4 xi = P.pos[p];
@@ -1356,15 +1362,15 @@ __global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
       float r2 = dot_plain(rx, ry, rz, rx, ry, rz);
       float W, F;
       wf(P.kc, r2, W, F);
-      __stcs(P.nbrjf + (size_t)(k + u) * P.n + p, make_int2(j[u], __float_as_int(F)));
-      __stcs(P.nbrw + (size_t)(k + u) * P.n + p, W);
       float mj = xj.w;
+      const float4 gm = mass_grad(mj, F, rx, ry, rz, j[u]);
+      __stcs(P.nbrg + (size_t)(k + u) * P.n + p, gm);
+      __stcs(P.nbrw + (size_t)(k + u) * P.n + p, W);
       rho = ADF_FMA(mj, W, rho);
       float a = mj * inv_r0;
-      float aF = a * F;
-      Gx = ADF_FMA(aF, rx, Gx);
-      Gy = ADF_FMA(aF, ry, Gy);
-      Gz = ADF_FMA(aF, rz, Gz);
+      Gx = ADF_FMA(inv_r0, gm.x, Gx);
+      Gy = ADF_FMA(inv_r0, gm.y, Gy);
+      Gz = ADF_FMA(inv_r0, gm.z, Gz);
       sq = ADF_FMA(bi * a, (F * F) * r2, sq);
     }
   }
@@ -1396,28 +1402,22 @@ template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
-  float4 xi = P.pos[p];
   float4 vi = P.vel[p];
   float inv_r0 = 1.0f / vi.w;
   float rate = 0.0f;
   int c = P.cnt[p];
   for (int k = 0; k < c; k += NB) {
     int j[NB];
-    float fb[NB];
-    load_row_batch_f(P, p, c, k, j, fb);
-    float4 xb[NB], vb[NB];
+    float4 gb[NB];
+    load_row_batch_g(P, p, c, k, j, gb);
+    float4 vb[NB];
 #pragma unroll
-    for (int u = 0; u < NB; ++u) {
-      xb[u] = P.pos[j[u]];
-      vb[u] = P.vel[j[u]];
-    }
+    for (int u = 0; u < NB; ++u) vb[u] = P.vel[j[u]];
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
       if (k + u >= c) break;
-      float4 xj = xb[u], vj = vb[u];
-      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-      float aF = (xj.w * inv_r0) * fb[u];
-      rate = ADF_FMA(aF, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, rx, ry, rz), rate);
+      const float4 vj = vb[u], g = gb[u];
+      rate = ADF_FMA(inv_r0, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, g.x, g.y, g.z), rate);
     }
   }
   const int ns = slot_count(P, p);
@@ -1664,30 +1664,24 @@ __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
 // ------------------------------------------------------------------------------------------ Jacobi sweep
 // pressure.py:264-291: a_i = -sum_j m_j (k_i/rho0_i + k_j/rho0_j) grad W_ij - k_i sum_b dPsi_b
 template <int NB>
-__device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, float& ax, float& ay, float& az) {
+__device__ __forceinline__ void pressure_accel(const DevP& P, int p, float& ax, float& ay, float& az) {
   float ki = P.kr[p];
   ax = ay = az = 0.0f;
   int c = P.cnt[p];
   for (int k = 0; k < c; k += NB) {
     int j[NB];
-    float fb[NB];
-    load_row_batch_f(P, p, c, k, j, fb);
-    float4 xb[NB];
+    float4 gb[NB];
+    load_row_batch_g(P, p, c, k, j, gb);
     float kb[NB];
 #pragma unroll
-    for (int u = 0; u < NB; ++u) {
-      xb[u] = P.pos[j[u]];
-      kb[u] = P.kr[j[u]];
-    }
+    for (int u = 0; u < NB; ++u) kb[u] = P.kr[j[u]];
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
       if (k + u >= c) break;
-      float4 xj = xb[u];
-      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-      float cF = (xj.w * (ki + kb[u])) * fb[u];
-      ax = ADF_FMA(-cF, rx, ax);
-      ay = ADF_FMA(-cF, ry, ay);
-      az = ADF_FMA(-cF, rz, az);
+      const float cc = ki + kb[u];
+      ax = ADF_FMA(-cc, gb[u].x, ax);
+      ay = ADF_FMA(-cc, gb[u].y, ay);
+      az = ADF_FMA(-cc, gb[u].z, az);
     }
   }
   const int ns = slot_count(P, p);
@@ -1706,7 +1700,7 @@ __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
   if (!work_item(P, b, e)) return;
   for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
     float ax, ay, az;
-    pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
+    pressure_accel<NB>(P, p, ax, ay, az);
     P.acc[p] = make_float4(ax, ay, az, 0.0f);
   }
 }
@@ -1715,27 +1709,21 @@ __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
 // pressure.py:294-310: Ar_i of the accelerations in P.acc (the matrix-free product, before the compliance term)
 template <int NB>
 __device__ __forceinline__ float accel_divergence(const DevP& P, int p, float inv_r0) {
-  float4 xi = P.pos[p];
   float4 ai = P.acc[p];
   float ar = 0.0f;
   int c = P.cnt[p];
   for (int k = 0; k < c; k += NB) {
     int j[NB];
-    float fb[NB];
-    load_row_batch_f(P, p, c, k, j, fb);
-    float4 xb[NB], ab[NB];
+    float4 gb[NB];
+    load_row_batch_g(P, p, c, k, j, gb);
+    float4 ab[NB];
 #pragma unroll
-    for (int u = 0; u < NB; ++u) {
-      xb[u] = P.pos[j[u]];
-      ab[u] = P.acc[j[u]];
-    }
+    for (int u = 0; u < NB; ++u) ab[u] = P.acc[j[u]];
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
       if (k + u >= c) break;
-      float4 xj = xb[u], aj = ab[u];
-      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-      float aF = (xj.w * inv_r0) * fb[u];
-      ar = ADF_FMA(aF, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz), ar);
+      const float4 aj = ab[u], g = gb[u];
+      ar = ADF_FMA(inv_r0, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, g.x, g.y, g.z), ar);
     }
   }
   const int ns = slot_count(P, p);
@@ -1797,7 +1785,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel(DevP P, const float* vec, co
   Q.kappa = const_cast<float*>(vec);
   Q.kr = const_cast<float*>(vr);
   float ax, ay, az;
-  pressure_accel<NB>(Q, p, P.pos[p], ax, ay, az);
+  pressure_accel<NB>(Q, p, ax, ay, az);
   P.acc[p] = make_float4(ax, ay, az, 0.0f);
 }
 
@@ -1841,10 +1829,10 @@ __device__ __forceinline__ Team team_of(int& p) {
   return tm;
 }
 
-__device__ __forceinline__ int2 row_entry(const DevP& P, int p, int k) { return __ldcs(P.nbrjf + p + (size_t)k * P.n); }
+__device__ __forceinline__ float4 row_entry(const DevP& P, int p, int k) { return __ldcs(P.nbrg + p + (size_t)k * P.n); }
 
 // pressure_accel with the fields of Q (kappa, kr), valid in the team's first lane
-__device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, float4 xi, const Team& tm, float& ax, float& ay,
+__device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, const Team& tm, float& ax, float& ay,
                                                     float& az) {
   const float ki = Q.kr[p];
   ax = ay = az = 0.0f;
@@ -1856,13 +1844,12 @@ __device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, float4
       const int k = k0 + u * TL + tm.t;
       cf[u] = rx[u] = ry[u] = rz[u] = 0.0f;
       if (k < c) {
-        const int2 e = row_entry(Q, p, k);
-        const float4 xj = Q.pos[e.x];
-        const float kj = Q.kr[e.x];
-        rx[u] = xi.x - xj.x;
-        ry[u] = xi.y - xj.y;
-        rz[u] = xi.z - xj.z;
-        cf[u] = (xj.w * (ki + kj)) * __int_as_float(e.y);
+        const float4 e = row_entry(Q, p, k);
+        const float kj = Q.kr[__float_as_int(e.w)];
+        rx[u] = e.x;
+        ry[u] = e.y;
+        rz[u] = e.z;
+        cf[u] = ki + kj;
       }
     }
 #pragma unroll
@@ -1891,7 +1878,6 @@ __device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, float4
 
 // accel_divergence, valid in the team's first lane
 __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, float inv_r0, const Team& tm) {
-  const float4 xi = P.pos[p];
   const float4 ai = P.acc[p];
   float ar = 0.0f;
   const int c = P.cnt[p];
@@ -1902,11 +1888,10 @@ __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, flo
       const int k = k0 + u * TL + tm.t;
       af[u] = d[u] = 0.0f;
       if (k < c) {
-        const int2 e = row_entry(P, p, k);
-        const float4 xj = P.pos[e.x], aj = P.acc[e.x];
-        const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-        af[u] = (xj.w * inv_r0) * __int_as_float(e.y);
-        d[u] = dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz);
+        const float4 e = row_entry(P, p, k);
+        const float4 aj = P.acc[__float_as_int(e.w)];
+        af[u] = inv_r0;
+        d[u] = dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, e.x, e.y, e.z);
       }
     }
 #pragma unroll
@@ -1935,7 +1920,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* ve
   Q.kappa = const_cast<float*>(vec);
   Q.kr = const_cast<float*>(vr);
   float ax, ay, az;
-  pressure_accel_team(Q, p, P.pos[p], tm, ax, ay, az);
+  pressure_accel_team(Q, p, tm, ax, ay, az);
   if (tm.t == 0) P.acc[p] = make_float4(ax, ay, az, 0.0f);
 }
 
@@ -2208,55 +2193,108 @@ __device__ __forceinline__ bool grid_ticket(const DevP& P) {
   return last;
 }
 
-// The Jacobi iteration's stop test in one launch (k_chunk_sum, k_world_check and k_worklist fused): block c folds
-// chunk c (chunks of converged worlds keep their partials); the last block of a world to finish folds the world's
-// partials in the same fixed tree order as k_world_check and runs its stop test (pressure.py:370-390); the last block
-// of the grid lists the worlds still iterating for the next iteration and stores their count as the unconverged
-// count. The sums are those of the separate kernels bit for bit; only the launches are fewer.
-__global__ void __launch_bounds__(256) k_check_fused(DevP P) {
-  __shared__ double smd[8];
-  __shared__ float smf[8];
-  __shared__ bool wlast, glast;
-  const int c = blockIdx.x;
-  const int w = P.chunk_world[c];
-  const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
-  bool ticket = c == c0;  // the world's grid ticket: its first chunk's block if it had converged, else its last block
-  if (!P.converged[w]) {
-    const int i = P.chunk_begin[c] + threadIdx.x;
-    const bool in = i < P.chunk_end[c];
-    const float x = in ? P.err_orig[i] : 0.0f;
-    const double s = fold256(in ? (double)x : 0.0, smd);
-    const float m = block_max256(in ? x : -3.4e38f, smf);
-    if (threadIdx.x == 0) {
-      P.part_sum[c] = s;
-      P.part_max[c] = m;
-      wlast = world_ticket(P, w, c1 - c0);
-    }
-    __syncthreads();
-    if (wlast) {
-      __threadfence();
-      double a = 0.0;
-      float mm = -3.4e38f;
-      for (int k = c0 + threadIdx.x; k < c1; k += 256) {
-        a = a + __ldcg(&P.part_sum[k]);
-        mm = fmaxf(mm, __ldcg(&P.part_max[k]));
-      }
-      const double sw = fold256(a, smd);
-      const float mx = maxr(block_max256(mm, smf), 0.0f);
-      if (threadIdx.x == 0) {
-        P.emax[w] = mx;
-        const int it = P.iters[w] + 1;
-        P.iters[w] = it;
-        const double na = P.n_active[w];
-        const float mean = (float)(sw / (na > 1.0 ? na : 1.0));
-        P.err_mean[w] = mean;
-        if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
-      }
-    }
-    ticket = wlast;
+// fold256's tree computed by one warp: value L of the 256 (group L / 32, lane L % 32) comes from value(L); each group
+// of 32 folds by the same shuffles (offsets 16..1), then the 8 group sums fold with offsets 4, 2, 1. Valid in lane 0.
+template <class F>
+__device__ __forceinline__ double fold256_warp(F value) {
+  const int lane = threadIdx.x & 31;
+  double s[8];
+#pragma unroll
+  for (int g = 0; g < 8; ++g) {
+    double v = value(32 * g + lane);
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+    s[g] = v;
   }
-  if (!ticket) return;
-  if (threadIdx.x == 0) glast = grid_ticket(P);
+#pragma unroll
+  for (int o = 4; o >= 1; o >>= 1)
+#pragma unroll
+    for (int l = 0; l < o; ++l) s[l] = s[l] + s[l + o];
+  return s[0];
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// The Jacobi iteration's stop test in one launch (k_chunk_sum, k_world_check and k_worklist fused), one warp per
+// 256-particle chunk (8 chunks per block): the warp folds its chunk in fold256's tree order (chunks of converged worlds
+// keep their partials); the last warp of a world to finish folds the world's partials in k_world_check's order and runs
+// its stop test (pressure.py:370-390); the block whose tickets complete the grid lists the worlds still iterating and
+// stores their count as the unconverged count. The sums are those of the separate kernels bit for bit. A block per
+// chunk instead (80k blocks on the pour workload) spent most of its time scheduling blocks. The world's last warp folds its
+// partials (its 32 lanes stand in for the 256 of k_world_check: value L sums partials L, L + 256, ... serially); a
+// block takes one grid ticket for all the worlds its warps completed (or that had converged and start in one of its
+// chunks), and the block whose tickets complete the grid lists the worlds still iterating.
+constexpr int CHECK_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * CHECK_WARPS) k_check_warps(DevP P) {
+  __shared__ int tickets[CHECK_WARPS];
+  __shared__ bool glast;
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const int c = blockIdx.x * CHECK_WARPS + wq;
+  int ticket = 0;
+  if (c < P.n_chunks) {
+    const int w = P.chunk_world[c];
+    const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
+    ticket = c == c0 ? 1 : 0;
+    if (!P.converged[w]) {
+      const int b = P.chunk_begin[c], e = P.chunk_end[c];
+      float m = -3.4e38f;
+      const double sum = fold256_warp([&](int L) -> double {
+        const int i = b + L;
+        const float x = i < e ? P.err_orig[i] : 0.0f;
+        if (i < e) m = fmaxf(m, x);
+        return i < e ? (double)x : 0.0;
+      });
+      m = warp_max(m);
+      bool last = false;
+      if (lane == 0) {
+        P.part_sum[c] = sum;
+        P.part_max[c] = m;
+        last = world_ticket(P, w, c1 - c0);
+      }
+      last = __shfl_sync(0xffffffffu, last, 0);
+      if (last) {
+        __threadfence();
+        float mm = -3.4e38f;
+        const double sw = fold256_warp([&](int L) -> double {
+          double a = 0.0;
+          for (int k = c0 + L; k < c1; k += 256) {
+            a = a + __ldcg(&P.part_sum[k]);
+            mm = fmaxf(mm, __ldcg(&P.part_max[k]));
+          }
+          return a;
+        });
+        const float mx = maxr(warp_max(mm), 0.0f);
+        if (lane == 0) {
+          P.emax[w] = mx;
+          const int it = P.iters[w] + 1;
+          P.iters[w] = it;
+          const double na = P.n_active[w];
+          const float mean = (float)(sw / (na > 1.0 ? na : 1.0));
+          P.err_mean[w] = mean;
+          if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+        }
+      }
+      ticket = last ? 1 : 0;
+    }
+  }
+  if (lane == 0) tickets[wq] = ticket;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int k = 0; k < CHECK_WARPS; ++k) t += tickets[k];
+    glast = false;
+    if (t > 0) {
+      __threadfence();
+      const unsigned before = atomicAdd(P.gdone, (unsigned)t);
+      glast = before + (unsigned)t == (unsigned)P.n_chunk_worlds;
+      if (glast) *P.gdone = 0u;
+    }
+  }
   __syncthreads();
   if (glast) {
     __threadfence();
@@ -2276,7 +2314,7 @@ __global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int b
   const int c = blockIdx.x;
   const int w = P.chunk_world[c];
   const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
-  bool ticket = c == c0;  // as in k_check_fused
+  bool ticket = c == c0;  // as in k_check_warps
   if (!P.converged[w]) {
     const int i = P.chunk_begin[c] + threadIdx.x;
     const bool in = i < P.chunk_end[c];
@@ -2371,7 +2409,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
     }
   }
   float ax, ay, az;
-  pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
+  pressure_accel<NB>(P, p, ax, ay, az);
   P.acc[p] = make_float4(ax, ay, az, 0.0f);
   float vx = ADF_FMA(dt, ax, vi.x), vy = ADF_FMA(dt, ay, vi.y), vz = ADF_FMA(dt, az, vi.z);
   // pressure.py:417-458: Coulomb friction of a lone particle on its walls after the update: the walls' push
