@@ -407,7 +407,11 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   prof_begin(s, 1, st);
   if (P.skin_on) {
     LAUNCH(s, k_skin_ref, blocks(n), BLOCK, st, P);
-    LAUNCH(s, k_skin_build, blocks(n, 128), 128, st, P);
+    {
+      const size_t smem = P.sup_cap <= SKIN_SMEM_CAP ? sizeof(int) * (size_t)P.sup_cap * SKIN_THREADS : 0;
+      k_skin_build<<<blocks(n, SKIN_THREADS), SKIN_THREADS, smem, st>>>(P);
+      ++s->launches;
+    }
     LAUNCH(s, k_skin_filter, blocks(n), BLOCK, st, P);
   } else if (s->K <= LU_ROW) {
     run_tk(s, TK_LISTS, st, P);
@@ -1096,6 +1100,8 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     CKC(cudaMemset(s->mass0, 0, 8 * W));
   }
   CKC(cudaGetLastError());
+  CKC(cudaFuncSetAttribute(k_skin_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(int) * (size_t)SKIN_SMEM_CAP * SKIN_THREADS)));
   CKC(cudaFuncSetAttribute(k_lists_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(int) * (size_t)s->K * LS_THREADS)));
   CKC(cudaHostAlloc((void**)&s->pinned, 2 * sizeof(int), cudaHostAllocDefault));

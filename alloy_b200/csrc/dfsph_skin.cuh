@@ -75,8 +75,14 @@ __device__ __forceinline__ void skin_insert(int* row, size_t stride, int& m, int
 
 // neighbors_skin.py:60-110 for the flagged worlds' liquid (sorted order): the superset row within h + s from the
 // cells within skin_reach, or, when it holds more than sup_cap entries, this step's plain radius-h row (from the 27
-// cells, as the plain build) and a forced rebuild next step.
-__global__ void __launch_bounds__(128) k_skin_build(DevP P) {
+// cells, as the plain build) and a forced rebuild next step. A row is sorted in the thread's column of the block's
+// shared buffer (sup_cap x SKIN_THREADS ids, when sup_cap <= SKIN_SMEM_CAP) and then copied out; larger capacities
+// sort in place in global memory.
+constexpr int SKIN_THREADS = 128;
+constexpr int SKIN_SMEM_CAP = 96;
+
+__global__ void __launch_bounds__(SKIN_THREADS) k_skin_build(DevP P) {
+  extern __shared__ int sbuf[];
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
@@ -89,7 +95,9 @@ __global__ void __launch_bounds__(128) k_skin_build(DevP P) {
   int cx, cy, cz;
   cell_coords(g, xi.x, xi.y, xi.z, cx, cy, cz);
   const int R = P.skin_reach, cap = P.sup_cap;
-  int* row = P.sup + s;
+  const bool in_smem = cap <= SKIN_SMEM_CAP;
+  int* row = in_smem ? sbuf + threadIdx.x : P.sup + s;
+  const size_t stride = in_smem ? (size_t)SKIN_THREADS : (size_t)P.n;
   int m = 0, total = 0;
   for (int z = max(cz - R, 0); z <= min(cz + R, g.nz - 1); ++z)
     for (int y = max(cy - R, 0); y <= min(cy + R, g.ny - 1); ++y)
@@ -100,11 +108,13 @@ __global__ void __launch_bounds__(128) k_skin_build(DevP P) {
           const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
           if (dot_plain(dx, dy, dz, dx, dy, dz) < P.skin_r2) {
             ++total;
-            skin_insert(row, P.n, m, cap, P.id_of[j]);
+            skin_insert(row, stride, m, cap, P.id_of[j]);
           }
         }
       });
   if (total <= cap) {
+    if (in_smem)
+      for (int k = 0; k < m; ++k) P.sup[(size_t)k * P.n + s] = row[(size_t)k * SKIN_THREADS];
     P.sup_cnt[s] = m;
     return;
   }
