@@ -112,7 +112,6 @@ struct DevP {
   float* kd_s;
   int* nbr;     // [K][n] sorted positions, ascending original id
   float4* nbrg;  // [K][n] (m_j grad W_ij = m_j F(r_ij) r_ij, bits of the row entry), written by k_density_alpha
-  float* nbrw;  // [K][n] kernel value W(r_ij) of each row entry, written by k_density_alpha, read by k_xsph
   int* cnt;
   // Boundary slots (boundary.py:36): slot b of sorted particle p at b * n + p of each array, nearest wall first.
   float4* slot_g;   // dPsi/dx (3), psi; with slot_cap 1, psi < 0: no slot
@@ -1365,7 +1364,6 @@ __global__ void __launch_bounds__(BLOCK, 3) k_density_alpha(DevP P) {
       float mj = xj.w;
       const float4 gm = mass_grad(mj, F, rx, ry, rz, j[u]);
       __stcs(P.nbrg + (size_t)(k + u) * P.n + p, gm);
-      __stcs(P.nbrw + (size_t)(k + u) * P.n + p, W);
       rho = ADF_FMA(mj, W, rho);
       float a = mj * inv_r0;
       Gx = ADF_FMA(inv_r0, gm.x, Gx);
@@ -2443,7 +2441,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
 // The output array becomes the velocity array for the rest of the step (the host swaps them), so boundary
 // particles carry their own velocity across: the wall advance in k_finish reads it.
 template <int NB>
-__global__ void __launch_bounds__(BLOCK, 3) k_xsph(DevP P) {
+__global__ void __launch_bounds__(BLOCK, 2) k_xsph(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = P.nfw[0];
   if (p >= nf) {
@@ -2469,25 +2467,25 @@ __global__ void __launch_bounds__(BLOCK, 3) k_xsph(DevP P) {
     int cn = P.cnt[p];
     for (int k = 0; k < cn; k += NB) {
       int j[NB];
-      float wb[NB];
       load_row_batch(P, p, cn, k, j);
-#pragma unroll
-      for (int u = 0; u < NB; ++u) wb[u] = (k + u < cn) ? __ldcs(P.nbrw + (size_t)(k + u) * P.n + p) : 0.0f;
-      float4 vb[NB];
-      float rb[NB], mb[NB];
+      float4 vb[NB], xb[NB];
+      float rb[NB];
 #pragma unroll
       for (int u = 0; u < NB; ++u) {
         vb[u] = P.vel[j[u]];
         rb[u] = P.ratio[j[u]];
-        mb[u] = reinterpret_cast<const float*>(P.pos)[4 * (size_t)j[u] + 3];  // mass (pos.w) only
+        xb[u] = P.pos[j[u]];
       }
 #pragma unroll
       for (int u = 0; u < NB; ++u) {
         if (k + u >= cn) break;
-        float4 vj = vb[u];
+        float4 vj = vb[u], xj = xb[u];
         float rho_bar = 0.5f * (rho_i + rb[u] * vj.w);
         if (rho_bar > 0.0f) {
-          float cw = (mb[u] / rho_bar) * wb[u];  // W(r_ij) as k_density_alpha evaluated it for this entry
+          const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+          float W, F;
+          wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);  // the value k_density_alpha had for this entry
+          float cw = (xj.w / rho_bar) * W;
           cx = ADF_FMA(cw, vj.x - vi.x, cx);
           cy = ADF_FMA(cw, vj.y - vi.y, cy);
           cz = ADF_FMA(cw, vj.z - vi.z, cz);

@@ -15,6 +15,8 @@ captured graph. The held particles at build (phase ``PHASE_HELD``) are the reser
 
 from __future__ import annotations
 
+import weakref
+
 import numpy as np
 import torch
 
@@ -26,7 +28,7 @@ class SPHPort:
     """The port of one ``SolverDFSPH`` (``solver.port``)."""
 
     def __init__(self, solver):
-        self.solver = solver
+        self.solver = weakref.proxy(solver)  # no reference cycle: the solver's device memory goes with the solver
         W = solver.world_count
         n = solver.n
         ph = solver._phase0.cpu().numpy() if n else np.zeros(0, np.int8)
