@@ -113,6 +113,7 @@ struct adf_solver {
   std::vector<int> world_cells_h;
   int total_cells = 0, n_keys = 0, n_tiles = 0;
   int max_items = 0;  // grid of the pressure iterations: an upper bound of their work items (k_worklist)
+  int max_world_chunks = 0;  // the largest world's 256-particle chunks (chooses the stop-test kernel)
   DevP d{};
   std::vector<void*> owned;
   int* world_cells = nullptr;
@@ -505,10 +506,13 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   LAUNCH(s, k_cg_direction, blocks(n), BLOCK, st, P);
 }
 
-// The stop test of an iteration and the next iteration's work list (one launch: k_check_warps).
+// The stop test of an iteration and the next iteration's work list (one launch: k_check_warps or k_check_fused).
 void check_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   if (P.n_chunks > 0) {
-    LAUNCH(s, k_check_warps, (P.n_chunks + CHECK_WARPS - 1) / CHECK_WARPS, 32 * CHECK_WARPS, st, P);
+    if (s->max_world_chunks <= WARP_FOLD_MAX_CHUNKS)
+      LAUNCH(s, k_check_warps, (P.n_chunks + CHECK_WARPS - 1) / CHECK_WARPS, 32 * CHECK_WARPS, st, P);
+    else
+      LAUNCH(s, k_check_fused, P.n_chunks, 256, st, P);
   } else {
     cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st);
     if (s->W > 0) LAUNCH(s, k_worklist, 1, 1024, st, P);
@@ -860,6 +864,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     cs.push_back((int)cb.size());
   }
   d.n_chunks = (int)cb.size();
+  for (size_t k = 0; k + 1 < cs.size(); ++k) s->max_world_chunks = std::max(s->max_world_chunks, cs[k + 1] - cs[k]);
   d.n_chunk_worlds = 0;
   for (size_t k = 0; k + 1 < cs.size(); ++k) d.n_chunk_worlds += cs[k + 1] > cs[k] ? 1 : 0;
   // sum over worlds of ceil(liquid_w / 256) <= n / 256 + W, whatever the worlds' sizes

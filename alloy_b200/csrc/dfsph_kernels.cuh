@@ -2191,6 +2191,64 @@ __device__ __forceinline__ bool grid_ticket(const DevP& P) {
   return last;
 }
 
+// The Jacobi iteration's stop test in one launch (k_chunk_sum, k_world_check and k_worklist fused): block c folds
+// chunk c (chunks of converged worlds keep their partials); the last block of a world to finish folds the world's
+// partials in the same fixed tree order as k_world_check and runs its stop test (pressure.py:370-390); the last block
+// of the grid lists the worlds still iterating for the next iteration and stores their count as the unconverged
+// count. The sums are those of the separate kernels bit for bit; only the launches are fewer. Used when a world
+// has more than WARP_FOLD_MAX_CHUNKS chunks (k_check_warps otherwise), where 256 threads fold its partials in parallel.
+__global__ void __launch_bounds__(256) k_check_fused(DevP P) {
+  __shared__ double smd[8];
+  __shared__ float smf[8];
+  __shared__ bool wlast, glast;
+  const int c = blockIdx.x;
+  const int w = P.chunk_world[c];
+  const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
+  bool ticket = c == c0;  // the world's grid ticket: its first chunk's block if it had converged, else its last block
+  if (!P.converged[w]) {
+    const int i = P.chunk_begin[c] + threadIdx.x;
+    const bool in = i < P.chunk_end[c];
+    const float x = in ? P.err_orig[i] : 0.0f;
+    const double s = fold256(in ? (double)x : 0.0, smd);
+    const float m = block_max256(in ? x : -3.4e38f, smf);
+    if (threadIdx.x == 0) {
+      P.part_sum[c] = s;
+      P.part_max[c] = m;
+      wlast = world_ticket(P, w, c1 - c0);
+    }
+    __syncthreads();
+    if (wlast) {
+      __threadfence();
+      double a = 0.0;
+      float mm = -3.4e38f;
+      for (int k = c0 + threadIdx.x; k < c1; k += 256) {
+        a = a + __ldcg(&P.part_sum[k]);
+        mm = fmaxf(mm, __ldcg(&P.part_max[k]));
+      }
+      const double sw = fold256(a, smd);
+      const float mx = maxr(block_max256(mm, smf), 0.0f);
+      if (threadIdx.x == 0) {
+        P.emax[w] = mx;
+        const int it = P.iters[w] + 1;
+        P.iters[w] = it;
+        const double na = P.n_active[w];
+        const float mean = (float)(sw / (na > 1.0 ? na : 1.0));
+        P.err_mean[w] = mean;
+        if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+      }
+    }
+    ticket = wlast;
+  }
+  if (!ticket) return;
+  if (threadIdx.x == 0) glast = grid_ticket(P);
+  __syncthreads();
+  if (glast) {
+    __threadfence();
+    const int listed = build_worklist(P, true);
+    if (threadIdx.x == 0) *P.n_unconv = listed;
+  }
+}
+
 // fold256's tree computed by one warp: value L of the 256 (group L / 32, lane L % 32) comes from value(L); each group
 // of 32 folds by the same shuffles (offsets 16..1), then the 8 group sums fold with offsets 4, 2, 1. Valid in lane 0.
 template <class F>
@@ -2217,16 +2275,19 @@ __device__ __forceinline__ float warp_max(float v) {
   return __shfl_sync(0xffffffffu, v, 0);
 }
 
-// The Jacobi iteration's stop test in one launch (k_chunk_sum, k_world_check and k_worklist fused), one warp per
-// 256-particle chunk (8 chunks per block): the warp folds its chunk in fold256's tree order (chunks of converged worlds
-// keep their partials); the last warp of a world to finish folds the world's partials in k_world_check's order and runs
-// its stop test (pressure.py:370-390); the block whose tickets complete the grid lists the worlds still iterating and
-// stores their count as the unconverged count. The sums are those of the separate kernels bit for bit. A block per
-// chunk instead (80k blocks on the pour workload) spent most of its time scheduling blocks. The world's last warp folds its
+// k_check_fused with one warp per 256-particle chunk (8 chunks per block), for models whose worlds have at most
+// WARP_FOLD_MAX_CHUNKS chunks (many small worlds): the warp folds its chunk in fold256's tree order (chunks of converged
+// worlds keep their partials); the last warp of a world to finish folds the world's partials in k_world_check's order
+// and runs its stop test (pressure.py:370-390); the block whose tickets complete the grid lists the worlds still
+// iterating and stores their count as the unconverged count. The sums are those of the separate kernels bit for bit.
+// A block per chunk (80k blocks on the 4,096-world pour) spent most of its time scheduling blocks; a warp folding a
+// large world's thousands of partials alone (the 1M dam break's 4,096) waits on them serially. The world's last warp
+// folds its
 // partials (its 32 lanes stand in for the 256 of k_world_check: value L sums partials L, L + 256, ... serially); a
 // block takes one grid ticket for all the worlds its warps completed (or that had converged and start in one of its
 // chunks), and the block whose tickets complete the grid lists the worlds still iterating.
 constexpr int CHECK_WARPS = 8;
+constexpr int WARP_FOLD_MAX_CHUNKS = 256;  // a lane folds at most one partial per group of the 256-lane tree
 
 __global__ void __launch_bounds__(32 * CHECK_WARPS) k_check_warps(DevP P) {
   __shared__ int tickets[CHECK_WARPS];
@@ -2312,7 +2373,7 @@ __global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int b
   const int c = blockIdx.x;
   const int w = P.chunk_world[c];
   const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
-  bool ticket = c == c0;  // as in k_check_warps
+  bool ticket = c == c0;  // as in k_check_fused
   if (!P.converged[w]) {
     const int i = P.chunk_begin[c] + threadIdx.x;
     const bool in = i < P.chunk_end[c];
