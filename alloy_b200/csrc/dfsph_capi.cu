@@ -892,7 +892,8 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.kv_s, n);
   rc |= s->alloc(&d.kd_s, n);
   rc |= s->alloc(&d.nbr, (size_t)s->K * n);
-  rc |= s->alloc(&d.nbrg, (size_t)s->K * n);
+  rc |= s->alloc(&d.nbrjf, (size_t)s->K * n);
+  rc |= s->alloc(&d.nbrw, (size_t)s->K * n);
   rc |= s->alloc(&d.cnt, n);
   rc |= s->alloc(&d.slot_g, (size_t)d.slot_cap * n);
   rc |= s->alloc(&d.slot_vb, (size_t)d.slot_cap * n);

@@ -111,7 +111,8 @@ struct DevP {
   float* kv_s;
   float* kd_s;
   int* nbr;     // [K][n] sorted positions, ascending original id
-  float4* nbrg;  // [K][n] (m_j grad W_ij = m_j F(r_ij) r_ij, bits of the row entry), written by k_density_alpha
+  int2* nbrjf;  // [K][n] (row entry, bits of its gradient factor F(r_ij)), written by k_density_alpha
+  float* nbrw;  // [K][n] kernel value W(r_ij) of each row entry, written by k_density_alpha, read by k_xsph
   int* cnt;
   // Boundary slots (boundary.py:36): slot b of sorted particle p at b * n + p of each array, nearest wall first.
   float4* slot_g;   // dPsi/dx (3), psi; with slot_cap 1, psi < 0: no slot
@@ -1314,30 +1315,24 @@ __device__ __forceinline__ void load_row_batch(const DevP& P, int p, int c, int 
   for (int u = 0; u < NB; ++u) j[u] = (k + u < c) ? __ldcs(row + (size_t)(k + u) * P.n) : p;
 }
 
-// m_j grad W_ij = (m_j F(r)) r_ij for r_ij = x_i - x_j, F = W'(r) / r (kernels.py:59-77 gives grad W = r_ij F; the
-// mass is folded in once per pair). The oracle's mass_grad is the same expression.
-__device__ __forceinline__ float4 mass_grad(float mj, float F, float rx, float ry, float rz, int j) {
-  const float s = mj * F;
-  return make_float4(s * rx, s * ry, s * rz, __int_as_float(j));
-}
-
-// Row entries with their pair gradient m_j grad W_ij (stored by k_density_alpha) in one 16-byte load: the pressure
-// loops then gather only the neighbour's field they combine (velocity, kappa / rho0 or acceleration), not its
-// position and mass, and the values are those of the formula, so every sum is unchanged.
+// Row entries with their gradient factor F(r_ij) (the value wf() gives for the pair, stored by k_density_alpha) in
+// one 8-byte load: the later loops read F instead of re-evaluating sqrt, branches and a division; the value is the
+// same, so every sum is unchanged.
 template <int NB>
-__device__ __forceinline__ void load_row_batch_g(const DevP& P, int p, int c, int k, int (&j)[NB], float4 (&g)[NB]) {
-  const float4* row = P.nbrg + p;
+__device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, int k, int (&j)[NB], float (&f)[NB]) {
+  const int2* row = P.nbrjf + p;
 #pragma unroll
   for (int u = 0; u < NB; ++u) {
-    g[u] = (k + u < c) ? __ldcs(row + (size_t)(k + u) * P.n) : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(p));
-    j[u] = __float_as_int(g[u].w);
+    int2 e = (k + u < c) ? __ldcs(row + (size_t)(k + u) * P.n) : make_int2(p, 0);
+    j[u] = e.x;
+    f[u] = __int_as_float(e.y);
   }
 }
 
 // ------------------------------------------------------------------------------------------ density, factor
 // pressure.py:144-193
 template <int NB>
-__global__ void __launch_bounds__(BLOCK, 3) k_density_alpha(DevP P) {
+__global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   float4 xi = P.pos[p];
@@ -1361,14 +1356,15 @@ __global__ void __launch_bounds__(BLOCK, 3) k_density_alpha(DevP P) {
       float r2 = dot_plain(rx, ry, rz, rx, ry, rz);
       float W, F;
       wf(P.kc, r2, W, F);
+      __stcs(P.nbrjf + (size_t)(k + u) * P.n + p, make_int2(j[u], __float_as_int(F)));
+      __stcs(P.nbrw + (size_t)(k + u) * P.n + p, W);
       float mj = xj.w;
-      const float4 gm = mass_grad(mj, F, rx, ry, rz, j[u]);
-      __stcs(P.nbrg + (size_t)(k + u) * P.n + p, gm);
       rho = ADF_FMA(mj, W, rho);
       float a = mj * inv_r0;
-      Gx = ADF_FMA(inv_r0, gm.x, Gx);
-      Gy = ADF_FMA(inv_r0, gm.y, Gy);
-      Gz = ADF_FMA(inv_r0, gm.z, Gz);
+      float aF = a * F;
+      Gx = ADF_FMA(aF, rx, Gx);
+      Gy = ADF_FMA(aF, ry, Gy);
+      Gz = ADF_FMA(aF, rz, Gz);
       sq = ADF_FMA(bi * a, (F * F) * r2, sq);
     }
   }
@@ -1400,22 +1396,28 @@ template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
+  float4 xi = P.pos[p];
   float4 vi = P.vel[p];
   float inv_r0 = 1.0f / vi.w;
   float rate = 0.0f;
   int c = P.cnt[p];
   for (int k = 0; k < c; k += NB) {
     int j[NB];
-    float4 gb[NB];
-    load_row_batch_g(P, p, c, k, j, gb);
-    float4 vb[NB];
+    float fb[NB];
+    load_row_batch_f(P, p, c, k, j, fb);
+    float4 xb[NB], vb[NB];
 #pragma unroll
-    for (int u = 0; u < NB; ++u) vb[u] = P.vel[j[u]];
+    for (int u = 0; u < NB; ++u) {
+      xb[u] = P.pos[j[u]];
+      vb[u] = P.vel[j[u]];
+    }
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
       if (k + u >= c) break;
-      const float4 vj = vb[u], g = gb[u];
-      rate = ADF_FMA(inv_r0, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, g.x, g.y, g.z), rate);
+      float4 xj = xb[u], vj = vb[u];
+      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      float aF = (xj.w * inv_r0) * fb[u];
+      rate = ADF_FMA(aF, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, rx, ry, rz), rate);
     }
   }
   const int ns = slot_count(P, p);
@@ -1662,24 +1664,30 @@ __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
 // ------------------------------------------------------------------------------------------ Jacobi sweep
 // pressure.py:264-291: a_i = -sum_j m_j (k_i/rho0_i + k_j/rho0_j) grad W_ij - k_i sum_b dPsi_b
 template <int NB>
-__device__ __forceinline__ void pressure_accel(const DevP& P, int p, float& ax, float& ay, float& az) {
+__device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, float& ax, float& ay, float& az) {
   float ki = P.kr[p];
   ax = ay = az = 0.0f;
   int c = P.cnt[p];
   for (int k = 0; k < c; k += NB) {
     int j[NB];
-    float4 gb[NB];
-    load_row_batch_g(P, p, c, k, j, gb);
+    float fb[NB];
+    load_row_batch_f(P, p, c, k, j, fb);
+    float4 xb[NB];
     float kb[NB];
 #pragma unroll
-    for (int u = 0; u < NB; ++u) kb[u] = P.kr[j[u]];
+    for (int u = 0; u < NB; ++u) {
+      xb[u] = P.pos[j[u]];
+      kb[u] = P.kr[j[u]];
+    }
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
       if (k + u >= c) break;
-      const float cc = ki + kb[u];
-      ax = ADF_FMA(-cc, gb[u].x, ax);
-      ay = ADF_FMA(-cc, gb[u].y, ay);
-      az = ADF_FMA(-cc, gb[u].z, az);
+      float4 xj = xb[u];
+      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      float cF = (xj.w * (ki + kb[u])) * fb[u];
+      ax = ADF_FMA(-cF, rx, ax);
+      ay = ADF_FMA(-cF, ry, ay);
+      az = ADF_FMA(-cF, rz, az);
     }
   }
   const int ns = slot_count(P, p);
@@ -1698,7 +1706,7 @@ __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
   if (!work_item(P, b, e)) return;
   for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
     float ax, ay, az;
-    pressure_accel<NB>(P, p, ax, ay, az);
+    pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
     P.acc[p] = make_float4(ax, ay, az, 0.0f);
   }
 }
@@ -1707,21 +1715,27 @@ __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
 // pressure.py:294-310: Ar_i of the accelerations in P.acc (the matrix-free product, before the compliance term)
 template <int NB>
 __device__ __forceinline__ float accel_divergence(const DevP& P, int p, float inv_r0) {
+  float4 xi = P.pos[p];
   float4 ai = P.acc[p];
   float ar = 0.0f;
   int c = P.cnt[p];
   for (int k = 0; k < c; k += NB) {
     int j[NB];
-    float4 gb[NB];
-    load_row_batch_g(P, p, c, k, j, gb);
-    float4 ab[NB];
+    float fb[NB];
+    load_row_batch_f(P, p, c, k, j, fb);
+    float4 xb[NB], ab[NB];
 #pragma unroll
-    for (int u = 0; u < NB; ++u) ab[u] = P.acc[j[u]];
+    for (int u = 0; u < NB; ++u) {
+      xb[u] = P.pos[j[u]];
+      ab[u] = P.acc[j[u]];
+    }
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
       if (k + u >= c) break;
-      const float4 aj = ab[u], g = gb[u];
-      ar = ADF_FMA(inv_r0, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, g.x, g.y, g.z), ar);
+      float4 xj = xb[u], aj = ab[u];
+      float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      float aF = (xj.w * inv_r0) * fb[u];
+      ar = ADF_FMA(aF, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz), ar);
     }
   }
   const int ns = slot_count(P, p);
@@ -1783,7 +1797,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel(DevP P, const float* vec, co
   Q.kappa = const_cast<float*>(vec);
   Q.kr = const_cast<float*>(vr);
   float ax, ay, az;
-  pressure_accel<NB>(Q, p, ax, ay, az);
+  pressure_accel<NB>(Q, p, P.pos[p], ax, ay, az);
   P.acc[p] = make_float4(ax, ay, az, 0.0f);
 }
 
@@ -1827,10 +1841,10 @@ __device__ __forceinline__ Team team_of(int& p) {
   return tm;
 }
 
-__device__ __forceinline__ float4 row_entry(const DevP& P, int p, int k) { return __ldcs(P.nbrg + p + (size_t)k * P.n); }
+__device__ __forceinline__ int2 row_entry(const DevP& P, int p, int k) { return __ldcs(P.nbrjf + p + (size_t)k * P.n); }
 
 // pressure_accel with the fields of Q (kappa, kr), valid in the team's first lane
-__device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, const Team& tm, float& ax, float& ay,
+__device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, float4 xi, const Team& tm, float& ax, float& ay,
                                                     float& az) {
   const float ki = Q.kr[p];
   ax = ay = az = 0.0f;
@@ -1842,12 +1856,13 @@ __device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, const 
       const int k = k0 + u * TL + tm.t;
       cf[u] = rx[u] = ry[u] = rz[u] = 0.0f;
       if (k < c) {
-        const float4 e = row_entry(Q, p, k);
-        const float kj = Q.kr[__float_as_int(e.w)];
-        rx[u] = e.x;
-        ry[u] = e.y;
-        rz[u] = e.z;
-        cf[u] = ki + kj;
+        const int2 e = row_entry(Q, p, k);
+        const float4 xj = Q.pos[e.x];
+        const float kj = Q.kr[e.x];
+        rx[u] = xi.x - xj.x;
+        ry[u] = xi.y - xj.y;
+        rz[u] = xi.z - xj.z;
+        cf[u] = (xj.w * (ki + kj)) * __int_as_float(e.y);
       }
     }
 #pragma unroll
@@ -1876,6 +1891,7 @@ __device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, const 
 
 // accel_divergence, valid in the team's first lane
 __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, float inv_r0, const Team& tm) {
+  const float4 xi = P.pos[p];
   const float4 ai = P.acc[p];
   float ar = 0.0f;
   const int c = P.cnt[p];
@@ -1886,10 +1902,11 @@ __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, flo
       const int k = k0 + u * TL + tm.t;
       af[u] = d[u] = 0.0f;
       if (k < c) {
-        const float4 e = row_entry(P, p, k);
-        const float4 aj = P.acc[__float_as_int(e.w)];
-        af[u] = inv_r0;
-        d[u] = dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, e.x, e.y, e.z);
+        const int2 e = row_entry(P, p, k);
+        const float4 xj = P.pos[e.x], aj = P.acc[e.x];
+        const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+        af[u] = (xj.w * inv_r0) * __int_as_float(e.y);
+        d[u] = dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz);
       }
     }
 #pragma unroll
@@ -1918,7 +1935,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* ve
   Q.kappa = const_cast<float*>(vec);
   Q.kr = const_cast<float*>(vr);
   float ax, ay, az;
-  pressure_accel_team(Q, p, tm, ax, ay, az);
+  pressure_accel_team(Q, p, P.pos[p], tm, ax, ay, az);
   if (tm.t == 0) P.acc[p] = make_float4(ax, ay, az, 0.0f);
 }
 
@@ -2468,7 +2485,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
     }
   }
   float ax, ay, az;
-  pressure_accel<NB>(P, p, ax, ay, az);
+  pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
   P.acc[p] = make_float4(ax, ay, az, 0.0f);
   float vx = ADF_FMA(dt, ax, vi.x), vy = ADF_FMA(dt, ay, vi.y), vz = ADF_FMA(dt, az, vi.z);
   // pressure.py:417-458: Coulomb friction of a lone particle on its walls after the update: the walls' push
@@ -2502,7 +2519,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
 // The output array becomes the velocity array for the rest of the step (the host swaps them), so boundary
 // particles carry their own velocity across: the wall advance in k_finish reads it.
 template <int NB>
-__global__ void __launch_bounds__(BLOCK, 2) k_xsph(DevP P) {
+__global__ void __launch_bounds__(BLOCK, 3) k_xsph(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = P.nfw[0];
   if (p >= nf) {
@@ -2528,25 +2545,25 @@ __global__ void __launch_bounds__(BLOCK, 2) k_xsph(DevP P) {
     int cn = P.cnt[p];
     for (int k = 0; k < cn; k += NB) {
       int j[NB];
+      float wb[NB];
       load_row_batch(P, p, cn, k, j);
-      float4 vb[NB], xb[NB];
-      float rb[NB];
+#pragma unroll
+      for (int u = 0; u < NB; ++u) wb[u] = (k + u < cn) ? __ldcs(P.nbrw + (size_t)(k + u) * P.n + p) : 0.0f;
+      float4 vb[NB];
+      float rb[NB], mb[NB];
 #pragma unroll
       for (int u = 0; u < NB; ++u) {
         vb[u] = P.vel[j[u]];
         rb[u] = P.ratio[j[u]];
-        xb[u] = P.pos[j[u]];
+        mb[u] = reinterpret_cast<const float*>(P.pos)[4 * (size_t)j[u] + 3];  // mass (pos.w) only
       }
 #pragma unroll
       for (int u = 0; u < NB; ++u) {
         if (k + u >= cn) break;
-        float4 vj = vb[u], xj = xb[u];
+        float4 vj = vb[u];
         float rho_bar = 0.5f * (rho_i + rb[u] * vj.w);
         if (rho_bar > 0.0f) {
-          const float rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-          float W, F;
-          wf(P.kc, dot_plain(rx, ry, rz, rx, ry, rz), W, F);  // the value k_density_alpha had for this entry
-          float cw = (xj.w / rho_bar) * W;
+          float cw = (mb[u] / rho_bar) * wb[u];  // W(r_ij) as k_density_alpha evaluated it for this entry
           cx = ADF_FMA(cw, vj.x - vi.x, cx);
           cy = ADF_FMA(cw, vj.y - vi.y, cy);
           cz = ADF_FMA(cw, vj.z - vi.z, cz);

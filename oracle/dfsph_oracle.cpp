@@ -64,12 +64,6 @@ template <class R> inline V3<R> sub(V3<R> a, V3<R> b) { return {a.x - b.x, a.y -
 template <class R> inline R dot_plain(V3<R> a, V3<R> b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
 // fused dot used everywhere else
 template <class R> inline R dotf(V3<R> a, V3<R> b) { return fma_(a.z, b.z, fma_(a.y, b.y, a.x * b.x)); }
-// m_j grad W_ij = (m_j F(r)) r_ij, F = W'(r) / r: the pair term every pressure loop reads (kernels.py:59-77 gives
-// grad W = r_ij F; the mass is folded in once per pair)
-template <class R> inline V3<R> mass_grad(R mj, R F, V3<R> rv) {
-  const R s = mj * F;
-  return {s * rv.x, s * rv.y, s * rv.z};
-}
 
 struct OrcParams {
   int kind;
@@ -695,10 +689,10 @@ template <class R> struct Solver {
         R mj = R(mass[j]);
         rho = fma_(mj, Wv, rho);
         R a = mj * inv_r0;
-        const V3<R> gm = mass_grad(mj, F, rv);
-        G.x = fma_(inv_r0, gm.x, G.x);
-        G.y = fma_(inv_r0, gm.y, G.y);
-        G.z = fma_(inv_r0, gm.z, G.z);
+        R aF = a * F;
+        G.x = fma_(aF, rv.x, G.x);
+        G.y = fma_(aF, rv.y, G.y);
+        G.z = fma_(aF, rv.z, G.z);
         sq = fma_(bi * a, (F * F) * r2, sq);
       }
       R psi = R(0), lam = R(0);  // boundary slots, nearest first; lam: the opposing-wall compliance
@@ -737,7 +731,8 @@ template <class R> struct Solver {
         V3<R> rv = sub(xi, q[j]);
         R Wv, F;
         wf(kc, dot_plain(rv, rv), Wv, F);
-        rate = fma_(inv_r0, dotf(sub(vi, v[j]), mass_grad(R(mass[j]), F, rv)), rate);
+        R aF = (R(mass[j]) * inv_r0) * F;
+        rate = fma_(aF, dotf(sub(vi, v[j]), rv), rate);
       }
       for (int b = 0; b < s_cnt[i]; ++b) {
         const size_t o = (size_t)i * NS + b;
@@ -777,11 +772,10 @@ template <class R> struct Solver {
       V3<R> rv = sub(xi, q[j]);
       R Wv, F;
       wf(kc, dot_plain(rv, rv), Wv, F);
-      const V3<R> gm = mass_grad(R(mass[j]), F, rv);
-      const R c = ki + kr[j];
-      a.x = fma_(-c, gm.x, a.x);
-      a.y = fma_(-c, gm.y, a.y);
-      a.z = fma_(-c, gm.z, a.z);
+      R cF = (R(mass[j]) * (ki + kr[j])) * F;
+      a.x = fma_(-cF, rv.x, a.x);
+      a.y = fma_(-cF, rv.y, a.y);
+      a.z = fma_(-cF, rv.z, a.z);
     }
     for (int b = 0; b < s_cnt[i]; ++b) {
       const R k = kvec[i];
@@ -822,7 +816,8 @@ template <class R> struct Solver {
       V3<R> rv = sub(xi, q[j]);
       R Wv, F;
       wf(kc, dot_plain(rv, rv), Wv, F);
-      ar = fma_(inv_r0, dotf(sub(ai, acc[j]), mass_grad(R(mass[j]), F, rv)), ar);
+      R aF = (R(mass[j]) * inv_r0) * F;
+      ar = fma_(aF, dotf(sub(ai, acc[j]), rv), ar);
     }
     for (int b = 0; b < s_cnt[i]; ++b) ar = ar + dotf(ai, s_g[(size_t)i * NS + b]);
     return ar;
