@@ -27,7 +27,16 @@ struct WarmSrc {
   float* pred_kv;
   float* pred_kd;
   int n;
+  const int* world_s;  // world of each sorted liquid particle
+  const int* need;     // [W] worlds that need predictions this step (null: all)
   __device__ int rows() const { return n; }
+  // a tile of sorted particles [r0, r1) spans worlds world_s[r0] .. world_s[r1 - 1] (worlds are contiguous)
+  __device__ bool skip_tile(int r0, int r1) const {
+    if (!need || r1 <= r0) return false;
+    for (int w = world_s[r0]; w <= world_s[r1 - 1]; ++w)
+      if (need[w]) return false;
+    return true;
+  }
   __device__ void features(int row, float (&f)[16]) const {
     const float4* p = reinterpret_cast<const float4*>(feat + (size_t)row * 16);
 #pragma unroll
@@ -46,7 +55,7 @@ struct WarmSrc {
 };
 
 __global__ void __launch_bounds__(mlp::TILE) k_mlp_warm(DevP P, mlp::Net net) {
-  WarmSrc s{P.feat, P.pred_kv, P.pred_kd, P.nfw[0]};
+  WarmSrc s{P.feat, P.pred_kv, P.pred_kd, P.nfw[0], P.world_s, P.warm_need};
   mlp::forward_rows(net, s);
 }
 
@@ -150,6 +159,7 @@ struct adf_solver {
   // scratch of the between-step calls (adf_energy, adf_stable_dt)
   float* energy_max = nullptr;
   int *cw2 = nullptr, *cseg2 = nullptr, *n_cw2 = nullptr;  // work list of the learned start's first sweep
+  int* warm_need = nullptr;  // [W] worlds that evaluate the learned start in this step (k_warm_need)
   int* speed_bits = nullptr;
   // host side of the iteration loop
   int* pinned = nullptr;
@@ -654,6 +664,10 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
   if (warm) CK(cudaMemsetAsync(P.err2, 0, sizeof(float) * n, st));
   CK(cudaMemsetAsync(P.n_unconv, 0, sizeof(int), st));
   P.feat_on = (first && (s->warm_on || s->feat_rec)) ? 1 : 0;
+  // under the judge only the worlds that evaluate the learned start in this step need features and predictions
+  const bool subset = warm && first && s->judge && !s->cg && !s->feat_rec;
+  P.warm_need = subset ? s->warm_need : nullptr;
+  if (subset) LAUNCH(s, k_warm_need, blocks(W), BLOCK, st, P, s->warm_need);
   prof_begin(s, 4, st);
   run_tk(s, TK_SOLVE_INIT, st, P);
   prof_end(s, st);
@@ -1410,6 +1424,7 @@ static int ensure_warm(adf_solver* s) {
   rc |= s->alloc(&s->cw2, W);
   rc |= s->alloc(&s->cseg2, (size_t)W + 1);
   rc |= s->alloc(&s->n_cw2, 1);
+  rc |= s->alloc(&s->warm_need, W);
   rc |= s->alloc(&d.sum_c, W);
   rc |= s->alloc(&d.sum_l, W);
   rc |= s->alloc(&d.max_c, W);

@@ -214,6 +214,7 @@ struct DevP {
   int* probe_skip;  // [W] 1: this solve does not evaluate the learned start in the world
   int* probe_gap;   // [2][W] solves between evaluations (per solve kind)
   int* probe_wait;  // [2][W] solves of this kind left before the next evaluation
+  const int* warm_need;  // [W] worlds whose learned start is evaluated in one of this step's solves (null: all)
   // projected preconditioned CG (krylov.py; null unless the CG pressure solver is selected)
   float* cg_pd;     // search direction p, and p / rho0 (sorted)
   float* cg_pdr;
@@ -1477,7 +1478,7 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   P.lower[p] = lb;
   P.kappa[p] = kap;
   P.kr[p] = kap / vi.w;
-  if (P.feat_on) {  // warm-start network features (their order is documented in solvers/sph/warmstart.py)
+  if (P.feat_on && (!P.warm_need || P.warm_need[P.world_s[p]])) {  // warm-start network features (order: warmstart.py)
     const float ratio = P.ratio[p], al = P.alpha[p], kvp = P.kv_s[p], kdp = P.kd_s[p];
     const float drate = dt * rate;
     const bool on = ns > 0;  // the nearest wall's slot
@@ -1558,6 +1559,15 @@ __global__ void k_choose_start(DevP P) {
     P.probe_gap[o] = gap;
     P.probe_wait[o] = gap - 1;
   }
+}
+
+// Worlds that evaluate the learned start in either solve of this step (their schedules wait 0 solves): only their
+// particles need features and predictions.
+__global__ void k_warm_need(DevP P, int* need) {
+  pdl_entry();
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W) return;
+  need[w] = (P.n_active[w] > 0.0 && (P.probe_wait[w] == 0 || P.probe_wait[P.W + w] == 0)) ? 1 : 0;
 }
 
 // The masked worlds' schedules back to "evaluate at the next solve".
