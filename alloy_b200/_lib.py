@@ -23,8 +23,7 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs", "adf_add_emitters",
            "adf_prime", "adf_iteration_work", "adf_set_tuned_config", "adf_get_state_storage", "adf_port_take",
            "adf_port_emit", "adf_energy", "adf_stable_dt", "adf_skin_flags",
-           "adf_add_patch_emitter", "adf_trigger", "adf_mlp_set_wait_limit", "adf_mlp_clear_status",
-           "adf_set_programmatic_launch")
+           "adf_add_patch_emitter", "adf_trigger", "adf_mlp_set_wait_limit", "adf_mlp_clear_status")
 TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph", "lists")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
@@ -142,7 +141,6 @@ def lib() -> C.CDLL:
     L.adf_trigger.argtypes = [P, C.c_int, vp, C.c_int, vp]
     L.adf_mlp_set_wait_limit.argtypes = [P, C.c_uint32]
     L.adf_mlp_clear_status.argtypes = [P]
-    L.adf_set_programmatic_launch.argtypes = [P, C.c_int]
     for name in EXPORTS:
         if name not in ("adf_destroy", "adf_last_error", "adf_kernel_launches", "adf_mlp_destroy"):
             getattr(L, name).restype = C.c_int

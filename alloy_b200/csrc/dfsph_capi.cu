@@ -190,7 +190,6 @@ struct adf_solver {
   // learned warm start (adf_set_warm_model) and feature recording (adf_set_feature_recording)
   bool warm_on = false, feat_rec = false, warm_alloc = false, judge = true;
   bool cg = false;  // projected preconditioned CG pressure solve (adf_params.cg)
-  bool pdl = true;  // launch with programmatic stream serialization (adf_set_programmatic_launch)
   bool cg_team = false;  // CG products by teams of TL lanes per particle (models of at most CG_TEAM_MAX particles)
   __nv_bfloat16 *mw1 = nullptr, *mw2 = nullptr;
   float *mparams = nullptr, *mnorm = nullptr;
@@ -214,33 +213,10 @@ struct adf_solver {
 
 namespace {
 
-// Launches of the library's kernels: with programmatic stream serialization (pdl_entry in dfsph_kernels.cuh) unless
-// the solver is timing kernels (tuning or profiling), where each launch must run alone, or it is switched off.
-template <class... KArgs, class... Args>
-void launch_k(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
-  if (!pdl) {
-    kern<<<grid, block, smem, st>>>(args...);
-    return;
-  }
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
-}
-
-#define PDL_ON(s) ((s)->pdl && !(s)->tuning && !(s)->prof_on)
-
-#define LAUNCH(s, kern, grid, block, stream, ...)                                                  \
-  do {                                                                                             \
-    launch_k(PDL_ON(s), kern, dim3(grid), dim3(block), 0, (cudaStream_t)(stream), __VA_ARGS__);    \
-    ++(s)->launches;                                                                               \
+#define LAUNCH(s, kern, grid, block, stream, ...)          \
+  do {                                                     \
+    kern<<<(grid), (block), 0, (cudaStream_t)(stream)>>>(__VA_ARGS__); \
+    ++(s)->launches;                                       \
   } while (0)
 
 void prof_begin(adf_solver* s, int kind, cudaStream_t st) {
@@ -258,13 +234,13 @@ void prof_end(adf_solver* s, cudaStream_t st) {
   s->prof_open = -1;
 }
 
-#define NB_DISPATCH(kern, nb, grid, block, st, ...)                                                \
-  do {                                                                                             \
-    switch (nb) {                                                                                  \
-      case 4: launch_k(PDL_ON(s), kern<4>, dim3(grid), dim3(block), 0, (st), __VA_ARGS__); break;    \
-      case 16: launch_k(PDL_ON(s), kern<16>, dim3(grid), dim3(block), 0, (st), __VA_ARGS__); break;  \
-      default: launch_k(PDL_ON(s), kern<8>, dim3(grid), dim3(block), 0, (st), __VA_ARGS__); break;   \
-    }                                                                                              \
+#define NB_DISPATCH(kern, nb, grid, block, st, ...)                      \
+  do {                                                                   \
+    switch (nb) {                                                        \
+      case 4: kern<4><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;   \
+      case 16: kern<16><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break; \
+      default: kern<8><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;  \
+    }                                                                    \
   } while (0)
 
 // One launch of a tuned kernel with configuration c (the pressure iterations' grid is the work-item bound, each block
@@ -277,8 +253,8 @@ void launch_tk(adf_solver* s, int id, const TuneCfg& c, cudaStream_t st, const D
     case TK_ACCEL: NB_DISPATCH(k_accel, c.nb, s->max_items, c.block, st, P); break;
     case TK_JACOBI: NB_DISPATCH(k_jacobi, c.nb, s->max_items, c.block, st, P); break;
     case TK_LISTS:
-      if (c.nb == 16) launch_k(PDL_ON(s), k_lists_union<16>, dim3(blocks(n, 16 * LU_WARPS)), dim3(32 * LU_WARPS), 0, st, P);
-      else launch_k(PDL_ON(s), k_lists_union<32>, dim3(blocks(n, 32 * LU_WARPS)), dim3(32 * LU_WARPS), 0, st, P);
+      if (c.nb == 16) k_lists_union<16><<<blocks(n, 16 * LU_WARPS), 32 * LU_WARPS, 0, st>>>(P);
+      else k_lists_union<32><<<blocks(n, 32 * LU_WARPS), 32 * LU_WARPS, 0, st>>>(P);
       break;
     default: NB_DISPATCH(k_xsph, c.nb, blocks(n, c.block), c.block, st, P); break;
   }
@@ -444,7 +420,7 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
     LAUNCH(s, k_skin_ref, blocks(n), BLOCK, st, P);
     {
       const size_t smem = P.sup_cap <= SKIN_SMEM_CAP ? sizeof(int) * (size_t)P.sup_cap * SKIN_THREADS : 0;
-      launch_k(PDL_ON(s), k_skin_build, dim3(blocks(n, SKIN_THREADS)), dim3(SKIN_THREADS), smem, st, P);
+      k_skin_build<<<blocks(n, SKIN_THREADS), SKIN_THREADS, smem, st>>>(P);
       ++s->launches;
     }
     LAUNCH(s, k_skin_filter, blocks(n), BLOCK, st, P);
@@ -452,7 +428,7 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
     run_tk(s, TK_LISTS, st, P);
   } else {
     const size_t smem = sizeof(int) * (size_t)s->K * LS_THREADS;
-    launch_k(PDL_ON(s), k_lists_smem, dim3(blocks(n, LS_THREADS)), dim3(LS_THREADS), smem, st, P);
+    k_lists_smem<<<blocks(n, LS_THREADS), LS_THREADS, smem, st>>>(P);
     ++s->launches;
   }
   prof_end(s, st);
@@ -474,14 +450,12 @@ void cg_product(adf_solver* s, DevP& P, cudaStream_t st, const float* vec, const
   const TuneCfg& ca = s->tune[TK_ACCEL];
   const TuneCfg& cj = s->tune[TK_JACOBI];
   prof_begin(s, 5, st);
-  if (s->cg_team) launch_k(PDL_ON(s), k_cg_accel_team, dim3(blocks((long long)n * TL)), dim3(BLOCK), 0, st, P, vec, vr, gated);
+  if (s->cg_team) k_cg_accel_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, vec, vr, gated);
   else NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, vec, vr, gated);
   ++s->launches;
   prof_end(s, st);
   prof_begin(s, 6, st);
-  if (s->cg_team)
-    launch_k(PDL_ON(s), k_cg_apply_team, dim3(blocks((long long)n * TL)), dim3(BLOCK), 0, st, P, vec, out, gated, bias,
-             accumulate);
+  if (s->cg_team) k_cg_apply_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, vec, out, gated, bias, accumulate);
   else NB_DISPATCH(k_cg_apply, cj.nb, blocks(n, cj.block), cj.block, st, P, vec, out, gated, bias, accumulate);
   ++s->launches;
   prof_end(s, st);
@@ -517,15 +491,15 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
     const TuneCfg& cj = s->tune[TK_JACOBI];
     prof_begin(s, 5, st);
     if (s->cg_team)
-      launch_k(PDL_ON(s), k_cg_accel_team, dim3(blocks((long long)n * TL)), dim3(BLOCK), 0, st, P,
-               (const float*)P.cg_corr, (const float*)P.cg_corrr, 1);
+      k_cg_accel_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, (const float*)P.cg_corr, (const float*)P.cg_corrr,
+                                                                   1);
     else
       NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, (const float*)P.cg_corr,
                   (const float*)P.cg_corrr, 1);
     ++s->launches;
     prof_end(s, st);
     prof_begin(s, 6, st);
-    if (s->cg_team) launch_k(PDL_ON(s), k_cg_apply_finish_team, dim3(blocks((long long)n * TL)), dim3(BLOCK), 0, st, P);
+    if (s->cg_team) k_cg_apply_finish_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P);
     else NB_DISPATCH(k_cg_apply_finish, cj.nb, blocks(n, cj.block), cj.block, st, P);
     ++s->launches;
     prof_end(s, st);
@@ -1322,13 +1296,6 @@ int adf_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_out,
   }
   if (!s->use_graphs || s->prof_on) return enqueue_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st, false);
   return graph_step(s, q_in, qd_in, q_out, qd_out, f_ext, dt, st);
-}
-
-int adf_set_programmatic_launch(adf_solver* s, int enable) {
-  if (!s) return fail(ADF_ERR_VALUE, "adf_set_programmatic_launch: null solver");
-  if (s->pdl != (enable != 0)) ++s->table_version;  // graphs recorded before hold the other kind of launch
-  s->pdl = enable != 0;
-  return ADF_OK;
 }
 
 int adf_set_graphs(adf_solver* s, int enable) {

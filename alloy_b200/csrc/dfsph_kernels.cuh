@@ -16,16 +16,6 @@
 
 namespace adf {
 
-// Programmatic dependent launch: every kernel here starts with pdl_entry(). Launched with programmatic stream
-// serialization (the library's default for its own launches), a kernel may be scheduled while its predecessor in the
-// stream is still running: it lets its own dependents be scheduled in turn, then waits until its predecessor's grid
-// has completed and its writes are visible, before it touches any memory. A dependent can only start once every block
-// of its predecessor has started, so waiting blocks never hold back the grid they wait for. Without a programmatic
-// launch both instructions do nothing.
-__device__ __forceinline__ void pdl_entry() {
-  asm volatile("griddepcontrol.launch_dependents;\n\tgriddepcontrol.wait;" ::: "memory");
-}
-
 constexpr int BLOCK = 256;
 constexpr int MAXCAP = 128;      // largest neighbor_capacity
 constexpr int WT = 4;            // lanes per near-wall particle in k_wall_slots
@@ -259,7 +249,6 @@ __device__ __forceinline__ void cell_coords(const WorldGrid& g, float x, float y
 // Groups (neighbors.py:36-51): fluid = ACTIVE and phase >= 1; wall = a boundary particle (PROXY at creation),
 // ACTIVE, in a world; every other particle stays out of the sorted arrays.
 __global__ void k_classify(DevP P) {
-  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
   int w = P.world[i];
@@ -312,7 +301,6 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* smem, int& total
 }
 
 __global__ void k_scan_tiles(const int* in, int n, int* tile_sums) {
-  pdl_entry();
   __shared__ int smem[32];
   int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
   int s = 0;
@@ -324,7 +312,6 @@ __global__ void k_scan_tiles(const int* in, int n, int* tile_sums) {
 }
 
 __global__ void k_scan_tile_sums(int* tile_sums, int n_tiles) {
-  pdl_entry();
   __shared__ int smem[32];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
@@ -343,7 +330,6 @@ __global__ void k_scan_tile_sums(int* tile_sums, int n_tiles) {
 }
 
 __global__ void k_scan_apply(const int* in, int n, const int* tile_off, int* out) {
-  pdl_entry();
   __shared__ int smem[32];
   int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
   int v[SCAN_ITEMS];
@@ -366,7 +352,6 @@ __global__ void k_scan_apply(const int* in, int n, const int* tile_off, int* out
 
 // Fluid and wall counts, and each world's liquid count (n_active, an exact integer in float64).
 __global__ void k_post_scan(DevP P, const int* world_cells) {
-  pdl_entry();
   int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w == 0) {
     int nf = P.cell_start[P.total_cells];
@@ -382,7 +367,6 @@ __global__ void k_post_scan(DevP P, const int* world_cells) {
 
 // Place each particle in its cell's range and gather its data into the sorted arrays. The counts go back to zero.
 __global__ void k_scatter(DevP P) {
-  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
   int key = P.key_of[i];
@@ -411,7 +395,6 @@ __global__ void k_scatter(DevP P) {
 constexpr int LS_THREADS = 128;
 
 __global__ void __launch_bounds__(LS_THREADS) k_lists_smem(DevP P) {
-  pdl_entry();
   extern __shared__ int srow[];
   const int p = blockIdx.x * LS_THREADS + threadIdx.x;
   if (p >= P.nfw[0]) return;
@@ -523,7 +506,6 @@ __device__ __forceinline__ void sort16_registers(unsigned (&key)[16]) {
 // two lanes' sorted runs are merged on write by lane l). The rows are the same either way.
 template <int G>
 __global__ void __launch_bounds__(32 * LU_WARPS) k_lists_union(DevP P) {
-  pdl_entry();
   __shared__ unsigned rows[LU_WARPS][LU_ROW][32];  // [warp][entry][lane]: lanes of one entry in distinct banks
   __shared__ __align__(8) float cxs[LU_WARPS][32];  // staged candidates, one coordinate per array so that two
   __shared__ __align__(8) float cys[LU_WARPS][32];  // neighbouring candidates are one 8-byte broadcast load
@@ -922,7 +904,6 @@ __device__ __forceinline__ void wall_slot_fill(const DevP& P, int p, float4 xi, 
 // teams of the block's lanes: most liquid particles see no wall particle, and the near-wall ones of a block are
 // usually a minority of it.
 __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
-  pdl_entry();
   __shared__ int list[BLOCK];
   __shared__ int wcount[BLOCK / 32];
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1191,7 +1172,6 @@ __device__ __forceinline__ int shape_insert(int (&shp)[4], float (&ph)[4], float
 // start-of-step plane kept for the projection), then overlapping walls combined by inclusion-exclusion (Psi as
 // filled, gradients as rewritten slot by slot). Empty slots are zero with wall id -1.
 __global__ void __launch_bounds__(BLOCK) k_shape_slots(DevP P) {
-  pdl_entry();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
@@ -1354,7 +1334,6 @@ __device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, in
 // pressure.py:144-193
 template <int NB>
 __global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   float4 xi = P.pos[p];
@@ -1416,7 +1395,6 @@ __global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
 // pressure.py:196-261
 template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   float4 xi = P.pos[p];
@@ -1502,7 +1480,6 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
 // network's correction, capped like the stored warm start and kept above the solve's lower bound (a non-finite
 // correction ends at the cap). kv_s / kd_s still hold the previous step's values when each solve starts.
 __global__ void __launch_bounds__(BLOCK) k_learned_start(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const float dt = P.dt;
@@ -1520,7 +1497,6 @@ __global__ void __launch_bounds__(BLOCK) k_learned_start(DevP P) {
 
 // Without the first-sweep judge every world with liquid takes the learned start.
 __global__ void k_mark_learned(DevP P) {
-  pdl_entry();
   int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W) return;
   P.learned[P.mode * P.W + w] = P.n_active[w] > 0.0 ? 1 : 0;
@@ -1534,7 +1510,6 @@ __global__ void k_mark_learned(DevP P) {
 constexpr int PROBE_GAP_MAX = 16;
 
 __global__ void k_probe_plan(DevP P) {
-  pdl_entry();
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W) return;
   const int o = P.mode * P.W + w;
@@ -1546,7 +1521,6 @@ __global__ void k_probe_plan(DevP P) {
 // After the first sweep from both starts: an evaluated world keeps the learned start unless its residual sum exceeds
 // the plain start's (equal liquid counts, so the sums order the mean errors); its schedule is updated.
 __global__ void k_choose_start(DevP P) {
-  pdl_entry();
   int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W) return;
   const bool probed = P.probe_skip[w] == 0;
@@ -1572,7 +1546,6 @@ __global__ void k_warm_need(DevP P, int* need) {
 
 // The masked worlds' schedules back to "evaluate at the next solve".
 __global__ void k_probe_reset(int W, const uint8_t* __restrict__ mask, int* gap, int* wait) {
-  pdl_entry();
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W || !mask[w]) return;
   gap[w] = gap[W + w] = 1;
@@ -1580,7 +1553,6 @@ __global__ void k_probe_reset(int W, const uint8_t* __restrict__ mask, int* gap,
 }
 
 __global__ void __launch_bounds__(BLOCK) k_select_start(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   if (!P.use_l[P.world_s[p]]) return;
@@ -1595,7 +1567,6 @@ __global__ void __launch_bounds__(BLOCK) k_select_start(DevP P) {
 // the loop (cap < 0) resets it, and a loop stops after `cap` iterations whatever the unconverged count says (every
 // world stops at max_iterations before that, so the cap only guards the loop against a count that never drops).
 __global__ void k_set_cond(cudaGraphConditionalHandle h, const int* n_unconv, unsigned long long* runs, int cap) {
-  pdl_entry();
   bool more = *n_unconv > 0;
   if (cap < 0) {
     runs[1] = 0ull;
@@ -1608,7 +1579,6 @@ __global__ void k_set_cond(cudaGraphConditionalHandle h, const int* n_unconv, un
 }
 
 __global__ void k_begin_solve(DevP P) {
-  pdl_entry();
   int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W) return;
   P.iters[w] = 0;
@@ -1674,8 +1644,7 @@ __device__ __forceinline__ int build_worklist(const DevP& P, bool fresh) {
   return listed;
 }
 
-__global__ void __launch_bounds__(1024) k_worklist(DevP P) {
-  pdl_entry(); build_worklist(P, false); }
+__global__ void __launch_bounds__(1024) k_worklist(DevP P) { build_worklist(P, false); }
 
 // The sorted range [b, e) of this block's work item; false (for the whole block) past the last item.
 __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
@@ -1743,7 +1712,6 @@ __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, 
 
 template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
-  pdl_entry();
   int b, e;
   if (!work_item(P, b, e)) return;
   for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
@@ -1817,7 +1785,6 @@ __device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
 
 template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
-  pdl_entry();
   int b, e;
   if (!work_item(P, b, e)) return;
   for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one<NB>(P, p);
@@ -1834,7 +1801,6 @@ __device__ __forceinline__ bool cg_skip(const DevP& P, int w, int gated) {
 // krylov.py:71-80: acc = pressure acceleration of the field vec (vr = vec / rho0)
 template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_cg_accel(DevP P, const float* vec, const float* vr, int gated) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
   DevP Q = P;
@@ -1849,7 +1815,6 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel(DevP P, const float* vec, co
 template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_cg_apply(DevP P, const float* vec, float* out, int gated, int bias,
                                                     int accumulate) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
   const float dt = P.dt;
@@ -1973,7 +1938,6 @@ __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, flo
 
 // k_cg_accel by teams (grid: TL threads per particle)
 __global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* vec, const float* vr, int gated) {
-  pdl_entry();
   int p;
   const Team tm = team_of(p);
   if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
@@ -1988,7 +1952,6 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* ve
 // k_cg_apply by teams
 __global__ void __launch_bounds__(BLOCK) k_cg_apply_team(DevP P, const float* vec, float* out, int gated, int bias,
                                                          int accumulate) {
-  pdl_entry();
   int p;
   const Team tm = team_of(p);
   if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
@@ -2008,7 +1971,6 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_team(DevP P, const float* ve
 
 // krylov.py:104-133: active set, z = M^-1 r on F (r = -w), first direction p = z; pair.x = r.z
 __global__ void __launch_bounds__(BLOCK) k_cg_init(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const float dt = P.dt;
@@ -2024,7 +1986,6 @@ __global__ void __launch_bounds__(BLOCK) k_cg_init(DevP P) {
 }
 
 __global__ void k_cg_first_rz(DevP P) {
-  pdl_entry();
   int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W) return;
   P.cg_rz[w] = P.cg_sums[w].x;
@@ -2034,7 +1995,6 @@ __global__ void k_cg_first_rz(DevP P) {
 
 // krylov.py:146-170: k += a p on F, projected onto k >= k_lo (the clamped part into corr); w += a A p
 __global__ void __launch_bounds__(BLOCK) k_cg_step(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
@@ -2088,7 +2048,6 @@ __device__ __forceinline__ void cg_finish_one(const DevP& P, int p, int w, float
 
 template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
@@ -2108,7 +2067,6 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
 
 // k_cg_apply_finish by teams
 __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish_team(DevP P) {
-  pdl_entry();
   int p;
   const Team tm = team_of(p);
   if (p >= P.nfw[0]) return;
@@ -2148,7 +2106,6 @@ __device__ __forceinline__ void cg_beta_world(const DevP& P, int w) {
 }
 
 __global__ void k_cg_beta(DevP P) {
-  pdl_entry();
   int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W || P.converged[w]) return;
   cg_beta_world(P, w);
@@ -2157,7 +2114,6 @@ __global__ void k_cg_beta(DevP P) {
 
 // krylov.py:236-246: p = z + beta p on F, 0 elsewhere
 __global__ void __launch_bounds__(BLOCK) k_cg_direction(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
@@ -2170,7 +2126,6 @@ __global__ void __launch_bounds__(BLOCK) k_cg_direction(DevP P) {
 // Per-world (sum x, sum y, max y) of the CG pairs for models without chunks (no particles): one block per world in
 // the fixed tree order of k_world_check; k_sums2_fused does it in one launch otherwise.
 __global__ void __launch_bounds__(256) k_world_sum2(DevP P, int with_max) {
-  pdl_entry();
   __shared__ double smd[8];
   __shared__ float smf[8];
   const int w = blockIdx.x;
@@ -2196,7 +2151,6 @@ __global__ void __launch_bounds__(256) k_world_sum2(DevP P, int with_max) {
 __global__ void __launch_bounds__(256) k_chunk_sum(const float* __restrict__ v, const int* chunk_begin,
                                                    const int* chunk_end, double* part_sum, float* part_max,
                                                    int* n_unconv, const int* chunk_world, const int* converged) {
-  pdl_entry();
   __shared__ double smd[8];
   __shared__ float smf[8];
   int c = blockIdx.x;
@@ -2216,7 +2170,6 @@ __global__ void __launch_bounds__(256) k_chunk_sum(const float* __restrict__ v, 
 // One block per world: the chunk partials (lane l takes chunks l, l + 256, ...), then the stop test
 // (pressure.py:370-390) when `check` is set.
 __global__ void __launch_bounds__(256) k_world_check(DevP P, int check, double* out_sum, float* out_max) {
-  pdl_entry();
   __shared__ double smd[8];
   __shared__ float smf[8];
   int w = blockIdx.x;
@@ -2272,7 +2225,6 @@ __device__ __forceinline__ bool grid_ticket(const DevP& P) {
 // count. The sums are those of the separate kernels bit for bit; only the launches are fewer. Used when a world
 // has more than WARP_FOLD_MAX_CHUNKS chunks (k_check_warps otherwise), where 256 threads fold its partials in parallel.
 __global__ void __launch_bounds__(256) k_check_fused(DevP P) {
-  pdl_entry();
   __shared__ double smd[8];
   __shared__ float smf[8];
   __shared__ bool wlast, glast;
@@ -2365,7 +2317,6 @@ constexpr int CHECK_WARPS = 8;
 constexpr int WARP_FOLD_MAX_CHUNKS = 256;  // a lane folds at most one partial per group of the 256-lane tree
 
 __global__ void __launch_bounds__(32 * CHECK_WARPS) k_check_warps(DevP P) {
-  pdl_entry();
   __shared__ int tickets[CHECK_WARPS];
   __shared__ bool glast;
   const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
@@ -2442,7 +2393,6 @@ __global__ void __launch_bounds__(32 * CHECK_WARPS) k_check_warps(DevP P) {
 // the world's last block also runs k_cg_beta's stop test and beta for its world, and the grid's last block stores the
 // count of worlds still iterating as the unconverged count.
 __global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int beta) {
-  pdl_entry();
   __shared__ double smd[8];
   __shared__ float smf[8];
   __shared__ int smi[32];
@@ -2503,7 +2453,6 @@ __global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int b
 // (v += dt a, warm start stored dt-free). A lone particle has no neighbours, so no other particle reads its kappa.
 template <int NB>
 __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const float dt = P.dt;
@@ -2581,7 +2530,6 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
 // particles carry their own velocity across: the wall advance in k_finish reads it.
 template <int NB>
 __global__ void __launch_bounds__(BLOCK, 3) k_xsph(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = P.nfw[0];
   if (p >= nf) {
@@ -2763,7 +2711,6 @@ __device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float 
 }
 
 __global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   int nf = P.nfw[0];
   if (p >= nf + P.nfw[1]) return;
@@ -2850,7 +2797,6 @@ __global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
 // emitters.py:67-126: per emitter a layer clock; each due layer places its particles (spares of the emitter's
 // pool, in pool order) at the region's lattice offsets with the emitter's velocity; the cursor then advances.
 __global__ void k_emit_clock(const Emit* em, int n_e, float dt, const int* enabled, float* t_acc, int* emit_now) {
-  pdl_entry();
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_e) return;
   emit_now[e] = 0;
@@ -2866,7 +2812,6 @@ __global__ void k_emit_clock(const Emit* em, int n_e, float dt, const int* enabl
 __global__ void k_emit(DevP P, const Emit* em, int n_off, const int* off_emitter, const int* off_rank,
                        const float* off_local, const int* emit_now, const int* cursor, const int* pool_ids,
                        long long* mass_in, int* emit_overflow) {
-  pdl_entry();
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_off) return;
   int e = off_emitter[c];
@@ -2900,7 +2845,6 @@ __global__ void k_emit(DevP P, const Emit* em, int n_off, const int* off_emitter
 }
 
 __global__ void k_emit_cursor(const Emit* em, int n_e, const int* emit_now, int* cursor) {
-  pdl_entry();
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_e) return;
   if (emit_now[e] != 0) cursor[e] = min(cursor[e] + em[e].n_layer, em[e].pool_size);
@@ -2909,14 +2853,12 @@ __global__ void k_emit_cursor(const Emit* em, int n_e, const int* emit_now, int*
 // prime.py:80-85: the solved divergence warm starts back in the caller's order, then kd = kv dt and kv = 0 for every
 // particle (the density solve of the first step starts from the hydrostatic pressure).
 __global__ void k_prime_gather(DevP P) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   P.kv[P.id_of[p]] = P.kv_s[p];
 }
 
 __global__ void k_prime_store(int n, float dt, float* kv, float* kd) {
-  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   kd[i] = kv[i] * dt;
@@ -2925,7 +2867,6 @@ __global__ void k_prime_store(int n, float dt, float* kv, float* kd) {
 
 // ------------------------------------------------------------------------------------------------- misc
 __global__ void k_wall_volume(int n, const int32_t* flags, const float* radius, float* wall_vol) {
-  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float r = radius[i];
@@ -2935,7 +2876,6 @@ __global__ void k_wall_volume(int n, const int32_t* flags, const float* radius, 
 // Exact int64 sum per world; a warp whose particles all belong to one world adds its shuffle-reduced total with one
 // atomic (integer addition, so the order does not matter).
 __global__ void k_active_mass(DevP P, long long* out) {
-  pdl_entry();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   int w = -1;
   long long v = 0;
@@ -2958,7 +2898,6 @@ __global__ void k_active_mass(DevP P, long long* out) {
 
 __global__ void k_unsort_n(int n, const int* nfw, const int* id_of, const float* f, int stride, int comp, float* out,
                            int ncomp) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n || p >= nfw[0]) return;
   int i = id_of[p];
@@ -2966,14 +2905,12 @@ __global__ void k_unsort_n(int n, const int* nfw, const int* id_of, const float*
 }
 
 __global__ void k_fill_ones(int n, const int* nfw, const int* id_of, float* out) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n || p >= nfw[0]) return;
   out[id_of[p]] = 1.0f;
 }
 
 __global__ void k_count_entries(int n, const int* nfw, const int* cnt, long long* out) {
-  pdl_entry();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   int c = (p < n && p < nfw[0]) ? cnt[p] : 0;
 #pragma unroll
@@ -2984,7 +2921,6 @@ __global__ void k_count_entries(int n, const int* nfw, const int* cnt, long long
 // Diagnostics: slot k's wall id (-1 empty; the particle wall's id is n_shapes) or, with k < 0, the number of slots in
 // use, of each liquid particle, written as floats at its caller index.
 __global__ void k_slot_info(DevP P, int k, float* out) {
-  pdl_entry();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int ns = slot_count(P, p);
@@ -2994,7 +2930,6 @@ __global__ void k_slot_info(DevP P, int k, float* out) {
 }
 
 __global__ void k_reset(DevP P, const uint8_t* mask, const int32_t* flags0, const int8_t* phase0) {
-  pdl_entry();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
   int w = P.world[i];

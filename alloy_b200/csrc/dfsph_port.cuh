@@ -63,7 +63,6 @@ __global__ void __launch_bounds__(256) k_port_take(const int* __restrict__ ws, c
                                                    int keep, int32_t* flags, int8_t* phase,
                                                    const float* __restrict__ mass, float* qd, int* stack, int* top,
                                                    int* taken, int* total, long long* mass_out) {
-  pdl_entry();
   __shared__ int sm[9];
   __shared__ long long sml[8];
   const int w = blockIdx.x;
@@ -109,7 +108,6 @@ __global__ void __launch_bounds__(256) k_port_emit(const int* __restrict__ ws, c
                                                    int32_t* flags, int8_t* phase, const float* __restrict__ mass,
                                                    const int* __restrict__ stack, int* top, int* granted, int* total,
                                                    long long* mass_in) {
-  pdl_entry();
   __shared__ long long sml[8];
   const int w = blockIdx.x;
   const int b = ws[w], t0 = top[w];
@@ -141,7 +139,6 @@ __global__ void __launch_bounds__(256) k_port_emit(const int* __restrict__ ws, c
 __global__ void __launch_bounds__(256) k_port_reset(int W, const int* __restrict__ ws, const uint8_t* __restrict__ mask,
                              const int* __restrict__ stack0, const int* __restrict__ top0, int* stack, int* top,
                              int* absorbed, int* emitted, int* retired, int* taken, int* granted) {
-  pdl_entry();
   const int w = blockIdx.x;
   if (w >= W || !mask[w]) return;
   for (int i = ws[w] + threadIdx.x; i < ws[w + 1]; i += blockDim.x) stack[i] = stack0[i];
@@ -157,7 +154,6 @@ __global__ void __launch_bounds__(256) k_port_reset(int W, const int* __restrict
 // k_world_check's.
 __global__ void __launch_bounds__(256) k_energy_chunk(DevP P, const float* __restrict__ q,
                                                       const float* __restrict__ qd, const double* __restrict__ z_ref) {
-  pdl_entry();
   __shared__ double smd[8];
   const int c = blockIdx.x;
   const int i = P.chunk_begin[c] + threadIdx.x;
@@ -182,7 +178,6 @@ __global__ void __launch_bounds__(256) k_energy_chunk(DevP P, const float* __res
 // runtime.py:82-90 (_speed_only_kernel): per-world max |v| of the liquid, non-finite speeds as 1e30; float bits of
 // non-negative values order as integers, so an integer atomicMax is the float max.
 __global__ void k_speed_max(DevP P, const float* __restrict__ qd, int* speed_bits) {
-  pdl_entry();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n || !is_fluid_orig(P, i)) return;
   const size_t b = 3 * (size_t)i;
@@ -195,7 +190,6 @@ __global__ void k_speed_max(DevP P, const float* __restrict__ qd, int* speed_bit
 // runtime.py:55-62 (_stable_dt_kernel): dt_max at rest, else clamp(cfl spacing / v, dt_min, dt_max).
 __global__ void k_stable_dt(int W, const int* __restrict__ speed_bits, float cfl, float spacing, float dt_min,
                             float dt_max, float* out) {
-  pdl_entry();
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W) return;
   const float v = __int_as_float(speed_bits[w]);
@@ -210,7 +204,6 @@ __global__ void k_stable_dt(int W, const int* __restrict__ speed_bits, float cfl
 // patch.py:65-79: arm the entries [e0, e1) whose world is flagged (int32 or bool flags [W]) and has not fired yet.
 __global__ void k_patch_trigger(int e0, int e1, const void* __restrict__ flags, int is_bool,
                                 const int* __restrict__ world, const int* __restrict__ fired, int* pending) {
-  pdl_entry();
   const int e = e0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= e1) return;
   const int w = world[e];
@@ -227,7 +220,6 @@ __global__ void __launch_bounds__(256) k_patch_emit(DevP P, int E, const int* __
                                                     const int* __restrict__ pool, const float* __restrict__ points,
                                                     const int* __restrict__ group, const float* __restrict__ vel,
                                                     long long* mass_in) {
-  pdl_entry();
   __shared__ long long sml[8];
   const int e = blockIdx.x;
   if (e >= E || pending[e] == 0 || fired[e] != 0) return;
@@ -252,7 +244,6 @@ __global__ void __launch_bounds__(256) k_patch_emit(DevP P, int E, const int* __
 
 // patch.py:110-115: an armed entry has fired; every entry is disarmed.
 __global__ void k_patch_fire(int E, int* pending, int* fired) {
-  pdl_entry();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E) return;
   if (pending[e] != 0 && fired[e] == 0) fired[e] = 1;
@@ -262,7 +253,6 @@ __global__ void k_patch_fire(int E, int* pending, int* fired) {
 // patch.py:225-234 (reset): the masked worlds' entries re-armed (pending and fired cleared).
 __global__ void k_patch_reset(int E, const int* __restrict__ world, const uint8_t* __restrict__ mask, int* pending,
                               int* fired) {
-  pdl_entry();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E || !mask[world[e]]) return;
   pending[e] = 0;

@@ -23,7 +23,6 @@ namespace adf {
 
 // neighbors_skin.py:34-40: each world's rebuild flag starts as its force flag, which is cleared.
 __global__ void k_skin_seed(DevP P) {
-  pdl_entry();
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W) return;
   P.skin_flag[w] = P.skin_force[w];
@@ -36,7 +35,6 @@ __device__ __forceinline__ int skin_group(const DevP& P, int i, int w) { return 
 // neighbors_skin.py:43-57, over the caller's particles: a world is flagged when a particle's group changed or it
 // moved more than 0.49 s since its world's last build (a NaN position moves).
 __global__ void k_skin_check(DevP P) {
-  pdl_entry();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
   const int w = P.world[i];
@@ -53,7 +51,6 @@ __global__ void k_skin_check(DevP P) {
 
 // The flagged worlds' reference positions and groups (neighbors_skin.py:76-78), over the caller's particles.
 __global__ void k_skin_ref(DevP P) {
-  pdl_entry();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.n) return;
   const int w = P.world[i];
@@ -85,7 +82,6 @@ constexpr int SKIN_THREADS = 128;
 constexpr int SKIN_SMEM_CAP = 96;
 
 __global__ void __launch_bounds__(SKIN_THREADS) k_skin_build(DevP P) {
-  pdl_entry();
   extern __shared__ int sbuf[];
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
@@ -153,7 +149,6 @@ __global__ void __launch_bounds__(SKIN_THREADS) k_skin_build(DevP P) {
 // neighbors_skin.py:113-140 (sorted order): the rows of this step from the superset rows, by the plain build's test
 // (d = x_j - x_i, d.d < h^2), in row order, the first K of them; overfull rows count in the world's overflow.
 __global__ void __launch_bounds__(BLOCK) k_skin_filter(DevP P) {
-  pdl_entry();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int s = P.skin_slot[P.id_of[p]];

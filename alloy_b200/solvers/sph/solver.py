@@ -474,11 +474,6 @@ class SolverDFSPH:
     def kernel_launches(self) -> int:
         return int(self._lib.adf_kernel_launches(self._h))
 
-    def programmatic_launch(self, enable: bool) -> None:
-        """Launch each kernel with programmatic stream serialization (default) or in plain stream order; the results
-        are the same bit for bit (include/alloy_dfsph.h adf_set_programmatic_launch)."""
-        _lib.check(self._lib.adf_set_programmatic_launch(self._h, int(bool(enable))), "programmatic_launch")
-
     def use_graphs(self, enable: bool) -> None:
         """Replay each step as one CUDA graph (default) or launch its kernels one by one (include/alloy_dfsph.h)."""
         _lib.check(self._lib.adf_set_graphs(self._h, int(bool(enable))), "use_graphs")

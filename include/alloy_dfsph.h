@@ -131,12 +131,6 @@ int adf_step(adf_solver* solver, const float* q_in, const float* qd_in, float* q
  * stream that the caller is capturing always joins that capture with WHILE nodes. */
 int adf_set_graphs(adf_solver* solver, int enable);
 
-/* Kernel launches (no counterpart in the reference). enable = 1 (default): each kernel of a step is launched with
- * programmatic stream serialization, so it is scheduled while its predecessor finishes and starts its work when the
- * predecessor's results are visible (the tuning step and profiled steps launch without it); 0: plain stream order.
- * Results are the same bit for bit either way. */
-int adf_set_programmatic_launch(adf_solver* solver, int enable);
-
 /* Autotuner (no counterpart in the reference; Warp picks its own launch shapes). enable = 1 (the default at creation):
  * the next adf_step on a stream that is not capturing is a tuning step: it launches its kernels one by one and, the
  * first time each neighbour-loop kernel (density and factor, solve start, pressure acceleration and its application,

@@ -141,31 +141,3 @@ def test_moving_particle_wall_bit_exact(cuda):
         np.testing.assert_array_equal(a.particle_qd.cpu().numpy(), qd, err_msg=f"qd step {k}")
     v = a.particle_qd.cpu().numpy()[walls.start:walls.stop]
     np.testing.assert_array_equal(v, np.tile(np.float32([0.1, 0.0, -0.2]), (len(v), 1)))
-
-
-@pytest.mark.parametrize("solver", ["jacobi", "cg"])
-def test_programmatic_launches_equal_plain_stream_order(cuda, solver):
-    """Every kernel of a step launched with programmatic stream serialization (the default: scheduled while its
-    predecessor finishes, waiting for its results before any memory access) gives the bits of plain stream order, in
-    graph replay and kernel by kernel, with box walls and several worlds."""
-    from alloy_b200.solvers.sph.testing import batched_worlds, water_column
-
-    scenes = [water_column(6, 6, 8, worlds=3, r=2.0e-3, device=cuda, pressure_solver=solver),
-              batched_worlds(worlds=4, lo=300, hi=1500, seed=9, device=cuda, pressure_solver=solver)]
-    for sc in scenes:
-        out = {}
-        for pdl in (True, False):
-            for graphs in (True, False):
-                sol = SolverDFSPH(sc.model, sc.config)
-                sol.programmatic_launch(pdl)
-                sol.use_graphs(graphs)
-                a, b = sc.model.state(), sc.model.state()
-                for _ in range(8):
-                    sol.step(a, b, None, None, sc.dt)
-                    a, b = b, a
-                torch.cuda.synchronize(cuda)
-                out[(pdl, graphs)] = (a.particle_q.cpu().numpy().tobytes() + a.particle_qd.cpu().numpy().tobytes(),
-                                      sol.report().iters_density.tolist())
-        ref = out[(False, False)]
-        for k, v in out.items():
-            assert v == ref, (sc.name, k)
