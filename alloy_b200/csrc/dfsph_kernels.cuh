@@ -1538,7 +1538,6 @@ __global__ void k_choose_start(DevP P) {
 // Worlds that evaluate the learned start in either solve of this step (their schedules wait 0 solves): only their
 // particles need features and predictions.
 __global__ void k_warm_need(DevP P, int* need) {
-  pdl_entry();
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= P.W) return;
   need[w] = (P.n_active[w] > 0.0 && (P.probe_wait[w] == 0 || P.probe_wait[P.W + w] == 0)) ? 1 : 0;

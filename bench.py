@@ -66,8 +66,6 @@ def parse():
     ap.add_argument("--no-warm", action="store_true", help="skip the arms beside the headline (plain or learned, CG, "
                                                               "per-world, FP64 check)")
     ap.add_argument("--plain", action="store_true", help="headline the plain solve instead of the warm-started one")
-    ap.add_argument("--no-pdl", action="store_true", help="launch the kernels in plain stream order (no programmatic "
-                                                           "dependent launches), for comparison")
     return ap.parse_args()
 
 
@@ -405,7 +403,6 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
     full = make_scene(args.workload, dev, **cfg_kw)
     sc = rank_scene(full, args.workload, rank, world, dev)
     sol = SolverDFSPH(sc.model, sc.config)
-    sol.programmatic_launch(not args.no_pdl)
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
     if judge is not None:
         sol.set_warm_model(default_model())
@@ -604,7 +601,6 @@ def run_b200(args):
     sc = rank_scene(full, args.workload, rank, world, dev)
     note(f"solver for {sc.model.particle_count} particles")
     sol = SolverDFSPH(sc.model, sc.config)
-    sol.programmatic_launch(not args.no_pdl)
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
     headline_warm = not args.plain
     if headline_warm:  # the shipped network's starts, judged by the first sweep against the plain start per world
@@ -824,7 +820,6 @@ def run_b200(args):
             "parallelism": ("world shards" if args.workload in MULTI_WORLD else "replicas") if world > 1
             else "single GPU",
             "headline": "warm_started (learned start, judged)" if headline_warm else "plain",
-            "programmatic_launch": not args.no_pdl,
             "e2e": e2e, "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "traffic_src": traffic_src,
