@@ -234,13 +234,24 @@ void prof_end(adf_solver* s, cudaStream_t st) {
   s->prof_open = -1;
 }
 
-#define NB_DISPATCH(kern, nb, grid, block, st, ...)                      \
-  do {                                                                   \
-    switch (nb) {                                                        \
-      case 4: kern<4><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;   \
-      case 16: kern<16><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break; \
-      default: kern<8><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;  \
-    }                                                                    \
+// A neighbour-loop kernel's instance: gathers in flight nb, with MS_FLAG when the model has box walls (solver s in scope)
+#define NB_DISPATCH(kern, nb, grid, block, st, ...)                                          \
+  do {                                                                                       \
+    switch ((nb) | (s->d.slot_cap > 1 ? MS_FLAG : 0)) {                                      \
+      case 4: kern<4><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;                       \
+      case 16: kern<16><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;                     \
+      case 4 | MS_FLAG: kern<4 | MS_FLAG><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;     \
+      case 8 | MS_FLAG: kern<8 | MS_FLAG><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;     \
+      case 16 | MS_FLAG: kern<16 | MS_FLAG><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;   \
+      default: kern<8><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;                      \
+    }                                                                                        \
+  } while (0)
+
+// A team kernel's instance (box walls or not)
+#define MS_DISPATCH(kern, grid, block, st, ...)                                                  \
+  do {                                                                                           \
+    if (s->d.slot_cap > 1) kern<true><<<(grid), (block), 0, (st)>>>(__VA_ARGS__);                \
+    else kern<false><<<(grid), (block), 0, (st)>>>(__VA_ARGS__);                                \
   } while (0)
 
 // One launch of a tuned kernel with configuration c (the pressure iterations' grid is the work-item bound, each block
@@ -450,12 +461,12 @@ void cg_product(adf_solver* s, DevP& P, cudaStream_t st, const float* vec, const
   const TuneCfg& ca = s->tune[TK_ACCEL];
   const TuneCfg& cj = s->tune[TK_JACOBI];
   prof_begin(s, 5, st);
-  if (s->cg_team) k_cg_accel_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, vec, vr, gated);
+  if (s->cg_team) MS_DISPATCH(k_cg_accel_team, blocks((long long)n * TL), BLOCK, st, P, vec, vr, gated);
   else NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, vec, vr, gated);
   ++s->launches;
   prof_end(s, st);
   prof_begin(s, 6, st);
-  if (s->cg_team) k_cg_apply_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, vec, out, gated, bias, accumulate);
+  if (s->cg_team) MS_DISPATCH(k_cg_apply_team, blocks((long long)n * TL), BLOCK, st, P, vec, out, gated, bias, accumulate);
   else NB_DISPATCH(k_cg_apply, cj.nb, blocks(n, cj.block), cj.block, st, P, vec, out, gated, bias, accumulate);
   ++s->launches;
   prof_end(s, st);
@@ -491,15 +502,15 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
     const TuneCfg& cj = s->tune[TK_JACOBI];
     prof_begin(s, 5, st);
     if (s->cg_team)
-      k_cg_accel_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P, (const float*)P.cg_corr, (const float*)P.cg_corrr,
-                                                                   1);
+      MS_DISPATCH(k_cg_accel_team, blocks((long long)n * TL), BLOCK, st, P, (const float*)P.cg_corr,
+                  (const float*)P.cg_corrr, 1);
     else
       NB_DISPATCH(k_cg_accel, ca.nb, blocks(n, ca.block), ca.block, st, P, (const float*)P.cg_corr,
                   (const float*)P.cg_corrr, 1);
     ++s->launches;
     prof_end(s, st);
     prof_begin(s, 6, st);
-    if (s->cg_team) k_cg_apply_finish_team<<<blocks((long long)n * TL), BLOCK, 0, st>>>(P);
+    if (s->cg_team) MS_DISPATCH(k_cg_apply_finish_team, blocks((long long)n * TL), BLOCK, st, P);
     else NB_DISPATCH(k_cg_apply_finish, cj.nb, blocks(n, cj.block), cj.block, st, P);
     ++s->launches;
     prof_end(s, st);
@@ -1204,7 +1215,8 @@ int enqueue_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_
   rc = solve(s, P, 1, dt, st, graph);
   if (rc) return rc;
   prof_begin(s, 10, st);
-  LAUNCH(s, k_finish, blocks(s->n), BLOCK, st, P);
+  MS_DISPATCH(k_finish, blocks(s->n), BLOCK, st, P);
+  ++s->launches;
   prof_end(s, st);
   const int ne = (int)s->em_h.size();
   if (ne > 0) {

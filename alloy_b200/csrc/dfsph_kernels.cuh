@@ -229,6 +229,22 @@ __device__ __forceinline__ int slot_count(const DevP& P, int p) {
 }
 __device__ __forceinline__ size_t slot_at(const DevP& P, int b, int p) { return (size_t)b * P.n + p; }
 
+// Neighbour-loop kernels take one template integer NBX: the gathers they keep in flight, NB = NBX & NB_MASK, plus
+// MS_FLAG when the model has box walls (up to four slots per particle). Without the flag a kernel is compiled for the
+// particle-wall build's single slot, one pass of the multi-slot arithmetic, so the common case carries no loop.
+constexpr int NB_MASK = 31, MS_FLAG = 32;
+
+// f(b, o) for each wall slot of sorted liquid particle p, nearest first (o: the slot's index in the slot arrays)
+template <bool MS, class F>
+__device__ __forceinline__ void for_slots(const DevP& P, int p, F f) {
+  if constexpr (MS) {
+    const int ns = P.slot_cnt[p];
+    for (int b = 0; b < ns; ++b) f(b, slot_at(P, b, p));
+  } else {
+    if (P.slot_g[p].w >= 0.0f) f(0, (size_t)p);
+  }
+}
+
 __device__ __forceinline__ bool is_fluid_orig(const DevP& P, int i) {
   return (P.flags[i] & FLAG_ACTIVE) != 0 && P.phase[i] >= 1;
 }
@@ -1332,8 +1348,10 @@ __device__ __forceinline__ void load_row_batch_f(const DevP& P, int p, int c, in
 
 // ------------------------------------------------------------------------------------------ density, factor
 // pressure.py:144-193
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
+  constexpr int NB = NBX & NB_MASK;
+  constexpr bool MS = (NBX & MS_FLAG) != 0;
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   float4 xi = P.pos[p];
@@ -1370,18 +1388,20 @@ __global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
     }
   }
   float psi = 0.0f, lam = 0.0f;  // boundary slots, nearest first; lam: the opposing-wall compliance
-  const int ns = slot_count(P, p);
-  for (int b = 0; b < ns; ++b) {
-    const float4 sg = P.slot_g[slot_at(P, b, p)];
+  for_slots<MS>(P, p, [&](int b, size_t o) {
+    const float4 sg = P.slot_g[o];
     psi = psi + sg.w;
     Gx = Gx + sg.x;
     Gy = Gy + sg.y;
     Gz = Gz + sg.z;
-    for (int c = b + 1; c < ns; ++c) {
-      const float4 gc = P.slot_g[slot_at(P, c, p)];
-      lam = lam + maxr(-2.0f * dot_plain(sg.x, sg.y, sg.z, gc.x, gc.y, gc.z), 0.0f);
+    if constexpr (MS) {
+      const int ns = P.slot_cnt[p];
+      for (int c = b + 1; c < ns; ++c) {
+        const float4 gc = P.slot_g[slot_at(P, c, p)];
+        lam = lam + maxr(-2.0f * dot_plain(sg.x, sg.y, sg.z, gc.x, gc.y, gc.z), 0.0f);
+      }
     }
-  }
+  });
   float tot = (dotf(Gx, Gy, Gz, Gx, Gy, Gz) + sq) + lam;
   lam = lam + maxr(P.tot_min - tot, 0.0f);
   tot = maxr(tot, P.tot_min);
@@ -1393,8 +1413,10 @@ __global__ void __launch_bounds__(BLOCK, 5) k_density_alpha(DevP P) {
 
 // --------------------------------------------------------------------------------------------- solve start
 // pressure.py:196-261
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
+  constexpr int NB = NBX & NB_MASK;
+  constexpr bool MS = (NBX & MS_FLAG) != 0;
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   float4 xi = P.pos[p];
@@ -1421,12 +1443,10 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
       rate = ADF_FMA(aF, dotf(vi.x - vj.x, vi.y - vj.y, vi.z - vj.z, rx, ry, rz), rate);
     }
   }
-  const int ns = slot_count(P, p);
-  for (int b = 0; b < ns; ++b) {
-    const size_t o = slot_at(P, b, p);
+  for_slots<MS>(P, p, [&](int, size_t o) {
     const float4 sg = P.slot_g[o], vb = P.slot_vb[o];
     rate = rate + dotf(vi.x - vb.x, vi.y - vb.y, vi.z - vb.z, sg.x, sg.y, sg.z);
-  }
+  });
   const float dt = P.dt;
   float kap, lb, s;
   if (P.mode == 0) {
@@ -1459,7 +1479,7 @@ __global__ void __launch_bounds__(BLOCK) k_solve_init(DevP P) {
   if (P.feat_on && (!P.warm_need || P.warm_need[P.world_s[p]])) {  // warm-start network features (order: warmstart.py)
     const float ratio = P.ratio[p], al = P.alpha[p], kvp = P.kv_s[p], kdp = P.kd_s[p];
     const float drate = dt * rate;
-    const bool on = ns > 0;  // the nearest wall's slot
+    const bool on = slot_count(P, p) > 0;  // the nearest wall's slot
     const float4 sg = P.slot_g[p];
     const float phi = on ? P.slot_vb[p].w : P.kc.h;
     const float4 f0 = make_float4(ratio - 1.0f, P.neff[p] / P.n_full, drate, kvp);
@@ -1672,8 +1692,10 @@ __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
 
 // ------------------------------------------------------------------------------------------ Jacobi sweep
 // pressure.py:264-291: a_i = -sum_j m_j (k_i/rho0_i + k_j/rho0_j) grad W_ij - k_i sum_b dPsi_b
-template <int NB>
+template <int NBX>
 __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, float& ax, float& ay, float& az) {
+  constexpr int NB = NBX & NB_MASK;
+  constexpr bool MS = (NBX & MS_FLAG) != 0;
   float ki = P.kr[p];
   ax = ay = az = 0.0f;
   int c = P.cnt[p];
@@ -1699,31 +1721,32 @@ __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, 
       az = ADF_FMA(-cF, rz, az);
     }
   }
-  const int ns = slot_count(P, p);
-  for (int b = 0; b < ns; ++b) {
-    const float4 sg = P.slot_g[slot_at(P, b, p)];
+  for_slots<MS>(P, p, [&](int, size_t o) {
+    const float4 sg = P.slot_g[o];
     const float kk = P.kappa[p];
     ax = ADF_FMA(-kk, sg.x, ax);
     ay = ADF_FMA(-kk, sg.y, ay);
     az = ADF_FMA(-kk, sg.z, az);
-  }
+  });
 }
 
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
   int b, e;
   if (!work_item(P, b, e)) return;
   for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
     float ax, ay, az;
-    pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
+    pressure_accel<NBX>(P, p, P.pos[p], ax, ay, az);
     P.acc[p] = make_float4(ax, ay, az, 0.0f);
   }
 }
 
 // pressure.py:294-352
 // pressure.py:294-310: Ar_i of the accelerations in P.acc (the matrix-free product, before the compliance term)
-template <int NB>
+template <int NBX>
 __device__ __forceinline__ float accel_divergence(const DevP& P, int p, float inv_r0) {
+  constexpr int NB = NBX & NB_MASK;
+  constexpr bool MS = (NBX & MS_FLAG) != 0;
   float4 xi = P.pos[p];
   float4 ai = P.acc[p];
   float ar = 0.0f;
@@ -1747,19 +1770,18 @@ __device__ __forceinline__ float accel_divergence(const DevP& P, int p, float in
       ar = ADF_FMA(aF, dotf(ai.x - aj.x, ai.y - aj.y, ai.z - aj.z, rx, ry, rz), ar);
     }
   }
-  const int ns = slot_count(P, p);
-  for (int b = 0; b < ns; ++b) {
-    const float4 sg = P.slot_g[slot_at(P, b, p)];
+  for_slots<MS>(P, p, [&](int, size_t o) {
+    const float4 sg = P.slot_g[o];
     ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
-  }
+  });
   return ar;
 }
 
-template <int NB>
+template <int NBX>
 __device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
   float r0 = P.vel[p].w;
   float inv_r0 = 1.0f / r0;
-  float ar = accel_divergence<NB>(P, p, inv_r0);
+  float ar = accel_divergence<NBX>(P, p, inv_r0);
   float kap = P.kappa[p];
   ar = ADF_FMA(-P.reg[p], kap, ar);
   const float dt = P.dt;
@@ -1782,11 +1804,11 @@ __device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
   P.err_orig[P.id_of[p]] = e;
 }
 
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
   int b, e;
   if (!work_item(P, b, e)) return;
-  for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one<NB>(P, p);
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one<NBX>(P, p);
 }
 
 // ------------------------------------------------------------------------------------ projected CG (krylov.py)
@@ -1798,7 +1820,7 @@ __device__ __forceinline__ bool cg_skip(const DevP& P, int w, int gated) {
 }
 
 // krylov.py:71-80: acc = pressure acceleration of the field vec (vr = vec / rho0)
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK) k_cg_accel(DevP P, const float* vec, const float* vr, int gated) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
@@ -1806,12 +1828,12 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel(DevP P, const float* vec, co
   Q.kappa = const_cast<float*>(vec);
   Q.kr = const_cast<float*>(vr);
   float ax, ay, az;
-  pressure_accel<NB>(Q, p, P.pos[p], ax, ay, az);
+  pressure_accel<NBX>(Q, p, P.pos[p], ax, ay, az);
   P.acc[p] = make_float4(ax, ay, az, 0.0f);
 }
 
 // krylov.py:83-101: out (+)= A vec (- b); pair.x = vec_i (A vec)_i
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK) k_cg_apply(DevP P, const float* vec, float* out, int gated, int bias,
                                                     int accumulate) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1820,7 +1842,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply(DevP P, const float* vec, fl
   const bool div = P.mode == 0;
   const float scale = div ? dt : dt * dt;
   const float inv_r0 = 1.0f / P.vel[p].w;
-  const float t = ADF_FMA(-P.reg[p], vec[p], accel_divergence<NB>(P, p, inv_r0));
+  const float t = ADF_FMA(-P.reg[p], vec[p], accel_divergence<NBX>(P, p, inv_r0));
   float v = -(scale * t);
   P.cg_pair[P.id_of[p]] = make_float2(vec[p] * v, 0.0f);
   if (bias) v = v - (div ? P.src[p] : P.src[p] - 1.0f);
@@ -1853,6 +1875,7 @@ __device__ __forceinline__ Team team_of(int& p) {
 __device__ __forceinline__ int2 row_entry(const DevP& P, int p, int k) { return __ldcs(P.nbrjf + p + (size_t)k * P.n); }
 
 // pressure_accel with the fields of Q (kappa, kr), valid in the team's first lane
+template <bool MS>
 __device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, float4 xi, const Team& tm, float& ax, float& ay,
                                                     float& az) {
   const float ki = Q.kr[p];
@@ -1888,17 +1911,17 @@ __device__ __forceinline__ void pressure_accel_team(const DevP& Q, int p, float4
       }
     }
   }
-  const int ns = slot_count(Q, p);
-  for (int b = 0; b < ns; ++b) {
-    const float4 sg = Q.slot_g[slot_at(Q, b, p)];
+  for_slots<MS>(Q, p, [&](int, size_t o) {
+    const float4 sg = Q.slot_g[o];
     const float kk = Q.kappa[p];
     ax = ADF_FMA(-kk, sg.x, ax);
     ay = ADF_FMA(-kk, sg.y, ay);
     az = ADF_FMA(-kk, sg.z, az);
-  }
+  });
 }
 
 // accel_divergence, valid in the team's first lane
+template <bool MS>
 __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, float inv_r0, const Team& tm) {
   const float4 xi = P.pos[p];
   const float4 ai = P.acc[p];
@@ -1927,15 +1950,15 @@ __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, flo
       }
     }
   }
-  const int ns = slot_count(P, p);
-  for (int b = 0; b < ns; ++b) {
-    const float4 sg = P.slot_g[slot_at(P, b, p)];
+  for_slots<MS>(P, p, [&](int, size_t o) {
+    const float4 sg = P.slot_g[o];
     ar = ar + dotf(ai.x, ai.y, ai.z, sg.x, sg.y, sg.z);
-  }
+  });
   return ar;
 }
 
 // k_cg_accel by teams (grid: TL threads per particle)
+template <bool MS>
 __global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* vec, const float* vr, int gated) {
   int p;
   const Team tm = team_of(p);
@@ -1944,18 +1967,19 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* ve
   Q.kappa = const_cast<float*>(vec);
   Q.kr = const_cast<float*>(vr);
   float ax, ay, az;
-  pressure_accel_team(Q, p, P.pos[p], tm, ax, ay, az);
+  pressure_accel_team<MS>(Q, p, P.pos[p], tm, ax, ay, az);
   if (tm.t == 0) P.acc[p] = make_float4(ax, ay, az, 0.0f);
 }
 
 // k_cg_apply by teams
+template <bool MS>
 __global__ void __launch_bounds__(BLOCK) k_cg_apply_team(DevP P, const float* vec, float* out, int gated, int bias,
                                                          int accumulate) {
   int p;
   const Team tm = team_of(p);
   if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
   const float inv_r0 = 1.0f / P.vel[p].w;
-  const float ar = accel_divergence_team(P, p, inv_r0, tm);
+  const float ar = accel_divergence_team<MS>(P, p, inv_r0, tm);
   if (tm.t != 0) return;
   const float dt = P.dt;
   const bool div = P.mode == 0;
@@ -2045,7 +2069,7 @@ __device__ __forceinline__ void cg_finish_one(const DevP& P, int p, int w, float
   P.cg_pair[i] = make_float2(-wv * zi, e);
 }
 
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
@@ -2057,7 +2081,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
   float wv = P.cg_w[p];
   if (P.cg_restart[w] != 0) {
     const float inv_r0 = 1.0f / P.vel[p].w;
-    const float t = ADF_FMA(-P.reg[p], P.cg_corr[p], accel_divergence<NB>(P, p, inv_r0));
+    const float t = ADF_FMA(-P.reg[p], P.cg_corr[p], accel_divergence<NBX>(P, p, inv_r0));
     wv = -(scale * t) + wv;
     P.cg_w[p] = wv;
   }
@@ -2065,6 +2089,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
 }
 
 // k_cg_apply_finish by teams
+template <bool MS>
 __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish_team(DevP P) {
   int p;
   const Team tm = team_of(p);
@@ -2077,7 +2102,7 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish_team(DevP P) {
   float wv = P.cg_w[p];
   if (P.cg_restart[w] != 0) {
     const float inv_r0 = 1.0f / P.vel[p].w;
-    const float ar = accel_divergence_team(P, p, inv_r0, tm);
+    const float ar = accel_divergence_team<MS>(P, p, inv_r0, tm);
     if (tm.t == 0) {
       const float t = ADF_FMA(-P.reg[p], P.cg_corr[p], ar);
       wv = -(scale * t) + wv;
@@ -2450,21 +2475,20 @@ __global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int b
 // ---------------------------------------------------------------------------------------- apply pressure
 // pressure.py:393-414 (lone particles: a push limited like a rigid contact's depenetration) and 461-480
 // (v += dt a, warm start stored dt-free). A lone particle has no neighbours, so no other particle reads its kappa.
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
+  constexpr bool MS = (NBX & MS_FLAG) != 0;
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const float dt = P.dt;
   float4 vi = P.vel[p];
   float kap = P.kappa[p];
-  const int ns = slot_count(P, p);
-  const bool lone = P.cnt[p] == 0 && kap > 0.0f && ns > 0;
+  const bool lone = P.cnt[p] == 0 && kap > 0.0f && slot_count(P, p) > 0;
   // the walls' summed gradient, the Psi-weighted wall velocity, the Psi sum and the largest-Psi slot
   float Gx = 0.0f, Gy = 0.0f, Gz = 0.0f, vbx = 0.0f, vby = 0.0f, vbz = 0.0f, ps = 0.0f, pbest = 0.0f;
   int best = -1;
   if (lone) {
-    for (int b = 0; b < ns; ++b) {
-      const size_t o = slot_at(P, b, p);
+    for_slots<MS>(P, p, [&](int b, size_t o) {
       const float4 sg = P.slot_g[o], vbs = P.slot_vb[o];
       Gx = Gx + sg.x;
       Gy = Gy + sg.y;
@@ -2477,7 +2501,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
         pbest = sg.w;
         best = b;
       }
-    }
+    });
     const float g = __fsqrt_rn(dot_plain(Gx, Gy, Gz, Gx, Gy, Gz));
     if (g > 0.0f) {
       float ux = vbx, uy = vby, uz = vbz;
@@ -2494,13 +2518,13 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
     }
   }
   float ax, ay, az;
-  pressure_accel<NB>(P, p, P.pos[p], ax, ay, az);
+  pressure_accel<NBX>(P, p, P.pos[p], ax, ay, az);
   P.acc[p] = make_float4(ax, ay, az, 0.0f);
   float vx = ADF_FMA(dt, ax, vi.x), vy = ADF_FMA(dt, ay, vi.y), vz = ADF_FMA(dt, az, vi.z);
   // pressure.py:417-458: Coulomb friction of a lone particle on its walls after the update: the walls' push
   // dv_n = dt k |G| takes up to mu dv_n of its tangential speed relative to them, never reversing it; mu is that of
   // the wall in its largest-Psi slot (a particle wall has none)
-  if (lone && P.wall_friction && P.n_shapes > 0 && kap > 0.0f && best >= 0) {
+  if (MS && lone && P.wall_friction && P.n_shapes > 0 && kap > 0.0f && best >= 0) {  // box walls only
     const float g = __fsqrt_rn(dot_plain(Gx, Gy, Gz, Gx, Gy, Gz));
     const int sh = P.slot_cap > 1 ? __float_as_int(P.slot_n[slot_at(P, best, p)].w) : P.n_shapes;
     if (g > 0.0f && ps > 0.0f && sh >= 0 && sh < P.n_shapes && P.sh_half[sh].w > 0.0f) {
@@ -2527,8 +2551,9 @@ __global__ void __launch_bounds__(BLOCK) k_apply(DevP P) {
 // integrate.py:150-178: gravity, external force, XSPH with Monaghan's symmetric weight m_j / rho_bar_ij.
 // The output array becomes the velocity array for the rest of the step (the host swaps them), so boundary
 // particles carry their own velocity across: the wall advance in k_finish reads it.
-template <int NB>
+template <int NBX>
 __global__ void __launch_bounds__(BLOCK, 3) k_xsph(DevP P) {
+  constexpr int NB = NBX & NB_MASK;
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int nf = P.nfw[0];
   if (p >= nf) {
@@ -2709,6 +2734,7 @@ __device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float 
   if (moved) atomicAdd(&P.projected[w], 1);
 }
 
+template <bool MS>
 __global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   int nf = P.nfw[0];
@@ -2726,7 +2752,7 @@ __global__ void __launch_bounds__(BLOCK) k_finish(DevP P) {
   }
   int w = P.world_s[p];
   float vx = vi.x, vy = vi.y, vz = vi.z;
-  if (P.slot_cap > 1) {
+  if constexpr (MS) {
     finish_walls(P, p, w, dt, x, y, z, vx, vy, vz);
   } else if (P.slot_g[p].w >= 0.0f) {
     float4 nn = P.slot_n[p], vb = P.slot_vb[p], xb = P.slot_xb[p];
