@@ -536,6 +536,12 @@ def fp64_check(args, dev, warm: bool, worlds: int = 16, steps: int = 30) -> dict
     q64, v64 = orc.state64()
     comp = {"fp64_oracle": _fp64_compression(sc, q64.astype(np.float32), v64.astype(np.float32))}
     for key, learned in (("gpu_learned", True), ("gpu_plain", False)) if warm else (("gpu_plain", False),):
+        # a fresh model per run: a run's emitters and sinks change the model's phase and flags in place
+        keep, WORLDS = WORLDS, worlds
+        try:
+            sc = make_scene(args.workload, dev)
+        finally:
+            WORLDS = keep
         sol = SolverDFSPH(sc.model, sc.config)
         sol.add_emitters([(w, c, h, r, v, p) for w, c, h, r, v, p, _, _ in spouts(sc)])
         if learned:
