@@ -474,7 +474,9 @@ void cg_product(adf_solver* s, DevP& P, cudaStream_t st, const float* vec, const
 
 void cg_sums(adf_solver* s, DevP& P, cudaStream_t st, int with_max) {
   prof_begin(s, 7, st);
-  if (P.n_chunks > 0) LAUNCH(s, k_sums2_fused, P.n_chunks, 256, st, P, with_max, 0);
+  if (P.n_chunks > 0 && s->max_world_chunks <= WARP_FOLD_MAX_CHUNKS)
+    LAUNCH(s, k_sums2_warps, (P.n_chunks + CHECK_WARPS - 1) / CHECK_WARPS, 32 * CHECK_WARPS, st, P, with_max, 0);
+  else if (P.n_chunks > 0) LAUNCH(s, k_sums2_fused, P.n_chunks, 256, st, P, with_max, 0);
   else LAUNCH(s, k_world_sum2, s->W, 256, st, P, with_max);
   prof_end(s, st);
 }
@@ -517,7 +519,10 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
   }
   if (P.n_chunks > 0) {  // sums with the maximum, stop test and beta per world, unconverged count: one launch
     prof_begin(s, 7, st);
-    LAUNCH(s, k_sums2_fused, P.n_chunks, 256, st, P, 1, 1);
+    if (s->max_world_chunks <= WARP_FOLD_MAX_CHUNKS)
+      LAUNCH(s, k_sums2_warps, (P.n_chunks + CHECK_WARPS - 1) / CHECK_WARPS, 32 * CHECK_WARPS, st, P, 1, 1);
+    else
+      LAUNCH(s, k_sums2_fused, P.n_chunks, 256, st, P, 1, 1);
     prof_end(s, st);
   } else {
     cg_sums(s, P, st, 1);
@@ -622,8 +627,8 @@ void dual_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
     prof_end(s, st);
     prof_begin(s, 7, st);
     if (P.n_chunks > 0)
-      LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, (const float*)Q.err_orig, P.chunk_begin, P.chunk_end, P.part_sum,
-             P.part_max, (int*)nullptr, (const int*)nullptr, (const int*)nullptr);
+      LAUNCH(s, k_chunk_sum, (P.n_chunks + 7) / 8, 256, st, (const float*)Q.err_orig, P.chunk_begin, P.chunk_end,
+             P.n_chunks, P.part_sum, P.part_max);
     LAUNCH(s, k_world_check, W, 256, st, P, 0, pass == 0 ? P.sum_c : P.sum_l, pass == 0 ? P.max_c : P.max_l);
     prof_end(s, st);
   }
@@ -1881,8 +1886,8 @@ int adf_world_sum(adf_solver* s, const float* values, double* out_sum, float* ou
   cudaStream_t st = (cudaStream_t)stream;
   const DevP& P = s->d;
   if (P.n_chunks > 0)
-    LAUNCH(s, k_chunk_sum, P.n_chunks, 256, st, values, P.chunk_begin, P.chunk_end, P.part_sum, P.part_max,
-           (int*)nullptr, (const int*)nullptr, (const int*)nullptr);
+    LAUNCH(s, k_chunk_sum, (P.n_chunks + 7) / 8, 256, st, values, P.chunk_begin, P.chunk_end, P.n_chunks, P.part_sum,
+           P.part_max);
   LAUNCH(s, k_world_check, s->W, 256, st, P, 0, out_sum, out_max);
   return check_launch();
 }

@@ -2170,24 +2170,52 @@ __global__ void __launch_bounds__(256) k_world_sum2(DevP P, int with_max) {
   if (with_max) P.emax[w] = maxr(mx, 0.0f);
 }
 
-// Chunk partials of the per-world sums. With `converged` given, chunks of converged worlds keep their partials (their
-// values no longer change) except chunk 0, whose block also clears the unconverged count.
-__global__ void __launch_bounds__(256) k_chunk_sum(const float* __restrict__ v, const int* chunk_begin,
-                                                   const int* chunk_end, double* part_sum, float* part_max,
-                                                   int* n_unconv, const int* chunk_world, const int* converged) {
-  __shared__ double smd[8];
-  __shared__ float smf[8];
-  int c = blockIdx.x;
-  if (converged && c != 0 && converged[chunk_world[c]]) return;
-  int i = chunk_begin[c] + threadIdx.x;
-  bool in = i < chunk_end[c];
-  float x = in ? v[i] : 0.0f;
-  double s = fold256(in ? (double)x : 0.0, smd);
-  float m = block_max256(in ? x : -3.4e38f, smf);
-  if (threadIdx.x == 0) {
-    part_sum[c] = s;
+// fold256's tree computed by one warp: value L of the 256 (group L / 32, lane L % 32) comes from value(L); each group
+// of 32 folds by the same shuffles (offsets 16..1), then the 8 group sums fold with offsets 4, 2, 1. Valid in lane 0.
+template <class F>
+__device__ __forceinline__ double fold256_warp(F value) {
+  const int lane = threadIdx.x & 31;
+  double s[8];
+#pragma unroll
+  for (int g = 0; g < 8; ++g) {
+    double v = value(32 * g + lane);
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+    s[g] = v;
+  }
+#pragma unroll
+  for (int o = 4; o >= 1; o >>= 1)
+#pragma unroll
+    for (int l = 0; l < o; ++l) s[l] = s[l] + s[l + o];
+  return s[0];
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Per-chunk float64 sums (fold256's tree) and maxima of v, one warp per 256-value chunk, 8 chunks per block (a block
+// per chunk spent most of its time being scheduled on workloads of tens of thousands of chunks).
+__global__ void __launch_bounds__(256) k_chunk_sum(const float* __restrict__ v, const int* __restrict__ chunk_begin,
+                                                   const int* __restrict__ chunk_end, int n_chunks, double* part_sum,
+                                                   float* part_max) {
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (c >= n_chunks) return;
+  const int b = chunk_begin[c], e = chunk_end[c];
+  float m = -3.4e38f;
+  const double sum = fold256_warp([&](int L) -> double {
+    const int i = b + L;
+    const float x = i < e ? v[i] : 0.0f;
+    if (i < e) m = fmaxf(m, x);
+    return i < e ? (double)x : 0.0;
+  });
+  m = warp_max(m);
+  if (lane == 0) {
+    part_sum[c] = sum;
     part_max[c] = m;
-    if (c == 0 && n_unconv) *n_unconv = 0;
   }
 }
 
@@ -2298,32 +2326,6 @@ __global__ void __launch_bounds__(256) k_check_fused(DevP P) {
     const int listed = build_worklist(P, true);
     if (threadIdx.x == 0) *P.n_unconv = listed;
   }
-}
-
-// fold256's tree computed by one warp: value L of the 256 (group L / 32, lane L % 32) comes from value(L); each group
-// of 32 folds by the same shuffles (offsets 16..1), then the 8 group sums fold with offsets 4, 2, 1. Valid in lane 0.
-template <class F>
-__device__ __forceinline__ double fold256_warp(F value) {
-  const int lane = threadIdx.x & 31;
-  double s[8];
-#pragma unroll
-  for (int g = 0; g < 8; ++g) {
-    double v = value(32 * g + lane);
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
-    s[g] = v;
-  }
-#pragma unroll
-  for (int o = 4; o >= 1; o >>= 1)
-#pragma unroll
-    for (int l = 0; l < o; ++l) s[l] = s[l] + s[l + o];
-  return s[0];
-}
-
-__device__ __forceinline__ float warp_max(float v) {
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
-  return __shfl_sync(0xffffffffu, v, 0);
 }
 
 // k_check_fused with one warp per 256-particle chunk (8 chunks per block), for models whose worlds have at most
@@ -2466,6 +2468,114 @@ __global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int b
     __threadfence();
     int open = 0;
     for (int k = threadIdx.x; k < P.W; k += 256) open += __ldcg(&P.converged[k]) ? 0 : 1;
+    int tot;
+    block_exclusive_scan(open, smi, tot);
+    if (threadIdx.x == 0) *P.n_unconv = tot;
+  }
+}
+
+// fold256_warp for two sums at once (value(L, x, y) gives value L of each)
+template <class F>
+__device__ __forceinline__ void fold256_warp2(F value, double& rx, double& ry) {
+  double sx[8], sy[8];
+#pragma unroll
+  for (int g = 0; g < 8; ++g) {
+    double x, y;
+    value(32 * g + (threadIdx.x & 31), x, y);
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      x = x + __shfl_down_sync(0xffffffffu, x, o);
+      y = y + __shfl_down_sync(0xffffffffu, y, o);
+    }
+    sx[g] = x;
+    sy[g] = y;
+  }
+#pragma unroll
+  for (int o = 4; o >= 1; o >>= 1)
+#pragma unroll
+    for (int l = 0; l < o; ++l) {
+      sx[l] = sx[l] + sx[l + o];
+      sy[l] = sy[l] + sy[l + o];
+    }
+  rx = sx[0];
+  ry = sy[0];
+}
+
+// k_sums2_fused with one warp per chunk (8 per block), for models whose worlds have at most WARP_FOLD_MAX_CHUNKS
+// chunks: the same partials, world folds, stop tests, beta and unconverged count in the same tree orders.
+__global__ void __launch_bounds__(32 * CHECK_WARPS) k_sums2_warps(DevP P, int with_max, int beta) {
+  __shared__ int tickets[CHECK_WARPS];
+  __shared__ int smi[32];
+  __shared__ bool glast;
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const int c = blockIdx.x * CHECK_WARPS + wq;
+  int ticket = 0;
+  if (c < P.n_chunks) {
+    const int w = P.chunk_world[c];
+    const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
+    ticket = c == c0 ? 1 : 0;
+    if (!P.converged[w]) {
+      const int b = P.chunk_begin[c], e = P.chunk_end[c];
+      float m = -3.4e38f;
+      double sx, sy;
+      fold256_warp2([&](int L, double& x, double& y) {
+        const int i = b + L;
+        const float2 v = i < e ? P.cg_pair[i] : make_float2(0.0f, 0.0f);
+        if (i < e) m = fmaxf(m, v.y);
+        x = i < e ? (double)v.x : 0.0;
+        y = i < e ? (double)v.y : 0.0;
+      }, sx, sy);
+      m = warp_max(m);
+      bool last = false;
+      if (lane == 0) {
+        P.part2[c] = make_double2(sx, sy);
+        P.part_max[c] = m;
+        last = world_ticket(P, w, c1 - c0);
+      }
+      last = __shfl_sync(0xffffffffu, last, 0);
+      if (last) {
+        __threadfence();
+        float mm = -3.4e38f;
+        double wx, wy;
+        fold256_warp2([&](int L, double& x, double& y) {
+          x = 0.0;
+          y = 0.0;
+          for (int k = c0 + L; k < c1; k += 256) {
+            const double2 pk = __ldcg(&P.part2[k]);
+            x = x + pk.x;
+            y = y + pk.y;
+            mm = fmaxf(mm, __ldcg(&P.part_max[k]));
+          }
+        }, wx, wy);
+        const float mx = warp_max(mm);
+        if (lane == 0) {
+          P.cg_sums[w] = make_double2(wx, wy);
+          if (with_max) P.emax[w] = maxr(mx, 0.0f);
+          if (beta) cg_beta_world(P, w);
+        }
+      }
+      ticket = last ? 1 : 0;
+    }
+  }
+  if (!beta) return;  // the same for every thread of the launch
+  if (lane == 0) tickets[wq] = ticket;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int k = 0; k < CHECK_WARPS; ++k) t += tickets[k];
+    glast = false;
+    if (t > 0) {
+      __threadfence();
+      const unsigned before = atomicAdd(P.gdone, (unsigned)t);
+      glast = before + (unsigned)t == (unsigned)P.n_chunk_worlds;
+      if (glast) *P.gdone = 0u;
+    }
+  }
+  __syncthreads();
+  if (glast) {
+    __threadfence();
+    int open = 0;
+    for (int k = threadIdx.x; k < P.W; k += blockDim.x) open += __ldcg(&P.converged[k]) ? 0 : 1;
     int tot;
     block_exclusive_scan(open, smi, tot);
     if (threadIdx.x == 0) *P.n_unconv = tot;
