@@ -830,7 +830,33 @@ __device__ __forceinline__ void wall_volume(const DevP& P, float phi, float& psi
 }
 
 __device__ __forceinline__ void wall_slot_fill(const DevP& P, int p, float4 xi, float c, float gx, float gy, float gz,
-                                               float mx, float my, float mz);
+                                               float mx, float my, float mz, float phi);
+
+// colour_distance (particle_walls.py:87-98, 30 bisection steps) by a team of WT lanes, two steps per round: with
+// mid m1 of [lo, hi], lanes 0, 1 and 2 evaluate Psi at m0 = mid(lo, m1), m1 and m2 = mid(m1, hi), the two possible
+// midpoints of the second step, so the 15 rounds choose exactly the intervals of the 30 serial steps.
+__device__ __forceinline__ float colour_distance_team(const KC& k, float c, int t, int t0, unsigned mask) {
+  float lo = -k.h, hi = k.h;
+#pragma unroll 1
+  for (int r = 0; r < 15; ++r) {
+    const float m1 = __fmul_rn(0.5f, __fadd_rn(lo, hi));
+    const float m0 = __fmul_rn(0.5f, __fadd_rn(lo, m1)), m2 = __fmul_rn(0.5f, __fadd_rn(m1, hi));
+    float psi, dpsi;
+    halfspace(k, t == 0 ? m0 : (t == 2 ? m2 : m1), psi, dpsi);
+    const int gt = psi > c ? 1 : 0;
+    const int g0 = __shfl_sync(mask, gt, t0), g1 = __shfl_sync(mask, gt, t0 + 1), g2 = __shfl_sync(mask, gt, t0 + 2);
+    if (g1) {
+      lo = m1;
+      if (g2) lo = m2;
+      else hi = m2;
+    } else {
+      hi = m1;
+      if (g0) lo = m0;
+      else hi = m0;
+    }
+  }
+  return __fmul_rn(0.5f, __fadd_rn(lo, hi));
+}
 
 // One listed liquid particle's wall slot, by one lane (a cell of its 27 holds boundary particles).
 __device__ __forceinline__ void wall_slot_one(const DevP& P, int p) {
@@ -891,19 +917,18 @@ __device__ __forceinline__ void wall_slot_one(const DevP& P, int p) {
     my = ADF_FMA(wj, vj.y, my);
     mz = ADF_FMA(wj, vj.z, mz);
   }
-  wall_slot_fill(P, p, xi, c, gx, gy, gz, mx, my, mz);
+  wall_slot_fill(P, p, xi, c, gx, gy, gz, mx, my, mz, colour_distance(P.kc, minr(c, 1.0f)));
 }
 
-// The slot of liquid particle p from its colour sums over the wall particles within h (ascending wall id): mean wall
-// velocity, distance by bisection, amplitude, taper, and the four slot records.
+// The slot of liquid particle p from its colour sums over the wall particles within h (ascending wall id) and the
+// colour distance phi of c (colour_distance): mean wall velocity, amplitude, taper, and the four slot records.
 __device__ __forceinline__ void wall_slot_fill(const DevP& P, int p, float4 xi, float c, float gx, float gy, float gz,
-                                               float mx, float my, float mz) {
+                                               float mx, float my, float mz, float phi) {
   mx = mx / c;
   my = my / c;
   mz = mz / c;
   float lg = __fsqrt_rn(dot_plain(gx, gy, gz, gx, gy, gz));
   if (c < (float)(1.0e-4) || lg <= 0.0f) return;
-  float phi = colour_distance(P.kc, minr(c, 1.0f));
   if (!(phi < P.reach && phi + P.wall_offset < P.kc.h)) return;
   float nx = -gx / lg, ny = -gy / lg, nz = -gz / lg;
   float psi, dpsi;
@@ -1060,9 +1085,13 @@ __global__ void __launch_bounds__(BLOCK) k_wall_slots(DevP P) {
         }
       }
     }
-    if (act && t == 0) {
-      if (!team) wall_slot_one(P, q);
-      else if (mt > 0) wall_slot_fill(P, q, xi, c, gx, gy, gz, mx, my, mz);
+    if (act && team && mt > 0) {  // the whole team bisects the colour distance of its first lane's sums
+      static_assert(WT >= 3, "the team bisection evaluates three points per round");
+      const unsigned tmask = ((1u << WT) - 1u) << t0;
+      const float phi = colour_distance_team(P.kc, minr(__shfl_sync(tmask, c, t0), 1.0f), t, t0, tmask);
+      if (t == 0) wall_slot_fill(P, q, xi, c, gx, gy, gz, mx, my, mz, phi);
+    } else if (act && t == 0 && !team) {
+      wall_slot_one(P, q);
     }
     __syncwarp();
   }
