@@ -200,10 +200,11 @@ def train(features: np.ndarray, targets: np.ndarray, *, epochs: int = 20, batch:
 
 
 def collect_pairs(solver, state_a, state_b, dt: float, steps: int, every: int = 1, per_record: int | None = None,
-                  seed: int = 0):
+                  seed: int = 0, drive=None):
     """Run ``steps`` steps of ``solver`` (the plain start unless a model is set) and gather (features, corrections of
-    the converged warm starts to the plain starts) of the liquid particles every ``every`` steps; ``per_record`` rows drawn without replacement per
-    record (all when None). Returns float32 arrays [N][16] and [N][2] and the final (state_a, state_b)."""
+    the converged warm starts to the plain starts) of the liquid particles every ``every`` steps; ``per_record`` rows
+    drawn without replacement per record (all when None); ``drive(state, k)`` before step k moves the scene's
+    kinematic walls. Returns float32 arrays [N][16] and [N][2] and the final (state_a, state_b)."""
     import torch
 
     solver.record_features(True)
@@ -214,6 +215,8 @@ def collect_pairs(solver, state_a, state_b, dt: float, steps: int, every: int = 
         live = None
         if k % every == 0:
             live = ((model.particle_flags & 1) != 0) & (model.sph.phase >= 1)
+        if drive is not None:
+            drive(state_a, k)
         solver.step(state_a, state_b, None, None, dt)
         state_a, state_b = state_b, state_a
         if live is None:
@@ -231,20 +234,27 @@ def collect_pairs(solver, state_a, state_b, dt: float, steps: int, every: int = 
     return np.concatenate(feats).astype(np.float32), np.concatenate(targs).astype(np.float32), state_a, state_b
 
 
-def generate_pairs(device=None, pairs: int = 2_000_000, seed: int = 1, steps: int = 200, log=None):
-    """Training pairs from seeded runs of the two plain workloads (half each): the 1,048,576-particle dam break and
-    the 256 batched worlds with spouts, ``steps`` steps each, a record every 4 steps."""
+SOURCES = ("large_dam_break", "batched_worlds", "pour_bowls")
+
+
+def generate_pairs(device=None, pairs: int = 2_000_000, seed: int = 1, steps: int = 200, log=None,
+                   sources=SOURCES[:2]):
+    """Training pairs from seeded runs of plain workloads (an equal share each): the 1,048,576-particle dam break, the
+    256 batched worlds with spouts, and 256 worlds of the pour (moving bowls, spouts), ``steps`` steps each, a record
+    every 4 steps."""
     import torch
 
     from .solver import SolverDFSPH, layer_offsets
-    from .testing import batched_worlds, large_dam_break
+    from .testing import batched_worlds, large_dam_break, pour_bowls
 
     dev = device or torch.device("cuda", 0)
     every = 4
-    per = int(np.ceil(pairs / 2 / (steps // every)))
+    per = int(np.ceil(pairs / len(sources) / (steps // every)))
     out_f, out_t = [], []
-    for make in (large_dam_break, batched_worlds):
-        sc = make(device=dev, seed=seed)
+    makers = {"large_dam_break": large_dam_break, "batched_worlds": batched_worlds,
+              "pour_bowls": lambda device, seed: pour_bowls(worlds=256, device=device, seed=seed)}
+    for name in sources:
+        sc = makers[name](device=dev, seed=seed)
         sol = SolverDFSPH(sc.model, sc.config)
         host = sc.model.host()
         specs = []
@@ -257,7 +267,8 @@ def generate_pairs(device=None, pairs: int = 2_000_000, seed: int = 1, steps: in
             specs.append((e["world"], e["centre"], e["half"], rate, e["velocity"], e["pool"]))
         sol.add_emitters(specs)
         a, b = sc.model.state(), sc.model.state()
-        f, t, _, _ = collect_pairs(sol, a, b, sc.dt, steps, every=every, per_record=per, seed=seed)
+        drive = None if sc.motion is None else (lambda st, k, m=sc.motion, dt=sc.dt: m.apply(st, k * dt, dt))
+        f, t, _, _ = collect_pairs(sol, a, b, sc.dt, steps, every=every, per_record=per, seed=seed, drive=drive)
         if log is not None:
             log(f"{sc.name}: {len(f)} pairs")
         out_f.append(f)
@@ -277,8 +288,10 @@ def main(argv=None) -> None:
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--sources", default="large_dam_break,batched_worlds",
+                    help="comma-separated workloads to draw pairs from: " + ", ".join(SOURCES))
     a = ap.parse_args(argv)
-    f, t = generate_pairs(pairs=a.pairs, seed=a.seed, log=print)
+    f, t = generate_pairs(pairs=a.pairs, seed=a.seed, log=print, sources=tuple(a.sources.split(",")))
     m = train(f, t, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, log=print)
     m.save(a.out)
     print(f"saved {a.out}: {len(f)} pairs")

@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--no-warm", action="store_true", help="skip the arms beside the headline (plain or learned, CG, "
                                                               "per-world, FP64 check)")
     ap.add_argument("--plain", action="store_true", help="headline the plain solve instead of the warm-started one")
+    ap.add_argument("--warm-model", default=None, help="a warm-start network file (.npz) instead of the shipped one")
     return ap.parse_args()
 
 
@@ -119,6 +120,13 @@ class Stepper:
             self.sol.step(self.a, self.b, None, None, self.sc.dt)
             self.a, self.b = self.b, self.a
             self.k += 1
+
+
+def warm_model(args):
+    """The warm-start network of the learned arms: ``--warm-model`` or the shipped one."""
+    from alloy_b200.solvers.sph.warmstart import WarmModel, default_model
+
+    return WarmModel.load(args.warm_model) if args.warm_model else default_model()
 
 
 def spouts(sc):
@@ -398,14 +406,14 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
     import torch
 
     from alloy_b200.solvers.sph import SolverDFSPH
-    from alloy_b200.solvers.sph.warmstart import DEFAULT_MODEL, default_model
+    from alloy_b200.solvers.sph.warmstart import DEFAULT_MODEL
 
     full = make_scene(args.workload, dev, **cfg_kw)
     sc = rank_scene(full, args.workload, rank, world, dev)
     sol = SolverDFSPH(sc.model, sc.config)
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
     if judge is not None:
-        sol.set_warm_model(default_model())
+        sol.set_warm_model(warm_model(args))
         sol.warm_judging(judge)
     run = Stepper(sol, sc, sc.model.state(), sc.model.state())
     stream = torch.cuda.current_stream(dev)
@@ -446,7 +454,7 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
         out.update({"rebuilt_world_share": float(np.mean(rebuilt)),
                     "sort_and_rows_ms_per_step": {k: round(prof[k][0] / 20.0, 4) for k in ("sort", "lists")}})
     if judge is not None:
-        out.update({"judge": judge, "model": str(DEFAULT_MODEL.relative_to(ROOT)),
+        out.update({"judge": judge, "model": args.warm_model or str(DEFAULT_MODEL.relative_to(ROOT)),
                     "learned_start_kept": float(np.mean(kept))})
     return out
 
@@ -516,7 +524,6 @@ def fp64_check(args, dev, warm: bool, worlds: int = 16, steps: int = 30) -> dict
 
     from alloy_b200.solvers.sph import SolverDFSPH
     from alloy_b200.solvers.sph.solver import _xform7
-    from alloy_b200.solvers.sph.warmstart import default_model
 
     global WORLDS
     keep, WORLDS = WORLDS, worlds
@@ -545,7 +552,7 @@ def fp64_check(args, dev, warm: bool, worlds: int = 16, steps: int = 30) -> dict
         sol = SolverDFSPH(sc.model, sc.config)
         sol.add_emitters([(w, c, h, r, v, p) for w, c, h, r, v, p, _, _ in spouts(sc)])
         if learned:
-            sol.set_warm_model(default_model())
+            sol.set_warm_model(warm_model(args))
             sol.warm_judging(True)
         run = Stepper(sol, sc, sc.model.state(), sc.model.state())
         err[key] = 0.0
@@ -610,9 +617,9 @@ def run_b200(args):
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
     headline_warm = not args.plain
     if headline_warm:  # the shipped network's starts, judged by the first sweep against the plain start per world
-        from alloy_b200.solvers.sph.warmstart import DEFAULT_MODEL, default_model
+        from alloy_b200.solvers.sph.warmstart import DEFAULT_MODEL
 
-        sol.set_warm_model(default_model())
+        sol.set_warm_model(warm_model(args))
         sol.warm_judging(True)
     run = Stepper(sol, sc, sc.model.state(), sc.model.state())
     stream = torch.cuda.current_stream(dev)
@@ -793,7 +800,7 @@ def run_b200(args):
                 r.pop(k)
         if headline_warm:
             warm["warm_started"] = {"value": value, "vs_plain": value / plain_value, "judge": True,
-                                    "model": str(DEFAULT_MODEL.relative_to(ROOT)),
+                                    "model": args.warm_model or str(DEFAULT_MODEL.relative_to(ROOT)),
                                     "learned_start_kept": float(np.mean(kept)) if kept else None,
                                     "iters_density_mean": float(np.mean(it_den)),
                                     "iters_divergence_mean": float(np.mean(it_div)),
