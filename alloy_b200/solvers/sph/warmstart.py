@@ -158,8 +158,10 @@ DEFAULT_MODEL = __import__("pathlib").Path(__file__).resolve().parent / "data" /
 
 def default_model() -> WarmModel:
     """The network shipped with the package: trained by ``python -m alloy_b200.solvers.sph.warmstart --out
-    alloy_b200/solvers/sph/data/warm_model.npz`` (2,000,000 pairs from seed-1 runs of the 1,048,576-particle dam break
-    and of the 256 batched worlds, 200 steps each, Adam at 1e-3, batch 65,536, 20 epochs)."""
+    alloy_b200/solvers/sph/data/warm_model.npz`` (2,000,000 pairs from a seed-1 run of 256 worlds of the pour, moving
+    bowls and spouts, 200 steps, Adam at 1e-3, batch 65,536, 20 epochs). Trained on the pour alone, it lowers the
+    iterations more on every measured workload than networks trained on the dam break and the batched worlds, or on
+    all three."""
     return WarmModel.load(DEFAULT_MODEL)
 
 
@@ -238,7 +240,7 @@ SOURCES = ("large_dam_break", "batched_worlds", "pour_bowls")
 
 
 def generate_pairs(device=None, pairs: int = 2_000_000, seed: int = 1, steps: int = 200, log=None,
-                   sources=SOURCES[:2]):
+                   sources=("pour_bowls",)):
     """Training pairs from seeded runs of plain workloads (an equal share each): the 1,048,576-particle dam break, the
     256 batched worlds with spouts, and 256 worlds of the pour (moving bowls, spouts), ``steps`` steps each, a record
     every 4 steps."""
@@ -288,7 +290,7 @@ def main(argv=None) -> None:
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--sources", default="large_dam_break,batched_worlds",
+    ap.add_argument("--sources", default="pour_bowls",
                     help="comma-separated workloads to draw pairs from: " + ", ".join(SOURCES))
     a = ap.parse_args(argv)
     f, t = generate_pairs(pairs=a.pairs, seed=a.seed, log=print, sources=tuple(a.sources.split(",")))
