@@ -23,7 +23,8 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_warm_features", "adf_set_warm_judging", "adf_set_autotune", "adf_tuned_configs", "adf_add_emitters",
            "adf_prime", "adf_iteration_work", "adf_set_tuned_config", "adf_get_state_storage", "adf_port_take",
            "adf_port_emit", "adf_energy", "adf_stable_dt", "adf_skin_flags",
-           "adf_add_patch_emitter", "adf_trigger", "adf_mlp_set_wait_limit", "adf_mlp_clear_status")
+           "adf_add_patch_emitter", "adf_trigger", "adf_mlp_set_wait_limit", "adf_mlp_clear_status",
+           "adf_set_persistent", "adf_set_barrier_wait", "adf_clear_status")
 TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph", "lists")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
@@ -42,7 +43,8 @@ class Params(C.Structure):
                 ("capacity", C.c_int), ("v_sep", C.c_double), ("relief_speed", C.c_double),
                 ("project_eps", C.c_double), ("has_bounds", C.c_int), ("bounds_lo", C.c_double * 3),
                 ("bounds_hi", C.c_double * 3), ("cg", C.c_int), ("wall_friction", C.c_int), ("skin", C.c_double),
-                ("skin_cap", C.c_int)]
+                ("skin_cap", C.c_int), ("jitter_speed", C.c_double), ("jitter_ratio", C.c_double),
+                ("tol_den_min", C.c_double)]
 
 
 class ModelDesc(C.Structure):
@@ -129,6 +131,9 @@ def lib() -> C.CDLL:
     L.adf_set_feature_recording.argtypes = [P, i]
     L.adf_warm_features.argtypes = [P, vp, vp]
     L.adf_set_warm_judging.argtypes = [P, i]
+    L.adf_set_persistent.argtypes = [P, i]
+    L.adf_set_barrier_wait.argtypes = [P, C.c_longlong, i]
+    L.adf_clear_status.argtypes = [P]
     L.adf_set_autotune.argtypes = [P, i]
     L.adf_tuned_configs.argtypes = [P, vp, vp, vp]
     L.adf_get_state_storage.argtypes = [P, C.POINTER(StateStorage)]

@@ -18,7 +18,8 @@ LIBDIR = PKG / "lib"
 LIB = LIBDIR / "liballoy_dfsph.so"
 SOURCES = [CSRC / "dfsph_capi.cu", CSRC / "dfsph_noalloc.cu", CSRC / "dfsph_mlp.cu"]
 DEPENDS = SOURCES + [CSRC / "dfsph_kernels.cuh", CSRC / "dfsph_mlp.cuh", CSRC / "dfsph_math.cuh", CSRC / "dfsph_reduce.cuh",
-                     CSRC / "dfsph_port.cuh", CSRC / "dfsph_skin.cuh", PKG.parent / "include" / "alloy_dfsph.h"]
+                     CSRC / "dfsph_port.cuh", CSRC / "dfsph_skin.cuh", CSRC / "dfsph_persist.cuh",
+                     PKG.parent / "include" / "alloy_dfsph.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false", "-prec-div=true",
               "-prec-sqrt=true", "-ftz=false", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 

@@ -14,6 +14,7 @@
 #include "../../include/alloy_dfsph.h"
 #include "dfsph_kernels.cuh"
 #include "dfsph_mlp.cuh"
+#include "dfsph_persist.cuh"
 #include "dfsph_port.cuh"
 #include "dfsph_skin.cuh"
 
@@ -191,6 +192,16 @@ struct adf_solver {
   bool warm_on = false, feat_rec = false, warm_alloc = false, judge = true;
   bool cg = false;  // projected preconditioned CG pressure solve (adf_params.cg)
   bool cg_team = false;  // CG products by teams of TL lanes per particle (models of at most CG_TEAM_MAX particles)
+  // the persistent CG solve (k_cg_solve) of team-product models: on unless adf_set_persistent turned it off
+  bool persist_on = true;
+  int persist_cap[2] = {0, 0};       // co-resident blocks of k_cg_solve<false/true> on this device
+  unsigned persist_extra = 0;        // extra arrivals a barrier waits for (only the wait-expiry test sets it)
+  long long persist_wait = 1 << 22;  // polls of one barrier wait (about a second) before it gives up
+  unsigned* parrive = nullptr;       // device [1]: barrier arrivals of the running launch
+  int* perr = nullptr;               // device [1]: a barrier wait gave up
+  // the resting-jitter rule (adf_params.jitter_speed > 0): per-world tolerance factor and its float64 sums
+  float* jit_scale = nullptr;                 // [W]
+  double *jit_part = nullptr, *jit_flow = nullptr, *jit_head = nullptr;  // [chunks][4], [W][4], [W][4]
   __nv_bfloat16 *mw1 = nullptr, *mw2 = nullptr;
   float *mparams = nullptr, *mnorm = nullptr;
   int* merr = nullptr;
@@ -409,6 +420,7 @@ void set_solve_params(adf_solver* s, DevP& P, int mode, double dt) {
   double tol = mode == 0 ? p.tol_div : p.tol_den;
   P.tol = (float)tol;
   P.tol_max = (float)(tol * p.max_error_factor);
+  P.tol_scale = (mode == 1 && s->jit_scale) ? s->jit_scale : nullptr;  // the density solve under the rule
   P.relief = (mode == 1 && p.relief_speed > 0.0) ? (float)(p.relief_speed * dt * p.lattice_grad) : (float)(1.0e30);
 }
 
@@ -530,6 +542,54 @@ void cg_iteration(adf_solver* s, DevP& P, cudaStream_t st) {
     LAUNCH(s, k_cg_beta, blocks(s->W), BLOCK, st, P);
   }
   LAUNCH(s, k_cg_direction, blocks(n), BLOCK, st, P);
+}
+
+// The CG solve as one persistent launch (k_cg_solve) for team-product models with chunks, outside profiled runs
+// (those time each kernel group of the multi-launch path).
+bool persistent_solve(const adf_solver* s, const DevP& P) {
+  return s->cg && s->cg_team && s->persist_on && !s->prof_on && P.n_chunks > 0 && s->W > 0;
+}
+
+int persistent_cg(adf_solver* s, DevP& P, cudaStream_t st) {
+  const bool ms = s->d.slot_cap > 1;
+  int& cap = s->persist_cap[ms ? 1 : 0];
+  if (cap == 0) {
+    int per_sm = 0, sms = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ms ? k_cg_solve<true> : k_cg_solve<false>, BLOCK, 0));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    cap = per_sm * sms;
+    if (cap <= 0) return fail(ADF_ERR_CUDA, "k_cg_solve: no block of it fits on an SM");
+  }
+  const int n = s->n;
+  CgPersist R{};
+  R.pt_blocks = blocks(n);
+  R.team_blocks = blocks((long long)n * TL);
+  R.warp_fold = s->max_world_chunks <= WARP_FOLD_MAX_CHUNKS ? 1 : 0;
+  R.sum_blocks = R.warp_fold ? (P.n_chunks + CHECK_WARPS - 1) / CHECK_WARPS : P.n_chunks;
+  R.w_blocks = blocks(s->W);
+  R.cap = P.max_it + 2;  // as the WHILE node's cap
+  const int grid = std::min(cap, std::max(std::max(R.pt_blocks, R.team_blocks), std::max(R.sum_blocks, R.w_blocks)));
+  R.expect = (unsigned)grid + s->persist_extra;
+  R.wait_limit = s->persist_wait;
+  R.arrive = s->parrive;
+  R.status = s->perr;
+  CK(cudaMemsetAsync(s->parrive, 0, sizeof(unsigned), st));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(BLOCK);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;  // every block resident: the barriers wait on all of them
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  prof_begin(s, 5, st);
+  if (ms) CK(cudaLaunchKernelEx(&cfg, k_cg_solve<true>, P, R));
+  else CK(cudaLaunchKernelEx(&cfg, k_cg_solve<false>, P, R));
+  ++s->launches;
+  prof_end(s, st);
+  return check_launch();
 }
 
 // The stop test of an iteration and the next iteration's work list (one launch: k_check_warps or k_check_fused).
@@ -658,6 +718,18 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
   const bool subset = warm && first && s->judge && !s->cg && !s->feat_rec;
   P.warm_need = subset ? s->warm_need : nullptr;
   if (subset) LAUNCH(s, k_warm_need, blocks(W), BLOCK, st, P, s->warm_need);
+  if (mode == 1 && s->jit_scale && W > 0) {  // this step's density tolerance per world (solve_driver.py:99-110)
+    if (P.n_chunks > 0) {
+      LAUNCH(s, k_jitter_chunks, (P.n_chunks + 7) / 8, 256, st, P, 1, s->jit_part);
+      LAUNCH(s, k_jitter_worlds, (W + 7) / 8, 256, st, P, 1, (const double*)s->jit_part, s->jit_head);
+    } else {
+      CK(cudaMemsetAsync(s->jit_head, 0, sizeof(double) * JIT_TERMS * W, st));
+    }
+    const adf_params& p = s->prm;
+    LAUNCH(s, k_tol_scale, blocks(W), BLOCK, st, P, (const double*)s->jit_head,
+           p.jitter_ratio > 0.0 ? (const double*)s->jit_flow : nullptr, (float)dt, (float)p.jitter_speed,
+           (float)p.jitter_ratio, (float)p.tol_den, (float)p.tol_den_min, s->jit_scale, s->den_tol);
+  }
   prof_begin(s, 4, st);
   run_tk(s, TK_SOLVE_INIT, st, P);
   prof_end(s, st);
@@ -688,12 +760,12 @@ int solve(adf_solver* s, DevP& P, int mode, double dt, cudaStream_t st, bool gra
   if (rc) return rc;
   const bool dual = warm && s->judge && !s->cg;  // the first-sweep judge is a Jacobi sweep
   if (dual) dual_iteration(s, P, st);
-  if (s->cg && W > 0) cg_init(s, P, st);
-  if (graph) {
-    rc = capture_iterations(s, P, st);
+  if (persistent_solve(s, P)) {  // the CG start and its iterations in one launch
+    rc = persistent_cg(s, P, st);
     if (rc) return rc;
   } else {
-    rc = host_iterations(s, P, st, dual ? 1 : 0);
+    if (s->cg && W > 0) cg_init(s, P, st);
+    rc = graph ? capture_iterations(s, P, st) : host_iterations(s, P, st, dual ? 1 : 0);
     if (rc) return rc;
   }
   prof_begin(s, 8, st);
@@ -1012,6 +1084,12 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&world_chunk_start, cs.size());
   rc |= s->alloc(&d.part_sum, cb.size());
   rc |= s->alloc(&d.part_max, cb.size());
+  if (p.jitter_speed > 0.0) {
+    rc |= s->alloc(&s->jit_scale, W);
+    rc |= s->alloc(&s->jit_part, JIT_TERMS * std::max<size_t>(cb.size(), 1));
+    rc |= s->alloc(&s->jit_flow, JIT_TERMS * (size_t)W);
+    rc |= s->alloc(&s->jit_head, JIT_TERMS * (size_t)W);
+  }
   rc |= s->alloc(&d.emax, W);
   rc |= s->alloc(&s->iters_den, W);
   rc |= s->alloc(&s->iters_div, W);
@@ -1124,6 +1202,11 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   CKC(cudaMemset(d.n_active, 0, 8 * W));
   std::vector<float> tol(W, (float)p.tol_den);
   CKC(cudaMemcpy(s->den_tol, tol.data(), sizeof(float) * W, cudaMemcpyHostToDevice));
+  if (s->jit_scale) {
+    const std::vector<float> one(W, 1.0f);
+    CKC(cudaMemcpy(s->jit_scale, one.data(), sizeof(float) * W, cudaMemcpyHostToDevice));
+    CKC(cudaMemset(s->jit_flow, 0, sizeof(double) * JIT_TERMS * W));
+  }
   if (s->n > 0) {
     k_wall_volume<<<blocks(s->n), BLOCK>>>(s->n, m->flags, m->radius, wall_vol);
     ++s->launches;
@@ -1144,6 +1227,9 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   CKC(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
   CKC(cudaMalloc(&s->body_runs, 2 * sizeof(unsigned long long)));
   CKC(cudaMemset(s->body_runs, 0, 2 * sizeof(unsigned long long)));
+  CKC(cudaMalloc(&s->parrive, sizeof(unsigned)));
+  CKC(cudaMalloc(&s->perr, sizeof(int)));
+  CKC(cudaMemset(s->perr, 0, sizeof(int)));
   CKC(cudaEventCreate(&s->tev[0]));
   CKC(cudaEventCreate(&s->tev[1]));
   CKC(cudaMalloc(&s->snap_kappa, sizeof(float) * n));
@@ -1175,6 +1261,8 @@ void adf_destroy(adf_solver* s) {
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->list_entries) cudaFree(s->list_entries);
   if (s->body_runs) cudaFree(s->body_runs);
+  if (s->parrive) cudaFree(s->parrive);
+  if (s->perr) cudaFree(s->perr);
   for (auto& g : s->graphs) cudaGraphExecDestroy(g.exec);
   if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
   if (s->body_stream) cudaStreamDestroy(s->body_stream);
@@ -1208,6 +1296,10 @@ int enqueue_step(adf_solver* s, const float* q_in, const float* qd_in, float* q_
   CK(cudaMemsetAsync(P.max_speed_bits, 0, sizeof(int) * std::max(s->W, 1), st));
   int rc = prepare(s, P, st);
   if (rc) return rc;
+  if (s->jit_scale && s->prm.jitter_ratio > 0.0 && P.n_chunks > 0) {  // the liquid's mean start velocity per world
+    LAUNCH(s, k_jitter_chunks, (P.n_chunks + 7) / 8, 256, st, P, 0, s->jit_part);
+    LAUNCH(s, k_jitter_worlds, (s->W + 7) / 8, 256, st, P, 0, (const double*)s->jit_part, s->jit_flow);
+  }
   if (s->prm.divergence_solve) {
     rc = solve(s, P, 0, dt, st, graph);
     if (rc) return rc;
@@ -1384,6 +1476,12 @@ int adf_get_report(adf_solver* s, adf_report* r, void* stream) {
     CK(cudaMemcpy(&e, s->merr, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) return fail(ADF_ERR_STATE, "warm-start network: a tensor-core wait expired; the learned starts are invalid");
   }
+  if (s->perr) {
+    int e = 0;
+    CK(cudaMemcpy(&e, s->perr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(ADF_ERR_STATE, "pressure solve: a grid-barrier wait of the persistent CG solve expired; the "
+                                      "step's results are invalid");
+  }
   return ADF_OK;
 }
 
@@ -1545,6 +1643,34 @@ int adf_tuned_configs(adf_solver* s, int32_t* block, int32_t* nb, float* ms) {
     if (nb) nb[k] = s->tune[k].nb;
     if (ms) ms[k] = s->tuned[k] ? s->tune_ms[k] : -1.0f;
   }
+  return ADF_OK;
+}
+
+int adf_set_persistent(adf_solver* s, int enable) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_persistent: null solver");
+  if (s->persist_on != (enable != 0)) ++s->table_version;
+  s->persist_on = enable != 0;
+  return ADF_OK;
+}
+
+int adf_set_barrier_wait(adf_solver* s, long long polls, int extra_arrivals) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_barrier_wait: null solver");
+  if (polls < 1 || extra_arrivals < 0) return fail(ADF_ERR_VALUE, "adf_set_barrier_wait: polls >= 1, extra >= 0");
+  s->persist_wait = polls;
+  s->persist_extra = (unsigned)extra_arrivals;
+  ++s->table_version;
+  return ADF_OK;
+}
+
+int adf_clear_status(adf_solver* s) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_clear_status: null solver");
+  CK(cudaSetDevice(s->device));
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemset(s->perr, 0, sizeof(int)));
+  if (s->merr) CK(cudaMemset(s->merr, 0, sizeof(int)));
+  // a launch that left at a barrier may have left the reductions' tickets counted part way
+  CK(cudaMemset(s->d.wdone, 0, sizeof(int) * std::max(s->W, 1)));
+  CK(cudaMemset(s->d.gdone, 0, sizeof(unsigned)));
   return ADF_OK;
 }
 

@@ -75,6 +75,7 @@ struct DevP {
   int mode;  // 0 divergence, 1 density
   int two_sided;
   float tol, tol_max;
+  const float* tol_scale;  // [W] factor of tol and tol_max per world (the resting-jitter rule), null: 1
   int min_it, max_it;
   int has_bounds;
   float blo[3], bhi[3];
@@ -1844,6 +1845,13 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
 // One CG per world on w = A k - b, k >= k_lo (krylov.py:1-17), A k = -dt^n (Ar(k) - reg k). Each kernel follows
 // the reference kernel of the same name (krylov.py:71-246); a + b c updates are fused (the oracle fuses the same
 // ones), per-world dot products are the float64 sums of k_sums2_fused in the caller's order.
+// The stop test of a world at iteration `it` (pressure.py:370-390, krylov.py:236-241): converged after min_it when the
+// mean and the maximum are within tol and tol_max, both times the world's tolerance factor, or at max_it.
+__device__ __forceinline__ bool stop_test(const DevP& P, int w, int it, float mean, float mx) {
+  const float ts = P.tol_scale != nullptr ? P.tol_scale[w] : 1.0f;
+  return (it >= P.min_it && mean <= P.tol * ts && mx <= P.tol_max * ts) || it >= P.max_it;
+}
+
 __device__ __forceinline__ bool cg_skip(const DevP& P, int w, int gated) {
   return P.converged[w] != 0 || (gated && P.cg_restart[w] == 0);
 }
@@ -1891,8 +1899,9 @@ struct Team {
   unsigned mask;   // the team's lanes
 };
 
-__device__ __forceinline__ Team team_of(int& p) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+// The team of this thread in block `vb` of BLOCK threads (a launch's own block, or a persistent kernel's virtual one).
+__device__ __forceinline__ Team team_at(int vb, int& p) {
+  const int g = vb * BLOCK + threadIdx.x;
   p = g / TL;
   Team tm;
   tm.t = g % TL;
@@ -1900,6 +1909,8 @@ __device__ __forceinline__ Team team_of(int& p) {
   tm.mask = ((1u << TL) - 1u) << tm.t0;
   return tm;
 }
+
+__device__ __forceinline__ Team team_of(int& p) { return team_at(blockIdx.x, p); }
 
 __device__ __forceinline__ int2 row_entry(const DevP& P, int p, int k) { return __ldcs(P.nbrjf + p + (size_t)k * P.n); }
 
@@ -1986,11 +1997,12 @@ __device__ __forceinline__ float accel_divergence_team(const DevP& P, int p, flo
   return ar;
 }
 
-// k_cg_accel by teams (grid: TL threads per particle)
+// k_cg_accel by teams (grid: TL threads per particle). The kernels below are bodies run for one block `vb` of BLOCK
+// threads, launched one block each by their __global__ wrappers or looped over by the persistent solve (k_cg_solve).
 template <bool MS>
-__global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* vec, const float* vr, int gated) {
+__device__ __forceinline__ void cg_accel_team_at(const DevP& P, const float* vec, const float* vr, int gated, int vb) {
   int p;
-  const Team tm = team_of(p);
+  const Team tm = team_at(vb, p);
   if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
   DevP Q = P;
   Q.kappa = const_cast<float*>(vec);
@@ -2000,12 +2012,17 @@ __global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* ve
   if (tm.t == 0) P.acc[p] = make_float4(ax, ay, az, 0.0f);
 }
 
+template <bool MS>
+__global__ void __launch_bounds__(BLOCK) k_cg_accel_team(DevP P, const float* vec, const float* vr, int gated) {
+  cg_accel_team_at<MS>(P, vec, vr, gated, blockIdx.x);
+}
+
 // k_cg_apply by teams
 template <bool MS>
-__global__ void __launch_bounds__(BLOCK) k_cg_apply_team(DevP P, const float* vec, float* out, int gated, int bias,
-                                                         int accumulate) {
+__device__ __forceinline__ void cg_apply_team_at(const DevP& P, const float* vec, float* out, int gated, int bias,
+                                                 int accumulate, int vb) {
   int p;
-  const Team tm = team_of(p);
+  const Team tm = team_at(vb, p);
   if (p >= P.nfw[0] || cg_skip(P, P.world_s[p], gated)) return;
   const float inv_r0 = 1.0f / P.vel[p].w;
   const float ar = accel_divergence_team<MS>(P, p, inv_r0, tm);
@@ -2021,9 +2038,15 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_team(DevP P, const float* ve
   out[p] = v;
 }
 
+template <bool MS>
+__global__ void __launch_bounds__(BLOCK) k_cg_apply_team(DevP P, const float* vec, float* out, int gated, int bias,
+                                                         int accumulate) {
+  cg_apply_team_at<MS>(P, vec, out, gated, bias, accumulate, blockIdx.x);
+}
+
 // krylov.py:104-133: active set, z = M^-1 r on F (r = -w), first direction p = z; pair.x = r.z
-__global__ void __launch_bounds__(BLOCK) k_cg_init(DevP P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void cg_init_at(const DevP& P, int vb) {
+  const int p = vb * BLOCK + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const float dt = P.dt;
   const float scale = P.mode == 0 ? dt : dt * dt;
@@ -2037,17 +2060,21 @@ __global__ void __launch_bounds__(BLOCK) k_cg_init(DevP P) {
   P.cg_pair[P.id_of[p]] = make_float2(-w * zi, 0.0f);
 }
 
-__global__ void k_cg_first_rz(DevP P) {
-  int w = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(BLOCK) k_cg_init(DevP P) { cg_init_at(P, blockIdx.x); }
+
+__device__ __forceinline__ void cg_first_rz_at(const DevP& P, int vb) {
+  const int w = vb * BLOCK + threadIdx.x;
   if (w >= P.W) return;
   P.cg_rz[w] = P.cg_sums[w].x;
   P.cg_restart[w] = 0;
   P.cg_act_new[w] = 0;
 }
 
+__global__ void __launch_bounds__(BLOCK) k_cg_first_rz(DevP P) { cg_first_rz_at(P, blockIdx.x); }
+
 // krylov.py:146-170: k += a p on F, projected onto k >= k_lo (the clamped part into corr); w += a A p
-__global__ void __launch_bounds__(BLOCK) k_cg_step(DevP P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void cg_step_at(const DevP& P, int vb) {
+  const int p = vb * BLOCK + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
   if (P.converged[w]) return;
@@ -2071,6 +2098,8 @@ __global__ void __launch_bounds__(BLOCK) k_cg_step(DevP P) {
   P.cg_corrr[p] = c / r0;
   P.cg_w[p] = ADF_FMA(a, P.cg_ap[p], P.cg_w[p]);
 }
+
+__global__ void __launch_bounds__(BLOCK) k_cg_step(DevP P) { cg_step_at(P, blockIdx.x); }
 
 // krylov.py:148-204 after the step: in worlds where k_cg_step clamped a variable, w += A corr (the correction
 // product of k_cg_apply: its acceleration field comes from k_cg_accel, launched for the same worlds); then in every
@@ -2119,9 +2148,9 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish(DevP P) {
 
 // k_cg_apply_finish by teams
 template <bool MS>
-__global__ void __launch_bounds__(BLOCK) k_cg_apply_finish_team(DevP P) {
+__device__ __forceinline__ void cg_apply_finish_team_at(const DevP& P, int vb) {
   int p;
-  const Team tm = team_of(p);
+  const Team tm = team_at(vb, p);
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
   if (P.converged[w]) return;
@@ -2141,6 +2170,9 @@ __global__ void __launch_bounds__(BLOCK) k_cg_apply_finish_team(DevP P) {
   if (tm.t == 0) cg_finish_one(P, p, w, wv, scale, div);
 }
 
+template <bool MS>
+__global__ void __launch_bounds__(BLOCK) k_cg_apply_finish_team(DevP P) { cg_apply_finish_team_at<MS>(P, blockIdx.x); }
+
 // krylov.py:207-233: per world the stop test (as k_world_check), then beta = r.z_new / r.z (0 after a set change)
 __device__ __forceinline__ void cg_beta_world(const DevP& P, int w) {
   const int it = P.iters[w] + 1;
@@ -2155,7 +2187,7 @@ __device__ __forceinline__ void cg_beta_world(const DevP& P, int w) {
   P.cg_act_new[w] = 0;
   P.cg_rz[w] = sm.x;
   P.cg_step[w] = beta;
-  if ((it >= P.min_it && mean <= P.tol && P.emax[w] <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+  if (stop_test(P, w, it, mean, P.emax[w])) P.converged[w] = 1;
 }
 
 __global__ void k_cg_beta(DevP P) {
@@ -2166,8 +2198,8 @@ __global__ void k_cg_beta(DevP P) {
 }
 
 // krylov.py:236-246: p = z + beta p on F, 0 elsewhere
-__global__ void __launch_bounds__(BLOCK) k_cg_direction(DevP P) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void cg_direction_at(const DevP& P, int vb) {
+  const int p = vb * BLOCK + threadIdx.x;
   if (p >= P.nfw[0]) return;
   const int w = P.world_s[p];
   if (P.converged[w]) return;
@@ -2175,6 +2207,8 @@ __global__ void __launch_bounds__(BLOCK) k_cg_direction(DevP P) {
   P.cg_pd[p] = pd;
   P.cg_pdr[p] = pd / P.vel[p].w;
 }
+
+__global__ void __launch_bounds__(BLOCK) k_cg_direction(DevP P) { cg_direction_at(P, blockIdx.x); }
 
 // Per-world (sum x, sum y, max y) of the CG pairs for models without chunks (no particles): one block per world in
 // the fixed tree order of k_world_check; k_sums2_fused does it in one launch otherwise.
@@ -2223,6 +2257,86 @@ __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
   for (int o = 16; o >= 1; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
   return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// --------------------------------------------------------------------------- resting-jitter rule (solve_driver.py)
+// Per world and step the density solve's tolerance is tol x tol_scale[w] (solve_driver.py:5-21): tol_scale =
+// clamp(v dt / (H tol), tol_min / tol, 1) with H = 1.5 S2 / (S1 dt^2 |g|) from the density warm starts kd
+// (S1 = sum kd+, S2 = sum kd+^2 over the world's liquid, kd+ = max(kd, 0)) and v = max(speed, ratio |U|), U the mean
+// velocity of the liquid in the step's start state. The sums are float64 over the caller's order in the tree order of
+// the other per-world sums (chunks of 256 by one warp each, then each world's chunks).
+constexpr int JIT_TERMS = 4;
+
+// term k of particle i (caller's order), 0 unless liquid: flow (k: v_z, 1, v_x, v_y; solve_driver.py:40-51, the
+// step's start velocity) or head (k: kd+, kd+ kd+; solve_driver.py:27-37)
+__device__ __forceinline__ float jitter_term(const DevP& P, int i, int head, int k) {
+  if (!is_fluid_orig(P, i)) return 0.0f;
+  if (!head) {
+    const float* v = P.qd + 3 * (size_t)i;
+    return k == 0 ? v[2] : k == 1 ? 1.0f : k == 2 ? v[0] : v[1];
+  }
+  const float kd = maxr(P.kd[i], 0.0f);
+  return k == 0 ? kd : kd * kd;
+}
+
+// per chunk (one warp each, 8 per block): the float64 sums of the terms (2 for head, 4 for flow) into part[c][k]
+__global__ void __launch_bounds__(256) k_jitter_chunks(DevP P, int head, double* part) {
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (c >= P.n_chunks) return;
+  const int b = P.chunk_begin[c], e = P.chunk_end[c];
+  const int K = head ? 2 : JIT_TERMS;
+  for (int k = 0; k < K; ++k) {
+    const double sum = fold256_warp([&](int L) -> double {
+      const int i = b + L;
+      return i < e ? (double)jitter_term(P, i, head, k) : 0.0;
+    });
+    if (lane == 0) part[(size_t)c * JIT_TERMS + k] = sum;
+  }
+}
+
+// per world (one warp each): its chunks' partials folded into out[w][k]
+__global__ void __launch_bounds__(256) k_jitter_worlds(DevP P, int head, const double* part, double* out) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (w >= P.W) return;
+  const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
+  const int K = head ? 2 : JIT_TERMS;
+  for (int k = 0; k < K; ++k) {
+    const double sum = fold256_warp([&](int L) -> double {
+      double a = 0.0;
+      for (int c = c0 + L; c < c1; c += 256) a = a + part[(size_t)c * JIT_TERMS + k];
+      return a;
+    });
+    if (lane == 0) out[(size_t)w * JIT_TERMS + k] = sum;
+  }
+}
+
+// solve_driver.py:54-74 (tol_scale_kernel) and runtime.py:115-116 (the reported tolerance tol x scale); `flow` null
+// when the flow ratio is 0
+__global__ void k_tol_scale(DevP P, const double* head, const double* flow, float dt, float speed, float ratio,
+                            float tol, float tol_min, float* scale, float* den_tol) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= P.W) return;
+  float s = 1.0f;
+  const float gx = P.gravity[3 * w], gy = P.gravity[3 * w + 1], gz = P.gravity[3 * w + 2];
+  const float g = __fsqrt_rn(dot_plain(gx, gy, gz, gx, gy, gz));
+  const float s1 = (float)head[(size_t)w * JIT_TERMS], s2 = (float)head[(size_t)w * JIT_TERMS + 1];
+  float v = speed;
+  if (flow != nullptr) {
+    const double n = flow[(size_t)w * JIT_TERMS + 1];
+    if (ratio > 0.0f && n > 0.0) {
+      const float ux = (float)(flow[(size_t)w * JIT_TERMS + 2] / n), uy = (float)(flow[(size_t)w * JIT_TERMS + 3] / n);
+      const float uz = (float)(flow[(size_t)w * JIT_TERMS] / n);
+      v = maxr(v, ratio * __fsqrt_rn(dot_plain(ux, uy, uz, ux, uy, uz)));
+    }
+  }
+  if (g > 0.0f && s1 > 0.0f && s2 > 0.0f) {
+    const float depth = (1.5f * s2) / (((s1 * dt) * dt) * g);
+    s = minr(maxr((v * dt) / (depth * tol), tol_min / tol), 1.0f);
+  }
+  scale[w] = s;
+  den_tol[w] = tol * s;
 }
 
 // Per-chunk float64 sums (fold256's tree) and maxima of v, one warp per 256-value chunk, 8 chunks per block (a block
@@ -2277,7 +2391,7 @@ __global__ void __launch_bounds__(256) k_world_check(DevP P, int check, double* 
   double na = P.n_active[w];
   float mean = (float)(s / (na > 1.0 ? na : 1.0));
   P.err_mean[w] = mean;
-  if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+  if (stop_test(P, w, it, mean, mx)) P.converged[w] = 1;
   else atomicAdd(P.n_unconv, 1);
 }
 
@@ -2342,7 +2456,7 @@ __global__ void __launch_bounds__(256) k_check_fused(DevP P) {
         const double na = P.n_active[w];
         const float mean = (float)(sw / (na > 1.0 ? na : 1.0));
         P.err_mean[w] = mean;
-        if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+        if (stop_test(P, w, it, mean, mx)) P.converged[w] = 1;
       }
     }
     ticket = wlast;
@@ -2417,7 +2531,7 @@ __global__ void __launch_bounds__(32 * CHECK_WARPS) k_check_warps(DevP P) {
           const double na = P.n_active[w];
           const float mean = (float)(sw / (na > 1.0 ? na : 1.0));
           P.err_mean[w] = mean;
-          if ((it >= P.min_it && mean <= P.tol && mx <= P.tol_max) || it >= P.max_it) P.converged[w] = 1;
+          if (stop_test(P, w, it, mean, mx)) P.converged[w] = 1;
         }
       }
       ticket = last ? 1 : 0;
@@ -2447,12 +2561,12 @@ __global__ void __launch_bounds__(32 * CHECK_WARPS) k_check_warps(DevP P) {
 // The CG reductions in one launch (chunk partials and k_world_sum2's world fold, same tree order); with `beta`
 // the world's last block also runs k_cg_beta's stop test and beta for its world, and the grid's last block stores the
 // count of worlds still iterating as the unconverged count.
-__global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int beta) {
+__device__ __forceinline__ void sums2_fused_at(const DevP& P, int with_max, int beta, int vb) {
   __shared__ double smd[8];
   __shared__ float smf[8];
   __shared__ int smi[32];
   __shared__ bool wlast, glast;
-  const int c = blockIdx.x;
+  const int c = vb;
   const int w = P.chunk_world[c];
   const int c0 = P.world_chunk_start[w], c1 = P.world_chunk_start[w + 1];
   bool ticket = c == c0;  // as in k_check_fused
@@ -2503,6 +2617,10 @@ __global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int b
   }
 }
 
+__global__ void __launch_bounds__(256) k_sums2_fused(DevP P, int with_max, int beta) {
+  sums2_fused_at(P, with_max, beta, blockIdx.x);
+}
+
 // fold256_warp for two sums at once (value(L, x, y) gives value L of each)
 template <class F>
 __device__ __forceinline__ void fold256_warp2(F value, double& rx, double& ry) {
@@ -2532,12 +2650,12 @@ __device__ __forceinline__ void fold256_warp2(F value, double& rx, double& ry) {
 
 // k_sums2_fused with one warp per chunk (8 per block), for models whose worlds have at most WARP_FOLD_MAX_CHUNKS
 // chunks: the same partials, world folds, stop tests, beta and unconverged count in the same tree orders.
-__global__ void __launch_bounds__(32 * CHECK_WARPS) k_sums2_warps(DevP P, int with_max, int beta) {
+__device__ __forceinline__ void sums2_warps_at(const DevP& P, int with_max, int beta, int vb) {
   __shared__ int tickets[CHECK_WARPS];
   __shared__ int smi[32];
   __shared__ bool glast;
   const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
-  const int c = blockIdx.x * CHECK_WARPS + wq;
+  const int c = vb * CHECK_WARPS + wq;
   int ticket = 0;
   if (c < P.n_chunks) {
     const int w = P.chunk_world[c];
@@ -2609,6 +2727,10 @@ __global__ void __launch_bounds__(32 * CHECK_WARPS) k_sums2_warps(DevP P, int wi
     block_exclusive_scan(open, smi, tot);
     if (threadIdx.x == 0) *P.n_unconv = tot;
   }
+}
+
+__global__ void __launch_bounds__(32 * CHECK_WARPS) k_sums2_warps(DevP P, int with_max, int beta) {
+  sums2_warps_at(P, with_max, beta, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------------------- apply pressure

@@ -12,8 +12,8 @@ Scope of the CUDA path: cubic or Wendland kernel, projected preconditioned CG (t
 or relaxed Jacobi pressure solves, XSPH, particle walls (boundary particles flagged PROXY), static axis-aligned box
 walls evaluated through their SDF (up to four wall slots per particle, projection and the sweep past fast steps, wall
 friction), emitters, sinks and the escape box. Settings outside it are refused in the constructor (``DFSPHConfig.unsupported``); CG falls back to Jacobi
-with a warning when particle masses or rest densities differ, as the reference does (solver.py:89-91), and the
-resting-jitter rule falls back to the base tolerance with a warning.
+with a warning when particle masses or rest densities differ, as the reference does (solver.py:89-91). The
+resting-jitter rule sets each world's density tolerance per step (solve_driver.py:1-118).
 """
 
 from __future__ import annotations
@@ -205,9 +205,6 @@ class SolverDFSPH:
                 log.warning("SolverDFSPH: pressure_solver 'cg' needs one particle mass and rest density; using "
                             "'jacobi'")
                 self.pressure_solver = "jacobi"
-        if cfg.rest_jitter_speed:
-            log.warning("SolverDFSPH: the resting-jitter tolerance rule is not in this build's CUDA path; the density"
-                        " solve runs at max_density_error")
         self._check_capacity(capacity_per_world, phase, ws)
         from .shapes import shape_table
 
@@ -296,6 +293,9 @@ class SolverDFSPH:
         p.relief_speed = cfg.compression_relief_speed or 0.0
         p.project_eps = hc.project_eps
         p.wall_friction = int(bool(cfg.wall_friction))
+        p.jitter_speed = cfg.rest_jitter_speed or 0.0  # the resting-jitter rule (solve_driver.py:1-118)
+        p.jitter_ratio = cfg.rest_jitter_flow_ratio
+        p.tol_den_min = min(cfg.min_density_error, cfg.max_density_error)
         if cfg.world_bounds is not None:
             p.has_bounds = 1
             for a in range(3):
@@ -425,6 +425,21 @@ class SolverDFSPH:
         """Tune block size and gathers in flight of the neighbour-loop kernels at the next step (on by default;
         include/alloy_dfsph.h adf_set_autotune). Off: the default configuration."""
         _lib.check(self._lib.adf_set_autotune(self._h, int(bool(enable))), "autotune")
+
+    def persistent(self, enable: bool = True) -> None:
+        """Run each projected-CG pressure solve of a model of at most 131,072 particles as one persistent launch with
+        grid-wide barriers (on by default; include/alloy_dfsph.h adf_set_persistent). Off: one launch per kernel and
+        iteration. The results are the same bits either way."""
+        _lib.check(self._lib.adf_set_persistent(self._h, int(bool(enable))), "persistent")
+
+    def barrier_wait(self, polls: int = 1 << 22, extra_arrivals: int = 0) -> None:
+        """Test hook of the persistent solve's bounded barrier waits (adf_set_barrier_wait): polls per wait, and
+        arrivals a barrier waits for beyond the grid's blocks (nonzero makes every wait run out)."""
+        _lib.check(self._lib.adf_set_barrier_wait(self._h, int(polls), int(extra_arrivals)), "barrier_wait")
+
+    def clear_status(self) -> None:
+        """Clear the status of the bounded waits after one gave up (adf_clear_status)."""
+        _lib.check(self._lib.adf_clear_status(self._h), "clear_status")
 
     def tuned_configs(self) -> dict[str, dict]:
         """{kernel: {"block", "nb", "ms"}} of the configuration in use (ms < 0: not tuned)."""

@@ -117,9 +117,9 @@ def tank_dam_break(width: int = 32, height: int = 30, depth: int = 32, tank: int
     """The reference harness's dam break (alloy/testing/sph.py:101-115): a width x depth x height lattice block
     against the x_lo wall of an open tank (tank x depth x (height + 10)) spacings, of box shapes h thick (``walls``
     "sdf", the reference's) or one layer of boundary particles ("particles"). The reference's default config
-    (projected CG, CFL 0.2) with the resting-jitter rule off; dt is the CFL step at the Ritter front speed
-    2 sqrt(g H), snapped down to 0.02 s / 2^j (test_speed_gpu.py:30-31)."""
-    cfg = DFSPHConfig(particle_radius=r, **{"rest_jitter_speed": None, **cfg_kw})
+    (projected CG, CFL 0.2, the resting-jitter rule on); dt is the CFL step at the Ritter front speed 2 sqrt(g H),
+    snapped down to 0.02 s / 2^j (test_speed_gpu.py:30-31)."""
+    cfg = DFSPHConfig(particle_radius=r, **cfg_kw)
     cfg.validate()
     s = cfg.spacing
     dt = snap_down(stable_dt(cfg, 2.0 * (9.81 * height * s) ** 0.5), 0.02)

@@ -195,11 +195,11 @@ def workload_config(sc, name: str) -> dict:
     extra = ""
     if name in LIQ9 and name != "dam_break_30k":
         extra = (", resting column(s) at r = 2 mm primed before stepping, dt_max 1.25 ms, projected CG, fast preset "
-                 "(the reference's LIQ-9 speed harness), box tank of boundary particles")
+                 "(the reference's LIQ-9 speed harness), open tank of box walls h thick (their SDF)")
     if name == "dam_break_30k":
         extra = (", 32 x 32 x 30 block against the wall of a 96-spacing tank at r = 2 mm, primed before stepping, "
-                 "default config (projected CG, CFL 0.2) with the resting-jitter rule off, dt the CFL step at the "
-                 "Ritter front speed (the reference's LIQ-9 speed harness), box tank of boundary particles")
+                 "default config (projected CG, CFL 0.2, the resting-jitter rule on), dt the CFL step at the "
+                 "Ritter front speed (the reference's LIQ-9 speed harness), open tank of box walls h thick (their SDF)")
     if name == "batched_worlds":
         extra = ", one spout per world (64 particles per 10 steps)"
     elif name == "pour_bowls":

@@ -62,6 +62,13 @@ typedef struct {
                                Superset rows within h + s are reused per world until a particle of the world moves
                                more than s / 2 or the world's liquid set changes; the rows equal a plain build's */
   int skin_cap;             /* superset row capacity (neighbors_skin.py:155-166 skin_capacity) when skin > 0 */
+  double jitter_speed;      /* [m/s] Config.rest_jitter_speed: the resting-jitter rule of the density solve's tolerance
+                               (solve_driver.py:1-118); 0: off, every world stops at tol_den. On: per world and step
+                               the tolerance is min(tol_den, v dt / H), floored at tol_den_min, with H the liquid's
+                               hydrostatic depth from the density warm starts (1.5 sum k^2 / (|g| sum k)) and
+                               v = max(jitter_speed, jitter_ratio |mean liquid velocity at the step's start|) */
+  double jitter_ratio;      /* Config.rest_jitter_flow_ratio (0: v = jitter_speed) */
+  double tol_den_min;       /* min(Config.min_density_error, max_density_error): the rule's floor */
 } adf_params;
 
 /* The model's particle arrays (Newton Model + sph:* attributes), bound once at creation. */
@@ -146,6 +153,23 @@ int adf_set_tuned_config(adf_solver* solver, int kernel, int block, int nb);
 /* The configuration in use per tuned kernel (host [ADF_TUNE_KERNELS] each, any may be NULL): threads per block,
  * gathers in flight, and the winning trial's milliseconds (-1 if not tuned). */
 int adf_tuned_configs(adf_solver* solver, int32_t* block, int32_t* nb, float* ms);
+
+/* Persistent CG solve (no reference counterpart; the reference launches each CG kernel per iteration, krylov.py:254-297,
+ * inside wp.capture_while, solve_driver.py:186). With the projected CG on models of at most 131,072 particles, each
+ * pressure solve (its start and every iteration) runs as ONE cooperative launch whose phases are separated by
+ * grid-wide barriers, instead of about nine launches per iteration; the results are the multi-launch path's bit for
+ * bit. enable = 1 (the default at creation) uses it wherever it applies (not in steps timed kernel by kernel, which
+ * take the multi-launch path); 0 always takes the multi-launch path. Every barrier wait is bounded: a wait that gives
+ * up sets the solver's status, after which adf_get_report returns ADF_ERR_STATE until adf_clear_status. */
+int adf_set_persistent(adf_solver* solver, int enable);
+/* Test hook of the bounded barrier waits: each wait polls at most `polls` times (default 4,194,304, about a second),
+ * and a barrier waits for `extra_arrivals` more blocks than the grid has (default 0; any other value makes every wait
+ * run out, which is what the wait-expiry test checks). */
+int adf_set_barrier_wait(adf_solver* solver, long long polls, int extra_arrivals);
+/* Clears the status words of the bounded waits (the persistent solve's barriers and the warm-start network's
+ * tensor-core waits) and the per-world reduction tickets a launch that gave up may have left counted, after
+ * synchronising the device. */
+int adf_clear_status(adf_solver* solver);
 
 /* Replaces SolverDFSPH.prime (solver.py:369-372, prime.py:52-87): with the divergence warm starts holding the
  * hydrostatic guess x dt (adf_set_warm_starts), one divergence solve of the velocity a gravity step adds to the

@@ -81,6 +81,9 @@ struct OrcParams {
   double bounds_lo[3], bounds_hi[3];
   int cg;  // pressure iteration: 1 projected preconditioned CG (krylov.py), 0 relaxed Jacobi
   int wall_friction;  // Config.wall_friction: Coulomb friction of lone particles and projections on shape walls
+  double jitter_speed;  // Config.rest_jitter_speed (0: the resting-jitter rule is off)
+  double jitter_ratio;  // Config.rest_jitter_flow_ratio
+  double tol_den_min;   // min(Config.min_density_error, max_density_error)
 };
 
 // Kernel constants in the working precision, derived from double host values exactly as the CUDA side does.
@@ -270,6 +273,10 @@ template <class R> struct Solver {
   std::vector<int> overflow, escaped, projected, nonfinite, emit_overflow;
   std::vector<int> iters_den, iters_div, converged, iters;
   std::vector<float> den_err, div_err, den_err_max, max_speed, err_mean, den_tol;
+  // the resting-jitter rule (solve_driver.py): per-world flow sums of the step's start state (sum v_z, count,
+  // sum v_x, sum v_y) and the density solve's tolerance factor
+  std::vector<double> flow_sum[4];
+  std::vector<float> tol_scale;
   std::vector<int64_t> mass_in, mass_out, mass0;
   std::vector<double> n_active;
   std::vector<Emitter> emitters;
@@ -989,7 +996,8 @@ template <class R> struct Solver {
         cg_restart[w] = 0;
         cg_rz[w] = rz_new;
         cg_step[w] = beta;
-        if ((it >= P.min_it && mean <= tol && cg_emax[w] <= tol_max) || it >= P.max_it) converged[w] = 1;
+        const float ts = tol_scale[w];
+        if ((it >= P.min_it && mean <= tol * ts && cg_emax[w] <= tol_max * ts) || it >= P.max_it) converged[w] = 1;
         else n_unconv++;
       }
       // krylov.py:236-246: p = z + beta p on F
@@ -1010,6 +1018,8 @@ template <class R> struct Solver {
     const float tol = (float)tol_d, tol_max = (float)(tol_d * P.max_error_factor);
     R relief = R(1.0e30);
     if (!div && P.relief_speed > 0.0) relief = R(P.relief_speed * dt_d * P.lattice_grad);
+    if (div) tol_scale.assign(W, 1.0f);
+    else density_tolerance(dt);
     solve_init(div, dt, relief);
     refresh_kr();
     int n_unconv = 0;
@@ -1033,7 +1043,7 @@ template <class R> struct Solver {
         iters[w] = it;
         float mean = (float)(esum[w] / std::max(n_active[w], 1.0));
         err_mean[w] = mean;
-        const float ts = 1.0f;
+        const float ts = tol_scale[w];
         if ((it >= P.min_it && mean <= tol * ts && emax[w] <= tol_max * ts) || it >= P.max_it) converged[w] = 1;
         else n_unconv++;
       }
@@ -1046,7 +1056,7 @@ template <class R> struct Solver {
       else { iters_den[w] = iters[w]; den_err[w] = err_mean[w]; }
     }
     if (!div) {
-      for (int w = 0; w < W; ++w) { den_err_max[w] = 0.0f; den_tol[w] = (float)tol_d; }
+      for (int w = 0; w < W; ++w) { den_err_max[w] = 0.0f; den_tol[w] = tol * tol_scale[w]; }
       for (int i = 0; i < n; ++i)
         if (is_fluid(i)) den_err_max[world[i]] = maxr(den_err_max[world[i]], (float)err[i]);
     }
@@ -1409,10 +1419,62 @@ template <class R> struct Solver {
     return it;
   }
 
+  // solve_driver.py:38-51 (_flow_speed): the per-world float64 sums of the liquid's start velocity (v_z, 1, v_x, v_y)
+  // in world_sum's tree order, when the rule and its flow ratio are on
+  void flow_sums() {
+    if (!(P.jitter_speed > 0.0) || !(P.jitter_ratio > 0.0)) return;
+    std::vector<R> t(n);
+    for (int k = 0; k < 4; ++k) {
+      for (int i = 0; i < n; ++i)
+        t[i] = !is_fluid(i) ? R(0) : k == 0 ? v[i].z : k == 1 ? R(1) : k == 2 ? v[i].x : v[i].y;
+      flow_sum[k].assign(W, 0.0);
+      world_sum<R>(W, ws.data(), t.data(), flow_sum[k].data(), nullptr);
+    }
+  }
+
+  // solve_driver.py:54-110 (_density_tolerance, tol_scale_kernel): per world the factor of the density solve's
+  // tolerance, clamp(v dt / (H tol), tol_min / tol, 1), H = 1.5 S2 / (S1 dt^2 |g|) from the density warm starts
+  // (S1 = sum kd+, S2 = sum kd+^2 over the liquid, kd+ = max(kd, 0)), v = max(speed, ratio |mean velocity|); float32
+  // arithmetic as the kernel's
+  void density_tolerance(R dt) {
+    tol_scale.assign(W, 1.0f);
+    if (!(P.jitter_speed > 0.0)) return;
+    std::vector<R> t1(n), t2(n);
+    for (int i = 0; i < n; ++i) {
+      const R k = is_fluid(i) ? maxr(kd[i], R(0)) : R(0);
+      t1[i] = k;
+      t2[i] = k * k;
+    }
+    std::vector<double> s1(W), s2(W);
+    world_sum<R>(W, ws.data(), t1.data(), s1.data(), nullptr);
+    world_sum<R>(W, ws.data(), t2.data(), s2.data(), nullptr);
+    const float fdt = (float)dt, speed = (float)P.jitter_speed, ratio = (float)P.jitter_ratio;
+    const float tol = (float)P.tol_den, tol_min = (float)P.tol_den_min;
+    for (int w = 0; w < W; ++w) {
+      float sc = 1.0f;
+      const float gx = gravity[3 * w], gy = gravity[3 * w + 1], gz = gravity[3 * w + 2];
+      const float g = std::sqrt((gx * gx + gy * gy) + gz * gz);
+      const float a = (float)s1[w], b = (float)s2[w];
+      float vs = speed;
+      if (ratio > 0.0f && !flow_sum[1].empty() && flow_sum[1][w] > 0.0) {
+        const double cnt = flow_sum[1][w];
+        const float ux = (float)(flow_sum[2][w] / cnt), uy = (float)(flow_sum[3][w] / cnt);
+        const float uz = (float)(flow_sum[0][w] / cnt);
+        vs = maxr(vs, ratio * std::sqrt((ux * ux + uy * uy) + uz * uz));
+      }
+      if (g > 0.0f && a > 0.0f && b > 0.0f) {
+        const float depth = (1.5f * b) / (((a * fdt) * fdt) * g);
+        sc = minr(maxr((vs * fdt) / (depth * tol), tol_min / tol), 1.0f);
+      }
+      tol_scale[w] = sc;
+    }
+  }
+
   // solver.py:218-268
   void step(double dt_d) {
     R dt = R(dt_d);
     prepare_density();
+    flow_sums();
     if (P.divergence_solve) solve(true, dt, dt_d);
     nonpressure(dt);
     solve(false, dt, dt_d);

@@ -40,7 +40,8 @@ class OrcParams(C.Structure):
                 ("divergence_solve", C.c_int), ("two_sided", C.c_int), ("xsph_c", C.c_double),
                 ("capacity", C.c_int), ("v_sep", C.c_double), ("relief_speed", C.c_double),
                 ("project_eps", C.c_double), ("has_bounds", C.c_int), ("bounds_lo", C.c_double * 3),
-                ("bounds_hi", C.c_double * 3), ("cg", C.c_int), ("wall_friction", C.c_int)]
+                ("bounds_hi", C.c_double * 3), ("cg", C.c_int), ("wall_friction", C.c_int),
+                ("jitter_speed", C.c_double), ("jitter_ratio", C.c_double), ("tol_den_min", C.c_double)]
 
 
 def params_from_config(cfg) -> OrcParams:
@@ -64,6 +65,9 @@ def params_from_config(cfg) -> OrcParams:
     p.relief_speed = cfg.compression_relief_speed or 0.0
     p.project_eps = hc.project_eps
     p.wall_friction = int(bool(cfg.wall_friction))
+    p.jitter_speed = cfg.rest_jitter_speed or 0.0
+    p.jitter_ratio = cfg.rest_jitter_flow_ratio
+    p.tol_den_min = min(cfg.min_density_error, cfg.max_density_error)
     if cfg.world_bounds is not None:
         p.has_bounds = 1
         for a in range(3):

@@ -171,6 +171,7 @@ def test_speed_harness_scenes_follow_the_reference_harness():
     assert many.fluid_count == 3 * 4096 and many.model.world_count == 3
     dam = tank_dam_break(32, 30, 32, 96, r=2.0e-3)
     assert dam.fluid_count == 30720 and dam.config.pressure_solver == "cg" and dam.config.cfl == 0.2
+    assert dam.config.rest_jitter_speed == 1.5e-3  # the default config: the resting-jitter rule on
     assert dam.dt == C.snap_down(C.stable_dt(dam.config, 2.0 * (9.81 * 30 * s) ** 0.5), 0.02) == 0.02 / 64
     hd = dam.model.host()
     inner_x = hd["shape_transform"][:, 0] - hd["shape_scale"][:, 0]
