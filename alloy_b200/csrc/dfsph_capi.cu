@@ -192,8 +192,8 @@ struct adf_solver {
   bool warm_on = false, feat_rec = false, warm_alloc = false, judge = true;
   bool cg = false;  // projected preconditioned CG pressure solve (adf_params.cg)
   bool cg_team = false;  // CG products by teams of TL lanes per particle (models of at most CG_TEAM_MAX particles)
-  // the persistent CG solve (k_cg_solve) of team-product models: on unless adf_set_persistent turned it off
-  bool persist_on = true;
+  // the persistent CG solve (k_cg_solve) of team-product models, when adf_set_persistent turned it on
+  bool persist_on = false;
   int persist_cap[2] = {0, 0};       // co-resident blocks of k_cg_solve<false/true> on this device
   unsigned persist_extra = 0;        // extra arrivals a barrier waits for (only the wait-expiry test sets it)
   long long persist_wait = 1 << 22;  // polls of one barrier wait (about a second) before it gives up

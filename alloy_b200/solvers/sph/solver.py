@@ -428,8 +428,8 @@ class SolverDFSPH:
 
     def persistent(self, enable: bool = True) -> None:
         """Run each projected-CG pressure solve of a model of at most 131,072 particles as one persistent launch with
-        grid-wide barriers (on by default; include/alloy_dfsph.h adf_set_persistent). Off: one launch per kernel and
-        iteration. The results are the same bits either way."""
+        grid-wide barriers (include/alloy_dfsph.h adf_set_persistent; off by default, the multi-launch path measured
+        slightly faster). The results are the same bits either way."""
         _lib.check(self._lib.adf_set_persistent(self._h, int(bool(enable))), "persistent")
 
     def barrier_wait(self, polls: int = 1 << 22, extra_arrivals: int = 0) -> None:

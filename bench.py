@@ -162,31 +162,32 @@ def rank_scene(sc, name: str, rank: int, world: int, device):
 
 def worlds_scene(sc, mine: list[int], device, name: str):
     """The scene of the worlds ``mine`` of a multi-world scene, renumbered 0.. in that order: their particles, spouts
-    and kinematic bowls."""
+    and kinematic bowls (vectorised over worlds: a shard holds up to thousands of them)."""
     from alloy_b200.solvers.sph.sharding import sub_model
     from alloy_b200.solvers.sph.testing import Scene
 
-    ws = sc.model.host()["world_start"]
+    ws = np.asarray(sc.model.host()["world_start"], np.int64)
+    mine = [int(w) for w in mine]
     sub = sub_model(sc.model, mine, device)
-    sws = np.concatenate([[0], np.cumsum([ws[w + 1] - ws[w] for w in mine])])
-    ems = []
-    for e in sc.emitters:
-        if e["world"] in mine:
-            k = mine.index(e["world"])
-            ems.append({**e, "world": k, "pool": np.asarray(e["pool"]) - ws[e["world"]] + sws[k]})
-    fl = int(sum(np.sum(sub.host()["phase"][sws[k]:sws[k + 1]] >= 1) for k in range(len(mine))))
+    counts = ws[np.asarray(mine, np.int64) + 1] - ws[np.asarray(mine, np.int64)] if mine else np.zeros(0, np.int64)
+    sws = np.concatenate([[0], np.cumsum(counts)])
+    slot = {w: k for k, w in enumerate(mine)}
+    ems = [{**e, "world": slot[e["world"]], "pool": np.asarray(e["pool"]) - ws[e["world"]] + sws[slot[e["world"]]]}
+           for e in sc.emitters if e["world"] in slot]
+    fl = int(np.sum(sub.host()["phase"] >= 1))
     out = Scene(sub, sc.config, sc.dt, sc.steps, fl, 0, ems, name=name)
-    if sc.motion is not None:  # the worlds' bowls, renumbered into the sub-model
+    if sc.motion is not None:  # the worlds' bowls, renumbered into the sub-model (walls grouped by new world, in order)
         from alloy_b200.solvers.sph.testing import BowlMotion
 
         m = sc.motion
-        idx, wof = [], []
-        for k, w in enumerate(mine):
-            sel = m.wall_world == w
-            idx.append(m.wall_index[sel] - ws[w] + sws[k])
-            wof.append(np.full(int(sel.sum()), k))
-        out.motion = BowlMotion(np.concatenate(idx), np.concatenate(wof), m.direction[mine], m.phase[mine],
-                                m.amplitude, m.period)
+        new = np.full(len(ws) - 1, -1, np.int64)
+        new[mine] = np.arange(len(mine))
+        k = new[m.wall_world]
+        sel = np.nonzero(k >= 0)[0]
+        sel = sel[np.argsort(k[sel], kind="stable")]
+        kk = k[sel]
+        idx = m.wall_index[sel] - ws[m.wall_world[sel]] + sws[kk]
+        out.motion = BowlMotion(idx, kk, m.direction[mine], m.phase[mine], m.amplitude, m.period)
     return out
 
 
@@ -575,13 +576,83 @@ def liq9_fields(workload: str, sc, step_s: float) -> dict:
     """The reference harness's own figures for its workloads (test_speed_gpu.py:24-39): the real-time factor of one
     world and the world-seconds per wall-second of many (its targets on an L4: >= 0.5 and >= 50)."""
     if workload == "column_30k":
-        return {"rt_factor": sc.dt / step_s, "published_l4": "4.6 ms per step, fast preset (config.py:151-152)"}
+        return {"rt_factor": sc.dt / step_s,
+                "published_l4": "4.6 ms per step with the fast preset, 10.6 ms with the default config (the "
+                                "default_config arm) (config.py:151-152)"}
     if workload == "dam_break_30k":
         return {"rt_factor": sc.dt / step_s, "target_l4": ">= 0.5x real time (LIQ-9 target)"}
     if workload == "columns_256x4k":
         W = int(sc.model.world_count)
         return {"world_s_per_wall_s": W * sc.dt / step_s, "target_l4": ">= 50 world-s per wall-s (LIQ-9 target)"}
     return {}
+
+
+E2E_SHARDS = 4  # world shards of a multi-world scene in the end-to-end pass, each stepped on a stream of its own
+
+
+def e2e_pipelined(args, sc, dev, headline_warm: bool, steps_before: int):
+    """The end-to-end pass of a multi-world scene through the public API with host buffers: its worlds in E2E_SHARDS
+    shards (longest-processing-time by particle count), each a SolverDFSPH of its own (same settings and spouts as the
+    timed run) on a CUDA stream of its own, brought untimed to the timed run's step (``steps_before`` steps), then
+    ``args.steps`` wall-clock-timed steps in which every shard, every step, copies its q and qd in from pinned host
+    memory, steps, copies q and qd back and has its per-world report read. One shard's copies overlap the others'
+    steps, as a caller overlaps host I/O by stepping independent worlds on separate streams. Returns (liquid
+    particle-steps, seconds, H2D bytes per step, D2H bytes per step, description)."""
+    from types import SimpleNamespace
+
+    import torch
+
+    from alloy_b200.solvers.sph import SolverDFSPH
+    from alloy_b200.solvers.sph.sharding import shard_worlds
+
+    ws = sc.model.host()["world_start"]
+    parts = []
+    for i, mine in enumerate(g for g in shard_worlds(np.diff(ws), E2E_SHARDS) if g):
+        s = worlds_scene(sc, sorted(mine), dev, f"{sc.name}_e2e{i}")
+        sol = SolverDFSPH(s.model, s.config)
+        sol.add_emitters([(w, c, h, rate, vel, pool) for w, c, h, rate, vel, pool, _, _ in spouts(s)])
+        if headline_warm:
+            sol.set_warm_model(warm_model(args))
+            sol.warm_judging(True)
+        n = s.model.particle_count
+        parts.append(SimpleNamespace(sol=sol, sc=s, run=Stepper(sol, s, s.model.state(), s.model.state()),
+                                     stream=torch.cuda.Stream(dev), n=n,
+                                     hq=torch.empty((n, 3), dtype=torch.float32, pin_memory=True),
+                                     hqd=torch.empty((n, 3), dtype=torch.float32, pin_memory=True)))
+    for p in parts:  # untimed: the same step of the pour as the timed run's state
+        with torch.cuda.stream(p.stream):
+            if args.workload in LIQ9:
+                p.sol.prime(p.run.a, p.sc.dt)
+            p.run(steps_before)
+            p.hq.copy_(p.run.a.particle_q)
+            p.hqd.copy_(p.run.a.particle_qd)
+    torch.cuda.synchronize(dev)
+    nf0 = sum(p.sol.list_stats()[0] for p in parts)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for p in parts:
+            with torch.cuda.stream(p.stream):
+                a, b = p.run.a, p.run.b
+                a.particle_q.copy_(p.hq, non_blocking=True)
+                a.particle_qd.copy_(p.hqd, non_blocking=True)
+                p.run.drive(a)
+                p.sol.step(a, b, None, None, p.sc.dt)
+                p.run.a, p.run.b = b, a
+                p.run.k += 1
+                p.hq.copy_(b.particle_q, non_blocking=True)
+                p.hqd.copy_(b.particle_qd, non_blocking=True)
+        for p in parts:
+            with torch.cuda.stream(p.stream):
+                p.sol.report()  # synchronises the shard's stream and reads its per-world result
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter() - t0
+    nf1 = sum(p.sol.list_stats()[0] for p in parts)
+    h2d = sum(2 * p.n * 12 for p in parts)
+    d2h = h2d + sum(p.sol.world_count * 64 for p in parts)
+    how = (f"{len(parts)} world shards, each a solver on its own stream; each step every shard: H2D of q and qd, the "
+           "step, D2H of q, qd and the per-world report; one shard's copies overlap the other shards' steps")
+    del parts
+    return 0.5 * (nf0 + nf1) * args.steps, t, h2d, d2h, how
 
 
 def pcg_off(sol) -> bool:
@@ -717,33 +788,39 @@ def run_b200(args):
 
     # end to end through the public API with host buffers: H2D of the state, the step, D2H of the state and report
     note("end-to-end pass")
-    n = sc.model.particle_count
-    a, b = run.a, run.b
-    hq = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-    hqd = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-    hq.copy_(a.particle_q)
-    hqd.copy_(a.particle_qd)
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        a.particle_q.copy_(hq, non_blocking=True)
-        a.particle_qd.copy_(hqd, non_blocking=True)
-        run.drive(a)
-        sol.step(a, b, None, None, sc.dt)
-        run.k += 1
-        hq.copy_(b.particle_q, non_blocking=True)
-        hqd.copy_(b.particle_qd, non_blocking=True)
-        sol.report()  # synchronises the stream and reads the per-world result
-    torch.cuda.synchronize(dev)
-    t_e2e = time.perf_counter() - t0
-    nf2 = sol.list_stats()[0]
+    if args.workload in MULTI_WORLD and sc.model.world_count >= E2E_SHARDS:
+        ps_e2e, t_e2e, h2d, d2h, how = e2e_pipelined(args, sc, dev, headline_warm, run.k)
+    else:
+        n = sc.model.particle_count
+        a, b = run.a, run.b
+        hq = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        hqd = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        hq.copy_(a.particle_q)
+        hqd.copy_(a.particle_qd)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            a.particle_q.copy_(hq, non_blocking=True)
+            a.particle_qd.copy_(hqd, non_blocking=True)
+            run.drive(a)
+            sol.step(a, b, None, None, sc.dt)
+            run.k += 1
+            hq.copy_(b.particle_q, non_blocking=True)
+            hqd.copy_(b.particle_qd, non_blocking=True)
+            sol.report()  # synchronises the stream and reads the per-world result
+        torch.cuda.synchronize(dev)
+        t_e2e = time.perf_counter() - t0
+        nf2 = sol.list_stats()[0]
+        ps_e2e = 0.5 * (nf1 + nf2) * args.steps
+        h2d, d2h = 2 * n * 12, 2 * n * 12 + sol.world_count * 64
+        how = "one solver, one stream: each step H2D of q and qd, the step, D2H of q, qd and the per-world report"
     te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-    pe = torch.tensor([0.5 * (nf1 + nf2) * args.steps], dtype=torch.float64, device=dev)
+    pe = torch.tensor([ps_e2e], dtype=torch.float64, device=dev)
     if world > 1:  # wall clock of each rank's own loop, the slowest rank's; particle-steps of all ranks
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
         dist.all_reduce(pe, op=dist.ReduceOp.SUM)
-    e2e = {"value": float(pe.item()) / float(te.item()), "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
-           "d2h_bytes_per_step": 2 * n * 12 + sol.world_count * 64}
+    e2e = {"value": float(pe.item()) / float(te.item()), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "how": how}
 
     nf, entries = sol.list_stats()
     nbar = entries / max(nf, 1)
@@ -785,6 +862,8 @@ def run_b200(args):
                 ("warm_started_unjudged", {"judge": False}), (other, {"pressure_solver": other})]
         if args.workload in LIQ9:  # Verlet-skin reuse of the rows (reneighbor_skin 0.1 h, config.py:78-80)
             arms.append(("reneighbor_skin_0.1", {"reneighbor_skin": 0.1}))
+        if args.workload in ("column_30k", "columns_256x4k"):  # the resting columns in the harness's own config
+            arms.append(("default_config", {"rest_jitter_speed": 1.5e-3, "cfl": 0.2}))
         for key, kw in arms:
             note(f"arm {key}")
             r = variant_arm(args, dev, rank, world, **kw)

@@ -158,8 +158,9 @@ int adf_tuned_configs(adf_solver* solver, int32_t* block, int32_t* nb, float* ms
  * inside wp.capture_while, solve_driver.py:186). With the projected CG on models of at most 131,072 particles, each
  * pressure solve (its start and every iteration) runs as ONE cooperative launch whose phases are separated by
  * grid-wide barriers, instead of about nine launches per iteration; the results are the multi-launch path's bit for
- * bit. enable = 1 (the default at creation) uses it wherever it applies (not in steps timed kernel by kernel, which
- * take the multi-launch path); 0 always takes the multi-launch path. Every barrier wait is bounded: a wait that gives
+ * bit. enable = 1 uses it wherever it applies (not in steps timed kernel by kernel, which take the multi-launch path);
+ * 0 (the default at creation) takes the multi-launch path, which measured 2-4 % faster on a B200: under a replayed
+ * step graph a grid barrier costs about what a kernel boundary does. Every barrier wait is bounded: a wait that gives
  * up sets the solver's status, after which adf_get_report returns ADF_ERR_STATE until adf_clear_status. */
 int adf_set_persistent(adf_solver* solver, int enable);
 /* Test hook of the bounded barrier waits: each wait polls at most `polls` times (default 4,194,304, about a second),

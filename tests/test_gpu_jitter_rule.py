@@ -39,8 +39,9 @@ def _columns(cfg, device, worlds=(8, 25)):
     return b.finalize(device)
 
 
-def _lockstep(model, cfg, dt, steps, kick=0.0, prime=True):
+def _lockstep(model, cfg, dt, steps, kick=0.0, prime=True, persistent=False):
     sol = SolverDFSPH(model, cfg)
+    sol.persistent(persistent)
     orc = Oracle(model.host(), cfg)
     a, b = model.state(), model.state()
     if prime:
@@ -74,7 +75,7 @@ def _lockstep(model, cfg, dt, steps, kick=0.0, prime=True):
 def test_jitter_rule_columns_cg_bit_exact(cuda):
     cfg = DFSPHConfig(particle_radius=2.0e-3)
     assert cfg.rest_jitter_speed and cfg.pressure_solver == "cg"
-    tols = _lockstep(_columns(cfg, cuda), cfg, DT, 25)
+    tols = _lockstep(_columns(cfg, cuda), cfg, DT, 25, persistent=True)
     assert (tols[5:] < cfg.max_density_error).all()  # at rest the rule tightens every world's tolerance
 
 

@@ -11,8 +11,8 @@ with bounded waits (krylov.py:254-297 with the loop of solve_driver.py:121-186).
   fails with ADF_ERR_STATE instead of returning results, and after the status is cleared the solver steps on and
   equals a fresh solver bit for bit (no GPU fault, no unbounded wait).
 
-The tests against the oracle (test_gpu_cg.py, test_gpu_prime.py, test_gpu_box_walls.py) run the persistent path too,
-as it is the default wherever it applies.
+The multi-launch path, the default, is the one the tests against the oracle run; test_gpu_jitter_rule.py runs the
+persistent one against the oracle as well.
 """
 
 from __future__ import annotations
@@ -43,6 +43,7 @@ def _lockstep(make, steps, graphs, spouts=False, prime=False):
     scenes = [make(), make()]
     sc = scenes[0]
     sols = [SolverDFSPH(x.model, x.config) for x in scenes]
+    sols[0].persistent(True)
     sols[1].persistent(False)
     states = [[x.model.state(), x.model.state()] for x in scenes]
     for sol, st, x in zip(sols, states, scenes):
@@ -100,6 +101,7 @@ def test_persistent_barrier_wait_expires_with_status(cuda):
 
     sc, sr = make(), make()  # each solver on its own model
     sol, ref = SolverDFSPH(sc.model, sc.config), SolverDFSPH(sr.model, sr.config)
+    sol.persistent(True)
     a, b = sc.model.state(), sc.model.state()
     c, d = sr.model.state(), sr.model.state()
     sol.barrier_wait(polls=2000, extra_arrivals=1)  # every barrier waits for a block that does not exist
