@@ -1438,12 +1438,14 @@ int adf_density_ratio(adf_solver* s, const float* q, const float* qd, float* rat
 int adf_get_report(adf_solver* s, adf_report* r, void* stream) {
   if (!s || !r) return fail(ADF_ERR_VALUE, "adf_get_report: null argument");
   CK(cudaSetDevice(s->device));
-  CK(cudaStreamSynchronize((cudaStream_t)stream));
+  const cudaStream_t st = (cudaStream_t)stream;
   const int W = s->W;
-  if (W == 0) return ADF_OK;
+  if (W == 0) return cudaStreamSynchronize(st) == cudaSuccess ? ADF_OK : fail(ADF_ERR_CUDA, "adf_get_report: sync");
+  // every copy is ordered on the caller's stream (never the legacy default stream, which would wait for the work of
+  // other streams too); one synchronisation at the end
   auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
     if (!dst) return ADF_OK;
-    CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
     return ADF_OK;
   };
   int rc = 0;
@@ -1471,17 +1473,14 @@ int adf_get_report(adf_solver* s, adf_report* r, void* stream) {
     if (r->learned_density) std::memset(r->learned_density, 0, 4 * (size_t)W);
   }
   if (rc) return ADF_ERR_CUDA;
-  if (s->merr) {
-    int e = 0;
-    CK(cudaMemcpy(&e, s->merr, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) return fail(ADF_ERR_STATE, "warm-start network: a tensor-core wait expired; the learned starts are invalid");
-  }
-  if (s->perr) {
-    int e = 0;
-    CK(cudaMemcpy(&e, s->perr, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) return fail(ADF_ERR_STATE, "pressure solve: a grid-barrier wait of the persistent CG solve expired; the "
-                                      "step's results are invalid");
-  }
+  int merr = 0, perr = 0;
+  if (s->merr) CK(cudaMemcpyAsync(&merr, s->merr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (s->perr) CK(cudaMemcpyAsync(&perr, s->perr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (merr) return fail(ADF_ERR_STATE, "warm-start network: a tensor-core wait expired; the learned starts are invalid");
+  if (perr)
+    return fail(ADF_ERR_STATE, "pressure solve: a grid-barrier wait of the persistent CG solve expired; the step's "
+                               "results are invalid");
   return ADF_OK;
 }
 
@@ -1713,8 +1712,8 @@ int adf_active_mass(adf_solver* s, int64_t* out_host, void* stream) {
   const int W = std::max(s->W, 1);
   CK(cudaMemsetAsync(s->tmp_mass, 0, 8 * W, st));
   if (s->n > 0) LAUNCH(s, k_active_mass, blocks(s->n), BLOCK, st, s->d, s->tmp_mass);
+  if (s->W) CK(cudaMemcpyAsync(out_host, s->tmp_mass, 8 * s->W, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  if (s->W) CK(cudaMemcpy(out_host, s->tmp_mass, 8 * s->W, cudaMemcpyDeviceToHost));
   return check_launch();
 }
 

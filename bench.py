@@ -587,74 +587,6 @@ def liq9_fields(workload: str, sc, step_s: float) -> dict:
     return {}
 
 
-E2E_SHARDS = 4  # world shards of a multi-world scene in the end-to-end pass, each stepped on a stream of its own
-
-
-def e2e_pipelined(args, sc, dev, headline_warm: bool, steps_before: int):
-    """The end-to-end pass of a multi-world scene through the public API with host buffers: its worlds in E2E_SHARDS
-    shards (longest-processing-time by particle count), each a SolverDFSPH of its own (same settings and spouts as the
-    timed run) on a CUDA stream of its own, brought untimed to the timed run's step (``steps_before`` steps), then
-    ``args.steps`` wall-clock-timed steps in which every shard, every step, copies its q and qd in from pinned host
-    memory, steps, copies q and qd back and has its per-world report read. One shard's copies overlap the others'
-    steps, as a caller overlaps host I/O by stepping independent worlds on separate streams. Returns (liquid
-    particle-steps, seconds, H2D bytes per step, D2H bytes per step, description)."""
-    from types import SimpleNamespace
-
-    import torch
-
-    from alloy_b200.solvers.sph import SolverDFSPH
-    from alloy_b200.solvers.sph.sharding import shard_worlds
-
-    ws = sc.model.host()["world_start"]
-    parts = []
-    for i, mine in enumerate(g for g in shard_worlds(np.diff(ws), E2E_SHARDS) if g):
-        s = worlds_scene(sc, sorted(mine), dev, f"{sc.name}_e2e{i}")
-        sol = SolverDFSPH(s.model, s.config)
-        sol.add_emitters([(w, c, h, rate, vel, pool) for w, c, h, rate, vel, pool, _, _ in spouts(s)])
-        if headline_warm:
-            sol.set_warm_model(warm_model(args))
-            sol.warm_judging(True)
-        n = s.model.particle_count
-        parts.append(SimpleNamespace(sol=sol, sc=s, run=Stepper(sol, s, s.model.state(), s.model.state()),
-                                     stream=torch.cuda.Stream(dev), n=n,
-                                     hq=torch.empty((n, 3), dtype=torch.float32, pin_memory=True),
-                                     hqd=torch.empty((n, 3), dtype=torch.float32, pin_memory=True)))
-    for p in parts:  # untimed: the same step of the pour as the timed run's state
-        with torch.cuda.stream(p.stream):
-            if args.workload in LIQ9:
-                p.sol.prime(p.run.a, p.sc.dt)
-            p.run(steps_before)
-            p.hq.copy_(p.run.a.particle_q)
-            p.hqd.copy_(p.run.a.particle_qd)
-    torch.cuda.synchronize(dev)
-    nf0 = sum(p.sol.list_stats()[0] for p in parts)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for p in parts:
-            with torch.cuda.stream(p.stream):
-                a, b = p.run.a, p.run.b
-                a.particle_q.copy_(p.hq, non_blocking=True)
-                a.particle_qd.copy_(p.hqd, non_blocking=True)
-                p.run.drive(a)
-                p.sol.step(a, b, None, None, p.sc.dt)
-                p.run.a, p.run.b = b, a
-                p.run.k += 1
-                p.hq.copy_(b.particle_q, non_blocking=True)
-                p.hqd.copy_(b.particle_qd, non_blocking=True)
-        for p in parts:
-            with torch.cuda.stream(p.stream):
-                p.sol.report()  # synchronises the shard's stream and reads its per-world result
-    torch.cuda.synchronize(dev)
-    t = time.perf_counter() - t0
-    nf1 = sum(p.sol.list_stats()[0] for p in parts)
-    h2d = sum(2 * p.n * 12 for p in parts)
-    d2h = h2d + sum(p.sol.world_count * 64 for p in parts)
-    how = (f"{len(parts)} world shards, each a solver on its own stream; each step every shard: H2D of q and qd, the "
-           "step, D2H of q, qd and the per-world report; one shard's copies overlap the other shards' steps")
-    del parts
-    return 0.5 * (nf0 + nf1) * args.steps, t, h2d, d2h, how
-
-
 def pcg_off(sol) -> bool:
     """The Jacobi path (whose iterations the library's work counter covers)."""
     return sol.pressure_solver == "jacobi"
@@ -788,17 +720,16 @@ def run_b200(args):
 
     # end to end through the public API with host buffers: H2D of the state, the step, D2H of the state and report
     note("end-to-end pass")
-    if args.workload in MULTI_WORLD and sc.model.world_count >= E2E_SHARDS:
-        ps_e2e, t_e2e, h2d, d2h, how = e2e_pipelined(args, sc, dev, headline_warm, run.k)
-    else:
-        n = sc.model.particle_count
-        a, b = run.a, run.b
-        hq = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-        hqd = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-        hq.copy_(a.particle_q)
-        hqd.copy_(a.particle_qd)
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
+    n = sc.model.particle_count
+    a, b = run.a, run.b
+    hq = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    hqd = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+    hq.copy_(a.particle_q)
+    hqd.copy_(a.particle_qd)
+    e2e_stream = torch.cuda.Stream(dev)  # the caller's stream: copies, step and report read ordered on it
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    with torch.cuda.stream(e2e_stream):
         for _ in range(args.steps):
             a.particle_q.copy_(hq, non_blocking=True)
             a.particle_qd.copy_(hqd, non_blocking=True)
@@ -808,12 +739,13 @@ def run_b200(args):
             hq.copy_(b.particle_q, non_blocking=True)
             hqd.copy_(b.particle_qd, non_blocking=True)
             sol.report()  # synchronises the stream and reads the per-world result
-        torch.cuda.synchronize(dev)
-        t_e2e = time.perf_counter() - t0
-        nf2 = sol.list_stats()[0]
-        ps_e2e = 0.5 * (nf1 + nf2) * args.steps
-        h2d, d2h = 2 * n * 12, 2 * n * 12 + sol.world_count * 64
-        how = "one solver, one stream: each step H2D of q and qd, the step, D2H of q, qd and the per-world report"
+    torch.cuda.synchronize(dev)
+    t_e2e = time.perf_counter() - t0
+    nf2 = sol.list_stats()[0]
+    ps_e2e = 0.5 * (nf1 + nf2) * args.steps
+    h2d, d2h = 2 * n * 12, 2 * n * 12 + sol.world_count * 64
+    how = ("one solver on a CUDA stream of the caller's: each step H2D of q and qd from pinned host memory, the step, "
+           "D2H of q and qd, and the per-world report read")
     te = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
     pe = torch.tensor([ps_e2e], dtype=torch.float64, device=dev)
     if world > 1:  # wall clock of each rank's own loop, the slowest rank's; particle-steps of all ranks
