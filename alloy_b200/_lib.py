@@ -53,7 +53,8 @@ class ModelDesc(C.Structure):
                 ("q_host", C.POINTER(C.c_float)), ("mass", C.c_void_p), ("rest_density", C.c_void_p),
                 ("radius", C.c_void_p), ("flags", C.c_void_p), ("phase", C.c_void_p), ("world", C.c_void_p),
                 ("gravity", C.c_void_p), ("n_shapes", C.c_int), ("shape_start", C.POINTER(C.c_int32)),
-                ("shape_ids", C.POINTER(C.c_int32)), ("shape_box", C.POINTER(C.c_float)), ("sweep_len", C.c_double)]
+                ("shape_ids", C.POINTER(C.c_int32)), ("shape_box", C.POINTER(C.c_float)), ("sweep_len", C.c_double),
+                ("shape_geo", C.POINTER(C.c_int32))]
 
 
 class Report(C.Structure):

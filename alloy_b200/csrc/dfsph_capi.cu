@@ -899,6 +899,12 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     for (int k = 0; k < m->n_shapes; ++k)
       for (int a = 0; a < 8; ++a)
         if (!std::isfinite(m->shape_box[8 * k + a])) return fail(ADF_ERR_VALUE, "shape_box holds a non-finite value");
+    if (m->shape_geo)  // the walls a world sees (shapes no world lists are never evaluated)
+      for (int c = 0; c < total; ++c) {
+        const int g = m->shape_geo[m->shape_ids[c]];
+        if (g != GEO_BOX && g != GEO_SPHERE && g != GEO_CAPSULE && g != GEO_PLANE)
+          return fail(ADF_ERR_VALUE, "shape_geo: only boxes (7), spheres (3), capsules (4) and planes (1)");
+      }
   }
   CK(cudaSetDevice(device));
   adf_solver* s = new adf_solver();
@@ -1003,12 +1009,14 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.slot_xb, (size_t)d.slot_cap * n);
   int *sh_start = nullptr, *sh_ids = nullptr;
   float4 *sh_pos = nullptr, *sh_half = nullptr;
+  int* sh_geo = nullptr;
   if (d.slot_cap > 1) {
     rc |= s->alloc(&d.slot_cnt, n);
     rc |= s->alloc(&sh_start, (size_t)W + 1);
     rc |= s->alloc(&sh_ids, (size_t)n_box_refs);
     rc |= s->alloc(&sh_pos, (size_t)m->n_shapes);
     rc |= s->alloc(&sh_half, (size_t)m->n_shapes);
+    rc |= s->alloc(&sh_geo, (size_t)m->n_shapes);
   }
   rc |= s->alloc(&d.swept, W);
   d.skin_on = p.skin > 0.0;
@@ -1121,6 +1129,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   d.sh_ids = sh_ids;
   d.sh_pos = sh_pos;
   d.sh_half = sh_half;
+  d.sh_geo = sh_geo;
   d.chunk_begin = chunk_begin;
   d.chunk_end = chunk_end;
   d.world_chunk_start = world_chunk_start;
@@ -1166,6 +1175,9 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     CKC(cudaMemcpy(sh_ids, m->shape_ids, sizeof(int) * n_box_refs, cudaMemcpyHostToDevice));
     CKC(cudaMemcpy(sh_pos, bp.data(), sizeof(float4) * bp.size(), cudaMemcpyHostToDevice));
     CKC(cudaMemcpy(sh_half, bh.data(), sizeof(float4) * bh.size(), cudaMemcpyHostToDevice));
+    std::vector<int> geo(m->n_shapes, GEO_BOX);
+    if (m->shape_geo) std::copy(m->shape_geo, m->shape_geo + m->n_shapes, geo.begin());
+    CKC(cudaMemcpy(sh_geo, geo.data(), sizeof(int) * geo.size(), cudaMemcpyHostToDevice));
   }
   {  // the port's reservoir: each world's build-time held particles, popped in ascending id order (ports.py:124-133)
     std::vector<int8_t> ph(s->n);

@@ -127,7 +127,9 @@ struct DevP {
   const int* sh_start;    // [W + 1]: world w's walls are sh_ids[sh_start[w] .. sh_start[w + 1])
   const int* sh_ids;
   const float4* sh_pos;   // centre (3), bounding radius
-  const float4* sh_half;  // half extents (3), Coulomb friction mu
+  const float4* sh_half;  // the shape's scale (3: box half extents; sphere radius; capsule radius, half height; plane
+                          // half width, half length, 0 for an infinite plane), Coulomb friction mu
+  const int* sh_geo;      // newton GeoType per shape (GEO_BOX, GEO_SPHERE, GEO_CAPSULE, GEO_PLANE)
   float sweep_len;        // a step longer than this is swept against the world's boxes (integrate.py:42-49)
   float prad;             // particle radius
   int wall_friction;      // Config.wall_friction
@@ -1143,6 +1145,62 @@ __device__ __forceinline__ void box_normal(float x, float y, float z, const floa
   normalized3(nx, ny, nz);
 }
 
+// newton GeoType ids of the static shapes this path evaluates (geometry/types.py:73-118)
+constexpr int GEO_PLANE = 1, GEO_SPHERE = 3, GEO_CAPSULE = 4, GEO_BOX = 7;
+
+// The signed distance of shape `geo` (scale s.xyz) at shape-frame point (x, y, z), as newton's eval_shape_sdf evaluates
+// the analytic shapes (soft_contacts_sdf.py:249-280, geometry/kernels.py): a box (sdf_box :310-333), a sphere
+// (sdf_sphere :277-288), a capsule along the shape's z axis (sdf_capsule :374-393), a plane through the shape's origin
+// with normal +z (sdf_plane :708-729: finite for positive half width and length, an L-infinity distance to the quad).
+__device__ __forceinline__ float shape_phi(int geo, const float4& s, float x, float y, float z) {
+  if (geo == GEO_BOX) return box_sdf(x, y, z, s);
+  if (geo == GEO_PLANE) {
+    if (s.x > 0.0f && s.y > 0.0f) return maxr(maxr(fabsf(x) - s.x, fabsf(y) - s.y), fabsf(z));
+    return z;
+  }
+  float cz = z;
+  if (geo == GEO_CAPSULE) cz = z > s.y ? z - s.y : (z < -s.y ? z + s.y : 0.0f);
+  return __fsqrt_rn(dot_plain(x, y, cz, x, y, cz)) - s.x;
+}
+
+// Its outward unit normal there: the gradient (box: sdf_box_grad; sphere and capsule: the direction from the nearest
+// point of the centre or axis segment, +z at it, -z below the lower cap; plane: +z), normalised again as the
+// reference's slot code does (boundary.py:226-231).
+__device__ __forceinline__ void shape_normal(int geo, const float4& s, float x, float y, float z, float& nx, float& ny,
+                                             float& nz) {
+  if (geo == GEO_BOX) {
+    box_normal(x, y, z, s, nx, ny, nz);
+    return;
+  }
+  if (geo == GEO_PLANE) {
+    nx = 0.0f;
+    ny = 0.0f;
+    nz = 1.0f;
+    return;
+  }
+  float cz = z, dz = 1.0f;
+  if (geo == GEO_CAPSULE) {
+    if (z > s.y) cz = z - s.y;
+    else if (z < -s.y) {
+      cz = z + s.y;
+      dz = -1.0f;
+    } else {
+      cz = 0.0f;
+    }
+  }
+  const float l = __fsqrt_rn(dot_plain(x, y, cz, x, y, cz));
+  if (l > 1.0e-8f) {
+    nx = x / l;
+    ny = y / l;
+    nz = cz / l;
+  } else {
+    nx = 0.0f;
+    ny = 0.0f;
+    nz = dz;
+  }
+  normalized3(nx, ny, nz);
+}
+
 // boundary_slots.py:13-37: (sh, phi) into a phi-ascending row of n_ slots; the slot used, or -1
 __device__ __forceinline__ int slot_insert(int (&shp)[4], float (&ph)[4], int n_, int sh, float phi) {
   int pos = n_, k = n_ - 1;
@@ -1232,13 +1290,14 @@ __global__ void __launch_bounds__(BLOCK) k_shape_slots(DevP P) {
   for (int c = P.sh_start[w]; c < P.sh_start[w + 1]; ++c) {
     const int sh = P.sh_ids[c];
     const float4 cp = P.sh_pos[sh];
+    const int geo = P.sh_geo[sh];
     const float lx = xi.x - cp.x, ly = xi.y - cp.y, lz = xi.z - cp.z;
-    if (__fsqrt_rn(dot_plain(lx, ly, lz, lx, ly, lz)) > cp.w + h) continue;
+    if (geo != GEO_PLANE && __fsqrt_rn(dot_plain(lx, ly, lz, lx, ly, lz)) > cp.w + h) continue;
     const float4 hx = P.sh_half[sh];
-    const float phi = box_sdf(lx, ly, lz, hx);
+    const float phi = shape_phi(geo, hx, lx, ly, lz);
     if (phi < P.reach && phi + P.wall_offset < h) {
       float nx, ny, nz;
-      box_normal(lx, ly, lz, hx, nx, ny, nz);
+      shape_normal(geo, hx, lx, ly, lz, nx, ny, nz);
       if (shape_insert(shp, ph, nr, ns, sh, phi, make_float3(nx, ny, nz), near) > 0 && ns < 4) ++ns;
     }
   }
@@ -1257,10 +1316,11 @@ __global__ void __launch_bounds__(BLOCK) k_shape_slots(DevP P) {
       sx[k] = xb0;
     } else {
       const float4 cp = P.sh_pos[sh], hx = P.sh_half[sh];
+      const int geo = P.sh_geo[sh];
       const float lx = xi.x - cp.x, ly = xi.y - cp.y, lz = xi.z - cp.z;
-      const float phi = box_sdf(lx, ly, lz, hx);
+      const float phi = shape_phi(geo, hx, lx, ly, lz);
       float nx, ny, nz, psi, dpsi;
-      box_normal(lx, ly, lz, hx, nx, ny, nz);
+      shape_normal(geo, hx, lx, ly, lz, nx, ny, nz);
       wall_volume(P, phi, psi, dpsi);
       sg[k] = make_float4(dpsi * nx, dpsi * ny, dpsi * nz, psi);
       sv[k] = make_float4(0.0f, 0.0f, 0.0f, phi);
@@ -1327,6 +1387,34 @@ __device__ __forceinline__ float box_entry(const float4& h, float ox, float oy, 
   }
   if (lo <= hi && lo <= 1.0f && hi >= 0.0f) return maxr(lo, 0.0f);
   return 2.0f;
+}
+
+// integrate.py:48-58 and 98-115 (path_entry) for a static shape other than a box: the path o -> e (shape frame) sampled
+// at `samples` evenly spaced parameters; the first sample inside and the last one before it are bisected 8 times, and
+// the last outside parameter is returned; 2 when the path stays outside or starts inside.
+constexpr int SWEEP_SAMPLES = 64, SWEEP_BISECT = 8;
+
+__device__ __forceinline__ float shape_entry(int geo, const float4& s, float ox, float oy, float oz, float ex, float ey,
+                                             float ez, int samples) {
+  if (geo == GEO_BOX) return box_entry(s, ox, oy, oz, ex, ey, ez);
+  if (shape_phi(geo, s, ox, oy, oz) < 0.0f) return 2.0f;
+  const float dx = ex - ox, dy = ey - oy, dz = ez - oz;
+  auto inside = [&](float t) {
+    return shape_phi(geo, s, ADF_FMA(t, dx, ox), ADF_FMA(t, dy, oy), ADF_FMA(t, dz, oz)) < 0.0f;
+  };
+  float t_lo = 0.0f, t_hi = 2.0f;
+  for (int k = 1; k <= samples && t_hi > 1.0f; ++k) {
+    const float t = (float)k / (float)samples;
+    if (inside(t)) t_hi = t;
+    else t_lo = t;
+  }
+  if (t_hi > 1.0f) return 2.0f;
+  for (int b = 0; b < SWEEP_BISECT; ++b) {
+    const float tm = 0.5f * (t_lo + t_hi);
+    if (inside(tm)) t_hi = tm;
+    else t_lo = tm;
+  }
+  return t_lo;
 }
 
 // integrate.py:192-205: Coulomb friction of a projection onto box sh (Config.wall_friction), after the inward speed
@@ -2896,16 +2984,20 @@ __device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float 
   if (c1 > c0 && __fsqrt_rn(dot_plain(stx, sty, stz, stx, sty, stz)) > P.sweep_len) {
     const float x0 = x - stx, y0 = y - sty, z0 = z - stz;
     const float spx = x - x0, spy = y - y0, spz = z - z0;
-    const float reach = __fsqrt_rn(dot_plain(spx, spy, spz, spx, spy, spz)) + P.prad;
+    const float len = __fsqrt_rn(dot_plain(spx, spy, spz, spx, spy, spz));
+    const float reach = len + P.prad;
+    // integrate.py:56-58: samples of a path against a shape other than a box, one per particle radius, 8 to 64
+    const int samples = min(max((int)ceilf(len / P.prad) + 1, 8), SWEEP_SAMPLES);
     float best = 2.0f, lhx = 0.0f, lhy = 0.0f, lhz = 0.0f;
     int hit = -1;
     for (int c = c0; c < c1; ++c) {
       const int sh = P.sh_ids[c];
       const float4 cp = P.sh_pos[sh];
+      const int geo = P.sh_geo[sh];
       const float ox = x0 - cp.x, oy = y0 - cp.y, oz = z0 - cp.z;
-      if (!(__fsqrt_rn(dot_plain(ox, oy, oz, ox, oy, oz)) <= cp.w + reach)) continue;
+      if (geo != GEO_PLANE && !(__fsqrt_rn(dot_plain(ox, oy, oz, ox, oy, oz)) <= cp.w + reach)) continue;
       const float ex = x - cp.x, ey = y - cp.y, ez = z - cp.z;
-      const float t = box_entry(P.sh_half[sh], ox, oy, oz, ex, ey, ez);
+      const float t = shape_entry(geo, P.sh_half[sh], ox, oy, oz, ex, ey, ez, samples);
       if (t < best) {
         best = t;
         hit = sh;
@@ -2916,9 +3008,10 @@ __device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float 
     }
     if (hit >= 0) {
       const float4 cp = P.sh_pos[hit], hx = P.sh_half[hit];
-      const float phi = box_sdf(lhx, lhy, lhz, hx);
+      const int geo = P.sh_geo[hit];
+      const float phi = shape_phi(geo, hx, lhx, lhy, lhz);
       float nx, ny, nz;
-      box_normal(lhx, lhy, lhz, hx, nx, ny, nz);
+      shape_normal(geo, hx, lhx, lhy, lhz, nx, ny, nz);
       const float push = maxr(P.eps - phi, 0.0f);
       x = ADF_FMA(push, nx, lhx + cp.x);
       y = ADF_FMA(push, ny, lhy + cp.y);
@@ -2958,13 +3051,14 @@ __device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float 
           }
           moved = busy = 1;
         }
-      } else if (sh >= 0) {  // a static box: its SDF at the new place, its start plane when that holds it
+      } else if (sh >= 0) {  // a static shape: its SDF at the new place, its start plane when that holds it
         const float4 cp = P.sh_pos[sh], hx = P.sh_half[sh];
+        const int geo = P.sh_geo[sh];
         const float lx = x - cp.x, ly = y - cp.y, lz = z - cp.z;
-        const float phi = box_sdf(lx, ly, lz, hx);
+        const float phi = shape_phi(geo, hx, lx, ly, lz);
         if (phi < P.eps) {
           float nx, ny, nz;
-          box_normal(lx, ly, lz, hx, nx, ny, nz);
+          shape_normal(geo, hx, lx, ly, lz, nx, ny, nz);
           float push = P.eps - phi;
           if (vb.w >= 0.0f) {
             const float push_s = P.eps - dotf(nn.x, nn.y, nn.z, x - (xb.x + cp.x), y - (xb.y + cp.y), z - (xb.z + cp.z));

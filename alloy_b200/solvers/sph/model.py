@@ -128,19 +128,16 @@ class ModelBuilder:
     def shape_count(self) -> int:
         return len(self._shapes["type"])
 
-    def add_shape_box(self, body: int = -1, xform=None, hx: float = 0.5, hy: float = 0.5, hz: float = 0.5,
-                      mu: float = 1.0, collide_particles: bool = True, sph_boundary: int = 0) -> int:
-        """A box shape (half extents hx, hy, hz) at ``xform`` = (px, py, pz[, qx, qy, qz, qw]) in the current world
-        (global, world -1, when no world is open), as newton.ModelBuilder.add_shape_box; ``sph_boundary`` is the
-        sph:shape_boundary attribute (0 auto, 1 sdf, 2 akinci, 3 ignore). Returns the shape id."""
+    def _add_shape(self, geo: int, scale, body: int, xform, mu: float, collide_particles: bool,
+                   sph_boundary: int) -> int:
         x = np.zeros(7, np.float32)
         x[6] = 1.0
         if xform is not None:
             v = np.asarray(tuple(xform), np.float32).reshape(-1)
             x[: v.size] = v
         sh = self._shapes
-        sh["type"].append(int(GeoType.BOX))
-        sh["scale"].append((float(hx), float(hy), float(hz)))
+        sh["type"].append(int(geo))
+        sh["scale"].append(tuple(float(a) for a in scale))
         sh["xform"].append(x)
         sh["world"].append(self._world)
         sh["flags"].append(int(ShapeFlags.VISIBLE | ShapeFlags.COLLIDE_SHAPES |
@@ -149,6 +146,39 @@ class ModelBuilder:
         sh["mu"].append(float(mu))
         sh["boundary"].append(int(sph_boundary))
         return len(sh["type"]) - 1
+
+    def add_shape_box(self, body: int = -1, xform=None, hx: float = 0.5, hy: float = 0.5, hz: float = 0.5,
+                      mu: float = 1.0, collide_particles: bool = True, sph_boundary: int = 0) -> int:
+        """A box shape (half extents hx, hy, hz) at ``xform`` = (px, py, pz[, qx, qy, qz, qw]) in the current world
+        (global, world -1, when no world is open), as newton.ModelBuilder.add_shape_box; ``sph_boundary`` is the
+        sph:shape_boundary attribute (0 auto, 1 sdf, 2 akinci, 3 ignore). Returns the shape id."""
+        return self._add_shape(GeoType.BOX, (hx, hy, hz), body, xform, mu, collide_particles, sph_boundary)
+
+    def add_shape_sphere(self, body: int = -1, xform=None, radius: float = 1.0, mu: float = 1.0,
+                         collide_particles: bool = True, sph_boundary: int = 0) -> int:
+        """A sphere shape (scale (radius, 0, 0)), as newton.ModelBuilder.add_shape_sphere."""
+        return self._add_shape(GeoType.SPHERE, (radius, 0.0, 0.0), body, xform, mu, collide_particles, sph_boundary)
+
+    def add_shape_capsule(self, body: int = -1, xform=None, radius: float = 1.0, half_height: float = 0.5,
+                          mu: float = 1.0, collide_particles: bool = True, sph_boundary: int = 0) -> int:
+        """A capsule along the shape's z axis (scale (radius, half_height, 0)), as newton.ModelBuilder.add_shape_capsule
+        with its axis along z."""
+        return self._add_shape(GeoType.CAPSULE, (radius, half_height, 0.0), body, xform, mu, collide_particles,
+                               sph_boundary)
+
+    def add_shape_plane(self, body: int = -1, xform=None, width: float = 0.0, length: float = 0.0, mu: float = 1.0,
+                        collide_particles: bool = True, sph_boundary: int = 0) -> int:
+        """A plane through the shape's origin with normal along its z axis, finite (half width, half length) when both
+        are positive, else infinite, as newton.ModelBuilder.add_shape_plane."""
+        return self._add_shape(GeoType.PLANE, (width, length, 0.0), body, xform, mu, collide_particles, sph_boundary)
+
+    def add_ground_plane(self, height: float = 0.0, mu: float = 1.0) -> int:
+        """The infinite ground plane z = height, normal +z (newton.ModelBuilder.add_ground_plane with z up), global."""
+        world, self._world = self._world, -1
+        try:
+            return self.add_shape_plane(-1, (0.0, 0.0, height), mu=mu)
+        finally:
+            self._world = world
 
     @property
     def particle_count(self) -> int:

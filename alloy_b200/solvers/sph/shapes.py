@@ -4,8 +4,9 @@ layout.py:131-164 radius and thinnest wall, layout.py:207-246 ``shape_table``).
 
 A shape bounds the liquid when it collides with particles (``ShapeFlags.COLLIDE_PARTICLES``), has a signed distance
 field, and its ``sph:shape_boundary`` is not ``ignore``; each world sees its own shapes, then the global ones
-(world -1). This path evaluates box shapes (``GeoType.BOX``, the walls of ``add_box_tank``) that are static (no
-body) and axis-aligned; the constructor refuses other particle-colliding shapes with a message naming them.
+(world -1). This path evaluates static shapes (no body) with closed-form distances: axis-aligned boxes (the walls of
+``add_box_tank``), spheres, capsules along z and planes with normal +z (a ground plane); the constructor refuses other
+particle-colliding shapes with a message naming them.
 """
 
 from __future__ import annotations
@@ -26,15 +27,32 @@ class ShapeTable:
     start: np.ndarray   # int32 [W + 1]: world w's shapes are ids[start[w]:start[w + 1]]
     ids: np.ndarray     # int32: shape ids, each world's own then the global ones
     geo: np.ndarray     # int32 [S]
-    scale: np.ndarray   # float32 [S][3]: box half extents
+    scale: np.ndarray   # float32 [S][3]: box half extents; sphere radius; capsule radius, half height; plane half sizes
     xform: np.ndarray   # float32 [S][7]: (p, q xyzw)
-    radius: np.ndarray  # float32 [S]: bounding radius about the shape origin (|half extents| for a box)
+    radius: np.ndarray  # float32 [S]: bounding radius about the shape origin (newton geometry/utils.py:77-110)
     mu: np.ndarray      # float32 [S]: Coulomb friction of the wall
-    thinnest: float     # [m] thinnest wall of the table (twice a box's smallest half extent), inf without shapes
+    thinnest: float     # [m] thinnest wall of the table (layout.py:131-149), inf without shapes
 
     @property
     def count(self) -> int:
         return int(len(self.geo))
+
+
+PATH_GEOS = (int(GeoType.BOX), int(GeoType.SPHERE), int(GeoType.CAPSULE), int(GeoType.PLANE))
+THIN_AXES = {int(GeoType.BOX): (0, 1, 2), int(GeoType.SPHERE): (0,), int(GeoType.CAPSULE): (0,)}
+
+
+def shape_radius(geo: int, scale) -> float:
+    """The radius about the shape's origin that encloses it (newton geometry/utils.py:77-110; a plane's is unused:
+    planes are never culled by distance, boundary.py:219)."""
+    s = np.abs(np.asarray(scale, np.float64))
+    if geo == int(GeoType.SPHERE):
+        return float(s[0])
+    if geo == int(GeoType.CAPSULE):
+        return float(s[0] + s[1])
+    if geo == int(GeoType.PLANE):
+        return float(np.linalg.norm(s)) * 0.5 if s[0] > 0.0 and s[1] > 0.0 else 1.0e6
+    return float(np.linalg.norm(s))
 
 
 def _host(a) -> np.ndarray:
@@ -59,16 +77,19 @@ def shape_table(model) -> ShapeTable:
     usable = ((flags & int(ShapeFlags.COLLIDE_PARTICLES)) != 0) & np.isin(geo, [int(g) for g in SDF_GEOS])
     usable &= boundary != BOUNDARY_IGNORE
     bad = []
+    identity = np.array([0.0, 0.0, 0.0, 1.0], np.float32)
     for s in np.flatnonzero(usable):
-        if geo[s] != int(GeoType.BOX):
-            bad.append(f"shape {s} ({GeoType(int(geo[s])).name.lower()})")
+        name = GeoType(int(geo[s])).name.lower()
+        if int(geo[s]) not in PATH_GEOS:
+            bad.append(f"shape {s} ({name})")
         elif body[s] >= 0:
-            bad.append(f"shape {s} (a box on body {body[s]})")
-        elif not np.array_equal(xform[s, 3:], np.array([0.0, 0.0, 0.0, 1.0], np.float32)):
-            bad.append(f"shape {s} (a rotated box)")
+            bad.append(f"shape {s} (a {name} on body {body[s]})")
+        elif int(geo[s]) != int(GeoType.SPHERE) and not np.array_equal(xform[s, 3:], identity):
+            bad.append(f"shape {s} (a rotated {name})")
     if bad:
-        raise ValueError("SolverDFSPH (B200 build): the liquid's shape walls must be static axis-aligned boxes "
-                         "(add_box_tank, wall_box); not on this build's CUDA path: " + ", ".join(bad[:8]))
+        raise ValueError("SolverDFSPH (B200 build): the liquid's shape walls must be static boxes, spheres, capsules "
+                         "along z or planes facing +z (add_box_tank, wall_box, add_shape_sphere, add_shape_capsule, "
+                         "add_ground_plane), unrotated; not on this build's CUDA path: " + ", ".join(bad[:8]))
     glob = np.flatnonzero(usable & (world < 0))
     start, ids = [0], []
     for w in range(W):
@@ -76,7 +97,11 @@ def shape_table(model) -> ShapeTable:
         ids.extend(int(s) for s in glob)
         start.append(len(ids))
     ids = np.asarray(ids, np.int32)
-    radius = np.array([float(np.linalg.norm(np.abs(scale[s].astype(np.float64)))) for s in range(S)], np.float32)
-    thin = float(2.0 * scale[np.unique(ids)].astype(np.float64).min()) if len(ids) else float("inf")
+    radius = np.array([shape_radius(int(geo[s]), scale[s]) for s in range(S)], np.float32)
+    thin = float("inf")  # layout.py:131-149: planes count as thick
+    for s in np.unique(ids):
+        axes = THIN_AXES.get(int(geo[s]))
+        if axes is not None:
+            thin = min(thin, 2.0 * float(min(float(scale[s][k]) for k in axes)))
     return ShapeTable(np.asarray(start, np.int32), ids, geo, scale, xform, radius,
                       _host(model.shape_material_mu).astype(np.float32), thin)

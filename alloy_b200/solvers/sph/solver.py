@@ -9,11 +9,12 @@ library's sm_100a kernels; this module holds host logic only (validation, consta
 fallback: without a CUDA device or the library it raises.
 
 Scope of the CUDA path: cubic or Wendland kernel, projected preconditioned CG (the reference's default, krylov.py)
-or relaxed Jacobi pressure solves, XSPH, particle walls (boundary particles flagged PROXY), static axis-aligned box
-walls evaluated through their SDF (up to four wall slots per particle, projection and the sweep past fast steps, wall
-friction), emitters, sinks and the escape box. Settings outside it are refused in the constructor (``DFSPHConfig.unsupported``); CG falls back to Jacobi
-with a warning when particle masses or rest densities differ, as the reference does (solver.py:89-91). The
-resting-jitter rule sets each world's density tolerance per step (solve_driver.py:1-118).
+or relaxed Jacobi pressure solves, XSPH, particle walls (boundary particles flagged PROXY), static shape walls
+(axis-aligned boxes, spheres, capsules along z, planes facing +z) evaluated through their SDF (up to four wall slots
+per particle, projection and the sweep past fast steps, wall friction), emitters, sinks and the escape box.
+Settings outside it are refused in the constructor (``DFSPHConfig.unsupported``); CG falls back to Jacobi with a
+warning when particle masses or rest densities differ, as the reference does (solver.py:89-91). The resting-jitter
+rule sets each world's density tolerance per step (solve_driver.py:1-118).
 """
 
 from __future__ import annotations
@@ -246,6 +247,8 @@ class SolverDFSPH:
         md.shape_start = sh_start.ctypes.data_as(C.POINTER(C.c_int32))
         md.shape_ids = sh_ids.ctypes.data_as(C.POINTER(C.c_int32))
         md.shape_box = box.ctypes.data_as(C.POINTER(C.c_float))
+        geo = np.ascontiguousarray(tab.geo if tab.count else np.full(1, 7), np.int32)
+        md.shape_geo = geo.ctypes.data_as(C.POINTER(C.c_int32))
         md.sweep_len = min(0.5 * cfg.h, 0.5 * tab.thinnest)  # integrate.py:42-49
         handle = C.c_void_p()
         with torch.cuda.device(self.device):

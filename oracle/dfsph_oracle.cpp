@@ -266,6 +266,7 @@ template <class R> struct Solver {
   int S = 0;
   std::vector<int> sh_start, sh_ids;
   std::vector<float> sh_pos, sh_half, sh_radius, sh_mu;
+  std::vector<int> sh_geo;  // newton GeoType per shape (box, sphere, capsule along z, plane facing +z)
   double sweep_len = 1.0e30;
   std::vector<int> swept;
   std::vector<R> ratio, alpha, neff, active, reg, src, kappa, lower, err;
@@ -465,7 +466,42 @@ template <class R> struct Solver {
     if ((qy > qx && qy > qz) || (qx == R(0) && qz == R(0))) return {R(0), sy, R(0)};
     return {R(0), R(0), sz};
   }
-  V3<R> shape_local(int sh, const V3<R>& x) const {  // static axis-aligned box: the frame is its centre
+  // newton eval_shape_sdf (soft_contacts_sdf.py:249-280) for the analytic shapes of this path: the signed distance of
+  // shape sh at shape-local p (box sdf_box; sphere sdf_sphere; capsule along z sdf_capsule; plane facing +z sdf_plane,
+  // finite for positive half sizes) and its outward unit gradient (sdf_*_grad; +z at a sphere's centre or a capsule's
+  // axis, -z below its lower cap; +z for a plane)
+  static constexpr int GEO_PLANE = 1, GEO_SPHERE = 3, GEO_CAPSULE = 4, GEO_BOX = 7;
+  R shape_phi(int sh, const V3<R>& p) const {
+    const float* s = &sh_half[3 * sh];
+    const int g = sh_geo[sh];
+    if (g == GEO_BOX) return box_sdf(p, s);
+    if (g == GEO_PLANE) {
+      if (s[0] > 0.0f && s[1] > 0.0f)
+        return maxr(maxr(std::fabs(p.x) - R(s[0]), std::fabs(p.y) - R(s[1])), std::fabs(p.z));
+      return p.z;
+    }
+    R cz = p.z;
+    if (g == GEO_CAPSULE) cz = p.z > R(s[1]) ? p.z - R(s[1]) : (p.z < -R(s[1]) ? p.z + R(s[1]) : R(0));
+    const V3<R> v{p.x, p.y, cz};
+    return std::sqrt(dot_plain(v, v)) - R(s[0]);
+  }
+  V3<R> shape_grad(int sh, const V3<R>& p) const {
+    const float* s = &sh_half[3 * sh];
+    const int g = sh_geo[sh];
+    if (g == GEO_BOX) return box_grad(p, s);
+    if (g == GEO_PLANE) return {R(0), R(0), R(1)};
+    R cz = p.z, dz = R(1);
+    if (g == GEO_CAPSULE) {
+      if (p.z > R(s[1])) cz = p.z - R(s[1]);
+      else if (p.z < -R(s[1])) { cz = p.z + R(s[1]); dz = R(-1); }
+      else cz = R(0);
+    }
+    const V3<R> v{p.x, p.y, cz};
+    const R l = std::sqrt(dot_plain(v, v));
+    if (l > R(1.0e-8)) return {v.x / l, v.y / l, v.z / l};
+    return {R(0), R(0), dz};
+  }
+  V3<R> shape_local(int sh, const V3<R>& x) const {  // static unrotated shape: the frame is its origin
     return {x.x - R(sh_pos[3 * sh]), x.y - R(sh_pos[3 * sh + 1]), x.z - R(sh_pos[3 * sh + 2])};
   }
   V3<R> shape_world(int sh, const V3<R>& l) const {
@@ -570,11 +606,11 @@ template <class R> struct Solver {
         for (int c = sh_start[w]; c < sh_start[w + 1]; ++c) {
           const int sh = sh_ids[c];
           const V3<R> d{x.x - R(sh_pos[3 * sh]), x.y - R(sh_pos[3 * sh + 1]), x.z - R(sh_pos[3 * sh + 2])};
-          if (std::sqrt(dot_plain(d, d)) > R(sh_radius[sh]) + kc.h) continue;
+          if (sh_geo[sh] != GEO_PLANE && std::sqrt(dot_plain(d, d)) > R(sh_radius[sh]) + kc.h) continue;
           const V3<R> xl = shape_local(sh, x);
-          const R phi = box_sdf(xl, &sh_half[3 * sh]);
+          const R phi = shape_phi(sh, xl);
           if (phi < reach && phi + offset < kc.h) {
-            const V3<R> nw = normalized(box_grad(xl, &sh_half[3 * sh]));
+            const V3<R> nw = normalized(shape_grad(sh, xl));
             if (shape_insert(i, ns, sh, phi, nw, nr, near) > 0 && ns < NS) ++ns;
           }
         }
@@ -633,8 +669,8 @@ template <class R> struct Solver {
             s_nbl[o] = nrm;
           } else {
             const V3<R> xl = shape_local(sh, x);
-            phi = box_sdf(xl, &sh_half[3 * sh]);
-            const V3<R> gl = box_grad(xl, &sh_half[3 * sh]);
+            phi = shape_phi(sh, xl);
+            const V3<R> gl = shape_grad(sh, xl);
             nrm = normalized(gl);
             s_nbl[o] = nrm;
             s_xbl[o] = {fma_(-phi, nrm.x, xl.x), fma_(-phi, nrm.y, xl.y), fma_(-phi, nrm.z, xl.z)};
@@ -1196,6 +1232,29 @@ template <class R> struct Solver {
     return R(2);
   }
 
+  // integrate.py:48-58 and 98-115 (path_entry) for a shape other than a box: the path l0 -> l1 sampled at `samples`
+  // evenly spaced parameters, the first sample inside and the last before it bisected 8 times; the last outside
+  // parameter, or 2 when the path stays outside or starts inside
+  R shape_entry(int sh, const V3<R>& l0, const V3<R>& l1, int samples) const {
+    if (sh_geo[sh] == GEO_BOX) return box_entry(sh, l0, l1);
+    if (shape_phi(sh, l0) < R(0)) return R(2);
+    const V3<R> d{l1.x - l0.x, l1.y - l0.y, l1.z - l0.z};
+    auto inside = [&](R t) { return shape_phi(sh, V3<R>{fma_(t, d.x, l0.x), fma_(t, d.y, l0.y), fma_(t, d.z, l0.z)}) < R(0); };
+    R t_lo = R(0), t_hi = R(2);
+    for (int k = 1; k <= samples && t_hi > R(1); ++k) {
+      const R t = R(k) / R(samples);
+      if (inside(t)) t_hi = t;
+      else t_lo = t;
+    }
+    if (t_hi > R(1)) return R(2);
+    for (int b = 0; b < 8; ++b) {
+      const R tm = R(0.5) * (t_lo + t_hi);
+      if (inside(tm)) t_hi = tm;
+      else t_lo = tm;
+    }
+    return t_lo;
+  }
+
   // integrate.py:192-205: Coulomb friction of a projection (Config.wall_friction) after the inward speed -vn went
   V3<R> wall_friction_v(V3<R> vv, const V3<R>& vb, const V3<R>& nn, R vn, int sh) const {
     if (!P.wall_friction) return vv;
@@ -1233,16 +1292,18 @@ template <class R> struct Solver {
       if (sh_start[w + 1] > sh_start[w] && std::sqrt(dot_plain(step, step)) > sweep) {
         const V3<R> x0{x.x - step.x, x.y - step.y, x.z - step.z};
         const V3<R> span = sub(x, x0);
-        const R reach = std::sqrt(dot_plain(span, span)) + r;
+        const R len = std::sqrt(dot_plain(span, span));
+        const R reach = len + r;
+        const int samples = std::min(std::max((int)std::ceil(len / r) + 1, 8), 64);  // integrate.py:48, 56-58
         R best = R(2);
         int hit = -1;
         V3<R> lh{R(0), R(0), R(0)};
         for (int c = sh_start[w]; c < sh_start[w + 1]; ++c) {
           const int sh = sh_ids[c];
           const V3<R> d0{x0.x - R(sh_pos[3 * sh]), x0.y - R(sh_pos[3 * sh + 1]), x0.z - R(sh_pos[3 * sh + 2])};
-          if (!(std::sqrt(dot_plain(d0, d0)) <= R(sh_radius[sh]) + reach)) continue;
+          if (sh_geo[sh] != GEO_PLANE && !(std::sqrt(dot_plain(d0, d0)) <= R(sh_radius[sh]) + reach)) continue;
           const V3<R> l0 = shape_local(sh, x0), l1 = shape_local(sh, x);
-          const R t = box_entry(sh, l0, l1);
+          const R t = shape_entry(sh, l0, l1, samples);
           if (t < best) {
             best = t;
             hit = sh;
@@ -1250,8 +1311,8 @@ template <class R> struct Solver {
           }
         }
         if (hit >= 0) {
-          const R phi = box_sdf(lh, &sh_half[3 * hit]);
-          const V3<R> nn = normalized(box_grad(lh, &sh_half[3 * hit]));
+          const R phi = shape_phi(hit, lh);
+          const V3<R> nn = normalized(shape_grad(hit, lh));
           const V3<R> xw = shape_world(hit, lh);
           const R push = maxr(eps - phi, R(0));
           x = {fma_(push, nn.x, xw.x), fma_(push, nn.y, xw.y), fma_(push, nn.z, xw.z)};
@@ -1281,11 +1342,11 @@ template <class R> struct Solver {
               if (vn < R(0)) vv = {fma_(-vn, nn.x, vv.x), fma_(-vn, nn.y, vv.y), fma_(-vn, nn.z, vv.z)};
               moved = busy = 1;
             }
-          } else if (sh >= 0) {  // a static box: its SDF at the new place, its start plane when that holds it
+          } else if (sh >= 0) {  // a static shape: its SDF at the new place, its start plane when that holds it
             const V3<R> xl = shape_local(sh, x);
-            const R phi = box_sdf(xl, &sh_half[3 * sh]);
+            const R phi = shape_phi(sh, xl);
             if (phi < eps) {
-              V3<R> nn = normalized(box_grad(xl, &sh_half[3 * sh]));
+              V3<R> nn = normalized(shape_grad(sh, xl));
               R push = eps - phi;
               if (s_phi[o] >= R(0)) {
                 const V3<R> ns = s_nbl[o];
@@ -1624,9 +1685,11 @@ void orc_get_slot_shapes(void* hp, int* out) {
 // box's centre pos[S][3], half extents half[S][3], bounding radius[S] and friction mu[S]; sweep length
 // min(h / 2, thinnest / 2) (integrate.py:42-49).
 void orc_set_shapes(void* hp, int S, const int* start, const int* ids, const float* pos, const float* half,
-                    const float* radius, const float* mu, double thinnest) {
+                    const float* radius, const float* mu, double thinnest, const int* geo) {
   DISPATCH({
     s.S = S;
+    s.sh_geo.assign(S, 7);
+    if (geo) s.sh_geo.assign(geo, geo + S);
     s.sh_start.assign(start, start + s.W + 1);
     s.sh_ids.assign(ids, ids + start[s.W]);
     s.sh_pos.assign(pos, pos + 3 * S);
@@ -1634,6 +1697,20 @@ void orc_set_shapes(void* hp, int S, const int* start, const int* ids, const flo
     s.sh_radius.assign(radius, radius + S);
     s.sh_mu.assign(mu, mu + S);
     s.sweep_len = std::min(0.5 * s.P.h, 0.5 * thinnest);
+  });
+}
+
+// The signed distance and outward unit gradient of shape sh at shape-local point p (out: phi, gx, gy, gz), as the
+// slots, the sweep and the projection evaluate it.
+void orc_shape_sdf(void* hp, int sh, const double* p, double* out) {
+  DISPATCH({
+    using RT = typename std::remove_reference<decltype(s.kv)>::type::value_type;
+    const V3<RT> x{RT(p[0]), RT(p[1]), RT(p[2])};
+    const V3<RT> g = s.shape_grad(sh, x);
+    out[0] = (double)s.shape_phi(sh, x);
+    out[1] = (double)g.x;
+    out[2] = (double)g.y;
+    out[3] = (double)g.z;
   });
 }
 
