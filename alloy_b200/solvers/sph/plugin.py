@@ -5,8 +5,8 @@ build this solver where it builds its own.
 
 ``_factory(view, kwargs)`` follows ``plugin.py:36-61``: ``config`` (a DFSPHConfig) or DFSPHConfig fields as kwargs,
 plus ``capacity_per_world``; unknown kwargs raise ``TypeError``; without ``config`` and without a ``world_bounds``
-kwarg the escape box comes from the scene's content (``escape_box.py:69-94``: the particles' box padded by
-``max(0.25 m, its largest extent)`` on every side). ``register(registry)`` hands the capability and the adapters to
+kwarg the escape box comes from the scene's content (``escape_box.py:44-94``: the box of the finite shapes and the
+particles, padded by ``max(0.25 m, its largest extent)`` on every side). ``register(registry)`` hands the capability and the adapters to
 alloy's registry when one is given (``alloy.core.registry.register_solver`` and friends), else records them in this
 module's ``REGISTRY``.
 """
@@ -28,19 +28,40 @@ log = logging.getLogger("alloy.sph")
 
 _CONFIG_FIELDS = frozenset(f.name for f in dataclasses.fields(DFSPHConfig))
 AUTO_PAD_MIN = 0.25  # escape_box.py:30
+PLANE_RADIUS = 1.0e5  # escape_box.py:32: shapes with a larger bounding radius (planes) are not content
+
+
+def content_box(model: Any):
+    """(lo, hi) of the model's finite shapes (their bounding spheres about their origins; planes are left out) and of
+    every particle with a finite position (active ones and spares), over all worlds; None for an empty model
+    (escape_box.py:44-75)."""
+    pts = np.zeros((0, 3))
+    if int(getattr(model, "particle_count", 0) or 0):
+        q = _host(model.particle_q).astype(np.float64).reshape(-1, 3)
+        pts = q[np.isfinite(q).all(axis=1)]
+    lo_s, hi_s = np.zeros((0, 3)), np.zeros((0, 3))
+    S = int(getattr(model, "shape_count", 0) or 0)
+    if S:
+        from .shapes import shape_radius
+
+        geo = _host(model.shape_type).astype(np.int32)
+        scale = _host(model.shape_scale).astype(np.float64).reshape(-1, 3)
+        c = _host(model.shape_transform).astype(np.float64).reshape(-1, 7)[:, :3]
+        r = np.array([shape_radius(int(geo[k]), scale[k]) for k in range(S)])
+        keep = np.isfinite(r) & (r < PLANE_RADIUS) & np.isfinite(c).all(axis=1)
+        lo_s, hi_s = c[keep] - r[keep, None], c[keep] + r[keep, None]
+    if len(pts) == 0 and len(lo_s) == 0:
+        return None
+    return np.vstack([lo_s, pts]).min(axis=0), np.vstack([hi_s, pts]).max(axis=0)
 
 
 def auto_box(model: Any, pad_min: float = AUTO_PAD_MIN):
-    """((lo, hi), pad): the box of every particle with a finite position (active ones and spares), padded by
-    max(pad_min, its largest extent) on every side; None for a model without particles (escape_box.py:69-88; the
-    model has no SDF shapes on this path)."""
-    if not int(getattr(model, "particle_count", 0) or 0):
+    """((lo, hi), pad): the content box padded by max(pad_min, its largest extent) on every side; None for an empty
+    model (escape_box.py:78-94)."""
+    box = content_box(model)
+    if box is None:
         return None
-    q = _host(model.particle_q).astype(np.float64).reshape(-1, 3)
-    q = q[np.isfinite(q).all(axis=1)]
-    if len(q) == 0:
-        return None
-    lo, hi = q.min(axis=0), q.max(axis=0)
+    lo, hi = box
     pad = max(float(pad_min), float((hi - lo).max()))
     return (tuple(float(v) for v in lo - pad), tuple(float(v) for v in hi + pad)), pad
 
