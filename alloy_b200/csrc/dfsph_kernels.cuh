@@ -128,7 +128,7 @@ struct DevP {
   const int* sh_ids;
   const float4* sh_pos;   // centre (3), bounding radius
   const float4* sh_half;  // the shape's scale (3: box half extents; sphere radius; capsule radius, half height; plane
-                          // half width, half length, 0 for an infinite plane), Coulomb friction mu
+                          // width, length, 0 for an infinite plane), Coulomb friction mu
   const int* sh_geo;      // newton GeoType per shape (GEO_BOX, GEO_SPHERE, GEO_CAPSULE, GEO_PLANE)
   float sweep_len;        // a step longer than this is swept against the world's boxes (integrate.py:42-49)
   float prad;             // particle radius
@@ -1151,12 +1151,28 @@ constexpr int GEO_PLANE = 1, GEO_SPHERE = 3, GEO_CAPSULE = 4, GEO_BOX = 7;
 // The signed distance of shape `geo` (scale s.xyz) at shape-frame point (x, y, z), as newton's eval_shape_sdf evaluates
 // the analytic shapes (soft_contacts_sdf.py:249-280, geometry/kernels.py): a box (sdf_box :310-333), a sphere
 // (sdf_sphere :277-288), a capsule along the shape's z axis (sdf_capsule :374-393), a plane through the shape's origin
-// with normal +z (sdf_plane :708-729: finite for positive half width and length, an L-infinity distance to the quad).
+// with normal +z (soft_contacts_sdf.py:73-102 _eval_plane_sdf with depth 0: infinite unless width s.x and length
+// s.y are both positive; a finite plane is a two-sided sheet, z over its footprint from above, else the distance to
+// its nearest point).
+__device__ __forceinline__ bool plane_over(const float4& s, float x, float y, float z) {
+  const float hw = 0.5f * s.x, hl = 0.5f * s.y;
+  return !(hw > 0.0f && hl > 0.0f) || (fabsf(x) <= hw && fabsf(y) <= hl && z >= 0.0f);
+}
+
+__device__ __forceinline__ void plane_delta(const float4& s, float x, float y, float z, float& dx, float& dy, float& dz) {
+  const float hw = 0.5f * s.x, hl = 0.5f * s.y;
+  dx = x - minr(maxr(x, -hw), hw);
+  dy = y - minr(maxr(y, -hl), hl);
+  dz = z - 0.0f;
+}
+
 __device__ __forceinline__ float shape_phi(int geo, const float4& s, float x, float y, float z) {
   if (geo == GEO_BOX) return box_sdf(x, y, z, s);
   if (geo == GEO_PLANE) {
-    if (s.x > 0.0f && s.y > 0.0f) return maxr(maxr(fabsf(x) - s.x, fabsf(y) - s.y), fabsf(z));
-    return z;
+    if (plane_over(s, x, y, z)) return z;
+    float dx, dy, dz;
+    plane_delta(s, x, y, z, dx, dy, dz);
+    return __fsqrt_rn(dot_plain(dx, dy, dz, dx, dy, dz));
   }
   float cz = z;
   if (geo == GEO_CAPSULE) cz = z > s.y ? z - s.y : (z < -s.y ? z + s.y : 0.0f);
@@ -1176,6 +1192,17 @@ __device__ __forceinline__ void shape_normal(int geo, const float4& s, float x, 
     nx = 0.0f;
     ny = 0.0f;
     nz = 1.0f;
+    if (!plane_over(s, x, y, z)) {
+      float dx, dy, dz;
+      plane_delta(s, x, y, z, dx, dy, dz);
+      const float d = __fsqrt_rn(dot_plain(dx, dy, dz, dx, dy, dz));
+      if (d > 0.0f) {
+        nx = dx / d;
+        ny = dy / d;
+        nz = dz / d;
+      }
+    }
+    normalized3(nx, ny, nz);
     return;
   }
   float cz = z, dz = 1.0f;

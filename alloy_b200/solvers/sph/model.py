@@ -168,8 +168,8 @@ class ModelBuilder:
 
     def add_shape_plane(self, body: int = -1, xform=None, width: float = 0.0, length: float = 0.0, mu: float = 1.0,
                         collide_particles: bool = True, sph_boundary: int = 0) -> int:
-        """A plane through the shape's origin with normal along its z axis, finite (half width, half length) when both
-        are positive, else infinite, as newton.ModelBuilder.add_shape_plane."""
+        """A plane through the shape's origin with normal along its z axis, finite (width along x, length along y) when
+        both are positive, else infinite, as newton.ModelBuilder.add_shape_plane."""
         return self._add_shape(GeoType.PLANE, (width, length, 0.0), body, xform, mu, collide_particles, sph_boundary)
 
     def add_ground_plane(self, height: float = 0.0, mu: float = 1.0) -> int:

@@ -27,7 +27,7 @@ class ShapeTable:
     start: np.ndarray   # int32 [W + 1]: world w's shapes are ids[start[w]:start[w + 1]]
     ids: np.ndarray     # int32: shape ids, each world's own then the global ones
     geo: np.ndarray     # int32 [S]
-    scale: np.ndarray   # float32 [S][3]: box half extents; sphere radius; capsule radius, half height; plane half sizes
+    scale: np.ndarray   # float32 [S][3]: box half extents; sphere radius; capsule radius, half height; plane width, length
     xform: np.ndarray   # float32 [S][7]: (p, q xyzw)
     radius: np.ndarray  # float32 [S]: bounding radius about the shape origin (newton geometry/utils.py:77-110)
     mu: np.ndarray      # float32 [S]: Coulomb friction of the wall

@@ -101,7 +101,7 @@ def shape_obstacles(spacing: float = 0.02, dt: float = 1.0e-3, steps: int = 20, 
     add_box_tank(b, (0.0, 0.0, 0.0), (0.3, 0.3, 0.4), wall=cfg.h, open_top=True, floor=False)
     b.add_shape_sphere(-1, (0.15, 0.15, 0.08), radius=0.05, mu=0.4)
     b.add_shape_capsule(-1, (0.07, 0.22, 0.08), radius=0.025, half_height=0.04, mu=0.6)
-    b.add_shape_plane(-1, (0.23, 0.07, 0.12), width=0.04, length=0.04, mu=0.3)
+    b.add_shape_plane(-1, (0.23, 0.07, 0.12), width=0.08, length=0.08, mu=0.3)
     b.end_world()
     b.add_ground_plane(0.0, mu=0.5)
     return Scene(b.finalize(device), cfg, dt, steps, len(fl) + len(lone), 0, name="shape_obstacles")

@@ -91,8 +91,8 @@ typedef struct {
   const int32_t* shape_start;    /* host [W + 1]: world w's walls are shape_ids[shape_start[w] .. shape_start[w + 1]) */
   const int32_t* shape_ids;      /* host [shape_start[W]] */
   const float* shape_box;        /* host [S][8]: centre xyz, bounding radius, scale xyz (box half extents; sphere
-                                    radius; capsule radius, half height; plane half width, half length, 0 for an
-                                    infinite plane), Coulomb friction */
+                                    radius; capsule radius, half height; plane width, length, 0 for an infinite
+                                    plane), Coulomb friction */
   double sweep_len;              /* [m] a step longer than this is swept against the shapes: min(h, thinnest) / 2
                                     (integrate.py:42-49) */
   const int32_t* shape_geo;      /* host [S]: newton GeoType per shape (7 box, 3 sphere, 4 capsule, 1 plane); NULL: all

@@ -467,18 +467,28 @@ template <class R> struct Solver {
     return {R(0), R(0), sz};
   }
   // newton eval_shape_sdf (soft_contacts_sdf.py:249-280) for the analytic shapes of this path: the signed distance of
-  // shape sh at shape-local p (box sdf_box; sphere sdf_sphere; capsule along z sdf_capsule; plane facing +z sdf_plane,
-  // finite for positive half sizes) and its outward unit gradient (sdf_*_grad; +z at a sphere's centre or a capsule's
+  // shape sh at shape-local p (box sdf_box; sphere sdf_sphere; capsule along z sdf_capsule; plane facing +z
+  // _eval_plane_sdf) and its outward unit gradient (sdf_*_grad; +z at a sphere's centre or a capsule's
   // axis, -z below its lower cap; +z for a plane)
   static constexpr int GEO_PLANE = 1, GEO_SPHERE = 3, GEO_CAPSULE = 4, GEO_BOX = 7;
+  // soft_contacts_sdf.py:73-102 (_eval_plane_sdf, depth 0): infinite unless width and length are both positive; a
+  // finite plane is a two-sided sheet, its z over the footprint from above, else the distance to its nearest point
+  static bool plane_over(const float* s, const V3<R>& p) {
+    const R hw = R(0.5) * R(s[0]), hl = R(0.5) * R(s[1]);
+    return !(hw > R(0) && hl > R(0)) || (std::fabs(p.x) <= hw && std::fabs(p.y) <= hl && p.z >= R(0));
+  }
+  static V3<R> plane_delta(const float* s, const V3<R>& p) {
+    const R hw = R(0.5) * R(s[0]), hl = R(0.5) * R(s[1]);
+    return {p.x - clampr(p.x, -hw, hw), p.y - clampr(p.y, -hl, hl), p.z - R(0)};
+  }
   R shape_phi(int sh, const V3<R>& p) const {
     const float* s = &sh_half[3 * sh];
     const int g = sh_geo[sh];
     if (g == GEO_BOX) return box_sdf(p, s);
     if (g == GEO_PLANE) {
-      if (s[0] > 0.0f && s[1] > 0.0f)
-        return maxr(maxr(std::fabs(p.x) - R(s[0]), std::fabs(p.y) - R(s[1])), std::fabs(p.z));
-      return p.z;
+      if (plane_over(s, p)) return p.z;
+      const V3<R> d = plane_delta(s, p);
+      return std::sqrt(dot_plain(d, d));
     }
     R cz = p.z;
     if (g == GEO_CAPSULE) cz = p.z > R(s[1]) ? p.z - R(s[1]) : (p.z < -R(s[1]) ? p.z + R(s[1]) : R(0));
@@ -489,7 +499,13 @@ template <class R> struct Solver {
     const float* s = &sh_half[3 * sh];
     const int g = sh_geo[sh];
     if (g == GEO_BOX) return box_grad(p, s);
-    if (g == GEO_PLANE) return {R(0), R(0), R(1)};
+    if (g == GEO_PLANE) {
+      if (plane_over(s, p)) return {R(0), R(0), R(1)};
+      const V3<R> d = plane_delta(s, p);
+      const R l = std::sqrt(dot_plain(d, d));
+      if (l > R(0)) return {d.x / l, d.y / l, d.z / l};
+      return {R(0), R(0), R(1)};
+    }
     R cz = p.z, dz = R(1);
     if (g == GEO_CAPSULE) {
       if (p.z > R(s[1])) cz = p.z - R(s[1]);

@@ -2,9 +2,10 @@
 """The liquid's static shape walls beyond boxes, on CPU: the shape table (layout.py:131-249) takes static boxes,
 spheres, capsules along z and planes facing +z, refuses the rest by name, and keeps newton's bounding radii and the
 thinnest wall; the oracle's signed distances and gradients of those shapes equal the vendored Newton functions
-(alloy/_vendor/newton/_src/geometry/kernels.py sdf_box, sdf_sphere, sdf_capsule, sdf_plane and their gradients,
-evaluated from the reference's source into tests/golden/reference_shape_sdf.json by make_golden.py): in float64 within
-5e-8 (the shape table's scales are float32, as the model's are) and in float32 within 2e-6."""
+eval_shape_sdf calls (geometry/kernels.py sdf_box, sdf_sphere, sdf_capsule and their gradients; soft_contacts_sdf.py
+_eval_plane_sdf for planes, a finite one a two-sided sheet), evaluated from the reference's source into
+tests/golden/reference_shape_sdf.json by make_golden.py: in float64 within 5e-8 (the shape table's scales are
+float32, as the model's are) and in float32 within 2e-6."""
 
 from __future__ import annotations
 
