@@ -54,7 +54,7 @@ class ModelDesc(C.Structure):
                 ("radius", C.c_void_p), ("flags", C.c_void_p), ("phase", C.c_void_p), ("world", C.c_void_p),
                 ("gravity", C.c_void_p), ("n_shapes", C.c_int), ("shape_start", C.POINTER(C.c_int32)),
                 ("shape_ids", C.POINTER(C.c_int32)), ("shape_box", C.POINTER(C.c_float)), ("sweep_len", C.c_double),
-                ("shape_geo", C.POINTER(C.c_int32))]
+                ("shape_geo", C.POINTER(C.c_int32)), ("shape_quat", C.POINTER(C.c_float))]
 
 
 class Report(C.Structure):

@@ -902,8 +902,12 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     if (m->shape_geo)  // the walls a world sees (shapes no world lists are never evaluated)
       for (int c = 0; c < total; ++c) {
         const int g = m->shape_geo[m->shape_ids[c]];
-        if (g != GEO_BOX && g != GEO_SPHERE && g != GEO_CAPSULE && g != GEO_PLANE)
-          return fail(ADF_ERR_VALUE, "shape_geo: only boxes (7), spheres (3), capsules (4) and planes (1)");
+        if (g != GEO_BOX && g != GEO_SPHERE && g != GEO_CAPSULE && g != GEO_CYLINDER && g != GEO_PLANE)
+          return fail(ADF_ERR_VALUE, "shape_geo: only boxes (7), spheres (3), capsules (4), cylinders (6), planes (1)");
+      }
+    if (m->shape_quat)
+      for (int k = 0; k < 4 * m->n_shapes; ++k) {
+        if (!std::isfinite(m->shape_quat[k])) return fail(ADF_ERR_VALUE, "shape_quat holds a non-finite value");
       }
   }
   CK(cudaSetDevice(device));
@@ -1010,6 +1014,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   int *sh_start = nullptr, *sh_ids = nullptr;
   float4 *sh_pos = nullptr, *sh_half = nullptr;
   int* sh_geo = nullptr;
+  float4* sh_quat = nullptr;
   if (d.slot_cap > 1) {
     rc |= s->alloc(&d.slot_cnt, n);
     rc |= s->alloc(&sh_start, (size_t)W + 1);
@@ -1017,6 +1022,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     rc |= s->alloc(&sh_pos, (size_t)m->n_shapes);
     rc |= s->alloc(&sh_half, (size_t)m->n_shapes);
     rc |= s->alloc(&sh_geo, (size_t)m->n_shapes);
+    rc |= s->alloc(&sh_quat, (size_t)m->n_shapes);
   }
   rc |= s->alloc(&d.swept, W);
   d.skin_on = p.skin > 0.0;
@@ -1130,6 +1136,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   d.sh_pos = sh_pos;
   d.sh_half = sh_half;
   d.sh_geo = sh_geo;
+  d.sh_quat = sh_quat;
   d.chunk_begin = chunk_begin;
   d.chunk_end = chunk_end;
   d.world_chunk_start = world_chunk_start;
@@ -1178,6 +1185,13 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
     std::vector<int> geo(m->n_shapes, GEO_BOX);
     if (m->shape_geo) std::copy(m->shape_geo, m->shape_geo + m->n_shapes, geo.begin());
     CKC(cudaMemcpy(sh_geo, geo.data(), sizeof(int) * geo.size(), cudaMemcpyHostToDevice));
+    std::vector<float4> quat(m->n_shapes, make_float4(0.0f, 0.0f, 0.0f, 1.0f));
+    if (m->shape_quat)
+      for (int k = 0; k < m->n_shapes; ++k) {
+        const float* r = m->shape_quat + 4 * (size_t)k;
+        quat[k] = make_float4(r[0], r[1], r[2], r[3]);
+      }
+    CKC(cudaMemcpy(sh_quat, quat.data(), sizeof(float4) * quat.size(), cudaMemcpyHostToDevice));
   }
   {  // the port's reservoir: each world's build-time held particles, popped in ascending id order (ports.py:124-133)
     std::vector<int8_t> ph(s->n);

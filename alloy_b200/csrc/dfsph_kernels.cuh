@@ -129,7 +129,9 @@ struct DevP {
   const float4* sh_pos;   // centre (3), bounding radius
   const float4* sh_half;  // the shape's scale (3: box half extents; sphere radius; capsule radius, half height; plane
                           // width, length, 0 for an infinite plane), Coulomb friction mu
-  const int* sh_geo;      // newton GeoType per shape (GEO_BOX, GEO_SPHERE, GEO_CAPSULE, GEO_PLANE)
+  const int* sh_geo;      // newton GeoType per shape (GEO_BOX, GEO_SPHERE, GEO_CAPSULE, GEO_CYLINDER, GEO_PLANE)
+  const float4* sh_quat;  // the shape frame's rotation (x, y, z, w); slots hold world normals and world-oriented
+                          // offsets of their closest points from the shape's origin
   float sweep_len;        // a step longer than this is swept against the world's boxes (integrate.py:42-49)
   float prad;             // particle radius
   int wall_friction;      // Config.wall_friction
@@ -1146,7 +1148,39 @@ __device__ __forceinline__ void box_normal(float x, float y, float z, const floa
 }
 
 // newton GeoType ids of the static shapes this path evaluates (geometry/types.py:73-118)
-constexpr int GEO_PLANE = 1, GEO_SPHERE = 3, GEO_CAPSULE = 4, GEO_BOX = 7;
+constexpr int GEO_PLANE = 1, GEO_SPHERE = 3, GEO_CAPSULE = 4, GEO_CYLINDER = 6, GEO_BOX = 7;
+
+// A shape's frame: its quaternion q (x, y, z, w); the identity leaves points and directions as they are (the frames of
+// unrotated shapes are their translations only, and their arithmetic is exactly the translation's).
+__device__ __forceinline__ bool rotated(const float4& q) {
+  return !(q.x == 0.0f && q.y == 0.0f && q.z == 0.0f && q.w == 1.0f);
+}
+__device__ __forceinline__ void to_frame(const float4& q, float& x, float& y, float& z) {  // world direction -> shape
+  if (!rotated(q)) return;
+  const float c[4] = {-q.x, -q.y, -q.z, q.w};
+  float ox, oy, oz;
+  quat_rotate(c, x, y, z, ox, oy, oz);
+  x = ox;
+  y = oy;
+  z = oz;
+}
+__device__ __forceinline__ void from_frame(const float4& q, float& x, float& y, float& z) {  // shape direction -> world
+  if (!rotated(q)) return;
+  const float c[4] = {q.x, q.y, q.z, q.w};
+  float ox, oy, oz;
+  quat_rotate(c, x, y, z, ox, oy, oz);
+  x = ox;
+  y = oy;
+  z = oz;
+}
+
+// newton geometry/kernels.py:515-546 (sdf_cylinder, straight sides, along z): the radial and axial excesses
+__device__ __forceinline__ void cylinder_parts(const float4& s, float x, float y, float z, float& rho, float& dx,
+                                               float& dy) {
+  rho = __fsqrt_rn(dot_plain(x, y, 0.0f, x, y, 0.0f));
+  dx = rho - s.x;
+  dy = fabsf(z) - s.y;
+}
 
 // The signed distance of shape `geo` (scale s.xyz) at shape-frame point (x, y, z), as newton's eval_shape_sdf evaluates
 // the analytic shapes (soft_contacts_sdf.py:249-280, geometry/kernels.py): a box (sdf_box :310-333), a sphere
@@ -1168,6 +1202,12 @@ __device__ __forceinline__ void plane_delta(const float4& s, float x, float y, f
 
 __device__ __forceinline__ float shape_phi(int geo, const float4& s, float x, float y, float z) {
   if (geo == GEO_BOX) return box_sdf(x, y, z, s);
+  if (geo == GEO_CYLINDER) {
+    float rho, dx, dy;
+    cylinder_parts(s, x, y, z, rho, dx, dy);
+    const float ex = maxr(dx, 0.0f), ey = maxr(dy, 0.0f);
+    return minr(maxr(dx, dy), 0.0f) + __fsqrt_rn(ex * ex + ey * ey);
+  }
   if (geo == GEO_PLANE) {
     if (plane_over(s, x, y, z)) return z;
     float dx, dy, dz;
@@ -1186,6 +1226,40 @@ __device__ __forceinline__ void shape_normal(int geo, const float4& s, float x, 
                                              float& nz) {
   if (geo == GEO_BOX) {
     box_normal(x, y, z, s, nx, ny, nz);
+    return;
+  }
+  if (geo == GEO_CYLINDER) {  // newton geometry/kernels.py:549-600 (sdf_cylinder_grad, straight sides)
+    float rho, dx, dy;
+    cylinder_parts(s, x, y, z, rho, dx, dy);
+    float rx = 0.0f, ry = 0.0f, rz = 1.0f;
+    if (rho > 1.0e-8f) {
+      rx = x / rho;
+      ry = y / rho;
+      rz = 0.0f;
+    }
+    const float az = z < 0.0f ? -1.0f : 1.0f;
+    if (dx > 0.0f && dy > 0.0f) {
+      const float gx = rx * dx, gy = ry * dx, gz = ADF_FMA(az, dy, rz * dx);
+      const float gl = __fsqrt_rn(dot_plain(gx, gy, gz, gx, gy, gz));
+      if (gl > 1.0e-8f) {
+        nx = gx / gl;
+        ny = gy / gl;
+        nz = gz / gl;
+      } else {
+        nx = rx;
+        ny = ry;
+        nz = rz;
+      }
+    } else if (dx > dy) {
+      nx = rx;
+      ny = ry;
+      nz = rz;
+    } else {
+      nx = 0.0f;
+      ny = 0.0f;
+      nz = az;
+    }
+    normalized3(nx, ny, nz);
     return;
   }
   if (geo == GEO_PLANE) {
@@ -1297,11 +1371,12 @@ __device__ __forceinline__ int shape_insert(int (&shp)[4], float (&ph)[4], float
   return 1;
 }
 
-// boundary.py:190-238 (find), 254-334 (fill) and 336-396 (combine), after k_wall_slots, when the model has box walls:
-// every liquid particle's slots from its world's boxes within reach (in the world's shape order) and the particle
-// wall's slot k_wall_slots left in slot 0, nearest first; each box's slot filled from its SDF (the box-frame
-// start-of-step plane kept for the projection), then overlapping walls combined by inclusion-exclusion (Psi as
-// filled, gradients as rewritten slot by slot). Empty slots are zero with wall id -1.
+// boundary.py:190-238 (find), 254-334 (fill) and 336-396 (combine), after k_wall_slots, when the model has shape
+// walls: every liquid particle's slots from its world's shapes within reach (in the world's shape order, each
+// evaluated in its own frame) and the particle wall's slot k_wall_slots left in slot 0, nearest first; each shape's
+// slot filled from its SDF (the start-of-step closest point and normal kept, world-oriented, for the projection),
+// then overlapping walls combined by inclusion-exclusion (Psi as filled, gradients as rewritten slot by slot). Empty
+// slots are zero with wall id -1.
 __global__ void __launch_bounds__(BLOCK) k_shape_slots(DevP P) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nfw[0]) return;
@@ -1318,13 +1393,15 @@ __global__ void __launch_bounds__(BLOCK) k_shape_slots(DevP P) {
     const int sh = P.sh_ids[c];
     const float4 cp = P.sh_pos[sh];
     const int geo = P.sh_geo[sh];
-    const float lx = xi.x - cp.x, ly = xi.y - cp.y, lz = xi.z - cp.z;
+    float lx = xi.x - cp.x, ly = xi.y - cp.y, lz = xi.z - cp.z;
     if (geo != GEO_PLANE && __fsqrt_rn(dot_plain(lx, ly, lz, lx, ly, lz)) > cp.w + h) continue;
-    const float4 hx = P.sh_half[sh];
+    const float4 hx = P.sh_half[sh], q = P.sh_quat[sh];
+    to_frame(q, lx, ly, lz);
     const float phi = shape_phi(geo, hx, lx, ly, lz);
     if (phi < P.reach && phi + P.wall_offset < h) {
       float nx, ny, nz;
       shape_normal(geo, hx, lx, ly, lz, nx, ny, nz);
+      from_frame(q, nx, ny, nz);
       if (shape_insert(shp, ph, nr, ns, sh, phi, make_float3(nx, ny, nz), near) > 0 && ns < 4) ++ns;
     }
   }
@@ -1344,15 +1421,20 @@ __global__ void __launch_bounds__(BLOCK) k_shape_slots(DevP P) {
     } else {
       const float4 cp = P.sh_pos[sh], hx = P.sh_half[sh];
       const int geo = P.sh_geo[sh];
-      const float lx = xi.x - cp.x, ly = xi.y - cp.y, lz = xi.z - cp.z;
+      const float4 q = P.sh_quat[sh];
+      float lx = xi.x - cp.x, ly = xi.y - cp.y, lz = xi.z - cp.z;
+      to_frame(q, lx, ly, lz);
       const float phi = shape_phi(geo, hx, lx, ly, lz);
       float nx, ny, nz, psi, dpsi;
       shape_normal(geo, hx, lx, ly, lz, nx, ny, nz);
+      float bx = ADF_FMA(-phi, nx, lx), by = ADF_FMA(-phi, ny, ly), bz = ADF_FMA(-phi, nz, lz);
+      from_frame(q, bx, by, bz);
+      from_frame(q, nx, ny, nz);
       wall_volume(P, phi, psi, dpsi);
       sg[k] = make_float4(dpsi * nx, dpsi * ny, dpsi * nz, psi);
       sv[k] = make_float4(0.0f, 0.0f, 0.0f, phi);
       sn[k] = make_float4(nx, ny, nz, __int_as_float(sh));
-      sx[k] = make_float4(ADF_FMA(-phi, nx, lx), ADF_FMA(-phi, ny, ly), ADF_FMA(-phi, nz, lz), 0.0f);
+      sx[k] = make_float4(bx, by, bz, 0.0f);
     }
   }
   if (ns > 1) {
@@ -3021,9 +3103,12 @@ __device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float 
       const int sh = P.sh_ids[c];
       const float4 cp = P.sh_pos[sh];
       const int geo = P.sh_geo[sh];
-      const float ox = x0 - cp.x, oy = y0 - cp.y, oz = z0 - cp.z;
+      float ox = x0 - cp.x, oy = y0 - cp.y, oz = z0 - cp.z;
       if (geo != GEO_PLANE && !(__fsqrt_rn(dot_plain(ox, oy, oz, ox, oy, oz)) <= cp.w + reach)) continue;
-      const float ex = x - cp.x, ey = y - cp.y, ez = z - cp.z;
+      float ex = x - cp.x, ey = y - cp.y, ez = z - cp.z;
+      const float4 q = P.sh_quat[sh];
+      to_frame(q, ox, oy, oz);
+      to_frame(q, ex, ey, ez);
       const float t = shape_entry(geo, P.sh_half[sh], ox, oy, oz, ex, ey, ez, samples);
       if (t < best) {
         best = t;
@@ -3036,9 +3121,12 @@ __device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float 
     if (hit >= 0) {
       const float4 cp = P.sh_pos[hit], hx = P.sh_half[hit];
       const int geo = P.sh_geo[hit];
+      const float4 q = P.sh_quat[hit];
       const float phi = shape_phi(geo, hx, lhx, lhy, lhz);
       float nx, ny, nz;
       shape_normal(geo, hx, lhx, lhy, lhz, nx, ny, nz);
+      from_frame(q, nx, ny, nz);
+      from_frame(q, lhx, lhy, lhz);  // the entry point, world-oriented about the shape's origin
       const float push = maxr(P.eps - phi, 0.0f);
       x = ADF_FMA(push, nx, lhx + cp.x);
       y = ADF_FMA(push, ny, lhy + cp.y);
@@ -3081,11 +3169,14 @@ __device__ __forceinline__ void finish_walls(const DevP& P, int p, int w, float 
       } else if (sh >= 0) {  // a static shape: its SDF at the new place, its start plane when that holds it
         const float4 cp = P.sh_pos[sh], hx = P.sh_half[sh];
         const int geo = P.sh_geo[sh];
-        const float lx = x - cp.x, ly = y - cp.y, lz = z - cp.z;
+        const float4 q = P.sh_quat[sh];
+        float lx = x - cp.x, ly = y - cp.y, lz = z - cp.z;
+        to_frame(q, lx, ly, lz);
         const float phi = shape_phi(geo, hx, lx, ly, lz);
         if (phi < P.eps) {
           float nx, ny, nz;
           shape_normal(geo, hx, lx, ly, lz, nx, ny, nz);
+          from_frame(q, nx, ny, nz);
           float push = P.eps - phi;
           if (vb.w >= 0.0f) {
             const float push_s = P.eps - dotf(nn.x, nn.y, nn.z, x - (xb.x + cp.x), y - (xb.y + cp.y), z - (xb.z + cp.z));

@@ -131,7 +131,7 @@ class DFSPHConfig:
                 raise ValueError(f"SolverDFSPH.Config: {msg}")
 
     def unsupported(self, viscosity_max: float = 1.0e-3) -> list[str]:
-        """Settings this build's CUDA path does not implement (beside the reference's own fallbacks)."""
+        """Settings the B200 CUDA path does not implement (beside the reference's own fallbacks)."""
         out = []
         visc = resolve_viscosity(self, viscosity_max)
         if visc == "weiler2018":

@@ -166,6 +166,13 @@ class ModelBuilder:
         return self._add_shape(GeoType.CAPSULE, (radius, half_height, 0.0), body, xform, mu, collide_particles,
                                sph_boundary)
 
+    def add_shape_cylinder(self, body: int = -1, xform=None, radius: float = 1.0, half_height: float = 0.5,
+                           mu: float = 1.0, collide_particles: bool = True, sph_boundary: int = 0) -> int:
+        """A straight cylinder along the shape's z axis (scale (radius, half_height, 0)), as
+        newton.ModelBuilder.add_shape_cylinder."""
+        return self._add_shape(GeoType.CYLINDER, (radius, half_height, 0.0), body, xform, mu, collide_particles,
+                               sph_boundary)
+
     def add_shape_plane(self, body: int = -1, xform=None, width: float = 0.0, length: float = 0.0, mu: float = 1.0,
                         collide_particles: bool = True, sph_boundary: int = 0) -> int:
         """A plane through the shape's origin with normal along its z axis, finite (width along x, length along y) when

@@ -4,9 +4,9 @@ layout.py:131-164 radius and thinnest wall, layout.py:207-246 ``shape_table``).
 
 A shape bounds the liquid when it collides with particles (``ShapeFlags.COLLIDE_PARTICLES``), has a signed distance
 field, and its ``sph:shape_boundary`` is not ``ignore``; each world sees its own shapes, then the global ones
-(world -1). This path evaluates static shapes (no body) with closed-form distances: axis-aligned boxes (the walls of
-``add_box_tank``), spheres, capsules along z and planes with normal +z (a ground plane); the constructor refuses other
-particle-colliding shapes with a message naming them.
+(world -1). This path evaluates static shapes (no body) with closed-form distances, each in its own frame: boxes (the
+walls of ``add_box_tank``), spheres, capsules and straight cylinders along their z axis, and planes with normal along
+their z axis (a ground plane); the constructor refuses other particle-colliding shapes with a message naming them.
 """
 
 from __future__ import annotations
@@ -27,7 +27,7 @@ class ShapeTable:
     start: np.ndarray   # int32 [W + 1]: world w's shapes are ids[start[w]:start[w + 1]]
     ids: np.ndarray     # int32: shape ids, each world's own then the global ones
     geo: np.ndarray     # int32 [S]
-    scale: np.ndarray   # float32 [S][3]: box half extents; sphere radius; capsule radius, half height; plane width, length
+    scale: np.ndarray   # float32 [S][3]: box half extents; sphere radius; capsule/cylinder radius, half height; plane w, l
     xform: np.ndarray   # float32 [S][7]: (p, q xyzw)
     radius: np.ndarray  # float32 [S]: bounding radius about the shape origin (newton geometry/utils.py:77-110)
     mu: np.ndarray      # float32 [S]: Coulomb friction of the wall
@@ -38,8 +38,9 @@ class ShapeTable:
         return int(len(self.geo))
 
 
-PATH_GEOS = (int(GeoType.BOX), int(GeoType.SPHERE), int(GeoType.CAPSULE), int(GeoType.PLANE))
-THIN_AXES = {int(GeoType.BOX): (0, 1, 2), int(GeoType.SPHERE): (0,), int(GeoType.CAPSULE): (0,)}
+PATH_GEOS = (int(GeoType.BOX), int(GeoType.SPHERE), int(GeoType.CAPSULE), int(GeoType.CYLINDER), int(GeoType.PLANE))
+THIN_AXES = {int(GeoType.BOX): (0, 1, 2), int(GeoType.SPHERE): (0,), int(GeoType.CAPSULE): (0,),
+             int(GeoType.CYLINDER): (0, 1)}
 
 
 def shape_radius(geo: int, scale) -> float:
@@ -48,7 +49,7 @@ def shape_radius(geo: int, scale) -> float:
     s = np.abs(np.asarray(scale, np.float64))
     if geo == int(GeoType.SPHERE):
         return float(s[0])
-    if geo == int(GeoType.CAPSULE):
+    if geo in (int(GeoType.CAPSULE), int(GeoType.CYLINDER)):
         return float(s[0] + s[1])
     if geo == int(GeoType.PLANE):
         return float(np.linalg.norm(s)) * 0.5 if s[0] > 0.0 and s[1] > 0.0 else 1.0e6
@@ -77,19 +78,20 @@ def shape_table(model) -> ShapeTable:
     usable = ((flags & int(ShapeFlags.COLLIDE_PARTICLES)) != 0) & np.isin(geo, [int(g) for g in SDF_GEOS])
     usable &= boundary != BOUNDARY_IGNORE
     bad = []
-    identity = np.array([0.0, 0.0, 0.0, 1.0], np.float32)
     for s in np.flatnonzero(usable):
         name = GeoType(int(geo[s])).name.lower()
         if int(geo[s]) not in PATH_GEOS:
             bad.append(f"shape {s} ({name})")
         elif body[s] >= 0:
             bad.append(f"shape {s} (a {name} on body {body[s]})")
-        elif int(geo[s]) != int(GeoType.SPHERE) and not np.array_equal(xform[s, 3:], identity):
-            bad.append(f"shape {s} (a rotated {name})")
+        elif int(geo[s]) == int(GeoType.CYLINDER) and scale[s, 2] != 0.0:
+            bad.append(f"shape {s} (a barrel cylinder)")
+        elif abs(float(np.linalg.norm(xform[s, 3:].astype(np.float64))) - 1.0) > 1.0e-4:
+            bad.append(f"shape {s} (a {name} whose rotation is not a unit quaternion)")
     if bad:
-        raise ValueError("SolverDFSPH (B200 build): the liquid's shape walls must be static boxes, spheres, capsules "
-                         "along z or planes facing +z (add_box_tank, wall_box, add_shape_sphere, add_shape_capsule, "
-                         "add_ground_plane), unrotated; not on this build's CUDA path: " + ", ".join(bad[:8]))
+        raise ValueError("SolverDFSPH (B200 build): the liquid's shape walls must be static boxes, spheres, capsules, "
+                         "straight cylinders or planes (add_box_tank, wall_box, add_shape_sphere, add_shape_capsule, "
+                         "add_shape_cylinder, add_ground_plane); not on the B200 CUDA path: " + ", ".join(bad[:8]))
     glob = np.flatnonzero(usable & (world < 0))
     start, ids = [0], []
     for w in range(W):

@@ -10,7 +10,7 @@ fallback: without a CUDA device or the library it raises.
 
 Scope of the CUDA path: cubic or Wendland kernel, projected preconditioned CG (the reference's default, krylov.py)
 or relaxed Jacobi pressure solves, XSPH, particle walls (boundary particles flagged PROXY), static shape walls
-(axis-aligned boxes, spheres, capsules along z, planes facing +z) evaluated through their SDF (up to four wall slots
+(boxes, spheres, capsules, straight cylinders and planes, each in its own frame) evaluated through their SDF (up to four wall slots
 per particle, projection and the sweep past fast steps, wall friction), emitters, sinks and the escape box.
 Settings outside it are refused in the constructor (``DFSPHConfig.unsupported``); CG falls back to Jacobi with a
 warning when particle masses or rest densities differ, as the reference does (solver.py:89-91). The resting-jitter
@@ -168,7 +168,7 @@ class SolverDFSPH:
         self.config = cfg = config or DFSPHConfig()
         cfg.validate()
         if soft_particles is not None:
-            raise ValueError("SolverDFSPH: soft walls (VBD faces) are not part of this build's CUDA path")
+            raise ValueError("SolverDFSPH: soft walls (VBD faces) are not part of the B200 CUDA path")
         self._lib = _lib.lib()
         n = int(model.particle_count)
         W = int(model.world_count)
@@ -249,6 +249,8 @@ class SolverDFSPH:
         md.shape_box = box.ctypes.data_as(C.POINTER(C.c_float))
         geo = np.ascontiguousarray(tab.geo if tab.count else np.full(1, 7), np.int32)
         md.shape_geo = geo.ctypes.data_as(C.POINTER(C.c_int32))
+        quat = np.ascontiguousarray(tab.xform[:, 3:7] if tab.count else np.array([[0.0, 0.0, 0.0, 1.0]]), np.float32)
+        md.shape_quat = quat.ctypes.data_as(C.POINTER(C.c_float))
         md.sweep_len = min(0.5 * cfg.h, 0.5 * tab.thinnest)  # integrate.py:42-49
         handle = C.c_void_p()
         with torch.cuda.device(self.device):
@@ -711,7 +713,7 @@ class SolverDFSPH:
         """This path has no proxy bodies (coupling_hooks.py:74-86 integrates them): only an empty mapping is valid."""
         del out_body_f, kwargs
         if len(body_local_to_proxy_global):
-            raise ValueError("SolverDFSPH (B200 build): proxy bodies are not part of this build's CUDA path")
+            raise ValueError("SolverDFSPH (B200 build): proxy bodies are not part of the B200 CUDA path")
 
     def coupling_rewind_proxy_particle(self, particle_local_to_proxy_global, state, coupling_forces,
                                        particle_gravity_acceleration, dt: float) -> None:
@@ -731,7 +733,7 @@ class SolverDFSPH:
         if not dt > 0.0:
             raise ValueError("SolverDFSPH harvest requires dt > 0")
         raise ValueError("SolverDFSPH (B200 build): two-way particle walls (reaction forces on proxies) are not part "
-                         "of this build's CUDA path")
+                         "of the B200 CUDA path")
 
     # ------------------------------------------------------------------------------------------------ emitters
     def _spares(self, w: int) -> np.ndarray:

@@ -10,7 +10,8 @@
   world or many, primed before stepping; ``tank_dam_break`` is the same harness's 30k-particle dam break.
 - ``pour_bowls``: thousands of worlds, each a hemisphere bowl of boundary particles moving on a seeded sinusoid
   (``BowlMotion`` drives the wall velocities between steps) with liquid resting in it and a spout pouring in.
-- ``tank_impacts``, ``shape_obstacles``: parity scenes for walls hit hard (box tanks; spheres, capsules and planes).
+- ``tank_impacts``, ``shape_obstacles``: parity scenes for walls hit hard (box tanks; spheres, capsules, cylinders,
+  planes and turned boxes).
 Config: cubic kernel, h = 4r = 2 spacings, rho0 1000, XSPH 0.01, Jacobi, tolerances 1e-3, resting-jitter rule off.
 """
 
@@ -85,23 +86,28 @@ def tank_impacts(spacing: float = 0.02, dt: float = 1.0e-3, steps: int = 10, dev
 
 
 def shape_obstacles(spacing: float = 0.02, dt: float = 1.0e-3, steps: int = 20, device="cpu", **cfg_kw) -> Scene:
-    """Static shapes other than boxes (a parity scene for their slots, sweep and projection): a 6 x 6 x 5 jittered
-    block falling at 0.5 m/s onto a sphere (r 0.05 m) and a capsule along z (r 0.025 m, half height 0.04 m) standing on
-    the infinite ground plane z = 0, beside a finite plane (a 0.08 m square shelf), inside side walls of box shapes h
-    thick with no floor; four lone particles at 30 m/s, past the CFL step, towards the sphere, the capsule's cap, the
-    ground and the capsule's side (swept)."""
+    """Static shapes other than axis-aligned boxes (a parity scene for their slots, sweep and projection): a 6 x 6 x 5
+    jittered block falling at 0.5 m/s onto a sphere (r 0.05 m) and a capsule along z (r 0.025 m, half height 0.04 m)
+    standing on the infinite ground plane z = 0, beside a finite plane (a 0.08 m square shelf), a box turned 45 degrees
+    about z and a cylinder lying along y, inside side walls of box shapes h thick with no floor; six lone particles at
+    30 m/s, past the CFL step, towards the sphere, the capsule's cap and side, the ground, the cylinder and the turned
+    box (swept)."""
     cfg = benchmark_config(spacing, **cfg_kw)
     b = ModelBuilder(gravity=(0.0, 0.0, -9.81))
     b.begin_world()
     fl = add_fluid_block(b, cfg, (0.06, 0.06, 0.16), (6, 6, 5), jitter=0.01, seed=4, velocity=(0.0, 0.0, -0.5))
     lone = [((0.15, 0.15, 0.20), (0.0, 0.0, -30.0)), ((0.07, 0.22, 0.17), (0.5, 0.0, -30.0)),
-            ((0.25, 0.25, 0.02), (1.0, 0.0, -30.0)), ((0.12, 0.22, 0.08), (-30.0, 0.5, 0.0))]
+            ((0.25, 0.25, 0.02), (1.0, 0.0, -30.0)), ((0.12, 0.22, 0.08), (-30.0, 0.5, 0.0)),
+            ((0.06, 0.08, 0.09), (0.0, 0.3, -30.0)), ((0.24, 0.22, 0.15), (0.2, 0.0, -30.0))]
     for x, v in lone:
         add_fluid_points(b, cfg, np.asarray([x]), velocity=v)
     add_box_tank(b, (0.0, 0.0, 0.0), (0.3, 0.3, 0.4), wall=cfg.h, open_top=True, floor=False)
     b.add_shape_sphere(-1, (0.15, 0.15, 0.08), radius=0.05, mu=0.4)
     b.add_shape_capsule(-1, (0.07, 0.22, 0.08), radius=0.025, half_height=0.04, mu=0.6)
     b.add_shape_plane(-1, (0.23, 0.07, 0.12), width=0.08, length=0.08, mu=0.3)
+    b.add_shape_box(-1, (0.24, 0.22, 0.05, 0.0, 0.0, 0.38268343, 0.9238795), 0.03, 0.015, 0.05, mu=0.2)
+    b.add_shape_cylinder(-1, (0.06, 0.08, 0.03, 0.70710677, 0.0, 0.0, 0.70710677), radius=0.02, half_height=0.05,
+                         mu=0.5)
     b.end_world()
     b.add_ground_plane(0.0, mu=0.5)
     return Scene(b.finalize(device), cfg, dt, steps, len(fl) + len(lone), 0, name="shape_obstacles")

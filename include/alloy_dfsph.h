@@ -85,18 +85,19 @@ typedef struct {
   const int32_t* world;          /* device [n] particle_world */
   const float* gravity;          /* device [W][3] Model.gravity */
   /* The liquid's static shape walls (layout.py:207-246 shape_table; boundary.py:70-87 per world: the world's own
-   * shapes, then the global ones): axis-aligned boxes, spheres, capsules along z, planes with normal +z. n_shapes = 0:
-   * particle walls only, and the rest may be NULL. */
+   * shapes, then the global ones): boxes, spheres, capsules, straight cylinders and planes, each in its own frame.
+   * n_shapes = 0: particle walls only, and the rest may be NULL. */
   int n_shapes;                  /* S: size of the model's shape table (ids index it; the particle wall's id is S) */
   const int32_t* shape_start;    /* host [W + 1]: world w's walls are shape_ids[shape_start[w] .. shape_start[w + 1]) */
   const int32_t* shape_ids;      /* host [shape_start[W]] */
   const float* shape_box;        /* host [S][8]: centre xyz, bounding radius, scale xyz (box half extents; sphere
-                                    radius; capsule radius, half height; plane width, length, 0 for an infinite
-                                    plane), Coulomb friction */
+                                    radius; capsule and cylinder radius, half height; plane width, length, 0 for an
+                                    infinite plane), Coulomb friction */
   double sweep_len;              /* [m] a step longer than this is swept against the shapes: min(h, thinnest) / 2
                                     (integrate.py:42-49) */
-  const int32_t* shape_geo;      /* host [S]: newton GeoType per shape (7 box, 3 sphere, 4 capsule, 1 plane); NULL: all
-                                    boxes */
+  const int32_t* shape_geo;      /* host [S]: newton GeoType per shape (7 box, 3 sphere, 4 capsule and 6 cylinder along
+                                    their z axis, 1 plane with normal z); NULL: all boxes */
+  const float* shape_quat;       /* host [S][4]: the shape frame's rotation (x, y, z, w; unit); NULL: unrotated */
 } adf_model;
 
 /* Per-world host outputs of adf_get_report; any pointer may be NULL. SPHReport (types.py:11-28) and

@@ -266,7 +266,8 @@ template <class R> struct Solver {
   int S = 0;
   std::vector<int> sh_start, sh_ids;
   std::vector<float> sh_pos, sh_half, sh_radius, sh_mu;
-  std::vector<int> sh_geo;  // newton GeoType per shape (box, sphere, capsule along z, plane facing +z)
+  std::vector<int> sh_geo;  // newton GeoType per shape (box, sphere, capsule and cylinder along z, plane facing +z)
+  std::vector<float> sh_quat;  // [S][4] the shape frame's rotation (x, y, z, w)
   double sweep_len = 1.0e30;
   std::vector<int> swept;
   std::vector<R> ratio, alpha, neff, active, reg, src, kappa, lower, err;
@@ -470,7 +471,41 @@ template <class R> struct Solver {
   // shape sh at shape-local p (box sdf_box; sphere sdf_sphere; capsule along z sdf_capsule; plane facing +z
   // _eval_plane_sdf) and its outward unit gradient (sdf_*_grad; +z at a sphere's centre or a capsule's
   // axis, -z below its lower cap; +z for a plane)
-  static constexpr int GEO_PLANE = 1, GEO_SPHERE = 3, GEO_CAPSULE = 4, GEO_BOX = 7;
+  static constexpr int GEO_PLANE = 1, GEO_SPHERE = 3, GEO_CAPSULE = 4, GEO_CYLINDER = 6, GEO_BOX = 7;
+  // the shape's frame: identity rotations leave vectors as they are (an unrotated frame is a translation only)
+  bool rotated(int sh) const {
+    const float* q = &sh_quat[4 * sh];
+    return !(q[0] == 0.0f && q[1] == 0.0f && q[2] == 0.0f && q[3] == 1.0f);
+  }
+  V3<R> to_frame(int sh, const V3<R>& v) const {
+    if (!rotated(sh)) return v;
+    const float* q = &sh_quat[4 * sh];
+    const float c[4] = {-q[0], -q[1], -q[2], q[3]};
+    return quat_rotate(c, v);
+  }
+  V3<R> from_frame(int sh, const V3<R>& v) const { return rotated(sh) ? quat_rotate(&sh_quat[4 * sh], v) : v; }
+  // geometry/kernels.py:515-600 (sdf_cylinder, sdf_cylinder_grad; straight sides along z)
+  R cylinder_phi(const float* s, const V3<R>& p) const {
+    const V3<R> v{p.x, p.y, R(0)};
+    const R rho = std::sqrt(dot_plain(v, v)), dx = rho - R(s[0]), dy = std::fabs(p.z) - R(s[1]);
+    const R ex = maxr(dx, R(0)), ey = maxr(dy, R(0));
+    return minr(maxr(dx, dy), R(0)) + std::sqrt(ex * ex + ey * ey);
+  }
+  V3<R> cylinder_grad(const float* s, const V3<R>& p) const {
+    const V3<R> v{p.x, p.y, R(0)};
+    const R rho = std::sqrt(dot_plain(v, v)), dx = rho - R(s[0]), dy = std::fabs(p.z) - R(s[1]);
+    V3<R> rad{R(0), R(0), R(1)};
+    if (rho > R(1.0e-8)) rad = {p.x / rho, p.y / rho, R(0)};
+    const R az = p.z < R(0) ? R(-1) : R(1);
+    if (dx > R(0) && dy > R(0)) {
+      const V3<R> g{rad.x * dx, rad.y * dx, fma_(az, dy, rad.z * dx)};
+      const R gl = std::sqrt(dot_plain(g, g));
+      if (gl > R(1.0e-8)) return {g.x / gl, g.y / gl, g.z / gl};
+      return rad;
+    }
+    if (dx > dy) return rad;
+    return {R(0), R(0), az};
+  }
   // soft_contacts_sdf.py:73-102 (_eval_plane_sdf, depth 0): infinite unless width and length are both positive; a
   // finite plane is a two-sided sheet, its z over the footprint from above, else the distance to its nearest point
   static bool plane_over(const float* s, const V3<R>& p) {
@@ -485,6 +520,7 @@ template <class R> struct Solver {
     const float* s = &sh_half[3 * sh];
     const int g = sh_geo[sh];
     if (g == GEO_BOX) return box_sdf(p, s);
+    if (g == GEO_CYLINDER) return cylinder_phi(s, p);
     if (g == GEO_PLANE) {
       if (plane_over(s, p)) return p.z;
       const V3<R> d = plane_delta(s, p);
@@ -499,6 +535,7 @@ template <class R> struct Solver {
     const float* s = &sh_half[3 * sh];
     const int g = sh_geo[sh];
     if (g == GEO_BOX) return box_grad(p, s);
+    if (g == GEO_CYLINDER) return cylinder_grad(s, p);
     if (g == GEO_PLANE) {
       if (plane_over(s, p)) return {R(0), R(0), R(1)};
       const V3<R> d = plane_delta(s, p);
@@ -517,10 +554,10 @@ template <class R> struct Solver {
     if (l > R(1.0e-8)) return {v.x / l, v.y / l, v.z / l};
     return {R(0), R(0), dz};
   }
-  V3<R> shape_local(int sh, const V3<R>& x) const {  // static unrotated shape: the frame is its origin
-    return {x.x - R(sh_pos[3 * sh]), x.y - R(sh_pos[3 * sh + 1]), x.z - R(sh_pos[3 * sh + 2])};
+  V3<R> shape_local(int sh, const V3<R>& x) const {  // static shape: its frame's origin and rotation
+    return to_frame(sh, {x.x - R(sh_pos[3 * sh]), x.y - R(sh_pos[3 * sh + 1]), x.z - R(sh_pos[3 * sh + 2])});
   }
-  V3<R> shape_world(int sh, const V3<R>& l) const {
+  V3<R> shape_world(int sh, const V3<R>& l) const {  // a world-oriented offset from the shape's origin to the point
     return {l.x + R(sh_pos[3 * sh]), l.y + R(sh_pos[3 * sh + 1]), l.z + R(sh_pos[3 * sh + 2])};
   }
 
@@ -626,7 +663,7 @@ template <class R> struct Solver {
           const V3<R> xl = shape_local(sh, x);
           const R phi = shape_phi(sh, xl);
           if (phi < reach && phi + offset < kc.h) {
-            const V3<R> nw = normalized(shape_grad(sh, xl));
+            const V3<R> nw = from_frame(sh, normalized(shape_grad(sh, xl)));
             if (shape_insert(i, ns, sh, phi, nw, nr, near) > 0 && ns < NS) ++ns;
           }
         }
@@ -688,8 +725,9 @@ template <class R> struct Solver {
             phi = shape_phi(sh, xl);
             const V3<R> gl = shape_grad(sh, xl);
             nrm = normalized(gl);
+            s_xbl[o] = from_frame(sh, V3<R>{fma_(-phi, nrm.x, xl.x), fma_(-phi, nrm.y, xl.y), fma_(-phi, nrm.z, xl.z)});
+            nrm = from_frame(sh, nrm);  // slots hold world normals and world-oriented closest points
             s_nbl[o] = nrm;
-            s_xbl[o] = {fma_(-phi, nrm.x, xl.x), fma_(-phi, nrm.y, xl.y), fma_(-phi, nrm.z, xl.z)};
             s_vb[o] = {R(0), R(0), R(0)};
           }
           wall_volume(phi, psi, dpsi);
@@ -1328,8 +1366,8 @@ template <class R> struct Solver {
         }
         if (hit >= 0) {
           const R phi = shape_phi(hit, lh);
-          const V3<R> nn = normalized(shape_grad(hit, lh));
-          const V3<R> xw = shape_world(hit, lh);
+          const V3<R> nn = from_frame(hit, normalized(shape_grad(hit, lh)));
+          const V3<R> xw = shape_world(hit, from_frame(hit, lh));
           const R push = maxr(eps - phi, R(0));
           x = {fma_(push, nn.x, xw.x), fma_(push, nn.y, xw.y), fma_(push, nn.z, xw.z)};
           const R vn = dotf(vv, nn);
@@ -1362,7 +1400,7 @@ template <class R> struct Solver {
             const V3<R> xl = shape_local(sh, x);
             const R phi = shape_phi(sh, xl);
             if (phi < eps) {
-              V3<R> nn = normalized(shape_grad(sh, xl));
+              V3<R> nn = from_frame(sh, normalized(shape_grad(sh, xl)));
               R push = eps - phi;
               if (s_phi[o] >= R(0)) {
                 const V3<R> ns = s_nbl[o];
@@ -1701,11 +1739,14 @@ void orc_get_slot_shapes(void* hp, int* out) {
 // box's centre pos[S][3], half extents half[S][3], bounding radius[S] and friction mu[S]; sweep length
 // min(h / 2, thinnest / 2) (integrate.py:42-49).
 void orc_set_shapes(void* hp, int S, const int* start, const int* ids, const float* pos, const float* half,
-                    const float* radius, const float* mu, double thinnest, const int* geo) {
+                    const float* radius, const float* mu, double thinnest, const int* geo, const float* quat) {
   DISPATCH({
     s.S = S;
     s.sh_geo.assign(S, 7);
     if (geo) s.sh_geo.assign(geo, geo + S);
+    s.sh_quat.assign(4 * (size_t)S, 0.0f);
+    for (int k = 0; k < S; ++k) s.sh_quat[4 * (size_t)k + 3] = 1.0f;
+    if (quat) s.sh_quat.assign(quat, quat + 4 * (size_t)S);
     s.sh_start.assign(start, start + s.W + 1);
     s.sh_ids.assign(ids, ids + start[s.W]);
     s.sh_pos.assign(pos, pos + 3 * S);

@@ -102,7 +102,7 @@ def lib():
         L.orc_get_field.argtypes = [P, C.c_char_p, fp]
         L.orc_get_slot_on.argtypes = [P, ip]
         L.orc_get_slot_shapes.argtypes = [P, ip]
-        L.orc_set_shapes.argtypes = [P, C.c_int, ip, ip, fp, fp, fp, fp, C.c_double, ip]
+        L.orc_set_shapes.argtypes = [P, C.c_int, ip, ip, fp, fp, fp, fp, C.c_double, ip, fp]
         L.orc_shape_sdf.argtypes = [P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_get_lists.argtypes = [P, ip, ip]
         L.orc_get_report.argtypes = [P, ip, fp, C.POINTER(C.c_int64)]
@@ -173,11 +173,12 @@ class Oracle:
                                                                                 np.zeros(1, np.int32), np.int32),
                 np.ascontiguousarray(tab.xform[:, :3], np.float32), np.ascontiguousarray(tab.scale, np.float32),
                 np.ascontiguousarray(tab.radius, np.float32), np.ascontiguousarray(tab.mu, np.float32),
-                np.ascontiguousarray(tab.geo if tab.count else np.full(1, 7), np.int32)]
+                np.ascontiguousarray(tab.geo if tab.count else np.full(1, 7), np.int32),
+                np.ascontiguousarray(tab.xform[:, 3:7] if tab.count else np.array([[0.0, 0.0, 0.0, 1.0]]), np.float32)]
         self._shape_keep = keep
         self.L.orc_set_shapes(self.h, tab.count, _p(keep[0], C.c_int), _p(keep[1], C.c_int), _p(keep[2], C.c_float),
                               _p(keep[3], C.c_float), _p(keep[4], C.c_float), _p(keep[5], C.c_float),
-                              float(tab.thinnest), _p(keep[6], C.c_int))
+                              float(tab.thinnest), _p(keep[6], C.c_int), _p(keep[7], C.c_float))
 
     def shape_sdf(self, sh: int, p) -> tuple[float, np.ndarray]:
         """(phi, outward unit gradient) of shape ``sh`` at shape-local point ``p``."""

@@ -11,7 +11,7 @@ rounding. Sources used (paths inside the alloy project):
                                   boundary_fit, lattice_diagonal, _half_lattice
   alloy/solvers/sph/config.py     particle_mass, full_neighbor_count (function bodies extracted with ast)
   alloy/solvers/sph/particle_walls.py  colour_distance, pw_project (function bodies extracted with ast)
-  alloy/_vendor/newton/_src/geometry/kernels.py  sdf_box, sdf_sphere, sdf_capsule and their gradients, and
+  alloy/_vendor/newton/_src/geometry/kernels.py  sdf_box, sdf_sphere, sdf_capsule, sdf_cylinder and gradients, and
   alloy/_vendor/newton/_src/geometry/soft_contacts_sdf.py  _eval_plane_sdf (reference_shape_sdf.json)
 
 Usage: python tests/golden/make_golden.py /path/to/alloy-checkout
@@ -150,7 +150,7 @@ def main(root: Path) -> None:
 def shape_sdf_cases(root: Path) -> None:
     """tests/golden/reference_shape_sdf.json: the vendored Newton signed distances and gradients of the analytic shapes
     the liquid's walls use, as eval_shape_sdf (soft_contacts_sdf.py:249-280) calls them: sdf_box, sdf_sphere,
-    sdf_capsule along z and their _grad functions (geometry/kernels.py), and _eval_plane_sdf with depth 0 for planes
+    sdf_capsule and sdf_cylinder (straight) along z and their _grad functions (geometry/kernels.py), and _eval_plane_sdf with depth 0 for planes
     (soft_contacts_sdf.py:73-102), evaluated in float64 at points inside, on and outside each shape."""
     from enum import IntEnum
 
@@ -164,7 +164,7 @@ def shape_sdf_cases(root: Path) -> None:
     wp.normalize = lambda v: v / np.linalg.norm(v)
     wp.sign = lambda x: -1.0 if x < 0.0 else 1.0
     names = ["_sdf_point_to_z_up", "_sdf_vector_from_z_up", "sdf_sphere", "sdf_sphere_grad", "sdf_box", "sdf_box_grad",
-             "sdf_capsule", "sdf_capsule_grad"]
+             "sdf_capsule", "sdf_capsule_grad", "sdf_cylinder", "sdf_cylinder_grad"]
     geom = root / "alloy" / "_vendor" / "newton" / "_src" / "geometry"
     f = extract(geom / "kernels.py", names, {"wp": wp, "Axis": Axis, "np": np, "math": math})
     f.update(extract(geom / "soft_contacts_sdf.py", ["_eval_plane_sdf"], {"wp": wp, "np": np, "math": math}))
@@ -172,7 +172,8 @@ def shape_sdf_cases(root: Path) -> None:
         fn.__globals__.update(f)
     rng = np.random.default_rng(7)
     shapes = [("box", 7, (0.03, 0.02, 0.05)), ("sphere", 3, (0.04, 0.0, 0.0)), ("capsule", 4, (0.02, 0.05, 0.0)),
-              ("plane", 1, (0.0, 0.0, 0.0)), ("finite_plane", 1, (0.1, 0.06, 0.0))]
+              ("plane", 1, (0.0, 0.0, 0.0)), ("finite_plane", 1, (0.1, 0.06, 0.0)),
+              ("cylinder", 6, (0.03, 0.04, 0.0))]
     out = []
     for name, geo, sc in shapes:
         pts = list(rng.uniform(-0.09, 0.09, size=(40, 3)))
@@ -184,6 +185,9 @@ def shape_sdf_cases(root: Path) -> None:
                 phi, g = f["sdf_box"](pnt, *sc), f["sdf_box_grad"](pnt, *sc)
             elif geo == 3:
                 phi, g = f["sdf_sphere"](pnt, sc[0]), f["sdf_sphere_grad"](pnt, sc[0])
+            elif geo == 6:
+                phi = f["sdf_cylinder"](pnt, sc[0], sc[1], int(Axis.Z), -1.0, sc[2])
+                g = f["sdf_cylinder_grad"](pnt, sc[0], sc[1], int(Axis.Z), -1.0, sc[2])
             elif geo == 4:
                 phi = f["sdf_capsule"](pnt, sc[0], sc[1], int(Axis.Z))
                 g = f["sdf_capsule_grad"](pnt, sc[0], sc[1], int(Axis.Z))

@@ -1,12 +1,13 @@
 # SPDX-License-Identifier: Apache-2.0
-"""Static shapes other than boxes on the CUDA path against the CPU oracle, bit for bit: spheres, capsules along z and
-planes facing +z (finite and infinite) through newton's closed-form distances (boundary.py:190-396 slots,
-integrate.py:98-115 the sampled sweep of non-box shapes, integrate.py:212-309 the projection with friction).
+"""Static shapes other than axis-aligned boxes on the CUDA path against the CPU oracle, bit for bit: spheres, capsules,
+straight cylinders, planes (finite and infinite) and turned boxes, each in its own frame, through newton's
+closed-form distances (boundary.py:190-396 slots, integrate.py:98-115 the sampled sweep of non-box shapes and the slab
+test of boxes in their frame, integrate.py:212-309 the projection with friction).
 
 - the slots of every liquid particle of the obstacle scene after the first build, with the liquid moved onto the
   shapes: count, wall ids in order, Psi, phi, gradient and normal of each slot;
 - 20 steps of the obstacle scene with Jacobi and with CG: a block falling onto a sphere and a capsule on the ground
-  plane beside a finite shelf, and lone particles at 30 m/s swept into the sphere, the capsule and the ground; the
+  plane beside a finite shelf, a turned box and a lying cylinder, and lone particles at 30 m/s swept into them; the
   state, iteration counts, per-world errors and the projection and sweep counters every step.
 """
 
@@ -26,14 +27,18 @@ def test_obstacle_slots_bit_exact(cuda):
     sc = shape_obstacles(device=cuda)
     q = sc.model.particle_q.clone()
     fluid = (sc.model.sph.phase.cpu().numpy() >= 1)
-    # move the block's particles onto the shapes: rings around the sphere and the capsule and a layer on the ground
+    # move the block's particles onto the shapes: rings around the sphere, the capsule, the lying cylinder and the
+    # turned box, and a layer on the ground under the shelf
     idx = np.flatnonzero(fluid)[:180]
     k = np.arange(len(idx))
     ang = 2.0 * np.pi * k / 23.0
     pts = np.stack([0.15 + 0.062 * np.cos(ang), 0.15 + 0.062 * np.sin(ang), 0.03 + 0.01 * (k % 9)], 1)
-    pts[60:120] = np.stack([0.07 + 0.04 * np.cos(ang[60:120]), 0.22 + 0.04 * np.sin(ang[60:120]),
-                            0.02 + 0.012 * (k[60:120] % 13)], 1)
-    pts[120:] = np.stack([0.22 + 0.006 * (k[120:] % 10), 0.04 + 0.006 * (k[120:] // 10 % 6), 0.004 + 0.0 * k[120:]], 1)
+    c, s_ = np.cos(ang), np.sin(ang)
+    pts[36:72] = np.stack([0.07 + 0.04 * c[36:72], 0.22 + 0.04 * s_[36:72], 0.02 + 0.012 * (k[36:72] % 13)], 1)
+    pts[72:108] = np.stack([0.06 + 0.027 * c[72:108], 0.04 + 0.008 * (k[72:108] % 11),
+                            0.03 + 0.027 * np.abs(s_[72:108])], 1)
+    pts[108:144] = np.stack([0.24 + 0.045 * c[108:144], 0.22 + 0.045 * s_[108:144], 0.02 + 0.01 * (k[108:144] % 8)], 1)
+    pts[144:] = np.stack([0.22 + 0.006 * (k[144:] % 10), 0.04 + 0.006 * (k[144:] // 10 % 4), 0.004 + 0.0 * k[144:]], 1)
     q[idx] = torch_tensor(pts, cuda)
     sc.model.particle_q.copy_(q)
     sol = SolverDFSPH(sc.model, sc.config)
@@ -49,7 +54,7 @@ def test_obstacle_slots_bit_exact(cuda):
             np.testing.assert_array_equal(sol.debug_field(f"{name}:{s}")[fluid], orc.field(f"{name}:{s}")[fluid],
                                           err_msg=f"{name}:{s}")
     seen = set(shapes[fluid].ravel().tolist())
-    assert {4, 5, 7} <= seen  # the sphere, the capsule and the ground plane hold slots
+    assert {4, 5, 7, 8, 9} <= seen  # the sphere, the capsule, the turned box, the lying cylinder and the ground
 
 
 def torch_tensor(a, device):
@@ -81,5 +86,5 @@ def test_obstacle_lockstep_with_sweeps(cuda, solver):
         q, qd = orc.state()
         np.testing.assert_array_equal(a.particle_q.cpu().numpy(), q, err_msg=f"q step {k}")
         np.testing.assert_array_equal(a.particle_qd.cpu().numpy(), qd, err_msg=f"qd step {k}")
-    assert swept >= 3 and projected > 0  # the sampled sweeps and the projections both ran
+    assert swept >= 5 and projected > 0  # the sampled sweeps and the projections both ran
     assert (a.particle_q.cpu().numpy()[:, 2] > 0.0).all()  # nothing went through the ground
