@@ -24,11 +24,11 @@ EXPORTS = ("adf_last_error", "adf_create", "adf_destroy", "adf_step", "adf_densi
            "adf_prime", "adf_iteration_work", "adf_set_tuned_config", "adf_get_state_storage", "adf_port_take",
            "adf_port_emit", "adf_energy", "adf_stable_dt", "adf_skin_flags",
            "adf_add_patch_emitter", "adf_trigger", "adf_mlp_set_wait_limit", "adf_mlp_clear_status",
-           "adf_set_persistent", "adf_set_barrier_wait", "adf_clear_status")
+           "adf_set_persistent", "adf_set_barrier_wait", "adf_clear_status", "adf_set_halo", "adf_halo_stats")
 TUNE_KERNELS = ("density_alpha", "solve_init", "accel", "jacobi", "xsph", "lists")  # ADF_TUNE_KERNELS, in order
 MLP_PARAMS, MLP_FEATURES = 5378, 16  # ADF_MLP_PARAMS, ADF_MLP_FEATURES
 PROF_KINDS = ("sort", "lists", "wall_slots", "density_alpha", "solve_init", "accel", "jacobi", "reduce_check",
-              "apply", "xsph", "finish", "emit", "warm_start")
+              "apply", "xsph", "finish", "emit", "warm_start", "halo")
 
 
 class Params(C.Structure):
@@ -133,6 +133,8 @@ def lib() -> C.CDLL:
     L.adf_warm_features.argtypes = [P, vp, vp]
     L.adf_set_warm_judging.argtypes = [P, i]
     L.adf_set_persistent.argtypes = [P, i]
+    L.adf_set_halo.argtypes = [P, i]
+    L.adf_halo_stats.argtypes = [P, vp, vp, vp]
     L.adf_set_barrier_wait.argtypes = [P, C.c_longlong, i]
     L.adf_clear_status.argtypes = [P]
     L.adf_set_autotune.argtypes = [P, i]

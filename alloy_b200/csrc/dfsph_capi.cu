@@ -67,6 +67,7 @@ enum TuneKernel { TK_DENSITY = 0, TK_SOLVE_INIT, TK_ACCEL, TK_JACOBI, TK_XSPH, T
 struct TuneCfg {
   int block = BLOCK;
   int nb = NB_DEFAULT;
+  int halo = 0;  // acceleration and Jacobi: 1 = the item-halo kernels (k_accel_h, k_jacobi_h)
 };
 constexpr int TUNE_BLOCKS[] = {128, 256};
 constexpr int TUNE_NB[] = {4, 8, 16};
@@ -194,6 +195,9 @@ struct adf_solver {
   bool cg_team = false;  // CG products by teams of TL lanes per particle (models of at most CG_TEAM_MAX particles)
   // the persistent CG solve (k_cg_solve) of team-product models, when adf_set_persistent turned it on
   bool persist_on = false;
+  // item halos of the pressure iterations (adf_set_halo): -1 the tuner times both forms, 0 off (the default), 1 always
+  int halo_mode = 0;
+  int halo_items = 0;  // item numbers k_halo covers: n / 256 + W + 1
   int persist_cap[2] = {0, 0};       // co-resident blocks of k_cg_solve<false/true> on this device
   unsigned persist_extra = 0;        // extra arrivals a barrier waits for (only the wait-expiry test sets it)
   long long persist_wait = 1 << 22;  // polls of one barrier wait (about a second) before it gives up
@@ -246,17 +250,18 @@ void prof_end(adf_solver* s, cudaStream_t st) {
 }
 
 // A neighbour-loop kernel's instance: gathers in flight nb, with MS_FLAG when the model has box walls (solver s in scope)
-#define NB_DISPATCH(kern, nb, grid, block, st, ...)                                          \
-  do {                                                                                       \
-    switch ((nb) | (s->d.slot_cap > 1 ? MS_FLAG : 0)) {                                      \
-      case 4: kern<4><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;                       \
-      case 16: kern<16><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;                     \
-      case 4 | MS_FLAG: kern<4 | MS_FLAG><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;     \
-      case 8 | MS_FLAG: kern<8 | MS_FLAG><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;     \
-      case 16 | MS_FLAG: kern<16 | MS_FLAG><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;   \
-      default: kern<8><<<(grid), (block), 0, (st)>>>(__VA_ARGS__); break;                      \
-    }                                                                                        \
+#define NB_DISPATCH_SM(kern, nb, grid, block, smem, st, ...)                                          \
+  do {                                                                                                \
+    switch ((nb) | (s->d.slot_cap > 1 ? MS_FLAG : 0)) {                                               \
+      case 4: kern<4><<<(grid), (block), (smem), (st)>>>(__VA_ARGS__); break;                           \
+      case 16: kern<16><<<(grid), (block), (smem), (st)>>>(__VA_ARGS__); break;                         \
+      case 4 | MS_FLAG: kern<4 | MS_FLAG><<<(grid), (block), (smem), (st)>>>(__VA_ARGS__); break;         \
+      case 8 | MS_FLAG: kern<8 | MS_FLAG><<<(grid), (block), (smem), (st)>>>(__VA_ARGS__); break;         \
+      case 16 | MS_FLAG: kern<16 | MS_FLAG><<<(grid), (block), (smem), (st)>>>(__VA_ARGS__); break;       \
+      default: kern<8><<<(grid), (block), (smem), (st)>>>(__VA_ARGS__); break;                          \
+    }                                                                                                 \
   } while (0)
+#define NB_DISPATCH(kern, nb, grid, block, st, ...) NB_DISPATCH_SM(kern, nb, grid, block, 0, st, __VA_ARGS__)
 
 // A team kernel's instance (box walls or not)
 #define MS_DISPATCH(kern, grid, block, st, ...)                                                  \
@@ -272,8 +277,14 @@ void launch_tk(adf_solver* s, int id, const TuneCfg& c, cudaStream_t st, const D
   switch (id) {
     case TK_DENSITY: NB_DISPATCH(k_density_alpha, c.nb, blocks(n, c.block), c.block, st, P); break;
     case TK_SOLVE_INIT: NB_DISPATCH(k_solve_init, c.nb, blocks(n, c.block), c.block, st, P); break;
-    case TK_ACCEL: NB_DISPATCH(k_accel, c.nb, s->max_items, c.block, st, P); break;
-    case TK_JACOBI: NB_DISPATCH(k_jacobi, c.nb, s->max_items, c.block, st, P); break;
+    case TK_ACCEL:
+      if (c.halo) NB_DISPATCH_SM(k_accel_h, c.nb, s->max_items, c.block, HALO_SMEM_ACCEL, st, P);
+      else NB_DISPATCH(k_accel, c.nb, s->max_items, c.block, st, P);
+      break;
+    case TK_JACOBI:
+      if (c.halo) NB_DISPATCH_SM(k_jacobi_h, c.nb, s->max_items, c.block, HALO_SMEM_JACOBI, st, P);
+      else NB_DISPATCH(k_jacobi, c.nb, s->max_items, c.block, st, P);
+      break;
     case TK_LISTS:
       if (c.nb == 16) k_lists_union<16><<<blocks(n, 16 * LU_WARPS), 32 * LU_WARPS, 0, st>>>(P);
       else k_lists_union<32><<<blocks(n, 32 * LU_WARPS), 32 * LU_WARPS, 0, st>>>(P);
@@ -316,8 +327,13 @@ void tune_kernel(adf_solver* s, int id, cudaStream_t st, const DevP& P) {
   if (id == TK_LISTS) {
     for (int g : TUNE_PPW) cands.push_back(TuneCfg{32 * LU_WARPS, g});
   } else {
-    for (int block : TUNE_BLOCKS)
-      for (int nbv : TUNE_NB) cands.push_back(TuneCfg{block, nbv});
+    const bool staged = id == TK_ACCEL || id == TK_JACOBI;
+    for (int halo = 0; halo < 2; ++halo) {
+      if (halo && !staged) continue;
+      if (staged && s->halo_mode >= 0 && halo != s->halo_mode) continue;
+      for (int block : TUNE_BLOCKS)
+        for (int nbv : TUNE_NB) cands.push_back(TuneCfg{block, nbv, halo});
+    }
   }
   {
     for (const TuneCfg& c : cands) {
@@ -342,6 +358,15 @@ void tune_kernel(adf_solver* s, int id, cudaStream_t st, const DevP& P) {
   s->tune[id] = pick;
   s->tune_ms[id] = best;
   s->tuned[id] = true;
+}
+
+// Whether this step builds the item halos: always when forced on; with the tuner deciding, in the tuning step (its
+// trials time both forms) and whenever the acceleration or Jacobi choice is the staged form.
+bool halo_needed(const adf_solver* s) {
+  if (s->halo_mode == 0) return false;
+  if (s->halo_mode == 1) return true;
+  return (s->tuning && !(s->tuned[TK_ACCEL] && s->tuned[TK_JACOBI])) || s->tune[TK_ACCEL].halo ||
+         s->tune[TK_JACOBI].halo;
 }
 
 // A tuned kernel's launch at its place in the step (tuning it first when this is the tuning step).
@@ -462,6 +487,12 @@ int prepare(adf_solver* s, DevP& P, cudaStream_t st) {
   prof_begin(s, 3, st);
   run_tk(s, TK_DENSITY, st, P);
   prof_end(s, st);
+  if (halo_needed(s)) {
+    prof_begin(s, 13, st);
+    k_halo<<<s->halo_items, ITEM, HALO_SMEM_BUILD, st>>>(P);
+    ++s->launches;
+    prof_end(s, st);
+  }
   s->built = true;
   return check_launch();
 }
@@ -1006,6 +1037,11 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.nbr, (size_t)s->K * n);
   rc |= s->alloc(&d.nbrjf, (size_t)s->K * n);
   rc |= s->alloc(&d.nbrw, (size_t)s->K * n);
+  s->halo_items = (int)std::max<long long>((long long)n / ITEM + s->W + 1, 1);
+  rc |= s->alloc(&d.halo_n, (size_t)s->halo_items);
+  rc |= s->alloc(&d.halo_idx, (size_t)s->halo_items * HALO_CAP);
+  rc |= s->alloc(&d.halo_row, (size_t)s->K * n);
+  rc |= s->alloc(&d.halo_f, (size_t)s->K * n);
   rc |= s->alloc(&d.cnt, n);
   rc |= s->alloc(&d.slot_g, (size_t)d.slot_cap * n);
   rc |= s->alloc(&d.slot_vb, (size_t)d.slot_cap * n);
@@ -1248,6 +1284,16 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
                            (int)(sizeof(int) * (size_t)SKIN_SMEM_CAP * SKIN_THREADS)));
   CKC(cudaFuncSetAttribute(k_lists_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(sizeof(int) * (size_t)s->K * LS_THREADS)));
+  CKC(cudaFuncSetAttribute(k_halo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HALO_SMEM_BUILD));
+  CKC(cudaFuncSetAttribute(k_jacobi_h<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HALO_SMEM_JACOBI));
+  CKC(cudaFuncSetAttribute(k_jacobi_h<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HALO_SMEM_JACOBI));
+  CKC(cudaFuncSetAttribute(k_jacobi_h<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HALO_SMEM_JACOBI));
+  CKC(cudaFuncSetAttribute(k_jacobi_h<4 | MS_FLAG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)HALO_SMEM_JACOBI));
+  CKC(cudaFuncSetAttribute(k_jacobi_h<8 | MS_FLAG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)HALO_SMEM_JACOBI));
+  CKC(cudaFuncSetAttribute(k_jacobi_h<16 | MS_FLAG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)HALO_SMEM_JACOBI));
   CKC(cudaHostAlloc((void**)&s->pinned, 2 * sizeof(int), cudaHostAllocDefault));
   CKC(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
   CKC(cudaStreamCreateWithFlags(&s->body_stream, cudaStreamNonBlocking));
@@ -1667,6 +1713,40 @@ int adf_tuned_configs(adf_solver* s, int32_t* block, int32_t* nb, float* ms) {
     if (block) block[k] = s->tune[k].block;
     if (nb) nb[k] = s->tune[k].nb;
     if (ms) ms[k] = s->tuned[k] ? s->tune_ms[k] : -1.0f;
+  }
+  return ADF_OK;
+}
+
+int adf_set_halo(adf_solver* s, int mode) {
+  if (!s) return fail(ADF_ERR_VALUE, "adf_set_halo: null solver");
+  if (mode < -1 || mode > 1) return fail(ADF_ERR_VALUE, "adf_set_halo: mode is -1 (tuned), 0 (off) or 1 (on)");
+  s->halo_mode = mode;
+  for (int id : {TK_ACCEL, TK_JACOBI}) {
+    if (mode >= 0) s->tune[id].halo = mode;
+    else if (!s->tuned[id]) s->tune[id].halo = 0;
+  }
+  ++s->table_version;  // cached step graphs hold the other kernels
+  return ADF_OK;
+}
+
+int adf_halo_stats(adf_solver* s, int32_t* in_use, int64_t* stats, void* stream) {
+  if (!s || !in_use || !stats) return fail(ADF_ERR_VALUE, "adf_halo_stats: null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  in_use[0] = s->tune[TK_ACCEL].halo;
+  in_use[1] = s->tune[TK_JACOBI].halo;
+  for (int k = 0; k < 4; ++k) stats[k] = 0;
+  if (!s->built || !halo_needed(s)) return ADF_OK;
+  std::vector<int> h((size_t)s->halo_items);
+  CK(cudaMemcpyAsync(h.data(), s->d.halo_n, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int v : h) {
+    if (v > 0) {
+      ++stats[0];
+      stats[2] += v;
+      stats[3] = std::max<int64_t>(stats[3], v);
+    } else if (v < 0) {
+      ++stats[1];
+    }
   }
   return ADF_OK;
 }

@@ -9,6 +9,7 @@
 // ascending wall-particle id, and per-world float64 reductions run over the caller's particle order.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 
 #include "dfsph_math.cuh"
@@ -115,6 +116,12 @@ struct DevP {
   int2* nbrjf;  // [K][n] (row entry, bits of its gradient factor F(r_ij)), written by k_density_alpha
   float* nbrw;  // [K][n] kernel value W(r_ij) of each row entry, written by k_density_alpha, read by k_xsph
   int* cnt;
+  // Item halos of the pressure iterations (k_halo): per 256-particle work item g (world w, first particle b:
+  // g = b / 256 + w) the ascending sorted positions its rows address, and the rows as 16-bit indices into that list.
+  int* halo_n;              // [G] records of item g; -1: not staged (too many, or too wide a span)
+  int* halo_idx;            // [G][HALO_CAP] sorted positions
+  unsigned short* halo_row;  // [K][n] row entry as an index into its item's halo
+  float* halo_f;            // [K][n] the entry's F(r_ij), as in nbrjf
   // Boundary slots (boundary.py:36): slot b of sorted particle p at b * n + p of each array, nearest wall first.
   float4* slot_g;   // dPsi/dx (3), psi; with slot_cap 1, psi < 0: no slot
   float4* slot_vb;  // wall velocity (3), phi
@@ -1893,12 +1900,12 @@ __device__ __forceinline__ int build_worklist(const DevP& P, bool fresh) {
 __global__ void __launch_bounds__(1024) k_worklist(DevP P) { build_worklist(P, false); }
 
 // The sorted range [b, e) of this block's work item; false (for the whole block) past the last item.
-__device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
-  __shared__ int sb, se;
+__device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e, int& w) {
+  __shared__ int sb, se, sw;
   if (threadIdx.x == 0) {
     const int n = *P.n_cw;
     const int t = blockIdx.x;
-    sb = se = 0;
+    sb = se = sw = 0;
     if (n > 0 && t < P.cseg[n]) {
       int lo = 0, hi = n - 1;  // the last listed world whose first item is <= t
       while (lo < hi) {
@@ -1906,7 +1913,8 @@ __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
         if (P.cseg[mid] <= t) lo = mid;
         else hi = mid - 1;
       }
-      const int2 r = P.wrange[P.cw[lo]];
+      sw = P.cw[lo];
+      const int2 r = P.wrange[sw];
       sb = r.x + (t - P.cseg[lo]) * ITEM;
       se = min(sb + ITEM, r.y);
     }
@@ -1914,13 +1922,52 @@ __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
   __syncthreads();
   b = sb;
   e = se;
+  w = sw;
   return b < e;
 }
 
+__device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e) {
+  int w;
+  return work_item(P, b, e, w);
+}
+
 // ------------------------------------------------------------------------------------------ Jacobi sweep
+// Where the pressure loops read a row and the neighbours' records: the rows in HBM and the particle arrays
+// (GlobalRows), or the work item's halo staged in shared memory, addressed by 16-bit row entries (HaloRows). Both give
+// every entry the same values, so the sums are the same bits.
+struct GlobalRows {
+  template <int NB>
+  __device__ __forceinline__ void row(const DevP& P, int p, int c, int k, int (&j)[NB], float (&f)[NB]) const {
+    load_row_batch_f(P, p, c, k, j, f);
+  }
+  __device__ __forceinline__ float4 pos(const DevP& P, int j) const { return P.pos[j]; }
+  __device__ __forceinline__ float4 acc(const DevP& P, int j) const { return P.acc[j]; }
+  __device__ __forceinline__ float kr(const DevP& P, int j) const { return P.kr[j]; }
+};
+
+struct HaloRows {
+  const float4* hpos;  // [H] positions of the item's halo
+  const float4* hacc;  // [H] accelerations (Jacobi) or nullptr
+  const float* hkr;    // [H] kappa / rho0 (acceleration) or nullptr
+  // Entries past the row's end read record 0 (a row with entries implies a halo of at least one) and are skipped.
+  template <int NB>
+  __device__ __forceinline__ void row(const DevP& P, int p, int c, int k, int (&j)[NB], float (&f)[NB]) const {
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+      const size_t o = (size_t)(k + u) * P.n + p;
+      j[u] = (k + u < c) ? (int)__ldcs(P.halo_row + o) : 0;
+      f[u] = (k + u < c) ? __ldcs(P.halo_f + o) : 0.0f;
+    }
+  }
+  __device__ __forceinline__ float4 pos(const DevP&, int j) const { return hpos[j]; }
+  __device__ __forceinline__ float4 acc(const DevP&, int j) const { return hacc[j]; }
+  __device__ __forceinline__ float kr(const DevP&, int j) const { return hkr[j]; }
+};
+
 // pressure.py:264-291: a_i = -sum_j m_j (k_i/rho0_i + k_j/rho0_j) grad W_ij - k_i sum_b dPsi_b
-template <int NBX>
-__device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, float& ax, float& ay, float& az) {
+template <int NBX, class R = GlobalRows>
+__device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, float& ax, float& ay, float& az,
+                                               const R& src = R()) {
   constexpr int NB = NBX & NB_MASK;
   constexpr bool MS = (NBX & MS_FLAG) != 0;
   float ki = P.kr[p];
@@ -1929,13 +1976,13 @@ __device__ __forceinline__ void pressure_accel(const DevP& P, int p, float4 xi, 
   for (int k = 0; k < c; k += NB) {
     int j[NB];
     float fb[NB];
-    load_row_batch_f(P, p, c, k, j, fb);
+    src.template row<NB>(P, p, c, k, j, fb);
     float4 xb[NB];
     float kb[NB];
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
-      xb[u] = P.pos[j[u]];
-      kb[u] = P.kr[j[u]];
+      xb[u] = src.pos(P, j[u]);
+      kb[u] = src.kr(P, j[u]);
     }
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
@@ -1970,8 +2017,8 @@ __global__ void __launch_bounds__(BLOCK) k_accel(DevP P) {
 
 // pressure.py:294-352
 // pressure.py:294-310: Ar_i of the accelerations in P.acc (the matrix-free product, before the compliance term)
-template <int NBX>
-__device__ __forceinline__ float accel_divergence(const DevP& P, int p, float inv_r0) {
+template <int NBX, class R = GlobalRows>
+__device__ __forceinline__ float accel_divergence(const DevP& P, int p, float inv_r0, const R& src = R()) {
   constexpr int NB = NBX & NB_MASK;
   constexpr bool MS = (NBX & MS_FLAG) != 0;
   float4 xi = P.pos[p];
@@ -1981,12 +2028,12 @@ __device__ __forceinline__ float accel_divergence(const DevP& P, int p, float in
   for (int k = 0; k < c; k += NB) {
     int j[NB];
     float fb[NB];
-    load_row_batch_f(P, p, c, k, j, fb);
+    src.template row<NB>(P, p, c, k, j, fb);
     float4 xb[NB], ab[NB];
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
-      xb[u] = P.pos[j[u]];
-      ab[u] = P.acc[j[u]];
+      xb[u] = src.pos(P, j[u]);
+      ab[u] = src.acc(P, j[u]);
     }
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
@@ -2004,11 +2051,11 @@ __device__ __forceinline__ float accel_divergence(const DevP& P, int p, float in
   return ar;
 }
 
-template <int NBX>
-__device__ __forceinline__ void jacobi_one(const DevP& P, int p) {
+template <int NBX, class R = GlobalRows>
+__device__ __forceinline__ void jacobi_one(const DevP& P, int p, const R& src = R()) {
   float r0 = P.vel[p].w;
   float inv_r0 = 1.0f / r0;
-  float ar = accel_divergence<NBX>(P, p, inv_r0);
+  float ar = accel_divergence<NBX>(P, p, inv_r0, src);
   float kap = P.kappa[p];
   ar = ADF_FMA(-P.reg[p], kap, ar);
   const float dt = P.dt;
@@ -2037,6 +2084,217 @@ __global__ void __launch_bounds__(BLOCK) k_jacobi(DevP P) {
   if (!work_item(P, b, e)) return;
   for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one<NBX>(P, p);
 }
+
+// ------------------------------------------------------------------------------------ item halos
+// The pressure iterations run one block per 256-particle work item (the item's particles are a compact brick of
+// cells in the sorted order). Each row entry gathers two 16-byte records from scattered sorted positions, which is
+// what bounds those loops in L1. k_halo, once per step after the rows' F are written, lists per item the distinct
+// sorted positions its rows address (ascending: liquid, then walls) and rewrites the rows as 16-bit indices into
+// that list with F beside them; the staged kernels then copy the item's records into shared memory with runs of
+// consecutive loads and gather from there. Items are numbered g = b / 256 + w for the item of world w starting at
+// sorted position b, which is strictly increasing over worlds and items and below nf / 256 + W + 1.
+constexpr int HALO_CAP = 1280;    // records an item stages (20 KB of positions + 20 KB of accelerations)
+constexpr int HALO_WORDS = 8192;  // bitmap words over the two spans of sorted positions an item addresses
+
+__device__ __forceinline__ int halo_first(const DevP& P, int w) { return P.wrange[w].x / ITEM + w; }
+
+__device__ __forceinline__ void block_min_max(int& lo, int& hi, int* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&red[0], lo);
+    atomicMax(&red[1], hi);
+  }
+}
+
+// One block of 256 threads per item number g (numbers between worlds' items are idle); dynamic shared memory:
+// HALO_WORDS bitmap words and HALO_WORDS prefix counts.
+__global__ void __launch_bounds__(ITEM) k_halo(DevP P) {
+  extern __shared__ unsigned int hsm[];
+  unsigned int* bits = hsm;
+  unsigned int* pre = hsm + HALO_WORDS;
+  __shared__ int sb, se, red[4], scan_smem[32];
+  const int g = blockIdx.x;
+  if (threadIdx.x == 0) {
+    sb = se = 0;
+    red[0] = red[2] = INT_MAX;
+    red[1] = red[3] = -1;
+    int lo = 0, hi = P.W - 1;  // the last world whose first item number is <= g
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (halo_first(P, mid) <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    if (P.W > 0 && halo_first(P, lo) <= g) {
+      const int2 r = P.wrange[lo];
+      const int t = g - halo_first(P, lo);
+      if (r.x + t * ITEM < r.y) {
+        sb = r.x + t * ITEM;
+        se = min(sb + ITEM, r.y);
+      }
+    }
+  }
+  __syncthreads();
+  const int b = sb, e = se;
+  if (b >= e) return;
+  const int nf = P.nfw[0];
+  const size_t n = (size_t)P.n;
+  // the spans of liquid and wall positions the item's rows address
+  int llo = INT_MAX, lhi = -1, wlo = INT_MAX, whi = -1;
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
+    const int c = P.cnt[p];
+    for (int k = 0; k < c; ++k) {
+      const int j = P.nbrjf[k * n + p].x;
+      if (j < nf) {
+        llo = min(llo, j);
+        lhi = max(lhi, j);
+      } else {
+        wlo = min(wlo, j);
+        whi = max(whi, j);
+      }
+    }
+  }
+  block_min_max(llo, lhi, red);
+  block_min_max(wlo, whi, red + 2);
+  __syncthreads();
+  const int lwords = red[1] >= 0 ? (red[1] - red[0]) / 32 + 1 : 0;
+  const int wwords = red[3] >= 0 ? (red[3] - red[2]) / 32 + 1 : 0;
+  const int words = lwords + wwords;
+  if (words > HALO_WORDS) {
+    if (threadIdx.x == 0) P.halo_n[g] = -1;
+    return;
+  }
+  const int l0 = red[0], w0 = red[2];
+  for (int i = threadIdx.x; i < words; i += blockDim.x) bits[i] = 0u;
+  __syncthreads();
+  auto bit_of = [&](int j) { return j < nf ? j - l0 : lwords * 32 + (j - w0); };
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
+    const int c = P.cnt[p];
+    for (int k = 0; k < c; ++k) {
+      const int x = bit_of(P.nbrjf[k * n + p].x);
+      atomicOr(&bits[x >> 5], 1u << (x & 31));
+    }
+  }
+  __syncthreads();
+  // each thread owns a run of words: their popcounts, the block's exclusive scan, then each word's prefix
+  const int per = (words + blockDim.x - 1) / blockDim.x;
+  const int w_beg = min(words, (int)threadIdx.x * per), w_end = min(words, w_beg + per);
+  int cntw = 0;
+  for (int i = w_beg; i < w_end; ++i) cntw += __popc(bits[i]);
+  int total;
+  int off = block_exclusive_scan(cntw, scan_smem, total);
+  if (total > HALO_CAP) {
+    if (threadIdx.x == 0) P.halo_n[g] = -1;
+    return;
+  }
+  int* hidx = P.halo_idx + (size_t)g * HALO_CAP;
+  for (int i = w_beg; i < w_end; ++i) {
+    pre[i] = (unsigned int)off;
+    unsigned int m = bits[i];
+    const int base = i < lwords ? l0 + i * 32 : w0 + (i - lwords) * 32;
+    while (m) {
+      const int t = __ffs(m) - 1;
+      hidx[off++] = base + t;
+      m &= m - 1u;
+    }
+  }
+  __syncthreads();
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
+    const int c = P.cnt[p];
+    for (int k = 0; k < c; ++k) {
+      const int2 jf = P.nbrjf[k * n + p];
+      const int x = bit_of(jf.x);
+      const unsigned int below = bits[x >> 5] & ((1u << (x & 31)) - 1u);
+      P.halo_row[k * n + p] = (unsigned short)(pre[x >> 5] + __popc(below));
+      P.halo_f[k * n + p] = __int_as_float(jf.y);
+    }
+  }
+  if (threadIdx.x == 0) P.halo_n[g] = total;
+}
+
+// Copies item g's H records into shared memory, four per thread in flight: positions into hpos, src2's records
+// (accelerations or kappa / rho0) into h2.
+template <class T>
+__device__ __forceinline__ void stage_halo(const DevP& P, int g, int H, float4* hpos, const T* src2, T* h2) {
+  const int* hidx = P.halo_idx + (size_t)g * HALO_CAP;
+  constexpr int U = 4;
+  for (int i0 = threadIdx.x; i0 < H; i0 += U * blockDim.x) {
+    int j[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * (int)blockDim.x;
+      j[u] = i < H ? __ldg(hidx + i) : -1;
+    }
+    float4 x[U];
+    T y[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (j[u] >= 0) {
+        x[u] = P.pos[j[u]];
+        y[u] = src2[j[u]];
+      }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (j[u] >= 0) {
+        const int i = i0 + u * (int)blockDim.x;
+        hpos[i] = x[u];
+        h2[i] = y[u];
+      }
+  }
+  __syncthreads();
+}
+
+// The staged pressure iterations (same work items and arithmetic as k_accel and k_jacobi): an item without a halo
+// takes the global gathers. Dynamic shared memory: HALO_CAP float4 positions, then HALO_CAP float4 accelerations
+// (Jacobi) or HALO_CAP floats of kappa / rho0 (acceleration).
+template <int NBX>
+__global__ void __launch_bounds__(BLOCK) k_accel_h(DevP P) {
+  extern __shared__ float4 hrec[];
+  int b, e, w;
+  if (!work_item(P, b, e, w)) return;
+  const int g = b / ITEM + w;
+  const int H = P.halo_n[g];
+  if (H < 0) {
+    for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
+      float ax, ay, az;
+      pressure_accel<NBX>(P, p, P.pos[p], ax, ay, az);
+      P.acc[p] = make_float4(ax, ay, az, 0.0f);
+    }
+    return;
+  }
+  float* hkr = reinterpret_cast<float*>(hrec + HALO_CAP);
+  stage_halo(P, g, H, hrec, (const float*)P.kr, hkr);
+  const HaloRows src{hrec, nullptr, hkr};
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) {
+    float ax, ay, az;
+    pressure_accel<NBX>(P, p, P.pos[p], ax, ay, az, src);
+    P.acc[p] = make_float4(ax, ay, az, 0.0f);
+  }
+}
+
+template <int NBX>
+__global__ void __launch_bounds__(BLOCK) k_jacobi_h(DevP P) {
+  extern __shared__ float4 hrec[];
+  int b, e, w;
+  if (!work_item(P, b, e, w)) return;
+  const int g = b / ITEM + w;
+  const int H = P.halo_n[g];
+  if (H < 0) {
+    for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one<NBX>(P, p);
+    return;
+  }
+  float4* hacc = hrec + HALO_CAP;
+  stage_halo(P, g, H, hrec, (const float4*)P.acc, hacc);
+  const HaloRows src{hrec, hacc, nullptr};
+  for (int p = b + threadIdx.x; p < e; p += blockDim.x) jacobi_one<NBX>(P, p, src);
+}
+
+constexpr size_t HALO_SMEM_BUILD = 2 * HALO_WORDS * sizeof(unsigned int);
+constexpr size_t HALO_SMEM_ACCEL = HALO_CAP * (sizeof(float4) + sizeof(float));
+constexpr size_t HALO_SMEM_JACOBI = HALO_CAP * 2 * sizeof(float4);
 
 // ------------------------------------------------------------------------------------ projected CG (krylov.py)
 // One CG per world on w = A k - b, k >= k_lo (krylov.py:1-17), A k = -dt^n (Ar(k) - reg k). Each kernel follows

@@ -437,6 +437,21 @@ class SolverDFSPH:
         slightly faster). The results are the same bits either way."""
         _lib.check(self._lib.adf_set_persistent(self._h, int(bool(enable))), "persistent")
 
+    def halo(self, mode: int = 1) -> None:
+        """Item halos of the Jacobi iterations (include/alloy_dfsph.h adf_set_halo): 1 staged, 0 global gathers (the
+        default, measured faster), -1 the autotuner times both forms for the acceleration and Jacobi kernels. Same
+        bits either way."""
+        _lib.check(self._lib.adf_set_halo(self._h, int(mode)), "halo")
+
+    def halo_stats(self) -> dict:
+        """The halo choice in use and, after a step that built them, the items staged and left on global gathers,
+        the staged records summed and the largest item's (adf_halo_stats)."""
+        use = np.zeros(2, np.int32)
+        st = np.zeros(4, np.int64)
+        _lib.check(self._lib.adf_halo_stats(self._h, use.ctypes.data, st.ctypes.data, self._stream()), "halo_stats")
+        return {"accel": bool(use[0]), "jacobi": bool(use[1]), "staged": int(st[0]), "global": int(st[1]),
+                "records": int(st[2]), "max_records": int(st[3])}
+
     def barrier_wait(self, polls: int = 1 << 22, extra_arrivals: int = 0) -> None:
         """Test hook of the persistent solve's bounded barrier waits (adf_set_barrier_wait): polls per wait, and
         arrivals a barrier waits for beyond the grid's blocks (nonzero makes every wait run out)."""

@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--no-warm", action="store_true", help="skip the arms beside the headline (plain or learned, CG, "
                                                               "per-world, FP64 check)")
     ap.add_argument("--plain", action="store_true", help="headline the plain solve instead of the warm-started one")
+    ap.add_argument("--halo", type=int, choices=(-1, 0, 1), default=0,
+                    help="item halos of the Jacobi iterations: 0 global gathers (the library's default), 1 staged, "
+                         "-1 the autotuner decides")
     ap.add_argument("--warm-model", default=None, help="a warm-start network file (.npz) instead of the shipped one")
     return ap.parse_args()
 
@@ -316,7 +319,8 @@ class Clocks:
         return bool(sm and mx and sm < 0.6 * mx and not clk.get("reasons"))
 
 
-KERNEL_NAMES = {"k_jacobi": "jacobi", "k_accel": "accel", "k_density_alpha": "density_alpha",
+KERNEL_NAMES = {"k_jacobi": "jacobi", "k_accel": "accel", "k_jacobi_h": "jacobi", "k_accel_h": "accel",
+                "k_halo": "halo", "k_density_alpha": "density_alpha",
                 "k_solve_init": "solve_init", "k_apply": "apply", "k_xsph": "xsph", "k_lists_union": "lists",
                 "k_wall_slots": "wall_slots", "k_finish": "finish"}
 
@@ -412,6 +416,7 @@ def variant_arm(args, dev, rank: int, world: int, judge: bool | None = None, **c
     full = make_scene(args.workload, dev, **cfg_kw)
     sc = rank_scene(full, args.workload, rank, world, dev)
     sol = SolverDFSPH(sc.model, sc.config)
+    sol.halo(args.halo)
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
     if judge is not None:
         sol.set_warm_model(warm_model(args))
@@ -617,6 +622,7 @@ def run_b200(args):
     sc = rank_scene(full, args.workload, rank, world, dev)
     note(f"solver for {sc.model.particle_count} particles")
     sol = SolverDFSPH(sc.model, sc.config)
+    sol.halo(args.halo)
     sol.add_emitters([(w, centre, half, rate, vel, pool) for w, centre, half, rate, vel, pool, _, _ in spouts(sc)])
     headline_warm = not args.plain
     if headline_warm:  # the shipped network's starts, judged by the first sweep against the plain start per world
@@ -757,6 +763,7 @@ def run_b200(args):
     nf, entries = sol.list_stats()
     nbar = entries / max(nf, 1)
     tuned = sol.tuned_configs()  # chosen in the first warm-up step
+    halo = sol.halo_stats()  # the item-halo choice and, for the last step, items staged and records
     pk = peaks()
     # algorithmic bytes per liquid particle and launch (element sizes of the reference, 2-byte list entries)
     alg = {"jacobi": 72.0 + 2.0 * nbar, "accel": 44.0 + 2.0 * nbar, "density_alpha": 52.0 + 2.0 * nbar,
@@ -856,7 +863,7 @@ def run_b200(args):
             "solver_stats": {"iters_density_mean": float(np.mean(it_den)), "iters_divergence_mean":
                              float(np.mean(it_div)), "density_err_mean_max_over_steps": float(np.max(den_err)),
                              "density_err_max_last_step": den_max[-1]},
-            **warm, "autotuned": tuned, "cpu_baseline": cpu, "clocks": clk}
+            **warm, "autotuned": tuned, "halo": halo, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

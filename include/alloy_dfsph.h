@@ -160,6 +160,23 @@ int adf_set_tuned_config(adf_solver* solver, int kernel, int block, int nb);
  * gathers in flight, and the winning trial's milliseconds (-1 if not tuned). */
 int adf_tuned_configs(adf_solver* solver, int32_t* block, int32_t* nb, float* ms);
 
+/* Item halos of the Jacobi iterations (no reference counterpart; the reference gathers every neighbour from global
+ * memory, pressure.py:264-352). The pressure acceleration and the Jacobi update run one block per 256-particle work
+ * item; with halos, a kernel after the density pass lists per item the distinct particles its neighbour rows address
+ * (at most 1,280) and rewrites the rows as 16-bit indices into that list, and the two kernels copy each item's records
+ * into shared memory and gather from there. Items whose rows address more particles, or too wide a range of sorted
+ * positions, keep the global gathers. Results are the same bits either way. mode 0 (the default at creation): global
+ * gathers; 1: halos; -1: the autotuner times both forms with the other choices (its trials leave out the halo build,
+ * which runs once per step). On a B200 the halos measured slower: the global gathers already hit L1 for about three
+ * in four entries, and the staging and the build cost more than the gathers they take off L1 (1M-particle dam
+ * break: 2.73 against 2.45 ms per step; the 4,096-world pour: 63.4 against 55.4 ms). */
+int adf_set_halo(adf_solver* solver, int mode);
+
+/* The halo choice in use (host int32[2]: acceleration, Jacobi; 1 = staged) and, after a step that built the halos,
+ * host int64[4]: items staged, items left on global gathers, staged records summed over items, the largest item's
+ * records. Synchronises `stream`. */
+int adf_halo_stats(adf_solver* solver, int32_t* in_use, int64_t* stats, void* stream);
+
 /* Persistent CG solve (no reference counterpart; the reference launches each CG kernel per iteration, krylov.py:254-297,
  * inside wp.capture_while, solve_driver.py:186). With the projected CG on models of at most 131,072 particles, each
  * pressure solve (its start and every iteration) runs as ONE cooperative launch whose phases are separated by
@@ -414,10 +431,10 @@ int64_t adf_kernel_launches(const adf_solver* solver);
 /* Live kernel timing with CUDA events on the launch stream (benchmarks). Kinds, in this order: 0 sort (classify,
  * scan, scatter), 1 neighbour rows, 2 wall slots, 3 density and factor, 4 solve start, 5 pressure acceleration,
  * 6 Jacobi update, 7 per-world reduction and stop test, 8 apply pressure, 9 XSPH, 10 advect/project/write-back,
- * 11 emitters, 12 warm-start network and learned start. adf_profile_read synchronises, returns the summed
+ * 11 emitters, 12 warm-start network and learned start, 13 item halos. adf_profile_read synchronises, returns the summed
  * milliseconds and launch counts per kind since the last read (host arrays of ADF_PROF_KINDS) and starts a new
  * window. */
-#define ADF_PROF_KINDS 13
+#define ADF_PROF_KINDS 14
 int adf_profile_enable(adf_solver* solver, int enable);
 int adf_profile_read(adf_solver* solver, double* ms, int64_t* launches);
 
