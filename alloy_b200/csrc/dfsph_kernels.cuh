@@ -1900,23 +1900,31 @@ __device__ __forceinline__ int build_worklist(const DevP& P, bool fresh) {
 __global__ void __launch_bounds__(1024) k_worklist(DevP P) { build_worklist(P, false); }
 
 // The sorted range [b, e) of this block's work item; false (for the whole block) past the last item.
+// The first warp searches the listed worlds 32 probes at a time (cseg rises strictly over listed worlds, so the probes
+// at or below t form a prefix of the lanes): about log32 of the worlds rounds of one load per lane.
 __device__ __forceinline__ bool work_item(const DevP& P, int& b, int& e, int& w) {
   __shared__ int sb, se, sw;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
     const int n = *P.n_cw;
     const int t = blockIdx.x;
-    sb = se = sw = 0;
+    if (lane == 0) sb = se = sw = 0;
     if (n > 0 && t < P.cseg[n]) {
-      int lo = 0, hi = n - 1;  // the last listed world whose first item is <= t
+      int lo = 0, hi = n - 1;  // the last listed world whose first item is <= t lies in [lo, hi]
       while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (P.cseg[mid] <= t) lo = mid;
-        else hi = mid - 1;
+        const int step = (hi - lo + 31) >> 5;
+        const int q = lo + (lane + 1) * step;
+        const unsigned below = __ballot_sync(0xffffffffu, q <= hi && P.cseg[q] <= t);
+        const int k = __popc(below);
+        hi = min(hi, lo + (k + 1) * step - 1);
+        lo = lo + k * step;
       }
-      sw = P.cw[lo];
-      const int2 r = P.wrange[sw];
-      sb = r.x + (t - P.cseg[lo]) * ITEM;
-      se = min(sb + ITEM, r.y);
+      if (lane == 0) {
+        sw = P.cw[lo];
+        const int2 r = P.wrange[sw];
+        sb = r.x + (t - P.cseg[lo]) * ITEM;
+        se = min(sb + ITEM, r.y);
+      }
     }
   }
   __syncthreads();
