@@ -1037,11 +1037,7 @@ int adf_create(const adf_params* params, const adf_model* m, int device, adf_sol
   rc |= s->alloc(&d.nbr, (size_t)s->K * n);
   rc |= s->alloc(&d.nbrjf, (size_t)s->K * n);
   rc |= s->alloc(&d.nbrw, (size_t)s->K * n);
-  s->halo_items = (int)std::max<long long>((long long)n / ITEM + s->W + 1, 1);
-  rc |= s->alloc(&d.halo_n, (size_t)s->halo_items);
-  rc |= s->alloc(&d.halo_idx, (size_t)s->halo_items * HALO_CAP);
-  rc |= s->alloc(&d.halo_row, (size_t)s->K * n);
-  rc |= s->alloc(&d.halo_f, (size_t)s->K * n);
+  s->halo_items = (int)std::max<long long>((long long)n / ITEM + s->W + 1, 1);  // buffers: adf_set_halo
   rc |= s->alloc(&d.cnt, n);
   rc |= s->alloc(&d.slot_g, (size_t)d.slot_cap * n);
   rc |= s->alloc(&d.slot_vb, (size_t)d.slot_cap * n);
@@ -1720,6 +1716,21 @@ int adf_tuned_configs(adf_solver* s, int32_t* block, int32_t* nb, float* ms) {
 int adf_set_halo(adf_solver* s, int mode) {
   if (!s) return fail(ADF_ERR_VALUE, "adf_set_halo: null solver");
   if (mode < -1 || mode > 1) return fail(ADF_ERR_VALUE, "adf_set_halo: mode is -1 (tuned), 0 (off) or 1 (on)");
+  if (mode != 0 && s->d.halo_f == nullptr) {  // the halo buffers exist only once halos may run: 6 bytes a row entry
+    CK(cudaSetDevice(s->device));
+    const size_t n = (size_t)std::max(s->n, 1), items = (size_t)s->halo_items;
+    int* hn = nullptr;
+    int* hi = nullptr;
+    unsigned short* hr = nullptr;
+    float* hf = nullptr;
+    if (s->alloc(&hn, items) != ADF_OK || s->alloc(&hi, items * HALO_CAP) != ADF_OK ||
+        s->alloc(&hr, (size_t)s->K * n) != ADF_OK || s->alloc(&hf, (size_t)s->K * n) != ADF_OK)
+      return fail(ADF_ERR_CAPACITY, "adf_set_halo: out of device memory for the item halos");
+    s->d.halo_n = hn;  // all four or none (what did get allocated is freed with the solver)
+    s->d.halo_idx = hi;
+    s->d.halo_row = hr;
+    s->d.halo_f = hf;
+  }
   s->halo_mode = mode;
   for (int id : {TK_ACCEL, TK_JACOBI}) {
     if (mode >= 0) s->tune[id].halo = mode;

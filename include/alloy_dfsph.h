@@ -169,7 +169,9 @@ int adf_tuned_configs(adf_solver* solver, int32_t* block, int32_t* nb, float* ms
  * gathers; 1: halos; -1: the autotuner times both forms with the other choices (its trials leave out the halo build,
  * which runs once per step). On a B200 the halos measured slower: the global gathers already hit L1 for about three
  * in four sectors, while the staged kernels' copy-in misses L1 and their shared memory halves the resident warps
- * (1M-particle dam break: 2.73 against 2.45 ms per step; the 4,096-world pour: 63.4 against 55.4 ms). */
+ * (1M-particle dam break: 2.73 against 2.45 ms per step; the 4,096-world pour: 63.4 against 55.4 ms). The first
+ * call with a nonzero mode allocates the halo buffers (6 bytes per row entry of the particle capacity, 5 KB per item)
+ * and returns ADF_ERR_CAPACITY, leaving the mode unchanged, if the device has no room for them. */
 int adf_set_halo(adf_solver* solver, int mode);
 
 /* The halo choice in use (host int32[2]: acceleration, Jacobi; 1 = staged) and, after a step that built the halos,
